@@ -1,0 +1,317 @@
+"""Python API of the B200 search path, mirroring the reference's host API.
+
+    Gpu(device)                      <- Gpu::new            src/search/scan.rs:66-77
+    Gpu.upload(state)                <- DeviceReady::upload src/search/scan.rs:110-124
+    Gpu.scan_periods(dev, p, bank)   <- scan_periods        src/search/scan.rs:363-408
+    Gpu.scan_bank(dev, p, bank, nb)  <- scan_bank           src/search/scan.rs:144-357
+    Gpu.signal_search(state, cfg)    <- signal_search       src/search/scan.rs:413-473
+    Gpu.compare_search(state, P, cfg)<- compare_search      src/search/evidence.rs:693-1003
+    family_state(...)                <- family_state        src/prep/curve.rs:541-569
+    prepared_family(...)             <- search_prepared's preparation, src/pipeline.rs:41-68
+    period_grid(...)                 <- period_grid         src/search/grid.rs:5-28
+
+Every call goes through the C ABI of libfbls_b200.so; errors raise FblsError
+with the library's message (the reference's text where it has one).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import math
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _native as N
+from .config import SearchConfig
+
+ROW_FIELDS = ("period", "epoch", "duration", "score", "depth")
+
+
+class FblsError(RuntimeError):
+    """Error raised by the native library (status code and message)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(N.c_double_p)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+@dataclasses.dataclass
+class Bank:
+    """Template bank of one band; mirrors Bank (scan.rs:127-139)."""
+    durations: Sequence[float]
+    rho: Sequence[float]
+    ingress: Sequence[float] = (0.0, 0.2, 0.45)
+    layers: int = 4
+    threshold: float = 7.1
+    shape_gate: float = 0.6 * 7.1
+    phase_oversample: int = 4
+    period_batch: int = 4096
+    max_fold_mib: float = 1024.0
+    prescan_factor: int = 2
+    prescan_fraction: float = 0.7
+
+    def _native(self):
+        d, r, g = _f64(self.durations), _f64(self.rho), _f64(self.ingress)
+        b = N.Bank(_dptr(d), _dptr(r), len(d), _dptr(g), len(g), self.layers, self.threshold, self.shape_gate,
+                   self.phase_oversample, self.period_batch, self.max_fold_mib, self.prescan_factor,
+                   self.prescan_fraction)
+        return b, (d, r, g)
+
+
+@dataclasses.dataclass
+class FamilyState:
+    """Prepared family: the Ready fields (curve.rs:46-54) and rho."""
+    time: np.ndarray        # relative to origin, ascending
+    v: np.ndarray
+    w: np.ndarray
+    baseline_norm: float
+    origin: float
+    residual_energy: float
+    durations: np.ndarray   # days, family order
+    rho: np.ndarray
+    inflation: float = 1.0
+    segments: int = 1
+
+    @property
+    def n(self) -> int:
+        return int(self.time.shape[0])
+
+
+def _config(cfg: SearchConfig):
+    ing = _f64(cfg.ingress_fractions)
+    c = N.Config(cfg.period_min, cfg.period_max, cfg.threshold, _dptr(ing), len(ing), cfg.shape_layers,
+                 cfg.phase_oversample, cfg.shape_gate_fraction, cfg.prescan_factor, cfg.prescan_fraction,
+                 cfg.period_oversample, cfg.period_batch, cfg.max_fold_mib, cfg.evidence_rtol, cfg.planet_prior,
+                 cfg.binary_prior, cfg.planet_depth_scale, cfg.binary_depth_scale, cfg.diluted_binary_depth_scale,
+                 math.nan if cfg.stellar_radius_solar is None else cfg.stellar_radius_solar,
+                 cfg.planet_radius_scale_rj, cfg.target_flux_fraction, int(cfg.precision_mode))
+    return c, ing
+
+
+def period_grid(minimum: float, maximum: float, baseline: float, minimum_duration: float,
+                oversample: float) -> np.ndarray:
+    lib = N.load()
+    count = lib.fbls_period_grid(minimum, maximum, baseline, minimum_duration, oversample, None, 0)
+    out = np.empty(count, dtype=np.float64)
+    lib.fbls_period_grid(minimum, maximum, baseline, minimum_duration, oversample, _dptr(out), count)
+    return out
+
+
+def family_state(time, flux, sigma, durations_days: Sequence[float], correlated: bool = True) -> FamilyState:
+    """family_state of a prepared curve (detrended relative flux, transits
+    negative, per-point errors): noise model, precision fields and rho."""
+    lib = N.load()
+    t, f, s = _f64(time), _f64(flux), _f64(sigma)
+    d = _f64(durations_days)
+    n_in = t.shape[0]
+    n_out = C.c_uint32(0)
+    to, vo, wo = (np.empty(max(n_in, 1)) for _ in range(3))
+    scal = np.empty(5)
+    rho = np.empty(max(len(d), 1))
+    err = C.create_string_buffer(256)
+    rc = lib.fbls_family_state(_dptr(t), _dptr(f), _dptr(s), n_in, _dptr(d), len(d), int(correlated),
+                               C.byref(n_out), _dptr(to), _dptr(vo), _dptr(wo), _dptr(scal), _dptr(rho), err, 256)
+    if rc:
+        raise FblsError(rc, err.value.decode())
+    n = n_out.value
+    return FamilyState(to[:n].copy(), vo[:n].copy(), wo[:n].copy(), float(scal[0]), float(scal[1]), float(scal[2]),
+                       d.copy(), rho[:len(d)].copy(), float(scal[3]), int(scal[4]))
+
+
+def prepared_family(time, flux, flux_err, cfg: SearchConfig) -> FamilyState:
+    """search_prepared's single family holding every duration (pipeline.rs:41-68)."""
+    return family_state(time, flux, flux_err, cfg.durations_days(), cfg.correlated_noise)
+
+
+class DeviceReady:
+    """A family's fields resident on the GPU (DeviceReady, scan.rs:101-124)."""
+
+    def __init__(self, gpu: "Gpu", handle: int, state: FamilyState):
+        self.gpu = gpu
+        self.handle = handle
+        self.n = state.n
+        self.origin = state.origin
+        self.baseline_norm = state.baseline_norm
+
+    def free(self) -> None:
+        if self.handle:
+            N.load().fbls_free_ready(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Gpu:
+    """One device context and stream (Gpu, scan.rs:39-99)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = N.load()
+        status = C.c_int(0)
+        self.ctx = self.lib.fbls_create(device, C.byref(status))
+        if not self.ctx:
+            raise FblsError(status.value, f"cannot create a context on device {device}")
+        self.device = device
+
+    def close(self) -> None:
+        if self.ctx:
+            self.lib.fbls_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            raise FblsError(rc, self.lib.fbls_last_error(self.ctx).decode())
+
+    def timer_start(self) -> None:
+        """Records a CUDA event on the context's stream."""
+        self._check(self.lib.fbls_timer_start(self.ctx))
+
+    def timer_stop(self) -> float:
+        """Milliseconds of device time on the context's stream since timer_start."""
+        ms = C.c_float(0.0)
+        self._check(self.lib.fbls_timer_stop(self.ctx, C.byref(ms)))
+        return float(ms.value)
+
+    def set_kernel_timing(self, enable: bool) -> None:
+        self._check(self.lib.fbls_set_kernel_timing(self.ctx, int(enable)))
+
+    def counters(self, reset: bool = False) -> dict:
+        c = N.Counters()
+        self._check(self.lib.fbls_read_counters(self.ctx, C.byref(c), int(reset)))
+        return c.as_dict()
+
+    def upload(self, state: FamilyState) -> DeviceReady:
+        t, v, w = _f64(state.time), _f64(state.v), _f64(state.w)
+        h = C.c_void_p()
+        self._check(self.lib.fbls_upload_ready(self.ctx, _dptr(t), _dptr(v), _dptr(w), t.shape[0],
+                                               state.baseline_norm, state.origin, state.residual_energy,
+                                               C.byref(h)))
+        return DeviceReady(self, h.value, state)
+
+    def scan_bank(self, dev: DeviceReady, periods, bank: Bank, nb: int, precision_mode: int = 0):
+        """Every period's winner at nb bins: (records Px9, score, depth, flags, stats)."""
+        p = _f64(periods)
+        P = p.shape[0]
+        rec = np.empty((P, 9))
+        score = np.empty(P)
+        depth = np.empty(P)
+        flags = np.empty(P, dtype=np.uint32)
+        st = N.ScanStats()
+        b, keep = bank._native()
+        rc = self.lib.fbls_scan_bank(self.ctx, dev.handle, _dptr(p), P, C.byref(b), nb, precision_mode, _dptr(rec),
+                                     _dptr(score), _dptr(depth), flags.ctypes.data_as(N.c_uint32_p), C.byref(st))
+        self._check(rc)
+        return rec, score, depth, flags, st.as_dict()
+
+    def scan_periods(self, dev: DeviceReady, periods, bank: Bank, precision_mode: int = 0):
+        """Rows (N x 5: period, epoch, duration, score, depth) at or above the threshold, and ScanStats."""
+        p = _f64(periods)
+        P = p.shape[0]
+        rows = (N.Row * max(P, 1))()
+        n = C.c_uint32(0)
+        st = N.ScanStats()
+        b, keep = bank._native()
+        self._check(self.lib.fbls_scan_periods(self.ctx, dev.handle, _dptr(p), P, C.byref(b), precision_mode, rows,
+                                               C.byref(n), C.byref(st)))
+        return _rows_array(rows, n.value), st.as_dict()
+
+    def signal_search(self, state: FamilyState, cfg: SearchConfig, dev: Optional[DeviceReady] = None):
+        """signal_search: (rows N x 5, grid length, per-band ScanStats)."""
+        own = dev is None
+        if own:
+            dev = self.upload(state)
+        try:
+            c, keep = _config(cfg)
+            d, r = _f64(state.durations), _f64(state.rho)
+            cap = 1 << 22
+            rows = (N.Row * cap)()
+            n = C.c_uint32(0)
+            glen = C.c_uint64(0)
+            stats = (N.ScanStats * 64)()
+            nb = C.c_uint32(0)
+            self._check(self.lib.fbls_signal_search(self.ctx, dev.handle, _dptr(d), _dptr(r), len(d), C.byref(c),
+                                                    rows, cap, C.byref(n), C.byref(glen), stats, C.byref(nb)))
+            return _rows_array(rows, n.value), int(glen.value), [stats[i].as_dict() for i in range(nb.value)]
+        finally:
+            if own:
+                dev.free()
+
+    def compare_search(self, state: FamilyState, period: float, cfg: SearchConfig,
+                       dev: Optional[DeviceReady] = None) -> List[dict]:
+        """Evidence rows (0, 1 or 2 dicts of EvidenceRow fields) at one period."""
+        own = dev is None
+        if own:
+            dev = self.upload(state)
+        try:
+            c, keep = _config(cfg)
+            d, r = _f64(state.durations), _f64(state.rho)
+            rows = (N.EvidenceRow * 2)()
+            n = C.c_uint32(0)
+            self._check(self.lib.fbls_compare_search(self.ctx, dev.handle, _dptr(d), _dptr(r), len(d), float(period),
+                                                     C.byref(c), rows, C.byref(n)))
+            return [rows[i].as_dict() for i in range(n.value)]
+        finally:
+            if own:
+                dev.free()
+
+
+def _rows_array(rows, n: int) -> np.ndarray:
+    if n == 0:
+        return np.zeros((0, 5))
+    buf = np.ctypeslib.as_array(C.cast(rows, N.c_double_p), shape=(n * 5,))
+    return buf.reshape(n, 5).copy()
+
+
+def band_plan(state: FamilyState, cfg: SearchConfig) -> Tuple[np.ndarray, List[dict]]:
+    """The grid and octave bands signal_search scans (scan.rs:418-471):
+    (grid, [{periods, durations, rho, nb}])."""
+    order = np.argsort(state.durations, kind="stable")
+    ds = state.durations[order]
+    rs = state.rho[order]
+    baseline = float(state.time[-1])
+    maximum = min(cfg.period_max, baseline)
+    minimum = max(cfg.period_min, 4.0 * ds[0] * (1.0 + 1e-9))
+    if maximum <= minimum:
+        return np.zeros(0), []
+    grid = period_grid(minimum, maximum, baseline, float(ds[0]), cfg.period_oversample)
+    bands = []
+    lo = grid[0]
+    last = grid[-1]
+    while lo <= last:
+        hi = lo * 2.0
+        sel = grid[(grid >= lo) & (grid < hi)]
+        chosen = ds < lo / 4.0
+        if sel.size and chosen.any():
+            d = ds[chosen]
+            nb = max(8, int(math.ceil(cfg.phase_oversample * sel[-1] / d.min())))
+            bands.append({"periods": sel, "durations": d, "rho": rs[chosen], "nb": nb})
+        lo = hi
+    return grid, bands
+
+
+def bank_for(band: dict, cfg: SearchConfig) -> Bank:
+    """The Bank signal_search builds for one band (scan.rs:453-465)."""
+    gate = cfg.shape_gate_fraction * cfg.threshold if cfg.ingress_fractions[0] == 0.0 else 0.0
+    return Bank(durations=band["durations"], rho=band["rho"], ingress=tuple(cfg.ingress_fractions),
+                layers=cfg.shape_layers, threshold=cfg.threshold, shape_gate=gate,
+                phase_oversample=cfg.phase_oversample, period_batch=cfg.period_batch,
+                max_fold_mib=cfg.max_fold_mib, prescan_factor=cfg.prescan_factor,
+                prescan_fraction=cfg.prescan_fraction)

@@ -1,0 +1,521 @@
+// Fold, doubled prefix sums, tile scan and merge of the FBLS signal scan on
+// sm_100a. Semantics follow src/search/kernels.rs; the layout of the work on
+// the GPU is this project's own:
+//
+//  * k_fold_prefix: one CTA per group of G periods. The CTA streams the
+//    family's observations once per group and bins them into G shared-memory
+//    histograms (f64 v and w, u32 count), then turns each histogram into the
+//    doubled exclusive prefix sums (f64 and (hi, lo) f32 pairs) with a
+//    warp-shuffle scan per (period, field) row. The histogram never leaves
+//    the SM (the reference writes it to HBM and re-reads it, scan.rs:230-292).
+//  * k_fold_global + k_prefix_global: the same for phase grids whose
+//    histograms do not fit shared memory.
+//  * k_scan_tiles: one CTA of TILE lanes per (tile, period), the reference's
+//    two-pass f32 pre-rank / f64 rescan (kernels.rs:610-845).
+//  * k_merge: best tile per period (kernels.rs:1115-1155).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace fbls {
+
+// floor(t * scale) mod nb for t >= 0 (kernels.rs:314-327). The multiply is
+// one rounded f64 product; the remainder is integer arithmetic.
+__device__ __forceinline__ uint32_t phase_cell(double t, double scale, uint32_t nb) {
+    double x = floor(__dmul_rn(t, scale));
+    uint32_t v = (uint32_t)x;
+    return v % nb;
+}
+
+__device__ __forceinline__ float2 split_pair(double value) {
+    float hi = __double2float_rn(value);
+    float lo = __double2float_rn(__dsub_rn(value, (double)hi));
+    return make_float2(hi, lo);
+}
+
+// Writes one doubled prefix row (2nb+1 entries, f64 and pairs) from a row of
+// bin values read through `load`, by one warp. Order of additions: inclusive
+// Hillis-Steele scan over 32 bins, plus the running carry of earlier chunks.
+template <typename Load>
+__device__ __forceinline__ void prefix_row_warp(Load load, int nb, double* __restrict__ out64,
+                                                float2* __restrict__ out32) {
+    const int lane = threadIdx.x & 31;
+    double carry = 0.0;
+    if (lane == 0) {
+        out64[0] = 0.0;
+        out32[0] = make_float2(0.f, 0.f);
+    }
+    for (int base = 0; base < nb; base += 32) {
+        int b = base + lane;
+        double x = b < nb ? load(b) : 0.0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            double o = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x = __dadd_rn(x, o);
+        }
+        double val = __dadd_rn(carry, x);
+        if (b < nb) {
+            out64[b + 1] = val;
+            out32[b + 1] = split_pair(val);
+        }
+        carry = __shfl_sync(0xffffffffu, val, 31);
+    }
+    const double total = carry;
+    for (int b = lane; b < nb; b += 32) {
+        double val = __dadd_rn(out64[b + 1], total);
+        out64[nb + b + 1] = val;
+        out32[nb + b + 1] = split_pair(val);
+    }
+}
+
+__global__ void __launch_bounds__(FOLD_THREADS) k_fold_prefix(FoldArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int nb = a.nb;
+    const int g0 = blockIdx.x * a.group;
+    const int g = min(a.group, a.periods - g0);
+    double* hv = reinterpret_cast<double*>(smem);
+    double* hw = hv + (size_t)a.group * nb;
+    uint32_t* hc = reinterpret_cast<uint32_t*>(hw + (size_t)a.group * nb);
+    __shared__ double s_scale[MAX_GROUP];
+    if (threadIdx.x < g) s_scale[threadIdx.x] = a.scales[g0 + threadIdx.x];
+    for (int i = threadIdx.x; i < g * nb; i += blockDim.x) {
+        hv[i] = 0.0;
+        hw[i] = 0.0;
+        hc[i] = 0u;
+    }
+    __syncthreads();
+    const uint32_t unb = (uint32_t)nb;
+    for (int i = threadIdx.x; i < a.n; i += blockDim.x) {
+        const double t = a.time[i];
+        const double xv = a.v[i];
+        const double xw = a.w[i];
+        for (int q = 0; q < g; q++) {
+            uint32_t cell = phase_cell(t, s_scale[q], unb) + (uint32_t)(q * nb);
+            atomicAdd(&hv[cell], xv);
+            atomicAdd(&hw[cell], xw);
+            atomicAdd(&hc[cell], 1u);
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const size_t stride = 2 * (size_t)nb + 1;
+    for (int row = warp; row < g * NF; row += nwarps) {
+        const int q = row / NF, f = row % NF;
+        double* out64 = a.cum + ((size_t)(g0 + q) * NF + f) * stride;
+        float2* out32 = a.cum32 + ((size_t)(g0 + q) * NF + f) * stride;
+        const size_t off = (size_t)q * nb;
+        if (f == F_V)
+            prefix_row_warp([&](int b) { return hv[off + b]; }, nb, out64, out32);
+        else if (f == F_W)
+            prefix_row_warp([&](int b) { return hw[off + b]; }, nb, out64, out32);
+        else
+            prefix_row_warp([&](int b) { return (double)hc[off + b]; }, nb, out64, out32);
+    }
+}
+
+// Global-memory histogram for grids too large for shared memory. Layout
+// hist[period][field][nb]; zeroed by the caller.
+__global__ void k_fold_global(FoldArgs a, double* __restrict__ hist) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const double t = a.time[i];
+    const double xv = a.v[i], xw = a.w[i];
+    const uint32_t unb = (uint32_t)a.nb;
+    const int p0 = blockIdx.y * GLOBAL_FOLD_PERIODS;
+    const int p1 = min(p0 + GLOBAL_FOLD_PERIODS, a.periods);
+    for (int p = p0; p < p1; p++) {
+        uint32_t cell = phase_cell(t, a.scales[p], unb);
+        double* h = hist + (size_t)p * NF * a.nb;
+        atomicAdd(&h[cell], xv);
+        atomicAdd(&h[a.nb + cell], xw);
+        atomicAdd(&h[2 * (size_t)a.nb + cell], 1.0);
+    }
+}
+
+// One CTA of NF warps per period: warp f scans field f.
+__global__ void k_prefix_global(FoldArgs a, const double* __restrict__ hist) {
+    const int p = blockIdx.x;
+    const int f = threadIdx.x >> 5;
+    const size_t stride = 2 * (size_t)a.nb + 1;
+    const double* h = hist + ((size_t)p * NF + f) * a.nb;
+    double* out64 = a.cum + ((size_t)p * NF + f) * stride;
+    float2* out32 = a.cum32 + ((size_t)p * NF + f) * stride;
+    prefix_row_warp([&](int b) { return h[b]; }, a.nb, out64, out32);
+}
+
+// ---------------------------------------------------------------------------
+// Tile scan (kernels.rs:610-845).
+// ---------------------------------------------------------------------------
+
+struct LaneState {
+    double best;
+    uint64_t key;
+    uint32_t di;
+    bool bad, sensitive, unsafe_merit;
+    __device__ void reset() {
+        best = neg_inf();
+        key = KEY_MAX;
+        di = 0;
+        bad = sensitive = unsafe_merit = false;
+    }
+};
+
+__device__ __forceinline__ float interval32(const float2* __restrict__ row, uint32_t start, uint32_t width) {
+    float2 s = row[start];
+    float2 e = row[start + width];
+    return __fadd_rn(__fsub_rn(e.x, s.x), __fsub_rn(e.y, s.y));
+}
+
+__device__ __forceinline__ double interval64(const double* __restrict__ row, uint32_t start, uint32_t width) {
+    return __dsub_rn(row[start + width], row[start]);
+}
+
+// f32 merit a^2 / (rho^2 (c norm - hp^2)) and the lane bookkeeping of
+// rank_fast (kernels.rs:389-425).
+__device__ __forceinline__ float rank_fast(LaneState& s, float a32, float hp32, float norm32, float rho2f,
+                                           float basef, bool valid, uint64_t key, uint32_t di) {
+    float cn = __fmul_rn(basef, norm32);
+    float qq = __fmul_rn(rho2f, __fsub_rn(cn, __fmul_rn(hp32, hp32)));
+    float merit = __fdiv_rn(__fmul_rn(a32, a32), qq);
+    bool safe = cn > 0.0f && qq >= __fmul_rn(0.001f, cn) && merit >= 1e-30f && merit <= 1e30f;
+    s.unsafe_merit |= valid && !safe;
+    float best = (float)s.best;
+    const float guard = 1e-5f;
+    bool near = best > 0.0f && fabsf(__fsub_rn(merit, best)) <= __fmul_rn(guard, rmaxf(merit, best));
+    bool far_better = merit > __fmul_rn(best, 1.00004f);
+    if (valid && safe && far_better)
+        s.sensitive = false;
+    else
+        s.sensitive = s.sensitive || (valid && safe && near);
+    bool better = valid && safe && (merit > best || (merit == best && key < s.key));
+    if (better) {
+        s.best = (double)merit;
+        s.key = key;
+        s.di = di;
+    }
+    return (valid && safe) ? merit : -__builtin_huge_valf();
+}
+
+// f64 score (a / rho) / sqrt(norm - hp^2 / c) and the bookkeeping of
+// rank_exact (kernels.rs:428-455).
+__device__ __forceinline__ double rank_exact(LaneState& s, double a, double hp, double norm, double rho,
+                                             double baseline, bool valid, uint64_t key, uint32_t di) {
+    double d = __ddiv_rn(__dmul_rn(hp, hp), baseline);
+    double q = __dsub_rn(norm, d);
+    s.bad |= valid && q <= 0.0;
+    double candidate = __ddiv_rn(__ddiv_rn(a, rho), __dsqrt_rn(rmax(q, 1e-300)));
+    double merit = (valid && q > 0.0 && candidate < __builtin_huge_val()) ? candidate : neg_inf();
+    bool better = merit > s.best || (merit == s.best && key < s.key);
+    if (better) {
+        s.best = merit;
+        s.key = key;
+        s.di = di;
+    }
+    return merit;
+}
+
+// Staircase sums of shape si at (j, k) in f64 (kernels.rs:84-113).
+__device__ __forceinline__ void shape_sums64(const double* __restrict__ rv, const double* __restrict__ rw, uint32_t j,
+                                             uint32_t k, double oa, double ohp, double onorm, double ing,
+                                             const double* __restrict__ factors, int si, int layers, double& a,
+                                             double& hp, double& norm) {
+    if (ing == 0.0) {
+        a = oa;
+        hp = ohp;
+        norm = onorm;
+        return;
+    }
+    const double l = (double)layers;
+    const double l2 = __dmul_rn(l, l);
+    a = __ddiv_rn(oa, l);
+    hp = __ddiv_rn(ohp, l);
+    norm = __ddiv_rn(onorm, l2);
+    for (int layer = 1; layer < layers; layer++) {
+        uint32_t width = layer_width(k, factors[si * layers + layer]);
+        uint32_t start = j + (k - width) / 2;
+        double dw = interval64(rw, start, width);
+        a = __dadd_rn(a, __ddiv_rn(interval64(rv, start, width), l));
+        hp = __dadd_rn(hp, __ddiv_rn(dw, l));
+        norm = __dadd_rn(norm, __dmul_rn(dw, __ddiv_rn(__dadd_rn(__dmul_rn(2.0, (double)layer), 1.0), l2)));
+    }
+}
+
+// The same sums in f32 from the (hi, lo) pairs (kernels.rs:117-146).
+__device__ __forceinline__ void shape_sums32(const float2* __restrict__ rv, const float2* __restrict__ rw, uint32_t j,
+                                             uint32_t k, float oa, float ohp, float onorm, double ing,
+                                             const double* __restrict__ factors, int si, int layers, float& a,
+                                             float& hp, float& norm) {
+    if (ing == 0.0) {
+        a = oa;
+        hp = ohp;
+        norm = onorm;
+        return;
+    }
+    const float l = (float)layers;
+    const float l2 = __fmul_rn(l, l);
+    a = __fdiv_rn(oa, l);
+    hp = __fdiv_rn(ohp, l);
+    norm = __fdiv_rn(onorm, l2);
+    for (int layer = 1; layer < layers; layer++) {
+        uint32_t width = layer_width(k, factors[si * layers + layer]);
+        uint32_t start = j + (k - width) / 2;
+        float dw = interval32(rw, start, width);
+        a = __fadd_rn(a, __fdiv_rn(interval32(rv, start, width), l));
+        hp = __fadd_rn(hp, __fdiv_rn(dw, l));
+        norm = __fadd_rn(norm, __fmul_rn(dw, __fdiv_rn(__fadd_rn(__fmul_rn(2.0f, (float)layer), 1.0f), l2)));
+    }
+}
+
+__global__ void __launch_bounds__(TILE) k_scan_tiles(ScanArgs a) {
+    __shared__ double s_dur[MAX_DURATIONS], s_rho[MAX_DURATIONS], s_ing[MAX_SHAPES];
+    __shared__ double s_fac[MAX_SHAPES * MAX_LAYERS];
+    __shared__ double s_wv[TILE / 32];
+    __shared__ unsigned long long s_wk[TILE / 32];
+    __shared__ int s_wl[TILE / 32];
+    __shared__ uint32_t s_di;
+
+    const int lane = threadIdx.x;
+    const int tile = blockIdx.x;
+    const int f = blockIdx.y;
+    const int nb = a.nb;
+    const int nd = a.nd, ns = a.ns, layers = a.layers;
+    for (int i = lane; i < nd; i += TILE) {
+        s_dur[i] = a.durations[i];
+        s_rho[i] = a.rho[i];
+    }
+    for (int i = lane; i < ns; i += TILE) s_ing[i] = a.ingress[i];
+    for (int i = lane; i < ns * layers; i += TILE) s_fac[i] = a.factors[i];
+    __syncthreads();
+
+    const uint32_t j = (uint32_t)(tile * TILE + lane);
+    const uint32_t jj = min(j, (uint32_t)(nb - 1));
+    const double scale = a.scales[f];
+    const size_t stride = 2 * (size_t)nb + 1;
+    const double* c64 = a.cum + (size_t)f * NF * stride;
+    const float2* c32 = a.cum32 + (size_t)f * NF * stride;
+    const double* rv64 = c64 + F_V * stride;
+    const double* rw64 = c64 + F_W * stride;
+    const double* rn64 = c64 + F_N * stride;
+    const float2* rv32 = c32 + F_V * stride;
+    const float2* rw32 = c32 + F_W * stride;
+    const float2* rn32 = c32 + F_N * stride;
+    const double baseline = a.baseline;
+    const float basef = (float)baseline;
+    const double nobs = a.n;
+    const uint64_t nb1 = (uint64_t)nb + 1;
+    const uint32_t half = (uint32_t)(nb / 2);
+
+    LaneState st;
+    st.reset();
+    bool fast = a.mixed != 0;
+    bool retry = false;
+    uint64_t winner_key = KEY_MAX;
+    uint32_t winner_di = 0;
+    double winner_value = neg_inf();
+    bool bad_any = false;
+    bool rescanned = false;
+
+    for (int pass = 0; pass < 2; pass++) {
+        if (pass == 1) {
+            if (!retry) break;
+            fast = false;
+            rescanned = true;
+            st.reset();
+        }
+        const double gate_value = fast ? __ddiv_rn(__dmul_rn(a.gate, a.gate), baseline) : a.gate;
+        for (int di = 0; di < nd; di++) {
+            const uint32_t raw_k = template_width(s_dur[di], scale);
+            const uint32_t k = min(raw_k, half);
+            const double r = s_rho[di];
+            const uint64_t key = (uint64_t)k * nb1 + jj;
+            bool usable, valid;
+            double merit;
+            float oa32 = 0.f, ow32 = 0.f;
+            if (fast) {
+                float count = interval32(rn32, jj, k);
+                ow32 = interval32(rw32, jj, k);
+                oa32 = interval32(rv32, jj, k);
+                usable = j < (uint32_t)nb && raw_k < half && count >= 3.0f && (double)count <= nobs - 3.0;
+                valid = usable && oa32 > 0.0f;
+                merit = (double)rank_fast(st, oa32, ow32, ow32, (float)(r * r), basef, valid, key, (uint32_t)di);
+            } else {
+                double count = interval64(rn64, jj, k);
+                double w = interval64(rw64, jj, k);
+                double av = interval64(rv64, jj, k);
+                usable = j < (uint32_t)nb && raw_k < half && count >= 3.0 && count <= nobs - 3.0;
+                valid = usable && av > 0.0;
+                merit = rank_exact(st, av, w, w, r, baseline, valid, key, (uint32_t)di);
+            }
+            // Tile-level shape gate (kernels.rs:715-726).
+            if (!__syncthreads_or(valid && merit >= gate_value)) continue;
+            for (int si = 1; si < ns; si++) {
+                const double ing = s_ing[si];
+                const uint64_t skey = ((uint64_t)si * nb1 + k) * nb1 + jj;
+                if (fast) {
+                    float sa, shp, snorm;
+                    shape_sums32(rv32, rw32, jj, k, oa32, ow32, ow32, ing, s_fac, si, layers, sa, shp, snorm);
+                    rank_fast(st, sa, shp, snorm, (float)(r * r), basef, usable && sa > 0.0f, skey, (uint32_t)di);
+                } else {
+                    double w = interval64(rw64, jj, k);
+                    double av = interval64(rv64, jj, k);
+                    double sa, shp, snorm;
+                    shape_sums64(rv64, rw64, jj, k, av, w, w, ing, s_fac, si, layers, sa, shp, snorm);
+                    rank_exact(st, sa, shp, snorm, r, baseline, usable && sa > 0.0, skey, (uint32_t)di);
+                }
+            }
+        }
+        if (fast && st.best <= 0.0) st.key = nb1 + jj;
+        // Block winner: largest value, then smallest key, then lowest lane.
+        double v = st.best;
+        unsigned long long k = st.key;
+        int l = lane;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, v, off);
+            unsigned long long ok = __shfl_xor_sync(0xffffffffu, k, off);
+            int ol = __shfl_xor_sync(0xffffffffu, l, off);
+            if (ov > v || (ov == v && (ok < k || (ok == k && ol < l)))) {
+                v = ov;
+                k = ok;
+                l = ol;
+            }
+        }
+        if ((lane & 31) == 0) {
+            s_wv[lane >> 5] = v;
+            s_wk[lane >> 5] = k;
+            s_wl[lane >> 5] = l;
+        }
+        __syncthreads();
+        double bv = s_wv[0];
+        unsigned long long bk = s_wk[0];
+        int bl = s_wl[0];
+#pragma unroll
+        for (int w = 1; w < TILE / 32; w++) {
+            double cv = s_wv[w];
+            unsigned long long ck = s_wk[w];
+            int cl = s_wl[w];
+            if (cv > bv || (cv == bv && (ck < bk || (ck == bk && cl < bl)))) {
+                bv = cv;
+                bk = ck;
+                bl = cl;
+            }
+        }
+        const double guard = fast ? 1e-5 : 1e-10;
+        const bool near_top = st.best > 0.0 && st.best >= __dmul_rn(bv, __dsub_rn(1.0, guard));
+        if (lane == bl) s_di = st.di;
+        const int near_count = __syncthreads_count(near_top);
+        const bool near_sensitive = __syncthreads_or(near_top && st.sensitive);
+        const bool unsafe_any = __syncthreads_or(st.unsafe_merit);
+        const bool bad = __syncthreads_or(st.bad);
+        winner_key = bk;
+        winner_value = bv;
+        winner_di = s_di;
+        retry = fast && (unsafe_any || near_count > 1 || near_sensitive);
+        bad_any = bad_any || bad;
+        __syncthreads();
+    }
+
+    if (lane == 0) {
+        // The winner recomputed in f64 (kernels.rs:800-843).
+        const uint32_t phase = (uint32_t)(winner_key % nb1);
+        const uint32_t width = (uint32_t)((winner_key / nb1) % nb1);
+        const uint32_t si = (uint32_t)(winner_key / (nb1 * nb1));
+        const int sic = min((int)si, ns - 1);
+        const double ing = s_ing[sic];
+        const double r = s_rho[winner_di];
+        const double w = interval64(rw64, phase, width);
+        const double av = interval64(rv64, phase, width);
+        double a0, hp, norm;
+        shape_sums64(rv64, rw64, phase, width, av, w, w, ing, s_fac, sic, layers, a0, hp, norm);
+        const double aa = __ddiv_rn(a0, r);
+        const double d = __ddiv_rn(__dmul_rn(hp, hp), baseline);
+        const double q = rmax(__dsub_rn(norm, d), 1e-300);
+        const double value = winner_value > neg_inf() ? __ddiv_rn(aa, __dsqrt_rn(q)) : neg_inf();
+        const double depth = __dmul_rn(__ddiv_rn(aa, q), r);
+        const size_t idx = (size_t)f * gridDim.x + tile;
+        double* out = a.parts + idx * PART_STRIDE;
+        out[0] = (double)phase;
+        out[1] = (double)width;
+        out[2] = aa;
+        out[3] = norm;
+        out[4] = d;
+        out[5] = ing;
+        out[6] = r;
+        out[7] = value;
+        out[8] = depth;
+        a.keys[idx] = winner_key;
+        a.flags[idx] = (uint32_t)retry | ((uint32_t)bad_any << 1) | ((uint32_t)rescanned << 2);
+    }
+}
+
+// Best tile per period by (score, lowest key) (kernels.rs:1115-1155). Writes
+// records at `offset` so one buffer collects a whole band; flags are ORed.
+__global__ void k_merge(MergeArgs a) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= a.periods) return;
+    double best = neg_inf();
+    uint64_t key = KEY_MAX;
+    int chosen = 0;
+    uint32_t fl = 0;
+    for (int t = 0; t < a.tiles; t++) {
+        const size_t idx = (size_t)f * a.tiles + t;
+        double v = a.parts[idx * PART_STRIDE + 7];
+        uint64_t k = a.keys[idx];
+        fl |= a.flags[idx];
+        if (v > best || (v == best && k < key)) {
+            best = v;
+            key = k;
+            chosen = t;
+        }
+    }
+    const double* part = a.parts + ((size_t)f * a.tiles + chosen) * PART_STRIDE;
+    const size_t g = (size_t)a.offset + f;
+    double* rec = a.records + g * RECORD_STRIDE;
+    rec[0] = a.periods_in[f];
+    rec[1] = a.scales[f];
+    for (int i = 0; i < 7; i++) rec[2 + i] = part[i];
+    a.score[g] = best;
+    a.depth[g] = part[8];
+    a.flags_out[g] = fl;
+}
+
+// ---------------------------------------------------------------------------
+// Launchers.
+// ---------------------------------------------------------------------------
+
+cudaError_t launch_fold_prefix(const FoldArgs& a, size_t smem_bytes, cudaStream_t stream) {
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_fold_prefix, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)MAX_FOLD_SMEM);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    int blocks = (a.periods + a.group - 1) / a.group;
+    k_fold_prefix<<<blocks, FOLD_THREADS, smem_bytes, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_global(const FoldArgs& a, double* hist, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(hist, 0, (size_t)a.periods * NF * a.nb * sizeof(double), stream);
+    if (e != cudaSuccess) return e;
+    dim3 grid((a.n + 255) / 256, (a.periods + GLOBAL_FOLD_PERIODS - 1) / GLOBAL_FOLD_PERIODS);
+    k_fold_global<<<grid, 256, 0, stream>>>(a, hist);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_prefix_global<<<a.periods, 32 * NF, 0, stream>>>(a, hist);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream) {
+    dim3 grid((a.nb + TILE - 1) / TILE, periods);
+    k_scan_tiles<<<grid, TILE, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge(const MergeArgs& a, cudaStream_t stream) {
+    k_merge<<<(a.periods + 127) / 128, 128, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace fbls

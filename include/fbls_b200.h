@@ -1,0 +1,240 @@
+/* fbls_b200: B200 (sm_100a) implementation of the FBLS search hot path.
+ *
+ * C ABI. Plain pointers and sizes only; every host array is owned by the
+ * caller and borrowed for the duration of the call. Device memory is owned by
+ * the library (per context and per uploaded family) and never exposed.
+ *
+ * The reference (isakruas/fbls) has no FFI layer: its Rust host calls its
+ * cuda-oxide kernels directly. The entry points below sit on the seams where
+ * that host would call into a native library:
+ *
+ *   fbls_create / fbls_destroy   <- Gpu::new / Gpu::shared      src/search/scan.rs:51-77
+ *   fbls_upload_ready            <- DeviceReady::upload         src/search/scan.rs:110-124
+ *   fbls_scan_periods            <- scan_periods                src/search/scan.rs:363-408
+ *   fbls_scan_bank               <- scan_bank (every period's   src/search/scan.rs:144-357
+ *                                   winner at one nb)
+ *   fbls_compare_search          <- compare_search              src/search/evidence.rs:693-1003
+ *
+ * Host-side mirror (C++ restatements of the Rust host functions around the
+ * path, for callers that do not have the Rust host):
+ *
+ *   fbls_period_grid             <- period_grid                 src/search/grid.rs:5-28
+ *   fbls_family_state            <- family_state (prepared)     src/prep/curve.rs:541-569
+ *   fbls_signal_search           <- signal_search               src/search/scan.rs:413-473
+ *
+ * Every call returns 0 on success or a nonzero status; fbls_last_error()
+ * then holds the message. Messages that the reference raises keep its text:
+ * "nonpositive template precision; inspect noise model" (scan.rs:336),
+ * "one folded period exceeds max_fold_mib" (scan.rs:181).
+ *
+ * Threading: one context is used by one host thread at a time (the
+ * reference keeps one context and stream per worker thread, scan.rs:47-64);
+ * different contexts may run concurrently.
+ */
+#ifndef FBLS_B200_H
+#define FBLS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FBLS_OK 0
+#define FBLS_ERR_ARGUMENT 1
+#define FBLS_ERR_CUDA 2
+#define FBLS_ERR_PRECISION 3 /* nonpositive template precision */
+#define FBLS_ERR_BUDGET 4    /* one folded period exceeds max_fold_mib */
+#define FBLS_ERR_DATA 5      /* preparation errors (too few observations, ...) */
+
+typedef struct fbls_ctx fbls_ctx;
+typedef struct fbls_ready fbls_ready;
+
+/* Template bank of one octave band; mirrors Bank, src/search/scan.rs:127-139.
+ * durations (days, ascending) and rho have nd entries; ingress has ns. */
+typedef struct {
+    const double* durations;
+    const double* rho;
+    uint32_t nd;
+    const double* ingress;
+    uint32_t ns;
+    uint32_t layers;
+    double threshold;
+    double shape_gate;
+    uint32_t phase_oversample;
+    uint32_t period_batch;
+    double max_fold_mib;
+    uint32_t prescan_factor;
+    double prescan_fraction;
+} fbls_bank;
+
+/* One qualifying period; mirrors Row, src/search/scan.rs:17-23. */
+typedef struct {
+    double period;
+    double epoch;
+    double duration;
+    double score;
+    double depth;
+} fbls_row;
+
+/* Mirrors ScanStats, src/search/scan.rs:26-37. exact_tile_retries keeps the
+ * reference's reported value (its flag word never carries the retry bit once
+ * the f64 rescan has run, kernels.rs:796, :841-842); tile_rescans counts the
+ * tiles whose f64 rescan actually ran. */
+typedef struct {
+    uint64_t periods;
+    uint64_t prescan_survivors;
+    uint64_t phase_bins;
+    uint64_t batches;
+    uint64_t templates_scanned;
+    uint64_t exact_tile_retries;
+    uint64_t tile_rescans;
+    double seconds;
+    double seconds_fold;
+    double seconds_cumulative;
+    double seconds_scan;
+} fbls_scan_stats;
+
+/* Search configuration fields read by the path; mirrors SearchConfig,
+ * src/config.rs:6-88 (defaults there). stellar_radius_solar = NaN means None. */
+typedef struct {
+    double period_min;
+    double period_max;
+    double threshold;
+    const double* ingress_fractions;
+    uint32_t n_ingress;
+    uint32_t shape_layers;
+    uint32_t phase_oversample;
+    double shape_gate_fraction;
+    uint32_t prescan_factor;
+    double prescan_fraction;
+    double period_oversample;
+    uint32_t period_batch;
+    double max_fold_mib;
+    double evidence_rtol;
+    double planet_prior;
+    double binary_prior;
+    double planet_depth_scale;
+    double binary_depth_scale;
+    double diluted_binary_depth_scale;
+    double stellar_radius_solar;
+    double planet_radius_scale_rj;
+    double target_flux_fraction;
+    /* Scan precision: 0 = the reference's mixed mode (f32 pre-rank from
+     * (hi, lo) pairs, f64 winner and rescans); 1 = f64 ranking throughout. */
+    uint32_t precision_mode;
+} fbls_config;
+
+/* Evidence row; mirrors EvidenceRow, src/search/evidence.rs:638-653. */
+typedef struct {
+    double period;
+    double epoch;
+    double duration;
+    double snr;
+    double depth;
+    double planet_log_odds;
+    double log_bf_planet_noise;
+    double log_bf_binary_noise;
+    double binary_secondary_ratio;
+    double binary_secondary_phase;
+    double binary_odd_even_ratio;
+    double binary_period_days;
+    double ingress_fraction;
+    uint32_t selection_flags;
+} fbls_evidence_row;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Replaces Gpu::new (scan.rs:66-77): device context, stream, workspace. */
+fbls_ctx* fbls_create(int device, int* status);
+void fbls_destroy(fbls_ctx* ctx);
+/* Message of the last failed call on this context (never NULL). */
+const char* fbls_last_error(const fbls_ctx* ctx);
+/* Library version string. */
+const char* fbls_version(void);
+
+/* ---- boundary --------------------------------------------------------- */
+
+/* Replaces DeviceReady::upload (scan.rs:110-124): uploads the prepared
+ * family fields (times relative to origin, ascending; v; w) of n
+ * observations. residual_energy is Ready::residual_energy (curve.rs:440). */
+int fbls_upload_ready(fbls_ctx* ctx, const double* time, const double* v, const double* w, uint32_t n,
+                      double baseline_norm, double origin, double residual_energy, fbls_ready** out);
+void fbls_free_ready(fbls_ready* ready);
+
+/* Replaces scan_periods (scan.rs:363-408): best template per period over
+ * the bank, coarse prescan then full scan on survivors; writes the rows whose
+ * score reaches bank->threshold (at most P) in period order. precision_mode
+ * as in fbls_config. */
+int fbls_scan_periods(fbls_ctx* ctx, const fbls_ready* ready, const double* periods, uint32_t P,
+                      const fbls_bank* bank, uint32_t precision_mode, fbls_row* rows_out, uint32_t* n_rows,
+                      fbls_scan_stats* stats);
+
+/* Every period's winner at nb phase bins (one scan_bank pass, scan.rs:144-357):
+ * records P x 9 (period, scale, phase, width, a, norm, d, ingress, rho),
+ * score and depth P each, flags P (OR of the tile flag words). */
+int fbls_scan_bank(fbls_ctx* ctx, const fbls_ready* ready, const double* periods, uint32_t P,
+                   const fbls_bank* bank, uint32_t nb, uint32_t precision_mode, double* records, double* score,
+                   double* depth, uint32_t* flags, fbls_scan_stats* stats);
+
+/* Replaces compare_search (evidence.rs:693-1003) at one trial period.
+ * durations/rho: the family's nd durations (days) and correlated-noise
+ * factors, any order. Writes 0, 1 or 2 rows. */
+int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
+                        uint32_t nd, double period, const fbls_config* cfg, fbls_evidence_row* rows_out,
+                        uint32_t* n_rows);
+
+/* ---- instrumentation (no counterpart in the reference; its FBLS_PROFILE
+ * synchronises after each kernel instead, scan.rs:152, :222-229) --------- */
+
+/* Device time of the context's stream between two calls, by CUDA events
+ * recorded on that stream (stop synchronises on its event). */
+int fbls_timer_start(fbls_ctx* ctx);
+int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
+
+typedef struct {
+    uint64_t launches;        /* every kernel this context launched */
+    uint64_t fold_launches;   /* fold + prefix launches */
+    double fold_ms;           /* their summed device time (timing enabled) */
+    double fold_bytes;        /* algorithmic bytes: 24 n + 48 (2 nb + 1) per period */
+    uint64_t scan_launches;   /* tile scan + merge launches */
+    double scan_ms;
+    double scan_bytes;        /* algorithmic bytes: 24 (2 nb + 1) + 84 tiles per period */
+    uint64_t fold_updates;    /* observation x period bin updates */
+} fbls_counters;
+
+/* Enables per-launch event timing of the fold and scan kernels (adds one
+ * event record per launch, no synchronisation). */
+int fbls_set_kernel_timing(fbls_ctx* ctx, int enable);
+/* Reads (and with reset != 0 clears) the context's counters. */
+int fbls_read_counters(fbls_ctx* ctx, fbls_counters* out, int reset);
+
+/* ---- host-side mirror ------------------------------------------------- */
+
+/* period_grid (grid.rs:5-28). Returns the count; writes it when capacity
+ * suffices (out may be NULL to query the count). */
+int64_t fbls_period_grid(double minimum, double maximum, double baseline, double minimum_duration,
+                         double oversample, double* out, int64_t capacity);
+
+/* family_state for a prepared curve (curve.rs:541-569 with
+ * fit_segment_noise at bin 0, prepare_ready, correlated_noise_factors).
+ * out arrays hold n_in entries; *n_out is the usable count. scalars_out:
+ * baseline_norm, origin, residual_energy, inflation, segments. Status
+ * FBLS_ERR_DATA with the reference's message on bad input. */
+int fbls_family_state(const double* time, const double* flux, const double* sigma, uint32_t n_in,
+                      const double* durations, uint32_t nd, int correlated, uint32_t* n_out, double* time_out,
+                      double* v_out, double* w_out, double* scalars_out, double* rho_out, char* error,
+                      uint32_t error_len);
+
+/* signal_search (scan.rs:413-473) for one family: octave bands over the
+ * family's grid. rows_out holds capacity rows (the grid length suffices);
+ * stats_out holds up to 64 bands. */
+int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
+                       uint32_t nd, const fbls_config* cfg, fbls_row* rows_out, uint32_t capacity,
+                       uint32_t* n_rows, uint64_t* grid_len, fbls_scan_stats* stats_out, uint32_t* n_bands);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FBLS_B200_H */

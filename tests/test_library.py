@@ -1,0 +1,105 @@
+"""The C-ABI library on CPU: it loads, exports every entry point the header
+declares, and its host-side code (period grid, prepared-mode family state,
+configuration) matches the oracle exactly. No GPU calls."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from fbls_b200 import _native, api, synth
+from fbls_b200.config import SearchConfig
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "fbls_b200.h"
+
+
+def _declared():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fbls_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _native.load()
+    names = _declared()
+    assert len(names) >= 12
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _native.SIGNATURES, name
+    assert lib.fbls_version().decode().startswith("fbls_b200")
+
+
+def test_period_grid_matches_oracle():
+    for args in [(0.5, 20.0, 50.0, 0.02, 3.0), (0.5, 13.7, 26.4, 0.5 / 24, 3.0), (0.3, 10.0, 356.2, 0.5 / 24, 3.0)]:
+        assert np.array_equal(api.period_grid(*args), oracle.period_grid(*args))
+
+
+@pytest.mark.parametrize("maker", [synth.small_curve, synth.single_sector])
+def test_family_state_matches_oracle_bit_exactly(maker):
+    c = maker()
+    cfg = synth.small_config() if maker is synth.small_curve else synth.single_sector_config()
+    d = cfg.durations_days()
+    a = api.family_state(c.time, c.flux, c.flux_err, d)
+    o = oracle.family_state(c.time, c.flux, c.flux_err, d)
+    assert a.n == o.n
+    for name in ("time", "v", "w", "rho"):
+        assert np.array_equal(getattr(a, name), getattr(o, name)), name
+    assert a.baseline_norm == o.baseline_norm
+    assert a.origin == o.origin
+    assert a.residual_energy == o.residual_energy
+    assert a.inflation == o.inflation
+
+
+def test_family_state_errors_keep_the_reference_messages():
+    t = np.arange(5.0)
+    with pytest.raises(api.FblsError, match="insufficient usable observations"):
+        api.family_state(t, np.zeros(5), np.ones(5), [0.1])
+    t = np.arange(20.0)
+    f = np.full(20, -2.0)  # 1 + flux has a negative median
+    with pytest.raises(api.FblsError, match="positive median"):
+        api.family_state(t, f, np.ones(20), [0.1])
+
+
+def test_family_state_drops_nonfinite_and_sorts():
+    c = synth.small_curve()
+    t = c.time.copy()
+    f = c.flux.copy()
+    e = c.flux_err.copy()
+    f[5] = np.nan
+    e[7] = 0.0
+    perm = np.random.default_rng(1).permutation(t.shape[0])
+    d = synth.small_config().durations_days()
+    a = api.family_state(t[perm], f[perm], e[perm], d)
+    o = oracle.family_state(t, f, e, d)
+    assert a.n == c.time.shape[0] - 2
+    assert np.array_equal(a.v, o.v)
+
+
+def test_config_defaults_and_validation():
+    cfg = SearchConfig()
+    cfg.validate()
+    assert cfg.durations_hours[:3] == [0.5, 0.625, 0.78125]
+    assert len(cfg.durations_days()) == 13
+    with pytest.raises(ValueError, match="quarter of period_min"):
+        SearchConfig(period_min=0.05).validate()
+    with pytest.raises(ValueError, match="ingress"):
+        SearchConfig(ingress_fractions=[0.5]).validate()
+
+
+def test_band_plan_matches_oracle():
+    c = synth.single_sector()
+    cfg = synth.single_sector_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    grid, bands = api.band_plan(st, cfg)
+    ost = oracle.family_state(c.time, c.flux, c.flux_err, cfg.durations_days())
+    ogrid, obands = oracle.band_plan(ost, cfg)
+    assert np.array_equal(grid, ogrid)
+    assert len(bands) == len(obands) == 5
+    for b, (sel, d, r) in zip(bands, obands):
+        assert np.array_equal(b["periods"], sel)
+        assert np.array_equal(b["durations"], d)
+    # The reference's rule at this configuration: 13,065 periods, nb 192 ... 2631.
+    assert grid.shape[0] == 13065
+    assert [b["nb"] for b in bands] == [192, 384, 768, 1536, 2631]

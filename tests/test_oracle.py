@@ -1,0 +1,148 @@
+"""The oracle against the reference's own known-answer tests, and brute-force
+identities of the fold / prefix / interval arithmetic. CPU only."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from fbls_b200 import synth
+
+# erfc known answers of the reference's test, src/search/math.rs:226-252.
+ERFC_KAT = [
+    (0.0, 1.0), (0.5, 0.4795001221869535), (1.0, 0.15729920705028513), (2.0, 0.004677734981047266),
+    (3.0, 2.209049699858544e-05), (5.0, 1.5374597944280347e-12), (10.0, 2.088487583762545e-45),
+    (-1.0, 1.8427007929497148), (-3.0, 1.9999779095030014), (0.3, 0.6713732405408726),
+    (0.46, 0.5153446099983203), (0.47, 0.5062549491139179), (3.99, 1.6739211364520824e-08),
+    (4.01, 1.4196939421371057e-08), (15.0, 7.212994172451209e-100), (26.0, 5.663192408856145e-296),
+]
+
+
+@pytest.mark.parametrize("x,want", ERFC_KAT)
+def test_erfc_reference_values(x, want):
+    # math.rs:248: relative error below 1e-14.
+    assert abs((oracle.erfc(x) - want) / want) < 1e-14
+
+
+def test_grid_bounds_and_drift():
+    # grid.rs:34-42.
+    g = oracle.period_grid(0.5, 20.0, 50.0, 0.02, 3.0)
+    assert g[0] == 0.5 and g[-1] == 20.0
+    assert np.all(50.0 * (g[1:] / g[:-1] - 1.0) <= 0.02 / 3.0 * (1.0 + 1e-9))
+
+
+def test_noise_model_normalizes_and_inflates():
+    # curve.rs:636-661.
+    n = 500
+    t = 1000.0 + np.arange(n) * 0.01
+    f = 2000.0 + 3.0 * np.sin(np.arange(n) * 1.7)
+    e = np.ones(n)
+    time, deficit, variance, origin, inflation, segments = oracle.fit_segment_noise(t, f, e, 0.75)
+    assert origin == 1000.0
+    assert time[0] == 0.0
+    median = np.sort(f)[(n - 1) // 2]
+    assert abs(deficit[0] - (1.0 - f[0] / median)) < 1e-12
+    assert inflation > 2.0
+    assert segments == 1
+
+
+def test_transit_mask_and_cycles():
+    # curve.rs:663-673.
+    t = np.arange(1000) * 0.01
+    m = oracle.transit_mask(t, 2.0, 1.0, 0.2, 0.0)
+    direct = sum(1 for x in t if abs(math.fmod(x - 1.0 + 1.0, 2.0) - 1.0) <= 0.1)
+    assert m.sum() == direct
+    assert 100 <= direct <= 110
+
+
+def test_log_add_and_evidence_limits():
+    assert oracle.log_add(-math.inf, -math.inf) == -math.inf
+    assert abs(oracle.log_add(0.0, 0.0) - math.log(2.0)) < 1e-15
+    # No data: the normalized half-normal prior integrates the likelihood ratio 1 to log 1 = 0.
+    assert oracle.positive_amplitude_evidence(0.0, 0.0, 0.01) == 0.0
+    # Continuity across the asymptotic branch at z = -26.
+    tau, q = 1.0, 0.0
+    lo = oracle.positive_amplitude_evidence(-26.0 - 1e-9, q, tau)
+    hi = oracle.positive_amplitude_evidence(-26.0 + 1e-9, q, tau)
+    assert abs(lo - hi) < 1e-6
+    assert oracle.subspace_upper(-1.0, -1.0, 1.0, 1.0, 0.0, 1.0) == pytest.approx(1e-6)
+
+
+@pytest.fixture(scope="module")
+def small_state():
+    c = synth.small_curve()
+    cfg = synth.small_config()
+    return oracle.family_state(c.time, c.flux, c.flux_err, cfg.durations_days()), cfg, c
+
+
+def test_prefix_matches_direct_box_sums(small_state):
+    """fold + doubled prefix + interval difference == direct per-observation sums,
+    including windows that wrap around phase zero."""
+    st, cfg, _ = small_state
+    nb = 97
+    scale = nb / 1.2345
+    folded, cum, cum32 = oracle.fold_prefix(st, scale, nb)
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        j = int(rng.integers(0, nb))
+        k = int(rng.integers(1, nb // 2 + 1))
+        direct = oracle.box_direct(st, scale, nb, j, k)
+        via = [cum[f, j + k] - cum[f, j] for f in (0, 1, 2)]
+        assert via[2] == direct[2]
+        assert abs(via[0] - direct[0]) <= 1e-9 * np.abs(st.v).sum()
+        assert abs(via[1] - direct[1]) <= 1e-12 * st.w.sum()
+    # (hi, lo) pairs represent the f64 prefix to f32 x f32 precision.
+    rec = cum32[..., 0].astype(np.float64) + cum32[..., 1].astype(np.float64)
+    assert np.all(np.abs(rec - cum) <= 1e-13 * np.abs(cum).max())
+    # Second copy = first + total.
+    assert np.array_equal(cum[:, nb + 1:], cum[:, 1:nb + 1] + cum[:, nb:nb + 1])
+
+
+def test_winner_is_the_f64_argmax_in_f64_mode(small_state):
+    """In f64-only mode each period's record is the argmax of the exact score
+    over every (phase, duration) box template (shapes gated off here)."""
+    st, cfg, _ = small_state
+    periods = np.array([0.77, 1.3, 2.2])
+    nb = 60
+    d = np.array(sorted(cfg.durations_days()))
+    rec, score, depth, flags, _ = oracle.scan_bank(st, periods, nb, d, st.rho, ingress=(0.0,), shape_gate=1e9, mode=1)
+    for i, p in enumerate(periods):
+        scale = nb / p
+        best = (-math.inf, None)
+        for di, dur in enumerate(d):
+            raw_k = max(1, math.floor(dur * scale + 0.5))
+            k = min(raw_k, nb // 2)
+            if raw_k >= nb // 2:
+                continue
+            for j in range(nb):
+                a, hp, cnt = oracle.box_direct(st, scale, nb, j, k)
+                if not (3 <= cnt <= st.n - 3 and a > 0):
+                    continue
+                q = hp - hp * hp / st.baseline_norm
+                s = (a / st.rho[di]) / math.sqrt(q)
+                if s > best[0] * (1 + 1e-12):
+                    best = (s, (j, k))
+        assert (int(rec[i, 2]), int(rec[i, 3])) == best[1]
+        assert score[i] == pytest.approx(best[0], rel=1e-9)
+
+
+def test_oracle_recovers_injected_signal(small_state):
+    st, cfg, c = small_state
+    rows, grid, stats = oracle.signal_search(st, cfg)
+    assert len(rows) > 0
+    best = rows[np.argmax(rows[:, 3])]
+    assert abs(best[0] / c.period - 1.0) < 0.01
+    phase = ((best[1] - c.epoch) / c.period + 0.5) % 1.0 - 0.5
+    assert abs(phase * c.period) < c.duration
+
+
+def test_mixed_and_f64_modes_agree_on_winners(small_state):
+    st, cfg, _ = small_state
+    periods = oracle.period_grid(0.5, 1.0, float(st.time[-1]), 0.75 / 24, 3.0)
+    d = np.array(sorted(cfg.durations_days()))[:3]
+    r0 = oracle.scan_bank(st, periods, 64, d, st.rho[:3], mode=0)
+    r1 = oracle.scan_bank(st, periods, 64, d, st.rho[:3], mode=1)
+    same = (r0[0][:, 2:4] == r1[0][:, 2:4]).all(axis=1) & (r0[0][:, 7] == r1[0][:, 7])
+    assert same.mean() > 0.99
+    ok = np.isfinite(r0[1])
+    assert np.allclose(r0[1][ok & same], r1[1][ok & same], rtol=1e-12)
