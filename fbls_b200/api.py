@@ -241,7 +241,7 @@ class Gpu:
         try:
             c, keep = _config(cfg)
             d, r = _f64(state.durations), _f64(state.rho)
-            cap = 1 << 22
+            cap = max(1, _grid_count(state, cfg))
             rows = (N.Row * cap)()
             n = C.c_uint32(0)
             glen = C.c_uint64(0)
@@ -271,6 +271,17 @@ class Gpu:
         finally:
             if own:
                 dev.free()
+
+
+def _grid_count(state: FamilyState, cfg: SearchConfig) -> int:
+    """Length of the period grid signal_search scans (an upper bound on its rows)."""
+    dmin = float(np.min(state.durations))
+    baseline = float(state.time[-1])
+    maximum = min(cfg.period_max, baseline)
+    minimum = max(cfg.period_min, 4.0 * dmin * (1.0 + 1e-9))
+    if maximum <= minimum:
+        return 0
+    return int(N.load().fbls_period_grid(minimum, maximum, baseline, dmin, cfg.period_oversample, None, 0))
 
 
 def _rows_array(rows, n: int) -> np.ndarray:

@@ -6,9 +6,9 @@
 // alternating primaries at twice the period), and the phase / duration /
 // shape sums are log-sum-exp'd per tile.
 //
-// Device work: k_fold_two bins the observations into a shared-memory
-// histogram per CTA (merged with f64 atomics), k_prefix_fields scans the
-// three fields, k_screen and k_joint evaluate one 64-phase tile per CTA.
+// Device work: the two-period fold runs on the deterministic fold kernel
+// (fold.cu) with one period and 2 nb bins, k_prefix_fields scans the three
+// fields, k_screen and k_joint evaluate one 64-phase tile per CTA.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -16,13 +16,11 @@
 
 #include "common.cuh"
 #include "evidence.h"
+#include "kernels.h"
 
 namespace fbls {
 
 namespace {
-
-constexpr int FOLD2_THREADS = 512;
-constexpr size_t FOLD2_SMEM_MAX = 200 * 1024;
 
 struct EvArgs {
     const double* cum;  // 3 x (nb2 + 1), field-major
@@ -75,59 +73,30 @@ __device__ __forceinline__ double tile_max(double v, double* s2) {
 
 }  // namespace
 
-// bin = floor(t * scale) rem_euclid 2nb (evidence.rs:75-92), per-CTA
-// shared-memory histograms merged into `hist` (3 x nb2, zeroed).
-__global__ void __launch_bounds__(FOLD2_THREADS) k_fold_two(const double* __restrict__ time,
-                                                            const double* __restrict__ v, const double* __restrict__ w,
-                                                            int n, double scale, int nb2, double* __restrict__ hist,
-                                                            int use_smem) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    double* sv = reinterpret_cast<double*>(smem);
-    double* sw = sv + nb2;
-    double* sc = sw + nb2;
-    if (use_smem) {
-        for (int i = threadIdx.x; i < 3 * nb2; i += blockDim.x) sv[i] = 0.0;
-        __syncthreads();
-    }
-    const uint64_t m = (uint64_t)nb2;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double x = floor(__dmul_rn(time[i], scale));
-        uint32_t cell = (uint32_t)((uint64_t)x % m);
-        if (use_smem) {
-            atomicAdd(&sv[cell], v[i]);
-            atomicAdd(&sw[cell], w[i]);
-            atomicAdd(&sc[cell], 1.0);
-        } else {
-            atomicAdd(&hist[cell], v[i]);
-            atomicAdd(&hist[nb2 + cell], w[i]);
-            atomicAdd(&hist[2 * (size_t)nb2 + cell], 1.0);
-        }
-    }
-    if (use_smem) {
-        __syncthreads();
-        for (int i = threadIdx.x; i < 3 * nb2; i += blockDim.x)
-            if (sv[i] != 0.0) atomicAdd(&hist[i], sv[i]);
-    }
-}
-
-// Exclusive prefix over 2nb bins per field (evidence.rs:96-144): warp f
-// scans field f.
-__global__ void k_prefix_fields(const double* __restrict__ hist, double* __restrict__ cum, int nb2) {
-    const int f = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const double* h = hist + (size_t)f * nb2;
-    double* out = cum + (size_t)f * (nb2 + 1);
+// Exclusive prefix over 2nb bins per field (evidence.rs:96-144), one CTA of
+// 256 threads per field with the reference's association: per segment a
+// block-wide Hillis-Steele scan (strides 1 .. 128) plus the running carry.
+__global__ void __launch_bounds__(256) k_prefix_fields(const double* __restrict__ hist, double* __restrict__ cum,
+                                                       int nb2) {
+    __shared__ double scan[256];
+    const int lane = threadIdx.x, field = blockIdx.x;
+    const double* h = hist + (size_t)field * nb2;
+    double* out = cum + (size_t)field * (nb2 + 1);
     if (lane == 0) out[0] = 0.0;
     double carry = 0.0;
-    for (int base = 0; base < nb2; base += 32) {
-        int b = base + lane;
-        double x = b < nb2 ? h[b] : 0.0;
-        for (int off = 1; off < 32; off <<= 1) {
-            double o = __shfl_up_sync(0xffffffffu, x, off);
-            if (lane >= off) x = __dadd_rn(x, o);
+    for (int seg = 0; seg < nb2; seg += 256) {
+        const int b = seg + lane;
+        scan[lane] = b < nb2 ? h[b] : 0.0;
+        __syncthreads();
+        for (int stride = 1; stride < 256; stride <<= 1) {
+            const double add = lane >= stride ? scan[lane - stride] : 0.0;
+            __syncthreads();
+            if (lane >= stride) scan[lane] = __dadd_rn(scan[lane], add);
+            __syncthreads();
         }
-        double val = __dadd_rn(carry, x);
-        if (b < nb2) out[b + 1] = val;
-        carry = __shfl_sync(0xffffffffu, val, 31);
+        if (b < nb2) out[b + 1] = __dadd_rn(scan[lane], carry);
+        carry = __dadd_rn(carry, scan[255]);
+        __syncthreads();
     }
 }
 
@@ -496,6 +465,10 @@ int compare_search(cudaStream_t stream, void*, size_t, const EvidenceReady& r, c
         return FBLS_ERR_ARGUMENT;
     }
     const double scale = (double)nb / period;
+    if (std::floor(r.t_last * scale) >= 4294967295.0 - 2.0 * (double)nb2 - 2.0) {
+        message = "phase cell exceeds 32 bits";
+        return FBLS_ERR_ARGUMENT;
+    }
     const double n = (double)r.n;
     std::vector<double> dlm(nd);
     for (int i = 0; i < nd; i++) {
@@ -571,8 +544,23 @@ int compare_search(cudaStream_t stream, void*, size_t, const EvidenceReady& r, c
     };
     const size_t o_dur = put(durations), o_rho = put(rho), o_dlm = put(dlm), o_shapes = put(shapes),
                  o_priors = put(priors), o_params = put(std::vector<double>(params, params + NPARAM)),
-                 o_orbit = put(orbit), o_floors = put(std::vector<double>(3, 0.0));
-    const size_t o_hist = consts.size();
+                 o_orbit = put(orbit), o_floors = put(std::vector<double>(3, 0.0)),
+                 o_scale = put(std::vector<double>(1, scale));
+    // Fold shape and chunks (ints, packed into the double workspace).
+    FoldShape shape = fold_group_shape((int)nb2, 1, 1);
+    std::vector<int> chunks((size_t)r.n + 2);
+    const int nchunks = fold_chunks(r.time_host, (int)r.n, scale, (int)nb2, shape.span_cap, shape.chunk_cap,
+                                    chunks.data(), (int)chunks.size());
+    if (nchunks < 1) {
+        message = "fold chunking failed";
+        return FBLS_ERR_ARGUMENT;
+    }
+    std::vector<double> packed(((size_t)nchunks + 2) / 2 + 1, 0.0);
+    std::memcpy(packed.data(), chunks.data(), ((size_t)nchunks + 1) * sizeof(int));
+    const size_t o_chunks = put(packed);
+    const bool fold_smem = shape.hist_in_smem;
+    const size_t o_fscratch = consts.size();
+    const size_t o_hist = o_fscratch + (fold_smem ? 0 : 3 * nb2);
     const size_t o_cum = o_hist + 3 * nb2;
     const size_t o_screen = o_cum + 3 * (nb2 + 1);
     const size_t o_parts = o_screen + (size_t)tiles * 4;
@@ -591,18 +579,25 @@ int compare_search(cudaStream_t stream, void*, size_t, const EvidenceReady& r, c
         return FBLS_ERR_CUDA;
     if (!check(cudaMemsetAsync(ws + o_hist, 0, (o_parts - o_hist) * sizeof(double), stream), "evidence zero"))
         return FBLS_ERR_CUDA;
-    const size_t smem = 3 * nb2 * sizeof(double);
-    const int use_smem = smem <= FOLD2_SMEM_MAX ? 1 : 0;
-    if (use_smem) {
-        if (!check(cudaFuncSetAttribute(k_fold_two, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FOLD2_SMEM_MAX),
-                   "fold_two attribute"))
-            return FBLS_ERR_CUDA;
-    }
-    int blocks = (int)((r.n + FOLD2_THREADS * 16 - 1) / (FOLD2_THREADS * 16));
-    blocks = std::max(1, std::min(blocks, 64));
-    k_fold_two<<<blocks, FOLD2_THREADS, use_smem ? smem : 0, stream>>>(r.time, r.v, r.w, (int)r.n, scale, (int)nb2,
-                                                                      ws + o_hist, use_smem);
-    k_prefix_fields<<<1, 96, 0, stream>>>(ws + o_hist, ws + o_cum, (int)nb2);
+    // fold_two (evidence.rs:75-92): bin = floor(t * scale) mod 2 nb.
+    FoldArgs fa{};
+    fa.time = r.time;
+    fa.v = r.v;
+    fa.w = r.w;
+    fa.scales = ws + o_scale;
+    fa.n = (int)r.n;
+    fa.nb = (int)nb2;
+    fa.periods = 1;
+    fa.group = 1;
+    fa.hist_global = fold_smem ? nullptr : ws + o_fscratch;
+    fa.hist_out = ws + o_hist;
+    fa.chunks = reinterpret_cast<const int*>(ws + o_chunks);
+    fa.nchunks = nchunks;
+    fa.stage_field = shape.stage_field;
+    fa.window = shape.window;
+    fa.row_stride = shape.row_stride;
+    if (!check(launch_fold(fa, shape, stream), "evidence fold")) return FBLS_ERR_CUDA;
+    k_prefix_fields<<<3, 256, 0, stream>>>(ws + o_hist, ws + o_cum, (int)nb2);
     EvArgs ea;
     ea.cum = ws + o_cum;
     ea.durations = ws + o_dur;

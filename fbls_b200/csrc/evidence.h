@@ -20,6 +20,8 @@ struct EvidenceReady {
     double baseline_norm;
     double origin;
     double residual_energy;
+    double t_last;            // last relative time
+    const double* time_host;  // host copy of time (fold chunk boundaries)
 };
 
 // compare_search (src/search/evidence.rs:693-1003). `workspace(bytes)`

@@ -9,6 +9,7 @@
 // The device work differs from the reference's: fold and prefix run as one
 // kernel with the histograms in shared memory, all batches of a band are
 // queued on one stream, and the band's records come back in one copy.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -46,7 +47,8 @@ struct fbls_ctx {
     fbls_counters counters{};
     // Workspace, grown on demand and reused across bands and calls.
     DevBuf bank, scales, periods, cum, cum32, hist, parts, keys, tflags, records, score, depth, rflags;
-    DevBuf evidence;
+    DevBuf evidence, chunks;
+    std::vector<int> host_chunks;
 };
 
 struct fbls_ready {
@@ -59,6 +61,7 @@ struct fbls_ready {
     double origin = 0.0;
     double residual_energy = 0.0;
     double t_last = 0.0;
+    std::vector<double> time_host;  // for the fold's chunk boundaries
 };
 
 namespace {
@@ -122,16 +125,22 @@ struct BandOut {
     std::vector<uint32_t> flags;
 };
 
-// Periods per fold CTA: enough CTAs to cover the SMs twice, as many periods
-// as fit in ~96 KiB of shared memory (two CTAs per SM).
-int fold_group(int nb, int periods, int sm_count) {
-    const size_t per = (size_t)nb * fold_bytes_per_bin;
-    int by_smem = (int)((96 * 1024) / per);
-    if (by_smem < 1) by_smem = 1;
-    int by_fill = (periods + 2 * sm_count - 1) / (2 * sm_count);
-    if (by_fill < 1) by_fill = 1;
-    int g = by_smem < by_fill ? by_smem : by_fill;
-    return g > MAX_GROUP ? MAX_GROUP : g;
+// Fold shape for a launch of up to `periods` periods at nb bins, and the
+// family's fold chunks for scales up to scale_max, uploaded to the device.
+int plan_fold(fbls_ctx* ctx, const fbls_ready* r, double scale_max, int nb, int periods, FoldShape* shape,
+              int* nchunks) {
+    *shape = fold_group_shape(nb, periods, ctx->sm_count);
+    std::vector<int>& h = ctx->host_chunks;
+    h.resize((size_t)r->n + 2);
+    const int count = fold_chunks(r->time_host.data(), (int)r->n, scale_max, nb, shape->span_cap, shape->chunk_cap,
+                                  h.data(), (int)h.size());
+    if (count < 1) return fail(ctx, FBLS_ERR_ARGUMENT, "fold chunking failed");
+    CK(ensure(ctx->chunks, ((size_t)count + 1) * sizeof(int)), "workspace");
+    CK(cudaMemcpyAsync(ctx->chunks.ptr, h.data(), ((size_t)count + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                       ctx->stream),
+       "upload chunks");
+    *nchunks = count;
+    return FBLS_OK;
 }
 
 // One scan_bank pass (scan.rs:144-357) of `periods` at nb bins.
@@ -159,7 +168,8 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
     if (budget < batch) batch = budget;
     if (P < batch) batch = P;
     if (batch == 0) batch = 1;
-    // The phase cell floor(t * scale) must fit u32 (kernels.rs:315).
+    // The phase cell floor(t * scale) must fit u32 (kernels.rs:315), with room
+    // for the fold's cell arithmetic (cell + 2 nb).
     double scale_max = 0.0;
     std::vector<double> scales(P);
     for (uint32_t i = 0; i < P; i++) {
@@ -168,7 +178,7 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
             return fail(ctx, FBLS_ERR_ARGUMENT, "periods must be positive and finite");
         if (scales[i] > scale_max) scale_max = scales[i];
     }
-    if (std::floor(r->t_last * scale_max) >= 4294967295.0)
+    if (std::floor(r->t_last * scale_max) >= 4294967295.0 - 2.0 * (double)nb - 2.0)
         return fail(ctx, FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
 
     const size_t stride = 2 * (size_t)nb + 1;
@@ -184,8 +194,16 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
     CK(ensure(ctx->score, (size_t)P * sizeof(double)), "workspace");
     CK(ensure(ctx->depth, (size_t)P * sizeof(double)), "workspace");
     CK(ensure(ctx->rflags, (size_t)P * sizeof(uint32_t)), "workspace");
-    const bool shared_fold = (size_t)nb * fold_bytes_per_bin <= MAX_FOLD_SMEM;
-    if (!shared_fold) CK(ensure(ctx->hist, batch * NF * (size_t)nb * sizeof(double)), "workspace");
+    FoldShape shape;
+    int nchunks = 0;
+    {
+        int rc = plan_fold(ctx, r, scale_max, (int)nb, (int)batch, &shape, &nchunks);
+        if (rc) return rc;
+    }
+    if (!shape.hist_in_smem) {
+        const size_t blocks = (batch + shape.group - 1) / shape.group;
+        CK(ensure(ctx->hist, blocks * shape.group * NF * (size_t)nb * sizeof(double)), "workspace");
+    }
 
     cudaStream_t s = ctx->stream;
     CK(cudaMemcpyAsync(ctx->bank.ptr, host_bank.data(), host_bank.size() * sizeof(double), cudaMemcpyHostToDevice, s),
@@ -220,15 +238,16 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
         fa.cum = as<double>(ctx->cum);
         fa.cum32 = as<float2>(ctx->cum32);
         if (timing) CK(cudaEventRecord(ctx->pool[3 * bi], s), "event");
-        if (shared_fold) {
-            fa.group = fold_group((int)nb, p, ctx->sm_count);
-            size_t smem = (size_t)fa.group * nb * fold_bytes_per_bin;
-            CK(launch_fold_prefix(fa, smem, s), "fold_prefix");
-            ctx->counters.launches += 1;
-        } else {
-            CK(launch_fold_global(fa, as<double>(ctx->hist), s), "fold_global");
-            ctx->counters.launches += 2;
-        }
+        fa.group = shape.group;
+        fa.hist_global = shape.hist_in_smem ? nullptr : as<double>(ctx->hist);
+        fa.hist_out = nullptr;
+        fa.chunks = as<int>(ctx->chunks);
+        fa.nchunks = nchunks;
+        fa.stage_field = shape.stage_field;
+        fa.window = shape.window;
+        fa.row_stride = shape.row_stride;
+        CK(launch_fold(fa, shape, s), "fold");
+        ctx->counters.launches += 1;
         ctx->counters.fold_launches += 1;
         ctx->counters.fold_bytes += (double)p * (24.0 * r->n + 48.0 * (double)stride);
         ctx->counters.fold_updates += (uint64_t)p * r->n;
@@ -406,7 +425,8 @@ void fbls_destroy(fbls_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf* bufs[] = {&ctx->bank,  &ctx->scales,  &ctx->periods, &ctx->cum,   &ctx->cum32,  &ctx->hist,    &ctx->parts,
-                      &ctx->keys,  &ctx->tflags,  &ctx->records, &ctx->score, &ctx->depth,  &ctx->rflags,  &ctx->evidence};
+                      &ctx->keys,  &ctx->tflags,  &ctx->records, &ctx->score, &ctx->depth,  &ctx->rflags,  &ctx->evidence,
+                      &ctx->chunks};
     for (DevBuf* b : bufs) release(*b);
     for (int i = 0; i < 4; i++)
         if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -463,6 +483,7 @@ int fbls_upload_ready(fbls_ctx* ctx, const double* time, const double* v, const 
     r->origin = origin;
     r->residual_energy = residual_energy;
     r->t_last = time[n - 1];
+    r->time_host.assign(time, time + n);
     const size_t bytes = (size_t)n * sizeof(double);
     cudaError_t e = cudaMalloc(&r->time, 3 * bytes);
     if (e != cudaSuccess) {
@@ -638,7 +659,7 @@ int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* du
         return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
     CK(cudaSetDevice(ctx->device), "set device");
     EvidenceReady er{ready->time, ready->v, ready->w, ready->n, ready->baseline_norm, ready->origin,
-                     ready->residual_energy};
+                     ready->residual_energy, ready->t_last, ready->time_host.data()};
     std::string message;
     int rc = compare_search(ctx->stream, ctx->evidence.ptr, ctx->evidence.bytes, er, durations, rho, nd, period, *cfg,
                             rows_out, n_rows, message, [&](size_t bytes) -> void* {

@@ -7,10 +7,8 @@
 
 namespace fbls {
 
-constexpr int FOLD_THREADS = 512;
 constexpr int MAX_GROUP = 32;               // periods per fold CTA
-constexpr size_t MAX_FOLD_SMEM = 225 * 1024;  // dynamic shared memory of k_fold_prefix
-constexpr int GLOBAL_FOLD_PERIODS = 4;
+constexpr size_t MAX_FOLD_SMEM = 225 * 1024;  // dynamic shared memory of k_fold
 constexpr int MAX_DURATIONS = 64;
 constexpr int MAX_SHAPES = 8;
 constexpr int MAX_LAYERS = 16;
@@ -26,9 +24,29 @@ struct FoldArgs {
     int n;
     int nb;
     int periods;
-    int group;             // periods per CTA (shared-memory path)
+    int group;             // periods per CTA
     double* cum;           // periods x NF x (2nb+1)
     float2* cum32;         // periods x NF x (2nb+1) (hi, lo)
+    double* hist_global;   // null: histograms in shared memory; else 3 G nb doubles per CTA
+    double* hist_out;      // non-null (one period): write the raw histogram [3][nb], no prefix
+    const int* chunks;     // nchunks + 1 observation offsets (fold_chunks)
+    int nchunks;
+    int stage_field;       // staged slots per field (FoldShape::stage_field)
+    int window;            // 0: whole histogram in shared memory; else window rows
+    int row_stride;        // FoldShape::row_stride
+};
+
+// Launch shape of k_fold (fold_group_shape).
+struct FoldShape {
+    int group;          // periods per CTA, a power of two <= MAX_GROUP
+    bool hist_in_smem;  // else window mode: 3 G nb doubles of global histogram per CTA
+    int window;         // 0 (full mode) or the window's rows (cells)
+    int row_stride;     // shared-memory row stride of a period's bins
+    int span_cap;       // cells a chunk may span (window mode)
+    int chunk_cap;      // observations per chunk at most
+    int threads;        // CTA size
+    int stage_field;    // staged slots per field: chunk_cap + segments
+    size_t smem;        // dynamic shared memory bytes
 };
 
 struct ScanArgs {
@@ -64,8 +82,13 @@ struct MergeArgs {
     uint32_t* flags_out;
 };
 
-cudaError_t launch_fold_prefix(const FoldArgs& a, size_t smem_bytes, cudaStream_t stream);
-cudaError_t launch_fold_global(const FoldArgs& a, double* hist, cudaStream_t stream);
+FoldShape fold_group_shape(int nb, int periods, int sm_count);
+// Cuts n ascending times into fold chunks of at most chunk_cap observations
+// spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.
+// Writes count + 1 offsets; returns count, or -1 when capacity is too small.
+int fold_chunks(const double* time, int n, double scale_max, int nb, int span_cap, int chunk_cap, int* out,
+                int capacity);
+cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream);
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream);
 cudaError_t launch_merge(const MergeArgs& a, cudaStream_t stream);
 

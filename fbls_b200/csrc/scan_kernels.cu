@@ -2,14 +2,7 @@
 // sm_100a. Semantics follow src/search/kernels.rs; the layout of the work on
 // the GPU is this project's own:
 //
-//  * k_fold_prefix: one CTA per group of G periods. The CTA streams the
-//    family's observations once per group and bins them into G shared-memory
-//    histograms (f64 v and w, u32 count), then turns each histogram into the
-//    doubled exclusive prefix sums (f64 and (hi, lo) f32 pairs) with a
-//    warp-shuffle scan per (period, field) row. The histogram never leaves
-//    the SM (the reference writes it to HBM and re-reads it, scan.rs:230-292).
-//  * k_fold_global + k_prefix_global: the same for phase grids whose
-//    histograms do not fit shared memory.
+//  * the fold and prefix sums are in fold.cu;
 //  * k_scan_tiles: one CTA of TILE lanes per (tile, period), the reference's
 //    two-pass f32 pre-rank / f64 rescan (kernels.rs:610-845).
 //  * k_merge: best tile per period (kernels.rs:1115-1155).
@@ -17,131 +10,6 @@
 #include "kernels.h"
 
 namespace fbls {
-
-// floor(t * scale) mod nb for t >= 0 (kernels.rs:314-327). The multiply is
-// one rounded f64 product; the remainder is integer arithmetic.
-__device__ __forceinline__ uint32_t phase_cell(double t, double scale, uint32_t nb) {
-    double x = floor(__dmul_rn(t, scale));
-    uint32_t v = (uint32_t)x;
-    return v % nb;
-}
-
-__device__ __forceinline__ float2 split_pair(double value) {
-    float hi = __double2float_rn(value);
-    float lo = __double2float_rn(__dsub_rn(value, (double)hi));
-    return make_float2(hi, lo);
-}
-
-// Writes one doubled prefix row (2nb+1 entries, f64 and pairs) from a row of
-// bin values read through `load`, by one warp. Order of additions: inclusive
-// Hillis-Steele scan over 32 bins, plus the running carry of earlier chunks.
-template <typename Load>
-__device__ __forceinline__ void prefix_row_warp(Load load, int nb, double* __restrict__ out64,
-                                                float2* __restrict__ out32) {
-    const int lane = threadIdx.x & 31;
-    double carry = 0.0;
-    if (lane == 0) {
-        out64[0] = 0.0;
-        out32[0] = make_float2(0.f, 0.f);
-    }
-    for (int base = 0; base < nb; base += 32) {
-        int b = base + lane;
-        double x = b < nb ? load(b) : 0.0;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            double o = __shfl_up_sync(0xffffffffu, x, off);
-            if (lane >= off) x = __dadd_rn(x, o);
-        }
-        double val = __dadd_rn(carry, x);
-        if (b < nb) {
-            out64[b + 1] = val;
-            out32[b + 1] = split_pair(val);
-        }
-        carry = __shfl_sync(0xffffffffu, val, 31);
-    }
-    const double total = carry;
-    for (int b = lane; b < nb; b += 32) {
-        double val = __dadd_rn(out64[b + 1], total);
-        out64[nb + b + 1] = val;
-        out32[nb + b + 1] = split_pair(val);
-    }
-}
-
-__global__ void __launch_bounds__(FOLD_THREADS) k_fold_prefix(FoldArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int nb = a.nb;
-    const int g0 = blockIdx.x * a.group;
-    const int g = min(a.group, a.periods - g0);
-    double* hv = reinterpret_cast<double*>(smem);
-    double* hw = hv + (size_t)a.group * nb;
-    uint32_t* hc = reinterpret_cast<uint32_t*>(hw + (size_t)a.group * nb);
-    __shared__ double s_scale[MAX_GROUP];
-    if (threadIdx.x < g) s_scale[threadIdx.x] = a.scales[g0 + threadIdx.x];
-    for (int i = threadIdx.x; i < g * nb; i += blockDim.x) {
-        hv[i] = 0.0;
-        hw[i] = 0.0;
-        hc[i] = 0u;
-    }
-    __syncthreads();
-    const uint32_t unb = (uint32_t)nb;
-    for (int i = threadIdx.x; i < a.n; i += blockDim.x) {
-        const double t = a.time[i];
-        const double xv = a.v[i];
-        const double xw = a.w[i];
-        for (int q = 0; q < g; q++) {
-            uint32_t cell = phase_cell(t, s_scale[q], unb) + (uint32_t)(q * nb);
-            atomicAdd(&hv[cell], xv);
-            atomicAdd(&hw[cell], xw);
-            atomicAdd(&hc[cell], 1u);
-        }
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5;
-    const int nwarps = blockDim.x >> 5;
-    const size_t stride = 2 * (size_t)nb + 1;
-    for (int row = warp; row < g * NF; row += nwarps) {
-        const int q = row / NF, f = row % NF;
-        double* out64 = a.cum + ((size_t)(g0 + q) * NF + f) * stride;
-        float2* out32 = a.cum32 + ((size_t)(g0 + q) * NF + f) * stride;
-        const size_t off = (size_t)q * nb;
-        if (f == F_V)
-            prefix_row_warp([&](int b) { return hv[off + b]; }, nb, out64, out32);
-        else if (f == F_W)
-            prefix_row_warp([&](int b) { return hw[off + b]; }, nb, out64, out32);
-        else
-            prefix_row_warp([&](int b) { return (double)hc[off + b]; }, nb, out64, out32);
-    }
-}
-
-// Global-memory histogram for grids too large for shared memory. Layout
-// hist[period][field][nb]; zeroed by the caller.
-__global__ void k_fold_global(FoldArgs a, double* __restrict__ hist) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    const double t = a.time[i];
-    const double xv = a.v[i], xw = a.w[i];
-    const uint32_t unb = (uint32_t)a.nb;
-    const int p0 = blockIdx.y * GLOBAL_FOLD_PERIODS;
-    const int p1 = min(p0 + GLOBAL_FOLD_PERIODS, a.periods);
-    for (int p = p0; p < p1; p++) {
-        uint32_t cell = phase_cell(t, a.scales[p], unb);
-        double* h = hist + (size_t)p * NF * a.nb;
-        atomicAdd(&h[cell], xv);
-        atomicAdd(&h[a.nb + cell], xw);
-        atomicAdd(&h[2 * (size_t)a.nb + cell], 1.0);
-    }
-}
-
-// One CTA of NF warps per period: warp f scans field f.
-__global__ void k_prefix_global(FoldArgs a, const double* __restrict__ hist) {
-    const int p = blockIdx.x;
-    const int f = threadIdx.x >> 5;
-    const size_t stride = 2 * (size_t)a.nb + 1;
-    const double* h = hist + ((size_t)p * NF + f) * a.nb;
-    double* out64 = a.cum + ((size_t)p * NF + f) * stride;
-    float2* out32 = a.cum32 + ((size_t)p * NF + f) * stride;
-    prefix_row_warp([&](int b) { return h[b]; }, a.nb, out64, out32);
-}
 
 // ---------------------------------------------------------------------------
 // Tile scan (kernels.rs:610-845).
@@ -482,30 +350,6 @@ __global__ void k_merge(MergeArgs a) {
 // ---------------------------------------------------------------------------
 // Launchers.
 // ---------------------------------------------------------------------------
-
-cudaError_t launch_fold_prefix(const FoldArgs& a, size_t smem_bytes, cudaStream_t stream) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_fold_prefix, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)MAX_FOLD_SMEM);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
-    int blocks = (a.periods + a.group - 1) / a.group;
-    k_fold_prefix<<<blocks, FOLD_THREADS, smem_bytes, stream>>>(a);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_fold_global(const FoldArgs& a, double* hist, cudaStream_t stream) {
-    cudaError_t e = cudaMemsetAsync(hist, 0, (size_t)a.periods * NF * a.nb * sizeof(double), stream);
-    if (e != cudaSuccess) return e;
-    dim3 grid((a.n + 255) / 256, (a.periods + GLOBAL_FOLD_PERIODS - 1) / GLOBAL_FOLD_PERIODS);
-    k_fold_global<<<grid, 256, 0, stream>>>(a, hist);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    k_prefix_global<<<a.periods, 32 * NF, 0, stream>>>(a, hist);
-    return cudaGetLastError();
-}
 
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream) {
     dim3 grid((a.nb + TILE - 1) / TILE, periods);

@@ -721,7 +721,52 @@ void scan_tile(const PeriodView& P, double scale, const Bank& B, int tile, bool 
     out_flags = (uint32_t)retry | ((uint32_t)bad_any << 1);
 }
 
-// Sequential fold in observation order, then the doubled prefix sums.
+// Inclusive scan of 32 values in the order of a warp-shuffle Hillis-Steele
+// scan (kernels.rs:221-232): step `off` adds the value `off` lanes below.
+inline void warp_scan32(double x[32]) {
+    for (int off = 1; off < 32; off <<= 1) {
+        double prev[32];
+        std::memcpy(prev, x, sizeof(prev));
+        for (int l = off; l < 32; l++) x[l] = prev[l] + prev[l - off];
+    }
+}
+
+// Doubled exclusive prefix of one field row with the association of the
+// reference's prefix_block (kernels.rs:237-309): segments of 256 bins, each
+// scanned as 8 warps of 32 (Hillis-Steele), warp offsets = carry plus the
+// earlier warp totals in order, the carry grows by the sum of the 8 totals;
+// the second copy is the first plus the final carry.
+void prefix_row(const double* h, int nb, double* row) {
+    row[0] = 0.0;
+    double carry = 0.0;
+    for (int seg = 0; seg < nb; seg += 256) {
+        double local[8][32], wt[8];
+        for (int wi = 0; wi < 8; wi++) {
+            for (int l = 0; l < 32; l++) {
+                int b = seg + wi * 32 + l;
+                local[wi][l] = b < nb ? h[b] : 0.0;
+            }
+            warp_scan32(local[wi]);
+            wt[wi] = local[wi][31];
+        }
+        for (int wi = 0; wi < 8; wi++) {
+            double offset = carry;
+            for (int u = 0; u < wi; u++) offset += wt[u];
+            for (int l = 0; l < 32; l++) {
+                int b = seg + wi * 32 + l;
+                if (b < nb) row[b + 1] = local[wi][l] + offset;
+            }
+        }
+        double total = 0.0;
+        for (int wi = 0; wi < 8; wi++) total += wt[wi];
+        carry += total;
+    }
+    for (int b = 0; b < nb; b++) row[nb + b + 1] = row[b + 1] + carry;
+}
+
+// Fold in observation order (each bin's additions in increasing observation
+// index, one valid order of the reference's unordered atomics), then the
+// doubled prefix sums and their (hi, lo) f32 pairs.
 void fold_and_prefix(const double* time, const double* v, const double* w, int64_t n, double scale, int nb,
                      std::vector<double>& folded, std::vector<double>& cum, std::vector<float>& cum32) {
     folded.assign((size_t)nb * NF, 0.0);
@@ -737,12 +782,11 @@ void fold_and_prefix(const double* time, const double* v, const double* w, int64
     int stride = 2 * nb + 1;
     cum.assign((size_t)NF * stride, 0.0);
     cum32.assign((size_t)NF * stride * 2, 0.0f);
+    std::vector<double> field(nb);
     for (int f = 0; f < NF; f++) {
         double* row = &cum[(size_t)f * stride];
-        row[0] = 0.0;
-        for (int b = 0; b < nb; b++) row[b + 1] = row[b] + folded[(size_t)b * NF + f];
-        double total = row[nb];
-        for (int b = 0; b < nb; b++) row[nb + b + 1] = row[b + 1] + total;
+        for (int b = 0; b < nb; b++) field[b] = folded[(size_t)b * NF + f];
+        prefix_row(field.data(), nb, row);
         float* r32 = &cum32[(size_t)f * stride * 2];
         for (int b = 0; b < stride; b++) {
             float hi = (float)row[b];
@@ -1394,11 +1438,24 @@ extern "C" int orc_compare_search(const double* time, const double* v, const dou
         folded[1 * nb2 + cell] += w[i];
         folded[2 * nb2 + cell] += 1.0;
     }
+    // prefix_fields (evidence.rs:96-144): per segment of 256 bins a block-wide
+    // Hillis-Steele scan (stride 1 .. 128), plus the running carry.
     std::vector<double> cum(3 * (nb2 + 1), 0.0);
     for (int f = 0; f < 3; f++) {
         double* row = &cum[(size_t)f * (nb2 + 1)];
         row[0] = 0.0;
-        for (size_t b = 0; b < nb2; b++) row[b + 1] = row[b] + folded[f * nb2 + b];
+        double carry = 0.0;
+        for (size_t seg = 0; seg < nb2; seg += 256) {
+            double scan[256], prev[256];
+            for (int l = 0; l < 256; l++) scan[l] = seg + l < nb2 ? folded[f * nb2 + seg + l] : 0.0;
+            for (int stride = 1; stride < 256; stride <<= 1) {
+                std::memcpy(prev, scan, sizeof(prev));
+                for (int l = stride; l < 256; l++) scan[l] = prev[l] + prev[l - stride];
+            }
+            for (int l = 0; l < 256; l++)
+                if (seg + l < nb2) row[seg + l + 1] = scan[l] + carry;
+            carry += scan[255];
+        }
     }
     EvidenceInputs E{cum.data(), scale, durations.data(), rho.data(), dlm.data(), shapes.data(), priors.data(), params,
                      orbit.data(), baseline_norm, threshold, (double)n, nb2, nd, ns, layers};

@@ -1,14 +1,12 @@
 """Parity of the CUDA scan path with the oracle, through the C ABI.
 
-Bar: exact phase / width / shape / duration indices per period, and score and
-depth within 1e-6 relative (the tolerance the path is specified to), except
-at genuine near-ties. The reference folds with unordered f64 atomics
-(kernels.rs:491, :540), so its own winners are not reproducible bit for bit
-where two templates tie to rounding; such periods are counted and must stay
-rare, and their scores must still agree to 1e-6.
+The fold adds each bin's observations in time order and the prefix sums use
+the reference's association (kernels.rs:237-309) on both sides, and every
+later operation rounds the same way (no fused multiply-adds), so the device
+results must equal the oracle's bit for bit: phase, width, shape and
+duration indices, a, norm, d, score and depth. This is stricter than the
+path's 1e-6 tolerance on power, which is also asserted explicitly.
 """
-import math
-
 import numpy as np
 import pytest
 
@@ -20,27 +18,17 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-6
 
 
-def _compare_records(g, o, max_tie_fraction=0.002):
+def _compare_records(g, o):
     grec, gscore, gdepth, gflags = g[:4]
     orec, oscore, odepth, oflags = o[:4]
     assert grec.shape == orec.shape
-    assert np.array_equal(grec[:, 0], orec[:, 0])  # period
-    assert np.array_equal(grec[:, 1], orec[:, 1])  # scale
     finite = np.isfinite(oscore)
-    assert np.array_equal(finite, np.isfinite(gscore))
-    same_key = (grec[:, 2] == orec[:, 2]) & (grec[:, 3] == orec[:, 3]) & (grec[:, 7] == orec[:, 7]) & (
-        grec[:, 8] == orec[:, 8])
     rel = np.abs(gscore[finite] - oscore[finite]) / np.abs(oscore[finite])
     assert rel.max(initial=0.0) <= RTOL, rel.max()
-    ties = ~same_key & finite
-    assert ties.mean() <= max_tie_fraction, (ties.sum(), np.nonzero(ties)[0][:10])
-    m = same_key & finite
-    drel = np.abs(gdepth[m] - odepth[m]) / np.maximum(np.abs(odepth[m]), 1e-300)
-    assert drel.max(initial=0.0) <= RTOL
-    # Unusable periods decode the same fallback template.
-    assert np.array_equal(same_key[~finite], np.ones((~finite).sum(), bool))
-    assert np.array_equal(gflags & 2, oflags & 2)
-    return int(ties.sum())
+    bad = np.nonzero(~(grec == orec).all(axis=1) | (gscore != oscore) | (gdepth != odepth))[0]
+    assert bad.size == 0, (bad[:5], grec[bad[:2]], orec[bad[:2]], gscore[bad[:2]], oscore[bad[:2]])
+    assert np.array_equal(gflags & 3, oflags & 3)
+    return 0
 
 
 @pytest.fixture(scope="module")
@@ -74,11 +62,7 @@ def test_signal_search_parity_small(gpu, small):
     rows, glen, stats = gpu.signal_search(st, cfg)
     orows, ogrid, ostats = oracle.signal_search(ost, cfg)
     assert glen == len(ogrid)
-    assert rows.shape == orows.shape
-    assert np.array_equal(rows[:, 0], orows[:, 0])
-    np.testing.assert_allclose(rows[:, 3], orows[:, 3], rtol=RTOL)
-    same = (rows[:, 1] == orows[:, 1]) & (rows[:, 2] == orows[:, 2])
-    assert same.mean() >= 0.99
+    assert np.array_equal(rows, orows)
     for s, o in zip(stats, ostats):
         for key in ("periods", "prescan_survivors", "phase_bins", "templates_scanned"):
             assert s[key] == o[key], key
@@ -94,7 +78,7 @@ def test_global_fold_path(gpu, small):
     nb = 12000
     g = gpu.scan_bank(dev, periods, bank, nb)
     o = oracle.scan_bank(ost, periods, nb, d, bank.rho)
-    _compare_records(g, o, max_tie_fraction=0.0)
+    _compare_records(g, o)
 
 
 def test_budget_error_keeps_reference_message(gpu, small):
@@ -105,24 +89,34 @@ def test_budget_error_keeps_reference_message(gpu, small):
         gpu.scan_bank(dev, [1.0], bank, 64)
 
 
-def _subsample_parity(gpu, curve, cfg, every, max_tie_fraction=0.002):
+def test_fold_is_deterministic(gpu, small):
+    c, cfg, st, ost = small
+    dev = gpu.upload(st)
+    grid, bands = api.band_plan(st, cfg)
+    band = bands[-1]
+    bank = api.bank_for(band, cfg)
+    first = gpu.scan_bank(dev, band["periods"], bank, band["nb"])
+    for _ in range(3):
+        again = gpu.scan_bank(dev, band["periods"], bank, band["nb"])
+        for x, y in zip(first[:4], again[:4]):
+            assert np.array_equal(x, y)
+
+
+def _subsample_parity(gpu, curve, cfg, every):
     st = api.prepared_family(curve.time, curve.flux, curve.flux_err, cfg)
     ost = oracle.family_state(curve.time, curve.flux, curve.flux_err, cfg.durations_days())
     assert np.array_equal(st.v, ost.v)
     dev = gpu.upload(st)
     grid, bands = api.band_plan(st, cfg)
-    ties = 0
-    total = 0
     for band in bands:
         sel = band["periods"][::every]
         bank = api.bank_for(band, cfg)
         for nb in (band["nb"] // 2, band["nb"]):
-            g = gpu.scan_bank(dev, sel, bank, nb)
-            o = oracle.scan_bank(ost, sel, nb, band["durations"], band["rho"], ingress=cfg.ingress_fractions,
-                                 layers=cfg.shape_layers, shape_gate=bank.shape_gate)
-            ties += _compare_records(g, o, max_tie_fraction=max(max_tie_fraction, 1.0 / len(sel)))
-            total += len(sel)
-    assert ties <= max(1, max_tie_fraction * total)
+            for mode in (0, 1):
+                g = gpu.scan_bank(dev, sel, bank, nb, precision_mode=mode)
+                o = oracle.scan_bank(ost, sel, nb, band["durations"], band["rho"], ingress=cfg.ingress_fractions,
+                                     layers=cfg.shape_layers, shape_gate=bank.shape_gate, mode=mode)
+                _compare_records(g, o)
 
 
 def test_single_sector_full_size_parity(gpu):

@@ -94,8 +94,9 @@ def test_prefix_matches_direct_box_sums(small_state):
     # (hi, lo) pairs represent the f64 prefix to f32 x f32 precision.
     rec = cum32[..., 0].astype(np.float64) + cum32[..., 1].astype(np.float64)
     assert np.all(np.abs(rec - cum) <= 1e-13 * np.abs(cum).max())
-    # Second copy = first + total.
-    assert np.array_equal(cum[:, nb + 1:], cum[:, 1:nb + 1] + cum[:, nb:nb + 1])
+    # Second copy = first + the row total (the carry of the segment scan).
+    total = cum[:, nb:nb + 1]
+    assert np.all(np.abs(cum[:, nb + 1:] - (cum[:, 1:nb + 1] + total)) <= 4e-16 * np.abs(cum).max())
 
 
 def test_winner_is_the_f64_argmax_in_f64_mode(small_state):
