@@ -560,7 +560,7 @@ int compare_search(cudaStream_t stream, void*, size_t, const EvidenceReady& r, c
     const size_t o_chunks = put(packed);
     const bool fold_smem = shape.hist_in_smem;
     const size_t o_fscratch = consts.size();
-    const size_t o_hist = o_fscratch + (fold_smem ? 0 : 3 * nb2);
+    const size_t o_hist = o_fscratch + (fold_smem ? 0 : 3 * (size_t)shape.row_stride);
     const size_t o_cum = o_hist + 3 * nb2;
     const size_t o_screen = o_cum + 3 * (nb2 + 1);
     const size_t o_parts = o_screen + (size_t)tiles * 4;

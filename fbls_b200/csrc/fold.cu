@@ -1,24 +1,20 @@
 // Deterministic phase fold and doubled prefix sums on sm_100a.
 //
-// One CTA folds G periods (a power of two, at most 32) of one family.
-// Because times are sorted, the cell floor(t * scale) never decreases along
-// the observations, so every cell is one contiguous run of observations.
-// The CTA needs no atomic:
+// One CTA folds G periods (a power of two) of one family, with 32 / G of its
+// warps per period. Because times are sorted, the cell floor(t * scale)
+// never decreases along the observations, so every cell is one contiguous
+// run of observations. The CTA needs no atomic:
 //
 //   1. the observations are cut (on the host) into chunks spanning at most
-//      min(nb - 2, SPAN) cells at every period of the launch, so the cells of
-//      one chunk fall in distinct bins;
-//   2. the chunk is split into NS equal segments. Lane (q, s) of the CTA owns
-//      period q and segment s and folds every run that starts in its
-//      segment, continuing past the segment's end while the run lasts: it
-//      loads the bin's sums, adds the run's observations one by one, and
-//      stores them back. With G = 32 a warp's lanes are the 32 periods of one
-//      segment: they step through the same observations together, so every
-//      shared-memory read is a broadcast and loop control is shared.
-//   3. the bins live in shared memory: the whole histogram when it fits
-//      ("full" mode), otherwise a window of the chunk's cells, loaded from
-//      and stored back to a global histogram around each chunk ("window"
-//      mode; the cells of a chunk are consecutive, so its bins are too).
+//      nb - 2 cells at every period of the launch, so the cells of one chunk
+//      fall in distinct bins; a chunk is staged in shared memory;
+//   2. each period's lanes split the chunk into equal segments, and every
+//      lane moves its segment's start forward to the first run boundary of
+//      its own period at or after it; a lane folds the runs from its start
+//      up to the next lane's start, so every run belongs to exactly one lane;
+//   3. the lanes of a warp step through their runs together, one
+//      observation per step: add (v, w) to the run's sums, and at a cell
+//      boundary store the sums to the bin and load the next bin's.
 //
 // Each bin's sums are thus formed in observation order, exactly as a
 // sequential fold does, so the result is reproducible run to run and equal
@@ -43,6 +39,10 @@ __device__ __forceinline__ uint32_t mod_nb(uint32_t v, uint32_t nb, double inv_n
     else if (r >= nb)
         r -= nb;
     return r;
+}
+
+__device__ __forceinline__ uint32_t cell_of(double t, double scale) {
+    return (uint32_t)floor(__dmul_rn(t, scale));
 }
 
 __device__ __forceinline__ float2 split_pair(double value) {
@@ -94,10 +94,9 @@ __device__ __forceinline__ void prefix_row(Load load, int nb, double* __restrict
     }
 }
 
-__global__ void __launch_bounds__(512, 2) k_fold(FoldArgs a) {
+__global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ double s_scale[MAX_GROUP];
-    __shared__ uint32_t s_v0[MAX_GROUP], s_r0[MAX_GROUP];
 
     const int tid = threadIdx.x;
     const int T = blockDim.x;
@@ -106,50 +105,45 @@ __global__ void __launch_bounds__(512, 2) k_fold(FoldArgs a) {
     const int nb = a.nb;
     const uint32_t unb = (uint32_t)nb;
     const double inv_nb = 1.0 / (double)nb;
-    const int G = a.group;  // power of two <= 32
-    const int gshift = __ffs(G) - 1;
-    const int S = 32 / G;   // segments per warp
-    const int NS = (T / 32) * S;
+    const int G = a.group;          // periods per CTA, a power of two
+    const int wpp = (T / 32) / G;   // warps per period (>= 1)
+    const int NS = wpp * 32;        // segments per period
     const int g0 = blockIdx.x * G;
     const int g = min(G, a.periods - g0);
-    const int q = lane & (G - 1);
-    const int seg = warp * S + (lane >> gshift);
-    const bool full = a.window == 0;
-    const int rows = full ? nb : a.window;  // bins per period held in shared memory
-    const int rs = a.row_stride;            // >= rows, odd
+    const int q = warp / wpp;
+    const int seg = (warp - q * wpp) * 32 + lane;
+    const int rs = a.row_stride;    // >= nb
 
-    // Shared memory: staging t, v, w [stage_field] | sums v, w [G][rs] | counts [G][rs].
+    // Shared memory: staging t, v, w [stage_field] | run starts [G][NS + 1]
+    // (padded to 16 bytes) | sums v, w [G][rs] | counts [G][rs]; the sums
+    // and counts live in global scratch instead when hist_global is set.
     double* st = reinterpret_cast<double*>(smem);
     double* sv = st + a.stage_field;
     double* sw = sv + a.stage_field;
-    double* rv = sw + a.stage_field;
-    double* rw = rv + (size_t)G * rs;
-    uint32_t* rc = reinterpret_cast<uint32_t*>(rw + (size_t)G * rs);
-    // Global histogram of this CTA's periods (window mode): [3][G][nb].
-    double* gv = a.hist_global ? a.hist_global + (size_t)blockIdx.x * G * nb * 3 : nullptr;
-    double* gw = gv ? gv + (size_t)G * nb : nullptr;
-    uint32_t* gc = gv ? reinterpret_cast<uint32_t*>(gw + (size_t)G * nb) : nullptr;
+    int* starts = reinterpret_cast<int*>(sw + a.stage_field);
+    const size_t starts_bytes = ((size_t)G * (NS + 1) * sizeof(int) + 15) & ~(size_t)15;
+    double* hv = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(starts) + starts_bytes);
+    double* hw = hv + (size_t)G * rs;
+    uint32_t* hc = reinterpret_cast<uint32_t*>(hw + (size_t)G * rs);
+    if (a.hist_global) {
+        hv = a.hist_global + (size_t)blockIdx.x * G * rs * 3;
+        hw = hv + (size_t)G * rs;
+        hc = reinterpret_cast<uint32_t*>(hw + (size_t)G * rs);
+    }
 
     if (tid < g) s_scale[tid] = a.scales[g0 + tid];
-    if (full) {
-        for (int e = tid; e < G * rs; e += T) {
-            rv[e] = 0.0;
-            rw[e] = 0.0;
-            rc[e] = 0u;
-        }
-    } else {
-        for (int e = tid; e < G * nb; e += T) {
-            gv[e] = 0.0;
-            gw[e] = 0.0;
-            gc[e] = 0u;
-        }
+    for (int e = tid; e < G * rs; e += T) {
+        hv[e] = 0.0;
+        hw[e] = 0.0;
+        hc[e] = 0u;
     }
     __syncthreads();
     const bool live = q < g;
     const double scale = live ? s_scale[q] : 0.0;
-    double* lv = rv + (size_t)q * rs;
-    double* lw = rw + (size_t)q * rs;
-    uint32_t* lc = rc + (size_t)q * rs;
+    double* lv = hv + (size_t)q * rs;
+    double* lw = hw + (size_t)q * rs;
+    uint32_t* lc = hc + (size_t)q * rs;
+    int* lstart = starts + q * (NS + 1);
 
     for (int c = 0; c < a.nchunks; c++) {
         const int i0 = a.chunks[c];
@@ -164,113 +158,89 @@ __global__ void __launch_bounds__(512, 2) k_fold(FoldArgs a) {
             sw[at] = a.w[i0 + k];
         }
         __syncthreads();
-        if (!full) {
-            // Window of the chunk's cells: slot u holds the bin of cell v0 + u.
-            if (tid < g) {
-                const uint32_t v0 = (uint32_t)floor(__dmul_rn(st[0], s_scale[tid]));
-                s_v0[tid] = v0;
-                s_r0[tid] = mod_nb(v0, unb, inv_nb);
-            }
-            __syncthreads();
-            for (int e = tid; e < g * rows; e += T) {
-                const int qq = e / rows, u = e - qq * rows;
-                uint32_t bin = s_r0[qq] + (uint32_t)u;
-                if (bin >= unb) bin -= unb;
-                const size_t src = (size_t)qq * nb + bin, dst = (size_t)qq * rs + u;
-                rv[dst] = gv[src];
-                rw[dst] = gw[src];
-                rc[dst] = gc[src];
-            }
-            __syncthreads();
-        }
 
-        const int a0 = seg * R;
-        const int e0 = min(a0 + R, len);
-        bool done = !live || a0 >= len;
-        bool skip = false;
-        int k = a0, j = 0, sk = seg, k0 = a0;
-        uint32_t slot = 0, c0 = 0, v0 = full ? 0u : (live ? s_v0[q] : 0u);
-        double nextb = 0.0, av = 0.0, aw = 0.0;
-        if (!done) {
-            const uint32_t v = (uint32_t)floor(__dmul_rn(st[seg], scale));
-            if (a0 > 0) skip = (uint32_t)floor(__dmul_rn(st[(R - 1) * NS + seg - 1], scale)) == v;
-            nextb = (double)v + 1.0;
-            slot = full ? mod_nb(v, unb, inv_nb) : v - v0;
-            if (!skip) {
-                av = lv[slot];
-                aw = lw[slot];
-                c0 = lc[slot];
+        // Aligned start: the first run start of this period at or after seg * R.
+        int k = seg * R, j = 0, sk = seg;
+        if (live && k < len && k > 0) {
+            uint32_t prev = cell_of(st[(R - 1) * NS + seg - 1], scale);
+            for (;;) {
+                const uint32_t v = cell_of(st[j * NS + sk], scale);
+                if (v != prev) break;
+                ++k;
+                if (++j == R) {
+                    j = 0;
+                    ++sk;
+                }
+                if (k >= len) break;
+                prev = v;
             }
         }
-        while (__any_sync(0xffffffffu, !done)) {
-            if (done) continue;
-            const int at = j * NS + sk;
-            if (!skip) {
+        if (k > len) k = len;
+        if (live) lstart[seg] = k;
+        if (live && seg == 0) lstart[NS] = len;
+        __syncthreads();
+        const int end = live ? lstart[seg + 1] : 0;
+
+        bool act = live && k < end;
+        uint32_t slot = 0, c0 = 0;
+        int k0 = k;
+        double nextb = 0.0, av = 0.0, aw = 0.0;
+        if (act) {
+            const uint32_t v = cell_of(st[j * NS + sk], scale);
+            nextb = (double)v + 1.0;
+            slot = mod_nb(v, unb, inv_nb);
+            av = lv[slot];
+            aw = lw[slot];
+            c0 = lc[slot];
+        }
+        while (__any_sync(0xffffffffu, act)) {
+            if (act) {
+                const int at = j * NS + sk;
                 av = __dadd_rn(av, sv[at]);
                 aw = __dadd_rn(aw, sw[at]);
-            }
-            ++k;
-            if (++j == R) {
-                j = 0;
-                ++sk;
-            }
-            bool bnd = true;
-            double x = 0.0;
-            if (k < len) {
-                x = __dmul_rn(st[j * NS + sk], scale);
-                bnd = x >= nextb;
-            }
-            if (bnd || (skip && k >= e0)) {
-                if (bnd && !skip) {
+                ++k;
+                if (++j == R) {
+                    j = 0;
+                    ++sk;
+                }
+                bool bnd = true;
+                double x = 0.0;
+                if (k < end) {
+                    x = __dmul_rn(st[j * NS + sk], scale);
+                    bnd = x >= nextb;
+                }
+                if (bnd) {
                     lv[slot] = av;
                     lw[slot] = aw;
                     lc[slot] = c0 + (uint32_t)(k - k0);
-                }
-                if (k >= e0) {
-                    done = true;  // the next run starts in the next segment
-                } else {
-                    const double after = __dadd_rn(nextb, 1.0);
-                    if (x < after) {  // the next cell
-                        nextb = after;
-                        slot = (full && slot + 1 == unb) ? 0u : slot + 1;
-                    } else {  // empty cells in between
-                        const uint32_t vn = (uint32_t)floor(x);
-                        nextb = (double)vn + 1.0;
-                        slot = full ? mod_nb(vn, unb, inv_nb) : vn - v0;
+                    if (k < end) {
+                        const double after = __dadd_rn(nextb, 1.0);
+                        if (x < after) {  // the next cell
+                            nextb = after;
+                            slot = slot + 1 == unb ? 0u : slot + 1;
+                        } else {  // empty cells in between
+                            const uint32_t vn = (uint32_t)floor(x);
+                            nextb = (double)vn + 1.0;
+                            slot = mod_nb(vn, unb, inv_nb);
+                        }
+                        av = lv[slot];
+                        aw = lw[slot];
+                        c0 = lc[slot];
+                        k0 = k;
                     }
-                    skip = false;
-                    av = lv[slot];
-                    aw = lw[slot];
-                    c0 = lc[slot];
-                    k0 = k;
                 }
-            }
-        }
-        __syncthreads();
-        if (!full) {
-            for (int e = tid; e < g * rows; e += T) {
-                const int qq = e / rows, u = e - qq * rows;
-                uint32_t bin = s_r0[qq] + (uint32_t)u;
-                if (bin >= unb) bin -= unb;
-                const size_t dst = (size_t)qq * nb + bin, src = (size_t)qq * rs + u;
-                gv[dst] = rv[src];
-                gw[dst] = rw[src];
-                gc[dst] = rc[src];
+                act = k < end;
             }
         }
         __syncthreads();
     }
 
-    // Histogram of period qq, bin b.
-    auto hv = [&](int qq, int b) { return full ? rv[(size_t)qq * rs + b] : gv[(size_t)qq * nb + b]; };
-    auto hw = [&](int qq, int b) { return full ? rw[(size_t)qq * rs + b] : gw[(size_t)qq * nb + b]; };
-    auto hc = [&](int qq, int b) { return full ? rc[(size_t)qq * rs + b] : gc[(size_t)qq * nb + b]; };
     if (a.hist_out) {
         // Raw histograms, field-major [3][nb] (the evidence fold, one period).
         for (int p = tid; p < nb; p += T) {
-            a.hist_out[p] = hv(0, p);
-            a.hist_out[nb + p] = hw(0, p);
-            a.hist_out[2 * (size_t)nb + p] = (double)hc(0, p);
+            a.hist_out[p] = hv[p];
+            a.hist_out[nb + p] = hw[p];
+            a.hist_out[2 * (size_t)nb + p] = (double)hc[p];
         }
         return;
     }
@@ -279,61 +249,59 @@ __global__ void __launch_bounds__(512, 2) k_fold(FoldArgs a) {
         const int qq = row / NF, f = row - (row / NF) * NF;
         double* out64 = a.cum + ((size_t)(g0 + qq) * NF + f) * stride;
         float2* out32 = a.cum32 + ((size_t)(g0 + qq) * NF + f) * stride;
+        const size_t off = (size_t)qq * rs;
         if (f == F_V)
-            prefix_row([&](int bb) { return hv(qq, bb); }, nb, out64, out32);
+            prefix_row([&](int bb) { return hv[off + bb]; }, nb, out64, out32);
         else if (f == F_W)
-            prefix_row([&](int bb) { return hw(qq, bb); }, nb, out64, out32);
+            prefix_row([&](int bb) { return hw[off + bb]; }, nb, out64, out32);
         else
-            prefix_row([&](int bb) { return (double)hc(qq, bb); }, nb, out64, out32);
+            prefix_row([&](int bb) { return (double)hc[off + bb]; }, nb, out64, out32);
     }
 }
 
 namespace {
-constexpr size_t FOLD_SMEM_TARGET = 110 * 1024;  // two CTAs per SM
-constexpr int FOLD_CTA_THREADS = 512;
-constexpr int FOLD_STAGE_CAP = 1024;              // observations per chunk at most
-constexpr int FOLD_SPAN_MAX = 256;                // window cells at most
 constexpr size_t BIN_BYTES = 2 * sizeof(double) + sizeof(uint32_t);
+constexpr size_t SLOT_BYTES = 3 * sizeof(double);
+constexpr int STAGE_MAX = 4096;
 }  // namespace
 
-// Launch shape: a power-of-two period group (32 when the launch fills every
-// SM twice), "full" mode when the group's histograms fit next to the
-// staging area in half of an SM's shared memory, else "window" mode with the
-// largest window that fits.
+// Launch shape: the largest power-of-two period group (<= 32 and at most
+// enough to give every SM one CTA) whose histograms leave room to stage at
+// least 2048 observations; the staging capacity is what is left (up to
+// STAGE_MAX); the CTA has 1024 threads, or 512 when segments would
+// otherwise be shorter than 16 observations. A single period whose
+// histogram does not fit folds into global scratch.
 FoldShape fold_group_shape(int nb, int periods, int sm_count) {
     FoldShape s{};
-    int g = MAX_GROUP;
-    while (g > 1 && (size_t)(g / 2) * 2 * sm_count >= (size_t)periods) g /= 2;
+    s.row_stride = nb | 1;
+    const size_t hist_per = (size_t)s.row_stride * BIN_BYTES;
+    const size_t stage_min = SLOT_BYTES * (2048 + 1024) + 4 * (1024 + 32);
+    int g = 1;
+    while (g < MAX_GROUP && (size_t)(2 * g) * hist_per + stage_min <= MAX_FOLD_SMEM) g *= 2;
+    const int fill = (periods + sm_count - 1) / sm_count;
+    while (g > 1 && g / 2 >= fill) g /= 2;
     s.group = g;
-    s.threads = FOLD_CTA_THREADS;
-    const int ns = (FOLD_CTA_THREADS / 32) * (32 / g);
-    s.stage_field = FOLD_STAGE_CAP + ns;
-    const size_t stage = 3 * sizeof(double) * (size_t)s.stage_field;
-    const size_t room = FOLD_SMEM_TARGET - stage;
-    const int full_rs = nb | 1;
-    if ((size_t)g * full_rs * BIN_BYTES <= room) {
-        s.window = 0;
-        s.row_stride = full_rs;
-        s.hist_in_smem = true;
-        s.span_cap = nb;
-    } else {
-        int rows = (int)(room / ((size_t)g * BIN_BYTES)) - 1;
-        if (rows > FOLD_SPAN_MAX + 1) rows = FOLD_SPAN_MAX + 1;
-        s.window = rows;  // cells v0 .. v0 + rows - 1
-        s.row_stride = rows | 1;
-        s.hist_in_smem = false;
-        s.span_cap = rows - 1;
-    }
-    s.chunk_cap = FOLD_STAGE_CAP;
-    s.smem = stage + (size_t)g * s.row_stride * BIN_BYTES;
+    s.hist_in_smem = (size_t)g * hist_per + stage_min <= MAX_FOLD_SMEM;
+    const size_t room = MAX_FOLD_SMEM - (s.hist_in_smem ? (size_t)g * hist_per : 0) - 4 * (1024 + 32);
+    int cap = (int)(room / SLOT_BYTES) - 1024;
+    if (cap > STAGE_MAX) cap = STAGE_MAX;
+    s.chunk_cap = cap;
+    s.threads = 1024;
+    if ((double)cap * g / 1024.0 < 16.0) s.threads = 512;
+    const int ns = (s.threads / 32 / g) * 32;
+    s.stage_field = cap + ns;
+    s.span_cap = nb;
+    s.window = 0;
+    const size_t starts_bytes = (sizeof(int) * (size_t)g * (ns + 1) + 15) & ~(size_t)15;
+    s.smem = SLOT_BYTES * (size_t)s.stage_field + starts_bytes + (s.hist_in_smem ? (size_t)g * hist_per : 0);
     return s;
 }
 
 int fold_chunks(const double* time, int n, double scale_max, int nb, int span_cap, int chunk_cap, int* out,
                 int capacity) {
     // A chunk spans less than `span` days, hence at most min(nb, span_cap) - 2
-    // + 1 distinct cells at any scale <= scale_max (floor(x) - floor(y) <
-    // x - y + 1): its cells are distinct bins and fit the window.
+    // distinct cells at any scale <= scale_max (floor(x) - floor(y) <
+    // x - y + 1): its cells are distinct bins.
     const int cells = (nb < span_cap ? nb : span_cap) - 4;
     const double span = (double)(cells > 1 ? cells : 1) / scale_max;
     int count = 0;
@@ -365,9 +333,9 @@ cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t 
         configured = true;
     }
     if (shape.smem > MAX_FOLD_SMEM || a.group != shape.group || a.group > MAX_GROUP || a.group < 1 ||
-        (a.group & (a.group - 1)) != 0 || a.nchunks < 1 || shape.threads != FOLD_CTA_THREADS ||
-        a.stage_field != shape.stage_field || a.window != shape.window || a.row_stride != shape.row_stride ||
-        (a.window != 0 && a.hist_global == nullptr))
+        (a.group & (a.group - 1)) != 0 || a.nchunks < 1 || (shape.threads != 1024 && shape.threads != 512) ||
+        a.group > shape.threads / 32 || a.stage_field != shape.stage_field || a.row_stride != shape.row_stride ||
+        (!shape.hist_in_smem && a.hist_global == nullptr))
         return cudaErrorInvalidValue;
     const int blocks = (a.periods + a.group - 1) / a.group;
     k_fold<<<blocks, shape.threads, shape.smem, stream>>>(a);

@@ -202,7 +202,7 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
     }
     if (!shape.hist_in_smem) {
         const size_t blocks = (batch + shape.group - 1) / shape.group;
-        CK(ensure(ctx->hist, blocks * shape.group * NF * (size_t)nb * sizeof(double)), "workspace");
+        CK(ensure(ctx->hist, blocks * shape.group * NF * (size_t)shape.row_stride * sizeof(double)), "workspace");
     }
 
     cudaStream_t s = ctx->stream;
