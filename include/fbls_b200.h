@@ -184,6 +184,28 @@ int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* du
                         uint32_t nd, double period, const fbls_config* cfg, fbls_evidence_row* rows_out,
                         uint32_t* n_rows);
 
+/* ---- no device allocation ----------------------------------------------
+ * No counterpart in the reference. For callers that cannot call cudaMalloc
+ * (their device memory is owned by someone else: a framework's caching
+ * allocator that must own every allocation, or a fixed per-process memory
+ * partition). Same results as fbls_scan_bank (one scan_bank pass of every
+ * period at nb bins), with every device buffer carved out of one file-scope
+ * __device__ array of FBLS_STATIC_SCRATCH_BYTES that each GPU loading the
+ * library holds until exit. All arrays are host arrays: time, v, w (n,
+ * relative times ascending), periods (P), outputs as in fbls_scan_bank.
+ * Inputs whose fields, chunk table and one period's intermediates do not fit
+ * the array are rejected (FBLS_ERR_ARGUMENT with the message in error);
+ * larger P is processed in batches that fit. The first call on a device
+ * resolves the array's address on that device; make that call before any
+ * stream capture. Calls share the array: calls that overlap on the GPU race.
+ * Runs on the legacy default stream and returns after the results are on
+ * the host. */
+#define FBLS_STATIC_SCRATCH_BYTES (64u * 1024u * 1024u)
+int fbls_scan_bank_static(int device, const double* time, const double* v, const double* w, uint32_t n,
+                          double baseline_norm, const double* periods, uint32_t P, const fbls_bank* bank,
+                          uint32_t nb, uint32_t precision_mode, double* records, double* score, double* depth,
+                          uint32_t* flags, char* error, uint32_t error_len);
+
 /* ---- instrumentation (no counterpart in the reference; its FBLS_PROFILE
  * synchronises after each kernel instead, scan.rs:152, :222-229) --------- */
 
