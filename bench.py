@@ -291,8 +291,33 @@ def run_gpu(args):
         torch.distributed.destroy_process_group()
 
 
+def run_profile_case(args):
+    """One bounded scan_bank pass for profiler captures: the 13-sector star's
+    octave band [8, 16) d at its coarse grid (1536 bins), first 4096 periods:
+    one k_fold, one k_scan_tiles and one k_merge launch, ~0.6 GB on device."""
+    from fbls_b200 import api, synth
+    curve, cfg = synth.multi_sector(), synth.multi_sector_config()
+    state = api.prepared_family(curve.time, curve.flux, curve.flux_err, cfg)
+    grid, bands = api.band_plan(state, cfg)
+    band = bands[4]
+    nb = band["nb"] // 2
+    periods = band["periods"][:4096]
+    with api.Gpu(0) as gpu:
+        dev = gpu.upload(state)
+        gpu.set_kernel_timing(True)
+        rec, score, depth, flags, stats = gpu.scan_bank(dev, periods, api.bank_for(band, cfg), nb)
+        ctr = gpu.counters()
+        dev.free()
+    print(json.dumps({"case": "fold", "nb": nb, "periods": len(periods), "observations": state.n,
+                      "fold_ms": ctr["fold_ms"], "fold_updates": ctr["fold_updates"],
+                      "fold_algorithmic_bytes": ctr["fold_bytes"], "scan_ms": ctr["scan_ms"],
+                      "templates": stats["templates_scanned"]}))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--profile-case", choices=["fold"], default=None,
+                    help="run one bounded launch set for profiler captures instead of the benchmark")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -301,7 +326,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

@@ -114,13 +114,11 @@ __global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
     const int seg = (warp - q * wpp) * 32 + lane;
     const int rs = a.row_stride;    // >= nb
 
-    // Shared memory: staging t, v, w [stage_field] | run starts [G][NS + 1]
+    // Shared memory: staging (t, v, w) triples [stage_field] | run starts [G][NS + 1]
     // (padded to 16 bytes) | sums v, w [G][rs] | counts [G][rs]; the sums
     // and counts live in global scratch instead when hist_global is set.
     double* st = reinterpret_cast<double*>(smem);
-    double* sv = st + a.stage_field;
-    double* sw = sv + a.stage_field;
-    int* starts = reinterpret_cast<int*>(sw + a.stage_field);
+    int* starts = reinterpret_cast<int*>(st + 3 * (size_t)a.stage_field);
     const size_t starts_bytes = ((size_t)G * (NS + 1) * sizeof(int) + 15) & ~(size_t)15;
     double* hv = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(starts) + starts_bytes);
     double* hw = hv + (size_t)G * rs;
@@ -148,31 +146,26 @@ __global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
     for (int c = 0; c < a.nchunks; c++) {
         const int i0 = a.chunks[c];
         const int len = a.chunks[c + 1] - i0;
-        const int R = (len + NS - 1) / NS;
-        // Stage the chunk, observation k at (k % R) * NS + k / R.
+        // Segment length, odd so that the lanes' (t, v, w) triples fall in
+        // different shared-memory banks.
+        const int R = ((len + NS - 1) / NS) | 1;
+        // Stage the chunk: observation k at st[3k .. 3k + 2] = (t, v, w).
         for (int k = tid; k < len; k += T) {
-            const int sk = k / R;
-            const int at = (k - sk * R) * NS + sk;
-            st[at] = a.time[i0 + k];
-            sv[at] = a.v[i0 + k];
-            sw[at] = a.w[i0 + k];
+            st[3 * k] = a.time[i0 + k];
+            st[3 * k + 1] = a.v[i0 + k];
+            st[3 * k + 2] = a.w[i0 + k];
         }
         __syncthreads();
 
         // Aligned start: the first run start of this period at or after seg * R.
-        int k = seg * R, j = 0, sk = seg;
+        int k = seg * R;
         if (live && k < len && k > 0) {
-            uint32_t prev = cell_of(st[(R - 1) * NS + seg - 1], scale);
-            for (;;) {
-                const uint32_t v = cell_of(st[j * NS + sk], scale);
+            uint32_t prev = cell_of(st[3 * (k - 1)], scale);
+            while (k < len) {
+                const uint32_t v = cell_of(st[3 * k], scale);
                 if (v != prev) break;
-                ++k;
-                if (++j == R) {
-                    j = 0;
-                    ++sk;
-                }
-                if (k >= len) break;
                 prev = v;
+                ++k;
             }
         }
         if (k > len) k = len;
@@ -181,35 +174,22 @@ __global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
         __syncthreads();
         const int end = live ? lstart[seg + 1] : 0;
 
-        bool act = live && k < end;
-        uint32_t slot = 0, c0 = 0;
-        int k0 = k;
-        double nextb = 0.0, av = 0.0, aw = 0.0;
-        if (act) {
-            const uint32_t v = cell_of(st[j * NS + sk], scale);
-            nextb = (double)v + 1.0;
-            slot = mod_nb(v, unb, inv_nb);
-            av = lv[slot];
-            aw = lw[slot];
-            c0 = lc[slot];
-        }
-        while (__any_sync(0xffffffffu, act)) {
-            if (act) {
-                const int at = j * NS + sk;
-                av = __dadd_rn(av, sv[at]);
-                aw = __dadd_rn(aw, sw[at]);
+        if (live && k < end) {
+            const double* p = st + 3 * k;
+            uint32_t v = cell_of(p[0], scale);
+            double nextb = (double)v + 1.0;
+            uint32_t slot = mod_nb(v, unb, inv_nb);
+            double av = lv[slot], aw = lw[slot];
+            uint32_t c0 = lc[slot];
+            int k0 = k;
+            while (k < end) {
+                av = __dadd_rn(av, p[1]);
+                aw = __dadd_rn(aw, p[2]);
+                p += 3;
                 ++k;
-                if (++j == R) {
-                    j = 0;
-                    ++sk;
-                }
-                bool bnd = true;
-                double x = 0.0;
-                if (k < end) {
-                    x = __dmul_rn(st[j * NS + sk], scale);
-                    bnd = x >= nextb;
-                }
-                if (bnd) {
+                // p[0] is staged or spare slack when k == end; it is unused then.
+                const double x = __dmul_rn(p[0], scale);
+                if (k == end || x >= nextb) {
                     lv[slot] = av;
                     lw[slot] = aw;
                     lc[slot] = c0 + (uint32_t)(k - k0);
@@ -229,7 +209,6 @@ __global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
                         k0 = k;
                     }
                 }
-                act = k < end;
             }
         }
         __syncthreads();
