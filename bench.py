@@ -26,6 +26,7 @@ reference (Rust + cuda-oxide) cannot be built here, so its CPU restatement
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import math
 import os
@@ -207,6 +208,8 @@ def run_gpu(args):
     clocks.start()
     times = []
     trials = 0
+    gc.collect()
+    gc.disable()  # no collector pauses inside the timed steps
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -237,6 +240,7 @@ def run_gpu(args):
                               state.origin, state.residual_energy, state.durations, state.rho)
         rows_e, glen_e, stats_e = gpu.signal_search(sub, cfg)
         e2e_ms.append(gpu.timer_stop())
+    gc.enable()
     e2e_total = sum(e2e_ms)
     if world > 1:
         t = torch.tensor([e2e_total], dtype=torch.float64, device=f"cuda:{local}")
@@ -269,6 +273,7 @@ def run_gpu(args):
                    "observations": state.n, "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "stars_per_s": world * args.steps / (total_ms * 1e-3),
+        "step_ms": [round(t, 2) for t in times],
         "trials_per_step": trials / args.steps / world,
         "rows_per_step": int(len(rows)),
         "gpu_launches": int(ctr["launches"]),

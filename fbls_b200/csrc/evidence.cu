@@ -564,7 +564,8 @@ int compare_search(cudaStream_t stream, void*, size_t, const EvidenceReady& r, c
     const size_t o_cum = o_hist + 3 * nb2;
     const size_t o_screen = o_cum + 3 * (nb2 + 1);
     const size_t o_parts = o_screen + (size_t)tiles * 4;
-    const size_t total = o_parts + (size_t)tiles * 2 * EV_PART;
+    const size_t o_fault = o_parts + (size_t)tiles * 2 * EV_PART;
+    const size_t total = o_fault + 1;
     double* ws = static_cast<double*>(workspace(total * sizeof(double)));
     if (!ws) {
         message = "evidence workspace allocation failed";
@@ -577,7 +578,8 @@ int compare_search(cudaStream_t stream, void*, size_t, const EvidenceReady& r, c
     if (!check(cudaMemcpyAsync(ws, consts.data(), consts.size() * sizeof(double), cudaMemcpyHostToDevice, stream),
                "evidence upload"))
         return FBLS_ERR_CUDA;
-    if (!check(cudaMemsetAsync(ws + o_hist, 0, (o_parts - o_hist) * sizeof(double), stream), "evidence zero"))
+    if (!check(cudaMemsetAsync(ws + o_hist, 0, (o_parts - o_hist) * sizeof(double), stream), "evidence zero") ||
+        !check(cudaMemsetAsync(ws + o_fault, 0, sizeof(double), stream), "evidence zero"))
         return FBLS_ERR_CUDA;
     // fold_two (evidence.rs:75-92): bin = floor(t * scale) mod 2 nb.
     FoldArgs fa{};
@@ -596,6 +598,7 @@ int compare_search(cudaStream_t stream, void*, size_t, const EvidenceReady& r, c
     fa.stage_field = shape.stage_field;
     fa.window = shape.window;
     fa.row_stride = shape.row_stride;
+    fa.fault = reinterpret_cast<uint32_t*>(ws + o_fault);
     if (!check(launch_fold(fa, shape, stream), "evidence fold")) return FBLS_ERR_CUDA;
     k_prefix_fields<<<3, 256, 0, stream>>>(ws + o_hist, ws + o_cum, (int)nb2);
     EvArgs ea;
@@ -619,11 +622,18 @@ int compare_search(cudaStream_t stream, void*, size_t, const EvidenceReady& r, c
     k_screen<<<tiles, EV_TILE, 0, stream>>>(ea, ws + o_screen);
     if (!check(cudaGetLastError(), "evidence screen")) return FBLS_ERR_CUDA;
     std::vector<double> screen((size_t)tiles * 4);
+    uint32_t fault = 0;
     if (!check(cudaMemcpyAsync(screen.data(), ws + o_screen, screen.size() * sizeof(double), cudaMemcpyDeviceToHost,
                                stream),
                "evidence screen download") ||
+        !check(cudaMemcpyAsync(&fault, ws + o_fault, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream),
+               "evidence fault download") ||
         !check(cudaStreamSynchronize(stream), "evidence screen"))
         return FBLS_ERR_CUDA;
+    if (fault) {
+        message = "evidence fold: staging copies did not complete";
+        return FBLS_ERR_CUDA;
+    }
     double maximum = neg_inf();
     for (int t = 0; t < tiles; t++) maximum = rmax(maximum, screen[(size_t)t * 4]);
     if (!(maximum >= cfg.threshold * (1.0 - 1e-12))) return 0;

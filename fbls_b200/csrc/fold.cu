@@ -20,6 +20,8 @@
 // sequential fold does, so the result is reproducible run to run and equal
 // bit for bit to the CPU oracle (the reference's f64 atomics,
 // src/search/kernels.rs:491, :540, give some order of the same additions).
+// k_fold_walk (below) is the same scheme with the chunks staged by TMA; it
+// folds every nb whose histograms fit shared memory, and k_fold the rest.
 // The doubled prefix sums then follow the association of the reference's
 // prefix_block (kernels.rs:237-309), one warp per (period, field) row, and
 // are written as f64 and (hi, lo) f32 pairs.
@@ -238,10 +240,238 @@ __global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// TMA staging: mbarrier helpers and the bulk copies of one chunk.
+
+namespace {
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Waits for the barrier phase with a bounded number of polls; false when the
+// copies did not land in time.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < (1u << 20); ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// Issues the three bulk copies of chunk [i0, i1), rounded out to whole
+// 16-byte pieces, into one staging buffer (fields at `field` doubles apart).
+__device__ __forceinline__ void stage_chunk(const FoldArgs& a, int i0, int i1, double* buf, int field, uint32_t bar) {
+    const int a0 = i0 & ~1, a1 = (i1 + 1) & ~1;
+    const uint32_t bytes = (uint32_t)(a1 - a0) * (uint32_t)sizeof(double);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, 3u * bytes);
+    bulk_load(smem_addr(buf), a.time + a0, bytes, bar);
+    bulk_load(smem_addr(buf + field), a.v + a0, bytes, bar);
+    bulk_load(smem_addr(buf + 2 * field), a.w + a0, bytes, bar);
+}
+
+}  // namespace
+
+
+// ---------------------------------------------------------------------------
+// Walking fold with TMA-staged chunks (the fold of every nb whose
+// histograms fit shared memory beside the staging).
+//
+// As in k_fold, each period's lanes split a staged chunk into segments whose
+// starts are moved to run boundaries, and each lane walks its runs in order,
+// keeping the current run's sums in registers. The bin of a cell is
+// cell - base (one wrap at most), base fixed per segment, so a cell change
+// costs a compare, a subtraction and the store/load of the bin's sums.
+// Chunks are staged by TMA bulk copies into two buffers (fields t, v, w),
+// one chunk ahead of the one being folded, so the copy overlaps the walk.
+
+template <int CAP>
+__global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
+    constexpr int F = CAP + 2;  // doubles per staged field
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ double s_scale[MAX_GROUP];
+    __shared__ __align__(8) uint64_t s_bar[2];
+
+    const int tid = threadIdx.x;
+    const int T = blockDim.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int nb = a.nb;
+    const uint32_t unb = (uint32_t)nb;
+    const double inv_nb = 1.0 / (double)nb;
+    const int G = a.group;
+    const int wpp = (T / 32) / G;
+    const int NS = wpp * 32;
+    const int g0 = blockIdx.x * G;
+    const int g = min(G, a.periods - g0);
+    const int q = warp / wpp;
+    const int seg = (warp - q * wpp) * 32 + lane;
+    const bool live = q < g;
+    const int rs = a.row_stride;
+
+    // Shared memory: staging [2][t | v | w][F] | run starts [G][NS + 1]
+    // (padded to 16 bytes) | sums (v, w) [G][rs] | counts [G][rs].
+    double* stage = reinterpret_cast<double*>(smem);
+    int* starts = reinterpret_cast<int*>(stage + 6 * F);
+    const size_t starts_bytes = ((size_t)G * (NS + 1) * sizeof(int) + 15) & ~(size_t)15;
+    double2* hvw = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(starts) + starts_bytes);
+    uint32_t* hc = reinterpret_cast<uint32_t*>(hvw + (size_t)G * rs);
+
+    if (tid < g) s_scale[tid] = a.scales[g0 + tid];
+    for (int e = tid; e < G * rs; e += T) {
+        hvw[e] = make_double2(0.0, 0.0);
+        hc[e] = 0u;
+    }
+    const uint32_t bar0 = smem_addr(&s_bar[0]);
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const double scale = live ? s_scale[q] : 0.0;
+    double2* lvw = hvw + (size_t)(live ? q : 0) * rs;
+    uint32_t* lc = hc + (size_t)(live ? q : 0) * rs;
+    int* lstart = starts + (live ? q : 0) * (NS + 1);
+    const float inv_ns = 1.0f / (float)NS;
+    const int nch = a.nchunks;
+    if (tid == 0) stage_chunk(a, a.chunks[0], a.chunks[1], stage, F, bar0);
+
+    for (int c = 0; c < nch; c++) {
+        const int buf = c & 1;
+        const bool landed = mbar_wait_bounded(bar0 + 8 * buf, (uint32_t)(c >> 1) & 1u);
+        if (!__syncthreads_and(landed)) {
+            if (tid == 0) atomicOr(a.fault, 1u);
+            return;
+        }
+        const int i0 = a.chunks[c];
+        const int len = a.chunks[c + 1] - i0;
+        if (tid == 0 && c + 1 < nch)
+            stage_chunk(a, a.chunks[c + 1], a.chunks[c + 2], stage + 3 * F * (buf ^ 1), F, bar0 + 8 * (buf ^ 1));
+        const double* tt = stage + 3 * F * buf + (i0 & 1);
+        // Segment length: at least ceil(len / NS), odd.
+        const int R = ((int)((float)len * inv_ns) + 1) | 1;
+        int k = seg * R;
+        if (live && k < len && k > 0) {
+            uint32_t prev = cell_of(tt[k - 1], scale);
+            while (k < len) {
+                const uint32_t v = cell_of(tt[k], scale);
+                if (v != prev) break;
+                ++k;
+            }
+        }
+        if (k > len) k = len;
+        if (live) lstart[seg] = k;
+        if (live && seg == 0) lstart[NS] = len;
+        __syncthreads();
+        const int end = live ? lstart[seg + 1] : 0;
+        if (live && k < end) {
+            uint32_t cur = cell_of(tt[k], scale);
+            const uint32_t s0 = mod_nb(cur, unb, inv_nb);
+            const uint32_t base = cur - s0;
+            uint32_t slot = s0;
+            double2 acc = lvw[slot];
+            uint32_t cnt = lc[slot];
+            for (int j = k; j < end; j++) {
+                const uint32_t cj = cell_of(tt[j], scale);
+                if (cj != cur) {
+                    lvw[slot] = acc;
+                    lc[slot] = cnt;
+                    uint32_t b = cj - base;
+                    slot = b >= unb ? b - unb : b;
+                    cur = cj;
+                    acc = lvw[slot];
+                    cnt = lc[slot];
+                }
+                acc.x = __dadd_rn(acc.x, tt[j + F]);
+                acc.y = __dadd_rn(acc.y, tt[j + 2 * F]);
+                cnt += 1u;
+            }
+            lvw[slot] = acc;
+            lc[slot] = cnt;
+        }
+    }
+    __syncthreads();
+
+    if (a.hist_out) {
+        for (int p = tid; p < nb; p += T) {
+            a.hist_out[p] = hvw[p].x;
+            a.hist_out[nb + p] = hvw[p].y;
+            a.hist_out[2 * (size_t)nb + p] = (double)hc[p];
+        }
+        return;
+    }
+    const size_t stride = 2 * (size_t)nb + 1;
+    for (int row = warp; row < g * NF; row += T / 32) {
+        const int qq = row / NF, f = row - (row / NF) * NF;
+        double* out64 = a.cum + ((size_t)(g0 + qq) * NF + f) * stride;
+        float2* out32 = a.cum32 + ((size_t)(g0 + qq) * NF + f) * stride;
+        const size_t o = (size_t)qq * rs;
+        if (f == F_V)
+            prefix_row([&](int bb) { return hvw[o + bb].x; }, nb, out64, out32);
+        else if (f == F_W)
+            prefix_row([&](int bb) { return hvw[o + bb].y; }, nb, out64, out32);
+        else
+            prefix_row([&](int bb) { return (double)hc[o + bb]; }, nb, out64, out32);
+    }
+}
+
 namespace {
 constexpr size_t BIN_BYTES = 2 * sizeof(double) + sizeof(uint32_t);
 constexpr size_t SLOT_BYTES = 3 * sizeof(double);
 constexpr int STAGE_MAX = 4096;
+constexpr int WALK_CAP = 2048;
+
+// Walking-fold shape: 1024 threads, chunks of up to WALK_CAP observations,
+// the largest power-of-two group whose histograms fit beside the staging.
+bool walk_shape(int nb, int periods, int sm_count, FoldShape* out) {
+    FoldShape s{};
+    s.kind = FOLD_WALK;
+    s.threads = 1024;
+    s.row_stride = nb | 1;
+    const size_t stage = 6 * sizeof(double) * (size_t)(WALK_CAP + 2);
+    const size_t hist_per = (size_t)s.row_stride * BIN_BYTES;
+    auto starts = [&](int g) { return ((size_t)g * (1024 / g + 1) * sizeof(int) + 15) & ~(size_t)15; };
+    if (stage + starts(1) + hist_per > MAX_FOLD_SMEM) return false;
+    int g = 1;
+    while (2 * g <= MAX_GROUP && stage + starts(2 * g) + (size_t)(2 * g) * hist_per <= MAX_FOLD_SMEM) g *= 2;
+    while (g > 1 && (g / 2 >= periods || (periods + g - 1) / g < sm_count)) g /= 2;
+    s.group = g;
+    s.hist_in_smem = true;
+    s.window = 0;
+    s.span_cap = nb;
+    s.chunk_cap = WALK_CAP;
+    s.stage_field = WALK_CAP + 2;
+    s.smem = stage + starts(g) + (size_t)g * hist_per;
+    *out = s;
+    return true;
+}
+
 }  // namespace
 
 // Launch shape: the largest power-of-two period group (<= 32 and at most
@@ -251,7 +481,10 @@ constexpr int STAGE_MAX = 4096;
 // otherwise be shorter than 16 observations. A single period whose
 // histogram does not fit folds into global scratch.
 FoldShape fold_group_shape(int nb, int periods, int sm_count) {
+    FoldShape w;
+    if (walk_shape(nb, periods, sm_count, &w)) return w;
     FoldShape s{};
+    s.kind = FOLD_SMEM;
     s.row_stride = nb | 1;
     const size_t hist_per = (size_t)s.row_stride * BIN_BYTES;
     const size_t stage_min = SLOT_BYTES * (2048 + 1024) + 4 * (1024 + 32);
@@ -308,8 +541,23 @@ cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t 
     static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(k_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_fold_walk<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)MAX_FOLD_SMEM);
         if (e != cudaSuccess) return e;
         configured = true;
+    }
+    if (shape.kind == FOLD_WALK) {
+        if (shape.smem > MAX_FOLD_SMEM || a.group != shape.group || a.group < 1 || a.group > MAX_GROUP ||
+            (a.group & (a.group - 1)) != 0 || shape.threads != 1024 || a.nchunks < 1 || a.nb < 2 ||
+            a.stage_field != WALK_CAP + 2 || shape.chunk_cap != WALK_CAP || a.row_stride != shape.row_stride ||
+            a.row_stride < a.nb || a.fault == nullptr || (a.hist_out != nullptr && a.group != 1) ||
+            (reinterpret_cast<uintptr_t>(a.time) & 15) || (reinterpret_cast<uintptr_t>(a.v) & 15) ||
+            (reinterpret_cast<uintptr_t>(a.w) & 15))
+            return cudaErrorInvalidValue;
+        const int blocks = (a.periods + a.group - 1) / a.group;
+        k_fold_walk<WALK_CAP><<<blocks, shape.threads, shape.smem, stream>>>(a);
+        return cudaGetLastError();
     }
     if (shape.smem > MAX_FOLD_SMEM || a.group != shape.group || a.group > MAX_GROUP || a.group < 1 ||
         (a.group & (a.group - 1)) != 0 || a.nchunks < 1 || (shape.threads != 1024 && shape.threads != 512) ||

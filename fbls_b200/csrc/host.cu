@@ -47,7 +47,7 @@ struct fbls_ctx {
     fbls_counters counters{};
     // Workspace, grown on demand and reused across bands and calls.
     DevBuf bank, scales, periods, cum, cum32, hist, parts, keys, tflags, records, score, depth, rflags;
-    DevBuf evidence, chunks;
+    DevBuf evidence, chunks, fault;
     std::vector<int> host_chunks;
 };
 
@@ -194,6 +194,7 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
     CK(ensure(ctx->score, (size_t)P * sizeof(double)), "workspace");
     CK(ensure(ctx->depth, (size_t)P * sizeof(double)), "workspace");
     CK(ensure(ctx->rflags, (size_t)P * sizeof(uint32_t)), "workspace");
+    CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
     FoldShape shape;
     int nchunks = 0;
     {
@@ -206,6 +207,7 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
     }
 
     cudaStream_t s = ctx->stream;
+    CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
     CK(cudaMemcpyAsync(ctx->bank.ptr, host_bank.data(), host_bank.size() * sizeof(double), cudaMemcpyHostToDevice, s),
        "upload bank");
     CK(cudaMemcpyAsync(ctx->scales.ptr, scales.data(), (size_t)P * sizeof(double), cudaMemcpyHostToDevice, s),
@@ -246,6 +248,7 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
         fa.stage_field = shape.stage_field;
         fa.window = shape.window;
         fa.row_stride = shape.row_stride;
+        fa.fault = as<uint32_t>(ctx->fault);
         CK(launch_fold(fa, shape, s), "fold");
         ctx->counters.launches += 1;
         ctx->counters.fold_launches += 1;
@@ -306,7 +309,10 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
     CK(cudaMemcpyAsync(out.depth.data(), ctx->depth.ptr, P * sizeof(double), cudaMemcpyDeviceToHost, s), "download");
     CK(cudaMemcpyAsync(out.flags.data(), ctx->rflags.ptr, P * sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
        "download");
+    uint32_t fault = 0;
+    CK(cudaMemcpyAsync(&fault, ctx->fault.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
     CK(cudaStreamSynchronize(s), "scan_bank");
+    if (fault) return fail(ctx, FBLS_ERR_CUDA, "fold: staging copies did not complete");
     double t_fold = 0.0, t_scan = 0.0;
     if (timing) {
         for (uint64_t b = 0; b < nbatches; b++) {
@@ -426,7 +432,7 @@ void fbls_destroy(fbls_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf* bufs[] = {&ctx->bank,  &ctx->scales,  &ctx->periods, &ctx->cum,   &ctx->cum32,  &ctx->hist,    &ctx->parts,
                       &ctx->keys,  &ctx->tflags,  &ctx->records, &ctx->score, &ctx->depth,  &ctx->rflags,  &ctx->evidence,
-                      &ctx->chunks};
+                      &ctx->chunks, &ctx->fault};
     for (DevBuf* b : bufs) release(*b);
     for (int i = 0; i < 4; i++)
         if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -485,14 +491,16 @@ int fbls_upload_ready(fbls_ctx* ctx, const double* time, const double* v, const 
     r->t_last = time[n - 1];
     r->time_host.assign(time, time + n);
     const size_t bytes = (size_t)n * sizeof(double);
-    cudaError_t e = cudaMalloc(&r->time, 3 * bytes);
+    const size_t stride = fold_field_stride(n);
+    cudaError_t e = cudaMalloc(&r->time, 3 * stride * sizeof(double));
     if (e != cudaSuccess) {
         delete r;
         return cuda_fail(ctx, e, "upload_ready");
     }
-    r->v = r->time + n;
-    r->w = r->v + n;
-    e = cudaMemcpyAsync(r->time, time, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    r->v = r->time + stride;
+    r->w = r->v + stride;
+    e = cudaMemsetAsync(r->time, 0, 3 * stride * sizeof(double), ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(r->time, time, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(r->v, v, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(r->w, w, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);

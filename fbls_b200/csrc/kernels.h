@@ -16,6 +16,18 @@ constexpr int MAX_LAYERS = 16;
 // Bytes of shared memory one period's histogram needs (f64 v, f64 w, u32 count).
 constexpr size_t fold_bytes_per_bin = 2 * sizeof(double) + sizeof(uint32_t);
 
+// Fold kernels: TMA-staged walk with shared-memory histograms (FOLD_WALK),
+// or the staged-by-threads fold that can also keep its histograms in global
+// scratch, for nb too large for the first (FOLD_SMEM).
+constexpr int FOLD_SMEM = 0;
+constexpr int FOLD_WALK = 2;
+
+// Device copies of the observations: time, v and w at a stride of
+// fold_field_stride(n) doubles, so each field starts on a 16-byte boundary
+// and has one readable slot past its end (the fold's bulk copies round a
+// chunk out to whole 16-byte pieces).
+inline size_t fold_field_stride(size_t n) { return (n + 2) & ~(size_t)1; }
+
 struct FoldArgs {
     const double* time;    // n, relative days, ascending
     const double* v;       // n
@@ -34,10 +46,12 @@ struct FoldArgs {
     int stage_field;       // staged slots per field (FoldShape::stage_field)
     int window;            // 0: whole histogram in shared memory; else window rows
     int row_stride;        // FoldShape::row_stride
+    uint32_t* fault;       // FOLD_WALK: set nonzero when a staging wait gives up
 };
 
-// Launch shape of k_fold (fold_group_shape).
+// Launch shape of the fold (fold_group_shape).
 struct FoldShape {
+    int kind;           // FOLD_WALK (k_fold_walk) or FOLD_SMEM (k_fold)
     int group;          // periods per CTA, a power of two <= MAX_GROUP
     bool hist_in_smem;  // else window mode: 3 G nb doubles of global histogram per CTA
     int window;         // 0 (full mode) or the window's rows (cells)

@@ -18,8 +18,9 @@
 //
 // Every call shares the one array and overwrites it: calls that overlap on
 // the GPU (from several host threads, or on several streams) race. Nothing in
-// the array needs to start at zero: every region a kernel reads is written
-// earlier in the same call (the fold zeroes its own histograms).
+// the array needs to start at zero: every region a kernel uses is written
+// earlier in the same call (the fold zeroes its own histograms; its bulk
+// copies also read the one padding slot past each field, which it ignores).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -116,7 +117,8 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
     for (uint32_t s = 0; s < ns; s++)
         for (uint32_t l = 0; l < layers; l++)
             host_bank.push_back(1.0 - 2.0 * bank->ingress[s] * (layers > 1 ? (double)l / (double)(layers - 1) : 0.0));
-    const size_t fields_bytes = align256(3 * sizeof(double) * (size_t)n);
+    const size_t fstride = fold_field_stride(n);
+    const size_t fields_bytes = align256(3 * sizeof(double) * fstride) + align256(sizeof(uint32_t));
     const size_t bank_bytes = align256(sizeof(double) * host_bank.size());
     const size_t chunk_bytes = align256(sizeof(int) * ((size_t)n + 2));
     const size_t fixed = fields_bytes + bank_bytes + chunk_bytes;
@@ -153,9 +155,10 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
         at += align256(bytes);
         return p;
     };
-    double* d_time = reinterpret_cast<double*>(take(3 * sizeof(double) * (size_t)n));
-    double* d_v = d_time + n;
-    double* d_w = d_v + n;
+    double* d_time = reinterpret_cast<double*>(take(3 * sizeof(double) * fstride));
+    double* d_v = d_time + fstride;
+    double* d_w = d_v + fstride;
+    uint32_t* d_fault = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t)));
     double* d_bank = reinterpret_cast<double*>(take(sizeof(double) * host_bank.size()));
     int* d_chunks = reinterpret_cast<int*>(take(sizeof(int) * ((size_t)nchunks + 1)));
     double* d_scales = reinterpret_cast<double*>(take(sizeof(double) * batch));
@@ -180,7 +183,8 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
         if (err != cudaSuccess) report(error, error_len, FBLS_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(err));
         return err == cudaSuccess;
     };
-    if (!ok(cudaMemcpyAsync(d_time, time, sizeof(double) * n, cudaMemcpyHostToDevice, s), "upload time") ||
+    if (!ok(cudaMemsetAsync(d_fault, 0, sizeof(uint32_t), s), "clear fault") ||
+        !ok(cudaMemcpyAsync(d_time, time, sizeof(double) * n, cudaMemcpyHostToDevice, s), "upload time") ||
         !ok(cudaMemcpyAsync(d_v, v, sizeof(double) * n, cudaMemcpyHostToDevice, s), "upload v") ||
         !ok(cudaMemcpyAsync(d_w, w, sizeof(double) * n, cudaMemcpyHostToDevice, s), "upload w") ||
         !ok(cudaMemcpyAsync(d_bank, host_bank.data(), sizeof(double) * host_bank.size(), cudaMemcpyHostToDevice, s),
@@ -215,6 +219,7 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
         fa.stage_field = shape.stage_field;
         fa.window = shape.window;
         fa.row_stride = shape.row_stride;
+        fa.fault = d_fault;
         if (!ok(launch_fold(fa, shape, s), "fold")) return FBLS_ERR_CUDA;
         ScanArgs sa{};
         sa.cum = d_cum;
@@ -263,6 +268,10 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
             return FBLS_ERR_CUDA;
         for (int i = 0; i < p; i++) bad = bad || (flags[cursor + i] & 2u);
     }
+    uint32_t fault = 0;
+    if (!ok(cudaMemcpy(&fault, d_fault, sizeof(uint32_t), cudaMemcpyDeviceToHost), "download fault"))
+        return FBLS_ERR_CUDA;
+    if (fault) return report(error, error_len, FBLS_ERR_CUDA, "fold: staging copies did not complete");
     if (bad) return report(error, error_len, FBLS_ERR_PRECISION, "nonpositive template precision; inspect noise model");
     return FBLS_OK;
 }
