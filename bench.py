@@ -255,12 +255,14 @@ def run_gpu(args):
     fold_ms_per = ctr["fold_ms"] / fold_launches
     fold_bytes_per = ctr["fold_bytes"] / fold_launches
     achieved = fold_bytes_per / (fold_ms_per * 1e-3) / 1e9 if fold_ms_per > 0 else 0.0
+    # DRAM bytes per fold launch, from the committed ncu launch list of this
+    # workload (measured once, not in this run).
     traffic = None
-    prof = ROOT / "profiles" / "fold_prefix_traffic.json"
+    prof = ROOT / "profiles" / "fold_traffic.json"
     if prof.exists():
         try:
             traffic = json.loads(prof.read_text()).get(args.workload)
-        except Exception:
+        except (OSError, ValueError):
             traffic = None
 
     if rank != 0:
@@ -278,9 +280,12 @@ def run_gpu(args):
         "rows_per_step": int(len(rows)),
         "gpu_launches": int(ctr["launches"]),
         "kernel_ms": {"fold_prefix": ctr["fold_ms"] / args.steps, "scan_tiles+merge": ctr["scan_ms"] / args.steps},
-        "roofline": {"kernel": "k_fold_prefix", "bound": "hbm", "achieved": achieved, "peak": peak,
+        "roofline": {"kernel": "k_fold_walk (fold + prefix)", "bound": "hbm", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": fold_bytes_per, "launch_ms": fold_ms_per},
+                     "algorithmic_bytes_per_launch": fold_bytes_per, "launch_ms": fold_ms_per,
+                     "note": "algorithmic bytes count the observation stream once per period (24 n B); it is "
+                             "served from shared memory, and the kernel is bound by the shared-memory pipe "
+                             "(profiles/k_fold_walk_multi_sector.md)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": e2e_total / args.steps},
         "clocks": clk,
