@@ -9,8 +9,12 @@ periods, full scan on the survivors) of one synthetic star:
       17.3 d; 20 durations 0.5-15 h, periods 0.5-20 d at period_oversample 3
       (189,216 periods under the reference's grid rule).
   single_sector: one sector (19,008 points), 12 durations, 13,065 periods.
+  survey: a step is one fbls_search_batch over --stars seeded survey stars
+      (1-13 sectors, 120/200/600 s cadence, 30 % with a box) with
+      --batch-workers host threads, each on its own stream; timed by the host
+      clock around the device-synchronised batch.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload survey]
 
 Trials are templates as the reference counts them (P x nd x ns x nb per
 scanned batch, scan.rs:352). `value` is whole-job trials/s with the star's
@@ -301,6 +305,114 @@ def run_gpu(args):
         torch.distributed.destroy_process_group()
 
 
+def _survey(count: int, seed: int):
+    """`count` seeded survey stars (1-13 sectors, 120/200/600 s cadence, 30 %
+    with an injected box), prepared: [(FamilyState, period_max)], base config."""
+    from fbls_b200 import api, synth
+    rng = np.random.default_rng(seed)
+    stars = []
+    for _ in range(count):
+        c = synth.survey_star(rng)
+        cfg = synth.survey_config(c)
+        stars.append((c, api.prepared_family(c.time, c.flux, c.flux_err, cfg), cfg.period_max))
+    return stars, synth.survey_config(stars[0][0])
+
+
+def run_survey(args):
+    """A step is one fbls_search_batch over a survey of args.stars stars."""
+    import torch
+    world, rank, local = _dist()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    from fbls_b200 import api
+
+    stars, cfg = _survey(args.stars, 1000 + rank)
+    states = [s for _, s, _ in stars]
+    pmax = [p for _, _, p in stars]
+    n_obs = sum(s.n for s in states)
+    gpu = api.Gpu(local)
+    devs = [gpu.upload(s) for s in states]
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step(resident=True):
+        return gpu.search_batch(states, cfg, period_max=pmax, devs=devs if resident else None,
+                                workers=args.batch_workers)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    gpu.counters(reset=True)
+    clocks = Clocks(local)
+    if world > 1:
+        torch.distributed.barrier()
+    clocks.start()
+    gc.collect()
+    gc.disable()
+    times, trials = [], 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = step()
+        times.append((time.perf_counter() - t0) * 1e3)
+        trials += sum(t for _, _, t in out)
+    clk = clocks.stop()
+    ctr = gpu.counters(reset=True)
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out_e = step(resident=False)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    gc.enable()
+    total_ms, e2e_total = sum(times), sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_total, float(trials)], dtype=torch.float64, device=f"cuda:{local}")
+        mx = t.clone()
+        torch.distributed.all_reduce(mx[:2], op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t[2:], op=torch.distributed.ReduceOp.SUM)
+        total_ms, e2e_total, trials = float(mx[0]), float(mx[1]), float(t[2])
+    if rank != 0:
+        return
+    value = trials / (total_ms * 1e-3)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"survey: {args.stars} seeded stars per GPU (1-13 sectors ~ Geometric(0.4), "
+                               "cadence 120/200/600 s, white + AR(1) 0.9 noise, 30 % with a box), 20 durations "
+                               "0.5-15 h, periods 0.5-min(20, baseline/2) d",
+                   "stars": args.stars * world, "observations": n_obs, "batch_workers": args.batch_workers,
+                   "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "stars_per_s": args.stars * world * args.steps / (total_ms * 1e-3),
+        "step_ms": [round(t, 2) for t in times],
+        "gpu_launches": int(ctr["launches"]),
+        "e2e": {"value": trials / (e2e_total * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": 24 * n_obs,
+                "d2h_bytes_per_step": sum(92 * g + 40 * len(r) for r, g, _ in out_e),
+                "ms_per_step": e2e_total / args.steps,
+                "stars_per_s": args.stars * world * args.steps / (e2e_total * 1e-3)},
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu:
+        st, every, threads, tr, sec = _cpu_sample(stars[0][0], cfg, args.cpu_seconds)
+        out["cpu_baseline"] = {"value": tr / sec, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"first survey star, every {every}th period of each band, {tr} trials, "
+                                         f"{sec:.1f} s"}
+    print(json.dumps(out))
+    for d in devs:
+        d.free()
+    gpu.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def run_profile_case(args):
     """One bounded scan_bank pass for profiler captures: the 13-sector star's
     octave band [8, 16) d at its coarse grid (1536 bins), first 4096 periods:
@@ -332,7 +444,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fbls_b200", choices=["fbls_b200", "reference"])
-    ap.add_argument("--workload", default="multi_sector", choices=["multi_sector", "single_sector"])
+    ap.add_argument("--workload", default="multi_sector", choices=["multi_sector", "single_sector", "survey"])
+    ap.add_argument("--stars", type=int, default=512, help="survey workload: stars per GPU")
+    ap.add_argument("--batch-workers", type=int, default=4, help="survey workload: host worker threads")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -340,6 +454,8 @@ def main():
         run_profile_case(args)
     elif args.impl == "reference":
         run_reference(args)
+    elif args.workload == "survey":
+        run_survey(args)
     else:
         run_gpu(args)
 

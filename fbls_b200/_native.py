@@ -38,6 +38,29 @@ class Row(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("period", "epoch", "duration", "score", "depth")]
 
 
+class Star(C.Structure):
+    _fields_ = [
+        ("ready", C.c_void_p),
+        ("time", C.POINTER(C.c_double)),
+        ("v", C.POINTER(C.c_double)),
+        ("w", C.POINTER(C.c_double)),
+        ("n", C.c_uint32),
+        ("baseline_norm", C.c_double),
+        ("origin", C.c_double),
+        ("residual_energy", C.c_double),
+        ("durations", C.POINTER(C.c_double)),
+        ("rho", C.POINTER(C.c_double)),
+        ("nd", C.c_uint32),
+        ("period_max", C.c_double),
+        ("rows", C.POINTER(Row)),
+        ("capacity", C.c_uint32),
+        ("n_rows", C.c_uint32),
+        ("grid_len", C.c_uint64),
+        ("templates", C.c_uint64),
+        ("status", C.c_int),
+    ]
+
+
 class ScanStats(C.Structure):
     _fields_ = [
         ("periods", C.c_uint64),
@@ -143,6 +166,7 @@ SIGNATURES = {
     "fbls_signal_search": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, c_double_p, C.c_uint32,
                                      C.POINTER(Config), C.POINTER(Row), C.c_uint32, c_uint32_p, c_uint64_p,
                                      C.POINTER(ScanStats), c_uint32_p]),
+    "fbls_search_batch": (C.c_int, [C.c_void_p, C.POINTER(Star), C.c_uint32, C.POINTER(Config), C.c_uint32]),
 }
 
 _lib = None

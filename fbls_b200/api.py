@@ -233,6 +233,44 @@ class Gpu:
                                                C.byref(n), C.byref(st)))
         return _rows_array(rows, n.value), st.as_dict()
 
+    def search_batch(self, states: Sequence[FamilyState], cfg: SearchConfig, period_max: Optional[Sequence[float]] = None,
+                     devs: Optional[Sequence[DeviceReady]] = None, workers: int = 4):
+        """signal_search over many stars with `workers` host threads, each
+        with its own stream: [(rows N x 5, grid length, templates)] per star.
+        period_max overrides cfg.period_max per star; devs are uploaded
+        families (else each worker uploads the star's host arrays)."""
+        count = len(states)
+        stars = (N.Star * max(count, 1))()
+        keep = []
+        for i, s in enumerate(states):
+            st = stars[i]
+            if devs is not None:
+                st.ready = devs[i].handle
+            else:
+                t, v, w = _f64(s.time), _f64(s.v), _f64(s.w)
+                keep += [t, v, w]
+                st.time, st.v, st.w = _dptr(t), _dptr(v), _dptr(w)
+                st.n = t.shape[0]
+            st.baseline_norm, st.origin, st.residual_energy = s.baseline_norm, s.origin, s.residual_energy
+            d, r = _f64(s.durations), _f64(s.rho)
+            keep += [d, r]
+            st.durations, st.rho, st.nd = _dptr(d), _dptr(r), len(d)
+            pm = math.nan if period_max is None else float(period_max[i])
+            st.period_max = pm
+            c1 = dataclasses.replace(cfg, period_max=pm) if math.isfinite(pm) else cfg
+            cap = max(1, _grid_count(s, c1))
+            rows = (N.Row * cap)()
+            keep.append(rows)
+            st.rows = C.cast(rows, C.POINTER(N.Row))
+            st.capacity = cap
+        c, ck = _config(cfg)
+        self._check(self.lib.fbls_search_batch(self.ctx, stars, count, C.byref(c), int(workers)))
+        out = []
+        for i in range(count):
+            st = stars[i]
+            out.append((_rows_array(st.rows, st.n_rows), int(st.grid_len), int(st.templates)))
+        return out
+
     def signal_search(self, state: FamilyState, cfg: SearchConfig, dev: Optional[DeviceReady] = None):
         """signal_search: (rows N x 5, grid length, per-band ScanStats)."""
         own = dev is None

@@ -25,6 +25,8 @@
 // The doubled prefix sums then follow the association of the reference's
 // prefix_block (kernels.rs:237-309), one warp per (period, field) row, and
 // are written as f64 and (hi, lo) f32 pairs.
+#include <mutex>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -538,14 +540,24 @@ int fold_chunks(const double* time, int n, double scale_max, int nb, int span_ca
 }
 
 cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_fold_walk<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)MAX_FOLD_SMEM);
+    // The shared-memory limit is a per-device attribute of each kernel; set it
+    // once per device (contexts of several host threads may launch).
+    {
+        static std::mutex mu;
+        static bool configured[64] = {};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
         if (e != cudaSuccess) return e;
-        configured = true;
+        if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+        std::lock_guard<std::mutex> lock(mu);
+        if (!configured[dev]) {
+            e = cudaFuncSetAttribute(k_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_fold_walk<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)MAX_FOLD_SMEM);
+            if (e != cudaSuccess) return e;
+            configured[dev] = true;
+        }
     }
     if (shape.kind == FOLD_WALK) {
         if (shape.smem > MAX_FOLD_SMEM || a.group != shape.group || a.group < 1 || a.group > MAX_GROUP ||

@@ -10,11 +10,13 @@
 // kernel with the histograms in shared memory, all batches of a band are
 // queued on one stream, and the band's records come back in one copy.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/fbls_b200.h"
@@ -48,7 +50,9 @@ struct fbls_ctx {
     // Workspace, grown on demand and reused across bands and calls.
     DevBuf bank, scales, periods, cum, cum32, hist, parts, keys, tflags, records, score, depth, rflags;
     DevBuf evidence, chunks, fault;
+    DevBuf family;  // observations of the star a batch worker is searching
     std::vector<int> host_chunks;
+    std::vector<fbls_ctx*> workers;  // fbls_search_batch worker contexts, kept for reuse
 };
 
 struct fbls_ready {
@@ -62,6 +66,7 @@ struct fbls_ready {
     double residual_energy = 0.0;
     double t_last = 0.0;
     std::vector<double> time_host;  // for the fold's chunk boundaries
+    bool owned = true;              // time/v/w allocated for this handle (else a context's buffer)
 };
 
 namespace {
@@ -107,6 +112,54 @@ void release(DevBuf& b) {
 template <typename T>
 T* as(DevBuf& b) {
     return reinterpret_cast<T*>(b.ptr);
+}
+
+// Checks and uploads a prepared family into `r` (DeviceReady::upload,
+// scan.rs:110-124): into a fresh allocation owned by `r` when `buf` is null,
+// else into the reusable context buffer `buf` (no allocation once it is
+// large enough, so a batch worker never synchronises the device on cudaFree).
+int upload_family(fbls_ctx* ctx, DevBuf* buf, const double* time, const double* v, const double* w, uint32_t n,
+                  double baseline_norm, double origin, double residual_energy, fbls_ready* r) {
+    if (!time || !v || !w) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (n < 6) return fail(ctx, FBLS_ERR_DATA, "at least six observations are required");
+    for (uint32_t i = 1; i < n; i++)
+        if (!(time[i] >= time[i - 1])) return fail(ctx, FBLS_ERR_ARGUMENT, "times must be ascending");
+    if (!(time[0] >= 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "times must be relative to the first observation");
+    r->ctx = ctx;
+    r->n = n;
+    r->baseline_norm = baseline_norm;
+    r->origin = origin;
+    r->residual_energy = residual_energy;
+    r->t_last = time[n - 1];
+    r->time_host.assign(time, time + n);
+    const size_t bytes = (size_t)n * sizeof(double);
+    const size_t stride = fold_field_stride(n);
+    cudaError_t e;
+    if (buf) {
+        e = ensure(*buf, 3 * stride * sizeof(double));
+        r->time = static_cast<double*>(buf->ptr);
+        r->owned = false;
+    } else {
+        e = cudaMalloc(&r->time, 3 * stride * sizeof(double));
+        r->owned = true;
+    }
+    if (e != cudaSuccess) {
+        r->time = nullptr;
+        return cuda_fail(ctx, e, "upload_ready");
+    }
+    r->v = r->time + stride;
+    r->w = r->v + stride;
+    e = cudaMemsetAsync(r->time, 0, 3 * stride * sizeof(double), ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(r->time, time, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(r->v, v, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(r->w, w, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        if (r->owned) cudaFree(r->time);
+        r->time = nullptr;
+        return cuda_fail(ctx, e, "upload_ready");
+    }
+    return FBLS_OK;
 }
 
 // Fold budget in MiB: the configured value capped at half of the free device
@@ -432,8 +485,9 @@ void fbls_destroy(fbls_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf* bufs[] = {&ctx->bank,  &ctx->scales,  &ctx->periods, &ctx->cum,   &ctx->cum32,  &ctx->hist,    &ctx->parts,
                       &ctx->keys,  &ctx->tflags,  &ctx->records, &ctx->score, &ctx->depth,  &ctx->rflags,  &ctx->evidence,
-                      &ctx->chunks, &ctx->fault};
+                      &ctx->chunks, &ctx->fault,  &ctx->family};
     for (DevBuf* b : bufs) release(*b);
+    for (fbls_ctx* w : ctx->workers) fbls_destroy(w);
     for (int i = 0; i < 4; i++)
         if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
     for (int i = 0; i < 2; i++)
@@ -476,38 +530,13 @@ int fbls_read_counters(fbls_ctx* ctx, fbls_counters* out, int reset) {
 
 int fbls_upload_ready(fbls_ctx* ctx, const double* time, const double* v, const double* w, uint32_t n,
                       double baseline_norm, double origin, double residual_energy, fbls_ready** out) {
-    if (!ctx || !out || !time || !v || !w) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    if (n < 6) return fail(ctx, FBLS_ERR_DATA, "at least six observations are required");
-    for (uint32_t i = 1; i < n; i++)
-        if (!(time[i] >= time[i - 1])) return fail(ctx, FBLS_ERR_ARGUMENT, "times must be ascending");
-    if (!(time[0] >= 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "times must be relative to the first observation");
+    if (!ctx || !out) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
     CK(cudaSetDevice(ctx->device), "set device");
     fbls_ready* r = new fbls_ready();
-    r->ctx = ctx;
-    r->n = n;
-    r->baseline_norm = baseline_norm;
-    r->origin = origin;
-    r->residual_energy = residual_energy;
-    r->t_last = time[n - 1];
-    r->time_host.assign(time, time + n);
-    const size_t bytes = (size_t)n * sizeof(double);
-    const size_t stride = fold_field_stride(n);
-    cudaError_t e = cudaMalloc(&r->time, 3 * stride * sizeof(double));
-    if (e != cudaSuccess) {
+    const int rc = upload_family(ctx, nullptr, time, v, w, n, baseline_norm, origin, residual_energy, r);
+    if (rc) {
         delete r;
-        return cuda_fail(ctx, e, "upload_ready");
-    }
-    r->v = r->time + stride;
-    r->w = r->v + stride;
-    e = cudaMemsetAsync(r->time, 0, 3 * stride * sizeof(double), ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(r->time, time, bytes, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(r->v, v, bytes, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(r->w, w, bytes, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) {
-        cudaFree(r->time);
-        delete r;
-        return cuda_fail(ctx, e, "upload_ready");
+        return rc;
     }
     *out = r;
     return FBLS_OK;
@@ -515,8 +544,10 @@ int fbls_upload_ready(fbls_ctx* ctx, const double* time, const double* v, const 
 
 void fbls_free_ready(fbls_ready* r) {
     if (!r) return;
-    if (r->ctx) cudaSetDevice(r->ctx->device);
-    cudaFree(r->time);
+    if (r->owned) {
+        if (r->ctx) cudaSetDevice(r->ctx->device);
+        cudaFree(r->time);
+    }
     delete r;
 }
 
@@ -675,6 +706,76 @@ int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* du
                                 return ctx->evidence.ptr;
                             });
     if (rc) return fail(ctx, rc, message);
+    return FBLS_OK;
+}
+
+// Many stars on one device: `workers` host threads (the caller's included),
+// each with its own context (stream, workspace and a reusable buffer for the
+// star's observations), take stars from a shared counter and run
+// signal_search on them, so one star's host work and small launches overlap
+// the others' kernels. The reference runs one star per device worker thread
+// (src/batch.rs:61-102) with one context per thread.
+int fbls_search_batch(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbls_config* cfg, uint32_t workers) {
+    if (!ctx || (count && !stars) || !cfg) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (count == 0) return FBLS_OK;
+    workers = std::max(1u, std::min({workers, count, 64u}));
+    CK(cudaSetDevice(ctx->device), "set device");
+    while (ctx->workers.size() < workers) {
+        int status = FBLS_OK;
+        fbls_ctx* w = fbls_create(ctx->device, &status);
+        if (!w) return fail(ctx, status ? status : FBLS_ERR_CUDA, "batch worker context");
+        ctx->workers.push_back(w);
+    }
+    for (uint32_t k = 0; k < workers; k++) ctx->workers[k]->kernel_timing = ctx->kernel_timing;
+    std::atomic<uint32_t> next{0};
+    std::vector<std::string> errors(count);
+    auto work = [&](fbls_ctx* wc) {
+        if (cudaSetDevice(wc->device) != cudaSuccess) return;
+        for (;;) {
+            const uint32_t i = next.fetch_add(1);
+            if (i >= count) break;
+            fbls_star& s = stars[i];
+            s.n_rows = 0;
+            s.grid_len = 0;
+            s.templates = 0;
+            fbls_ready local;
+            const fbls_ready* r = s.ready;
+            int rc = FBLS_OK;
+            if (!r) {
+                rc = upload_family(wc, &wc->family, s.time, s.v, s.w, s.n, s.baseline_norm, s.origin,
+                                   s.residual_energy, &local);
+                r = &local;
+            }
+            if (rc == FBLS_OK) {
+                fbls_config c = *cfg;
+                if (std::isfinite(s.period_max)) c.period_max = s.period_max;
+                fbls_scan_stats st[64];
+                uint32_t bands = 0;
+                rc = fbls_signal_search(wc, r, s.durations, s.rho, s.nd, &c, s.rows, s.capacity, &s.n_rows,
+                                        &s.grid_len, st, &bands);
+                for (uint32_t b = 0; rc == FBLS_OK && b < bands && b < 64; b++) s.templates += st[b].templates_scanned;
+            }
+            s.status = rc;
+            if (rc) errors[i] = wc->error;
+        }
+    };
+    std::vector<std::thread> threads;
+    for (uint32_t k = 1; k < workers; k++) threads.emplace_back(work, ctx->workers[k]);
+    work(ctx->workers[0]);
+    for (std::thread& t : threads) t.join();
+    for (uint32_t k = 0; k < workers; k++) {
+        ctx->counters.launches += ctx->workers[k]->counters.launches;
+        ctx->counters.fold_launches += ctx->workers[k]->counters.fold_launches;
+        ctx->counters.fold_ms += ctx->workers[k]->counters.fold_ms;
+        ctx->counters.fold_bytes += ctx->workers[k]->counters.fold_bytes;
+        ctx->counters.scan_launches += ctx->workers[k]->counters.scan_launches;
+        ctx->counters.scan_ms += ctx->workers[k]->counters.scan_ms;
+        ctx->counters.scan_bytes += ctx->workers[k]->counters.scan_bytes;
+        ctx->counters.fold_updates += ctx->workers[k]->counters.fold_updates;
+        std::memset(&ctx->workers[k]->counters, 0, sizeof(fbls_counters));
+    }
+    for (uint32_t i = 0; i < count; i++)
+        if (stars[i].status) return fail(ctx, stars[i].status, "star " + std::to_string(i) + ": " + errors[i]);
     return FBLS_OK;
 }
 

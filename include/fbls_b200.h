@@ -255,6 +255,45 @@ int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* dur
                        uint32_t nd, const fbls_config* cfg, fbls_row* rows_out, uint32_t capacity,
                        uint32_t* n_rows, uint64_t* grid_len, fbls_scan_stats* stats_out, uint32_t* n_bands);
 
+/* ---- batched search (replaces the reference's per-device worker threads,
+ * src/batch.rs:61-102, each running one star's search at a time) --------- */
+
+/* One star of a batch. Inputs: an uploaded family (`ready`), or a prepared
+ * family in host memory (time, v, w, n and its scalars) that the worker
+ * uploads itself; the family's durations and rho; period_max overrides
+ * cfg->period_max when finite (SearchConfig per star). Outputs: rows
+ * (caller-owned, capacity of them: the star's grid length suffices), the
+ * row count, grid length, templates scanned and the star's status. */
+typedef struct {
+    const fbls_ready* ready;
+    const double* time;
+    const double* v;
+    const double* w;
+    uint32_t n;
+    double baseline_norm;
+    double origin;
+    double residual_energy;
+    const double* durations;
+    const double* rho;
+    uint32_t nd;
+    double period_max;
+    fbls_row* rows;
+    uint32_t capacity;
+    uint32_t n_rows;
+    uint64_t grid_len;
+    uint64_t templates;
+    int status;
+} fbls_star;
+
+/* signal_search for every star of `stars` on the context's device, with
+ * `workers` host threads (1..64, the caller's thread included), each with its
+ * own stream and workspace (kept in ctx for later calls). Results are the
+ * same as one fbls_signal_search per star. Returns 0, or the status of the
+ * first failing star (its message in fbls_last_error, prefixed "star i: ");
+ * every star's own status is in its record. Do not share a context between
+ * concurrent calls. */
+int fbls_search_batch(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbls_config* cfg, uint32_t workers);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,47 @@
+"""fbls_search_batch: many stars on one device with several worker threads
+must give, star for star, the rows of one signal_search per star."""
+import numpy as np
+import pytest
+
+from fbls_b200 import api, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _stars(count, seed=11, max_sectors=2):
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < count:
+        c = synth.survey_star(rng)
+        if c.time[-1] - c.time[0] > 27.4 * max_sectors + 1:
+            continue
+        cfg = synth.survey_config(c)
+        out.append((api.prepared_family(c.time, c.flux, c.flux_err, cfg), cfg))
+    return out
+
+
+@pytest.mark.parametrize("uploaded", [False, True])
+def test_batch_matches_per_star_search(gpu, uploaded):
+    stars = _stars(6)
+    base = stars[0][1]
+    pmax = [cfg.period_max for _, cfg in stars]
+    want = [gpu.signal_search(st, cfg) for st, cfg in stars]
+    devs = [gpu.upload(st) for st, _ in stars] if uploaded else None
+    got = gpu.search_batch([st for st, _ in stars], base, period_max=pmax, devs=devs, workers=3)
+    for (rows, glen, templates), (wrows, wglen, wstats) in zip(got, want):
+        assert glen == wglen
+        assert templates == sum(s["templates_scanned"] for s in wstats)
+        assert np.array_equal(rows, wrows)
+    if devs:
+        for d in devs:
+            d.free()
+
+
+def test_batch_reports_the_failing_star(gpu):
+    stars = _stars(3)
+    st = stars[1][0]
+    short = api.FamilyState(st.time[:4], st.v[:4], st.w[:4], st.baseline_norm, st.origin, st.residual_energy,
+                            st.durations, st.rho)
+    states = [stars[0][0], short, stars[2][0]]
+    with pytest.raises(api.FblsError, match="star 1: at least six observations"):
+        gpu.search_batch(states, stars[0][1], period_max=[cfg.period_max for _, cfg in stars], workers=2)
