@@ -16,12 +16,14 @@ namespace fbls {
 // ---------------------------------------------------------------------------
 
 struct LaneState {
-    double best;
+    double best;  // f64 pass
+    float bestf;  // f32 pass: the reference keeps its f32 merits in the same f64 slot, exactly
     uint64_t key;
     uint32_t di;
     bool bad, sensitive, unsafe_merit;
     __device__ void reset() {
         best = neg_inf();
+        bestf = -__builtin_huge_valf();
         key = KEY_MAX;
         di = 0;
         bad = sensitive = unsafe_merit = false;
@@ -47,7 +49,7 @@ __device__ __forceinline__ float rank_fast(LaneState& s, float a32, float hp32, 
     float merit = __fdiv_rn(__fmul_rn(a32, a32), qq);
     bool safe = cn > 0.0f && qq >= __fmul_rn(0.001f, cn) && merit >= 1e-30f && merit <= 1e30f;
     s.unsafe_merit |= valid && !safe;
-    float best = (float)s.best;
+    const float best = s.bestf;
     const float guard = 1e-5f;
     bool near = best > 0.0f && fabsf(__fsub_rn(merit, best)) <= __fmul_rn(guard, rmaxf(merit, best));
     bool far_better = merit > __fmul_rn(best, 1.00004f);
@@ -57,7 +59,7 @@ __device__ __forceinline__ float rank_fast(LaneState& s, float a32, float hp32, 
         s.sensitive = s.sensitive || (valid && safe && near);
     bool better = valid && safe && (merit > best || (merit == best && key < s.key));
     if (better) {
-        s.best = (double)merit;
+        s.bestf = merit;
         s.key = key;
         s.di = di;
     }
@@ -134,22 +136,36 @@ __device__ __forceinline__ void shape_sums32(const float2* __restrict__ rv, cons
     }
 }
 
-__global__ void __launch_bounds__(TILE) k_scan_tiles(ScanArgs a) {
+// Eight CTAs per SM (64 registers): the f32 pass keeps its state in registers;
+// the few spills are on the f64 rescan and winner paths.
+__global__ void __launch_bounds__(TILE, 8) k_scan_tiles(ScanArgs a) {
     __shared__ double s_dur[MAX_DURATIONS], s_rho[MAX_DURATIONS], s_ing[MAX_SHAPES];
     __shared__ double s_fac[MAX_SHAPES * MAX_LAYERS];
     __shared__ double s_wv[TILE / 32];
     __shared__ unsigned long long s_wk[TILE / 32];
     __shared__ int s_wl[TILE / 32];
     __shared__ uint32_t s_di;
+    // Per duration, the same for every lane: width k = min(raw, nb / 2),
+    // whether raw < nb / 2, and rho^2 in f32.
+    __shared__ uint32_t s_k[MAX_DURATIONS];
+    __shared__ unsigned char s_kok[MAX_DURATIONS];
+    __shared__ float s_r2f[MAX_DURATIONS];
 
     const int lane = threadIdx.x;
     const int tile = blockIdx.x;
     const int f = blockIdx.y;
     const int nb = a.nb;
     const int nd = a.nd, ns = a.ns, layers = a.layers;
+    const uint32_t half = (uint32_t)(nb / 2);
+    const double scale = a.scales[f];
     for (int i = lane; i < nd; i += TILE) {
-        s_dur[i] = a.durations[i];
-        s_rho[i] = a.rho[i];
+        const double d = a.durations[i], r = a.rho[i];
+        s_dur[i] = d;
+        s_rho[i] = r;
+        const uint32_t raw_k = template_width(d, scale);
+        s_k[i] = min(raw_k, half);
+        s_kok[i] = raw_k < half;
+        s_r2f[i] = (float)(r * r);
     }
     for (int i = lane; i < ns; i += TILE) s_ing[i] = a.ingress[i];
     for (int i = lane; i < ns * layers; i += TILE) s_fac[i] = a.factors[i];
@@ -157,7 +173,6 @@ __global__ void __launch_bounds__(TILE) k_scan_tiles(ScanArgs a) {
 
     const uint32_t j = (uint32_t)(tile * TILE + lane);
     const uint32_t jj = min(j, (uint32_t)(nb - 1));
-    const double scale = a.scales[f];
     const size_t stride = 2 * (size_t)nb + 1;
     const double* c64 = a.cum + (size_t)f * NF * stride;
     const float2* c32 = a.cum32 + (size_t)f * NF * stride;
@@ -171,7 +186,9 @@ __global__ void __launch_bounds__(TILE) k_scan_tiles(ScanArgs a) {
     const float basef = (float)baseline;
     const double nobs = a.n;
     const uint64_t nb1 = (uint64_t)nb + 1;
-    const uint32_t half = (uint32_t)(nb / 2);
+    // For an f32 count c: (double)c <= nobs - 3 exactly when c <= count_max.
+    float count_max = (float)(nobs - 3.0);
+    if ((double)count_max > nobs - 3.0) count_max = nextafterf(count_max, -__builtin_huge_valf());
 
     LaneState st;
     st.reset();
@@ -191,38 +208,42 @@ __global__ void __launch_bounds__(TILE) k_scan_tiles(ScanArgs a) {
             st.reset();
         }
         const double gate_value = fast ? __ddiv_rn(__dmul_rn(a.gate, a.gate), baseline) : a.gate;
+        // For an f32 merit m: (double)m >= gate_value exactly when m >= gate_f.
+        float gate_f = (float)gate_value;
+        if ((double)gate_f < gate_value) gate_f = nextafterf(gate_f, __builtin_huge_valf());
         for (int di = 0; di < nd; di++) {
-            const uint32_t raw_k = template_width(s_dur[di], scale);
-            const uint32_t k = min(raw_k, half);
+            const uint32_t k = s_k[di];
+            const bool k_ok = s_kok[di] != 0;
             const double r = s_rho[di];
             const uint64_t key = (uint64_t)k * nb1 + jj;
-            bool usable, valid;
-            double merit;
+            bool usable, open;
             float oa32 = 0.f, ow32 = 0.f;
             if (fast) {
                 float count = interval32(rn32, jj, k);
                 ow32 = interval32(rw32, jj, k);
                 oa32 = interval32(rv32, jj, k);
-                usable = j < (uint32_t)nb && raw_k < half && count >= 3.0f && (double)count <= nobs - 3.0;
-                valid = usable && oa32 > 0.0f;
-                merit = (double)rank_fast(st, oa32, ow32, ow32, (float)(r * r), basef, valid, key, (uint32_t)di);
+                usable = j < (uint32_t)nb && k_ok && count >= 3.0f && count <= count_max;
+                const bool valid = usable && oa32 > 0.0f;
+                const float merit = rank_fast(st, oa32, ow32, ow32, s_r2f[di], basef, valid, key, (uint32_t)di);
+                open = valid && merit >= gate_f;
             } else {
                 double count = interval64(rn64, jj, k);
                 double w = interval64(rw64, jj, k);
                 double av = interval64(rv64, jj, k);
-                usable = j < (uint32_t)nb && raw_k < half && count >= 3.0 && count <= nobs - 3.0;
-                valid = usable && av > 0.0;
-                merit = rank_exact(st, av, w, w, r, baseline, valid, key, (uint32_t)di);
+                usable = j < (uint32_t)nb && k_ok && count >= 3.0 && count <= nobs - 3.0;
+                const bool valid = usable && av > 0.0;
+                const double merit = rank_exact(st, av, w, w, r, baseline, valid, key, (uint32_t)di);
+                open = valid && merit >= gate_value;
             }
             // Tile-level shape gate (kernels.rs:715-726).
-            if (!__syncthreads_or(valid && merit >= gate_value)) continue;
+            if (!__syncthreads_or(open)) continue;
             for (int si = 1; si < ns; si++) {
                 const double ing = s_ing[si];
                 const uint64_t skey = ((uint64_t)si * nb1 + k) * nb1 + jj;
                 if (fast) {
                     float sa, shp, snorm;
                     shape_sums32(rv32, rw32, jj, k, oa32, ow32, ow32, ing, s_fac, si, layers, sa, shp, snorm);
-                    rank_fast(st, sa, shp, snorm, (float)(r * r), basef, usable && sa > 0.0f, skey, (uint32_t)di);
+                    rank_fast(st, sa, shp, snorm, s_r2f[di], basef, usable && sa > 0.0f, skey, (uint32_t)di);
                 } else {
                     double w = interval64(rw64, jj, k);
                     double av = interval64(rv64, jj, k);
@@ -232,6 +253,7 @@ __global__ void __launch_bounds__(TILE) k_scan_tiles(ScanArgs a) {
                 }
             }
         }
+        if (fast) st.best = (double)st.bestf;
         if (fast && st.best <= 0.0) st.key = nb1 + jj;
         // Block winner: largest value, then smallest key, then lowest lane.
         double v = st.best;
