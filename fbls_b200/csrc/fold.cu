@@ -312,6 +312,10 @@ __device__ __forceinline__ void stage_chunk(const FoldArgs& a, int i0, int i1, d
 // Chunks are staged by TMA bulk copies into two buffers (fields t, v, w),
 // one chunk ahead of the one being folded, so the copy overlaps the walk.
 
+// Segments at least this long are walked in lockstep (measured: shorter ones
+// lose more to idle steps than the conflict-free reads gain).
+constexpr int LOCKSTEP_MIN_SEGMENT = 11;
+
 template <int CAP>
 __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
     constexpr int F = CAP + 2;  // doubles per staged field
@@ -392,30 +396,91 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
         if (live && seg == 0) lstart[NS] = len;
         __syncthreads();
         const int end = live ? lstart[seg + 1] : 0;
-        if (live && k < end) {
-            uint32_t cur = cell_of(tt[k], scale);
-            const uint32_t s0 = mod_nb(cur, unb, inv_nb);
-            const uint32_t base = cur - s0;
-            uint32_t slot = s0;
-            double2 acc = lvw[slot];
-            uint32_t cnt = lc[slot];
-            for (int j = k; j < end; j++) {
-                const uint32_t cj = cell_of(tt[j], scale);
-                if (cj != cur) {
+        if (R < LOCKSTEP_MIN_SEGMENT) {
+            // Short segments: each lane walks its own window.
+            if (live && k < end) {
+                uint32_t cur = cell_of(tt[k], scale);
+                const uint32_t s0 = mod_nb(cur, unb, inv_nb);
+                const uint32_t base = cur - s0;
+                uint32_t slot = s0;
+                double2 acc = lvw[slot];
+                uint32_t cnt = lc[slot];
+                for (int j = k; j < end; j++) {
+                    const uint32_t cj = cell_of(tt[j], scale);
+                    if (cj != cur) {
+                        lvw[slot] = acc;
+                        lc[slot] = cnt;
+                        const uint32_t b = cj - base;
+                        slot = b >= unb ? b - unb : b;
+                        cur = cj;
+                        acc = lvw[slot];
+                        cnt = lc[slot];
+                    }
+                    acc.x = __dadd_rn(acc.x, tt[j + F]);
+                    acc.y = __dadd_rn(acc.y, tt[j + 2 * F]);
+                    cnt += 1u;
+                }
+                lvw[slot] = acc;
+                lc[slot] = cnt;
+            }
+            continue;
+        }
+        // Lockstep walk: at step i every lane reads observation seg * R + i
+        // (R odd, so the lanes' reads fall in distinct banks) and folds it when
+        // it lies in the lane's window [k, end). Entering a cell takes the
+        // bin's sums prefetched at the previous cell change (the next cell's
+        // bin), and prefetches the bin after it.
+        const int b0 = seg * R;
+        const bool has = live && k < end;
+        const int steps = __reduce_max_sync(0xffffffffu, has ? end - b0 : 0);
+        if (steps > 0) {
+            uint32_t cur = 0, base = 0, slot = 0, nslot = 0, cnt = 0, pcnt = 0;
+            double2 acc = make_double2(0.0, 0.0), pre = acc;
+            if (has) {
+                cur = cell_of(tt[k], scale);
+                const uint32_t s0 = mod_nb(cur, unb, inv_nb);
+                base = cur - s0;  // bin = cell - base (- nb past the wrap)
+                slot = s0;
+                nslot = s0 + 1u == unb ? 0u : s0 + 1u;
+                acc = lvw[slot];
+                cnt = lc[slot];
+                pre = lvw[nslot];
+                pcnt = lc[nslot];
+            }
+            for (int i = 0; i < steps; i++) {
+                const int o = b0 + i;
+                const int j = min(o, len);  // staged slot (or slack) for every step
+                const double tj = tt[j], vj = tt[j + F], wj = tt[j + 2 * F];
+                const bool in = o >= k && o < end;
+                const uint32_t cj = cell_of(tj, scale);
+                if (in && cj != cur) {
                     lvw[slot] = acc;
                     lc[slot] = cnt;
-                    uint32_t b = cj - base;
-                    slot = b >= unb ? b - unb : b;
+                    if (cj == cur + 1u) {
+                        acc = pre;
+                        cnt = pcnt;
+                        slot = nslot;
+                    } else {  // empty cells skipped
+                        const uint32_t b = cj - base;
+                        slot = b >= unb ? b - unb : b;
+                        acc = lvw[slot];
+                        cnt = lc[slot];
+                    }
                     cur = cj;
-                    acc = lvw[slot];
-                    cnt = lc[slot];
+                    nslot = slot + 1u == unb ? 0u : slot + 1u;
+                    pre = lvw[nslot];
+                    pcnt = lc[nslot];
                 }
-                acc.x = __dadd_rn(acc.x, tt[j + F]);
-                acc.y = __dadd_rn(acc.y, tt[j + 2 * F]);
-                cnt += 1u;
+                if (in) {
+                    acc.x = __dadd_rn(acc.x, vj);
+                    acc.y = __dadd_rn(acc.y, wj);
+                    cnt += 1u;
+                }
             }
-            lvw[slot] = acc;
-            lc[slot] = cnt;
+            if (has) {
+                lvw[slot] = acc;
+                lc[slot] = cnt;
+            }
         }
     }
     __syncthreads();

@@ -235,14 +235,26 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
         return fail(ctx, FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
 
     const size_t stride = 2 * (size_t)nb + 1;
+    // Periods per launch: whole batches of the reference's size, as many as
+    // the fold budget holds in this path's buffers (cum, cum32 and tile parts;
+    // the histograms never reach device memory), up to 16,384, so bands with
+    // few bins fill the GPU with larger period groups. Statistics still count
+    // the reference's batches.
+    const double launch_period_bytes =
+        (double)(NF * stride * (sizeof(double) + sizeof(float2)) +
+                 tiles * (PART_STRIDE * sizeof(double) + sizeof(uint64_t) + sizeof(uint32_t)));
+    uint64_t launch = (uint64_t)std::floor(bank->max_fold_mib * 1048576.0 / launch_period_bytes);
+    launch = std::min<uint64_t>(launch, 16384);
+    launch = std::max<uint64_t>(launch / batch, 1) * batch;
+    if (launch > P) launch = P;
     CK(ensure(ctx->bank, host_bank.size() * sizeof(double)), "workspace");
     CK(ensure(ctx->scales, (size_t)P * sizeof(double)), "workspace");
     CK(ensure(ctx->periods, (size_t)P * sizeof(double)), "workspace");
-    CK(ensure(ctx->cum, batch * NF * stride * sizeof(double)), "workspace");
-    CK(ensure(ctx->cum32, batch * NF * stride * sizeof(float2)), "workspace");
-    CK(ensure(ctx->parts, batch * tiles * PART_STRIDE * sizeof(double)), "workspace");
-    CK(ensure(ctx->keys, batch * tiles * sizeof(uint64_t)), "workspace");
-    CK(ensure(ctx->tflags, batch * tiles * sizeof(uint32_t)), "workspace");
+    CK(ensure(ctx->cum, launch * NF * stride * sizeof(double)), "workspace");
+    CK(ensure(ctx->cum32, launch * NF * stride * sizeof(float2)), "workspace");
+    CK(ensure(ctx->parts, launch * tiles * PART_STRIDE * sizeof(double)), "workspace");
+    CK(ensure(ctx->keys, launch * tiles * sizeof(uint64_t)), "workspace");
+    CK(ensure(ctx->tflags, launch * tiles * sizeof(uint32_t)), "workspace");
     CK(ensure(ctx->records, (size_t)P * RECORD_STRIDE * sizeof(double)), "workspace");
     CK(ensure(ctx->score, (size_t)P * sizeof(double)), "workspace");
     CK(ensure(ctx->depth, (size_t)P * sizeof(double)), "workspace");
@@ -251,11 +263,11 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
     FoldShape shape;
     int nchunks = 0;
     {
-        int rc = plan_fold(ctx, r, scale_max, (int)nb, (int)batch, &shape, &nchunks);
+        int rc = plan_fold(ctx, r, scale_max, (int)nb, (int)launch, &shape, &nchunks);
         if (rc) return rc;
     }
     if (!shape.hist_in_smem) {
-        const size_t blocks = (batch + shape.group - 1) / shape.group;
+        const size_t blocks = (launch + shape.group - 1) / shape.group;
         CK(ensure(ctx->hist, blocks * shape.group * NF * (size_t)shape.row_stride * sizeof(double)), "workspace");
     }
 
@@ -270,7 +282,7 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
     const double* d_bank = as<double>(ctx->bank);
 
     const bool timing = ctx->profile || ctx->kernel_timing;
-    const uint64_t nbatches = (P + batch - 1) / batch;
+    const uint64_t nbatches = (P + launch - 1) / launch;
     if (timing) {
         while (ctx->pool.size() < 3 * nbatches) {
             cudaEvent_t e;
@@ -279,8 +291,8 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
         }
     }
     uint64_t bi = 0;
-    for (uint64_t cursor = 0; cursor < P; cursor += batch, bi++) {
-        const int p = (int)((P - cursor) < batch ? (P - cursor) : batch);
+    for (uint64_t cursor = 0; cursor < P; cursor += launch, bi++) {
+        const int p = (int)((P - cursor) < launch ? (P - cursor) : launch);
         FoldArgs fa;
         fa.time = r->time;
         fa.v = r->v;
@@ -348,7 +360,7 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
         ctx->counters.scan_bytes += (double)p * (24.0 * (double)stride + 84.0 * tiles);
         if (stats) {
             stats->templates_scanned += (uint64_t)p * nd * ns * nb;
-            stats->batches += 1;
+            stats->batches += ((uint64_t)p + batch - 1) / batch;
         }
     }
     out.records.resize((size_t)P * RECORD_STRIDE);
