@@ -7,8 +7,10 @@
 //                  full scan, threshold)
 //   signal_search  src/search/scan.rs:413-473 (octave bands)
 // The device work differs from the reference's: fold and prefix run as one
-// kernel with the histograms in shared memory, all batches of a band are
-// queued on one stream, and the band's records come back in one copy.
+// kernel with the histograms in shared memory, and a signal search runs as
+// two sessions (every band's first pass, then every band's survivor pass),
+// each with one upload from page-locked memory, all launches back to back on
+// one stream, one download and one synchronisation.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -34,6 +36,11 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+struct PinBuf {  // page-locked host memory
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
 }  // namespace
 
 struct fbls_ctx {
@@ -48,10 +55,11 @@ struct fbls_ctx {
     std::vector<cudaEvent_t> pool;  // per-launch timing events
     fbls_counters counters{};
     // Workspace, grown on demand and reused across bands and calls.
-    DevBuf bank, scales, periods, cum, cum32, hist, parts, keys, tflags, records, score, depth, rflags;
-    DevBuf evidence, chunks, fault;
+    DevBuf cum, cum32, hist, parts, keys, tflags;  // per launch
+    DevBuf pass_in, pass_out;  // per session: every pass's inputs and outputs
+    DevBuf evidence, fault;
     DevBuf family;  // observations of the star a batch worker is searching
-    std::vector<int> host_chunks;
+    PinBuf pin_up, pin_down, pin_down2;  // staging of a session's upload and download (two sessions in flight)
     std::vector<fbls_ctx*> workers;  // fbls_search_batch worker contexts, kept for reuse
 };
 
@@ -171,241 +179,14 @@ double fold_budget_mib(double configured) {
     return configured < cap ? configured : cap;
 }
 
+// A pass's outputs, read in place from its session's page-locked download
+// buffer (valid until that buffer serves another session).
 struct BandOut {
-    std::vector<double> records;  // P x 9
-    std::vector<double> score;
-    std::vector<double> depth;
-    std::vector<uint32_t> flags;
+    const double* records = nullptr;  // P x 9
+    const double* score = nullptr;
+    const double* depth = nullptr;
+    const uint32_t* flags = nullptr;
 };
-
-// Fold shape for a launch of up to `periods` periods at nb bins, and the
-// family's fold chunks for scales up to scale_max, uploaded to the device.
-int plan_fold(fbls_ctx* ctx, const fbls_ready* r, double scale_max, int nb, int periods, FoldShape* shape,
-              int* nchunks) {
-    *shape = fold_group_shape(nb, periods, ctx->sm_count);
-    std::vector<int>& h = ctx->host_chunks;
-    h.resize((size_t)r->n + 2);
-    const int count = fold_chunks(r->time_host.data(), (int)r->n, scale_max, nb, shape->span_cap, shape->chunk_cap,
-                                  h.data(), (int)h.size());
-    if (count < 1) return fail(ctx, FBLS_ERR_ARGUMENT, "fold chunking failed");
-    CK(ensure(ctx->chunks, ((size_t)count + 1) * sizeof(int)), "workspace");
-    CK(cudaMemcpyAsync(ctx->chunks.ptr, h.data(), ((size_t)count + 1) * sizeof(int), cudaMemcpyHostToDevice,
-                       ctx->stream),
-       "upload chunks");
-    *nchunks = count;
-    return FBLS_OK;
-}
-
-// One scan_bank pass (scan.rs:144-357) of `periods` at nb bins.
-int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_t P, const fbls_bank* bank, uint32_t nb,
-              bool mixed, BandOut& out, fbls_scan_stats* stats) {
-    const uint32_t nd = bank->nd, ns = bank->ns, layers = bank->layers;
-    if (stats) stats->phase_bins = nb;
-    if (nd == 0 || nd > (uint32_t)MAX_DURATIONS || ns == 0 || ns > (uint32_t)MAX_SHAPES || layers == 0 ||
-        layers > (uint32_t)MAX_LAYERS)
-        return fail(ctx, FBLS_ERR_ARGUMENT, "bank size outside the supported range");
-    if (nb < 2) return fail(ctx, FBLS_ERR_ARGUMENT, "nb must be at least 2");
-    // Shape factors 1 - 2 ing l / (L - 1) (scan.rs:157-171).
-    std::vector<double> host_bank;
-    host_bank.insert(host_bank.end(), bank->durations, bank->durations + nd);
-    host_bank.insert(host_bank.end(), bank->rho, bank->rho + nd);
-    host_bank.insert(host_bank.end(), bank->ingress, bank->ingress + ns);
-    for (uint32_t s = 0; s < ns; s++)
-        for (uint32_t l = 0; l < layers; l++)
-            host_bank.push_back(1.0 - 2.0 * bank->ingress[s] * (layers > 1 ? (double)l / (double)(layers - 1) : 0.0));
-    const uint32_t tiles = (nb + TILE - 1) / TILE;
-    const double per_period_bytes = (double)(NF * (4 * (size_t)nb + 2) * 8 + NF * (2 * (size_t)nb + 1) * 8);
-    const uint64_t budget = (uint64_t)std::floor((bank->max_fold_mib * 1048576.0) / per_period_bytes);
-    if (budget == 0) return fail(ctx, FBLS_ERR_BUDGET, "one folded period exceeds max_fold_mib");
-    uint64_t batch = bank->period_batch;
-    if (budget < batch) batch = budget;
-    if (P < batch) batch = P;
-    if (batch == 0) batch = 1;
-    // The phase cell floor(t * scale) must fit u32 (kernels.rs:315), with room
-    // for the fold's cell arithmetic (cell + 2 nb).
-    double scale_max = 0.0;
-    std::vector<double> scales(P);
-    for (uint32_t i = 0; i < P; i++) {
-        scales[i] = (double)nb / periods[i];
-        if (!(scales[i] > 0.0) || !std::isfinite(scales[i]))
-            return fail(ctx, FBLS_ERR_ARGUMENT, "periods must be positive and finite");
-        if (scales[i] > scale_max) scale_max = scales[i];
-    }
-    if (std::floor(r->t_last * scale_max) >= 4294967295.0 - 2.0 * (double)nb - 2.0)
-        return fail(ctx, FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
-
-    const size_t stride = 2 * (size_t)nb + 1;
-    // Periods per launch: whole batches of the reference's size, as many as
-    // the fold budget holds in this path's buffers (cum, cum32 and tile parts;
-    // the histograms never reach device memory), up to 16,384, so bands with
-    // few bins fill the GPU with larger period groups. Statistics still count
-    // the reference's batches.
-    const double launch_period_bytes =
-        (double)(NF * stride * (sizeof(double) + sizeof(float2)) +
-                 tiles * (PART_STRIDE * sizeof(double) + sizeof(uint64_t) + sizeof(uint32_t)));
-    uint64_t launch = (uint64_t)std::floor(bank->max_fold_mib * 1048576.0 / launch_period_bytes);
-    launch = std::min<uint64_t>(launch, 16384);
-    launch = std::max<uint64_t>(launch / batch, 1) * batch;
-    if (launch > P) launch = P;
-    CK(ensure(ctx->bank, host_bank.size() * sizeof(double)), "workspace");
-    CK(ensure(ctx->scales, (size_t)P * sizeof(double)), "workspace");
-    CK(ensure(ctx->periods, (size_t)P * sizeof(double)), "workspace");
-    CK(ensure(ctx->cum, launch * NF * stride * sizeof(double)), "workspace");
-    CK(ensure(ctx->cum32, launch * NF * stride * sizeof(float2)), "workspace");
-    CK(ensure(ctx->parts, launch * tiles * PART_STRIDE * sizeof(double)), "workspace");
-    CK(ensure(ctx->keys, launch * tiles * sizeof(uint64_t)), "workspace");
-    CK(ensure(ctx->tflags, launch * tiles * sizeof(uint32_t)), "workspace");
-    CK(ensure(ctx->records, (size_t)P * RECORD_STRIDE * sizeof(double)), "workspace");
-    CK(ensure(ctx->score, (size_t)P * sizeof(double)), "workspace");
-    CK(ensure(ctx->depth, (size_t)P * sizeof(double)), "workspace");
-    CK(ensure(ctx->rflags, (size_t)P * sizeof(uint32_t)), "workspace");
-    CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
-    FoldShape shape;
-    int nchunks = 0;
-    {
-        int rc = plan_fold(ctx, r, scale_max, (int)nb, (int)launch, &shape, &nchunks);
-        if (rc) return rc;
-    }
-    if (!shape.hist_in_smem) {
-        const size_t blocks = (launch + shape.group - 1) / shape.group;
-        CK(ensure(ctx->hist, blocks * shape.group * NF * (size_t)shape.row_stride * sizeof(double)), "workspace");
-    }
-
-    cudaStream_t s = ctx->stream;
-    CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
-    CK(cudaMemcpyAsync(ctx->bank.ptr, host_bank.data(), host_bank.size() * sizeof(double), cudaMemcpyHostToDevice, s),
-       "upload bank");
-    CK(cudaMemcpyAsync(ctx->scales.ptr, scales.data(), (size_t)P * sizeof(double), cudaMemcpyHostToDevice, s),
-       "upload scales");
-    CK(cudaMemcpyAsync(ctx->periods.ptr, periods, (size_t)P * sizeof(double), cudaMemcpyHostToDevice, s),
-       "upload periods");
-    const double* d_bank = as<double>(ctx->bank);
-
-    const bool timing = ctx->profile || ctx->kernel_timing;
-    const uint64_t nbatches = (P + launch - 1) / launch;
-    if (timing) {
-        while (ctx->pool.size() < 3 * nbatches) {
-            cudaEvent_t e;
-            CK(cudaEventCreate(&e), "event");
-            ctx->pool.push_back(e);
-        }
-    }
-    uint64_t bi = 0;
-    for (uint64_t cursor = 0; cursor < P; cursor += launch, bi++) {
-        const int p = (int)((P - cursor) < launch ? (P - cursor) : launch);
-        FoldArgs fa;
-        fa.time = r->time;
-        fa.v = r->v;
-        fa.w = r->w;
-        fa.scales = as<double>(ctx->scales) + cursor;
-        fa.n = (int)r->n;
-        fa.nb = (int)nb;
-        fa.periods = p;
-        fa.group = 1;
-        fa.cum = as<double>(ctx->cum);
-        fa.cum32 = as<float2>(ctx->cum32);
-        if (timing) CK(cudaEventRecord(ctx->pool[3 * bi], s), "event");
-        fa.group = shape.group;
-        fa.hist_global = shape.hist_in_smem ? nullptr : as<double>(ctx->hist);
-        fa.hist_out = nullptr;
-        fa.chunks = as<int>(ctx->chunks);
-        fa.nchunks = nchunks;
-        fa.stage_field = shape.stage_field;
-        fa.window = shape.window;
-        fa.row_stride = shape.row_stride;
-        fa.fault = as<uint32_t>(ctx->fault);
-        CK(launch_fold(fa, shape, s), "fold");
-        ctx->counters.launches += 1;
-        ctx->counters.fold_launches += 1;
-        ctx->counters.fold_bytes += (double)p * (24.0 * r->n + 48.0 * (double)stride);
-        ctx->counters.fold_updates += (uint64_t)p * r->n;
-        if (timing) CK(cudaEventRecord(ctx->pool[3 * bi + 1], s), "event");
-        ScanArgs sa;
-        sa.cum = as<double>(ctx->cum);
-        sa.cum32 = as<float2>(ctx->cum32);
-        sa.scales = fa.scales;
-        sa.durations = d_bank;
-        sa.rho = d_bank + nd;
-        sa.ingress = d_bank + 2 * nd;
-        sa.factors = d_bank + 2 * nd + ns;
-        sa.baseline = r->baseline_norm;
-        sa.gate = bank->shape_gate;
-        sa.n = (double)r->n;
-        sa.nb = (int)nb;
-        sa.nd = (int)nd;
-        sa.ns = (int)ns;
-        sa.layers = (int)layers;
-        sa.mixed = mixed ? 1 : 0;
-        sa.parts = as<double>(ctx->parts);
-        sa.keys = as<uint64_t>(ctx->keys);
-        sa.flags = as<uint32_t>(ctx->tflags);
-        CK(launch_scan_tiles(sa, p, s), "scan_tiles");
-        MergeArgs ma;
-        ma.parts = sa.parts;
-        ma.keys = sa.keys;
-        ma.flags = sa.flags;
-        ma.periods_in = as<double>(ctx->periods) + cursor;
-        ma.scales = fa.scales;
-        ma.periods = p;
-        ma.tiles = (int)tiles;
-        ma.offset = (int)cursor;
-        ma.records = as<double>(ctx->records);
-        ma.score = as<double>(ctx->score);
-        ma.depth = as<double>(ctx->depth);
-        ma.flags_out = as<uint32_t>(ctx->rflags);
-        CK(launch_merge(ma, s), "merge");
-        if (timing) CK(cudaEventRecord(ctx->pool[3 * bi + 2], s), "event");
-        ctx->counters.launches += 2;
-        ctx->counters.scan_launches += 1;
-        ctx->counters.scan_bytes += (double)p * (24.0 * (double)stride + 84.0 * tiles);
-        if (stats) {
-            stats->templates_scanned += (uint64_t)p * nd * ns * nb;
-            stats->batches += ((uint64_t)p + batch - 1) / batch;
-        }
-    }
-    out.records.resize((size_t)P * RECORD_STRIDE);
-    out.score.resize(P);
-    out.depth.resize(P);
-    out.flags.resize(P);
-    CK(cudaMemcpyAsync(out.records.data(), ctx->records.ptr, out.records.size() * sizeof(double),
-                       cudaMemcpyDeviceToHost, s),
-       "download records");
-    CK(cudaMemcpyAsync(out.score.data(), ctx->score.ptr, P * sizeof(double), cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaMemcpyAsync(out.depth.data(), ctx->depth.ptr, P * sizeof(double), cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaMemcpyAsync(out.flags.data(), ctx->rflags.ptr, P * sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
-       "download");
-    uint32_t fault = 0;
-    CK(cudaMemcpyAsync(&fault, ctx->fault.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaStreamSynchronize(s), "scan_bank");
-    if (fault) return fail(ctx, FBLS_ERR_CUDA, "fold: staging copies did not complete");
-    double t_fold = 0.0, t_scan = 0.0;
-    if (timing) {
-        for (uint64_t b = 0; b < nbatches; b++) {
-            float a = 0.f, c = 0.f;
-            CK(cudaEventElapsedTime(&a, ctx->pool[3 * b], ctx->pool[3 * b + 1]), "event");
-            CK(cudaEventElapsedTime(&c, ctx->pool[3 * b + 1], ctx->pool[3 * b + 2]), "event");
-            t_fold += a;
-            t_scan += c;
-        }
-        ctx->counters.fold_ms += t_fold;
-        ctx->counters.scan_ms += t_scan;
-    }
-    uint64_t rescans = 0, retries = 0;
-    bool bad = false;
-    for (uint32_t i = 0; i < P; i++) {
-        bad = bad || (out.flags[i] & 2u);
-        retries += (out.flags[i] & 1u) ? 1 : 0;
-        rescans += (out.flags[i] & 4u) ? 1 : 0;
-    }
-    if (stats) {
-        stats->exact_tile_retries += retries;
-        stats->tile_rescans += rescans;
-        stats->seconds_fold += t_fold * 1e-3;
-        stats->seconds_scan += t_scan * 1e-3;
-    }
-    if (bad) return fail(ctx, FBLS_ERR_PRECISION, "nonpositive template precision; inspect noise model");
-    return FBLS_OK;
-}
 
 double now_seconds() {
     timespec ts;
@@ -413,54 +194,436 @@ double now_seconds() {
     return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
 }
 
-// scan_periods (scan.rs:363-408). Rows are appended to `rows`.
-int scan_periods(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_t P, const fbls_bank* bank,
-                 bool mixed, std::vector<fbls_row>& rows, fbls_scan_stats* stats) {
-    const double start = now_seconds();
-    fbls_scan_stats st;
-    std::memset(&st, 0, sizeof(st));
-    st.periods = P;
-    if (P == 0 || bank->nd == 0) {
-        if (stats) *stats = st;
-        return FBLS_OK;
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+cudaError_t ensure_pinned(PinBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 256;
+    if (b.bytes >= bytes) return cudaSuccess;
+    if (b.ptr) {
+        cudaError_t e = cudaFreeHost(b.ptr);
+        if (e != cudaSuccess) return e;
+        b.ptr = nullptr;
+        b.bytes = 0;
     }
-    double dmin = __builtin_huge_val();
-    for (uint32_t i = 0; i < bank->nd; i++) dmin = rmin(dmin, bank->durations[i]);
-    uint64_t nb = as_u64(std::ceil((double)bank->phase_oversample * periods[P - 1] / dmin));
-    if (nb < 8) nb = 8;
-    if (nb > (1u << 24)) return fail(ctx, FBLS_ERR_ARGUMENT, "phase grid too large");
-    std::vector<double> survivors(periods, periods + P);
-    BandOut band;
-    if (bank->prescan_factor > 1 && nb / bank->prescan_factor >= 8) {
-        int rc = scan_bank(ctx, r, periods, P, bank, (uint32_t)(nb / bank->prescan_factor), mixed, band, &st);
-        if (rc) return rc;
-        survivors.clear();
-        const double cut = bank->prescan_fraction * bank->threshold;
-        for (uint32_t i = 0; i < P; i++) {
-            double sc = band.score[i];
-            if (std::isfinite(sc) && sc >= cut) survivors.push_back(band.records[(size_t)i * RECORD_STRIDE]);
+    size_t want = bytes + bytes / 4;
+    cudaError_t e = cudaHostAlloc(&b.ptr, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) return e;
+    b.bytes = want;
+    return cudaSuccess;
+}
+
+// One scan_bank pass (scan.rs:144-357): every period's best template at nb
+// bins. Planned on the host, then enqueued with the other passes of a session.
+struct Pass {
+    const double* periods = nullptr;
+    uint32_t P = 0;
+    const fbls_bank* bank = nullptr;
+    uint32_t nb = 0;
+    bool mixed = true;
+    // plan
+    uint64_t batch = 0, launch = 0;
+    FoldShape shape{};
+    std::vector<double> scales, host_bank;
+    std::vector<int> chunks;
+    size_t in_off = 0, in_scales = 0, in_periods = 0, in_bank = 0, in_chunks = 0, in_bytes = 0;
+    size_t out_off = 0, out_score = 0, out_depth = 0, out_flags = 0, out_bytes = 0;
+    size_t ev0 = 0, nlaunch = 0;
+    BandOut out;
+    fbls_scan_stats st{};
+};
+
+// Checks a pass and plans its batches, launches, fold shape and chunks
+// (scan.rs:144-199 for the bank factors, the budget and the batch size).
+int plan_pass(fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
+    const fbls_bank* bank = p.bank;
+    const uint32_t nd = bank->nd, ns = bank->ns, layers = bank->layers, nb = p.nb;
+    std::memset(&p.st, 0, sizeof(p.st));
+    p.st.phase_bins = nb;
+    p.st.periods = p.P;
+    if (nd == 0 || nd > (uint32_t)MAX_DURATIONS || ns == 0 || ns > (uint32_t)MAX_SHAPES || layers == 0 ||
+        layers > (uint32_t)MAX_LAYERS)
+        return fail(ctx, FBLS_ERR_ARGUMENT, "bank size outside the supported range");
+    if (nb < 2) return fail(ctx, FBLS_ERR_ARGUMENT, "nb must be at least 2");
+    // Shape factors 1 - 2 ing l / (L - 1) (scan.rs:157-171).
+    p.host_bank.assign(bank->durations, bank->durations + nd);
+    p.host_bank.insert(p.host_bank.end(), bank->rho, bank->rho + nd);
+    p.host_bank.insert(p.host_bank.end(), bank->ingress, bank->ingress + ns);
+    for (uint32_t s = 0; s < ns; s++)
+        for (uint32_t l = 0; l < layers; l++)
+            p.host_bank.push_back(1.0 - 2.0 * bank->ingress[s] *
+                                            (layers > 1 ? (double)l / (double)(layers - 1) : 0.0));
+    const uint32_t tiles = (nb + TILE - 1) / TILE;
+    const double per_period_bytes = (double)(NF * (4 * (size_t)nb + 2) * 8 + NF * (2 * (size_t)nb + 1) * 8);
+    const uint64_t budget = (uint64_t)std::floor((bank->max_fold_mib * 1048576.0) / per_period_bytes);
+    if (budget == 0) return fail(ctx, FBLS_ERR_BUDGET, "one folded period exceeds max_fold_mib");
+    uint64_t batch = bank->period_batch;
+    if (budget < batch) batch = budget;
+    if (p.P < batch) batch = p.P;
+    if (batch == 0) batch = 1;
+    // The phase cell floor(t * scale) must fit u32 (kernels.rs:315), with room
+    // for the fold's cell arithmetic (cell + 2 nb).
+    double scale_max = 0.0;
+    p.scales.resize(p.P);
+    for (uint32_t i = 0; i < p.P; i++) {
+        p.scales[i] = (double)nb / p.periods[i];
+        if (!(p.scales[i] > 0.0) || !std::isfinite(p.scales[i]))
+            return fail(ctx, FBLS_ERR_ARGUMENT, "periods must be positive and finite");
+        if (p.scales[i] > scale_max) scale_max = p.scales[i];
+    }
+    if (std::floor(r->t_last * scale_max) >= 4294967295.0 - 2.0 * (double)nb - 2.0)
+        return fail(ctx, FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
+    // Periods per launch: whole batches of the reference's size, as many as
+    // the fold budget holds in this path's buffers (cum, cum32 and tile parts;
+    // the histograms never reach device memory), up to 16,384, so bands with
+    // few bins fill the GPU with larger period groups. Statistics still count
+    // the reference's batches.
+    const size_t stride = 2 * (size_t)nb + 1;
+    const double launch_period_bytes =
+        (double)(NF * stride * (sizeof(double) + sizeof(float2)) +
+                 tiles * (PART_STRIDE * sizeof(double) + sizeof(uint64_t) + sizeof(uint32_t)));
+    uint64_t launch = (uint64_t)std::floor(bank->max_fold_mib * 1048576.0 / launch_period_bytes);
+    launch = std::min<uint64_t>(launch, 16384);
+    launch = std::max<uint64_t>(launch / batch, 1) * batch;
+    if (launch > p.P) launch = p.P;
+    p.batch = batch;
+    p.launch = launch;
+    p.shape = fold_group_shape((int)nb, (int)launch, ctx->sm_count);
+    p.chunks.resize((size_t)r->n + 2);
+    const int count = fold_chunks(r->time_host.data(), (int)r->n, scale_max, (int)nb, p.shape.span_cap,
+                                  p.shape.chunk_cap, p.chunks.data(), (int)p.chunks.size());
+    if (count < 1) return fail(ctx, FBLS_ERR_ARGUMENT, "fold chunking failed");
+    p.chunks.resize((size_t)count + 1);
+    // Device input region: scales | periods | bank | chunks; output region:
+    // records | score | depth | flags.
+    p.in_scales = 0;
+    p.in_periods = align256(p.P * sizeof(double));
+    p.in_bank = p.in_periods + align256(p.P * sizeof(double));
+    p.in_chunks = p.in_bank + align256(p.host_bank.size() * sizeof(double));
+    p.in_bytes = p.in_chunks + align256(p.chunks.size() * sizeof(int));
+    p.out_score = align256((size_t)p.P * RECORD_STRIDE * sizeof(double));
+    p.out_depth = p.out_score + align256(p.P * sizeof(double));
+    p.out_flags = p.out_depth + align256(p.P * sizeof(double));
+    p.out_bytes = p.out_flags + align256(p.P * sizeof(uint32_t));
+    p.nlaunch = (p.P + launch - 1) / launch;
+    return FBLS_OK;
+}
+
+// Runs a session of planned passes on ctx->stream: one upload of every
+// pass's inputs from page-locked memory, the fold / scan / merge launches of
+// all passes back to back, one download of all outputs into `down` and a
+// single synchronisation.
+int run_session(fbls_ctx* ctx, const fbls_ready* r, std::vector<Pass>& passes, PinBuf& down_buf) {
+    if (passes.empty()) return FBLS_OK;
+    size_t in_total = 0, out_total = 0, launches = 0;
+    size_t cum_max = 0, parts_max = 0, hist_max = 0;
+    for (Pass& p : passes) {
+        p.in_off = in_total;
+        in_total += p.in_bytes;
+        p.out_off = out_total;
+        out_total += p.out_bytes;
+        p.ev0 = launches;
+        launches += p.nlaunch;
+        const size_t stride = 2 * (size_t)p.nb + 1;
+        const size_t tiles = (p.nb + TILE - 1) / TILE;
+        cum_max = std::max(cum_max, (size_t)p.launch * NF * stride);
+        parts_max = std::max(parts_max, (size_t)p.launch * tiles);
+        if (!p.shape.hist_in_smem) {
+            const size_t blocks = (p.launch + p.shape.group - 1) / p.shape.group;
+            hist_max = std::max(hist_max, blocks * p.shape.group * NF * (size_t)p.shape.row_stride);
         }
-        st.prescan_survivors = survivors.size();
     }
-    if (!survivors.empty()) {
-        int rc = scan_bank(ctx, r, survivors.data(), (uint32_t)survivors.size(), bank, (uint32_t)nb, mixed, band, &st);
+    CK(ensure(ctx->pass_in, in_total), "workspace");
+    CK(ensure(ctx->pass_out, out_total), "workspace");
+    CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
+    CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
+    CK(ensure(ctx->parts, parts_max * PART_STRIDE * sizeof(double)), "workspace");
+    CK(ensure(ctx->keys, parts_max * sizeof(uint64_t)), "workspace");
+    CK(ensure(ctx->tflags, parts_max * sizeof(uint32_t)), "workspace");
+    if (hist_max) CK(ensure(ctx->hist, hist_max * sizeof(double)), "workspace");
+    CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
+    CK(ensure_pinned(ctx->pin_up, in_total), "pinned workspace");
+    CK(ensure_pinned(down_buf, out_total + 256), "pinned workspace");
+    const bool timing = ctx->profile || ctx->kernel_timing;
+    if (timing) {
+        while (ctx->pool.size() < 3 * launches) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e), "event");
+            ctx->pool.push_back(e);
+        }
+    }
+    unsigned char* up = static_cast<unsigned char*>(ctx->pin_up.ptr);
+    for (Pass& p : passes) {
+        unsigned char* b = up + p.in_off;
+        std::memcpy(b + p.in_scales, p.scales.data(), p.P * sizeof(double));
+        std::memcpy(b + p.in_periods, p.periods, p.P * sizeof(double));
+        std::memcpy(b + p.in_bank, p.host_bank.data(), p.host_bank.size() * sizeof(double));
+        std::memcpy(b + p.in_chunks, p.chunks.data(), p.chunks.size() * sizeof(int));
+    }
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
+    CK(cudaMemcpyAsync(ctx->pass_in.ptr, up, in_total, cudaMemcpyHostToDevice, s), "upload");
+    unsigned char* din = static_cast<unsigned char*>(ctx->pass_in.ptr);
+    unsigned char* dout = static_cast<unsigned char*>(ctx->pass_out.ptr);
+    for (Pass& p : passes) {
+        const uint32_t nb = p.nb, nd = p.bank->nd, ns = p.bank->ns, layers = p.bank->layers;
+        const uint32_t tiles = (nb + TILE - 1) / TILE;
+        const size_t stride = 2 * (size_t)nb + 1;
+        const double* d_scales = reinterpret_cast<const double*>(din + p.in_off + p.in_scales);
+        const double* d_periods = reinterpret_cast<const double*>(din + p.in_off + p.in_periods);
+        const double* d_bank = reinterpret_cast<const double*>(din + p.in_off + p.in_bank);
+        const int* d_chunks = reinterpret_cast<const int*>(din + p.in_off + p.in_chunks);
+        double* d_records = reinterpret_cast<double*>(dout + p.out_off);
+        double* d_score = reinterpret_cast<double*>(dout + p.out_off + p.out_score);
+        double* d_depth = reinterpret_cast<double*>(dout + p.out_off + p.out_depth);
+        uint32_t* d_flags = reinterpret_cast<uint32_t*>(dout + p.out_off + p.out_flags);
+        size_t li = p.ev0;
+        for (uint64_t cursor = 0; cursor < p.P; cursor += p.launch, li++) {
+            const int n = (int)std::min<uint64_t>(p.P - cursor, p.launch);
+            FoldArgs fa{};
+            fa.time = r->time;
+            fa.v = r->v;
+            fa.w = r->w;
+            fa.scales = d_scales + cursor;
+            fa.n = (int)r->n;
+            fa.nb = (int)nb;
+            fa.periods = n;
+            fa.group = p.shape.group;
+            fa.cum = as<double>(ctx->cum);
+            fa.cum32 = as<float2>(ctx->cum32);
+            fa.hist_global = p.shape.hist_in_smem ? nullptr : as<double>(ctx->hist);
+            fa.hist_out = nullptr;
+            fa.chunks = d_chunks;
+            fa.nchunks = (int)p.chunks.size() - 1;
+            fa.stage_field = p.shape.stage_field;
+            fa.window = p.shape.window;
+            fa.row_stride = p.shape.row_stride;
+            fa.fault = as<uint32_t>(ctx->fault);
+            if (timing) CK(cudaEventRecord(ctx->pool[3 * li], s), "event");
+            CK(launch_fold(fa, p.shape, s), "fold");
+            if (timing) CK(cudaEventRecord(ctx->pool[3 * li + 1], s), "event");
+            ScanArgs sa{};
+            sa.cum = fa.cum;
+            sa.cum32 = fa.cum32;
+            sa.scales = fa.scales;
+            sa.durations = d_bank;
+            sa.rho = d_bank + nd;
+            sa.ingress = d_bank + 2 * nd;
+            sa.factors = d_bank + 2 * nd + ns;
+            sa.baseline = r->baseline_norm;
+            sa.gate = p.bank->shape_gate;
+            sa.n = (double)r->n;
+            sa.nb = (int)nb;
+            sa.nd = (int)nd;
+            sa.ns = (int)ns;
+            sa.layers = (int)layers;
+            sa.mixed = p.mixed ? 1 : 0;
+            sa.parts = as<double>(ctx->parts);
+            sa.keys = as<uint64_t>(ctx->keys);
+            sa.flags = as<uint32_t>(ctx->tflags);
+            CK(launch_scan_tiles(sa, n, s), "scan_tiles");
+            MergeArgs ma{};
+            ma.parts = sa.parts;
+            ma.keys = sa.keys;
+            ma.flags = sa.flags;
+            ma.periods_in = d_periods + cursor;
+            ma.scales = fa.scales;
+            ma.periods = n;
+            ma.tiles = (int)tiles;
+            ma.offset = (int)cursor;
+            ma.records = d_records;
+            ma.score = d_score;
+            ma.depth = d_depth;
+            ma.flags_out = d_flags;
+            CK(launch_merge(ma, s), "merge");
+            if (timing) CK(cudaEventRecord(ctx->pool[3 * li + 2], s), "event");
+            ctx->counters.launches += 3;
+            ctx->counters.fold_launches += 1;
+            ctx->counters.scan_launches += 1;
+            ctx->counters.fold_bytes += (double)n * (24.0 * r->n + 48.0 * (double)stride);
+            ctx->counters.fold_updates += (uint64_t)n * r->n;
+            ctx->counters.scan_bytes += (double)n * (24.0 * (double)stride + 84.0 * tiles);
+            p.st.templates_scanned += (uint64_t)n * nd * ns * nb;
+            p.st.batches += ((uint64_t)n + p.batch - 1) / p.batch;
+        }
+    }
+    unsigned char* down = static_cast<unsigned char*>(down_buf.ptr);
+    CK(cudaMemcpyAsync(down, dout, out_total, cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaMemcpyAsync(down + out_total, ctx->fault.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaStreamSynchronize(s), "scan_bank");
+    uint32_t fault = 0;
+    std::memcpy(&fault, down + out_total, sizeof(uint32_t));
+    if (fault) return fail(ctx, FBLS_ERR_CUDA, "fold: staging copies did not complete");
+    bool bad = false;
+    for (Pass& p : passes) {
+        const unsigned char* b = down + p.out_off;
+        p.out.records = reinterpret_cast<const double*>(b);
+        p.out.score = reinterpret_cast<const double*>(b + p.out_score);
+        p.out.depth = reinterpret_cast<const double*>(b + p.out_depth);
+        p.out.flags = reinterpret_cast<const uint32_t*>(b + p.out_flags);
+        if (timing) {
+            double t_fold = 0.0, t_scan = 0.0;
+            for (size_t li = p.ev0; li < p.ev0 + p.nlaunch; li++) {
+                float a = 0.f, c = 0.f;
+                CK(cudaEventElapsedTime(&a, ctx->pool[3 * li], ctx->pool[3 * li + 1]), "event");
+                CK(cudaEventElapsedTime(&c, ctx->pool[3 * li + 1], ctx->pool[3 * li + 2]), "event");
+                t_fold += a;
+                t_scan += c;
+            }
+            ctx->counters.fold_ms += t_fold;
+            ctx->counters.scan_ms += t_scan;
+            p.st.seconds_fold += t_fold * 1e-3;
+            p.st.seconds_scan += t_scan * 1e-3;
+        }
+        for (uint32_t i = 0; i < p.P; i++) {
+            bad = bad || (p.out.flags[i] & 2u);
+            p.st.exact_tile_retries += (p.out.flags[i] & 1u) ? 1 : 0;
+            p.st.tile_rescans += (p.out.flags[i] & 4u) ? 1 : 0;
+        }
+    }
+    if (bad) return fail(ctx, FBLS_ERR_PRECISION, "nonpositive template precision; inspect noise model");
+    return FBLS_OK;
+}
+
+void add_pass_stats(fbls_scan_stats& st, const Pass& p) {
+    st.phase_bins = p.st.phase_bins;
+    st.batches += p.st.batches;
+    st.templates_scanned += p.st.templates_scanned;
+    st.exact_tile_retries += p.st.exact_tile_retries;
+    st.tile_rescans += p.st.tile_rescans;
+    st.seconds_fold += p.st.seconds_fold;
+    st.seconds_scan += p.st.seconds_scan;
+}
+
+// One scan_bank pass on its own (fbls_scan_bank).
+int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_t P, const fbls_bank* bank, uint32_t nb,
+              bool mixed, BandOut& out, fbls_scan_stats* stats) {
+    std::vector<Pass> passes(1);
+    Pass& p = passes[0];
+    p.periods = periods;
+    p.P = P;
+    p.bank = bank;
+    p.nb = nb;
+    p.mixed = mixed;
+    int rc = plan_pass(ctx, r, p);
+    if (rc == FBLS_OK) rc = run_session(ctx, r, passes, ctx->pin_down);
+    out = p.out;
+    if (stats) add_pass_stats(*stats, p);
+    return rc;
+}
+
+// scan_periods (scan.rs:363-408) of several bands at once: the first pass of
+// every band (its coarse prescan, or its full scan when there is none) in one
+// session, then the full scans of every band's survivors in a second one.
+// Rows are appended band after band; each band's stats get its passes'
+// counts and a share of the two sessions' wall time by templates scanned.
+struct BandJob {
+    const double* periods = nullptr;
+    uint32_t P = 0;
+    const fbls_bank* bank = nullptr;
+    fbls_scan_stats st{};
+    uint64_t nb = 0;
+    bool coarse = false;
+    std::vector<double> survivors;
+    int first = -1, second = -1;  // pass indices
+};
+
+int scan_bands(fbls_ctx* ctx, const fbls_ready* r, std::vector<BandJob>& jobs, bool mixed,
+               std::vector<fbls_row>& rows) {
+    std::vector<Pass> first, second;
+    for (BandJob& j : jobs) {
+        std::memset(&j.st, 0, sizeof(j.st));
+        j.st.periods = j.P;
+        if (j.P == 0 || j.bank->nd == 0) continue;
+        double dmin = __builtin_huge_val();
+        for (uint32_t i = 0; i < j.bank->nd; i++) dmin = rmin(dmin, j.bank->durations[i]);
+        j.nb = as_u64(std::ceil((double)j.bank->phase_oversample * j.periods[j.P - 1] / dmin));
+        if (j.nb < 8) j.nb = 8;
+        if (j.nb > (1u << 24)) return fail(ctx, FBLS_ERR_ARGUMENT, "phase grid too large");
+        j.coarse = j.bank->prescan_factor > 1 && j.nb / j.bank->prescan_factor >= 8;
+        Pass p;
+        p.periods = j.periods;
+        p.P = j.P;
+        p.bank = j.bank;
+        p.nb = (uint32_t)(j.coarse ? j.nb / j.bank->prescan_factor : j.nb);
+        p.mixed = mixed;
+        int rc = plan_pass(ctx, r, p);
         if (rc) return rc;
-        for (size_t i = 0; i < survivors.size(); i++) {
-            double sc = band.score[i];
-            if (!(std::isfinite(sc) && sc >= bank->threshold)) continue;
-            const double* rec = &band.records[i * RECORD_STRIDE];
+        j.first = (int)first.size();
+        first.push_back(std::move(p));
+    }
+    const double t0 = now_seconds();
+    int rc = run_session(ctx, r, first, ctx->pin_down);
+    if (rc) return rc;
+    const double t1 = now_seconds();
+    for (BandJob& j : jobs) {
+        if (j.first < 0) continue;
+        add_pass_stats(j.st, first[j.first]);
+        if (!j.coarse) continue;
+        const BandOut& band = first[j.first].out;
+        const double cut = j.bank->prescan_fraction * j.bank->threshold;
+        for (uint32_t i = 0; i < j.P; i++) {
+            const double sc = band.score[i];
+            if (std::isfinite(sc) && sc >= cut) j.survivors.push_back(band.records[(size_t)i * RECORD_STRIDE]);
+        }
+        j.st.prescan_survivors = j.survivors.size();
+        if (j.survivors.empty()) continue;
+        Pass p;
+        p.periods = j.survivors.data();
+        p.P = (uint32_t)j.survivors.size();
+        p.bank = j.bank;
+        p.nb = (uint32_t)j.nb;
+        p.mixed = mixed;
+        rc = plan_pass(ctx, r, p);
+        if (rc) return rc;
+        j.second = (int)second.size();
+        second.push_back(std::move(p));
+    }
+    rc = run_session(ctx, r, second, ctx->pin_down2);
+    if (rc) return rc;
+    const double t2 = now_seconds();
+    uint64_t tmpl_first = 0, tmpl_second = 0;
+    for (const Pass& p : first) tmpl_first += p.st.templates_scanned;
+    for (const Pass& p : second) tmpl_second += p.st.templates_scanned;
+    for (BandJob& j : jobs) {
+        if (j.first < 0) continue;
+        j.st.seconds =
+            (t1 - t0) * (double)first[j.first].st.templates_scanned / (double)std::max<uint64_t>(tmpl_first, 1);
+        const Pass* full = nullptr;
+        if (!j.coarse) {
+            full = &first[j.first];
+        } else if (j.second >= 0) {
+            full = &second[j.second];
+            add_pass_stats(j.st, *full);
+            j.st.seconds +=
+                (t2 - t1) * (double)full->st.templates_scanned / (double)std::max<uint64_t>(tmpl_second, 1);
+        }
+        if (!full) continue;
+        for (uint32_t i = 0; i < full->P; i++) {
+            const double sc = full->out.score[i];
+            if (!(std::isfinite(sc) && sc >= j.bank->threshold)) continue;
+            const double* rec = &full->out.records[(size_t)i * RECORD_STRIDE];
             fbls_row row;
             row.period = rec[0];
             row.epoch = (rec[2] + rec[3] / 2.0) / rec[1] + r->origin;
             row.duration = rec[3] / rec[1];
             row.score = sc;
-            row.depth = band.depth[i];
+            row.depth = full->out.depth[i];
             rows.push_back(row);
         }
     }
-    st.seconds = now_seconds() - start;
-    if (stats) *stats = st;
     return FBLS_OK;
+}
+
+// scan_periods (scan.rs:363-408). Rows are appended to `rows`.
+int scan_periods(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_t P, const fbls_bank* bank,
+                 bool mixed, std::vector<fbls_row>& rows, fbls_scan_stats* stats) {
+    std::vector<BandJob> jobs(1);
+    jobs[0].periods = periods;
+    jobs[0].P = P;
+    jobs[0].bank = bank;
+    int rc = scan_bands(ctx, r, jobs, mixed, rows);
+    if (stats) *stats = jobs[0].st;
+    return rc;
 }
 
 }  // namespace
@@ -495,10 +658,11 @@ void fbls_destroy(fbls_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    DevBuf* bufs[] = {&ctx->bank,  &ctx->scales,  &ctx->periods, &ctx->cum,   &ctx->cum32,  &ctx->hist,    &ctx->parts,
-                      &ctx->keys,  &ctx->tflags,  &ctx->records, &ctx->score, &ctx->depth,  &ctx->rflags,  &ctx->evidence,
-                      &ctx->chunks, &ctx->fault,  &ctx->family};
+    DevBuf* bufs[] = {&ctx->cum,     &ctx->cum32,    &ctx->hist,     &ctx->parts, &ctx->keys,  &ctx->tflags,
+                      &ctx->pass_in, &ctx->pass_out, &ctx->evidence, &ctx->fault, &ctx->family};
     for (DevBuf* b : bufs) release(*b);
+    for (PinBuf* b : {&ctx->pin_up, &ctx->pin_down, &ctx->pin_down2})
+        if (b->ptr) cudaFreeHost(b->ptr);
     for (fbls_ctx* w : ctx->workers) fbls_destroy(w);
     for (int i = 0; i < 4; i++)
         if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -579,10 +743,11 @@ int fbls_scan_bank(fbls_ctx* ctx, const fbls_ready* ready, const double* periods
     int rc = scan_bank(ctx, ready, periods, P, bank, nb, precision_mode == 0, band, &st);
     if (stats) *stats = st;
     if (rc && rc != FBLS_ERR_PRECISION) return rc;
-    if (records) std::memcpy(records, band.records.data(), band.records.size() * sizeof(double));
-    if (score) std::memcpy(score, band.score.data(), band.score.size() * sizeof(double));
-    if (depth) std::memcpy(depth, band.depth.data(), band.depth.size() * sizeof(double));
-    if (flags) std::memcpy(flags, band.flags.data(), band.flags.size() * sizeof(uint32_t));
+    if (!band.records) return rc;
+    if (records) std::memcpy(records, band.records, (size_t)P * RECORD_STRIDE * sizeof(double));
+    if (score) std::memcpy(score, band.score, (size_t)P * sizeof(double));
+    if (depth) std::memcpy(depth, band.depth, (size_t)P * sizeof(double));
+    if (flags) std::memcpy(flags, band.flags, (size_t)P * sizeof(uint32_t));
     return rc;
 }
 
@@ -657,49 +822,58 @@ int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* dur
     const double shape_gate = cfg->n_ingress > 0 && cfg->ingress_fractions[0] == 0.0
                                   ? cfg->shape_gate_fraction * cfg->threshold
                                   : 0.0;
-    std::vector<fbls_row> rows;
-    uint32_t bands = 0;
+    // Octave bands [lo, 2 lo) with the durations below lo / 4 (scan.rs:441-471);
+    // every band is scanned by scan_periods, the bands together (scan_bands).
+    struct Band {
+        std::vector<double> periods, durations, rho;
+        fbls_bank bank;
+    };
+    std::vector<Band> bands;
+    const double budget_mib = fold_budget_mib(cfg->max_fold_mib);
     double lo = grid[0];
     const double last = grid[grid.size() - 1];
     while (lo <= last) {
         const double hi = lo * 2.0;
-        std::vector<double> selected;
+        Band b;
         for (double p : grid)
-            if (p >= lo && p < hi) selected.push_back(p);
-        std::vector<double> bd, br;
+            if (p >= lo && p < hi) b.periods.push_back(p);
         for (auto& d : ds)
             if (d.first < lo / 4.0) {
-                bd.push_back(d.first);
-                br.push_back(d.second);
+                b.durations.push_back(d.first);
+                b.rho.push_back(d.second);
             }
-        if (!selected.empty() && !bd.empty()) {
-            fbls_bank bank;
-            bank.durations = bd.data();
-            bank.rho = br.data();
-            bank.nd = (uint32_t)bd.size();
-            bank.ingress = cfg->ingress_fractions;
-            bank.ns = cfg->n_ingress;
-            bank.layers = cfg->shape_layers;
-            bank.threshold = cfg->threshold;
-            bank.shape_gate = shape_gate;
-            bank.phase_oversample = cfg->phase_oversample;
-            bank.period_batch = cfg->period_batch;
-            bank.max_fold_mib = fold_budget_mib(cfg->max_fold_mib);
-            bank.prescan_factor = cfg->prescan_factor;
-            bank.prescan_fraction = cfg->prescan_fraction;
-            fbls_scan_stats st;
-            int rc = scan_periods(ctx, ready, selected.data(), (uint32_t)selected.size(), &bank,
-                                  cfg->precision_mode == 0, rows, &st);
-            if (rc) return rc;
-            if (stats_out && bands < 64) stats_out[bands] = st;
-            bands++;
-        }
+        if (!b.periods.empty() && !b.durations.empty()) bands.push_back(std::move(b));
         lo = hi;
     }
+    std::vector<BandJob> jobs(bands.size());
+    for (size_t i = 0; i < bands.size(); i++) {
+        fbls_bank& bank = bands[i].bank;
+        bank.durations = bands[i].durations.data();
+        bank.rho = bands[i].rho.data();
+        bank.nd = (uint32_t)bands[i].durations.size();
+        bank.ingress = cfg->ingress_fractions;
+        bank.ns = cfg->n_ingress;
+        bank.layers = cfg->shape_layers;
+        bank.threshold = cfg->threshold;
+        bank.shape_gate = shape_gate;
+        bank.phase_oversample = cfg->phase_oversample;
+        bank.period_batch = cfg->period_batch;
+        bank.max_fold_mib = budget_mib;
+        bank.prescan_factor = cfg->prescan_factor;
+        bank.prescan_fraction = cfg->prescan_fraction;
+        jobs[i].periods = bands[i].periods.data();
+        jobs[i].P = (uint32_t)bands[i].periods.size();
+        jobs[i].bank = &bank;
+    }
+    std::vector<fbls_row> rows;
+    const int rc = scan_bands(ctx, ready, jobs, cfg->precision_mode == 0, rows);
+    if (rc) return rc;
+    for (size_t i = 0; i < jobs.size() && stats_out && i < 64; i++) stats_out[i] = jobs[i].st;
+    const uint32_t n_scanned = (uint32_t)jobs.size();
     if (rows.size() > capacity) return fail(ctx, FBLS_ERR_ARGUMENT, "row capacity too small");
     std::memcpy(rows_out, rows.data(), rows.size() * sizeof(fbls_row));
     *n_rows = (uint32_t)rows.size();
-    if (n_bands) *n_bands = bands;
+    if (n_bands) *n_bands = n_scanned;
     return FBLS_OK;
 }
 

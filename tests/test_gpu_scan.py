@@ -89,6 +89,25 @@ def test_budget_error_keeps_reference_message(gpu, small):
         gpu.scan_bank(dev, [1.0], bank, 64)
 
 
+def test_launches_of_several_batches_keep_results_and_batch_count(gpu, small):
+    """A launch may cover several of the reference's batches; the records do
+    not depend on the batch size and ScanStats counts the reference's batches
+    (ceil(P / period_batch), scan.rs:190-199)."""
+    c, cfg, st, ost = small
+    dev = gpu.upload(st)
+    grid, bands = api.band_plan(st, cfg)
+    band = bands[-1]
+    periods = band["periods"]
+    whole = gpu.scan_bank(dev, periods, api.bank_for(band, cfg), band["nb"])
+    for batch in (7, 64, len(periods)):
+        bank = api.bank_for(band, cfg)
+        bank.period_batch = batch
+        got = gpu.scan_bank(dev, periods, bank, band["nb"])
+        for x, y in zip(got[:4], whole[:4]):
+            assert np.array_equal(x, y)
+        assert got[4]["batches"] == -(-len(periods) // batch)
+
+
 def test_fold_is_deterministic(gpu, small):
     c, cfg, st, ost = small
     dev = gpu.upload(st)
