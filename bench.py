@@ -413,6 +413,46 @@ def run_survey(args):
         torch.distributed.destroy_process_group()
 
 
+def run_precision_report(args):
+    """The reference's mixed mode (f32 pre-rank from (hi, lo) pairs, f64
+    winner) against f64 ranking throughout, on every period of every band at
+    the coarse and the full nb: how often the winning template differs, and
+    the relative error of the reported power (score) and depth."""
+    from fbls_b200 import api
+    curve, cfg, desc = _workload(args.workload)
+    state = api.prepared_family(curve.time, curve.flux, curve.flux_err, cfg)
+    grid, bands = api.band_plan(state, cfg)
+    out = {"report": "precision", "workload": desc, "passes": []}
+    with api.Gpu(0) as gpu:
+        dev = gpu.upload(state)
+        for band in bands:
+            bank = api.bank_for(band, cfg)
+            for nb in (band["nb"] // 2, band["nb"]):
+                mixed = gpu.scan_bank(dev, band["periods"], bank, nb, precision_mode=0)
+                exact = gpu.scan_bank(dev, band["periods"], bank, nb, precision_mode=1)
+                key = [2, 3, 7, 8]  # phase, width, ingress, rho
+                same = (mixed[0][:, key] == exact[0][:, key]).all(axis=1)
+                ok = np.isfinite(exact[1]) & (exact[1] != 0)
+                rel = np.abs(mixed[1][ok] - exact[1][ok]) / np.abs(exact[1][ok])
+                rdep = np.abs(mixed[2][ok] - exact[2][ok]) / np.maximum(np.abs(exact[2][ok]), 1e-300)
+                top = ok & (exact[1] >= bank.threshold * bank.prescan_fraction)
+                reltop = np.abs(mixed[1][top] - exact[1][top]) / np.abs(exact[1][top])
+                out["passes"].append({
+                    "nb": int(nb), "periods": int(len(band["periods"])),
+                    "same_template": float(same.mean()),
+                    "max_rel_score": float(rel.max(initial=0.0)), "max_rel_depth": float(rdep.max(initial=0.0)),
+                    "periods_over_prescan_cut": int(top.sum()),
+                    "max_rel_score_over_cut": float(reltop.max(initial=0.0)),
+                    "rescanned_tiles_mixed": int(mixed[4]["tile_rescans"]),
+                })
+        dev.free()
+    p = out["passes"]
+    out["same_template"] = float(np.average([x["same_template"] for x in p], weights=[x["periods"] for x in p]))
+    out["max_rel_score"] = max(x["max_rel_score"] for x in p)
+    out["max_rel_score_over_cut"] = max(x["max_rel_score_over_cut"] for x in p)
+    print(json.dumps(out))
+
+
 def run_profile_case(args):
     """One bounded scan_bank pass for profiler captures: the 13-sector star's
     octave band [8, 16) d at its coarse grid (1536 bins), first 4096 periods:
@@ -440,6 +480,8 @@ def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--profile-case", choices=["fold"], default=None,
                     help="run one bounded launch set for profiler captures instead of the benchmark")
+    ap.add_argument("--precision-report", action="store_true",
+                    help="compare the mixed f32/f64 ranking with f64 ranking on every period (one JSON line)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -450,7 +492,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
-    if args.profile_case:
+    if args.precision_report:
+        run_precision_report(args)
+    elif args.profile_case:
         run_profile_case(args)
     elif args.impl == "reference":
         run_reference(args)
