@@ -167,6 +167,8 @@ SIGNATURES = {
                                      C.POINTER(Config), C.POINTER(Row), C.c_uint32, c_uint32_p, c_uint64_p,
                                      C.POINTER(ScanStats), c_uint32_p]),
     "fbls_search_batch": (C.c_int, [C.c_void_p, C.POINTER(Star), C.c_uint32, C.POINTER(Config), C.c_uint32]),
+    "fbls_coarse_map": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, C.c_uint32, c_double_p, c_double_p, C.c_uint32,
+                                  C.c_double, C.POINTER(C.c_float)]),
 }
 
 _lib = None

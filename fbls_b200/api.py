@@ -233,6 +233,15 @@ class Gpu:
                                                C.byref(n), C.byref(st)))
         return _rows_array(rows, n.value), st.as_dict()
 
+    def coarse_map(self, dev: DeviceReady, periods, durations, rho, oversample: float = 2.0) -> np.ndarray:
+        """Best box score over phases per (period, duration): P x nd float32."""
+        p, d, r = _f64(periods), _f64(durations), _f64(rho)
+        out = np.empty((p.shape[0], d.shape[0]), dtype=np.float32)
+        self._check(self.lib.fbls_coarse_map(self.ctx, dev.handle, _dptr(p), p.shape[0], _dptr(d), _dptr(r),
+                                             d.shape[0], float(oversample),
+                                             out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
     def search_batch(self, states: Sequence[FamilyState], cfg: SearchConfig, period_max: Optional[Sequence[float]] = None,
                      devs: Optional[Sequence[DeviceReady]] = None, workers: int = 4):
         """signal_search over many stars with `workers` host threads, each

@@ -895,6 +895,137 @@ int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* du
     return FBLS_OK;
 }
 
+// Coarse periodogram of a family for the proposal network: periods are cut
+// into octave groups [lo, 2 lo), each folded at nb = max(8, ceil(oversample *
+// (group's longest period) / shortest duration)) and scanned by k_box_map.
+int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* ready, const double* periods, uint32_t P,
+                    const double* durations, const double* rho, uint32_t nd, double oversample, float* out) {
+    if (!ctx || !ready || !periods || !durations || !rho || !out) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (nd < 1 || nd > (uint32_t)MAP_MAX_DURATIONS) return fail(ctx, FBLS_ERR_ARGUMENT, "1 to 8 map durations");
+    if (P == 0) return FBLS_OK;
+    if (!(oversample > 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "oversample must be positive");
+    for (uint32_t i = 0; i < P; i++)
+        if (!(periods[i] > 0.0) || !std::isfinite(periods[i]) || (i && !(periods[i] > periods[i - 1])))
+            return fail(ctx, FBLS_ERR_ARGUMENT, "periods must be positive, finite and ascending");
+    double dmin = __builtin_huge_val();
+    for (uint32_t i = 0; i < nd; i++) {
+        if (!(durations[i] > 0.0) || !(rho[i] > 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "bad map duration");
+        dmin = rmin(dmin, durations[i]);
+    }
+    CK(cudaSetDevice(ctx->device), "set device");
+    struct Group {
+        uint32_t i0, count, nb;
+        FoldShape shape;
+        std::vector<int> chunks;
+        size_t off_scales, off_chunks;
+    };
+    std::vector<Group> groups;
+    size_t in_bytes = align256(2 * nd * sizeof(double)), cum_max = 0, hist_max = 0;
+    for (uint32_t i0 = 0; i0 < P;) {
+        uint32_t i1 = i0 + 1;
+        while (i1 < P && periods[i1] < 2.0 * periods[i0]) i1++;
+        Group g;
+        g.i0 = i0;
+        g.count = i1 - i0;
+        const uint64_t nb = std::max<uint64_t>(8, as_u64(std::ceil(oversample * periods[i1 - 1] / dmin)));
+        if (nb > (1u << 24)) return fail(ctx, FBLS_ERR_ARGUMENT, "phase grid too large");
+        g.nb = (uint32_t)nb;
+        const double scale_max = (double)nb / periods[i0];
+        if (std::floor(ready->t_last * scale_max) >= 4294967295.0 - 2.0 * (double)nb - 2.0)
+            return fail(ctx, FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
+        const size_t stride = 2 * (size_t)nb + 1;
+        const uint32_t per_launch =
+            (uint32_t)std::max<size_t>(1, std::min<size_t>(16384, (512ull << 20) / (NF * stride * 12)));
+        g.shape = fold_group_shape((int)nb, (int)std::min(g.count, per_launch), ctx->sm_count);
+        g.chunks.resize((size_t)ready->n + 2);
+        const int c = fold_chunks(ready->time_host.data(), (int)ready->n, scale_max, (int)nb, g.shape.span_cap,
+                                  g.shape.chunk_cap, g.chunks.data(), (int)g.chunks.size());
+        if (c < 1) return fail(ctx, FBLS_ERR_ARGUMENT, "fold chunking failed");
+        g.chunks.resize((size_t)c + 1);
+        g.off_scales = in_bytes;
+        in_bytes += align256(g.count * sizeof(double));
+        g.off_chunks = in_bytes;
+        in_bytes += align256(g.chunks.size() * sizeof(int));
+        const size_t launch = std::min(g.count, per_launch);
+        cum_max = std::max(cum_max, launch * NF * stride);
+        if (!g.shape.hist_in_smem)
+            hist_max = std::max(hist_max, ((launch + g.shape.group - 1) / g.shape.group) * g.shape.group * NF *
+                                              (size_t)g.shape.row_stride);
+        groups.push_back(std::move(g));
+        i0 = i1;
+    }
+    const size_t out_bytes = (size_t)P * nd * sizeof(float);
+    CK(ensure(ctx->pass_in, in_bytes), "workspace");
+    CK(ensure(ctx->pass_out, out_bytes), "workspace");
+    CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
+    CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
+    if (hist_max) CK(ensure(ctx->hist, hist_max * sizeof(double)), "workspace");
+    CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
+    CK(ensure_pinned(ctx->pin_up, in_bytes), "pinned workspace");
+    CK(ensure_pinned(ctx->pin_down, out_bytes + 256), "pinned workspace");
+    unsigned char* up = static_cast<unsigned char*>(ctx->pin_up.ptr);
+    std::memcpy(up, durations, nd * sizeof(double));
+    std::memcpy(up + nd * sizeof(double), rho, nd * sizeof(double));
+    for (const Group& g : groups) {
+        double* sc = reinterpret_cast<double*>(up + g.off_scales);
+        for (uint32_t i = 0; i < g.count; i++) sc[i] = (double)g.nb / periods[g.i0 + i];
+        std::memcpy(up + g.off_chunks, g.chunks.data(), g.chunks.size() * sizeof(int));
+    }
+    cudaStream_t s = ctx->stream;
+    unsigned char* din = static_cast<unsigned char*>(ctx->pass_in.ptr);
+    float* dout = static_cast<float*>(ctx->pass_out.ptr);
+    CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
+    CK(cudaMemcpyAsync(din, up, in_bytes, cudaMemcpyHostToDevice, s), "upload");
+    for (const Group& g : groups) {
+        const size_t stride = 2 * (size_t)g.nb + 1;
+        const uint32_t per_launch =
+            (uint32_t)std::max<size_t>(1, std::min<size_t>(16384, (512ull << 20) / (NF * stride * 12)));
+        for (uint32_t c = 0; c < g.count; c += per_launch) {
+            const int n = (int)std::min(g.count - c, per_launch);
+            FoldArgs fa{};
+            fa.time = ready->time;
+            fa.v = ready->v;
+            fa.w = ready->w;
+            fa.scales = reinterpret_cast<const double*>(din + g.off_scales) + c;
+            fa.n = (int)ready->n;
+            fa.nb = (int)g.nb;
+            fa.periods = n;
+            fa.group = g.shape.group;
+            fa.cum = as<double>(ctx->cum);
+            fa.cum32 = as<float2>(ctx->cum32);
+            fa.hist_global = g.shape.hist_in_smem ? nullptr : as<double>(ctx->hist);
+            fa.chunks = reinterpret_cast<const int*>(din + g.off_chunks);
+            fa.nchunks = (int)g.chunks.size() - 1;
+            fa.stage_field = g.shape.stage_field;
+            fa.window = g.shape.window;
+            fa.row_stride = g.shape.row_stride;
+            fa.fault = as<uint32_t>(ctx->fault);
+            CK(launch_fold(fa, g.shape, s), "fold");
+            MapArgs ma{};
+            ma.cum = fa.cum;
+            ma.scales = fa.scales;
+            ma.durations = reinterpret_cast<const double*>(din);
+            ma.rho = reinterpret_cast<const double*>(din) + nd;
+            ma.nd = (int)nd;
+            ma.nb = (int)g.nb;
+            ma.baseline = ready->baseline_norm;
+            ma.n = (double)ready->n;
+            ma.out = dout + (size_t)(g.i0 + c) * nd;
+            CK(launch_box_map(ma, n, s), "box map");
+            ctx->counters.launches += 2;
+        }
+    }
+    unsigned char* down = static_cast<unsigned char*>(ctx->pin_down.ptr);
+    CK(cudaMemcpyAsync(down, dout, out_bytes, cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaMemcpyAsync(down + out_bytes, ctx->fault.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaStreamSynchronize(s), "coarse map");
+    uint32_t fault = 0;
+    std::memcpy(&fault, down + out_bytes, sizeof(uint32_t));
+    if (fault) return fail(ctx, FBLS_ERR_CUDA, "fold: staging copies did not complete");
+    std::memcpy(out, down, out_bytes);
+    return FBLS_OK;
+}
+
 // Many stars on one device: `workers` host threads (the caller's included),
 // each with its own context (stream, workspace and a reusable buffer for the
 // star's observations), take stars from a shared counter and run

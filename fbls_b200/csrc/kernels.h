@@ -96,6 +96,20 @@ struct MergeArgs {
     uint32_t* flags_out;
 };
 
+// Coarse periodogram of the proposal path (proposal.cu).
+constexpr int MAP_MAX_DURATIONS = 8;
+struct MapArgs {
+    const double* cum;        // periods x NF x (2nb+1), from the fold
+    const double* scales;     // periods
+    const double* durations;  // nd
+    const double* rho;        // nd
+    int nd;
+    int nb;
+    double baseline;          // baseline_norm c
+    double n;                 // observation count
+    float* out;               // periods x nd: best box score per duration
+};
+
 FoldShape fold_group_shape(int nb, int periods, int sm_count);
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
 // spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.
@@ -105,5 +119,6 @@ int fold_chunks(const double* time, int n, double scale_max, int nb, int span_ca
 cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream);
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream);
 cudaError_t launch_merge(const MergeArgs& a, cudaStream_t stream);
+cudaError_t launch_box_map(const MapArgs& a, int periods, cudaStream_t stream);
 
 }  // namespace fbls

@@ -1,0 +1,80 @@
+// Kernels of the proposal path (north_star's learned form): the coarse
+// periodogram that feeds the proposal network.
+//
+// k_box_map: for each period of a launch and each duration of a small bank,
+// the best box score over every phase, (a / rho) / sqrt(norm - hp^2 / c)
+// with hp = norm = the template's weight sum, in f64 from the doubled prefix
+// sums the fold writes; a template counts when its width is below nb / 2,
+// it holds 3 .. n - 3 observations, a > 0 and the precision is positive, as in
+// the scan's f64 pass (src/search/kernels.rs:428-455, :679-700). 0 when no
+// template of the duration counts. One CTA of 256 threads per period.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace fbls {
+
+namespace {
+constexpr int MAP_THREADS = 256;
+}
+
+__global__ void __launch_bounds__(MAP_THREADS) k_box_map(MapArgs a) {
+    __shared__ double s_best[MAP_MAX_DURATIONS][MAP_THREADS / 32];
+    const int f = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int nb = a.nb;
+    const int nd = a.nd;
+    const size_t stride = 2 * (size_t)nb + 1;
+    const double* rv = a.cum + (size_t)f * NF * stride + F_V * stride;
+    const double* rw = a.cum + (size_t)f * NF * stride + F_W * stride;
+    const double* rn = a.cum + (size_t)f * NF * stride + F_N * stride;
+    const double scale = a.scales[f];
+    const uint32_t half = (uint32_t)(nb / 2);
+    uint32_t width[MAP_MAX_DURATIONS];
+    bool ok[MAP_MAX_DURATIONS];
+    double best[MAP_MAX_DURATIONS];
+#pragma unroll
+    for (int d = 0; d < MAP_MAX_DURATIONS; d++) {
+        const uint32_t raw = d < nd ? template_width(a.durations[d], scale) : 1u;
+        width[d] = min(raw, half);
+        ok[d] = d < nd && raw < half;
+        best[d] = 0.0;
+    }
+    for (int j = tid; j < nb; j += MAP_THREADS) {
+#pragma unroll
+        for (int d = 0; d < MAP_MAX_DURATIONS; d++) {
+            if (!ok[d]) continue;
+            const uint32_t k = width[d];
+            const double count = __dsub_rn(rn[j + k], rn[j]);
+            if (!(count >= 3.0 && count <= a.n - 3.0)) continue;
+            const double av = __dsub_rn(rv[j + k], rv[j]);
+            if (!(av > 0.0)) continue;
+            const double w = __dsub_rn(rw[j + k], rw[j]);
+            const double q = __dsub_rn(w, __ddiv_rn(__dmul_rn(w, w), a.baseline));
+            if (!(q > 0.0)) continue;
+            const double s = __ddiv_rn(__ddiv_rn(av, a.rho[d]), __dsqrt_rn(rmax(q, 1e-300)));
+            if (s > best[d]) best[d] = s;
+        }
+    }
+    const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int d = 0; d < MAP_MAX_DURATIONS; d++) {
+        double v = best[d];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+        if (lane == 0) s_best[d][warp] = v;
+    }
+    __syncthreads();
+    if (tid < nd) {
+        double v = s_best[tid][0];
+        for (int w = 1; w < MAP_THREADS / 32; w++) v = fmax(v, s_best[tid][w]);
+        a.out[(size_t)f * nd + tid] = (float)v;
+    }
+}
+
+cudaError_t launch_box_map(const MapArgs& a, int periods, cudaStream_t stream) {
+    if (a.nd < 1 || a.nd > MAP_MAX_DURATIONS || a.nb < 2 || periods < 1) return cudaErrorInvalidValue;
+    k_box_map<<<periods, MAP_THREADS, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace fbls

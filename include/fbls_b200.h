@@ -255,6 +255,19 @@ int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* dur
                        uint32_t nd, const fbls_config* cfg, fbls_row* rows_out, uint32_t capacity,
                        uint32_t* n_rows, uint64_t* grid_len, fbls_scan_stats* stats_out, uint32_t* n_bands);
 
+/* ---- proposal path (north_star's learned form; no counterpart in the
+ * reference) ------------------------------------------------------------- */
+
+/* Coarse periodogram of an uploaded family, the proposal network's input:
+ * out[i * nd + d] = best box score over all phases of period i (ascending)
+ * and duration d (1 <= nd <= 8), the score of the reference's f64 ranking
+ * (scan.rs template semantics: width below nb / 2, 3 .. n - 3 points, a > 0,
+ * positive precision), 0 when none counts. Periods are folded in octave
+ * groups at nb = max(8, ceil(oversample * longest period / shortest
+ * duration)). */
+int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* ready, const double* periods, uint32_t P,
+                    const double* durations, const double* rho, uint32_t nd, double oversample, float* out);
+
 /* ---- batched search (replaces the reference's per-device worker threads,
  * src/batch.rs:61-102, each running one star's search at a time) --------- */
 
