@@ -169,6 +169,17 @@ SIGNATURES = {
     "fbls_search_batch": (C.c_int, [C.c_void_p, C.POINTER(Star), C.c_uint32, C.POINTER(Config), C.c_uint32]),
     "fbls_coarse_map": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, C.c_uint32, c_double_p, c_double_p, C.c_uint32,
                                   C.c_double, C.POINTER(C.c_float)]),
+    # proposal network kernels: device pointers passed as integers
+    "fbls_nn_gemm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int] + [C.c_longlong] * 9
+                     + [C.c_int, C.c_float, C.c_float, C.c_void_p]),
+    "fbls_nn_im2col": (C.c_int, [C.c_void_p, C.c_void_p] + [C.c_int] * 5 + [C.c_void_p]),
+    "fbls_nn_col2im": (C.c_int, [C.c_void_p, C.c_void_p] + [C.c_int] * 5 + [C.c_void_p]),
+    "fbls_nn_bias_relu_pool": (C.c_int, [C.c_void_p] * 4 + [C.c_int] * 4 + [C.c_void_p]),
+    "fbls_nn_bias_relu_pool_bwd": (C.c_int, [C.c_void_p] * 5 + [C.c_int] * 4 + [C.c_void_p]),
+    "fbls_nn_head": (C.c_int, [C.c_void_p] * 7 + [C.c_int] * 4 + [C.c_void_p]),
+    "fbls_nn_head_bwd": (C.c_int, [C.c_void_p] * 6 + [C.c_int] * 4 + [C.c_void_p]),
+    "fbls_nn_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_float,
+                               C.c_float, C.c_float, C.c_int, C.c_void_p]),
 }
 
 _lib = None

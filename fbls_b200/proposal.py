@@ -1,0 +1,243 @@
+"""Proposal network of the learned form: a small 1D CNN that reads a star's
+coarse periodogram (best box score per period and duration, from
+fbls_coarse_map) and scores log-period bands, so that only the best bands get
+the exhaustive scan.
+
+Input: 4 durations x 4096 log-spaced periods over [0.5, 20] d. Four
+convolution layers (kernel 7, 32 channels, ReLU, max-pool 2, 2, 2, 4), then a
+1x1 head averaged over groups of 4 positions: 32 band logits. Every layer runs
+on this library's kernels (fbls_nn_*): convolutions as bf16 tensor-core GEMMs
+with f32 accumulation, trained by softmax cross-entropy and Adam. torch is
+used for device buffers only.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _native as N
+
+PMIN, PMAX = 0.5, 20.0
+T_IN = 4096
+BANDS = 32
+CH = 32
+KW = 7
+POOLS = (2, 2, 2, 4)
+HEAD_G = 4
+MAP_CHANNELS = 4
+
+
+def map_periods() -> np.ndarray:
+    return np.geomspace(PMIN, PMAX, T_IN)
+
+
+def band_of(period: float) -> int:
+    b = int(math.floor(BANDS * math.log(period / PMIN) / math.log(PMAX / PMIN)))
+    return min(max(b, 0), BANDS - 1)
+
+
+def band_range(b: int) -> Tuple[float, float]:
+    r = math.log(PMAX / PMIN) / BANDS
+    return PMIN * math.exp(r * b), PMIN * math.exp(r * (b + 1))
+
+
+def map_bank(state) -> Tuple[np.ndarray, np.ndarray]:
+    """Four of the family's durations (shortest, two inner, longest) and their rho."""
+    d = np.asarray(state.durations, dtype=np.float64)
+    order = np.argsort(d, kind="stable")
+    idx = order[np.unique(np.round(np.linspace(0, len(d) - 1, MAP_CHANNELS)).astype(int))]
+    while len(idx) < MAP_CHANNELS:
+        idx = np.append(idx, idx[-1])
+    return d[idx], np.asarray(state.rho, dtype=np.float64)[idx]
+
+
+def star_map(gpu, dev, state, period_max: float) -> np.ndarray:
+    """(4, T_IN) features of one star: log1p of the coarse map, standardised per
+    duration over the periods the star's search covers, 0 elsewhere."""
+    p = map_periods()
+    d, r = map_bank(state)
+    lo = max(PMIN, 4.0 * float(np.min(state.durations)) * (1.0 + 1e-9))
+    hi = min(period_max, float(state.time[-1]))
+    keep = (p >= lo) & (p <= hi)
+    x = np.zeros((MAP_CHANNELS, T_IN), dtype=np.float32)
+    if keep.sum() < 8:
+        return x
+    m = gpu.coarse_map(dev, p[keep], d, r, oversample=2.0)
+    f = np.log1p(np.maximum(m, 0.0)).T
+    mu = f.mean(axis=1, keepdims=True)
+    sd = f.std(axis=1, keepdims=True) + 1e-3
+    x[:, keep] = (f - mu) / sd
+    return x
+
+
+class Net:
+    """Parameters (one flat f32 buffer), Adam state and per-batch workspaces."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        import torch
+        self.torch = torch
+        self.dev = torch.device(f"cuda:{device}")
+        self.lib = N.load()
+        shapes = []
+        ci = MAP_CHANNELS
+        for _ in POOLS:
+            shapes += [("W", (CH, ci * KW)), ("b", (CH,))]
+            ci = CH
+        shapes += [("wh", (CH,)), ("bh", (1,))]
+        self.shapes = shapes
+        n = sum(int(np.prod(s)) for _, s in shapes)
+        g = torch.Generator().manual_seed(seed)
+        flat = torch.zeros(n, dtype=torch.float32)
+        o = 0
+        for kind, s in shapes:
+            k = int(np.prod(s))
+            if kind == "W":
+                flat[o:o + k] = torch.randn(k, generator=g) * math.sqrt(2.0 / s[1])
+            elif kind == "wh":
+                flat[o:o + k] = torch.randn(k, generator=g) * math.sqrt(1.0 / s[0])
+            o += k
+        self.w = flat.to(self.dev)
+        self.grad = torch.zeros_like(self.w)
+        self.m = torch.zeros_like(self.w)
+        self.v = torch.zeros_like(self.w)
+        self.t = 0
+        self.views = []
+        o = 0
+        for kind, s in shapes:
+            k = int(np.prod(s))
+            self.views.append((self.w[o:o + k].view(*s), self.grad[o:o + k].view(*s)))
+            o += k
+        self._ws: Dict[int, dict] = {}
+        self.ones = torch.ones(4096, dtype=torch.float32, device=self.dev)
+
+    # -- workspace -------------------------------------------------------
+    def _workspace(self, B: int) -> dict:
+        if B in self._ws:
+            return self._ws[B]
+        torch = self.torch
+        ws = {"X": [], "Xc": [], "Y": [], "Z": [], "idx": []}
+        T = T_IN
+        ci = MAP_CHANNELS
+        for P in POOLS:
+            ws["Xc"].append(torch.empty(ci * KW, B * T, device=self.dev))
+            ws["Y"].append(torch.empty(CH, B * T, device=self.dev))
+            ws["Z"].append(torch.empty(CH, B * (T // P), device=self.dev))
+            ws["idx"].append(torch.empty(CH * B * (T // P), dtype=torch.uint8, device=self.dev))
+            T //= P
+            ci = CH
+        ws["T_out"] = T
+        ws["logits"] = torch.empty(B, BANDS, device=self.dev)
+        ws["loss"] = torch.empty(B, device=self.dev)
+        ws["dlogits"] = torch.empty(B, BANDS, device=self.dev)
+        ws["labels"] = torch.empty(B, dtype=torch.int32, device=self.dev)
+        self._ws[B] = ws
+        return ws
+
+    @staticmethod
+    def _p(t) -> int:
+        return t.data_ptr()
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed with status {rc}")
+
+    def _gemm(self, A, B, Cm, M, Nn, K, sa, sb, sc, alpha=1.0, beta=0.0, batch=1, bs=(0, 0, 0)):
+        self._check(self.lib.fbls_nn_gemm(self._p(A), self._p(B), self._p(Cm), M, Nn, K, sa[0], sa[1], bs[0],
+                                          sb[0], sb[1], bs[1], sc[0], sc[1], bs[2], batch, alpha, beta, None),
+                    "gemm")
+
+    # -- forward / backward ------------------------------------------------
+    def forward(self, x, labels=None):
+        """x: device tensor (4, B, T_IN) f32 (channel-major). Returns logits (B, 32)
+        and, with labels (B,) int32, the mean loss (a device scalar)."""
+        B = x.shape[1]
+        ws = self._workspace(B)
+        lib = self.lib
+        X = x.contiguous()
+        T = T_IN
+        ci = MAP_CHANNELS
+        ws["X"] = [X]
+        for l, P in enumerate(POOLS):
+            W, _ = self.views[2 * l]
+            b, _ = self.views[2 * l + 1]
+            Xc, Y, Z, idx = ws["Xc"][l], ws["Y"][l], ws["Z"][l], ws["idx"][l]
+            self._check(lib.fbls_nn_im2col(self._p(X), self._p(Xc), B, ci, T, KW, KW // 2, None), "im2col")
+            n = B * T
+            # Y (CH x n) = W (CH x ci*KW) . Xc (ci*KW x n)
+            self._gemm(W, Xc, Y, CH, n, ci * KW, (ci * KW, 1), (n, 1), (n, 1))
+            self._check(lib.fbls_nn_bias_relu_pool(self._p(Y), self._p(b), self._p(Z), self._p(idx), B, CH, T, P,
+                                                   None), "pool")
+            X = Z
+            ws["X"].append(Z)
+            T //= P
+            ci = CH
+        wh, _ = self.views[-2]
+        bh, _ = self.views[-1]
+        lab = None
+        if labels is not None:
+            ws["labels"].copy_(labels)
+            lab = ws["labels"]
+        self._check(lib.fbls_nn_head(self._p(X), self._p(wh), self._p(bh), self._p(lab) if lab is not None else None,
+                                     self._p(ws["logits"]), self._p(ws["loss"]), self._p(ws["dlogits"]), B, CH, T,
+                                     HEAD_G, None), "head")
+        loss = ws["loss"].mean() if labels is not None else None
+        return ws["logits"], loss
+
+    def backward(self, B: int):
+        """Gradients of the mean loss of the last forward (with labels) into self.grad."""
+        ws = self._workspace(B)
+        lib = self.lib
+        torch = self.torch
+        self.grad.zero_()
+        T = ws["T_out"]
+        wh, dwh = self.views[-2]
+        bh, dbh = self.views[-1]
+        Zl = ws["X"][-1]
+        dZ = torch.empty_like(Zl)
+        self._check(lib.fbls_nn_head_bwd(self._p(Zl), self._p(wh), self._p(ws["dlogits"]), self._p(dZ), self._p(dwh),
+                                         self._p(dbh), B, CH, T, HEAD_G, None), "head backward")
+        Ts = [T_IN]
+        for P in POOLS:
+            Ts.append(Ts[-1] // P)
+        for l in reversed(range(len(POOLS))):
+            P = POOLS[l]
+            Tl = Ts[l]
+            ci = MAP_CHANNELS if l == 0 else CH
+            W, dW = self.views[2 * l]
+            _, db = self.views[2 * l + 1]
+            dY = torch.empty(CH, B * Tl, device=self.dev)
+            self._check(lib.fbls_nn_bias_relu_pool_bwd(self._p(dZ), self._p(ws["Z"][l]), self._p(ws["idx"][l]),
+                                                       self._p(dY), self._p(db), B, CH, Tl, P, None), "pool backward")
+            n = B * Tl
+            Xc = ws["Xc"][l]
+            kdim = ci * KW
+            # dW (CH x kdim) = dY (CH x n) . Xc^T (n x kdim), split over S chunks of n.
+            S = max(1, min(64, n // 8192))
+            while n % S:
+                S -= 1
+            part = torch.empty(S, CH * kdim, device=self.dev)
+            self._gemm(dY, Xc, part, CH, kdim, n // S, (n, 1), (1, n), (kdim, 1), batch=S,
+                       bs=(n // S, n // S, CH * kdim))
+            # dW += ones(1 x S) . part (S x CH*kdim)
+            self._gemm(self.ones, part, dW, 1, CH * kdim, S, (0, 1), (CH * kdim, 1), (0, 1), beta=1.0)
+            if l == 0:
+                break
+            # dXc (kdim x n) = W^T (kdim x CH) . dY (CH x n); dZ_prev = col2im(dXc)
+            dXc = torch.empty(kdim, n, device=self.dev)
+            self._gemm(W, dY, dXc, kdim, n, CH, (1, kdim), (n, 1), (n, 1))
+            dZ = torch.empty(ci, B * Tl, device=self.dev)
+            self._check(lib.fbls_nn_col2im(self._p(dXc), self._p(dZ), B, ci, Tl, KW, KW // 2, None), "col2im")
+
+    def adam(self, lr: float = 1e-3):
+        self.t += 1
+        self._check(self.lib.fbls_nn_adam(self._p(self.w), self._p(self.grad), self._p(self.m), self._p(self.v),
+                                          self.w.numel(), lr, 0.9, 0.999, 1e-8, self.t, None), "adam")
+
+    def state_dict(self) -> np.ndarray:
+        return self.w.detach().cpu().numpy().copy()
+
+    def load(self, flat: np.ndarray):
+        self.w.copy_(self.torch.from_numpy(np.asarray(flat, dtype=np.float32)))

@@ -268,6 +268,36 @@ int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* dur
 int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* ready, const double* periods, uint32_t P,
                     const double* durations, const double* rho, uint32_t nd, double oversample, float* out);
 
+/* Proposal network kernels. Every pointer is device memory; `stream` is a
+ * cudaStream_t (NULL: the legacy stream). Activations are f32 laid out
+ * [channel][curve][position]. Returns 0, FBLS_ERR_ARGUMENT or FBLS_ERR_CUDA. */
+
+/* C(m, n) = alpha sum_k A(m, k) B(k, n) + beta C(m, n) for `batch` problems,
+ * X(i, j) = X[i * s_i + j * s_j + batch index * s_b]; the operands are
+ * rounded to bf16 and multiplied on the tensor cores with f32 accumulation. */
+int fbls_nn_gemm(const float* A, const float* B, float* C, int M, int N, int K, long long sam, long long sak,
+                 long long sab, long long sbk, long long sbn, long long sbb, long long scm, long long scn,
+                 long long scb, int batch, float alpha, float beta, void* stream);
+/* Xcol[ci*KW + k][b][t] = X[ci][b][t + k - R] (0 outside), and its adjoint. */
+int fbls_nn_im2col(const float* X, float* Xcol, int B, int Ci, int T, int KW, int R, void* stream);
+int fbls_nn_col2im(const float* dXcol, float* dX, int B, int Ci, int T, int KW, int R, void* stream);
+/* Z = maxpool_P(relu(Y + bias)) with the argmax offsets, and the backward
+ * pass to dY (dbias accumulates). */
+int fbls_nn_bias_relu_pool(const float* Y, const float* bias, float* Z, uint8_t* idx, int B, int C, int T, int P,
+                           void* stream);
+int fbls_nn_bias_relu_pool_bwd(const float* dZ, const float* Z, const uint8_t* idx, float* dY, float* dbias, int B,
+                               int C, int T, int P, void* stream);
+/* Head: logits[b][j] = mean over a group of G positions of (wh . Z[:, b, t] +
+ * bh); with labels, the softmax cross-entropy per curve and d loss_mean /
+ * d logits; and its backward pass (dwh, dbh accumulate). */
+int fbls_nn_head(const float* Z, const float* wh, const float* bh, const int* labels, float* logits, float* loss,
+                 float* dlogits, int B, int C, int T, int G, void* stream);
+int fbls_nn_head_bwd(const float* Z, const float* wh, const float* dlogits, float* dZ, float* dwh, float* dbh, int B,
+                     int C, int T, int G, void* stream);
+/* Adam step t (>= 1) with bias correction over n parameters. */
+int fbls_nn_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+                 int t, void* stream);
+
 /* ---- batched search (replaces the reference's per-device worker threads,
  * src/batch.rs:61-102, each running one star's search at a time) --------- */
 

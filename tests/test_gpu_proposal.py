@@ -33,3 +33,91 @@ def test_coarse_map_matches_the_f64_box_scan(gpu, workload):
         assert np.array_equal(got[:, d], want), (d, np.nonzero(got[:, d] != want)[0][:5])
     assert (got > 0).any()
     dev.free()
+
+
+# ---- proposal network kernels against a PyTorch fp32 reference -------------
+
+def _torch_net(net, x, labels):
+    """The same network in PyTorch fp32 (reference only)."""
+    import torch
+    import torch.nn.functional as F
+    from fbls_b200 import proposal as pr
+    w = net.w.detach().clone().requires_grad_(True)
+    o = 0
+    params = []
+    for kind, s in net.shapes:
+        k = int(np.prod(s))
+        params.append(w[o:o + k].view(*s))
+        o += k
+    h = x.permute(1, 0, 2)  # (B, C, T)
+    ci = pr.MAP_CHANNELS
+    for l, P in enumerate(pr.POOLS):
+        W = params[2 * l].view(pr.CH, ci, pr.KW)
+        h = F.max_pool1d(F.relu(F.conv1d(h, W, params[2 * l + 1], padding=pr.KW // 2)), P)
+        ci = pr.CH
+    hh = torch.einsum("bct,c->bt", h, params[-2]) + params[-1]
+    logits = hh.view(hh.shape[0], -1, pr.HEAD_G).mean(dim=2)
+    loss = F.cross_entropy(logits, labels.long())
+    loss.backward()
+    return logits.detach(), loss.detach(), w.grad.detach()
+
+
+def test_nn_gemm_matches_torch(gpu):
+    import torch
+    from fbls_b200 import proposal as pr
+    net = pr.Net(0)
+    g = torch.Generator().manual_seed(1)
+    A = torch.randn(70, 130, generator=g).cuda()
+    B = torch.randn(130, 90, generator=g).cuda()
+    Cm = torch.zeros(70, 90).cuda()
+    net._gemm(A, B, Cm, 70, 90, 130, (130, 1), (90, 1), (90, 1))
+    ref = A.bfloat16().float() @ B.bfloat16().float()
+    assert torch.allclose(Cm, ref, rtol=1e-4, atol=1e-3)
+    # transposed operands through strides, batched, with beta
+    Ct = torch.ones(2, 90, 70).cuda()
+    At = torch.stack([A.t().contiguous(), 2 * A.t().contiguous()])  # (2, 130, 70): A(m,k) = At[k][m]
+    net._gemm(At, B, Ct, 70, 90, 130, (1, 70), (90, 1), (1, 70), beta=1.0, batch=2, bs=(130 * 70, 0, 90 * 70))
+    assert torch.allclose(Ct[0], ref.t() + 1, rtol=1e-4, atol=1e-3)
+    assert torch.allclose(Ct[1], 2 * ref.t() + 1, rtol=1e-4, atol=2e-3)
+
+
+def test_proposal_net_forward_and_gradients_match_torch(gpu):
+    import torch
+    from fbls_b200 import proposal as pr
+    net = pr.Net(0, seed=3)
+    B = 6
+    g = torch.Generator().manual_seed(2)
+    x = torch.randn(pr.MAP_CHANNELS, B, pr.T_IN, generator=g).cuda()
+    labels = torch.randint(0, pr.BANDS, (B,), generator=g, dtype=torch.int32).cuda()
+    logits, loss = net.forward(x, labels)
+    net.backward(B)
+    rl, rloss, rgrad = _torch_net(net, x, labels)
+    scale = rl.abs().max().item()
+    assert (logits - rl).abs().max().item() <= 0.03 * scale + 1e-3
+    assert abs(loss.item() - rloss.item()) <= 0.02 * abs(rloss.item()) + 1e-3
+    gv, rv = net.grad, rgrad
+    cos = torch.nn.functional.cosine_similarity(gv, rv, dim=0).item()
+    assert cos > 0.99, cos
+    assert (gv - rv).norm().item() <= 0.1 * rv.norm().item()
+
+
+def test_proposal_net_training_reduces_loss(gpu):
+    import torch
+    from fbls_b200 import proposal as pr
+    net = pr.Net(0, seed=4)
+    B = 16
+    g = torch.Generator().manual_seed(5)
+    labels = torch.randint(0, pr.BANDS, (B,), generator=g, dtype=torch.int32)
+    x = torch.randn(pr.MAP_CHANNELS, B, pr.T_IN, generator=g) * 0.1
+    for b in range(B):  # a bump at the label's band in every channel
+        lo = int(labels[b]) * (pr.T_IN // pr.BANDS)
+        x[:, b, lo:lo + pr.T_IN // pr.BANDS] += 2.0
+    x, labels = x.cuda(), labels.cuda()
+    first = None
+    for _ in range(60):
+        _, loss = net.forward(x, labels)
+        first = loss.item() if first is None else first
+        net.backward(B)
+        net.adam(3e-3)
+    _, loss = net.forward(x, labels)
+    assert loss.item() < 0.3 * first
