@@ -58,6 +58,8 @@ class Star(C.Structure):
         ("grid_len", C.c_uint64),
         ("templates", C.c_uint64),
         ("status", C.c_int),
+        ("ranges", C.POINTER(C.c_double)),
+        ("n_ranges", C.c_uint32),
     ]
 
 
@@ -166,6 +168,9 @@ SIGNATURES = {
     "fbls_signal_search": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, c_double_p, C.c_uint32,
                                      C.POINTER(Config), C.POINTER(Row), C.c_uint32, c_uint32_p, c_uint64_p,
                                      C.POINTER(ScanStats), c_uint32_p]),
+    "fbls_signal_search_ranges": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, c_double_p, C.c_uint32,
+                                            C.POINTER(Config), c_double_p, C.c_uint32, C.POINTER(Row), C.c_uint32,
+                                            c_uint32_p, c_uint64_p, C.POINTER(ScanStats), c_uint32_p]),
     "fbls_search_batch": (C.c_int, [C.c_void_p, C.POINTER(Star), C.c_uint32, C.POINTER(Config), C.c_uint32]),
     "fbls_coarse_map": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, C.c_uint32, c_double_p, c_double_p, C.c_uint32,
                                   C.c_double, C.POINTER(C.c_float)]),

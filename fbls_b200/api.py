@@ -243,11 +243,13 @@ class Gpu:
         return out
 
     def search_batch(self, states: Sequence[FamilyState], cfg: SearchConfig, period_max: Optional[Sequence[float]] = None,
-                     devs: Optional[Sequence[DeviceReady]] = None, workers: int = 4):
+                     devs: Optional[Sequence[DeviceReady]] = None, workers: int = 4,
+                     ranges: Optional[Sequence[Optional[Sequence[Tuple[float, float]]]]] = None):
         """signal_search over many stars with `workers` host threads, each
         with its own stream: [(rows N x 5, grid length, templates)] per star.
         period_max overrides cfg.period_max per star; devs are uploaded
-        families (else each worker uploads the star's host arrays)."""
+        families (else each worker uploads the star's host arrays); ranges
+        restrict a star's search to period ranges [lo, hi)."""
         count = len(states)
         stars = (N.Star * max(count, 1))()
         keep = []
@@ -272,6 +274,11 @@ class Gpu:
             keep.append(rows)
             st.rows = C.cast(rows, C.POINTER(N.Row))
             st.capacity = cap
+            if ranges is not None and ranges[i]:
+                rg = _f64(np.asarray(ranges[i], dtype=np.float64).reshape(-1))
+                keep.append(rg)
+                st.ranges = _dptr(rg)
+                st.n_ranges = rg.shape[0] // 2
         c, ck = _config(cfg)
         self._check(self.lib.fbls_search_batch(self.ctx, stars, count, C.byref(c), int(workers)))
         out = []
@@ -280,8 +287,10 @@ class Gpu:
             out.append((_rows_array(st.rows, st.n_rows), int(st.grid_len), int(st.templates)))
         return out
 
-    def signal_search(self, state: FamilyState, cfg: SearchConfig, dev: Optional[DeviceReady] = None):
-        """signal_search: (rows N x 5, grid length, per-band ScanStats)."""
+    def signal_search(self, state: FamilyState, cfg: SearchConfig, dev: Optional[DeviceReady] = None,
+                      ranges: Optional[Sequence[Tuple[float, float]]] = None):
+        """signal_search: (rows N x 5, grid length, per-band ScanStats); with
+        ranges, only the grid periods in those [lo, hi) ranges are scanned."""
         own = dev is None
         if own:
             dev = self.upload(state)
@@ -294,8 +303,10 @@ class Gpu:
             glen = C.c_uint64(0)
             stats = (N.ScanStats * 64)()
             nb = C.c_uint32(0)
-            self._check(self.lib.fbls_signal_search(self.ctx, dev.handle, _dptr(d), _dptr(r), len(d), C.byref(c),
-                                                    rows, cap, C.byref(n), C.byref(glen), stats, C.byref(nb)))
+            rg = _f64(np.asarray(ranges if ranges else [], dtype=np.float64).reshape(-1))
+            self._check(self.lib.fbls_signal_search_ranges(self.ctx, dev.handle, _dptr(d), _dptr(r), len(d),
+                                                           C.byref(c), _dptr(rg), rg.shape[0] // 2, rows, cap,
+                                                           C.byref(n), C.byref(glen), stats, C.byref(nb)))
             return _rows_array(rows, n.value), int(glen.value), [stats[i].as_dict() for i in range(nb.value)]
         finally:
             if own:

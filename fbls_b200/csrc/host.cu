@@ -519,6 +519,7 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
 struct BandJob {
     const double* periods = nullptr;
     uint32_t P = 0;
+    double nb_period = 0.0;  // period that sets nb (0: the last of `periods`)
     const fbls_bank* bank = nullptr;
     fbls_scan_stats st{};
     uint64_t nb = 0;
@@ -536,7 +537,8 @@ int scan_bands(fbls_ctx* ctx, const fbls_ready* r, std::vector<BandJob>& jobs, b
         if (j.P == 0 || j.bank->nd == 0) continue;
         double dmin = __builtin_huge_val();
         for (uint32_t i = 0; i < j.bank->nd; i++) dmin = rmin(dmin, j.bank->durations[i]);
-        j.nb = as_u64(std::ceil((double)j.bank->phase_oversample * j.periods[j.P - 1] / dmin));
+        const double p_nb = j.nb_period > 0.0 ? j.nb_period : j.periods[j.P - 1];
+        j.nb = as_u64(std::ceil((double)j.bank->phase_oversample * p_nb / dmin));
         if (j.nb < 8) j.nb = 8;
         if (j.nb > (1u << 24)) return fail(ctx, FBLS_ERR_ARGUMENT, "phase grid too large");
         j.coarse = j.bank->prescan_factor > 1 && j.nb / j.bank->prescan_factor >= 8;
@@ -801,8 +803,23 @@ int fbls_family_state(const double* time, const double* flux, const double* sigm
 int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
                        uint32_t nd, const fbls_config* cfg, fbls_row* rows_out, uint32_t capacity,
                        uint32_t* n_rows, uint64_t* grid_len, fbls_scan_stats* stats_out, uint32_t* n_bands) {
-    if (!ctx || !ready || !durations || !rho || !cfg || !n_rows) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    return fbls_signal_search_ranges(ctx, ready, durations, rho, nd, cfg, nullptr, 0, rows_out, capacity, n_rows,
+                                     grid_len, stats_out, n_bands);
+}
+
+int fbls_signal_search_ranges(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
+                              uint32_t nd, const fbls_config* cfg, const double* ranges, uint32_t n_ranges,
+                              fbls_row* rows_out, uint32_t capacity, uint32_t* n_rows, uint64_t* grid_len,
+                              fbls_scan_stats* stats_out, uint32_t* n_bands) {
+    if (!ctx || !ready || !durations || !rho || !cfg || !n_rows || (n_ranges && !ranges))
+        return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
     if (nd == 0) return fail(ctx, FBLS_ERR_ARGUMENT, "no durations");
+    auto kept = [&](double p) {
+        if (!n_ranges) return true;
+        for (uint32_t i = 0; i < n_ranges; i++)
+            if (p >= ranges[2 * i] && p < ranges[2 * i + 1]) return true;
+        return false;
+    };
     CK(cudaSetDevice(ctx->device), "set device");
     // Durations sorted with rho carried along (scan.rs:418-424).
     std::vector<std::pair<double, double>> ds(nd);
@@ -826,6 +843,7 @@ int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* dur
     // every band is scanned by scan_periods, the bands together (scan_bands).
     struct Band {
         std::vector<double> periods, durations, rho;
+        double nb_period = 0.0;  // the octave's last grid period (sets nb)
         fbls_bank bank;
     };
     std::vector<Band> bands;
@@ -836,7 +854,10 @@ int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* dur
         const double hi = lo * 2.0;
         Band b;
         for (double p : grid)
-            if (p >= lo && p < hi) b.periods.push_back(p);
+            if (p >= lo && p < hi) {
+                b.nb_period = p;
+                if (kept(p)) b.periods.push_back(p);
+            }
         for (auto& d : ds)
             if (d.first < lo / 4.0) {
                 b.durations.push_back(d.first);
@@ -863,6 +884,7 @@ int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* dur
         bank.prescan_fraction = cfg->prescan_fraction;
         jobs[i].periods = bands[i].periods.data();
         jobs[i].P = (uint32_t)bands[i].periods.size();
+        jobs[i].nb_period = bands[i].nb_period;
         jobs[i].bank = &bank;
     }
     std::vector<fbls_row> rows;
@@ -1068,8 +1090,8 @@ int fbls_search_batch(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbl
                 if (std::isfinite(s.period_max)) c.period_max = s.period_max;
                 fbls_scan_stats st[64];
                 uint32_t bands = 0;
-                rc = fbls_signal_search(wc, r, s.durations, s.rho, s.nd, &c, s.rows, s.capacity, &s.n_rows,
-                                        &s.grid_len, st, &bands);
+                rc = fbls_signal_search_ranges(wc, r, s.durations, s.rho, s.nd, &c, s.ranges, s.n_ranges, s.rows,
+                                               s.capacity, &s.n_rows, &s.grid_len, st, &bands);
                 for (uint32_t b = 0; rc == FBLS_OK && b < bands && b < 64; b++) s.templates += st[b].templates_scanned;
             }
             s.status = rc;

@@ -241,3 +241,142 @@ class Net:
 
     def load(self, flat: np.ndarray):
         self.w.copy_(self.torch.from_numpy(np.asarray(flat, dtype=np.float32)))
+
+
+# ---- data, training, proposal ------------------------------------------------
+
+def survey_stars(count: int, seed: int, max_sectors: int = 13, inject_fraction: float = 1.0):
+    """Seeded survey stars (the survey generator of synth), prepared:
+    [(FamilyState, period_max)] and the base SearchConfig."""
+    from . import api, synth
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < count:
+        c = synth.survey_star(rng, inject_fraction=inject_fraction)
+        if c.time[-1] - c.time[0] > 27.4 * max_sectors + 1.0:
+            continue
+        cfg = synth.survey_config(c)
+        out.append((api.prepared_family(c.time, c.flux, c.flux_err, cfg), cfg.period_max))
+    return out, synth.survey_config(synth.survey_star(np.random.default_rng(0)))
+
+
+def top_band(rows: np.ndarray) -> int:
+    """Band of the exhaustive search's best row (-1 when it found none)."""
+    if rows.shape[0] == 0:
+        return -1
+    return band_of(float(rows[int(np.argmax(rows[:, 3])), 0]))
+
+
+def features(gpu, stars, devs) -> np.ndarray:
+    """(4, count, T_IN) float32, channel-major."""
+    x = np.zeros((MAP_CHANNELS, len(stars), T_IN), dtype=np.float32)
+    for i, ((st, pmax), dev) in enumerate(zip(stars, devs)):
+        x[:, i, :] = star_map(gpu, dev, st, pmax)
+    return x
+
+
+def train(net: Net, x: np.ndarray, y: np.ndarray, epochs: int = 30, batch: int = 128, lr: float = 2e-3,
+          seed: int = 0, log=None):
+    """Adam on the softmax cross-entropy of the band labels y (>= 0)."""
+    torch = net.torch
+    keep = np.nonzero(y >= 0)[0]
+    xs = torch.from_numpy(x[:, keep, :]).to(net.dev)
+    ys = torch.from_numpy(y[keep].astype(np.int32)).to(net.dev)
+    rng = np.random.default_rng(seed)
+    n = keep.shape[0]
+    for ep in range(epochs):
+        order = torch.from_numpy(rng.permutation(n)).to(net.dev)
+        total = 0.0
+        for s in range(0, n - batch + 1, batch):
+            idx = order[s:s + batch]
+            _, loss = net.forward(xs[:, idx, :], ys[idx])
+            net.backward(batch)
+            net.adam(lr * (0.5 * (1 + math.cos(math.pi * ep / epochs))))
+            total += loss.item()
+        if log:
+            log(f"epoch {ep} loss {total / max(1, n // batch):.4f}")
+
+
+def scores(net: Net, x: np.ndarray, batch: int = 256) -> np.ndarray:
+    """Band logits (count, BANDS)."""
+    torch = net.torch
+    out = []
+    for s in range(0, x.shape[1], batch):
+        xb = torch.from_numpy(np.ascontiguousarray(x[:, s:s + batch, :])).to(net.dev)
+        logits, _ = net.forward(xb)
+        out.append(logits[:xb.shape[1]].detach().cpu().numpy().copy())
+    return np.concatenate(out, axis=0)
+
+
+def recall_at(logits: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """recall[k-1] = fraction of labelled stars whose band is in the top k."""
+    keep = y >= 0
+    order = np.argsort(-logits[keep], axis=1)
+    hit = order == y[keep][:, None]
+    return np.cumsum(hit, axis=1).sum(axis=0) / max(1, keep.sum()) if keep.any() else np.ones(BANDS)
+
+
+def ranges_for(logits_row: np.ndarray, k: int) -> List[Tuple[float, float]]:
+    """Period ranges of the k best bands, merged where adjacent."""
+    best = sorted(np.argsort(-logits_row)[:k].tolist())
+    out: List[Tuple[float, float]] = []
+    for b in best:
+        lo, hi = band_range(b)
+        if out and abs(out[-1][1] - lo) < 1e-12 * hi:
+            out[-1] = (out[-1][0], hi)
+        else:
+            out.append((lo, hi))
+    if out:  # the outermost bands reach the grid ends
+        if best[0] == 0:
+            out[0] = (0.0, out[0][1])
+        if best[-1] == BANDS - 1:
+            out[-1] = (out[-1][0], float("inf"))
+    return out
+
+
+def main(argv=None):
+    """Trains the proposal network on exhaustive-search labels of seeded survey
+    stars and writes its weights and held-out recall:
+
+        python -m fbls_b200.proposal --train 6000 --test 1500 --out weights.npz
+    """
+    import argparse
+    import json
+    import time
+    from . import api
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--train", type=int, default=6000)
+    ap.add_argument("--test", type=int, default=1500)
+    ap.add_argument("--max-sectors", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--out", required=True)
+    args = ap.parse_args(argv)
+    t0 = time.time()
+    log = lambda m: print(f"[{time.time() - t0:7.1f} s] {m}", flush=True)
+    stars, cfg = survey_stars(args.train + args.test, args.seed, args.max_sectors)
+    log(f"prepared {len(stars)} stars")
+    with api.Gpu(0) as gpu:
+        devs = [gpu.upload(s) for s, _ in stars]
+        res = gpu.search_batch([s for s, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs,
+                               workers=args.workers)
+        y = np.array([top_band(r) for r, _, _ in res])
+        log(f"exhaustive labels: {int((y >= 0).sum())} of {len(y)} stars with a detection")
+        x = features(gpu, stars, devs)
+        log("coarse maps done")
+        net = Net(0, seed=args.seed)
+        ntr = args.train
+        train(net, x[:, :ntr], y[:ntr], epochs=args.epochs, log=log)
+        lt = scores(net, x[:, ntr:])
+        rec = recall_at(lt, y[ntr:])
+        log("held-out recall@k " + " ".join(f"{k + 1}:{r:.4f}" for k, r in enumerate(rec[:12])))
+        np.savez(args.out, weights=net.state_dict(), recall=rec, train=ntr, test=args.test, seed=args.seed,
+                 max_sectors=args.max_sectors, epochs=args.epochs)
+        print(json.dumps({"recall": rec.tolist(), "labelled_test": int((y[ntr:] >= 0).sum())}))
+        for d in devs:
+            d.free()
+
+
+if __name__ == "__main__":
+    main()

@@ -298,6 +298,17 @@ int fbls_nn_head_bwd(const float* Z, const float* wh, const float* dlogits, floa
 int fbls_nn_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
                  int t, void* stream);
 
+/* signal_search restricted to period ranges [lo, hi) given as n_ranges
+ * pairs (no counterpart in the reference; the proposal path's pruned search):
+ * the same octave bands, durations and nb as the full search (nb from each
+ * octave's last grid period), scanning only the grid periods inside a range,
+ * so its rows are exactly the full search's rows in those ranges. n_ranges = 0
+ * is fbls_signal_search. */
+int fbls_signal_search_ranges(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
+                              uint32_t nd, const fbls_config* cfg, const double* ranges, uint32_t n_ranges,
+                              fbls_row* rows_out, uint32_t capacity, uint32_t* n_rows, uint64_t* grid_len,
+                              fbls_scan_stats* stats_out, uint32_t* n_bands);
+
 /* ---- batched search (replaces the reference's per-device worker threads,
  * src/batch.rs:61-102, each running one star's search at a time) --------- */
 
@@ -326,6 +337,9 @@ typedef struct {
     uint64_t grid_len;
     uint64_t templates;
     int status;
+    /* optional: search only these period ranges (see fbls_signal_search_ranges) */
+    const double* ranges;
+    uint32_t n_ranges;
 } fbls_star;
 
 /* signal_search for every star of `stars` on the context's device, with

@@ -121,3 +121,21 @@ def test_proposal_net_training_reduces_loss(gpu):
         net.adam(3e-3)
     _, loss = net.forward(x, labels)
     assert loss.item() < 0.3 * first
+
+
+def test_ranged_search_rows_are_the_full_search_rows_in_range(gpu):
+    from fbls_b200 import proposal as pr
+    c, cfg = synth.single_sector(), synth.single_sector_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    full, glen, _ = gpu.signal_search(st, cfg)
+    assert full.shape[0] > 0
+    ranges = pr.ranges_for(np.arange(pr.BANDS, dtype=float)[::-1] * 0 + np.eye(pr.BANDS)[[3, 12, 13, 20]].sum(0), 4)
+    part, glen2, _ = gpu.signal_search(st, cfg, ranges=ranges)
+    inside = np.zeros(full.shape[0], dtype=bool)
+    for lo, hi in ranges:
+        inside |= (full[:, 0] >= lo) & (full[:, 0] < hi)
+    assert glen2 == glen
+    assert np.array_equal(part, full[inside])
+    # the same through the batch runner
+    res = gpu.search_batch([st], cfg, period_max=[cfg.period_max], ranges=[ranges], workers=1)
+    assert np.array_equal(res[0][0], full[inside])
