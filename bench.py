@@ -413,6 +413,74 @@ def run_survey(args):
         torch.distributed.destroy_process_group()
 
 
+def run_proposal(args):
+    """Proposal-pruned search against the exhaustive search on the survey
+    workload: both timed on the same resident stars (host clock around the
+    device-synchronised batches), the top-1 recall of the pruned search (its
+    best row is the exhaustive best row), and the stars/s ratio."""
+    import torch
+    from fbls_b200 import api
+    from fbls_b200 import proposal as pr
+    torch.cuda.set_device(0)
+    stars, cfg = _survey(args.stars, 1000)
+    pstars = [(s, p) for _, s, p in stars]
+    gpu = api.Gpu(0)
+    devs = [gpu.upload(s) for s, _ in pstars]
+    net = pr.load_net(0)
+    states, pmax = [s for s, _ in pstars], [p for _, p in pstars]
+
+    def exhaustive():
+        return gpu.search_batch(states, cfg, period_max=pmax, devs=devs, workers=args.batch_workers)
+
+    def proposed():
+        return pr.search_proposed(gpu, net, pstars, devs, cfg, k=args.bands, workers=args.batch_workers)
+
+    for _ in range(args.warmup):
+        exhaustive()
+        proposed()
+    gc.collect()
+    gc.disable()
+    t_ex, t_pr = [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        full = exhaustive()
+        t_ex.append(time.perf_counter() - t0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pruned, logits = proposed()
+        t_pr.append(time.perf_counter() - t0)
+    gc.enable()
+    hits = labelled = 0
+    for (fr, _, _), (pr_rows, _, _) in zip(full, pruned):
+        if fr.shape[0] == 0:
+            continue
+        labelled += 1
+        best = fr[int(np.argmax(fr[:, 3]))]
+        if pr_rows.shape[0] and np.array_equal(pr_rows[int(np.argmax(pr_rows[:, 3]))], best):
+            hits += 1
+    tex, tpr = sum(t_ex) / len(t_ex), sum(t_pr) / len(t_pr)
+    rec = np.load(pr.WEIGHTS)
+    out = {
+        "metric": METRIC, "value": args.stars / tpr, "unit": "stars/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * tpr, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 search, bf16 network", "data": "synthetic",
+        "config": {"workload": f"proposal: {args.stars} seeded survey stars (as --workload survey), the "
+                               f"exhaustive search of the {args.bands} best of {pr.BANDS} log-period bands",
+                   "batch_workers": args.batch_workers, "bands_searched": args.bands},
+        "exhaustive_stars_per_s": args.stars / tex,
+        "proposal_stars_per_s": args.stars / tpr,
+        "speedup": tex / tpr,
+        "top1_recall": hits / max(labelled, 1), "stars_with_detection": labelled,
+        "network_heldout_recall_at_k": float(rec["recall"][args.bands - 1]),
+        "step_ms": {"exhaustive": [round(1e3 * t, 1) for t in t_ex], "proposal": [round(1e3 * t, 1) for t in t_pr]},
+    }
+    print(json.dumps(out))
+    for d in devs:
+        d.free()
+    gpu.close()
+
+
 def run_precision_report(args):
     """The reference's mixed mode (f32 pre-rank from (hi, lo) pairs, f64
     winner) against f64 ranking throughout, on every period of every band at
@@ -486,9 +554,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fbls_b200", choices=["fbls_b200", "reference"])
-    ap.add_argument("--workload", default="multi_sector", choices=["multi_sector", "single_sector", "survey"])
+    ap.add_argument("--workload", default="multi_sector", choices=["multi_sector", "single_sector", "survey", "proposal"])
     ap.add_argument("--stars", type=int, default=512, help="survey workload: stars per GPU")
     ap.add_argument("--batch-workers", type=int, default=4, help="survey workload: host worker threads")
+    ap.add_argument("--bands", type=int, default=3, help="proposal workload: log-period bands searched per star")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -500,6 +569,8 @@ def main():
         run_reference(args)
     elif args.workload == "survey":
         run_survey(args)
+    elif args.workload == "proposal":
+        run_proposal(args)
     else:
         run_gpu(args)
 

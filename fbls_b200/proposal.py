@@ -334,6 +334,28 @@ def ranges_for(logits_row: np.ndarray, k: int) -> List[Tuple[float, float]]:
     return out
 
 
+WEIGHTS = __import__("pathlib").Path(__file__).resolve().parent / "data" / "proposal_weights.npz"
+
+
+def load_net(device: int = 0, path=None) -> Net:
+    """The network with the committed weights (trained by main() below)."""
+    net = Net(device)
+    net.load(np.load(path or WEIGHTS)["weights"])
+    return net
+
+
+def search_proposed(gpu, net: Net, stars, devs, cfg, k: int = 3, workers: int = 8):
+    """The proposal-pruned search of many stars: coarse map, band scores, then
+    the exhaustive search of each star's k best bands only (its rows are the
+    full search's rows in those bands). Returns the batch results and logits."""
+    x = features(gpu, stars, devs)
+    logits = scores(net, x)
+    ranges = [ranges_for(l, k) for l in logits]
+    res = gpu.search_batch([s for s, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs,
+                           workers=workers, ranges=ranges)
+    return res, logits
+
+
 def main(argv=None):
     """Trains the proposal network on exhaustive-search labels of seeded survey
     stars and writes its weights and held-out recall:
