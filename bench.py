@@ -450,6 +450,7 @@ def run_proposal(args):
         t0 = time.perf_counter()
         pruned, logits = proposed()
         t_pr.append(time.perf_counter() - t0)
+        parts = dict(pr.search_proposed.last_ms)
     gc.enable()
     hits = labelled = 0
     for (fr, _, _), (pr_rows, _, _) in zip(full, pruned):
@@ -474,6 +475,7 @@ def run_proposal(args):
         "top1_recall": hits / max(labelled, 1), "stars_with_detection": labelled,
         "network_heldout_recall_at_k": float(rec["recall"][args.bands - 1]),
         "step_ms": {"exhaustive": [round(1e3 * t, 1) for t in t_ex], "proposal": [round(1e3 * t, 1) for t in t_pr]},
+        "proposal_ms_last_step": {k: round(v, 1) for k, v in parts.items()},
     }
     print(json.dumps(out))
     for d in devs:

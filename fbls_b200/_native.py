@@ -63,6 +63,20 @@ class Star(C.Structure):
     ]
 
 
+class MapJob(C.Structure):
+    _fields_ = [
+        ("ready", C.c_void_p),
+        ("periods", C.POINTER(C.c_double)),
+        ("P", C.c_uint32),
+        ("durations", C.POINTER(C.c_double)),
+        ("rho", C.POINTER(C.c_double)),
+        ("nd", C.c_uint32),
+        ("oversample", C.c_double),
+        ("out", C.POINTER(C.c_float)),
+        ("status", C.c_int),
+    ]
+
+
 class ScanStats(C.Structure):
     _fields_ = [
         ("periods", C.c_uint64),
@@ -174,6 +188,7 @@ SIGNATURES = {
     "fbls_search_batch": (C.c_int, [C.c_void_p, C.POINTER(Star), C.c_uint32, C.POINTER(Config), C.c_uint32]),
     "fbls_coarse_map": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, C.c_uint32, c_double_p, c_double_p, C.c_uint32,
                                   C.c_double, C.POINTER(C.c_float)]),
+    "fbls_coarse_map_batch": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, C.c_uint32]),
     # proposal network kernels: device pointers passed as integers
     "fbls_nn_gemm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int] + [C.c_longlong] * 9
                      + [C.c_int, C.c_float, C.c_float, C.c_void_p]),

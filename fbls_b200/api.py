@@ -242,6 +242,25 @@ class Gpu:
                                              out.ctypes.data_as(C.POINTER(C.c_float))))
         return out
 
+    def coarse_map_batch(self, devs: Sequence[DeviceReady], periods: Sequence, durations: Sequence, rho: Sequence,
+                         oversample: float = 2.0, workers: int = 8) -> List[np.ndarray]:
+        """coarse_map of many uploaded families on worker threads."""
+        count = len(devs)
+        jobs = (N.MapJob * max(count, 1))()
+        keep, outs = [], []
+        for i in range(count):
+            p, d, r = _f64(periods[i]), _f64(durations[i]), _f64(rho[i])
+            o = np.empty((p.shape[0], d.shape[0]), dtype=np.float32)
+            keep += [p, d, r]
+            outs.append(o)
+            j = jobs[i]
+            j.ready, j.periods, j.P = devs[i].handle, _dptr(p), p.shape[0]
+            j.durations, j.rho, j.nd = _dptr(d), _dptr(r), d.shape[0]
+            j.oversample = float(oversample)
+            j.out = o.ctypes.data_as(C.POINTER(C.c_float))
+        self._check(self.lib.fbls_coarse_map_batch(self.ctx, jobs, count, int(workers)))
+        return outs
+
     def search_batch(self, states: Sequence[FamilyState], cfg: SearchConfig, period_max: Optional[Sequence[float]] = None,
                      devs: Optional[Sequence[DeviceReady]] = None, workers: int = 4,
                      ranges: Optional[Sequence[Optional[Sequence[Tuple[float, float]]]]] = None):
@@ -253,6 +272,15 @@ class Gpu:
         count = len(states)
         stars = (N.Star * max(count, 1))()
         keep = []
+        # One row buffer for the batch, room for every grid period of each star
+        # (rows cannot outnumber them); only the rows written are touched.
+        caps = []
+        for i, s in enumerate(states):
+            pm = math.nan if period_max is None else float(period_max[i])
+            c1 = dataclasses.replace(cfg, period_max=pm) if math.isfinite(pm) else cfg
+            caps.append(max(1, _grid_count(s, c1)))
+        offs = np.concatenate([[0], np.cumsum(caps)])
+        rows_all = np.empty((int(offs[-1]), 5))
         for i, s in enumerate(states):
             st = stars[i]
             if devs is not None:
@@ -268,12 +296,8 @@ class Gpu:
             st.durations, st.rho, st.nd = _dptr(d), _dptr(r), len(d)
             pm = math.nan if period_max is None else float(period_max[i])
             st.period_max = pm
-            c1 = dataclasses.replace(cfg, period_max=pm) if math.isfinite(pm) else cfg
-            cap = max(1, _grid_count(s, c1))
-            rows = (N.Row * cap)()
-            keep.append(rows)
-            st.rows = C.cast(rows, C.POINTER(N.Row))
-            st.capacity = cap
+            st.rows = rows_all[offs[i]:].ctypes.data_as(C.POINTER(N.Row))
+            st.capacity = caps[i]
             if ranges is not None and ranges[i]:
                 rg = _f64(np.asarray(ranges[i], dtype=np.float64).reshape(-1))
                 keep.append(rg)
@@ -284,7 +308,7 @@ class Gpu:
         out = []
         for i in range(count):
             st = stars[i]
-            out.append((_rows_array(st.rows, st.n_rows), int(st.grid_len), int(st.templates)))
+            out.append((rows_all[offs[i]:offs[i] + st.n_rows].copy(), int(st.grid_len), int(st.templates)))
         return out
 
     def signal_search(self, state: FamilyState, cfg: SearchConfig, dev: Optional[DeviceReady] = None,
@@ -297,17 +321,18 @@ class Gpu:
         try:
             c, keep = _config(cfg)
             d, r = _f64(state.durations), _f64(state.rho)
-            cap = max(1, _grid_count(state, cfg))
-            rows = (N.Row * cap)()
+            cap = max(1, _grid_count(state, cfg))  # rows cannot outnumber grid periods
             n = C.c_uint32(0)
             glen = C.c_uint64(0)
             stats = (N.ScanStats * 64)()
             nb = C.c_uint32(0)
             rg = _f64(np.asarray(ranges if ranges else [], dtype=np.float64).reshape(-1))
+            rows = np.empty((cap, 5))  # not touched beyond the rows written
             self._check(self.lib.fbls_signal_search_ranges(self.ctx, dev.handle, _dptr(d), _dptr(r), len(d),
-                                                           C.byref(c), _dptr(rg), rg.shape[0] // 2, rows, cap,
-                                                           C.byref(n), C.byref(glen), stats, C.byref(nb)))
-            return _rows_array(rows, n.value), int(glen.value), [stats[i].as_dict() for i in range(nb.value)]
+                                                           C.byref(c), _dptr(rg), rg.shape[0] // 2,
+                                                           rows.ctypes.data_as(C.POINTER(N.Row)), cap, C.byref(n),
+                                                           C.byref(glen), stats, C.byref(nb)))
+            return rows[:n.value].copy(), int(glen.value), [stats[i].as_dict() for i in range(nb.value)]
         finally:
             if own:
                 dev.free()

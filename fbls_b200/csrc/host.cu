@@ -892,8 +892,9 @@ int fbls_signal_search_ranges(fbls_ctx* ctx, const fbls_ready* ready, const doub
     if (rc) return rc;
     for (size_t i = 0; i < jobs.size() && stats_out && i < 64; i++) stats_out[i] = jobs[i].st;
     const uint32_t n_scanned = (uint32_t)jobs.size();
-    if (rows.size() > capacity) return fail(ctx, FBLS_ERR_ARGUMENT, "row capacity too small");
-    std::memcpy(rows_out, rows.data(), rows.size() * sizeof(fbls_row));
+    // At most `capacity` rows are written; n_rows is the full count, so a
+    // caller that sees n_rows > capacity can ask again with room for all.
+    if (rows_out) std::memcpy(rows_out, rows.data(), std::min<size_t>(rows.size(), capacity) * sizeof(fbls_row));
     *n_rows = (uint32_t)rows.size();
     if (n_bands) *n_bands = n_scanned;
     return FBLS_OK;
@@ -1115,6 +1116,44 @@ int fbls_search_batch(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbl
     }
     for (uint32_t i = 0; i < count; i++)
         if (stars[i].status) return fail(ctx, stars[i].status, "star " + std::to_string(i) + ": " + errors[i]);
+    return FBLS_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// Coarse maps of many uploaded families on the batch worker contexts (the
+// proposal path's first step for a batch of stars).
+int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uint32_t workers) {
+    if (!ctx || (count && !jobs)) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (count == 0) return FBLS_OK;
+    workers = std::max(1u, std::min({workers, count, 64u}));
+    CK(cudaSetDevice(ctx->device), "set device");
+    while (ctx->workers.size() < workers) {
+        int status = FBLS_OK;
+        fbls_ctx* w = fbls_create(ctx->device, &status);
+        if (!w) return fail(ctx, status ? status : FBLS_ERR_CUDA, "batch worker context");
+        ctx->workers.push_back(w);
+    }
+    std::atomic<uint32_t> next{0};
+    std::vector<std::string> errors(count);
+    auto work = [&](fbls_ctx* wc) {
+        if (cudaSetDevice(wc->device) != cudaSuccess) return;
+        for (;;) {
+            const uint32_t i = next.fetch_add(1);
+            if (i >= count) break;
+            fbls_map_job& j = jobs[i];
+            j.status = fbls_coarse_map(wc, j.ready, j.periods, j.P, j.durations, j.rho, j.nd, j.oversample, j.out);
+            if (j.status) errors[i] = wc->error;
+        }
+    };
+    std::vector<std::thread> threads;
+    for (uint32_t k = 1; k < workers; k++) threads.emplace_back(work, ctx->workers[k]);
+    work(ctx->workers[0]);
+    for (std::thread& t : threads) t.join();
+    for (uint32_t i = 0; i < count; i++)
+        if (jobs[i].status) return fail(ctx, jobs[i].status, "map " + std::to_string(i) + ": " + errors[i]);
     return FBLS_OK;
 }
 

@@ -54,23 +54,36 @@ def map_bank(state) -> Tuple[np.ndarray, np.ndarray]:
     return d[idx], np.asarray(state.rho, dtype=np.float64)[idx]
 
 
-def star_map(gpu, dev, state, period_max: float) -> np.ndarray:
-    """(4, T_IN) features of one star: log1p of the coarse map, standardised per
-    duration over the periods the star's search covers, 0 elsewhere."""
+def map_plan(state, period_max: float):
+    """The map periods a star's search covers (mask over map_periods()) and
+    the map's durations and rho."""
     p = map_periods()
-    d, r = map_bank(state)
     lo = max(PMIN, 4.0 * float(np.min(state.durations)) * (1.0 + 1e-9))
     hi = min(period_max, float(state.time[-1]))
     keep = (p >= lo) & (p <= hi)
+    d, r = map_bank(state)
+    return keep, d, r
+
+
+def map_features(m: np.ndarray, keep: np.ndarray) -> np.ndarray:
+    """(4, T_IN) features: log1p of the coarse map, standardised per duration
+    over the covered periods, 0 elsewhere."""
     x = np.zeros((MAP_CHANNELS, T_IN), dtype=np.float32)
     if keep.sum() < 8:
         return x
-    m = gpu.coarse_map(dev, p[keep], d, r, oversample=2.0)
     f = np.log1p(np.maximum(m, 0.0)).T
     mu = f.mean(axis=1, keepdims=True)
     sd = f.std(axis=1, keepdims=True) + 1e-3
     x[:, keep] = (f - mu) / sd
     return x
+
+
+def star_map(gpu, dev, state, period_max: float) -> np.ndarray:
+    """(4, T_IN) features of one star."""
+    keep, d, r = map_plan(state, period_max)
+    if keep.sum() < 8:
+        return np.zeros((MAP_CHANNELS, T_IN), dtype=np.float32)
+    return map_features(gpu.coarse_map(dev, map_periods()[keep], d, r, oversample=2.0), keep)
 
 
 class Net:
@@ -267,11 +280,17 @@ def top_band(rows: np.ndarray) -> int:
     return band_of(float(rows[int(np.argmax(rows[:, 3])), 0]))
 
 
-def features(gpu, stars, devs) -> np.ndarray:
-    """(4, count, T_IN) float32, channel-major."""
+def features(gpu, stars, devs, workers: int = 8) -> np.ndarray:
+    """(4, count, T_IN) float32, channel-major; the maps run on the batch
+    worker threads."""
     x = np.zeros((MAP_CHANNELS, len(stars), T_IN), dtype=np.float32)
-    for i, ((st, pmax), dev) in enumerate(zip(stars, devs)):
-        x[:, i, :] = star_map(gpu, dev, st, pmax)
+    plans = [map_plan(st, pmax) for st, pmax in stars]
+    todo = [i for i, (keep, _, _) in enumerate(plans) if keep.sum() >= 8]
+    p = map_periods()
+    maps = gpu.coarse_map_batch([devs[i] for i in todo], [p[plans[i][0]] for i in todo],
+                                [plans[i][1] for i in todo], [plans[i][2] for i in todo], 2.0, workers)
+    for i, m in zip(todo, maps):
+        x[:, i, :] = map_features(m, plans[i][0])
     return x
 
 
@@ -348,11 +367,17 @@ def search_proposed(gpu, net: Net, stars, devs, cfg, k: int = 3, workers: int = 
     """The proposal-pruned search of many stars: coarse map, band scores, then
     the exhaustive search of each star's k best bands only (its rows are the
     full search's rows in those bands). Returns the batch results and logits."""
-    x = features(gpu, stars, devs)
+    import time
+    t0 = time.perf_counter()
+    x = features(gpu, stars, devs, workers)
+    t1 = time.perf_counter()
     logits = scores(net, x)
     ranges = [ranges_for(l, k) for l in logits]
+    t2 = time.perf_counter()
     res = gpu.search_batch([s for s, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs,
                            workers=workers, ranges=ranges)
+    t3 = time.perf_counter()
+    search_proposed.last_ms = {"maps": 1e3 * (t1 - t0), "network": 1e3 * (t2 - t1), "search": 1e3 * (t3 - t2)}
     return res, logits
 
 

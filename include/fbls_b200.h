@@ -249,8 +249,9 @@ int fbls_family_state(const double* time, const double* flux, const double* sigm
                       uint32_t error_len);
 
 /* signal_search (scan.rs:413-473) for one family: octave bands over the
- * family's grid. rows_out holds capacity rows (the grid length suffices);
- * stats_out holds up to 64 bands. */
+ * family's grid. At most `capacity` rows are written to rows_out and
+ * *n_rows is the number found (more than capacity: ask again with room for
+ * all; the grid length always suffices); stats_out holds up to 64 bands. */
 int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
                        uint32_t nd, const fbls_config* cfg, fbls_row* rows_out, uint32_t capacity,
                        uint32_t* n_rows, uint64_t* grid_len, fbls_scan_stats* stats_out, uint32_t* n_bands);
@@ -267,6 +268,25 @@ int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* dur
  * duration)). */
 int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* ready, const double* periods, uint32_t P,
                     const double* durations, const double* rho, uint32_t nd, double oversample, float* out);
+
+/* One coarse map of a batch: inputs as fbls_coarse_map, out (P x nd floats,
+ * caller-owned host memory) and the job's status. */
+typedef struct {
+    const fbls_ready* ready;
+    const double* periods;
+    uint32_t P;
+    const double* durations;
+    const double* rho;
+    uint32_t nd;
+    double oversample;
+    float* out;
+    int status;
+} fbls_map_job;
+
+/* Coarse maps of many uploaded families on `workers` host threads with their
+ * own streams (the contexts fbls_search_batch keeps). Returns 0 or the first
+ * failing job's status ("map i: " message). */
+int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uint32_t workers);
 
 /* Proposal network kernels. Every pointer is device memory; `stream` is a
  * cudaStream_t (NULL: the legacy stream). Activations are f32 laid out
@@ -316,8 +336,9 @@ int fbls_signal_search_ranges(fbls_ctx* ctx, const fbls_ready* ready, const doub
  * family in host memory (time, v, w, n and its scalars) that the worker
  * uploads itself; the family's durations and rho; period_max overrides
  * cfg->period_max when finite (SearchConfig per star). Outputs: rows
- * (caller-owned, capacity of them: the star's grid length suffices), the
- * row count, grid length, templates scanned and the star's status. */
+ * (caller-owned, capacity of them; n_rows counts every row found, so
+ * n_rows > capacity means the rows were cut short), the row count, grid
+ * length, templates scanned and the star's status. */
 typedef struct {
     const fbls_ready* ready;
     const double* time;

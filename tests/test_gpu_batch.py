@@ -45,3 +45,28 @@ def test_batch_reports_the_failing_star(gpu):
     states = [stars[0][0], short, stars[2][0]]
     with pytest.raises(api.FblsError, match="star 1: at least six observations"):
         gpu.search_batch(states, stars[0][1], period_max=[cfg.period_max for _, cfg in stars], workers=2)
+
+
+def test_signal_search_reports_every_row_when_the_buffer_is_short(gpu):
+    """With room for fewer rows than it finds, signal_search writes as many as
+    fit and reports the full count."""
+    import ctypes as C
+    from fbls_b200 import _native as N
+    c, cfg = synth.single_sector(), synth.single_sector_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    want = gpu.signal_search(st, cfg)[0]
+    assert want.shape[0] > 3
+    dev = gpu.upload(st)
+    cc, keep = api._config(cfg)
+    d, r = np.ascontiguousarray(st.durations), np.ascontiguousarray(st.rho)
+    rows = np.full((2, 5), -1.0)
+    n, glen, nb = C.c_uint32(0), C.c_uint64(0), C.c_uint32(0)
+    stats = (N.ScanStats * 64)()
+    rc = gpu.lib.fbls_signal_search(gpu.ctx, dev.handle, d.ctypes.data_as(N.c_double_p),
+                                    r.ctypes.data_as(N.c_double_p), len(d), C.byref(cc),
+                                    rows.ctypes.data_as(C.POINTER(N.Row)), 2, C.byref(n), C.byref(glen), stats,
+                                    C.byref(nb))
+    assert rc == 0
+    assert n.value == want.shape[0]
+    assert np.array_equal(rows, want[:2])
+    dev.free()

@@ -139,3 +139,14 @@ def test_ranged_search_rows_are_the_full_search_rows_in_range(gpu):
     # the same through the batch runner
     res = gpu.search_batch([st], cfg, period_max=[cfg.period_max], ranges=[ranges], workers=1)
     assert np.array_equal(res[0][0], full[inside])
+
+
+def test_coarse_map_batch_matches_single_maps(gpu):
+    from fbls_b200 import proposal as pr
+    stars, cfg = pr.survey_stars(5, seed=3, max_sectors=2)
+    devs = [gpu.upload(s) for s, _ in stars]
+    x = pr.features(gpu, stars, devs, workers=3)
+    for i, ((st, pmax), dev) in enumerate(zip(stars, devs)):
+        assert np.array_equal(x[:, i, :], pr.star_map(gpu, dev, st, pmax))
+    for d in devs:
+        d.free()
