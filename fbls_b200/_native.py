@@ -72,6 +72,7 @@ class MapJob(C.Structure):
         ("rho", C.POINTER(C.c_double)),
         ("nd", C.c_uint32),
         ("oversample", C.c_double),
+        ("bin_days", C.c_double),
         ("out", C.POINTER(C.c_float)),
         ("status", C.c_int),
     ]
@@ -187,7 +188,7 @@ SIGNATURES = {
                                             c_uint32_p, c_uint64_p, C.POINTER(ScanStats), c_uint32_p]),
     "fbls_search_batch": (C.c_int, [C.c_void_p, C.POINTER(Star), C.c_uint32, C.POINTER(Config), C.c_uint32]),
     "fbls_coarse_map": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, C.c_uint32, c_double_p, c_double_p, C.c_uint32,
-                                  C.c_double, C.POINTER(C.c_float)]),
+                                  C.c_double, C.c_double, C.POINTER(C.c_float)]),
     "fbls_coarse_map_batch": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, C.c_uint32]),
     # proposal network kernels: device pointers passed as integers
     "fbls_nn_gemm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int] + [C.c_longlong] * 9

@@ -233,17 +233,18 @@ class Gpu:
                                                C.byref(n), C.byref(st)))
         return _rows_array(rows, n.value), st.as_dict()
 
-    def coarse_map(self, dev: DeviceReady, periods, durations, rho, oversample: float = 2.0) -> np.ndarray:
+    def coarse_map(self, dev: DeviceReady, periods, durations, rho, oversample: float = 2.0,
+                   bin_days: float = 0.0) -> np.ndarray:
         """Best box score over phases per (period, duration): P x nd float32."""
         p, d, r = _f64(periods), _f64(durations), _f64(rho)
         out = np.empty((p.shape[0], d.shape[0]), dtype=np.float32)
         self._check(self.lib.fbls_coarse_map(self.ctx, dev.handle, _dptr(p), p.shape[0], _dptr(d), _dptr(r),
-                                             d.shape[0], float(oversample),
+                                             d.shape[0], float(oversample), float(bin_days),
                                              out.ctypes.data_as(C.POINTER(C.c_float))))
         return out
 
     def coarse_map_batch(self, devs: Sequence[DeviceReady], periods: Sequence, durations: Sequence, rho: Sequence,
-                         oversample: float = 2.0, workers: int = 8) -> List[np.ndarray]:
+                         oversample: float = 2.0, workers: int = 8, bin_days: float = 0.0) -> List[np.ndarray]:
         """coarse_map of many uploaded families on worker threads."""
         count = len(devs)
         jobs = (N.MapJob * max(count, 1))()
@@ -257,6 +258,7 @@ class Gpu:
             j.ready, j.periods, j.P = devs[i].handle, _dptr(p), p.shape[0]
             j.durations, j.rho, j.nd = _dptr(d), _dptr(r), d.shape[0]
             j.oversample = float(oversample)
+            j.bin_days = float(bin_days)
             j.out = o.ctypes.data_as(C.POINTER(C.c_float))
         self._check(self.lib.fbls_coarse_map_batch(self.ctx, jobs, count, int(workers)))
         return outs

@@ -59,6 +59,7 @@ struct fbls_ctx {
     DevBuf pass_in, pass_out;  // per session: every pass's inputs and outputs
     DevBuf evidence, fault;
     DevBuf family;  // observations of the star a batch worker is searching
+    DevBuf mapbin;  // time-binned observations of a coarse map
     PinBuf pin_up, pin_down, pin_down2;  // staging of a session's upload and download (two sessions in flight)
     std::vector<fbls_ctx*> workers;  // fbls_search_batch worker contexts, kept for reuse
 };
@@ -661,7 +662,7 @@ void fbls_destroy(fbls_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf* bufs[] = {&ctx->cum,     &ctx->cum32,    &ctx->hist,     &ctx->parts, &ctx->keys,  &ctx->tflags,
-                      &ctx->pass_in, &ctx->pass_out, &ctx->evidence, &ctx->fault, &ctx->family};
+                      &ctx->pass_in, &ctx->pass_out, &ctx->evidence, &ctx->fault, &ctx->family, &ctx->mapbin};
     for (DevBuf* b : bufs) release(*b);
     for (PinBuf* b : {&ctx->pin_up, &ctx->pin_down, &ctx->pin_down2})
         if (b->ptr) cudaFreeHost(b->ptr);
@@ -921,9 +922,11 @@ int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* du
 // Coarse periodogram of a family for the proposal network: periods are cut
 // into octave groups [lo, 2 lo), each folded at nb = max(8, ceil(oversample *
 // (group's longest period) / shortest duration)) and scanned by k_box_map.
-int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* ready, const double* periods, uint32_t P,
-                    const double* durations, const double* rho, uint32_t nd, double oversample, float* out) {
-    if (!ctx || !ready || !periods || !durations || !rho || !out) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* family, const double* periods, uint32_t P,
+                    const double* durations, const double* rho, uint32_t nd, double oversample, double bin_days,
+                    float* out) {
+    if (!ctx || !family || !periods || !durations || !rho || !out) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (!(bin_days >= 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "bin_days must not be negative");
     if (nd < 1 || nd > (uint32_t)MAP_MAX_DURATIONS) return fail(ctx, FBLS_ERR_ARGUMENT, "1 to 8 map durations");
     if (P == 0) return FBLS_OK;
     if (!(oversample > 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "oversample must be positive");
@@ -936,6 +939,47 @@ int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* ready, const double* period
         dmin = rmin(dmin, durations[i]);
     }
     CK(cudaSetDevice(ctx->device), "set device");
+    // Optional time bins: observations whose floor((t - t0) / bin_days) agree
+    // are summed (v, w) at their mean time, into the context's map buffer.
+    fbls_ready binned;
+    const fbls_ready* ready = family;
+    if (bin_days > 0.0) {
+        const std::vector<double>& t = family->time_host;
+        std::vector<int> starts;
+        std::vector<double>& tb = binned.time_host;
+        for (uint32_t i = 0; i < family->n;) {
+            const double b = std::floor((t[i] - t[0]) / bin_days);
+            uint32_t j = i;
+            double sum = 0.0;
+            while (j < family->n && std::floor((t[j] - t[0]) / bin_days) == b) sum += t[j++];
+            starts.push_back((int)i);
+            tb.push_back(sum / (double)(j - i));
+            i = j;
+        }
+        starts.push_back((int)family->n);
+        const uint32_t nbins = (uint32_t)tb.size();
+        const size_t stride = fold_field_stride(nbins);
+        CK(ensure(ctx->mapbin, 3 * stride * sizeof(double) + align256((nbins + 1) * sizeof(int))), "workspace");
+        double* base = static_cast<double*>(ctx->mapbin.ptr);
+        int* d_starts = reinterpret_cast<int*>(base + 3 * stride);
+        cudaStream_t s = ctx->stream;
+        CK(cudaMemsetAsync(base, 0, 3 * stride * sizeof(double), s), "workspace");
+        CK(cudaMemcpyAsync(base, tb.data(), nbins * sizeof(double), cudaMemcpyHostToDevice, s), "upload bins");
+        CK(cudaMemcpyAsync(d_starts, starts.data(), starts.size() * sizeof(int), cudaMemcpyHostToDevice, s),
+           "upload bins");
+        CK(launch_bin_fields(family->v, family->w, d_starts, (int)nbins, base + stride, base + 2 * stride, s), "bins");
+        binned.ctx = ctx;
+        binned.time = base;
+        binned.v = base + stride;
+        binned.w = base + 2 * stride;
+        binned.n = nbins;
+        binned.baseline_norm = family->baseline_norm;
+        binned.origin = family->origin;
+        binned.residual_energy = family->residual_energy;
+        binned.t_last = tb.back();
+        binned.owned = false;
+        ready = &binned;
+    }
     struct Group {
         uint32_t i0, count, nb;
         FoldShape shape;
@@ -1144,7 +1188,8 @@ int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uin
             const uint32_t i = next.fetch_add(1);
             if (i >= count) break;
             fbls_map_job& j = jobs[i];
-            j.status = fbls_coarse_map(wc, j.ready, j.periods, j.P, j.durations, j.rho, j.nd, j.oversample, j.out);
+            j.status = fbls_coarse_map(wc, j.ready, j.periods, j.P, j.durations, j.rho, j.nd, j.oversample,
+                                       j.bin_days, j.out);
             if (j.status) errors[i] = wc->error;
         }
     };

@@ -120,5 +120,7 @@ cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t 
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream);
 cudaError_t launch_merge(const MergeArgs& a, cudaStream_t stream);
 cudaError_t launch_box_map(const MapArgs& a, int periods, cudaStream_t stream);
+cudaError_t launch_bin_fields(const double* v, const double* w, const int* starts, int nbins, double* vb, double* wb,
+                              cudaStream_t stream);
 
 }  // namespace fbls

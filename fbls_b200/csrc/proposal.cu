@@ -71,6 +71,29 @@ __global__ void __launch_bounds__(MAP_THREADS) k_box_map(MapArgs a) {
     }
 }
 
+// Sums of v and w over runs of observations (the time bins of a coarse map):
+// bin b covers observations [starts[b], starts[b + 1]).
+__global__ void k_bin_fields(const double* v, const double* w, const int* starts, int nbins, double* vb,
+                             double* wb) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbins; b += gridDim.x * blockDim.x) {
+        double sv = 0.0, sw = 0.0;
+        for (int i = starts[b]; i < starts[b + 1]; i++) {
+            sv += v[i];
+            sw += w[i];
+        }
+        vb[b] = sv;
+        wb[b] = sw;
+    }
+}
+
+cudaError_t launch_bin_fields(const double* v, const double* w, const int* starts, int nbins, double* vb, double* wb,
+                              cudaStream_t stream) {
+    if (nbins < 1) return cudaErrorInvalidValue;
+    const int blocks = (nbins + 255) / 256;
+    k_bin_fields<<<blocks < 4096 ? blocks : 4096, 256, 0, stream>>>(v, w, starts, nbins, vb, wb);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_box_map(const MapArgs& a, int periods, cudaStream_t stream) {
     if (a.nd < 1 || a.nd > MAP_MAX_DURATIONS || a.nb < 2 || periods < 1) return cudaErrorInvalidValue;
     k_box_map<<<periods, MAP_THREADS, 0, stream>>>(a);

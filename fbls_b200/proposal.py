@@ -78,12 +78,13 @@ def map_features(m: np.ndarray, keep: np.ndarray) -> np.ndarray:
     return x
 
 
-def star_map(gpu, dev, state, period_max: float) -> np.ndarray:
-    """(4, T_IN) features of one star."""
+def star_map(gpu, dev, state, period_max: float, bin_days: float = 0.0) -> np.ndarray:
+    """(4, T_IN) features of one star (observations summed over bins of
+    bin_days first when it is positive)."""
     keep, d, r = map_plan(state, period_max)
     if keep.sum() < 8:
         return np.zeros((MAP_CHANNELS, T_IN), dtype=np.float32)
-    return map_features(gpu.coarse_map(dev, map_periods()[keep], d, r, oversample=2.0), keep)
+    return map_features(gpu.coarse_map(dev, map_periods()[keep], d, r, oversample=2.0, bin_days=bin_days), keep)
 
 
 class Net:
@@ -280,7 +281,7 @@ def top_band(rows: np.ndarray) -> int:
     return band_of(float(rows[int(np.argmax(rows[:, 3])), 0]))
 
 
-def features(gpu, stars, devs, workers: int = 8) -> np.ndarray:
+def features(gpu, stars, devs, workers: int = 8, bin_days: float = 0.0) -> np.ndarray:
     """(4, count, T_IN) float32, channel-major; the maps run on the batch
     worker threads."""
     x = np.zeros((MAP_CHANNELS, len(stars), T_IN), dtype=np.float32)
@@ -288,7 +289,7 @@ def features(gpu, stars, devs, workers: int = 8) -> np.ndarray:
     todo = [i for i, (keep, _, _) in enumerate(plans) if keep.sum() >= 8]
     p = map_periods()
     maps = gpu.coarse_map_batch([devs[i] for i in todo], [p[plans[i][0]] for i in todo],
-                                [plans[i][1] for i in todo], [plans[i][2] for i in todo], 2.0, workers)
+                                [plans[i][1] for i in todo], [plans[i][2] for i in todo], 2.0, workers, bin_days)
     for i, m in zip(todo, maps):
         x[:, i, :] = map_features(m, plans[i][0])
     return x
@@ -359,7 +360,9 @@ WEIGHTS = __import__("pathlib").Path(__file__).resolve().parent / "data" / "prop
 def load_net(device: int = 0, path=None) -> Net:
     """The network with the committed weights (trained by main() below)."""
     net = Net(device)
-    net.load(np.load(path or WEIGHTS)["weights"])
+    saved = np.load(path or WEIGHTS)
+    net.load(saved["weights"])
+    net.bin_days = float(saved["bin_days"]) if "bin_days" in saved.files else 0.0
     return net
 
 
@@ -369,7 +372,7 @@ def search_proposed(gpu, net: Net, stars, devs, cfg, k: int = 3, workers: int = 
     full search's rows in those bands). Returns the batch results and logits."""
     import time
     t0 = time.perf_counter()
-    x = features(gpu, stars, devs, workers)
+    x = features(gpu, stars, devs, workers, getattr(net, "bin_days", 0.0))
     t1 = time.perf_counter()
     logits = scores(net, x)
     ranges = [ranges_for(l, k) for l in logits]
@@ -398,6 +401,7 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--workers", type=int, default=8)
     ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--bin-minutes", type=float, default=10.0, help="time bins of the coarse map (0: none)")
     ap.add_argument("--out", required=True)
     args = ap.parse_args(argv)
     t0 = time.time()
@@ -410,7 +414,8 @@ def main(argv=None):
                                workers=args.workers)
         y = np.array([top_band(r) for r, _, _ in res])
         log(f"exhaustive labels: {int((y >= 0).sum())} of {len(y)} stars with a detection")
-        x = features(gpu, stars, devs)
+        bin_days = args.bin_minutes / 1440.0
+        x = features(gpu, stars, devs, args.workers, bin_days)
         log("coarse maps done")
         net = Net(0, seed=args.seed)
         ntr = args.train
@@ -419,7 +424,7 @@ def main(argv=None):
         rec = recall_at(lt, y[ntr:])
         log("held-out recall@k " + " ".join(f"{k + 1}:{r:.4f}" for k, r in enumerate(rec[:12])))
         np.savez(args.out, weights=net.state_dict(), recall=rec, train=ntr, test=args.test, seed=args.seed,
-                 max_sectors=args.max_sectors, epochs=args.epochs)
+                 max_sectors=args.max_sectors, epochs=args.epochs, bin_days=bin_days)
         print(json.dumps({"recall": rec.tolist(), "labelled_test": int((y[ntr:] >= 0).sum())}))
         for d in devs:
             d.free()

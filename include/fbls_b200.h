@@ -265,9 +265,12 @@ int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* dur
  * (scan.rs template semantics: width below nb / 2, 3 .. n - 3 points, a > 0,
  * positive precision), 0 when none counts. Periods are folded in octave
  * groups at nb = max(8, ceil(oversample * longest period / shortest
- * duration)). */
+ * duration)). bin_days > 0 first sums v and w over time bins of that width
+ * (floor((t - t0) / bin_days)), at each bin's mean time, and maps the bins;
+ * 0 maps the observations themselves. */
 int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* ready, const double* periods, uint32_t P,
-                    const double* durations, const double* rho, uint32_t nd, double oversample, float* out);
+                    const double* durations, const double* rho, uint32_t nd, double oversample, double bin_days,
+                    float* out);
 
 /* One coarse map of a batch: inputs as fbls_coarse_map, out (P x nd floats,
  * caller-owned host memory) and the job's status. */
@@ -279,6 +282,7 @@ typedef struct {
     const double* rho;
     uint32_t nd;
     double oversample;
+    double bin_days;
     float* out;
     int status;
 } fbls_map_job;

@@ -150,3 +150,35 @@ def test_coarse_map_batch_matches_single_maps(gpu):
         assert np.array_equal(x[:, i, :], pr.star_map(gpu, dev, st, pmax))
     for d in devs:
         d.free()
+
+
+def test_binned_coarse_map_is_the_map_of_the_binned_family(gpu):
+    c, cfg = synth.small_curve(), synth.small_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    bin_days = 1500.0 / 86400.0
+    t, v, w = st.time, st.v, st.w
+    key = np.floor((t - t[0]) / bin_days)
+    tb, vb, wb = [], [], []
+    i = 0
+    while i < len(t):
+        j, st_t, sv, sw = i, 0.0, 0.0, 0.0
+        while j < len(t) and key[j] == key[i]:
+            st_t += t[j]
+            sv += v[j]
+            sw += w[j]
+            j += 1
+        tb.append(st_t / (j - i))
+        vb.append(sv)
+        wb.append(sw)
+        i = j
+    binned = api.FamilyState(np.array(tb), np.array(vb), np.array(wb), st.baseline_norm, st.origin,
+                             st.residual_energy, st.durations, st.rho)
+    periods = np.geomspace(0.6, 2.2, 300)
+    d, r = st.durations[[0, -1]], st.rho[[0, -1]]
+    dev, devb = gpu.upload(st), gpu.upload(binned)
+    got = gpu.coarse_map(dev, periods, d, r, 2.0, bin_days=bin_days)
+    want = gpu.coarse_map(devb, periods, d, r, 2.0)
+    assert len(tb) < len(t)
+    assert np.array_equal(got, want)
+    dev.free()
+    devb.free()
