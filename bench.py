@@ -10,9 +10,10 @@ periods, full scan on the survivors) of one synthetic star:
       (189,216 periods under the reference's grid rule).
   single_sector: one sector (19,008 points), 12 durations, 13,065 periods.
   survey: a step is one fbls_search_batch over --stars seeded survey stars
-      (1-13 sectors, 120/200/600 s cadence, 30 % with a box) with
-      --batch-workers host threads, each on its own stream; timed by the host
-      clock around the device-synchronised batch.
+      (1-13 sectors, 120/200/600 s cadence, 30 % with a box), the stars'
+      band scans fused into job launches (--batch-workers 0) or spread over
+      host worker threads with their own streams; timed by the host clock
+      around the device-synchronised batch.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload survey]
 
@@ -558,7 +559,9 @@ def main():
     ap.add_argument("--impl", default="fbls_b200", choices=["fbls_b200", "reference"])
     ap.add_argument("--workload", default="multi_sector", choices=["multi_sector", "single_sector", "survey", "proposal"])
     ap.add_argument("--stars", type=int, default=512, help="survey workload: stars per GPU")
-    ap.add_argument("--batch-workers", type=int, default=4, help="survey workload: host worker threads")
+    ap.add_argument("--batch-workers", type=int, default=0,
+                    help="survey / proposal workloads: search_batch host worker threads (0: stars fused into "
+                         "job launches)")
     ap.add_argument("--bands", type=int, default=3, help="proposal workload: log-period bands searched per star")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")

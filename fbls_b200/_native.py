@@ -190,6 +190,8 @@ SIGNATURES = {
     "fbls_coarse_map": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, C.c_uint32, c_double_p, c_double_p, C.c_uint32,
                                   C.c_double, C.c_double, C.POINTER(C.c_float)]),
     "fbls_coarse_map_batch": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, C.c_uint32]),
+    "fbls_coarse_features": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, c_uint32_p, C.c_uint32,
+                                       C.c_uint32, C.POINTER(C.c_float)]),
     # proposal network kernels: device pointers passed as integers
     "fbls_nn_gemm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int] + [C.c_longlong] * 9
                      + [C.c_int, C.c_float, C.c_float, C.c_void_p]),

@@ -245,7 +245,8 @@ class Gpu:
 
     def coarse_map_batch(self, devs: Sequence[DeviceReady], periods: Sequence, durations: Sequence, rho: Sequence,
                          oversample: float = 2.0, workers: int = 8, bin_days: float = 0.0) -> List[np.ndarray]:
-        """coarse_map of many uploaded families on worker threads."""
+        """coarse_map of many uploaded families: on `workers` host threads,
+        or (workers == 0) all together in shared job launches."""
         count = len(devs)
         jobs = (N.MapJob * max(count, 1))()
         keep, outs = [], []
@@ -263,14 +264,39 @@ class Gpu:
         self._check(self.lib.fbls_coarse_map_batch(self.ctx, jobs, count, int(workers)))
         return outs
 
+    def coarse_features(self, devs: Sequence[DeviceReady], periods: Sequence, durations: Sequence, rho: Sequence,
+                        offsets: Sequence[int], T: int, oversample: float = 2.0, bin_days: float = 0.0) -> np.ndarray:
+        """The proposal network's input (channels, len(devs), T) float32: each
+        star's coarse map (channels = its durations), log1p'd and standardised
+        per channel, at positions [offset, offset + len(periods)) of its row."""
+        count = len(devs)
+        channels = len(durations[0]) if count else 1
+        jobs = (N.MapJob * max(count, 1))()
+        keep = []
+        for i in range(count):
+            p, d, r = _f64(periods[i]), _f64(durations[i]), _f64(rho[i])
+            keep += [p, d, r]
+            j = jobs[i]
+            j.ready, j.periods, j.P = devs[i].handle, _dptr(p), p.shape[0]
+            j.durations, j.rho, j.nd = _dptr(d), _dptr(r), d.shape[0]
+            j.oversample = float(oversample)
+            j.bin_days = float(bin_days)
+        offs = np.ascontiguousarray(offsets, dtype=np.uint32)
+        x = np.empty((channels, count, T), dtype=np.float32)
+        self._check(self.lib.fbls_coarse_features(self.ctx, jobs, count, offs.ctypes.data_as(N.c_uint32_p),
+                                                  channels, T, x.ctypes.data_as(C.POINTER(C.c_float))))
+        return x
+
     def search_batch(self, states: Sequence[FamilyState], cfg: SearchConfig, period_max: Optional[Sequence[float]] = None,
                      devs: Optional[Sequence[DeviceReady]] = None, workers: int = 4,
                      ranges: Optional[Sequence[Optional[Sequence[Tuple[float, float]]]]] = None):
-        """signal_search over many stars with `workers` host threads, each
-        with its own stream: [(rows N x 5, grid length, templates)] per star.
+        """signal_search over many stars: [(rows N x 5, grid length,
+        templates)] per star. workers >= 1 host threads each take one star at
+        a time on a stream of their own; workers == 0 searches groups of stars
+        together with job launches that cover every star of a group.
         period_max overrides cfg.period_max per star; devs are uploaded
-        families (else each worker uploads the star's host arrays); ranges
-        restrict a star's search to period ranges [lo, hi)."""
+        families (else the host arrays are uploaded); ranges restrict a star's
+        search to period ranges [lo, hi)."""
         count = len(states)
         stars = (N.Star * max(count, 1))()
         keep = []

@@ -98,8 +98,102 @@ __device__ __forceinline__ void prefix_row(Load load, int nb, double* __restrict
     }
 }
 
+// One (period, field) row of a walking-fold CTA's shared-memory histograms:
+// the v or w sums (every other double of the period's double2 bins) or the
+// counts. The prefix epilogues overwrite a bin with its prefix value once
+// they have read it (a count prefix is an integer below 2^32).
+struct HistRow {
+    double* d;    // v or w sums, stride 2 doubles; null for the counts
+    uint32_t* c;  // counts
+    __device__ __forceinline__ double load(int b) const { return d ? d[2 * b] : (double)c[b]; }
+    __device__ __forceinline__ void store(int b, double v) const {
+        if (d)
+            d[2 * b] = v;
+        else
+            c[b] = (uint32_t)v;
+    }
+};
+
+// Inclusive Hillis-Steele scan of a warp's 32 values (the association of
+// prefix_row and of the reference's prefix_block groups).
+__device__ __forceinline__ double warp_scan(double x, int lane) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double o = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x = __dadd_rn(x, o);
+    }
+    return x;
+}
+
+// prefix_row of a shared-memory row by one warp, with the first copy kept in
+// place, so the second copy (first + final carry) is read from shared memory
+// rather than back from the global rows.
+__device__ __forceinline__ void prefix_row_smem(const HistRow& r, int nb, double* __restrict__ out64,
+                                                float2* __restrict__ out32) {
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) {
+        out64[0] = 0.0;
+        out32[0] = make_float2(0.f, 0.f);
+    }
+    double carry = 0.0;
+    for (int seg = 0; seg < nb; seg += 256) {
+        double offset = carry;
+        double total = 0.0;
+#pragma unroll 1
+        for (int g = 0; g < 8; g++) {
+            const int b = seg + g * 32 + lane;
+            const double x = warp_scan(b < nb ? r.load(b) : 0.0, lane);
+            const double wt = __shfl_sync(0xffffffffu, x, 31);
+            if (b < nb) {
+                const double val = __dadd_rn(x, offset);
+                out64[b + 1] = val;
+                out32[b + 1] = split_pair(val);
+                r.store(b, val);
+            }
+            offset = __dadd_rn(offset, wt);
+            total = __dadd_rn(total, wt);
+        }
+        carry = __dadd_rn(carry, total);
+    }
+    for (int b = lane; b < nb; b += 32) {  // bins this lane stored above
+        const double val = __dadd_rn(r.load(b), carry);
+        out64[nb + b + 1] = val;
+        out32[nb + b + 1] = split_pair(val);
+    }
+}
+
+// The 256-bin segment `seg` of a row, by one warp, as prefix_row does it:
+// with `carry` (the carry entering the segment) and `final` (the row's last
+// carry) known, writes both copies and returns nothing; with them unknown
+// (write = false), returns the segment's total (the sum, in order, of its
+// eight group totals) and writes nothing.
+__device__ __forceinline__ double prefix_segment(const HistRow& r, int nb, int seg, double carry, double final,
+                                                 bool write, double* __restrict__ out64,
+                                                 float2* __restrict__ out32) {
+    const int lane = threadIdx.x & 31;
+    double offset = carry;
+    double total = 0.0;
+#pragma unroll 1
+    for (int g = 0; g < 8; g++) {
+        const int b = seg + g * 32 + lane;
+        const double x = warp_scan(b < nb ? r.load(b) : 0.0, lane);
+        const double wt = __shfl_sync(0xffffffffu, x, 31);
+        if (write && b < nb) {
+            const double val = __dadd_rn(x, offset);
+            out64[b + 1] = val;
+            out32[b + 1] = split_pair(val);
+            const double val2 = __dadd_rn(val, final);
+            out64[nb + b + 1] = val2;
+            out32[nb + b + 1] = split_pair(val2);
+        }
+        offset = __dadd_rn(offset, wt);
+        total = __dadd_rn(total, wt);
+    }
+    return total;
+}
+
 __global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     __shared__ double s_scale[MAX_GROUP];
 
     const int tid = threadIdx.x;
@@ -287,6 +381,11 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
 
 // Issues the three bulk copies of chunk [i0, i1), rounded out to whole
 // 16-byte pieces, into one staging buffer (fields at `field` doubles apart).
+// Named barrier `id` over `threads` threads of the CTA.
+__device__ __forceinline__ void group_sync(uint32_t id, uint32_t threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
 __device__ __forceinline__ void stage_chunk(const FoldArgs& a, int i0, int i1, double* buf, int field, uint32_t bar) {
     const int a0 = i0 & ~1, a1 = (i1 + 1) & ~1;
     const uint32_t bytes = (uint32_t)(a1 - a0) * (uint32_t)sizeof(double);
@@ -316,8 +415,10 @@ __device__ __forceinline__ void stage_chunk(const FoldArgs& a, int i0, int i1, d
 // lose more to idle steps than the conflict-free reads gain).
 constexpr int LOCKSTEP_MIN_SEGMENT = 11;
 
+// One CTA of the walking fold: CTA `cta` of the launch described by `a`
+// folds periods [cta * G, cta * G + G).
 template <int CAP>
-__global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
+__device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) {
     constexpr int F = CAP + 2;  // doubles per staged field
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ double s_scale[MAX_GROUP];
@@ -333,7 +434,7 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
     const int G = a.group;
     const int wpp = (T / 32) / G;
     const int NS = wpp * 32;
-    const int g0 = blockIdx.x * G;
+    const int g0 = cta * G;
     const int g = min(G, a.periods - g0);
     const int q = warp / wpp;
     const int seg = (warp - q * wpp) * 32 + lane;
@@ -366,20 +467,39 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
     int* lstart = starts + (live ? q : 0) * (NS + 1);
     const float inv_ns = 1.0f / (float)NS;
     const int nch = a.nchunks;
-    if (tid == 0) stage_chunk(a, a.chunks[0], a.chunks[1], stage, F, bar0);
+    // Staging blocks: runs of consecutive chunks of at most CAP observations
+    // in all, one bulk copy per field. Between the chunks of a block only the
+    // warps of a period group synchronise (named barrier 1 + warp / U over U
+    // warps, U >= the period's wpp warps, at most 8 groups): periods share no
+    // bins, so a CTA-wide barrier is needed only when a staging buffer turns
+    // over.
+    const int* ch = a.chunks;
+    auto block_end = [&](int c0) {
+        int c1 = c0 + 1;
+        while (c1 < nch && ch[c1 + 1] - ch[c0] <= CAP) c1++;
+        return c1;
+    };
+    const int U = wpp > 4 ? wpp : 4;
+    const uint32_t gbar = 1u + (uint32_t)(warp / U), gthreads = 32u * (uint32_t)U;
+    int blk_lo = 0, blk_hi = block_end(0);  // chunks of the block being folded
+    if (tid == 0) stage_chunk(a, ch[0], ch[blk_hi], stage, F, bar0);
 
-    for (int c = 0; c < nch; c++) {
-        const int buf = c & 1;
-        const bool landed = mbar_wait_bounded(bar0 + 8 * buf, (uint32_t)(c >> 1) & 1u);
+    for (int blk = 0; blk_lo < nch; blk++) {
+        const int buf = blk & 1;
+        const bool landed = mbar_wait_bounded(bar0 + 8 * buf, (uint32_t)(blk >> 1) & 1u);
         if (!__syncthreads_and(landed)) {
             if (tid == 0) atomicOr(a.fault, 1u);
             return;
         }
-        const int i0 = a.chunks[c];
-        const int len = a.chunks[c + 1] - i0;
-        if (tid == 0 && c + 1 < nch)
-            stage_chunk(a, a.chunks[c + 1], a.chunks[c + 2], stage + 3 * F * (buf ^ 1), F, bar0 + 8 * (buf ^ 1));
-        const double* tt = stage + 3 * F * buf + (i0 & 1);
+        const int next_lo = blk_hi, next_hi = next_lo < nch ? block_end(next_lo) : next_lo;
+        if (tid == 0 && next_lo < nch)
+            stage_chunk(a, ch[next_lo], ch[next_hi], stage + 3 * F * (buf ^ 1), F, bar0 + 8 * (buf ^ 1));
+        const int base_i = ch[blk_lo];
+        const double* sb = stage + 3 * F * buf + (base_i & 1);  // staged slot of observation i: sb[i - base_i]
+        for (int c = blk_lo; c < blk_hi; c++) {
+        const int i0 = ch[c];
+        const int len = ch[c + 1] - i0;
+        const double* tt = sb + (i0 - base_i);
         // Segment length: at least ceil(len / NS), odd.
         const int R = ((int)((float)len * inv_ns) + 1) | 1;
         int k = seg * R;
@@ -394,7 +514,7 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
         if (k > len) k = len;
         if (live) lstart[seg] = k;
         if (live && seg == 0) lstart[NS] = len;
-        __syncthreads();
+        group_sync(gbar, gthreads);
         const int end = live ? lstart[seg + 1] : 0;
         if (R < LOCKSTEP_MIN_SEGMENT) {
             // Short segments: each lane walks its own window.
@@ -423,8 +543,7 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
                 lvw[slot] = acc;
                 lc[slot] = cnt;
             }
-            continue;
-        }
+        } else {
         // Lockstep walk: at step i every lane reads observation seg * R + i
         // (R odd, so the lanes' reads fall in distinct banks) and folds it when
         // it lies in the lane's window [k, end). Entering a cell takes the
@@ -482,6 +601,11 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
                 lc[slot] = cnt;
             }
         }
+        }
+        group_sync(gbar, gthreads);  // the chunk's bins are written before the next chunk's walk
+        }
+        blk_lo = next_lo;
+        blk_hi = next_hi;
     }
     __syncthreads();
 
@@ -493,19 +617,91 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
         }
         return;
     }
+    // Doubled prefix rows. A row has S segments of 256 bins whose carries
+    // chain; with few rows (large nb, small G) the rows' segments are spread
+    // over every warp in three passes (segment totals, the carry chains, then
+    // the values with their carries known), else one warp takes a whole row.
+    // Both give prefix_row's values bit for bit.
     const size_t stride = 2 * (size_t)nb + 1;
-    for (int row = warp; row < g * NF; row += T / 32) {
-        const int qq = row / NF, f = row - (row / NF) * NF;
-        double* out64 = a.cum + ((size_t)(g0 + qq) * NF + f) * stride;
-        float2* out32 = a.cum32 + ((size_t)(g0 + qq) * NF + f) * stride;
+    const int W = T / 32;
+    const int rows = g * NF;
+    const int S = (nb + 255) >> 8;
+    auto row_of = [&](int row, double*& out64, float2*& out32) {
+        const int qq = row / NF, f = row - qq * NF;
+        out64 = a.cum + ((size_t)(g0 + qq) * NF + f) * stride;
+        out32 = a.cum32 + ((size_t)(g0 + qq) * NF + f) * stride;
         const size_t o = (size_t)qq * rs;
-        if (f == F_V)
-            prefix_row([&](int bb) { return hvw[o + bb].x; }, nb, out64, out32);
-        else if (f == F_W)
-            prefix_row([&](int bb) { return hvw[o + bb].y; }, nb, out64, out32);
-        else
-            prefix_row([&](int bb) { return (double)hc[o + bb]; }, nb, out64, out32);
+        HistRow r;
+        r.d = f == F_V ? &hvw[o].x : f == F_W ? &hvw[o].y : nullptr;
+        r.c = hc + o;
+        return r;
+    };
+    const int items = rows * S;
+    if (2 * ((items + W - 1) / W) < ((rows + W - 1) / W) * S && 2 * items + rows <= 6 * F) {
+        double* seg_total = stage;             // rows x S (the staging buffers are idle now)
+        double* seg_carry = stage + items;     // rows x S
+        double* row_final = stage + 2 * items; // rows
+        for (int it = warp; it < items; it += W) {
+            const int row = it / S, sg = it - row * S;
+            double* o64;
+            float2* o32;
+            const HistRow r = row_of(row, o64, o32);
+            const double tot = prefix_segment(r, nb, sg * 256, 0.0, 0.0, false, o64, o32);
+            if (lane == 0) seg_total[it] = tot;
+        }
+        __syncthreads();
+        for (int row = tid; row < rows; row += T) {
+            double carry = 0.0;
+            for (int sg = 0; sg < S; sg++) {
+                seg_carry[row * S + sg] = carry;
+                carry = __dadd_rn(carry, seg_total[row * S + sg]);
+            }
+            row_final[row] = carry;
+        }
+        __syncthreads();
+        for (int it = warp; it < items; it += W) {
+            const int row = it / S, sg = it - row * S;
+            double* o64;
+            float2* o32;
+            const HistRow r = row_of(row, o64, o32);
+            if (sg == 0 && lane == 0) {
+                o64[0] = 0.0;
+                o32[0] = make_float2(0.f, 0.f);
+            }
+            prefix_segment(r, nb, sg * 256, seg_carry[it], row_final[row], true, o64, o32);
+        }
+        return;
     }
+    for (int row = warp; row < rows; row += W) {
+        double* o64;
+        float2* o32;
+        const HistRow r = row_of(row, o64, o32);
+        prefix_row_smem(r, nb, o64, o32);
+    }
+}
+
+template <int CAP>
+__global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
+    fold_walk_cta<CAP>(a, blockIdx.x);
+}
+
+// Many folds in one launch (the batched search): CTA c runs CTA
+// c - cta0[j] of job j, where cta0[j] <= c < cta0[j + 1]. Every job uses the
+// walking fold with TMA staging; the launch's shared memory is the largest
+// job's.
+template <int CAP>
+__global__ void __launch_bounds__(1024, 1) k_fold_walk_jobs(const FoldArgs* __restrict__ jobs,
+                                                            const int* __restrict__ cta0, int njobs) {
+    int lo = 0, hi = njobs - 1;
+    const int c = blockIdx.x;
+    while (lo < hi) {  // last job with cta0[j] <= c
+        const int mid = (lo + hi + 1) / 2;
+        if (cta0[mid] <= c)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    fold_walk_cta<CAP>(jobs[lo], c - cta0[lo]);
 }
 
 namespace {
@@ -604,6 +800,38 @@ int fold_chunks(const double* time, int n, double scale_max, int nb, int span_ca
     return count;
 }
 
+cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, size_t smem,
+                             cudaStream_t stream) {
+    if (njobs < 1 || ctas < 1 || smem > MAX_FOLD_SMEM) return cudaErrorInvalidValue;
+    {
+        static std::mutex mu;
+        static bool configured[64] = {};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+        std::lock_guard<std::mutex> lock(mu);
+        if (!configured[dev]) {
+            e = cudaFuncSetAttribute(k_fold_walk_jobs<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)MAX_FOLD_SMEM);
+            if (e != cudaSuccess) return e;
+            configured[dev] = true;
+        }
+    }
+    k_fold_walk_jobs<WALK_CAP><<<ctas, 1024, smem, stream>>>(jobs, cta0, njobs);
+    return cudaGetLastError();
+}
+
+bool fold_job_ok(const FoldArgs& a, const FoldShape& shape) {
+    return shape.kind == FOLD_WALK && shape.smem <= MAX_FOLD_SMEM && a.group == shape.group && a.group >= 1 &&
+           a.group <= MAX_GROUP && (a.group & (a.group - 1)) == 0 && shape.threads == 1024 && a.nchunks >= 1 &&
+           a.nb >= 2 && a.stage_field == WALK_CAP + 2 && shape.chunk_cap == WALK_CAP &&
+           a.row_stride == shape.row_stride && a.row_stride >= a.nb && a.fault != nullptr && a.hist_out == nullptr &&
+           a.time && a.v && a.w && a.scales && a.chunks && a.cum && a.cum32 &&
+           !(reinterpret_cast<uintptr_t>(a.time) & 15) && !(reinterpret_cast<uintptr_t>(a.v) & 15) &&
+           !(reinterpret_cast<uintptr_t>(a.w) & 15);
+}
+
 cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream) {
     // The shared-memory limit is a per-device attribute of each kernel; set it
     // once per device (contexts of several host threads may launch).
@@ -624,6 +852,8 @@ cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t 
             configured[dev] = true;
         }
     }
+    if (!a.time || !a.v || !a.w || !a.scales || !a.chunks || (!a.hist_out && (!a.cum || !a.cum32)))
+        return cudaErrorInvalidValue;
     if (shape.kind == FOLD_WALK) {
         if (shape.smem > MAX_FOLD_SMEM || a.group != shape.group || a.group < 1 || a.group > MAX_GROUP ||
             (a.group & (a.group - 1)) != 0 || shape.threads != 1024 || a.nchunks < 1 || a.nb < 2 ||

@@ -60,6 +60,7 @@ struct fbls_ctx {
     DevBuf evidence, fault;
     DevBuf family;  // observations of the star a batch worker is searching
     DevBuf mapbin;  // time-binned observations of a coarse map
+    DevBuf feat;    // the proposal network's input made from coarse maps
     PinBuf pin_up, pin_down, pin_down2;  // staging of a session's upload and download (two sessions in flight)
     std::vector<fbls_ctx*> workers;  // fbls_search_batch worker contexts, kept for reuse
 };
@@ -127,13 +128,25 @@ T* as(DevBuf& b) {
 // scan.rs:110-124): into a fresh allocation owned by `r` when `buf` is null,
 // else into the reusable context buffer `buf` (no allocation once it is
 // large enough, so a batch worker never synchronises the device on cudaFree).
+// Checks a family's host arrays; a rejection's message goes to `err`.
+int check_family(std::string& err, const double* time, const double* v, const double* w, uint32_t n) {
+    auto bad = [&](int status, const char* message) {
+        err = message;
+        return status;
+    };
+    if (!time || !v || !w) return bad(FBLS_ERR_ARGUMENT, "null argument");
+    if (n < 6) return bad(FBLS_ERR_DATA, "at least six observations are required");
+    for (uint32_t i = 1; i < n; i++)
+        if (!(time[i] >= time[i - 1])) return bad(FBLS_ERR_ARGUMENT, "times must be ascending");
+    if (!(time[0] >= 0.0)) return bad(FBLS_ERR_ARGUMENT, "times must be relative to the first observation");
+    return FBLS_OK;
+}
+
 int upload_family(fbls_ctx* ctx, DevBuf* buf, const double* time, const double* v, const double* w, uint32_t n,
                   double baseline_norm, double origin, double residual_energy, fbls_ready* r) {
-    if (!time || !v || !w) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    if (n < 6) return fail(ctx, FBLS_ERR_DATA, "at least six observations are required");
-    for (uint32_t i = 1; i < n; i++)
-        if (!(time[i] >= time[i - 1])) return fail(ctx, FBLS_ERR_ARGUMENT, "times must be ascending");
-    if (!(time[0] >= 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "times must be relative to the first observation");
+    std::string err;
+    const int rc = check_family(err, time, v, w, n);
+    if (rc) return fail(ctx, rc, err);
     r->ctx = ctx;
     r->n = n;
     r->baseline_norm = baseline_norm;
@@ -216,6 +229,7 @@ cudaError_t ensure_pinned(PinBuf& b, size_t bytes) {
 // One scan_bank pass (scan.rs:144-357): every period's best template at nb
 // bins. Planned on the host, then enqueued with the other passes of a session.
 struct Pass {
+    const fbls_ready* r = nullptr;  // the family this pass scans
     const double* periods = nullptr;
     uint32_t P = 0;
     const fbls_bank* bank = nullptr;
@@ -231,20 +245,50 @@ struct Pass {
     size_t ev0 = 0, nlaunch = 0;
     BandOut out;
     fbls_scan_stats st{};
+    bool bad = false;  // a template's precision came out nonpositive
+    std::string err;   // plan_pass's message when it rejects the pass
+    int fail(int status, const char* message) {
+        err = message;
+        return status;
+    }
 };
 
+// Runs f(i) for i in [0, n) on up to 16 host threads, the caller's included.
+template <typename F>
+void parallel_for(size_t n, F f) {
+    const size_t threads = std::min<size_t>(n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+    if (threads <= 1) {
+        for (size_t i = 0; i < n; i++) f(i);
+        return;
+    }
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t i; (i = next.fetch_add(1)) < n;) f(i);
+    };
+    std::vector<std::thread> pool;
+    for (size_t k = 1; k < threads; k++) pool.emplace_back(work);
+    work();
+    for (std::thread& t : pool) t.join();
+}
+
+// plan_pass over every pass (in parallel: the passes are independent);
+// returns the first failure in pass order, its message in ctx.
+int plan_passes(fbls_ctx* ctx, std::vector<Pass>& passes);
+
 // Checks a pass and plans its batches, launches, fold shape and chunks
-// (scan.rs:144-199 for the bank factors, the budget and the batch size).
-int plan_pass(fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
+// (scan.rs:144-199 for the bank factors, the budget and the batch size). Reads
+// ctx but writes only p (a rejection's message goes to p.err).
+int plan_pass(const fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
     const fbls_bank* bank = p.bank;
     const uint32_t nd = bank->nd, ns = bank->ns, layers = bank->layers, nb = p.nb;
+    p.r = r;
     std::memset(&p.st, 0, sizeof(p.st));
     p.st.phase_bins = nb;
     p.st.periods = p.P;
     if (nd == 0 || nd > (uint32_t)MAX_DURATIONS || ns == 0 || ns > (uint32_t)MAX_SHAPES || layers == 0 ||
         layers > (uint32_t)MAX_LAYERS)
-        return fail(ctx, FBLS_ERR_ARGUMENT, "bank size outside the supported range");
-    if (nb < 2) return fail(ctx, FBLS_ERR_ARGUMENT, "nb must be at least 2");
+        return p.fail(FBLS_ERR_ARGUMENT, "bank size outside the supported range");
+    if (nb < 2) return p.fail(FBLS_ERR_ARGUMENT, "nb must be at least 2");
     // Shape factors 1 - 2 ing l / (L - 1) (scan.rs:157-171).
     p.host_bank.assign(bank->durations, bank->durations + nd);
     p.host_bank.insert(p.host_bank.end(), bank->rho, bank->rho + nd);
@@ -256,7 +300,7 @@ int plan_pass(fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
     const uint32_t tiles = (nb + TILE - 1) / TILE;
     const double per_period_bytes = (double)(NF * (4 * (size_t)nb + 2) * 8 + NF * (2 * (size_t)nb + 1) * 8);
     const uint64_t budget = (uint64_t)std::floor((bank->max_fold_mib * 1048576.0) / per_period_bytes);
-    if (budget == 0) return fail(ctx, FBLS_ERR_BUDGET, "one folded period exceeds max_fold_mib");
+    if (budget == 0) return p.fail(FBLS_ERR_BUDGET, "one folded period exceeds max_fold_mib");
     uint64_t batch = bank->period_batch;
     if (budget < batch) batch = budget;
     if (p.P < batch) batch = p.P;
@@ -268,11 +312,11 @@ int plan_pass(fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
     for (uint32_t i = 0; i < p.P; i++) {
         p.scales[i] = (double)nb / p.periods[i];
         if (!(p.scales[i] > 0.0) || !std::isfinite(p.scales[i]))
-            return fail(ctx, FBLS_ERR_ARGUMENT, "periods must be positive and finite");
+            return p.fail(FBLS_ERR_ARGUMENT, "periods must be positive and finite");
         if (p.scales[i] > scale_max) scale_max = p.scales[i];
     }
     if (std::floor(r->t_last * scale_max) >= 4294967295.0 - 2.0 * (double)nb - 2.0)
-        return fail(ctx, FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
+        return p.fail(FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
     // Periods per launch: whole batches of the reference's size, as many as
     // the fold budget holds in this path's buffers (cum, cum32 and tile parts;
     // the histograms never reach device memory), up to 16,384, so bands with
@@ -292,7 +336,7 @@ int plan_pass(fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
     p.chunks.resize((size_t)r->n + 2);
     const int count = fold_chunks(r->time_host.data(), (int)r->n, scale_max, (int)nb, p.shape.span_cap,
                                   p.shape.chunk_cap, p.chunks.data(), (int)p.chunks.size());
-    if (count < 1) return fail(ctx, FBLS_ERR_ARGUMENT, "fold chunking failed");
+    if (count < 1) return p.fail(FBLS_ERR_ARGUMENT, "fold chunking failed");
     p.chunks.resize((size_t)count + 1);
     // Device input region: scales | periods | bank | chunks; output region:
     // records | score | depth | flags.
@@ -309,11 +353,19 @@ int plan_pass(fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
     return FBLS_OK;
 }
 
+int plan_passes(fbls_ctx* ctx, std::vector<Pass>& passes) {
+    std::vector<int> rc(passes.size(), FBLS_OK);
+    parallel_for(passes.size(), [&](size_t i) { rc[i] = plan_pass(ctx, passes[i].r, passes[i]); });
+    for (size_t i = 0; i < passes.size(); i++)
+        if (rc[i]) return fail(ctx, rc[i], passes[i].err);
+    return FBLS_OK;
+}
+
 // Runs a session of planned passes on ctx->stream: one upload of every
 // pass's inputs from page-locked memory, the fold / scan / merge launches of
 // all passes back to back, one download of all outputs into `down` and a
 // single synchronisation.
-int run_session(fbls_ctx* ctx, const fbls_ready* r, std::vector<Pass>& passes, PinBuf& down_buf) {
+int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
     if (passes.empty()) return FBLS_OK;
     size_t in_total = 0, out_total = 0, launches = 0;
     size_t cum_max = 0, parts_max = 0, hist_max = 0;
@@ -366,6 +418,7 @@ int run_session(fbls_ctx* ctx, const fbls_ready* r, std::vector<Pass>& passes, P
     unsigned char* din = static_cast<unsigned char*>(ctx->pass_in.ptr);
     unsigned char* dout = static_cast<unsigned char*>(ctx->pass_out.ptr);
     for (Pass& p : passes) {
+        const fbls_ready* r = p.r;
         const uint32_t nb = p.nb, nd = p.bank->nd, ns = p.bank->ns, layers = p.bank->layers;
         const uint32_t tiles = (nb + TILE - 1) / TILE;
         const size_t stride = 2 * (size_t)nb + 1;
@@ -476,12 +529,298 @@ int run_session(fbls_ctx* ctx, const fbls_ready* r, std::vector<Pass>& passes, P
             p.st.seconds_scan += t_scan * 1e-3;
         }
         for (uint32_t i = 0; i < p.P; i++) {
-            bad = bad || (p.out.flags[i] & 2u);
+            p.bad = p.bad || (p.out.flags[i] & 2u);
+            p.st.exact_tile_retries += (p.out.flags[i] & 1u) ? 1 : 0;
+            p.st.tile_rescans += (p.out.flags[i] & 4u) ? 1 : 0;
+        }
+        bad = bad || p.bad;
+    }
+    if (bad) return fail(ctx, FBLS_ERR_PRECISION, "nonpositive template precision; inspect noise model");
+    return FBLS_OK;
+}
+
+// The same session as run_session with every pass's launches packed into job
+// launches: the (pass, launch) units are grouped into waves whose prefix-sum
+// workspace fits WAVE_BYTES, and each wave is one fold launch (walking-fold
+// units as jobs; other units on their own), one scan launch and one merge
+// launch, whatever the number of passes and stars. Results are the same as
+// run_session's, except that a pass with a nonpositive template precision is
+// only marked (Pass::bad) for its caller, so the other stars of a batch keep
+// their results.
+constexpr size_t WAVE_BYTES = 1536ull << 20;
+
+int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
+    if (passes.empty()) return FBLS_OK;
+    struct Unit {
+        int pass;
+        uint64_t cursor;
+        int n;
+        size_t cum_off, parts_off, hist_off;  // elements within the wave's workspace
+        bool walk;
+    };
+    struct Wave {
+        std::vector<Unit> units;
+        size_t cum = 0, parts = 0, hist = 0;
+        int fold_jobs = 0, fold_ctas = 0, scan_ctas = 0, merge_total = 0;
+        size_t smem = 0;
+        size_t off_fold = 0, off_fcta = 0, off_scan = 0, off_scta = 0, off_merge = 0, off_mp = 0;  // in the job blob
+    };
+    size_t in_total = 0, out_total = 0;
+    for (Pass& p : passes) {
+        p.in_off = in_total;
+        in_total += p.in_bytes;
+        p.out_off = out_total;
+        out_total += p.out_bytes;
+    }
+    std::vector<Wave> waves(1);
+    size_t cum_max = 0, parts_max = 0, hist_max = 0;
+    for (size_t pi = 0; pi < passes.size(); pi++) {
+        Pass& p = passes[pi];
+        const size_t stride = 2 * (size_t)p.nb + 1;
+        const size_t tiles = (p.nb + TILE - 1) / TILE;
+        for (uint64_t cursor = 0; cursor < p.P; cursor += p.launch) {
+            const int n = (int)std::min<uint64_t>(p.P - cursor, p.launch);
+            const size_t cum = (size_t)n * NF * stride, parts = (size_t)n * tiles;
+            const bool walk = p.shape.kind == FOLD_WALK;
+            const size_t hist = walk ? 0 : ((n + p.shape.group - 1) / p.shape.group) * (size_t)p.shape.group * NF *
+                                               (size_t)p.shape.row_stride;
+            if (!waves.back().units.empty() && (waves.back().cum + cum) * (sizeof(double) + sizeof(float2)) > WAVE_BYTES)
+                waves.emplace_back();
+            Wave& w = waves.back();
+            w.units.push_back({(int)pi, cursor, n, w.cum, w.parts, w.hist, walk});
+            w.cum += cum;
+            w.parts += parts;
+            w.hist += hist;
+            if (walk) {
+                w.fold_jobs++;
+                w.fold_ctas += (n + p.shape.group - 1) / p.shape.group;
+                w.smem = std::max(w.smem, p.shape.smem);
+            }
+            w.scan_ctas += n * (int)tiles;
+            w.merge_total += n;
+            p.st.templates_scanned += (uint64_t)n * p.bank->nd * p.bank->ns * p.nb;
+            p.st.batches += ((uint64_t)n + p.batch - 1) / p.batch;
+        }
+    }
+    // Job blob: per wave, fold jobs + CTA offsets, scan jobs + CTA offsets,
+    // merge jobs + period offsets.
+    size_t blob = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = blob;
+        blob += align256(bytes);
+        return at;
+    };
+    for (Wave& w : waves) {
+        cum_max = std::max(cum_max, w.cum);
+        parts_max = std::max(parts_max, w.parts);
+        hist_max = std::max(hist_max, w.hist);
+        const size_t nu = w.units.size();
+        w.off_fold = take(std::max(1, w.fold_jobs) * sizeof(FoldArgs));
+        w.off_fcta = take((w.fold_jobs + 1) * sizeof(int));
+        w.off_scan = take(nu * sizeof(ScanArgs));
+        w.off_scta = take((nu + 1) * sizeof(int));
+        w.off_merge = take(nu * sizeof(MergeArgs));
+        w.off_mp = take((nu + 1) * sizeof(int));
+    }
+    const size_t up_total = in_total + blob;
+    CK(ensure(ctx->pass_in, up_total), "workspace");
+    CK(ensure(ctx->pass_out, out_total), "workspace");
+    CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
+    CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
+    CK(ensure(ctx->parts, parts_max * PART_STRIDE * sizeof(double)), "workspace");
+    CK(ensure(ctx->keys, parts_max * sizeof(uint64_t)), "workspace");
+    CK(ensure(ctx->tflags, parts_max * sizeof(uint32_t)), "workspace");
+    if (hist_max) CK(ensure(ctx->hist, hist_max * sizeof(double)), "workspace");
+    CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
+    CK(ensure_pinned(ctx->pin_up, up_total), "pinned workspace");
+    CK(ensure_pinned(down_buf, out_total + 256), "pinned workspace");
+    unsigned char* up = static_cast<unsigned char*>(ctx->pin_up.ptr);
+    unsigned char* din = static_cast<unsigned char*>(ctx->pass_in.ptr);
+    unsigned char* dout = static_cast<unsigned char*>(ctx->pass_out.ptr);
+    for (Pass& p : passes) {
+        unsigned char* b = up + p.in_off;
+        std::memcpy(b + p.in_scales, p.scales.data(), p.P * sizeof(double));
+        std::memcpy(b + p.in_periods, p.periods, p.P * sizeof(double));
+        std::memcpy(b + p.in_bank, p.host_bank.data(), p.host_bank.size() * sizeof(double));
+        std::memcpy(b + p.in_chunks, p.chunks.data(), p.chunks.size() * sizeof(int));
+    }
+    // Jobs (device pointers into the buffers ensured above).
+    for (Wave& w : waves) {
+        FoldArgs* fj = reinterpret_cast<FoldArgs*>(up + in_total + w.off_fold);
+        int* fc = reinterpret_cast<int*>(up + in_total + w.off_fcta);
+        ScanArgs* sj = reinterpret_cast<ScanArgs*>(up + in_total + w.off_scan);
+        int* sc = reinterpret_cast<int*>(up + in_total + w.off_scta);
+        MergeArgs* mj = reinterpret_cast<MergeArgs*>(up + in_total + w.off_merge);
+        int* mp = reinterpret_cast<int*>(up + in_total + w.off_mp);
+        int nf = 0, fcta = 0, scta = 0, mtot = 0;
+        for (size_t u = 0; u < w.units.size(); u++) {
+            const Unit& un = w.units[u];
+            Pass& p = passes[un.pass];
+            const fbls_ready* r = p.r;
+            const uint32_t nb = p.nb, nd = p.bank->nd, ns = p.bank->ns, layers = p.bank->layers;
+            const int tiles = (int)((nb + TILE - 1) / TILE);
+            const double* d_scales = reinterpret_cast<const double*>(din + p.in_off + p.in_scales);
+            const double* d_periods = reinterpret_cast<const double*>(din + p.in_off + p.in_periods);
+            const double* d_bank = reinterpret_cast<const double*>(din + p.in_off + p.in_bank);
+            const int* d_chunks = reinterpret_cast<const int*>(din + p.in_off + p.in_chunks);
+            FoldArgs fa{};
+            fa.time = r->time;
+            fa.v = r->v;
+            fa.w = r->w;
+            fa.scales = d_scales + un.cursor;
+            fa.n = (int)r->n;
+            fa.nb = (int)nb;
+            fa.periods = un.n;
+            fa.group = p.shape.group;
+            fa.cum = as<double>(ctx->cum) + un.cum_off;
+            fa.cum32 = as<float2>(ctx->cum32) + un.cum_off;
+            fa.hist_global = un.walk ? nullptr : as<double>(ctx->hist) + un.hist_off;
+            fa.hist_out = nullptr;
+            fa.chunks = d_chunks;
+            fa.nchunks = (int)p.chunks.size() - 1;
+            fa.stage_field = p.shape.stage_field;
+            fa.window = p.shape.window;
+            fa.row_stride = p.shape.row_stride;
+            fa.fault = as<uint32_t>(ctx->fault);
+            if (un.walk) {
+                if (!fold_job_ok(fa, p.shape)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
+                fj[nf] = fa;
+                fc[nf++] = fcta;
+                fcta += (un.n + p.shape.group - 1) / p.shape.group;
+            }
+            ScanArgs sa{};
+            sa.cum = fa.cum;
+            sa.cum32 = fa.cum32;
+            sa.scales = fa.scales;
+            sa.durations = d_bank;
+            sa.rho = d_bank + nd;
+            sa.ingress = d_bank + 2 * nd;
+            sa.factors = d_bank + 2 * nd + ns;
+            sa.baseline = r->baseline_norm;
+            sa.gate = p.bank->shape_gate;
+            sa.n = (double)r->n;
+            sa.nb = (int)nb;
+            sa.nd = (int)nd;
+            sa.ns = (int)ns;
+            sa.layers = (int)layers;
+            sa.mixed = p.mixed ? 1 : 0;
+            sa.parts = as<double>(ctx->parts) + un.parts_off * PART_STRIDE;
+            sa.keys = as<uint64_t>(ctx->keys) + un.parts_off;
+            sa.flags = as<uint32_t>(ctx->tflags) + un.parts_off;
+            sj[u] = sa;
+            sc[u] = scta;
+            scta += un.n * tiles;
+            MergeArgs ma{};
+            ma.parts = sa.parts;
+            ma.keys = sa.keys;
+            ma.flags = sa.flags;
+            ma.periods_in = d_periods + un.cursor;
+            ma.scales = fa.scales;
+            ma.periods = un.n;
+            ma.tiles = tiles;
+            ma.offset = (int)un.cursor;
+            ma.records = reinterpret_cast<double*>(dout + p.out_off);
+            ma.score = reinterpret_cast<double*>(dout + p.out_off + p.out_score);
+            ma.depth = reinterpret_cast<double*>(dout + p.out_off + p.out_depth);
+            ma.flags_out = reinterpret_cast<uint32_t*>(dout + p.out_off + p.out_flags);
+            mj[u] = ma;
+            mp[u] = mtot;
+            mtot += un.n;
+            ctx->counters.fold_launches += 1;
+            ctx->counters.scan_launches += 1;
+            ctx->counters.fold_bytes += (double)un.n * (24.0 * r->n + 48.0 * (2.0 * nb + 1.0));
+            ctx->counters.fold_updates += (uint64_t)un.n * r->n;
+            ctx->counters.scan_bytes += (double)un.n * (24.0 * (2.0 * nb + 1.0) + 84.0 * tiles);
+        }
+        fc[nf] = fcta;
+        sc[w.units.size()] = scta;
+        mp[w.units.size()] = mtot;
+    }
+    cudaStream_t s = ctx->stream;
+    const bool timing = ctx->profile || ctx->kernel_timing;
+    if (timing) {
+        while (ctx->pool.size() < 3 * waves.size()) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e), "event");
+            ctx->pool.push_back(e);
+        }
+    }
+    CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
+    CK(cudaMemcpyAsync(din, up, up_total, cudaMemcpyHostToDevice, s), "upload");
+    for (size_t wi = 0; wi < waves.size(); wi++) {
+        Wave& w = waves[wi];
+        if (timing) CK(cudaEventRecord(ctx->pool[3 * wi], s), "event");
+        if (w.fold_jobs)
+            CK(launch_fold_jobs(reinterpret_cast<const FoldArgs*>(din + in_total + w.off_fold),
+                                reinterpret_cast<const int*>(din + in_total + w.off_fcta), w.fold_jobs, w.fold_ctas,
+                                w.smem, s),
+               "fold");
+        for (const Unit& un : w.units) {
+            if (un.walk) continue;
+            Pass& p = passes[un.pass];
+            // A unit whose histograms do not fit shared memory: its own launch.
+            const ScanArgs* sj = reinterpret_cast<const ScanArgs*>(up + in_total + w.off_scan);
+            const ScanArgs& sa = sj[&un - &w.units[0]];
+            FoldArgs fa{};
+            fa.time = p.r->time;
+            fa.v = p.r->v;
+            fa.w = p.r->w;
+            fa.scales = sa.scales;
+            fa.n = (int)p.r->n;
+            fa.nb = (int)p.nb;
+            fa.periods = un.n;
+            fa.group = p.shape.group;
+            fa.cum = const_cast<double*>(sa.cum);
+            fa.cum32 = const_cast<float2*>(sa.cum32);
+            fa.hist_global = as<double>(ctx->hist) + un.hist_off;
+            fa.chunks = reinterpret_cast<const int*>(din + p.in_off + p.in_chunks);
+            fa.nchunks = (int)p.chunks.size() - 1;
+            fa.stage_field = p.shape.stage_field;
+            fa.window = p.shape.window;
+            fa.row_stride = p.shape.row_stride;
+            fa.fault = as<uint32_t>(ctx->fault);
+            CK(launch_fold(fa, p.shape, s), "fold");
+        }
+        if (timing) CK(cudaEventRecord(ctx->pool[3 * wi + 1], s), "event");
+        CK(launch_scan_jobs(reinterpret_cast<const ScanArgs*>(din + in_total + w.off_scan),
+                            reinterpret_cast<const int*>(din + in_total + w.off_scta), (int)w.units.size(),
+                            w.scan_ctas, s),
+           "scan_tiles");
+        CK(launch_merge_jobs(reinterpret_cast<const MergeArgs*>(din + in_total + w.off_merge),
+                             reinterpret_cast<const int*>(din + in_total + w.off_mp), (int)w.units.size(),
+                             w.merge_total, s),
+           "merge");
+        if (timing) CK(cudaEventRecord(ctx->pool[3 * wi + 2], s), "event");
+        ctx->counters.launches += 3;
+    }
+    unsigned char* down = static_cast<unsigned char*>(down_buf.ptr);
+    CK(cudaMemcpyAsync(down, dout, out_total, cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaMemcpyAsync(down + out_total, ctx->fault.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaStreamSynchronize(s), "scan_bank");
+    uint32_t fault = 0;
+    std::memcpy(&fault, down + out_total, sizeof(uint32_t));
+    if (fault) return fail(ctx, FBLS_ERR_CUDA, "fold: staging copies did not complete");
+    if (timing) {
+        for (size_t wi = 0; wi < waves.size(); wi++) {
+            float a = 0.f, c = 0.f;
+            CK(cudaEventElapsedTime(&a, ctx->pool[3 * wi], ctx->pool[3 * wi + 1]), "event");
+            CK(cudaEventElapsedTime(&c, ctx->pool[3 * wi + 1], ctx->pool[3 * wi + 2]), "event");
+            ctx->counters.fold_ms += a;
+            ctx->counters.scan_ms += c;
+        }
+    }
+    for (Pass& p : passes) {
+        const unsigned char* b = down + p.out_off;
+        p.out.records = reinterpret_cast<const double*>(b);
+        p.out.score = reinterpret_cast<const double*>(b + p.out_score);
+        p.out.depth = reinterpret_cast<const double*>(b + p.out_depth);
+        p.out.flags = reinterpret_cast<const uint32_t*>(b + p.out_flags);
+        for (uint32_t i = 0; i < p.P; i++) {
+            p.bad = p.bad || (p.out.flags[i] & 2u);
             p.st.exact_tile_retries += (p.out.flags[i] & 1u) ? 1 : 0;
             p.st.tile_rescans += (p.out.flags[i] & 4u) ? 1 : 0;
         }
     }
-    if (bad) return fail(ctx, FBLS_ERR_PRECISION, "nonpositive template precision; inspect noise model");
     return FBLS_OK;
 }
 
@@ -506,18 +845,23 @@ int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_
     p.nb = nb;
     p.mixed = mixed;
     int rc = plan_pass(ctx, r, p);
-    if (rc == FBLS_OK) rc = run_session(ctx, r, passes, ctx->pin_down);
+    if (rc) return fail(ctx, rc, p.err);
+    rc = run_session(ctx, passes, ctx->pin_down);
     out = p.out;
     if (stats) add_pass_stats(*stats, p);
     return rc;
 }
 
-// scan_periods (scan.rs:363-408) of several bands at once: the first pass of
-// every band (its coarse prescan, or its full scan when there is none) in one
-// session, then the full scans of every band's survivors in a second one.
-// Rows are appended band after band; each band's stats get its passes'
-// counts and a share of the two sessions' wall time by templates scanned.
+// scan_periods (scan.rs:363-408) of several bands at once, of one star or of
+// many: the first pass of every band (its coarse prescan, or its full scan
+// when there is none) in one session, then the full scans of every band's
+// survivors in a second one. Each band's rows are appended to its `rows`
+// vector, band after band; each band's stats get its passes' counts and a
+// share of the two sessions' wall time by templates scanned. `fused` runs the
+// sessions as job launches (run_session_fused).
 struct BandJob {
+    const fbls_ready* r = nullptr;
+    std::vector<fbls_row>* rows = nullptr;
     const double* periods = nullptr;
     uint32_t P = 0;
     double nb_period = 0.0;  // period that sets nb (0: the last of `periods`)
@@ -527,11 +871,14 @@ struct BandJob {
     bool coarse = false;
     std::vector<double> survivors;
     int first = -1, second = -1;  // pass indices
+    int status = FBLS_OK;         // fused sessions: FBLS_ERR_PRECISION when a pass of this band was marked bad
 };
 
-int scan_bands(fbls_ctx* ctx, const fbls_ready* r, std::vector<BandJob>& jobs, bool mixed,
-               std::vector<fbls_row>& rows) {
+int scan_bands(fbls_ctx* ctx, std::vector<BandJob>& jobs, bool mixed, bool fused) {
     std::vector<Pass> first, second;
+    auto session = [&](std::vector<Pass>& passes, PinBuf& down) {
+        return fused ? run_session_fused(ctx, passes, down) : run_session(ctx, passes, down);
+    };
     for (BandJob& j : jobs) {
         std::memset(&j.st, 0, sizeof(j.st));
         j.st.periods = j.P;
@@ -544,23 +891,28 @@ int scan_bands(fbls_ctx* ctx, const fbls_ready* r, std::vector<BandJob>& jobs, b
         if (j.nb > (1u << 24)) return fail(ctx, FBLS_ERR_ARGUMENT, "phase grid too large");
         j.coarse = j.bank->prescan_factor > 1 && j.nb / j.bank->prescan_factor >= 8;
         Pass p;
+        p.r = j.r;
         p.periods = j.periods;
         p.P = j.P;
         p.bank = j.bank;
         p.nb = (uint32_t)(j.coarse ? j.nb / j.bank->prescan_factor : j.nb);
         p.mixed = mixed;
-        int rc = plan_pass(ctx, r, p);
-        if (rc) return rc;
         j.first = (int)first.size();
         first.push_back(std::move(p));
     }
+    int rc = plan_passes(ctx, first);
+    if (rc) return rc;
     const double t0 = now_seconds();
-    int rc = run_session(ctx, r, first, ctx->pin_down);
+    rc = session(first, ctx->pin_down);
     if (rc) return rc;
     const double t1 = now_seconds();
     for (BandJob& j : jobs) {
         if (j.first < 0) continue;
         add_pass_stats(j.st, first[j.first]);
+        if (first[j.first].bad) {
+            j.status = FBLS_ERR_PRECISION;
+            continue;
+        }
         if (!j.coarse) continue;
         const BandOut& band = first[j.first].out;
         const double cut = j.bank->prescan_fraction * j.bank->threshold;
@@ -571,17 +923,18 @@ int scan_bands(fbls_ctx* ctx, const fbls_ready* r, std::vector<BandJob>& jobs, b
         j.st.prescan_survivors = j.survivors.size();
         if (j.survivors.empty()) continue;
         Pass p;
+        p.r = j.r;
         p.periods = j.survivors.data();
         p.P = (uint32_t)j.survivors.size();
         p.bank = j.bank;
         p.nb = (uint32_t)j.nb;
         p.mixed = mixed;
-        rc = plan_pass(ctx, r, p);
-        if (rc) return rc;
         j.second = (int)second.size();
         second.push_back(std::move(p));
     }
-    rc = run_session(ctx, r, second, ctx->pin_down2);
+    rc = plan_passes(ctx, second);
+    if (rc) return rc;
+    rc = session(second, ctx->pin_down2);
     if (rc) return rc;
     const double t2 = now_seconds();
     uint64_t tmpl_first = 0, tmpl_second = 0;
@@ -589,6 +942,8 @@ int scan_bands(fbls_ctx* ctx, const fbls_ready* r, std::vector<BandJob>& jobs, b
     for (const Pass& p : second) tmpl_second += p.st.templates_scanned;
     for (BandJob& j : jobs) {
         if (j.first < 0) continue;
+        if (j.second >= 0 && second[j.second].bad) j.status = FBLS_ERR_PRECISION;
+        if (j.status) continue;
         j.st.seconds =
             (t1 - t0) * (double)first[j.first].st.templates_scanned / (double)std::max<uint64_t>(tmpl_first, 1);
         const Pass* full = nullptr;
@@ -607,11 +962,11 @@ int scan_bands(fbls_ctx* ctx, const fbls_ready* r, std::vector<BandJob>& jobs, b
             const double* rec = &full->out.records[(size_t)i * RECORD_STRIDE];
             fbls_row row;
             row.period = rec[0];
-            row.epoch = (rec[2] + rec[3] / 2.0) / rec[1] + r->origin;
+            row.epoch = (rec[2] + rec[3] / 2.0) / rec[1] + j.r->origin;
             row.duration = rec[3] / rec[1];
             row.score = sc;
             row.depth = full->out.depth[i];
-            rows.push_back(row);
+            j.rows->push_back(row);
         }
     }
     return FBLS_OK;
@@ -621,12 +976,656 @@ int scan_bands(fbls_ctx* ctx, const fbls_ready* r, std::vector<BandJob>& jobs, b
 int scan_periods(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_t P, const fbls_bank* bank,
                  bool mixed, std::vector<fbls_row>& rows, fbls_scan_stats* stats) {
     std::vector<BandJob> jobs(1);
+    jobs[0].r = r;
+    jobs[0].rows = &rows;
     jobs[0].periods = periods;
     jobs[0].P = P;
     jobs[0].bank = bank;
-    int rc = scan_bands(ctx, r, jobs, mixed, rows);
+    int rc = scan_bands(ctx, jobs, mixed, false);
     if (stats) *stats = jobs[0].st;
     return rc;
+}
+
+
+// The octave bands of signal_search (scan.rs:411-471) for one star: the grid
+// periods of each octave [lo, 2 lo) (those inside the [lo, hi) `ranges` when
+// any are given) with the durations below lo / 4, each band a BandJob over a
+// bank of its own. Jobs are appended to `jobs` with their rows going to
+// `rows`; they point into `sb`, which must outlive them. Touches no shared
+// state (a rejection's message goes to `err`), so stars are planned in
+// parallel.
+struct StarBands {
+    struct Band {
+        std::vector<double> periods, durations, rho;
+        double nb_period = 0.0;  // the octave's last grid period (sets nb)
+        fbls_bank bank{};
+    };
+    std::vector<Band> bands;
+    uint64_t grid_len = 0;
+};
+
+int plan_star_bands(std::string& err, const fbls_ready* ready, const double* durations, const double* rho,
+                    uint32_t nd, const fbls_config* cfg, const double* ranges, uint32_t n_ranges, double budget_mib,
+                    StarBands& sb, std::vector<BandJob>& jobs, std::vector<fbls_row>* rows) {
+    sb.bands.clear();
+    sb.grid_len = 0;
+    if (nd == 0) {
+        err = "no durations";
+        return FBLS_ERR_ARGUMENT;
+    }
+    auto kept = [&](double p) {
+        if (!n_ranges) return true;
+        for (uint32_t i = 0; i < n_ranges; i++)
+            if (p >= ranges[2 * i] && p < ranges[2 * i + 1]) return true;
+        return false;
+    };
+    // Durations sorted with rho carried along (scan.rs:418-424).
+    std::vector<std::pair<double, double>> ds(nd);
+    for (uint32_t i = 0; i < nd; i++) ds[i] = {durations[i], rho[i]};
+    std::stable_sort(ds.begin(), ds.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    const double baseline = ready->t_last;
+    const double maximum = rmin(cfg->period_max, baseline);
+    const double minimum = rmax(cfg->period_min, 4.0 * ds[0].first * (1.0 + 1e-9));
+    if (maximum <= minimum) return FBLS_OK;
+    const int64_t count = period_grid(minimum, maximum, baseline, ds[0].first, cfg->period_oversample, nullptr, 0);
+    std::vector<double> grid((size_t)count);
+    period_grid(minimum, maximum, baseline, ds[0].first, cfg->period_oversample, grid.data(), count);
+    sb.grid_len = (uint64_t)count;
+    const double shape_gate = cfg->n_ingress > 0 && cfg->ingress_fractions[0] == 0.0
+                                  ? cfg->shape_gate_fraction * cfg->threshold
+                                  : 0.0;
+    // Octave bands [lo, 2 lo) with the durations below lo / 4 (scan.rs:441-471);
+    // every band is scanned by scan_periods, the bands together (scan_bands).
+    // Octave k covers [los[k], los[k + 1] = 2 los[k]); one walk over the grid
+    // hands every period to its octave, in grid order.
+    std::vector<double> los;
+    const double last = grid[grid.size() - 1];
+    for (double lo = grid[0]; lo <= last; lo *= 2.0) los.push_back(lo);
+    std::vector<StarBands::Band> octaves(los.size());
+    size_t k = 0;
+    for (double p : grid) {
+        if (!(p >= los[0] && p < 2.0 * los.back())) continue;
+        while (p >= 2.0 * los[k]) k++;
+        while (p < los[k]) k--;
+        octaves[k].nb_period = p;
+        if (kept(p)) octaves[k].periods.push_back(p);
+    }
+    std::vector<StarBands::Band>& bands = sb.bands;
+    for (size_t o = 0; o < octaves.size(); o++) {
+        StarBands::Band& b = octaves[o];
+        for (auto& d : ds)
+            if (d.first < los[o] / 4.0) {
+                b.durations.push_back(d.first);
+                b.rho.push_back(d.second);
+            }
+        if (!b.periods.empty() && !b.durations.empty()) bands.push_back(std::move(b));
+    }
+    const size_t j0 = jobs.size();
+    jobs.resize(j0 + bands.size());
+    for (size_t i = 0; i < bands.size(); i++) {
+        fbls_bank& bank = bands[i].bank;
+        bank.durations = bands[i].durations.data();
+        bank.rho = bands[i].rho.data();
+        bank.nd = (uint32_t)bands[i].durations.size();
+        bank.ingress = cfg->ingress_fractions;
+        bank.ns = cfg->n_ingress;
+        bank.layers = cfg->shape_layers;
+        bank.threshold = cfg->threshold;
+        bank.shape_gate = shape_gate;
+        bank.phase_oversample = cfg->phase_oversample;
+        bank.period_batch = cfg->period_batch;
+        bank.max_fold_mib = budget_mib;
+        bank.prescan_factor = cfg->prescan_factor;
+        bank.prescan_fraction = cfg->prescan_fraction;
+        BandJob& j = jobs[j0 + i];
+        j.r = ready;
+        j.rows = rows;
+        j.periods = bands[i].periods.data();
+        j.P = (uint32_t)bands[i].periods.size();
+        j.nb_period = bands[i].nb_period;
+        j.bank = &bank;
+    }
+    return FBLS_OK;
+}
+
+
+// fbls_search_batch with workers == 0: the stars are taken in groups of at
+// most FUSED_GROUP_PERIODS grid periods (one star at least). The families of
+// a group that are not uploaded yet go up together into ctx->family, and the
+// bands of every star of the group are scanned by one scan_bands in fused
+// sessions: one fold, one scan and one merge launch per wave, whatever the
+// number of stars. Results are the same as one signal_search per star.
+constexpr uint64_t FUSED_GROUP_PERIODS = 1u << 21;
+
+int search_batch_fused(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbls_config* cfg,
+                       std::vector<std::string>& errors) {
+    const double budget_mib = fold_budget_mib(cfg->max_fold_mib);
+    const bool mixed = cfg->precision_mode == 0;
+    // A star's grid length, from the sizes alone (0 when its inputs are bad):
+    // what the groups are cut by.
+    auto grid_estimate = [&](const fbls_star& s) -> uint64_t {
+        if (!s.durations || !s.nd) return 0;
+        const double t_last = s.ready ? s.ready->t_last : (s.time && s.n ? s.time[s.n - 1] : 0.0);
+        double dmin = __builtin_huge_val();
+        for (uint32_t i = 0; i < s.nd; i++) dmin = rmin(dmin, s.durations[i]);
+        const double maximum = rmin(std::isfinite(s.period_max) ? s.period_max : cfg->period_max, t_last);
+        const double minimum = rmax(cfg->period_min, 4.0 * dmin * (1.0 + 1e-9));
+        if (!(maximum > minimum) || !(dmin > 0.0)) return 0;
+        return (uint64_t)std::max<int64_t>(0, period_grid(minimum, maximum, t_last, dmin, cfg->period_oversample,
+                                                          nullptr, 0));
+    };
+    uint32_t i0 = 0;
+    while (i0 < count) {
+        uint32_t i1 = i0;
+        for (uint64_t est = 0; i1 < count && (i1 == i0 || est < FUSED_GROUP_PERIODS); i1++) est += grid_estimate(stars[i1]);
+        const uint32_t g = i1 - i0;
+        std::vector<fbls_ready> local(g);  // families uploaded for this group
+        std::vector<uint8_t> upload(g, 0);  // bytes, not vector<bool>: set from the planning threads
+        std::vector<StarBands> sbs(g);
+        std::vector<std::vector<fbls_row>> rows(g);
+        std::vector<std::vector<BandJob>> star_jobs(g);
+        parallel_for(g, [&](size_t k) {
+            fbls_star& s = stars[i0 + k];
+            s.n_rows = 0;
+            s.grid_len = 0;
+            s.templates = 0;
+            std::string& err = errors[i0 + k];
+            const fbls_ready* r = s.ready;
+            int rc = FBLS_OK;
+            if (!s.durations || !s.rho || (s.n_ranges && !s.ranges)) {
+                err = "null argument";
+                rc = FBLS_ERR_ARGUMENT;
+            }
+            if (rc == FBLS_OK && !r) {
+                rc = check_family(err, s.time, s.v, s.w, s.n);
+                if (rc == FBLS_OK) {
+                    fbls_ready& f = local[k];
+                    f.ctx = ctx;
+                    f.n = s.n;
+                    f.baseline_norm = s.baseline_norm;
+                    f.origin = s.origin;
+                    f.residual_energy = s.residual_energy;
+                    f.t_last = s.time[s.n - 1];
+                    f.time_host.assign(s.time, s.time + s.n);
+                    f.owned = false;
+                    upload[k] = 1;
+                    r = &f;
+                }
+            }
+            if (rc == FBLS_OK) {
+                fbls_config c = *cfg;
+                if (std::isfinite(s.period_max)) c.period_max = s.period_max;
+                rc = plan_star_bands(err, r, s.durations, s.rho, s.nd, &c, s.ranges, s.n_ranges, budget_mib, sbs[k],
+                                     star_jobs[k], &rows[k]);
+                s.grid_len = sbs[k].grid_len;
+            }
+            s.status = rc;
+        });
+        std::vector<BandJob> jobs;
+        std::vector<uint32_t> job_star;
+        std::vector<std::pair<uint32_t, fbls_ready*>> uploads;
+        for (uint32_t k = 0; k < g; k++) {
+            if (upload[k]) uploads.push_back({i0 + k, &local[k]});
+            for (BandJob& j : star_jobs[k]) {
+                jobs.push_back(std::move(j));
+                job_star.push_back(i0 + k);
+            }
+        }
+        // The group's new families: one copy from page-locked staging, each at
+        // a 256-byte aligned offset, zero-padded like upload_family's.
+        if (!uploads.empty()) {
+            std::vector<size_t> offs;
+            size_t total = 0;
+            for (auto& u : uploads) {
+                offs.push_back(total);
+                total += align256(3 * fold_field_stride(u.second->n) * sizeof(double));
+            }
+            CK(ensure(ctx->family, total), "workspace");
+            CK(ensure_pinned(ctx->pin_up, total), "pinned workspace");
+            unsigned char* host = static_cast<unsigned char*>(ctx->pin_up.ptr);
+            parallel_for(uploads.size(), [&](size_t k) {
+                const fbls_star& s = stars[uploads[k].first];
+                fbls_ready* f = uploads[k].second;
+                const size_t stride = fold_field_stride(f->n);
+                double* h = reinterpret_cast<double*>(host + offs[k]);
+                const size_t end = (k + 1 < uploads.size() ? offs[k + 1] : total) / sizeof(double);
+                std::memset(h, 0, (end - offs[k] / sizeof(double)) * sizeof(double));
+                std::memcpy(h, s.time, f->n * sizeof(double));
+                std::memcpy(h + stride, s.v, f->n * sizeof(double));
+                std::memcpy(h + 2 * stride, s.w, f->n * sizeof(double));
+                f->time = reinterpret_cast<double*>(static_cast<unsigned char*>(ctx->family.ptr) + offs[k]);
+                f->v = f->time + stride;
+                f->w = f->v + stride;
+            });
+            CK(cudaMemcpyAsync(ctx->family.ptr, host, total, cudaMemcpyHostToDevice, ctx->stream), "upload_ready");
+            CK(cudaStreamSynchronize(ctx->stream), "upload_ready");  // the sessions reuse the staging buffer
+        }
+        const int rc = scan_bands(ctx, jobs, mixed, true);
+        for (size_t j = 0; j < jobs.size(); j++) {
+            fbls_star& s = stars[job_star[j]];
+            if (s.status) continue;
+            if (rc) {
+                s.status = rc;
+                errors[job_star[j]] = ctx->error;
+            } else if (jobs[j].status) {
+                s.status = jobs[j].status;
+                errors[job_star[j]] = "nonpositive template precision; inspect noise model";
+            } else {
+                s.templates += jobs[j].st.templates_scanned;
+            }
+        }
+        for (uint32_t i = i0; i < i1; i++) {
+            fbls_star& s = stars[i];
+            if (s.status) {
+                s.templates = 0;
+                continue;
+            }
+            const std::vector<fbls_row>& rr = rows[i - i0];  // filled by scan_bands
+            if (s.rows) std::memcpy(s.rows, rr.data(), std::min<size_t>(rr.size(), s.capacity) * sizeof(fbls_row));
+            s.n_rows = (uint32_t)rr.size();
+        }
+        i0 = i1;
+    }
+    return FBLS_OK;
+}
+
+
+// A coarse map (fbls_coarse_map) planned on the host: its time bins when
+// bin_days > 0 (observations whose floor((t - t0) / bin_days) agree, summed at
+// their mean time) and its octave groups [lo, 2 lo), each folded at nb =
+// max(8, ceil(oversample * (group's longest period) / shortest duration)) in
+// launches of at most per_launch periods. plan_map writes only the plan, so
+// the plans of a batch are made in parallel.
+struct MapPlan {
+    fbls_map_job* job = nullptr;
+    int star = 0;             // index of the job in its batch
+    bool need_out = true;     // job->out must be given (else only features are made)
+    bool use_bins = false;
+    fbls_ready bins;          // the binned family (use_bins); device fields set by run_maps
+    std::vector<int> starts;  // nbins + 1 observation offsets of the bins
+    struct Group {
+        uint32_t i0 = 0, count = 0, nb = 0, per_launch = 0;
+        FoldShape shape{};
+        std::vector<int> chunks;
+        size_t off_scales = 0, off_chunks = 0;
+    };
+    std::vector<Group> groups;
+    size_t off_time = 0, off_starts = 0, in_bytes = 0;  // within the plan's upload region (bank at 0)
+    size_t in_off = 0, out_off = 0, bin_off = 0;          // the plan's regions in its run
+    std::string err;
+    const fbls_ready* ready() const { return use_bins ? &bins : job->ready; }
+};
+
+int plan_map(const fbls_ctx* ctx, MapPlan& m) {
+    const fbls_map_job& j = *m.job;
+    auto bad = [&](int status, const char* message) {
+        m.err = message;
+        return status;
+    };
+    if (!j.ready || (j.P && !j.periods) || !j.durations || !j.rho || (m.need_out && !j.out))
+        return bad(FBLS_ERR_ARGUMENT, "null argument");
+    if (!(j.bin_days >= 0.0)) return bad(FBLS_ERR_ARGUMENT, "bin_days must not be negative");
+    if (j.nd < 1 || j.nd > (uint32_t)MAP_MAX_DURATIONS) return bad(FBLS_ERR_ARGUMENT, "1 to 8 map durations");
+    if (j.P == 0) return FBLS_OK;
+    if (!(j.oversample > 0.0)) return bad(FBLS_ERR_ARGUMENT, "oversample must be positive");
+    for (uint32_t i = 0; i < j.P; i++)
+        if (!(j.periods[i] > 0.0) || !std::isfinite(j.periods[i]) || (i && !(j.periods[i] > j.periods[i - 1])))
+            return bad(FBLS_ERR_ARGUMENT, "periods must be positive, finite and ascending");
+    double dmin = __builtin_huge_val();
+    for (uint32_t i = 0; i < j.nd; i++) {
+        if (!(j.durations[i] > 0.0) || !(j.rho[i] > 0.0)) return bad(FBLS_ERR_ARGUMENT, "bad map duration");
+        dmin = rmin(dmin, j.durations[i]);
+    }
+    const fbls_ready* family = j.ready;
+    if (j.bin_days > 0.0) {
+        const std::vector<double>& t = family->time_host;
+        std::vector<double>& tb = m.bins.time_host;
+        tb.clear();
+        m.starts.clear();
+        for (uint32_t i = 0; i < family->n;) {
+            const double b = std::floor((t[i] - t[0]) / j.bin_days);
+            uint32_t k = i;
+            double sum = 0.0;
+            while (k < family->n && std::floor((t[k] - t[0]) / j.bin_days) == b) sum += t[k++];
+            m.starts.push_back((int)i);
+            tb.push_back(sum / (double)(k - i));
+            i = k;
+        }
+        m.starts.push_back((int)family->n);
+        m.use_bins = true;
+        m.bins.n = (uint32_t)tb.size();
+        m.bins.baseline_norm = family->baseline_norm;
+        m.bins.origin = family->origin;
+        m.bins.residual_energy = family->residual_energy;
+        m.bins.t_last = tb.back();
+        m.bins.owned = false;
+    }
+    const fbls_ready* ready = m.ready();
+    size_t in_bytes = align256(2 * j.nd * sizeof(double));
+    if (m.use_bins) {
+        m.off_time = in_bytes;
+        in_bytes += align256(fold_field_stride(m.bins.n) * sizeof(double));
+        m.off_starts = in_bytes;
+        in_bytes += align256(m.starts.size() * sizeof(int));
+    }
+    m.groups.clear();
+    for (uint32_t i0 = 0; i0 < j.P;) {
+        uint32_t i1 = i0 + 1;
+        while (i1 < j.P && j.periods[i1] < 2.0 * j.periods[i0]) i1++;
+        MapPlan::Group g;
+        g.i0 = i0;
+        g.count = i1 - i0;
+        const uint64_t nb = std::max<uint64_t>(8, as_u64(std::ceil(j.oversample * j.periods[i1 - 1] / dmin)));
+        if (nb > (1u << 24)) return bad(FBLS_ERR_ARGUMENT, "phase grid too large");
+        g.nb = (uint32_t)nb;
+        const double scale_max = (double)nb / j.periods[i0];
+        if (std::floor(ready->t_last * scale_max) >= 4294967295.0 - 2.0 * (double)nb - 2.0)
+            return bad(FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
+        const size_t stride = 2 * (size_t)nb + 1;
+        g.per_launch = (uint32_t)std::max<size_t>(1, std::min<size_t>(16384, (512ull << 20) / (NF * stride * 12)));
+        g.shape = fold_group_shape((int)nb, (int)std::min(g.count, g.per_launch), ctx->sm_count);
+        g.chunks.resize((size_t)ready->n + 2);
+        const int c = fold_chunks(ready->time_host.data(), (int)ready->n, scale_max, (int)nb, g.shape.span_cap,
+                                  g.shape.chunk_cap, g.chunks.data(), (int)g.chunks.size());
+        if (c < 1) return bad(FBLS_ERR_ARGUMENT, "fold chunking failed");
+        g.chunks.resize((size_t)c + 1);
+        g.off_scales = in_bytes;
+        in_bytes += align256(g.count * sizeof(double));
+        g.off_chunks = in_bytes;
+        in_bytes += align256(g.chunks.size() * sizeof(int));
+        m.groups.push_back(std::move(g));
+        i0 = i1;
+    }
+    m.in_bytes = in_bytes;
+    return FBLS_OK;
+}
+
+// Runs planned maps on ctx->stream: one upload, one launch for every star's
+// bins, then waves of fold units (a group's launch of at most per_launch
+// periods) whose prefix sums fit MAP_WAVE_BYTES, each wave one fold launch
+// (walking folds as jobs; any other fold on its own) and one box-map launch;
+// with `feat`, one k_map_features launch writing the maps' network input into
+// feat->x (device); one download and one synchronisation; each map is copied
+// to its job's out when there is one.
+constexpr size_t MAP_WAVE_BYTES = 1536ull << 20;
+
+struct MapFeatures {
+    float* x = nullptr;  // device, channels x B x T, zeroed
+    int channels = 0, B = 0, T = 0;
+    const uint32_t* offsets = nullptr;  // per star
+};
+
+int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeatures* feat) {
+    if (plans.empty()) return FBLS_OK;
+    struct Unit {
+        MapPlan* m;
+        const MapPlan::Group* g;
+        uint32_t c0;
+        int n;
+        size_t cum_off, hist_off;
+        bool walk;
+    };
+    struct Wave {
+        std::vector<Unit> units;
+        size_t cum = 0, hist = 0, smem = 0;
+        int fold_jobs = 0, fold_ctas = 0, map_total = 0;
+        size_t off_fold = 0, off_fcta = 0, off_map = 0, off_mp = 0;
+    };
+    size_t in_total = 0, out_total = 0, bin_total = 0;
+    int nbinned = 0, bin_total_bins = 0;
+    std::vector<Wave> waves(1);
+    for (MapPlan* m : plans) {
+        m->in_off = in_total;
+        in_total += m->in_bytes;
+        m->out_off = out_total;
+        out_total += align256((size_t)m->job->P * m->job->nd * sizeof(float));
+        if (m->use_bins) {
+            m->bin_off = bin_total;
+            bin_total += align256(2 * fold_field_stride(m->bins.n) * sizeof(double));
+            nbinned++;
+            bin_total_bins += (int)m->bins.n;
+        }
+        for (const MapPlan::Group& g : m->groups) {
+            const size_t stride = 2 * (size_t)g.nb + 1;
+            for (uint32_t c0 = 0; c0 < g.count; c0 += g.per_launch) {
+                const int n = (int)std::min(g.count - c0, g.per_launch);
+                const size_t cum = (size_t)n * NF * stride;
+                const bool walk = g.shape.kind == FOLD_WALK;
+                const size_t hist = walk ? 0 : ((n + g.shape.group - 1) / g.shape.group) * (size_t)g.shape.group *
+                                                   NF * (size_t)g.shape.row_stride;
+                if (!waves.back().units.empty() &&
+                    (waves.back().cum + cum) * (sizeof(double) + sizeof(float2)) > MAP_WAVE_BYTES)
+                    waves.emplace_back();
+                Wave& w = waves.back();
+                w.units.push_back({m, &g, c0, n, w.cum, w.hist, walk});
+                w.cum += cum;
+                w.hist += hist;
+                if (walk) {
+                    w.fold_jobs++;
+                    w.fold_ctas += (n + g.shape.group - 1) / g.shape.group;
+                    w.smem = std::max(w.smem, g.shape.smem);
+                }
+                w.map_total += n;
+            }
+        }
+    }
+    size_t blob = in_total;
+    auto take = [&](size_t bytes) {
+        const size_t at = blob;
+        blob += align256(bytes);
+        return at;
+    };
+    const size_t off_bins = take(std::max(1, nbinned) * sizeof(BinJob)), off_b0 = take((nbinned + 1) * sizeof(int));
+    const size_t off_feat = take(plans.size() * sizeof(FeatJob));
+    size_t cum_max = 0, hist_max = 0;
+    for (Wave& w : waves) {
+        cum_max = std::max(cum_max, w.cum);
+        hist_max = std::max(hist_max, w.hist);
+        w.off_fold = take(std::max(1, w.fold_jobs) * sizeof(FoldArgs));
+        w.off_fcta = take((w.fold_jobs + 1) * sizeof(int));
+        w.off_map = take(w.units.size() * sizeof(MapArgs));
+        w.off_mp = take((w.units.size() + 1) * sizeof(int));
+    }
+    CK(ensure(ctx->pass_in, blob), "workspace");
+    CK(ensure(ctx->pass_out, out_total), "workspace");
+    CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
+    CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
+    if (hist_max) CK(ensure(ctx->hist, hist_max * sizeof(double)), "workspace");
+    if (bin_total) CK(ensure(ctx->mapbin, bin_total), "workspace");
+    CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
+    CK(ensure_pinned(ctx->pin_up, blob), "pinned workspace");
+    CK(ensure_pinned(ctx->pin_down, out_total + 256), "pinned workspace");
+    unsigned char* up = static_cast<unsigned char*>(ctx->pin_up.ptr);
+    unsigned char* din = static_cast<unsigned char*>(ctx->pass_in.ptr);
+    unsigned char* dout = static_cast<unsigned char*>(ctx->pass_out.ptr);
+    unsigned char* dbin = static_cast<unsigned char*>(ctx->mapbin.ptr);
+    BinJob* bj = reinterpret_cast<BinJob*>(up + off_bins);
+    int* b0 = reinterpret_cast<int*>(up + off_b0);
+    int nb_jobs = 0, nb_bins = 0;
+    for (MapPlan* m : plans) {
+        const fbls_map_job& j = *m->job;
+        unsigned char* b = up + m->in_off;
+        std::memcpy(b, j.durations, j.nd * sizeof(double));
+        std::memcpy(b + j.nd * sizeof(double), j.rho, j.nd * sizeof(double));
+        if (m->use_bins) {
+            const size_t stride = fold_field_stride(m->bins.n);
+            double* t = reinterpret_cast<double*>(b + m->off_time);
+            std::memcpy(t, m->bins.time_host.data(), m->bins.n * sizeof(double));
+            std::memset(t + m->bins.n, 0, (stride - m->bins.n) * sizeof(double));
+            std::memcpy(b + m->off_starts, m->starts.data(), m->starts.size() * sizeof(int));
+            m->bins.time = reinterpret_cast<double*>(din + m->in_off + m->off_time);
+            m->bins.v = reinterpret_cast<double*>(dbin + m->bin_off);
+            m->bins.w = m->bins.v + stride;
+            bj[nb_jobs] = {j.ready->v, j.ready->w, reinterpret_cast<const int*>(din + m->in_off + m->off_starts),
+                           (int)m->bins.n, m->bins.v, m->bins.w};
+            b0[nb_jobs++] = nb_bins;
+            nb_bins += (int)m->bins.n;
+        }
+        for (const MapPlan::Group& g : m->groups) {
+            double* sc = reinterpret_cast<double*>(b + g.off_scales);
+            for (uint32_t i = 0; i < g.count; i++) sc[i] = (double)g.nb / j.periods[g.i0 + i];
+            std::memcpy(b + g.off_chunks, g.chunks.data(), g.chunks.size() * sizeof(int));
+        }
+    }
+    b0[nb_jobs] = nb_bins;
+    FeatJob* fjobs = reinterpret_cast<FeatJob*>(up + off_feat);
+    bool any_out = false;
+    for (size_t k = 0; k < plans.size(); k++) {
+        const MapPlan* m = plans[k];
+        any_out = any_out || m->job->out;
+        fjobs[k] = {reinterpret_cast<const float*>(dout + m->out_off), (int)m->job->P, (int)m->job->nd, m->star,
+                    feat ? (int)feat->offsets[m->star] : 0};
+    }
+    std::vector<FoldArgs> own;  // folds that are not walking folds: their own launches
+    std::vector<const FoldShape*> own_shape;
+    std::vector<size_t> own_wave;
+    for (size_t wi = 0; wi < waves.size(); wi++) {
+        Wave& w = waves[wi];
+        FoldArgs* fj = reinterpret_cast<FoldArgs*>(up + w.off_fold);
+        int* fc = reinterpret_cast<int*>(up + w.off_fcta);
+        MapArgs* mj = reinterpret_cast<MapArgs*>(up + w.off_map);
+        int* mp = reinterpret_cast<int*>(up + w.off_mp);
+        int nf = 0, fcta = 0, mtot = 0;
+        for (size_t u = 0; u < w.units.size(); u++) {
+            const Unit& un = w.units[u];
+            const MapPlan& m = *un.m;
+            const MapPlan::Group& g = *un.g;
+            const fbls_ready* r = m.ready();
+            const unsigned char* b = din + m.in_off;
+            FoldArgs fa{};
+            fa.time = r->time;
+            fa.v = r->v;
+            fa.w = r->w;
+            fa.scales = reinterpret_cast<const double*>(b + g.off_scales) + un.c0;
+            fa.n = (int)r->n;
+            fa.nb = (int)g.nb;
+            fa.periods = un.n;
+            fa.group = g.shape.group;
+            fa.cum = as<double>(ctx->cum) + un.cum_off;
+            fa.cum32 = as<float2>(ctx->cum32) + un.cum_off;
+            fa.hist_global = un.walk ? nullptr : as<double>(ctx->hist) + un.hist_off;
+            fa.hist_out = nullptr;
+            fa.chunks = reinterpret_cast<const int*>(b + g.off_chunks);
+            fa.nchunks = (int)g.chunks.size() - 1;
+            fa.stage_field = g.shape.stage_field;
+            fa.window = g.shape.window;
+            fa.row_stride = g.shape.row_stride;
+            fa.fault = as<uint32_t>(ctx->fault);
+            if (un.walk) {
+                if (!fold_job_ok(fa, g.shape)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
+                fj[nf] = fa;
+                fc[nf++] = fcta;
+                fcta += (un.n + g.shape.group - 1) / g.shape.group;
+            } else {
+                own.push_back(fa);
+                own_shape.push_back(&g.shape);
+                own_wave.push_back(wi);
+            }
+            MapArgs ma{};
+            ma.cum = fa.cum;
+            ma.scales = fa.scales;
+            ma.durations = reinterpret_cast<const double*>(b);
+            ma.rho = reinterpret_cast<const double*>(b) + m.job->nd;
+            ma.nd = (int)m.job->nd;
+            ma.nb = (int)g.nb;
+            ma.baseline = r->baseline_norm;
+            ma.n = (double)r->n;
+            ma.out = reinterpret_cast<float*>(dout + m.out_off) + (size_t)(g.i0 + un.c0) * m.job->nd;
+            mj[u] = ma;
+            mp[u] = mtot;
+            mtot += un.n;
+            ctx->counters.fold_updates += (uint64_t)un.n * r->n;
+        }
+        fc[nf] = fcta;
+        mp[w.units.size()] = mtot;
+    }
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
+    if (bin_total) CK(cudaMemsetAsync(ctx->mapbin.ptr, 0, bin_total, s), "workspace");
+    CK(cudaMemcpyAsync(din, up, blob, cudaMemcpyHostToDevice, s), "upload");
+    if (nb_jobs) {
+        CK(launch_bin_fields_jobs(reinterpret_cast<const BinJob*>(din + off_bins),
+                                  reinterpret_cast<const int*>(din + off_b0), nb_jobs, nb_bins, s),
+           "bins");
+        ctx->counters.launches += 1;
+    }
+    size_t oi = 0;
+    for (size_t wi = 0; wi < waves.size(); wi++) {
+        const Wave& w = waves[wi];
+        if (w.fold_jobs) {
+            CK(launch_fold_jobs(reinterpret_cast<const FoldArgs*>(din + w.off_fold),
+                                reinterpret_cast<const int*>(din + w.off_fcta), w.fold_jobs, w.fold_ctas, w.smem, s),
+               "fold");
+            ctx->counters.launches += 1;
+        }
+        for (; oi < own.size() && own_wave[oi] == wi; oi++) {
+            CK(launch_fold(own[oi], *own_shape[oi], s), "fold");
+            ctx->counters.launches += 1;
+        }
+        CK(launch_box_map_jobs(reinterpret_cast<const MapArgs*>(din + w.off_map),
+                               reinterpret_cast<const int*>(din + w.off_mp), (int)w.units.size(), w.map_total, s),
+           "box map");
+        ctx->counters.launches += 1;
+    }
+    if (feat) {
+        CK(launch_map_features(reinterpret_cast<const FeatJob*>(din + off_feat), (int)plans.size(), feat->channels,
+                               feat->B, feat->T, feat->x, s),
+           "map features");
+        ctx->counters.launches += 1;
+    }
+    unsigned char* down = static_cast<unsigned char*>(ctx->pin_down.ptr);
+    if (any_out) CK(cudaMemcpyAsync(down, dout, out_total, cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaMemcpyAsync(down + out_total, ctx->fault.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaStreamSynchronize(s), "coarse map");
+    uint32_t fault = 0;
+    std::memcpy(&fault, down + out_total, sizeof(uint32_t));
+    if (fault) return fail(ctx, FBLS_ERR_CUDA, "fold: staging copies did not complete");
+    for (MapPlan* m : plans)
+        if (m->job->out) std::memcpy(m->job->out, down + m->out_off, (size_t)m->job->P * m->job->nd * sizeof(float));
+    return FBLS_OK;
+}
+
+// Plans (in parallel) and runs the maps of `jobs` on ctx, in runs of at most
+// MAP_RUN_PERIODS periods; every job's status is set, a failing job's message
+// goes to errors[i]. Returns a failure of the device work itself, else 0.
+constexpr uint64_t MAP_RUN_PERIODS = 1u << 22;
+
+int coarse_maps(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, std::vector<std::string>& errors,
+                const MapFeatures* feat = nullptr) {
+    std::vector<MapPlan> plans(count);
+    std::vector<int> rc(count, FBLS_OK);
+    for (uint32_t i = 0; i < count; i++) {
+        plans[i].job = &jobs[i];
+        plans[i].star = (int)i;
+        plans[i].need_out = feat == nullptr;
+    }
+    parallel_for(count, [&](size_t i) { rc[i] = plan_map(ctx, plans[i]); });
+    std::vector<MapPlan*> run;
+    uint64_t periods = 0;
+    for (uint32_t i = 0; i <= count; i++) {
+        if (i == count || (!run.empty() && periods + jobs[i].P > MAP_RUN_PERIODS)) {
+            const int e = run_maps(ctx, run, feat);
+            if (e) {
+                for (MapPlan* m : run) {
+                    m->job->status = e;
+                    errors[m->job - jobs] = ctx->error;
+                }
+                return e;
+            }
+            run.clear();
+            periods = 0;
+            if (i == count) break;
+        }
+        jobs[i].status = rc[i];
+        if (rc[i]) {
+            errors[i] = plans[i].err;
+            continue;
+        }
+        if (plans[i].groups.empty()) continue;
+        run.push_back(&plans[i]);
+        periods += jobs[i].P;
+    }
+    return FBLS_OK;
 }
 
 }  // namespace
@@ -662,7 +1661,7 @@ void fbls_destroy(fbls_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf* bufs[] = {&ctx->cum,     &ctx->cum32,    &ctx->hist,     &ctx->parts, &ctx->keys,  &ctx->tflags,
-                      &ctx->pass_in, &ctx->pass_out, &ctx->evidence, &ctx->fault, &ctx->family, &ctx->mapbin};
+                      &ctx->pass_in, &ctx->pass_out, &ctx->evidence, &ctx->fault, &ctx->family, &ctx->mapbin, &ctx->feat};
     for (DevBuf* b : bufs) release(*b);
     for (PinBuf* b : {&ctx->pin_up, &ctx->pin_down, &ctx->pin_down2})
         if (b->ptr) cudaFreeHost(b->ptr);
@@ -814,82 +1813,18 @@ int fbls_signal_search_ranges(fbls_ctx* ctx, const fbls_ready* ready, const doub
                               fbls_scan_stats* stats_out, uint32_t* n_bands) {
     if (!ctx || !ready || !durations || !rho || !cfg || !n_rows || (n_ranges && !ranges))
         return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    if (nd == 0) return fail(ctx, FBLS_ERR_ARGUMENT, "no durations");
-    auto kept = [&](double p) {
-        if (!n_ranges) return true;
-        for (uint32_t i = 0; i < n_ranges; i++)
-            if (p >= ranges[2 * i] && p < ranges[2 * i + 1]) return true;
-        return false;
-    };
     CK(cudaSetDevice(ctx->device), "set device");
-    // Durations sorted with rho carried along (scan.rs:418-424).
-    std::vector<std::pair<double, double>> ds(nd);
-    for (uint32_t i = 0; i < nd; i++) ds[i] = {durations[i], rho[i]};
-    std::stable_sort(ds.begin(), ds.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    const double baseline = ready->t_last;
-    const double maximum = rmin(cfg->period_max, baseline);
-    const double minimum = rmax(cfg->period_min, 4.0 * ds[0].first * (1.0 + 1e-9));
-    *n_rows = 0;
-    if (grid_len) *grid_len = 0;
-    if (n_bands) *n_bands = 0;
-    if (maximum <= minimum) return FBLS_OK;
-    const int64_t count = period_grid(minimum, maximum, baseline, ds[0].first, cfg->period_oversample, nullptr, 0);
-    std::vector<double> grid((size_t)count);
-    period_grid(minimum, maximum, baseline, ds[0].first, cfg->period_oversample, grid.data(), count);
-    if (grid_len) *grid_len = (uint64_t)count;
-    const double shape_gate = cfg->n_ingress > 0 && cfg->ingress_fractions[0] == 0.0
-                                  ? cfg->shape_gate_fraction * cfg->threshold
-                                  : 0.0;
-    // Octave bands [lo, 2 lo) with the durations below lo / 4 (scan.rs:441-471);
-    // every band is scanned by scan_periods, the bands together (scan_bands).
-    struct Band {
-        std::vector<double> periods, durations, rho;
-        double nb_period = 0.0;  // the octave's last grid period (sets nb)
-        fbls_bank bank;
-    };
-    std::vector<Band> bands;
-    const double budget_mib = fold_budget_mib(cfg->max_fold_mib);
-    double lo = grid[0];
-    const double last = grid[grid.size() - 1];
-    while (lo <= last) {
-        const double hi = lo * 2.0;
-        Band b;
-        for (double p : grid)
-            if (p >= lo && p < hi) {
-                b.nb_period = p;
-                if (kept(p)) b.periods.push_back(p);
-            }
-        for (auto& d : ds)
-            if (d.first < lo / 4.0) {
-                b.durations.push_back(d.first);
-                b.rho.push_back(d.second);
-            }
-        if (!b.periods.empty() && !b.durations.empty()) bands.push_back(std::move(b));
-        lo = hi;
-    }
-    std::vector<BandJob> jobs(bands.size());
-    for (size_t i = 0; i < bands.size(); i++) {
-        fbls_bank& bank = bands[i].bank;
-        bank.durations = bands[i].durations.data();
-        bank.rho = bands[i].rho.data();
-        bank.nd = (uint32_t)bands[i].durations.size();
-        bank.ingress = cfg->ingress_fractions;
-        bank.ns = cfg->n_ingress;
-        bank.layers = cfg->shape_layers;
-        bank.threshold = cfg->threshold;
-        bank.shape_gate = shape_gate;
-        bank.phase_oversample = cfg->phase_oversample;
-        bank.period_batch = cfg->period_batch;
-        bank.max_fold_mib = budget_mib;
-        bank.prescan_factor = cfg->prescan_factor;
-        bank.prescan_fraction = cfg->prescan_fraction;
-        jobs[i].periods = bands[i].periods.data();
-        jobs[i].P = (uint32_t)bands[i].periods.size();
-        jobs[i].nb_period = bands[i].nb_period;
-        jobs[i].bank = &bank;
-    }
+    StarBands sb;
+    std::vector<BandJob> jobs;
     std::vector<fbls_row> rows;
-    const int rc = scan_bands(ctx, ready, jobs, cfg->precision_mode == 0, rows);
+    std::string err;
+    int rc = plan_star_bands(err, ready, durations, rho, nd, cfg, ranges, n_ranges, fold_budget_mib(cfg->max_fold_mib),
+                             sb, jobs, &rows);
+    *n_rows = 0;
+    if (grid_len) *grid_len = sb.grid_len;
+    if (n_bands) *n_bands = 0;
+    if (rc) return fail(ctx, rc, err);
+    rc = scan_bands(ctx, jobs, cfg->precision_mode == 0, false);
     if (rc) return rc;
     for (size_t i = 0; i < jobs.size() && stats_out && i < 64; i++) stats_out[i] = jobs[i].st;
     const uint32_t n_scanned = (uint32_t)jobs.size();
@@ -919,177 +1854,18 @@ int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* du
     return FBLS_OK;
 }
 
-// Coarse periodogram of a family for the proposal network: periods are cut
-// into octave groups [lo, 2 lo), each folded at nb = max(8, ceil(oversample *
-// (group's longest period) / shortest duration)) and scanned by k_box_map.
+// Coarse periodogram of a family for the proposal network (plan_map, then
+// run_maps: the octave groups' folds and box maps as job launches).
 int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* family, const double* periods, uint32_t P,
                     const double* durations, const double* rho, uint32_t nd, double oversample, double bin_days,
                     float* out) {
-    if (!ctx || !family || !periods || !durations || !rho || !out) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    if (!(bin_days >= 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "bin_days must not be negative");
-    if (nd < 1 || nd > (uint32_t)MAP_MAX_DURATIONS) return fail(ctx, FBLS_ERR_ARGUMENT, "1 to 8 map durations");
-    if (P == 0) return FBLS_OK;
-    if (!(oversample > 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "oversample must be positive");
-    for (uint32_t i = 0; i < P; i++)
-        if (!(periods[i] > 0.0) || !std::isfinite(periods[i]) || (i && !(periods[i] > periods[i - 1])))
-            return fail(ctx, FBLS_ERR_ARGUMENT, "periods must be positive, finite and ascending");
-    double dmin = __builtin_huge_val();
-    for (uint32_t i = 0; i < nd; i++) {
-        if (!(durations[i] > 0.0) || !(rho[i] > 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "bad map duration");
-        dmin = rmin(dmin, durations[i]);
-    }
+    if (!ctx) return FBLS_ERR_ARGUMENT;
     CK(cudaSetDevice(ctx->device), "set device");
-    // Optional time bins: observations whose floor((t - t0) / bin_days) agree
-    // are summed (v, w) at their mean time, into the context's map buffer.
-    fbls_ready binned;
-    const fbls_ready* ready = family;
-    if (bin_days > 0.0) {
-        const std::vector<double>& t = family->time_host;
-        std::vector<int> starts;
-        std::vector<double>& tb = binned.time_host;
-        for (uint32_t i = 0; i < family->n;) {
-            const double b = std::floor((t[i] - t[0]) / bin_days);
-            uint32_t j = i;
-            double sum = 0.0;
-            while (j < family->n && std::floor((t[j] - t[0]) / bin_days) == b) sum += t[j++];
-            starts.push_back((int)i);
-            tb.push_back(sum / (double)(j - i));
-            i = j;
-        }
-        starts.push_back((int)family->n);
-        const uint32_t nbins = (uint32_t)tb.size();
-        const size_t stride = fold_field_stride(nbins);
-        CK(ensure(ctx->mapbin, 3 * stride * sizeof(double) + align256((nbins + 1) * sizeof(int))), "workspace");
-        double* base = static_cast<double*>(ctx->mapbin.ptr);
-        int* d_starts = reinterpret_cast<int*>(base + 3 * stride);
-        cudaStream_t s = ctx->stream;
-        CK(cudaMemsetAsync(base, 0, 3 * stride * sizeof(double), s), "workspace");
-        CK(cudaMemcpyAsync(base, tb.data(), nbins * sizeof(double), cudaMemcpyHostToDevice, s), "upload bins");
-        CK(cudaMemcpyAsync(d_starts, starts.data(), starts.size() * sizeof(int), cudaMemcpyHostToDevice, s),
-           "upload bins");
-        CK(launch_bin_fields(family->v, family->w, d_starts, (int)nbins, base + stride, base + 2 * stride, s), "bins");
-        binned.ctx = ctx;
-        binned.time = base;
-        binned.v = base + stride;
-        binned.w = base + 2 * stride;
-        binned.n = nbins;
-        binned.baseline_norm = family->baseline_norm;
-        binned.origin = family->origin;
-        binned.residual_energy = family->residual_energy;
-        binned.t_last = tb.back();
-        binned.owned = false;
-        ready = &binned;
-    }
-    struct Group {
-        uint32_t i0, count, nb;
-        FoldShape shape;
-        std::vector<int> chunks;
-        size_t off_scales, off_chunks;
-    };
-    std::vector<Group> groups;
-    size_t in_bytes = align256(2 * nd * sizeof(double)), cum_max = 0, hist_max = 0;
-    for (uint32_t i0 = 0; i0 < P;) {
-        uint32_t i1 = i0 + 1;
-        while (i1 < P && periods[i1] < 2.0 * periods[i0]) i1++;
-        Group g;
-        g.i0 = i0;
-        g.count = i1 - i0;
-        const uint64_t nb = std::max<uint64_t>(8, as_u64(std::ceil(oversample * periods[i1 - 1] / dmin)));
-        if (nb > (1u << 24)) return fail(ctx, FBLS_ERR_ARGUMENT, "phase grid too large");
-        g.nb = (uint32_t)nb;
-        const double scale_max = (double)nb / periods[i0];
-        if (std::floor(ready->t_last * scale_max) >= 4294967295.0 - 2.0 * (double)nb - 2.0)
-            return fail(ctx, FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
-        const size_t stride = 2 * (size_t)nb + 1;
-        const uint32_t per_launch =
-            (uint32_t)std::max<size_t>(1, std::min<size_t>(16384, (512ull << 20) / (NF * stride * 12)));
-        g.shape = fold_group_shape((int)nb, (int)std::min(g.count, per_launch), ctx->sm_count);
-        g.chunks.resize((size_t)ready->n + 2);
-        const int c = fold_chunks(ready->time_host.data(), (int)ready->n, scale_max, (int)nb, g.shape.span_cap,
-                                  g.shape.chunk_cap, g.chunks.data(), (int)g.chunks.size());
-        if (c < 1) return fail(ctx, FBLS_ERR_ARGUMENT, "fold chunking failed");
-        g.chunks.resize((size_t)c + 1);
-        g.off_scales = in_bytes;
-        in_bytes += align256(g.count * sizeof(double));
-        g.off_chunks = in_bytes;
-        in_bytes += align256(g.chunks.size() * sizeof(int));
-        const size_t launch = std::min(g.count, per_launch);
-        cum_max = std::max(cum_max, launch * NF * stride);
-        if (!g.shape.hist_in_smem)
-            hist_max = std::max(hist_max, ((launch + g.shape.group - 1) / g.shape.group) * g.shape.group * NF *
-                                              (size_t)g.shape.row_stride);
-        groups.push_back(std::move(g));
-        i0 = i1;
-    }
-    const size_t out_bytes = (size_t)P * nd * sizeof(float);
-    CK(ensure(ctx->pass_in, in_bytes), "workspace");
-    CK(ensure(ctx->pass_out, out_bytes), "workspace");
-    CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
-    CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
-    if (hist_max) CK(ensure(ctx->hist, hist_max * sizeof(double)), "workspace");
-    CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
-    CK(ensure_pinned(ctx->pin_up, in_bytes), "pinned workspace");
-    CK(ensure_pinned(ctx->pin_down, out_bytes + 256), "pinned workspace");
-    unsigned char* up = static_cast<unsigned char*>(ctx->pin_up.ptr);
-    std::memcpy(up, durations, nd * sizeof(double));
-    std::memcpy(up + nd * sizeof(double), rho, nd * sizeof(double));
-    for (const Group& g : groups) {
-        double* sc = reinterpret_cast<double*>(up + g.off_scales);
-        for (uint32_t i = 0; i < g.count; i++) sc[i] = (double)g.nb / periods[g.i0 + i];
-        std::memcpy(up + g.off_chunks, g.chunks.data(), g.chunks.size() * sizeof(int));
-    }
-    cudaStream_t s = ctx->stream;
-    unsigned char* din = static_cast<unsigned char*>(ctx->pass_in.ptr);
-    float* dout = static_cast<float*>(ctx->pass_out.ptr);
-    CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
-    CK(cudaMemcpyAsync(din, up, in_bytes, cudaMemcpyHostToDevice, s), "upload");
-    for (const Group& g : groups) {
-        const size_t stride = 2 * (size_t)g.nb + 1;
-        const uint32_t per_launch =
-            (uint32_t)std::max<size_t>(1, std::min<size_t>(16384, (512ull << 20) / (NF * stride * 12)));
-        for (uint32_t c = 0; c < g.count; c += per_launch) {
-            const int n = (int)std::min(g.count - c, per_launch);
-            FoldArgs fa{};
-            fa.time = ready->time;
-            fa.v = ready->v;
-            fa.w = ready->w;
-            fa.scales = reinterpret_cast<const double*>(din + g.off_scales) + c;
-            fa.n = (int)ready->n;
-            fa.nb = (int)g.nb;
-            fa.periods = n;
-            fa.group = g.shape.group;
-            fa.cum = as<double>(ctx->cum);
-            fa.cum32 = as<float2>(ctx->cum32);
-            fa.hist_global = g.shape.hist_in_smem ? nullptr : as<double>(ctx->hist);
-            fa.chunks = reinterpret_cast<const int*>(din + g.off_chunks);
-            fa.nchunks = (int)g.chunks.size() - 1;
-            fa.stage_field = g.shape.stage_field;
-            fa.window = g.shape.window;
-            fa.row_stride = g.shape.row_stride;
-            fa.fault = as<uint32_t>(ctx->fault);
-            CK(launch_fold(fa, g.shape, s), "fold");
-            MapArgs ma{};
-            ma.cum = fa.cum;
-            ma.scales = fa.scales;
-            ma.durations = reinterpret_cast<const double*>(din);
-            ma.rho = reinterpret_cast<const double*>(din) + nd;
-            ma.nd = (int)nd;
-            ma.nb = (int)g.nb;
-            ma.baseline = ready->baseline_norm;
-            ma.n = (double)ready->n;
-            ma.out = dout + (size_t)(g.i0 + c) * nd;
-            CK(launch_box_map(ma, n, s), "box map");
-            ctx->counters.launches += 2;
-        }
-    }
-    unsigned char* down = static_cast<unsigned char*>(ctx->pin_down.ptr);
-    CK(cudaMemcpyAsync(down, dout, out_bytes, cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaMemcpyAsync(down + out_bytes, ctx->fault.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaStreamSynchronize(s), "coarse map");
-    uint32_t fault = 0;
-    std::memcpy(&fault, down + out_bytes, sizeof(uint32_t));
-    if (fault) return fail(ctx, FBLS_ERR_CUDA, "fold: staging copies did not complete");
-    std::memcpy(out, down, out_bytes);
+    fbls_map_job job{family, periods, P, durations, rho, nd, oversample, bin_days, out, FBLS_OK};
+    std::vector<std::string> errors(1);
+    const int rc = coarse_maps(ctx, &job, 1, errors);
+    if (rc) return rc;
+    if (job.status) return fail(ctx, job.status, errors[0]);
     return FBLS_OK;
 }
 
@@ -1102,8 +1878,16 @@ int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* family, const double* perio
 int fbls_search_batch(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbls_config* cfg, uint32_t workers) {
     if (!ctx || (count && !stars) || !cfg) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
     if (count == 0) return FBLS_OK;
-    workers = std::max(1u, std::min({workers, count, 64u}));
     CK(cudaSetDevice(ctx->device), "set device");
+    if (workers == 0) {
+        std::vector<std::string> errors(count);
+        const int rc = search_batch_fused(ctx, stars, count, cfg, errors);
+        if (rc) return rc;
+        for (uint32_t i = 0; i < count; i++)
+            if (stars[i].status) return fail(ctx, stars[i].status, "star " + std::to_string(i) + ": " + errors[i]);
+        return FBLS_OK;
+    }
+    workers = std::min({workers, count, 64u});
     while (ctx->workers.size() < workers) {
         int status = FBLS_OK;
         fbls_ctx* w = fbls_create(ctx->device, &status);
@@ -1167,13 +1951,22 @@ int fbls_search_batch(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbl
 
 extern "C" {
 
-// Coarse maps of many uploaded families on the batch worker contexts (the
-// proposal path's first step for a batch of stars).
+// Coarse maps of many uploaded families (the proposal path's first step for a
+// batch of stars): on the batch worker contexts, or with workers == 0 planned
+// in parallel and run together as job launches on ctx (coarse_maps).
 int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uint32_t workers) {
     if (!ctx || (count && !jobs)) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
     if (count == 0) return FBLS_OK;
-    workers = std::max(1u, std::min({workers, count, 64u}));
     CK(cudaSetDevice(ctx->device), "set device");
+    if (workers == 0) {
+        std::vector<std::string> errors(count);
+        const int rc = coarse_maps(ctx, jobs, count, errors);
+        if (rc) return rc;
+        for (uint32_t i = 0; i < count; i++)
+            if (jobs[i].status) return fail(ctx, jobs[i].status, "map " + std::to_string(i) + ": " + errors[i]);
+        return FBLS_OK;
+    }
+    workers = std::min({workers, count, 64u});
     while (ctx->workers.size() < workers) {
         int status = FBLS_OK;
         fbls_ctx* w = fbls_create(ctx->device, &status);
@@ -1199,6 +1992,39 @@ int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uin
     for (std::thread& t : threads) t.join();
     for (uint32_t i = 0; i < count; i++)
         if (jobs[i].status) return fail(ctx, jobs[i].status, "map " + std::to_string(i) + ": " + errors[i]);
+    return FBLS_OK;
+}
+
+
+// The proposal network's input for a batch of stars (coarse_maps with
+// k_map_features): rows of x (channels x count x T) hold each map's
+// standardised log1p channels at [offsets[i], offsets[i] + P_i).
+int fbls_coarse_features(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, const uint32_t* offsets,
+                         uint32_t channels, uint32_t T, float* x) {
+    if (!ctx || (count && (!jobs || !offsets || !x))) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (channels < 1 || channels > (uint32_t)MAP_MAX_DURATIONS || T < 1)
+        return fail(ctx, FBLS_ERR_ARGUMENT, "1 to 8 channels and T >= 1");
+    if (count == 0) return FBLS_OK;
+    for (uint32_t i = 0; i < count; i++)
+        if (jobs[i].nd != channels || (uint64_t)offsets[i] + jobs[i].P > T)
+            return fail(ctx, FBLS_ERR_ARGUMENT, "map " + std::to_string(i) + ": does not fit its feature row");
+    CK(cudaSetDevice(ctx->device), "set device");
+    const size_t bytes = (size_t)channels * count * T * sizeof(float);
+    CK(ensure(ctx->feat, bytes), "workspace");
+    CK(cudaMemsetAsync(ctx->feat.ptr, 0, bytes, ctx->stream), "workspace");
+    MapFeatures feat;
+    feat.x = as<float>(ctx->feat);
+    feat.channels = (int)channels;
+    feat.B = (int)count;
+    feat.T = (int)T;
+    feat.offsets = offsets;
+    std::vector<std::string> errors(count);
+    const int rc = coarse_maps(ctx, jobs, count, errors, &feat);
+    if (rc) return rc;
+    for (uint32_t i = 0; i < count; i++)
+        if (jobs[i].status) return fail(ctx, jobs[i].status, "map " + std::to_string(i) + ": " + errors[i]);
+    CK(cudaMemcpyAsync(x, ctx->feat.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download");
+    CK(cudaStreamSynchronize(ctx->stream), "map features");
     return FBLS_OK;
 }
 

@@ -110,6 +110,27 @@ struct MapArgs {
     float* out;               // periods x nd: best box score per duration
 };
 
+// One star's time bins for k_bin_fields_jobs: vb[b], wb[b] = sums of v, w
+// over observations [starts[b], starts[b + 1]).
+struct BinJob {
+    const double* v;
+    const double* w;
+    const int* starts;  // nbins + 1
+    int nbins;
+    double* vb;
+    double* wb;
+};
+
+// One star's coarse map for k_map_features: map is P x nd floats on the
+// device; its features go to x[c][star][offset .. offset + P).
+struct FeatJob {
+    const float* map;
+    int P;
+    int nd;
+    int star;
+    int offset;
+};
+
 FoldShape fold_group_shape(int nb, int periods, int sm_count);
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
 // spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.
@@ -117,10 +138,22 @@ FoldShape fold_group_shape(int nb, int periods, int sm_count);
 int fold_chunks(const double* time, int n, double scale_max, int nb, int span_cap, int chunk_cap, int* out,
                 int capacity);
 cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream);
+// Job launches (the batched search): jobs and their first CTA / period
+// offsets (njobs + 1 entries, the last = total) live in device memory.
+bool fold_job_ok(const FoldArgs& a, const FoldShape& shape);  // a walking-fold job within limits
+cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, size_t smem,
+                             cudaStream_t stream);
+cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, cudaStream_t stream);
+cudaError_t launch_merge_jobs(const MergeArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream);
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream);
 cudaError_t launch_merge(const MergeArgs& a, cudaStream_t stream);
 cudaError_t launch_box_map(const MapArgs& a, int periods, cudaStream_t stream);
 cudaError_t launch_bin_fields(const double* v, const double* w, const int* starts, int nbins, double* vb, double* wb,
                               cudaStream_t stream);
+// Job launches of the maps: jobs and offsets (njobs + 1) in device memory.
+cudaError_t launch_box_map_jobs(const MapArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream);
+cudaError_t launch_bin_fields_jobs(const BinJob* jobs, const int* b0, int njobs, int total, cudaStream_t stream);
+cudaError_t launch_map_features(const FeatJob* jobs, int njobs, int channels, int B, int T, float* x,
+                                cudaStream_t stream);
 
 }  // namespace fbls

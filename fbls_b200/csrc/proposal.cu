@@ -7,7 +7,9 @@
 // sums the fold writes; a template counts when its width is below nb / 2,
 // it holds 3 .. n - 3 observations, a > 0 and the precision is positive, as in
 // the scan's f64 pass (src/search/kernels.rs:428-455, :679-700). 0 when no
-// template of the duration counts. One CTA of 256 threads per period.
+// template of the duration counts. One CTA of 256 threads per period; the job
+// form (k_box_map_jobs) covers the periods of many folds, of many stars, in
+// one launch.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -17,9 +19,8 @@ namespace {
 constexpr int MAP_THREADS = 256;
 }
 
-__global__ void __launch_bounds__(MAP_THREADS) k_box_map(MapArgs a) {
+__device__ __forceinline__ void box_map_period(const MapArgs& a, const int f) {
     __shared__ double s_best[MAP_MAX_DURATIONS][MAP_THREADS / 32];
-    const int f = blockIdx.x;
     const int tid = threadIdx.x;
     const int nb = a.nb;
     const int nd = a.nd;
@@ -71,6 +72,22 @@ __global__ void __launch_bounds__(MAP_THREADS) k_box_map(MapArgs a) {
     }
 }
 
+__global__ void __launch_bounds__(MAP_THREADS) k_box_map(MapArgs a) { box_map_period(a, blockIdx.x); }
+
+// Job j covers the CTAs [p0[j], p0[j + 1]), one per period of its fold.
+__global__ void __launch_bounds__(MAP_THREADS) k_box_map_jobs(const MapArgs* __restrict__ jobs,
+                                                              const int* __restrict__ p0, int njobs) {
+    const int c = blockIdx.x;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p0[mid] <= c) lo = mid;
+        else hi = mid - 1;
+    }
+    const MapArgs a = jobs[lo];
+    box_map_period(a, c - p0[lo]);
+}
+
 // Sums of v and w over runs of observations (the time bins of a coarse map):
 // bin b covers observations [starts[b], starts[b + 1]).
 __global__ void k_bin_fields(const double* v, const double* w, const int* starts, int nbins, double* vb,
@@ -84,6 +101,84 @@ __global__ void k_bin_fields(const double* v, const double* w, const int* starts
         vb[b] = sv;
         wb[b] = sw;
     }
+}
+
+// The bins of many stars: job j covers the global bin indices [b0[j], b0[j + 1]).
+__global__ void k_bin_fields_jobs(const BinJob* __restrict__ jobs, const int* __restrict__ b0, int njobs, int total) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (b0[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const BinJob& j = jobs[lo];
+        const int b = g - b0[lo];
+        double sv = 0.0, sw = 0.0;
+        for (int i = j.starts[b]; i < j.starts[b + 1]; i++) {
+            sv += j.v[i];
+            sw += j.w[i];
+        }
+        j.vb[b] = sv;
+        j.wb[b] = sw;
+    }
+}
+
+cudaError_t launch_bin_fields_jobs(const BinJob* jobs, const int* b0, int njobs, int total, cudaStream_t stream) {
+    if (njobs < 1 || total < 1) return cudaErrorInvalidValue;
+    const int blocks = (total + 255) / 256;
+    k_bin_fields_jobs<<<blocks < 4096 ? blocks : 4096, 256, 0, stream>>>(jobs, b0, njobs, total);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_box_map_jobs(const MapArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream) {
+    if (njobs < 1 || total < 1) return cudaErrorInvalidValue;
+    k_box_map_jobs<<<total, MAP_THREADS, 0, stream>>>(jobs, p0, njobs);
+    return cudaGetLastError();
+}
+
+// Network input of the proposal path: for map job j (star jobs[j].star) and
+// channel (duration) c, f_t = log1p(max(map[t][c], 0)) over the job's P
+// periods, standardised by its mean and (population) standard deviation + 1e-3,
+// written to x[c][star][offset + t] (x is C x B x T, zeroed beforehand). Jobs
+// with fewer than 8 periods are left at zero. One CTA per (job, channel).
+__global__ void __launch_bounds__(256) k_map_features(const FeatJob* __restrict__ jobs, int B, int T,
+                                                      float* __restrict__ x) {
+    __shared__ double s_sum[2][8];
+    const FeatJob j = jobs[blockIdx.x];
+    const int c = blockIdx.y;
+    if (j.P < 8 || c >= j.nd) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float* m = j.map;
+    double sum = 0.0;
+    for (int t = tid; t < j.P; t += blockDim.x) sum += (double)log1pf(fmaxf(m[(size_t)t * j.nd + c], 0.f));
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+    if (lane == 0) s_sum[0][warp] = sum;
+    __syncthreads();
+    double mu = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) mu += s_sum[0][w];
+    mu /= (double)j.P;
+    double var = 0.0;
+    for (int t = tid; t < j.P; t += blockDim.x) {
+        const double d = (double)log1pf(fmaxf(m[(size_t)t * j.nd + c], 0.f)) - mu;
+        var += d * d;
+    }
+    for (int off = 16; off > 0; off >>= 1) var += __shfl_xor_sync(0xffffffffu, var, off);
+    if (lane == 0) s_sum[1][warp] = var;
+    __syncthreads();
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += s_sum[1][w];
+    const double sd = sqrt(v / (double)j.P) + 1e-3;
+    float* out = x + ((size_t)c * B + j.star) * T + j.offset;
+    for (int t = tid; t < j.P; t += blockDim.x)
+        out[t] = (float)(((double)log1pf(fmaxf(m[(size_t)t * j.nd + c], 0.f)) - mu) / sd);
+}
+
+cudaError_t launch_map_features(const FeatJob* jobs, int njobs, int channels, int B, int T, float* x,
+                                cudaStream_t stream) {
+    if (njobs < 1 || channels < 1 || channels > MAP_MAX_DURATIONS || B < 1 || T < 1) return cudaErrorInvalidValue;
+    k_map_features<<<dim3(njobs, channels), 256, 0, stream>>>(jobs, B, T, x);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_bin_fields(const double* v, const double* w, const int* starts, int nbins, double* vb, double* wb,

@@ -136,10 +136,9 @@ __device__ __forceinline__ void shape_sums32(const float2* __restrict__ rv, cons
     }
 }
 
-// Eight CTAs per SM (64 registers): the f32 pass keeps its state in registers;
-// the few spills are on the f64 rescan and winner paths.
-__global__ void __launch_bounds__(TILE, 8) k_scan_tiles(ScanArgs a) {
-    __shared__ double s_dur[MAX_DURATIONS], s_rho[MAX_DURATIONS], s_ing[MAX_SHAPES];
+// One CTA of the tile scan: tile `tile` (of `tiles`) of period `f`.
+__device__ __forceinline__ void scan_tile_cta(const ScanArgs& a, const int tile, const int f, const int tiles) {
+    __shared__ double s_rho[MAX_DURATIONS], s_ing[MAX_SHAPES];
     __shared__ double s_fac[MAX_SHAPES * MAX_LAYERS];
     __shared__ double s_wv[TILE / 32];
     __shared__ unsigned long long s_wk[TILE / 32];
@@ -152,15 +151,12 @@ __global__ void __launch_bounds__(TILE, 8) k_scan_tiles(ScanArgs a) {
     __shared__ float s_r2f[MAX_DURATIONS];
 
     const int lane = threadIdx.x;
-    const int tile = blockIdx.x;
-    const int f = blockIdx.y;
     const int nb = a.nb;
     const int nd = a.nd, ns = a.ns, layers = a.layers;
     const uint32_t half = (uint32_t)(nb / 2);
     const double scale = a.scales[f];
     for (int i = lane; i < nd; i += TILE) {
         const double d = a.durations[i], r = a.rho[i];
-        s_dur[i] = d;
         s_rho[i] = r;
         const uint32_t raw_k = template_width(d, scale);
         s_k[i] = min(raw_k, half);
@@ -322,7 +318,7 @@ __global__ void __launch_bounds__(TILE, 8) k_scan_tiles(ScanArgs a) {
         const double q = rmax(__dsub_rn(norm, d), 1e-300);
         const double value = winner_value > neg_inf() ? __ddiv_rn(aa, __dsqrt_rn(q)) : neg_inf();
         const double depth = __dmul_rn(__ddiv_rn(aa, q), r);
-        const size_t idx = (size_t)f * gridDim.x + tile;
+        const size_t idx = (size_t)f * tiles + tile;
         double* out = a.parts + idx * PART_STRIDE;
         out[0] = (double)phase;
         out[1] = (double)width;
@@ -338,11 +334,34 @@ __global__ void __launch_bounds__(TILE, 8) k_scan_tiles(ScanArgs a) {
     }
 }
 
+// Eight CTAs per SM (64 registers): the f32 pass keeps its state in registers;
+// the few spills are on the f64 rescan and winner paths.
+__global__ void __launch_bounds__(TILE, 8) k_scan_tiles(ScanArgs a) {
+    scan_tile_cta(a, blockIdx.x, blockIdx.y, gridDim.x);
+}
+
+// Many scans in one launch: CTA c is tile (c - cta0[j]) % tiles of period
+// (c - cta0[j]) / tiles of job j, where cta0[j] <= c < cta0[j + 1].
+__global__ void __launch_bounds__(TILE, 8) k_scan_jobs(const ScanArgs* __restrict__ jobs,
+                                                       const int* __restrict__ cta0, int njobs) {
+    int lo = 0, hi = njobs - 1;
+    const int c = blockIdx.x;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (cta0[mid] <= c)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const ScanArgs& a = jobs[lo];
+    const int tiles = (a.nb + TILE - 1) / TILE;
+    const int local = c - cta0[lo];
+    scan_tile_cta(a, local % tiles, local / tiles, tiles);
+}
+
 // Best tile per period by (score, lowest key) (kernels.rs:1115-1155). Writes
 // records at `offset` so one buffer collects a whole band; flags are ORed.
-__global__ void k_merge(MergeArgs a) {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= a.periods) return;
+__device__ __forceinline__ void merge_period(const MergeArgs& a, const int f) {
     double best = neg_inf();
     uint64_t key = KEY_MAX;
     int chosen = 0;
@@ -376,6 +395,39 @@ __global__ void k_merge(MergeArgs a) {
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream) {
     dim3 grid((a.nb + TILE - 1) / TILE, periods);
     k_scan_tiles<<<grid, TILE, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+__global__ void k_merge(MergeArgs a) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < a.periods) merge_period(a, f);
+}
+
+// Many merges in one launch: thread i merges period i - p0[j] of job j.
+__global__ void k_merge_jobs(const MergeArgs* __restrict__ jobs, const int* __restrict__ p0, int njobs,
+                             int total) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (p0[mid] <= i)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    merge_period(jobs[lo], i - p0[lo]);
+}
+
+cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, cudaStream_t stream) {
+    if (njobs < 1 || ctas < 1) return cudaErrorInvalidValue;
+    k_scan_jobs<<<ctas, TILE, 0, stream>>>(jobs, cta0, njobs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge_jobs(const MergeArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream) {
+    if (njobs < 1 || total < 1) return cudaErrorInvalidValue;
+    k_merge_jobs<<<(total + 127) / 128, 128, 0, stream>>>(jobs, p0, njobs, total);
     return cudaGetLastError();
 }
 

@@ -67,7 +67,8 @@ def map_plan(state, period_max: float):
 
 def map_features(m: np.ndarray, keep: np.ndarray) -> np.ndarray:
     """(4, T_IN) features: log1p of the coarse map, standardised per duration
-    over the covered periods, 0 elsewhere."""
+    over the covered periods, 0 elsewhere. A numpy restatement of what
+    fbls_coarse_features computes on the device (the tests' reference)."""
     x = np.zeros((MAP_CHANNELS, T_IN), dtype=np.float32)
     if keep.sum() < 8:
         return x
@@ -81,10 +82,7 @@ def map_features(m: np.ndarray, keep: np.ndarray) -> np.ndarray:
 def star_map(gpu, dev, state, period_max: float, bin_days: float = 0.0) -> np.ndarray:
     """(4, T_IN) features of one star (observations summed over bins of
     bin_days first when it is positive)."""
-    keep, d, r = map_plan(state, period_max)
-    if keep.sum() < 8:
-        return np.zeros((MAP_CHANNELS, T_IN), dtype=np.float32)
-    return map_features(gpu.coarse_map(dev, map_periods()[keep], d, r, oversample=2.0, bin_days=bin_days), keep)
+    return features(gpu, [(state, period_max)], [dev], bin_days=bin_days)[:, 0, :]
 
 
 class Net:
@@ -281,18 +279,21 @@ def top_band(rows: np.ndarray) -> int:
     return band_of(float(rows[int(np.argmax(rows[:, 3])), 0]))
 
 
-def features(gpu, stars, devs, workers: int = 8, bin_days: float = 0.0) -> np.ndarray:
-    """(4, count, T_IN) float32, channel-major; the maps run on the batch
-    worker threads."""
-    x = np.zeros((MAP_CHANNELS, len(stars), T_IN), dtype=np.float32)
-    plans = [map_plan(st, pmax) for st, pmax in stars]
-    todo = [i for i, (keep, _, _) in enumerate(plans) if keep.sum() >= 8]
+def features(gpu, stars, devs, bin_days: float = 0.0) -> np.ndarray:
+    """(4, count, T_IN) float32, channel-major: every star's coarse map and
+    its features in one fbls_coarse_features call (map_features on the
+    device)."""
     p = map_periods()
-    maps = gpu.coarse_map_batch([devs[i] for i in todo], [p[plans[i][0]] for i in todo],
-                                [plans[i][1] for i in todo], [plans[i][2] for i in todo], 2.0, workers, bin_days)
-    for i, m in zip(todo, maps):
-        x[:, i, :] = map_features(m, plans[i][0])
-    return x
+    periods, ds, rs, offsets = [], [], [], []
+    for st, pmax in stars:
+        keep, d, r = map_plan(st, pmax)
+        idx = np.flatnonzero(keep)
+        lo = int(idx[0]) if idx.size else 0
+        periods.append(p[lo:lo + idx.size])
+        ds.append(d)
+        rs.append(r)
+        offsets.append(lo)
+    return gpu.coarse_features(devs, periods, ds, rs, offsets, T_IN, 2.0, bin_days)
 
 
 def train(net: Net, x: np.ndarray, y: np.ndarray, epochs: int = 30, batch: int = 128, lr: float = 2e-3,
@@ -366,13 +367,15 @@ def load_net(device: int = 0, path=None) -> Net:
     return net
 
 
-def search_proposed(gpu, net: Net, stars, devs, cfg, k: int = 3, workers: int = 8):
-    """The proposal-pruned search of many stars: coarse map, band scores, then
-    the exhaustive search of each star's k best bands only (its rows are the
-    full search's rows in those bands). Returns the batch results and logits."""
+def search_proposed(gpu, net: Net, stars, devs, cfg, k: int = 3, workers: int = 0):
+    """The proposal-pruned search of many stars: coarse maps and their
+    features in one call, band scores, then the exhaustive search of each
+    star's k best bands only (its rows are the full search's rows in those
+    bands), by search_batch with `workers` (0: the stars' band scans fused into
+    job launches). Returns the batch results and logits."""
     import time
     t0 = time.perf_counter()
-    x = features(gpu, stars, devs, workers, getattr(net, "bin_days", 0.0))
+    x = features(gpu, stars, devs, getattr(net, "bin_days", 0.0))
     t1 = time.perf_counter()
     logits = scores(net, x)
     ranges = [ranges_for(l, k) for l in logits]
@@ -399,7 +402,7 @@ def main(argv=None):
     ap.add_argument("--test", type=int, default=1500)
     ap.add_argument("--max-sectors", type=int, default=4)
     ap.add_argument("--epochs", type=int, default=30)
-    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--workers", type=int, default=0, help="search_batch workers of the labelling search")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--bin-minutes", type=float, default=10.0, help="time bins of the coarse map (0: none)")
     ap.add_argument("--out", required=True)
@@ -415,7 +418,7 @@ def main(argv=None):
         y = np.array([top_band(r) for r, _, _ in res])
         log(f"exhaustive labels: {int((y >= 0).sum())} of {len(y)} stars with a detection")
         bin_days = args.bin_minutes / 1440.0
-        x = features(gpu, stars, devs, args.workers, bin_days)
+        x = features(gpu, stars, devs, bin_days)
         log("coarse maps done")
         net = Net(0, seed=args.seed)
         ntr = args.train

@@ -287,10 +287,24 @@ typedef struct {
     int status;
 } fbls_map_job;
 
-/* Coarse maps of many uploaded families on `workers` host threads with their
- * own streams (the contexts fbls_search_batch keeps). Returns 0 or the first
- * failing job's status ("map i: " message). */
+/* Coarse maps of many uploaded families: on `workers` host threads with their
+ * own streams (the contexts fbls_search_batch keeps), or with `workers` == 0
+ * all together on the context's stream, every star's folds and box maps
+ * packed into shared launches. The maps are the same either way. Returns 0
+ * or the first failing job's status ("map i: " message). */
 int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uint32_t workers);
+
+/* The proposal network's input for a batch of stars: every job's coarse map
+ * (as fbls_coarse_map_batch with workers == 0; a job's `out` may be null) and
+ * x (host, channels x count x T floats, channel-major): row i of channel c
+ * holds (log1p(max(map, 0)) - mean) / (std + 1e-3) of the job's P map values
+ * of duration c at positions [offsets[i], offsets[i] + P), with mean and
+ * (population) std over those P values, and zeros elsewhere and for maps of
+ * fewer than 8 periods. Every job needs nd == channels (1..8) and
+ * offsets[i] + P <= T. Returns 0 or the first failing job's status ("map i: "
+ * message). */
+int fbls_coarse_features(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, const uint32_t* offsets,
+                         uint32_t channels, uint32_t T, float* x);
 
 /* Proposal network kernels. Every pointer is device memory; `stream` is a
  * cudaStream_t (NULL: the legacy stream). Activations are f32 laid out
@@ -367,10 +381,14 @@ typedef struct {
     uint32_t n_ranges;
 } fbls_star;
 
-/* signal_search for every star of `stars` on the context's device, with
- * `workers` host threads (1..64, the caller's thread included), each with its
- * own stream and workspace (kept in ctx for later calls). Results are the
- * same as one fbls_signal_search per star. Returns 0, or the status of the
+/* signal_search for every star of `stars` on the context's device. With
+ * `workers` >= 1, host threads (up to 64, the caller's thread included) take
+ * one star at a time, each with its own stream and workspace (kept in ctx for
+ * later calls). With `workers` == 0 the stars are searched together on the
+ * context's stream, in groups of up to 2^21 grid periods: each group's band
+ * scans run as job launches covering every star of the group (a bank the
+ * planner rejects fails the whole group). Results are the same as one
+ * fbls_signal_search per star either way. Returns 0, or the status of the
  * first failing star (its message in fbls_last_error, prefixed "star i: ");
  * every star's own status is in its record. Do not share a context between
  * concurrent calls. */

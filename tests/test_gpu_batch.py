@@ -20,14 +20,17 @@ def _stars(count, seed=11, max_sectors=2):
     return out
 
 
+@pytest.mark.parametrize("workers", [3, 0])
 @pytest.mark.parametrize("uploaded", [False, True])
-def test_batch_matches_per_star_search(gpu, uploaded):
+def test_batch_matches_per_star_search(gpu, uploaded, workers):
+    """workers 3: host threads, one star each; workers 0: the stars' band
+    scans fused into job launches."""
     stars = _stars(6)
     base = stars[0][1]
     pmax = [cfg.period_max for _, cfg in stars]
     want = [gpu.signal_search(st, cfg) for st, cfg in stars]
     devs = [gpu.upload(st) for st, _ in stars] if uploaded else None
-    got = gpu.search_batch([st for st, _ in stars], base, period_max=pmax, devs=devs, workers=3)
+    got = gpu.search_batch([st for st, _ in stars], base, period_max=pmax, devs=devs, workers=workers)
     for (rows, glen, templates), (wrows, wglen, wstats) in zip(got, want):
         assert glen == wglen
         assert templates == sum(s["templates_scanned"] for s in wstats)
@@ -37,14 +40,29 @@ def test_batch_matches_per_star_search(gpu, uploaded):
             d.free()
 
 
-def test_batch_reports_the_failing_star(gpu):
+@pytest.mark.parametrize("workers", [2, 0])
+def test_batch_reports_the_failing_star(gpu, workers):
     stars = _stars(3)
     st = stars[1][0]
     short = api.FamilyState(st.time[:4], st.v[:4], st.w[:4], st.baseline_norm, st.origin, st.residual_energy,
                             st.durations, st.rho)
     states = [stars[0][0], short, stars[2][0]]
     with pytest.raises(api.FblsError, match="star 1: at least six observations"):
-        gpu.search_batch(states, stars[0][1], period_max=[cfg.period_max for _, cfg in stars], workers=2)
+        gpu.search_batch(states, stars[0][1], period_max=[cfg.period_max for _, cfg in stars], workers=workers)
+
+
+def test_fused_batch_with_ranges_matches_ranged_search(gpu):
+    """Ranged searches (the proposal path's second step) fused over a batch."""
+    stars = _stars(5, seed=23)
+    base = stars[0][1]
+    pmax = [cfg.period_max for _, cfg in stars]
+    ranges = [[(0.9, 1.3), (4.0, 6.5)], None, [(2.0, 2.2)], [(0.5, 20.0)], [(7.5, 9.0), (11.0, 12.5)]]
+    want = [gpu.signal_search(st, cfg, ranges=rg) for (st, cfg), rg in zip(stars, ranges)]
+    got = gpu.search_batch([st for st, _ in stars], base, period_max=pmax, workers=0, ranges=ranges)
+    for (rows, glen, templates), (wrows, wglen, wstats) in zip(got, want):
+        assert glen == wglen
+        assert templates == sum(s["templates_scanned"] for s in wstats)
+        assert np.array_equal(rows, wrows)
 
 
 def test_signal_search_reports_every_row_when_the_buffer_is_short(gpu):
@@ -70,3 +88,21 @@ def test_signal_search_reports_every_row_when_the_buffer_is_short(gpu):
     assert n.value == want.shape[0]
     assert np.array_equal(rows, want[:2])
     dev.free()
+
+
+def test_fused_batch_uploads_every_star(gpu):
+    """The fused batch uploads a group's host families together (planned on
+    several threads): results equal those of the same stars uploaded
+    beforehand, for a batch large enough to plan in parallel."""
+    stars = _stars(40, seed=31, max_sectors=1)
+    base = stars[0][1]
+    pmax = [cfg.period_max for _, cfg in stars]
+    states = [st for st, _ in stars]
+    devs = [gpu.upload(st) for st in states]
+    want = gpu.search_batch(states, base, period_max=pmax, devs=devs, workers=0)
+    got = gpu.search_batch(states, base, period_max=pmax, workers=0)
+    for (rows, glen, templates), (wrows, wglen, wtemplates) in zip(got, want):
+        assert glen == wglen and templates == wtemplates
+        assert np.array_equal(rows, wrows)
+    for d in devs:
+        d.free()

@@ -141,15 +141,59 @@ def test_ranged_search_rows_are_the_full_search_rows_in_range(gpu):
     assert np.array_equal(res[0][0], full[inside])
 
 
-def test_coarse_map_batch_matches_single_maps(gpu):
+@pytest.mark.parametrize("bin_days", [0.0, 600.0 / 86400.0])
+def test_coarse_map_batch_matches_single_maps(gpu, bin_days):
+    """workers 3: one map per worker thread; workers 0: every star's folds and
+    box maps in shared job launches. Both equal one coarse_map per star."""
     from fbls_b200 import proposal as pr
     stars, cfg = pr.survey_stars(5, seed=3, max_sectors=2)
     devs = [gpu.upload(s) for s, _ in stars]
-    x = pr.features(gpu, stars, devs, workers=3)
-    for i, ((st, pmax), dev) in enumerate(zip(stars, devs)):
-        assert np.array_equal(x[:, i, :], pr.star_map(gpu, dev, st, pmax))
+    p = pr.map_periods()
+    plans = [pr.map_plan(st, pmax) for st, pmax in stars]
+    want = [gpu.coarse_map(dev, p[keep], d, r, 2.0, bin_days=bin_days) for dev, (keep, d, r) in zip(devs, plans)]
+    for workers in (3, 0):
+        got = gpu.coarse_map_batch(devs, [p[keep] for keep, _, _ in plans], [d for _, d, _ in plans],
+                                   [r for _, _, r in plans], 2.0, workers, bin_days)
+        assert all(np.array_equal(g, w) for g, w in zip(got, want))
     for d in devs:
         d.free()
+
+
+@pytest.mark.parametrize("bin_days", [0.0, 600.0 / 86400.0])
+def test_features_are_the_standardised_maps(gpu, bin_days):
+    """fbls_coarse_features: the batch's network input equals, star for star,
+    the features of one star, and map_features (numpy, f32) of its coarse map
+    to f32 rounding."""
+    from fbls_b200 import proposal as pr
+    stars, cfg = pr.survey_stars(6, seed=5, max_sectors=3)
+    devs = [gpu.upload(s) for s, _ in stars]
+    x = pr.features(gpu, stars, devs, bin_days=bin_days)
+    assert x.shape == (pr.MAP_CHANNELS, len(stars), pr.T_IN)
+    p = pr.map_periods()
+    for i, ((st, pmax), dev) in enumerate(zip(stars, devs)):
+        assert np.array_equal(x[:, i, :], pr.star_map(gpu, dev, st, pmax, bin_days))
+        keep, d, r = pr.map_plan(st, pmax)
+        ref = pr.map_features(gpu.coarse_map(dev, p[keep], d, r, 2.0, bin_days=bin_days), keep)
+        assert np.allclose(x[:, i, :], ref, rtol=1e-4, atol=1e-4)
+        assert np.all(x[:, i, ~keep] == 0)
+    for d in devs:
+        d.free()
+
+
+def test_coarse_map_batch_reports_the_failing_map(gpu):
+    c, cfg = synth.small_curve(), synth.small_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    dev = gpu.upload(st)
+    good = np.geomspace(0.6, 1.15, 100)
+    bad = good[::-1].copy()  # not ascending
+    d, r = st.durations[:2], st.rho[:2]
+    want = gpu.coarse_map(dev, good, d, r, 2.0)
+    for workers in (2, 0):
+        with pytest.raises(api.FblsError, match="map 1: periods must be positive, finite and ascending"):
+            gpu.coarse_map_batch([dev, dev, dev], [good, bad, good], [d] * 3, [r] * 3, 2.0, workers)
+        got = gpu.coarse_map_batch([dev, dev], [good, good], [d] * 2, [r] * 2, 2.0, workers)
+        assert all(np.array_equal(g, want) for g in got)
+    dev.free()
 
 
 def test_binned_coarse_map_is_the_map_of_the_binned_family(gpu):
