@@ -562,7 +562,7 @@ def main():
     ap.add_argument("--batch-workers", type=int, default=0,
                     help="survey / proposal workloads: search_batch host worker threads (0: stars fused into "
                          "job launches)")
-    ap.add_argument("--bands", type=int, default=3, help="proposal workload: log-period bands searched per star")
+    ap.add_argument("--bands", type=int, default=1, help="proposal workload: log-period bands searched per star")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

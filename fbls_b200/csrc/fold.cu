@@ -127,11 +127,12 @@ __device__ __forceinline__ double warp_scan(double x, int lane) {
 
 // prefix_row of a shared-memory row by one warp, with the first copy kept in
 // place, so the second copy (first + final carry) is read from shared memory
-// rather than back from the global rows.
-__device__ __forceinline__ void prefix_row_smem(const HistRow& r, int nb, double* __restrict__ out64,
-                                                float2* __restrict__ out32) {
+// rather than back from the global rows. With global = false only the
+// in-place copy is made. Returns the final carry.
+__device__ __forceinline__ double prefix_row_smem(const HistRow& r, int nb, bool global, double* __restrict__ out64,
+                                                  float2* __restrict__ out32) {
     const int lane = threadIdx.x & 31;
-    if (lane == 0) {
+    if (global && lane == 0) {
         out64[0] = 0.0;
         out32[0] = make_float2(0.f, 0.f);
     }
@@ -146,8 +147,10 @@ __device__ __forceinline__ void prefix_row_smem(const HistRow& r, int nb, double
             const double wt = __shfl_sync(0xffffffffu, x, 31);
             if (b < nb) {
                 const double val = __dadd_rn(x, offset);
-                out64[b + 1] = val;
-                out32[b + 1] = split_pair(val);
+                if (global) {
+                    out64[b + 1] = val;
+                    out32[b + 1] = split_pair(val);
+                }
                 r.store(b, val);
             }
             offset = __dadd_rn(offset, wt);
@@ -155,20 +158,23 @@ __device__ __forceinline__ void prefix_row_smem(const HistRow& r, int nb, double
         }
         carry = __dadd_rn(carry, total);
     }
-    for (int b = lane; b < nb; b += 32) {  // bins this lane stored above
-        const double val = __dadd_rn(r.load(b), carry);
-        out64[nb + b + 1] = val;
-        out32[nb + b + 1] = split_pair(val);
-    }
+    if (global)
+        for (int b = lane; b < nb; b += 32) {  // bins this lane stored above
+            const double val = __dadd_rn(r.load(b), carry);
+            out64[nb + b + 1] = val;
+            out32[nb + b + 1] = split_pair(val);
+        }
+    return carry;
 }
 
-// The 256-bin segment `seg` of a row, by one warp, as prefix_row does it:
-// with `carry` (the carry entering the segment) and `final` (the row's last
-// carry) known, writes both copies and returns nothing; with them unknown
-// (write = false), returns the segment's total (the sum, in order, of its
-// eight group totals) and writes nothing.
+// The 256-bin segment `seg` of a row, by one warp, as prefix_row does it.
+// SEG_TOTAL: returns the segment's total (the sum, in order, of its eight
+// group totals) and writes nothing. SEG_GLOBAL: with `carry` (entering the
+// segment) and `final` (the row's last carry) known, writes both copies to
+// the global rows. SEG_IN_PLACE: stores the first copy in place.
+constexpr int SEG_TOTAL = 0, SEG_GLOBAL = 1, SEG_IN_PLACE = 2;
 __device__ __forceinline__ double prefix_segment(const HistRow& r, int nb, int seg, double carry, double final,
-                                                 bool write, double* __restrict__ out64,
+                                                 int mode, double* __restrict__ out64,
                                                  float2* __restrict__ out32) {
     const int lane = threadIdx.x & 31;
     double offset = carry;
@@ -178,13 +184,15 @@ __device__ __forceinline__ double prefix_segment(const HistRow& r, int nb, int s
         const int b = seg + g * 32 + lane;
         const double x = warp_scan(b < nb ? r.load(b) : 0.0, lane);
         const double wt = __shfl_sync(0xffffffffu, x, 31);
-        if (write && b < nb) {
+        if (mode == SEG_GLOBAL && b < nb) {
             const double val = __dadd_rn(x, offset);
             out64[b + 1] = val;
             out32[b + 1] = split_pair(val);
             const double val2 = __dadd_rn(val, final);
             out64[nb + b + 1] = val2;
             out32[nb + b + 1] = split_pair(val2);
+        } else if (mode == SEG_IN_PLACE && b < nb) {
+            r.store(b, __dadd_rn(x, offset));
         }
         offset = __dadd_rn(offset, wt);
         total = __dadd_rn(total, wt);
@@ -415,6 +423,79 @@ __device__ __forceinline__ void stage_chunk(const FoldArgs& a, int i0, int i1, d
 // lose more to idle steps than the conflict-free reads gain).
 constexpr int LOCKSTEP_MIN_SEGMENT = 11;
 
+// The coarse-map epilogue of the walking fold (after the in-place prefix rows
+// and a barrier), out of line: it runs once per CTA.
+__device__ __noinline__ void fold_map_epilogue(float* map_out, const double* map_durations, const double* map_rho,
+                                               int nd, double baseline, int n, const double2* hvw,
+                                               const uint32_t* hc, const double* s_scale, const double* row_final,
+                                               double* part, int nb, int rs, int g, int g0, int W) {
+    // Coarse-map epilogue: for every (period, map duration) pair the best box
+    // score over all phases from the in-place prefix rows, exactly as
+    // k_box_map computes it from the global rows (the doubled row's entry i
+    // is 0 at i = 0, the kept value of bin i - 1 up to nb, and that of bin
+    // i - nb - 1 plus the row's final carry beyond). Pairs get W / pairs warps
+    // each (or one warp takes several pairs); partial maxima meet in shared
+    // memory.
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t unb = (uint32_t)nb;
+    const int pairs = g * nd;
+    const int per = pairs >= W ? 1 : W / pairs;
+    const uint32_t half = unb / 2u;
+    auto pre = [&](const HistRow& r, double carry, uint32_t i) -> double {
+        return i == 0 ? 0.0 : (i <= unb ? r.load((int)i - 1) : __dadd_rn(r.load((int)(i - unb) - 1), carry));
+    };
+    for (int p = warp / per; p < pairs && warp < per * pairs; p += (pairs >= W ? W : pairs)) {
+        const int qq = p / nd, d = p - qq * nd;
+        const int slice = warp - (warp / per) * per;
+        const double sc = s_scale[qq];
+        const uint32_t raw = template_width(map_durations[d], sc);
+        double best = 0.0;
+        if (raw < half) {
+            const uint32_t k = raw;
+            const size_t o = (size_t)qq * rs;
+            HistRow rv, rw, rn;
+            double2* hv = const_cast<double2*>(hvw);
+            uint32_t* hcc = const_cast<uint32_t*>(hc);
+            rv.d = &hv[o].x;
+            rv.c = hcc + o;
+            rw.d = &hv[o].y;
+            rw.c = hcc + o;
+            rn.d = nullptr;
+            rn.c = hcc + o;
+            const double cv = row_final[qq * NF + F_V], cw = row_final[qq * NF + F_W],
+                         cn = row_final[qq * NF + F_N];
+            for (uint32_t j = (uint32_t)(slice * 32 + lane); j < unb; j += (uint32_t)(per * 32)) {
+                const double count = __dsub_rn(pre(rn, cn, j + k), pre(rn, cn, j));
+                if (!(count >= 3.0 && count <= (double)n - 3.0)) continue;
+                const double av = __dsub_rn(pre(rv, cv, j + k), pre(rv, cv, j));
+                if (!(av > 0.0)) continue;
+                const double w = __dsub_rn(pre(rw, cw, j + k), pre(rw, cw, j));
+                const double q = __dsub_rn(w, __ddiv_rn(__dmul_rn(w, w), baseline));
+                if (!(q > 0.0)) continue;
+                const double s = __ddiv_rn(__ddiv_rn(av, map_rho[d]), __dsqrt_rn(rmax(q, 1e-300)));
+                if (s > best) best = s;
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, off));
+        if (per == 1) {
+            if (lane == 0) map_out[(size_t)(g0 + qq) * nd + d] = (float)best;
+        } else if (lane == 0) {
+            part[warp] = best;
+        }
+    }
+    if (per > 1) {
+        __syncthreads();
+        if (tid < pairs) {
+            double best = part[tid * per];
+            for (int k = 1; k < per; k++) best = fmax(best, part[tid * per + k]);
+            const int qq = tid / nd, d = tid - qq * nd;
+            map_out[(size_t)(g0 + qq) * nd + d] = (float)best;
+        }
+    }
+}
+
+
 // One CTA of the walking fold: CTA `cta` of the launch described by `a`
 // folds periods [cta * G, cta * G + G).
 template <int CAP>
@@ -637,16 +718,18 @@ __device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) 
         return r;
     };
     const int items = rows * S;
-    if (2 * ((items + W - 1) / W) < ((rows + W - 1) / W) * S && 2 * items + rows <= 6 * F) {
+    const bool map = a.map_out != nullptr;
+    double* row_final = stage;  // rows: each row's final carry (map epilogue)
+    if (2 * ((items + W - 1) / W) < ((rows + W - 1) / W) * S && 2 * items + rows + W <= 6 * F) {
         double* seg_total = stage;             // rows x S (the staging buffers are idle now)
         double* seg_carry = stage + items;     // rows x S
-        double* row_final = stage + 2 * items; // rows
+        row_final = stage + 2 * items;         // rows
         for (int it = warp; it < items; it += W) {
             const int row = it / S, sg = it - row * S;
             double* o64;
             float2* o32;
             const HistRow r = row_of(row, o64, o32);
-            const double tot = prefix_segment(r, nb, sg * 256, 0.0, 0.0, false, o64, o32);
+            const double tot = prefix_segment(r, nb, sg * 256, 0.0, 0.0, SEG_TOTAL, o64, o32);
             if (lane == 0) seg_total[it] = tot;
         }
         __syncthreads();
@@ -664,20 +747,27 @@ __device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) 
             double* o64;
             float2* o32;
             const HistRow r = row_of(row, o64, o32);
-            if (sg == 0 && lane == 0) {
+            if (!map && sg == 0 && lane == 0) {
                 o64[0] = 0.0;
                 o32[0] = make_float2(0.f, 0.f);
             }
-            prefix_segment(r, nb, sg * 256, seg_carry[it], row_final[row], true, o64, o32);
+            prefix_segment(r, nb, sg * 256, seg_carry[it], row_final[row], map ? SEG_IN_PLACE : SEG_GLOBAL, o64,
+                           o32);
         }
-        return;
+    } else {
+        for (int row = warp; row < rows; row += W) {
+            double* o64;
+            float2* o32;
+            const HistRow r = row_of(row, o64, o32);
+            const double carry = prefix_row_smem(r, nb, !map, o64, o32);
+            if (map && lane == 0) row_final[row] = carry;
+        }
     }
-    for (int row = warp; row < rows; row += W) {
-        double* o64;
-        float2* o32;
-        const HistRow r = row_of(row, o64, o32);
-        prefix_row_smem(r, nb, o64, o32);
-    }
+    if (!map) return;
+
+    __syncthreads();
+    fold_map_epilogue(a.map_out, a.map_durations, a.map_rho, a.map_nd, a.map_baseline, a.n, hvw, hc, s_scale,
+                      row_final, stage + 6 * F - W, nb, rs, g, g0, W);
 }
 
 template <int CAP>
@@ -827,7 +917,8 @@ bool fold_job_ok(const FoldArgs& a, const FoldShape& shape) {
            a.group <= MAX_GROUP && (a.group & (a.group - 1)) == 0 && shape.threads == 1024 && a.nchunks >= 1 &&
            a.nb >= 2 && a.stage_field == WALK_CAP + 2 && shape.chunk_cap == WALK_CAP &&
            a.row_stride == shape.row_stride && a.row_stride >= a.nb && a.fault != nullptr && a.hist_out == nullptr &&
-           a.time && a.v && a.w && a.scales && a.chunks && a.cum && a.cum32 &&
+           a.time && a.v && a.w && a.scales && a.chunks && (a.map_out || (a.cum && a.cum32)) &&
+           (!a.map_out || (a.map_nd >= 1 && a.map_nd <= MAP_MAX_DURATIONS && a.map_durations && a.map_rho)) &&
            !(reinterpret_cast<uintptr_t>(a.time) & 15) && !(reinterpret_cast<uintptr_t>(a.v) & 15) &&
            !(reinterpret_cast<uintptr_t>(a.w) & 15);
 }
@@ -852,7 +943,10 @@ cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t 
             configured[dev] = true;
         }
     }
-    if (!a.time || !a.v || !a.w || !a.scales || !a.chunks || (!a.hist_out && (!a.cum || !a.cum32)))
+    if (!a.time || !a.v || !a.w || !a.scales || !a.chunks || (!a.hist_out && !a.map_out && (!a.cum || !a.cum32)))
+        return cudaErrorInvalidValue;
+    if (a.map_out && (shape.kind != FOLD_WALK || a.hist_out || a.map_nd < 1 || a.map_nd > MAP_MAX_DURATIONS ||
+                      !a.map_durations || !a.map_rho))
         return cudaErrorInvalidValue;
     if (shape.kind == FOLD_WALK) {
         if (shape.smem > MAX_FOLD_SMEM || a.group != shape.group || a.group < 1 || a.group > MAX_GROUP ||

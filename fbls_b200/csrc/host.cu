@@ -1342,8 +1342,11 @@ int plan_map(const fbls_ctx* ctx, MapPlan& m) {
 
 // Runs planned maps on ctx->stream: one upload, one launch for every star's
 // bins, then waves of fold units (a group's launch of at most per_launch
-// periods) whose prefix sums fit MAP_WAVE_BYTES, each wave one fold launch
-// (walking folds as jobs; any other fold on its own) and one box-map launch;
+// periods), each wave one fold launch of the walking folds as jobs, whose
+// epilogue computes the box maps from the prefix rows in shared memory, and
+// for any other fold (too many bins for the walking fold) its own launch,
+// prefix rows in HBM (the wave's share under MAP_WAVE_BYTES) and a box-map
+// launch;
 // with `feat`, one k_map_features launch writing the maps' network input into
 // feat->x (device); one download and one synchronisation; each map is copied
 // to its job's out when there is one.
@@ -1368,7 +1371,7 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
     struct Wave {
         std::vector<Unit> units;
         size_t cum = 0, hist = 0, smem = 0;
-        int fold_jobs = 0, fold_ctas = 0, map_total = 0;
+        int fold_jobs = 0, fold_ctas = 0, map_jobs = 0, map_total = 0;
         size_t off_fold = 0, off_fcta = 0, off_map = 0, off_mp = 0;
     };
     size_t in_total = 0, out_total = 0, bin_total = 0;
@@ -1389,8 +1392,8 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
             const size_t stride = 2 * (size_t)g.nb + 1;
             for (uint32_t c0 = 0; c0 < g.count; c0 += g.per_launch) {
                 const int n = (int)std::min(g.count - c0, g.per_launch);
-                const size_t cum = (size_t)n * NF * stride;
-                const bool walk = g.shape.kind == FOLD_WALK;
+                const bool walk = g.shape.kind == FOLD_WALK;  // box maps in the fold's epilogue: no prefix rows
+                const size_t cum = walk ? 0 : (size_t)n * NF * stride;
                 const size_t hist = walk ? 0 : ((n + g.shape.group - 1) / g.shape.group) * (size_t)g.shape.group *
                                                    NF * (size_t)g.shape.row_stride;
                 if (!waves.back().units.empty() &&
@@ -1404,8 +1407,10 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
                     w.fold_jobs++;
                     w.fold_ctas += (n + g.shape.group - 1) / g.shape.group;
                     w.smem = std::max(w.smem, g.shape.smem);
+                } else {
+                    w.map_jobs++;
+                    w.map_total += n;
                 }
-                w.map_total += n;
             }
         }
     }
@@ -1423,13 +1428,15 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
         hist_max = std::max(hist_max, w.hist);
         w.off_fold = take(std::max(1, w.fold_jobs) * sizeof(FoldArgs));
         w.off_fcta = take((w.fold_jobs + 1) * sizeof(int));
-        w.off_map = take(w.units.size() * sizeof(MapArgs));
-        w.off_mp = take((w.units.size() + 1) * sizeof(int));
+        w.off_map = take(std::max(1, w.map_jobs) * sizeof(MapArgs));
+        w.off_mp = take((w.map_jobs + 1) * sizeof(int));
     }
     CK(ensure(ctx->pass_in, blob), "workspace");
     CK(ensure(ctx->pass_out, out_total), "workspace");
-    CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
-    CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
+    if (cum_max) {
+        CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
+        CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
+    }
     if (hist_max) CK(ensure(ctx->hist, hist_max * sizeof(double)), "workspace");
     if (bin_total) CK(ensure(ctx->mapbin, bin_total), "workspace");
     CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
@@ -1485,7 +1492,7 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
         int* fc = reinterpret_cast<int*>(up + w.off_fcta);
         MapArgs* mj = reinterpret_cast<MapArgs*>(up + w.off_map);
         int* mp = reinterpret_cast<int*>(up + w.off_mp);
-        int nf = 0, fcta = 0, mtot = 0;
+        int nf = 0, fcta = 0, nm = 0, mtot = 0;
         for (size_t u = 0; u < w.units.size(); u++) {
             const Unit& un = w.units[u];
             const MapPlan& m = *un.m;
@@ -1501,8 +1508,8 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
             fa.nb = (int)g.nb;
             fa.periods = un.n;
             fa.group = g.shape.group;
-            fa.cum = as<double>(ctx->cum) + un.cum_off;
-            fa.cum32 = as<float2>(ctx->cum32) + un.cum_off;
+            fa.cum = un.walk ? nullptr : as<double>(ctx->cum) + un.cum_off;
+            fa.cum32 = un.walk ? nullptr : as<float2>(ctx->cum32) + un.cum_off;
             fa.hist_global = un.walk ? nullptr : as<double>(ctx->hist) + un.hist_off;
             fa.hist_out = nullptr;
             fa.chunks = reinterpret_cast<const int*>(b + g.off_chunks);
@@ -1511,7 +1518,13 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
             fa.window = g.shape.window;
             fa.row_stride = g.shape.row_stride;
             fa.fault = as<uint32_t>(ctx->fault);
+            float* out = reinterpret_cast<float*>(dout + m.out_off) + (size_t)(g.i0 + un.c0) * m.job->nd;
             if (un.walk) {
+                fa.map_out = out;
+                fa.map_durations = reinterpret_cast<const double*>(b);
+                fa.map_rho = reinterpret_cast<const double*>(b) + m.job->nd;
+                fa.map_nd = (int)m.job->nd;
+                fa.map_baseline = r->baseline_norm;
                 if (!fold_job_ok(fa, g.shape)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
                 fj[nf] = fa;
                 fc[nf++] = fcta;
@@ -1521,23 +1534,25 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
                 own_shape.push_back(&g.shape);
                 own_wave.push_back(wi);
             }
-            MapArgs ma{};
-            ma.cum = fa.cum;
-            ma.scales = fa.scales;
-            ma.durations = reinterpret_cast<const double*>(b);
-            ma.rho = reinterpret_cast<const double*>(b) + m.job->nd;
-            ma.nd = (int)m.job->nd;
-            ma.nb = (int)g.nb;
-            ma.baseline = r->baseline_norm;
-            ma.n = (double)r->n;
-            ma.out = reinterpret_cast<float*>(dout + m.out_off) + (size_t)(g.i0 + un.c0) * m.job->nd;
-            mj[u] = ma;
-            mp[u] = mtot;
-            mtot += un.n;
+            if (!un.walk) {
+                MapArgs ma{};
+                ma.cum = fa.cum;
+                ma.scales = fa.scales;
+                ma.durations = reinterpret_cast<const double*>(b);
+                ma.rho = reinterpret_cast<const double*>(b) + m.job->nd;
+                ma.nd = (int)m.job->nd;
+                ma.nb = (int)g.nb;
+                ma.baseline = r->baseline_norm;
+                ma.n = (double)r->n;
+                ma.out = out;
+                mj[nm] = ma;
+                mp[nm++] = mtot;
+                mtot += un.n;
+            }
             ctx->counters.fold_updates += (uint64_t)un.n * r->n;
         }
         fc[nf] = fcta;
-        mp[w.units.size()] = mtot;
+        mp[nm] = mtot;
     }
     cudaStream_t s = ctx->stream;
     CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
@@ -1562,10 +1577,12 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
             CK(launch_fold(own[oi], *own_shape[oi], s), "fold");
             ctx->counters.launches += 1;
         }
-        CK(launch_box_map_jobs(reinterpret_cast<const MapArgs*>(din + w.off_map),
-                               reinterpret_cast<const int*>(din + w.off_mp), (int)w.units.size(), w.map_total, s),
-           "box map");
-        ctx->counters.launches += 1;
+        if (w.map_jobs) {
+            CK(launch_box_map_jobs(reinterpret_cast<const MapArgs*>(din + w.off_map),
+                                   reinterpret_cast<const int*>(din + w.off_mp), w.map_jobs, w.map_total, s),
+               "box map");
+            ctx->counters.launches += 1;
+        }
     }
     if (feat) {
         CK(launch_map_features(reinterpret_cast<const FeatJob*>(din + off_feat), (int)plans.size(), feat->channels,

@@ -47,6 +47,15 @@ struct FoldArgs {
     int window;            // 0: whole histogram in shared memory; else window rows
     int row_stride;        // FoldShape::row_stride
     uint32_t* fault;       // FOLD_WALK: set nonzero when a staging wait gives up
+    // Coarse-map epilogue (FOLD_WALK only): when map_out is set, the prefix
+    // rows stay in shared memory (cum / cum32 unused) and each period's best
+    // box score per map duration, as k_box_map computes it, goes to
+    // map_out[period * map_nd + d].
+    float* map_out;
+    const double* map_durations;  // map_nd
+    const double* map_rho;        // map_nd
+    int map_nd;
+    double map_baseline;          // baseline_norm c
 };
 
 // Launch shape of the fold (fold_group_shape).

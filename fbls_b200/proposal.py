@@ -30,8 +30,13 @@ HEAD_G = 4
 MAP_CHANNELS = 4
 
 
+_MAP_PERIODS = np.geomspace(PMIN, PMAX, T_IN)
+_MAP_PERIODS.setflags(write=False)
+
+
 def map_periods() -> np.ndarray:
-    return np.geomspace(PMIN, PMAX, T_IN)
+    """The network's T_IN log-spaced map periods over [PMIN, PMAX] (read-only)."""
+    return _MAP_PERIODS
 
 
 def band_of(period: float) -> int:
@@ -54,13 +59,21 @@ def map_bank(state) -> Tuple[np.ndarray, np.ndarray]:
     return d[idx], np.asarray(state.rho, dtype=np.float64)[idx]
 
 
+def map_range(state, period_max: float) -> Tuple[int, int]:
+    """[i0, i1): the map periods a star's search covers (contiguous)."""
+    lo = max(PMIN, 4.0 * float(np.min(state.durations)) * (1.0 + 1e-9))
+    hi = min(period_max, float(state.time[-1]))
+    i0 = int(np.searchsorted(_MAP_PERIODS, lo, side="left"))
+    i1 = int(np.searchsorted(_MAP_PERIODS, hi, side="right"))
+    return i0, max(i0, i1)
+
+
 def map_plan(state, period_max: float):
     """The map periods a star's search covers (mask over map_periods()) and
     the map's durations and rho."""
-    p = map_periods()
-    lo = max(PMIN, 4.0 * float(np.min(state.durations)) * (1.0 + 1e-9))
-    hi = min(period_max, float(state.time[-1]))
-    keep = (p >= lo) & (p <= hi)
+    i0, i1 = map_range(state, period_max)
+    keep = np.zeros(T_IN, dtype=bool)
+    keep[i0:i1] = True
     d, r = map_bank(state)
     return keep, d, r
 
@@ -283,16 +296,18 @@ def features(gpu, stars, devs, bin_days: float = 0.0) -> np.ndarray:
     """(4, count, T_IN) float32, channel-major: every star's coarse map and
     its features in one fbls_coarse_features call (map_features on the
     device)."""
-    p = map_periods()
     periods, ds, rs, offsets = [], [], [], []
+    banks = {}
     for st, pmax in stars:
-        keep, d, r = map_plan(st, pmax)
-        idx = np.flatnonzero(keep)
-        lo = int(idx[0]) if idx.size else 0
-        periods.append(p[lo:lo + idx.size])
+        i0, i1 = map_range(st, pmax)
+        key = (st.durations.tobytes(), st.rho.tobytes())
+        if key not in banks:
+            banks[key] = map_bank(st)
+        d, r = banks[key]
+        periods.append(_MAP_PERIODS[i0:i1])
         ds.append(d)
         rs.append(r)
-        offsets.append(lo)
+        offsets.append(i0)
     return gpu.coarse_features(devs, periods, ds, rs, offsets, T_IN, 2.0, bin_days)
 
 
