@@ -484,6 +484,104 @@ def run_proposal(args):
     gpu.close()
 
 
+def _rescore_bytes(time_rel, origin, rows, n_all):
+    """Algorithmic bytes of one rescoring block: every observation the
+    windowed kernels visit (t, v, w and the exclusion byte for the family;
+    t and the byte for the merged times), two binary searches per transit
+    window, and the rows in and results out."""
+    period, epoch, duration = rows[:, 0], rows[:, 1], rows[:, 2]
+    total = 0.0
+    for t, c, per_visit in ((time_rel, epoch - origin, 25.0), (time_rel + origin, epoch, 9.0)):
+        klo = np.floor((t[0] - c) / period) - 1.0
+        khi = np.ceil((t[-1] - c) / period) + 1.0
+        for r in range(rows.shape[0]):
+            ks = c[r] + np.arange(klo[r], khi[r] + 1.0) * period[r]
+            lo = np.searchsorted(t, ks - duration[r] / 2.0 - 1e-6, side="left")
+            hi = np.searchsorted(t, ks + duration[r] / 2.0 + 1e-6, side="right")
+            visits = int(np.maximum(hi - np.maximum(lo, np.concatenate([[0], np.maximum.accumulate(hi)[:-1]])), 0).sum())
+            total += per_visit * visits + len(ks) * 2 * math.ceil(math.log2(t.shape[0] + 1)) * 8.0
+    return total + rows.shape[0] * (2 * 24.0 + 24.0 + 8.0)
+
+
+def run_rescore(args):
+    """Peak-selection rescoring (SURVEY's next row 1): a step is one refresh
+    block of select_peaks on the 13-sector star, 8192 rows rescored, i.e.
+    fbls_rescore_rows over the family outside the excluded set plus
+    fbls_count_rows over the merged times, through the C ABI with host
+    arrays. value: rows per second of kernel time (CUDA events on the
+    context's stream); e2e: rows per second of the whole calls."""
+    import torch
+    import oracle
+    from fbls_b200 import api, synth
+    torch.cuda.set_device(0)
+    c, cfg = synth.multi_sector(), synth.multi_sector_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    rng = np.random.default_rng(17)
+    R = args.rows
+    ta = st.time + st.origin
+    period = np.exp(rng.uniform(math.log(0.5), math.log(20.0), R))
+    rows = np.column_stack([period, ta[0] + rng.uniform(0.0, 1.0, R) * period, rng.choice(st.durations, R)])
+    ex = (rng.uniform(size=st.n) < 0.05).astype(np.uint8)
+    gpu = api.Gpu(0)
+    dev = gpu.upload(st)
+
+    def step():
+        return gpu.rescore_rows(dev, ex, rows), gpu.count_rows(ta, ex, rows)
+
+    for _ in range(args.warmup):
+        step()
+    gpu.set_kernel_timing(True)
+    gpu.counters(reset=True)
+    clocks = Clocks(0)
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sums, counts = step()
+        times.append((time.perf_counter() - t0) * 1e3)
+    clk = clocks.stop()
+    ctr = gpu.counters(reset=True)
+    kernel_ms = ctr["rescore_ms"] / args.steps
+    wall_ms = sum(times) / args.steps
+    algo = _rescore_bytes(st.time, st.origin, rows, ta.shape[0])
+    peak, peak_kind = _peaks()
+    out = {
+        "metric": "rescored rows/s (peak selection, rescore_rows + count_rows)", "value": R / (kernel_ms * 1e-3),
+        "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": kernel_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"rescore: {R} rows (period log-U[0.5, 20] d, the family's durations) of the "
+                               "13-sector star (247,104 observations), 5 % excluded",
+                   "rows": R, "observations": int(st.n),
+                   "l2": "inputs (2.2 MB) stay in L2; the kernels visit only transit windows"},
+        "step_ms": [round(t, 3) for t in times],
+        "gpu_launches": int(ctr["rescore_launches"]),
+        "e2e": {"value": R / (wall_ms * 1e-3), "unit": "rows/s", "ms_per_step": wall_ms,
+                "h2d_bytes_per_step": 2 * R * 24 + 2 * st.n + 8 * st.n,
+                "d2h_bytes_per_step": R * 24 + R * 8},
+        "roofline": {"kernel": "k_rescore_rows + k_count_rows", "bound": "hbm", "achieved": algo / (kernel_ms * 1e-3) / 1e9,
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": algo / (kernel_ms * 1e-3) / 1e9 / peak, "traffic": None,
+                     "algorithmic_bytes_per_step": algo,
+                     "note": "bytes the windowed walk must touch; the kernels are latency-bound (binary searches, "
+                             "one CTA per row), not bandwidth-bound"},
+        "clocks": clk,
+    }
+    if not args.no_cpu:
+        sample = 16
+        t0 = time.perf_counter()
+        oracle.rescore_rows(st.time, st.v, st.w, ex, rows[:sample], st.origin)
+        oracle.count_rows(ta, ex, rows[:sample])
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": sample / sec, "unit": "rows/s", "cores": 1, "kind": "port",
+                               "sample": f"the first {sample} rows through the oracle's full scan (the reference "
+                                         f"kernels' loops, single thread), {sec:.2f} s"}
+        assert np.array_equal(sums[:sample], oracle.rescore_rows(st.time, st.v, st.w, ex, rows[:sample], st.origin))
+    print(json.dumps(out))
+    dev.free()
+    gpu.close()
+
+
 def run_precision_report(args):
     """The reference's mixed mode (f32 pre-rank from (hi, lo) pairs, f64
     winner) against f64 ranking throughout, on every period of every band at
@@ -557,7 +655,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fbls_b200", choices=["fbls_b200", "reference"])
-    ap.add_argument("--workload", default="multi_sector", choices=["multi_sector", "single_sector", "survey", "proposal"])
+    ap.add_argument("--workload", default="multi_sector",
+                    choices=["multi_sector", "single_sector", "survey", "proposal", "rescore"])
+    ap.add_argument("--rows", type=int, default=8192, help="rescore workload: rows per step")
     ap.add_argument("--stars", type=int, default=512, help="survey workload: stars per GPU")
     ap.add_argument("--batch-workers", type=int, default=0,
                     help="survey / proposal workloads: search_batch host worker threads (0: stars fused into "
@@ -576,6 +676,8 @@ def main():
         run_survey(args)
     elif args.workload == "proposal":
         run_proposal(args)
+    elif args.workload == "rescore":
+        run_rescore(args)
     else:
         run_gpu(args)
 

@@ -145,6 +145,8 @@ class Counters(C.Structure):
         ("scan_ms", C.c_double),
         ("scan_bytes", C.c_double),
         ("fold_updates", C.c_uint64),
+        ("rescore_launches", C.c_uint64),
+        ("rescore_ms", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -192,6 +194,10 @@ SIGNATURES = {
     "fbls_coarse_map_batch": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, C.c_uint32]),
     "fbls_coarse_features": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, c_uint32_p, C.c_uint32,
                                        C.c_uint32, C.POINTER(C.c_float)]),
+    "fbls_rescore_rows": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint8), c_double_p, C.c_uint32,
+                                    c_double_p]),
+    "fbls_count_rows": (C.c_int, [C.c_void_p, c_double_p, C.c_uint32, C.POINTER(C.c_uint8), c_double_p, C.c_uint32,
+                                  c_uint32_p]),
     # proposal network kernels: device pointers passed as integers
     "fbls_nn_gemm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int] + [C.c_longlong] * 9
                      + [C.c_int, C.c_float, C.c_float, C.c_void_p]),

@@ -264,6 +264,32 @@ class Gpu:
         self._check(self.lib.fbls_coarse_map_batch(self.ctx, jobs, count, int(workers)))
         return outs
 
+    def rescore_rows(self, dev: DeviceReady, excluded, rows) -> np.ndarray:
+        """(R, 3) box sums a, hp, norm of rows (R x 3: period, epoch, duration)
+        over the family's observations with excluded == 0 (rescore_rows,
+        kernels.rs:936-990)."""
+        r = _f64(rows).reshape(-1, 3)
+        ex = np.ascontiguousarray(excluded, dtype=np.uint8)
+        if ex.shape[0] != dev.n:
+            raise ValueError("excluded must have one entry per family observation")
+        out = np.empty((r.shape[0], 3))
+        self._check(self.lib.fbls_rescore_rows(self.ctx, dev.handle, ex.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                               _dptr(r), r.shape[0], _dptr(out)))
+        return out
+
+    def count_rows(self, time, excluded, rows) -> np.ndarray:
+        """(R, 2) in-transit counts of rows over an ascending time vector, and
+        of those the not-excluded ones (count_rows, kernels.rs:993-1042)."""
+        t = _f64(time)
+        r = _f64(rows).reshape(-1, 3)
+        ex = np.ascontiguousarray(excluded, dtype=np.uint8)
+        if ex.shape[0] != t.shape[0]:
+            raise ValueError("excluded must have one entry per time")
+        out = np.empty((r.shape[0], 2), dtype=np.uint32)
+        self._check(self.lib.fbls_count_rows(self.ctx, _dptr(t), t.shape[0], ex.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                             _dptr(r), r.shape[0], out.ctypes.data_as(N.c_uint32_p)))
+        return out
+
     def coarse_features(self, devs: Sequence[DeviceReady], periods: Sequence, durations: Sequence, rho: Sequence,
                         offsets: Sequence[int], T: int, oversample: float = 2.0, bin_days: float = 0.0) -> np.ndarray:
         """The proposal network's input (channels, len(devs), T) float32: each

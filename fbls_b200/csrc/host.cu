@@ -61,6 +61,7 @@ struct fbls_ctx {
     DevBuf family;  // observations of the star a batch worker is searching
     DevBuf mapbin;  // time-binned observations of a coarse map
     DevBuf feat;    // the proposal network's input made from coarse maps
+    DevBuf rescore; // peak-selection rescoring: rows, masks, times and results
     PinBuf pin_up, pin_down, pin_down2;  // staging of a session's upload and download (two sessions in flight)
     std::vector<fbls_ctx*> workers;  // fbls_search_batch worker contexts, kept for reuse
 };
@@ -1678,7 +1679,8 @@ void fbls_destroy(fbls_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf* bufs[] = {&ctx->cum,     &ctx->cum32,    &ctx->hist,     &ctx->parts, &ctx->keys,  &ctx->tflags,
-                      &ctx->pass_in, &ctx->pass_out, &ctx->evidence, &ctx->fault, &ctx->family, &ctx->mapbin, &ctx->feat};
+                      &ctx->pass_in, &ctx->pass_out, &ctx->evidence, &ctx->fault, &ctx->family, &ctx->mapbin, &ctx->feat,
+                      &ctx->rescore};
     for (DevBuf* b : bufs) release(*b);
     for (PinBuf* b : {&ctx->pin_up, &ctx->pin_down, &ctx->pin_down2})
         if (b->ptr) cudaFreeHost(b->ptr);
@@ -1961,6 +1963,93 @@ int fbls_search_batch(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbl
     }
     for (uint32_t i = 0; i < count; i++)
         if (stars[i].status) return fail(ctx, stars[i].status, "star " + std::to_string(i) + ": " + errors[i]);
+    return FBLS_OK;
+}
+
+// Peak-selection rescoring (src/select/peaks.rs:148-252 calls these): the
+// rows' box sums over an uploaded family's observations outside `excluded`,
+// and their in-transit counts over a time vector. Host arrays in and out;
+// one upload, one launch, one download each.
+int fbls_rescore_rows(fbls_ctx* ctx, const fbls_ready* family, const uint8_t* excluded, const double* rows,
+                      uint32_t R, double* sums) {
+    if (!ctx || !family || (family->n && !excluded) || (R && (!rows || !sums)))
+        return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (R == 0) return FBLS_OK;
+    CK(cudaSetDevice(ctx->device), "set device");
+    const size_t o_rows = 0, o_sums = align256((size_t)R * 3 * sizeof(double)),
+                 o_ex = o_sums + align256((size_t)R * 3 * sizeof(double)),
+                 total = o_ex + align256((size_t)family->n + 1);
+    CK(ensure(ctx->rescore, total), "workspace");
+    unsigned char* d = static_cast<unsigned char*>(ctx->rescore.ptr);
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(d + o_rows, rows, (size_t)R * 3 * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
+    if (family->n) CK(cudaMemcpyAsync(d + o_ex, excluded, family->n, cudaMemcpyHostToDevice, s), "upload");
+    RescoreArgs a{};
+    a.time = family->time;
+    a.v = family->v;
+    a.w = family->w;
+    a.excluded = d + o_ex;
+    a.rows = reinterpret_cast<const double*>(d + o_rows);
+    a.origin = family->origin;
+    a.n = (int)family->n;
+    a.R = (int)R;
+    a.sums = reinterpret_cast<double*>(d + o_sums);
+    const bool timing = ctx->profile || ctx->kernel_timing;
+    if (timing) CK(cudaEventRecord(ctx->ev[0], s), "event");
+    CK(launch_rescore_rows(a, s), "rescore_rows");
+    if (timing) CK(cudaEventRecord(ctx->ev[1], s), "event");
+    ctx->counters.launches += 1;
+    ctx->counters.rescore_launches += 1;
+    CK(cudaMemcpyAsync(sums, d + o_sums, (size_t)R * 3 * sizeof(double), cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaStreamSynchronize(s), "rescore_rows");
+    if (timing) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]), "event");
+        ctx->counters.rescore_ms += ms;
+    }
+    return FBLS_OK;
+}
+
+int fbls_count_rows(fbls_ctx* ctx, const double* time, uint32_t n, const uint8_t* excluded, const double* rows,
+                    uint32_t R, uint32_t* counts) {
+    if (!ctx || (n && (!time || !excluded)) || (R && (!rows || !counts)))
+        return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    for (uint32_t i = 1; i < n; i++)
+        if (!(time[i] >= time[i - 1])) return fail(ctx, FBLS_ERR_ARGUMENT, "times must be ascending");
+    if (R == 0) return FBLS_OK;
+    CK(cudaSetDevice(ctx->device), "set device");
+    const size_t o_rows = 0, o_counts = align256((size_t)R * 3 * sizeof(double)),
+                 o_time = o_counts + align256((size_t)R * 2 * sizeof(uint32_t)),
+                 o_ex = o_time + align256((size_t)n * sizeof(double) + 8), total = o_ex + align256((size_t)n + 1);
+    CK(ensure(ctx->rescore, total), "workspace");
+    unsigned char* d = static_cast<unsigned char*>(ctx->rescore.ptr);
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(d + o_rows, rows, (size_t)R * 3 * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
+    if (n) {
+        CK(cudaMemcpyAsync(d + o_time, time, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
+        CK(cudaMemcpyAsync(d + o_ex, excluded, n, cudaMemcpyHostToDevice, s), "upload");
+    }
+    RescoreArgs a{};
+    a.time = reinterpret_cast<const double*>(d + o_time);
+    a.excluded = d + o_ex;
+    a.rows = reinterpret_cast<const double*>(d + o_rows);
+    a.n = (int)n;
+    a.R = (int)R;
+    a.counts = reinterpret_cast<uint32_t*>(d + o_counts);
+    const bool timing = ctx->profile || ctx->kernel_timing;
+    if (timing) CK(cudaEventRecord(ctx->ev[0], s), "event");
+    CK(launch_count_rows(a, s), "count_rows");
+    if (timing) CK(cudaEventRecord(ctx->ev[1], s), "event");
+    ctx->counters.launches += 1;
+    ctx->counters.rescore_launches += 1;
+    CK(cudaMemcpyAsync(counts, d + o_counts, (size_t)R * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
+       "download");
+    CK(cudaStreamSynchronize(s), "count_rows");
+    if (timing) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]), "event");
+        ctx->counters.rescore_ms += ms;
+    }
     return FBLS_OK;
 }
 

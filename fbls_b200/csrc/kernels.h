@@ -140,6 +140,22 @@ struct FeatJob {
     int offset;
 };
 
+// Peak-selection rescoring (rescore.cu): rows are (period, epoch, duration)
+// triples; RESCORE_BLOCK lanes per row (kernels.rs:41).
+constexpr int RESCORE_BLOCK = 256;
+struct RescoreArgs {
+    const double* time;        // n, ascending: family-relative (rescore) or absolute (count)
+    const double* v;           // n (rescore)
+    const double* w;           // n (rescore)
+    const uint8_t* excluded;   // n
+    const double* rows;        // R x 3
+    double origin;             // added to time before the phase (rescore)
+    int n;
+    int R;
+    double* sums;              // R x 3: a, hp, norm (rescore)
+    uint32_t* counts;          // R x 2: in transit, of which not excluded (count)
+};
+
 FoldShape fold_group_shape(int nb, int periods, int sm_count);
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
 // spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.
@@ -162,6 +178,8 @@ cudaError_t launch_bin_fields(const double* v, const double* w, const int* start
 // Job launches of the maps: jobs and offsets (njobs + 1) in device memory.
 cudaError_t launch_box_map_jobs(const MapArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream);
 cudaError_t launch_bin_fields_jobs(const BinJob* jobs, const int* b0, int njobs, int total, cudaStream_t stream);
+cudaError_t launch_rescore_rows(const RescoreArgs& a, cudaStream_t stream);
+cudaError_t launch_count_rows(const RescoreArgs& a, cudaStream_t stream);
 cudaError_t launch_map_features(const FeatJob* jobs, int njobs, int channels, int B, int T, float* x,
                                 cudaStream_t stream);
 

@@ -223,10 +223,12 @@ typedef struct {
     double scan_ms;
     double scan_bytes;        /* algorithmic bytes: 24 (2 nb + 1) + 84 tiles per period */
     uint64_t fold_updates;    /* observation x period bin updates */
+    uint64_t rescore_launches; /* rescore_rows + count_rows launches */
+    double rescore_ms;        /* their summed device time (timing enabled) */
 } fbls_counters;
 
-/* Enables per-launch event timing of the fold and scan kernels (adds one
- * event record per launch, no synchronisation). */
+/* Enables per-launch event timing of the fold, scan and rescoring kernels
+ * (adds one event record per launch, no synchronisation). */
 int fbls_set_kernel_timing(fbls_ctx* ctx, int enable);
 /* Reads (and with reset != 0 clears) the context's counters. */
 int fbls_read_counters(fbls_ctx* ctx, fbls_counters* out, int reset);
@@ -305,6 +307,23 @@ int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uin
  * message). */
 int fbls_coarse_features(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, const uint32_t* offsets,
                          uint32_t channels, uint32_t T, float* x);
+
+/* Peak-selection rescoring, replacing the kernels rescore_rows and
+ * count_rows (src/search/kernels.rs:936-1042) that Rescorer::evaluate
+ * (src/select/peaks.rs:148-252) launches. rows: R x 3 (period, epoch,
+ * duration; days, epoch absolute). fbls_rescore_rows: per row the sums
+ * (a = sum v, hp = sum w, norm = sum w) over the uploaded family's
+ * observations with excluded[i] == 0 and |phase| <= duration / 2, where x =
+ * ((t + origin) - epoch) / period + 0.5 and phase = (x - floor(x) - 0.5) *
+ * period; sums: R x 3. fbls_count_rows: per row the observations of `time`
+ * (absolute, ascending, n) in transit (phase from t - epoch) and, of those,
+ * the ones with excluded[i] == 0; counts: R x 2. The sums are the reference's
+ * bit for bit (same per-lane order and reduction tree). Returns 0,
+ * FBLS_ERR_ARGUMENT or FBLS_ERR_CUDA. */
+int fbls_rescore_rows(fbls_ctx* ctx, const fbls_ready* family, const uint8_t* excluded, const double* rows,
+                      uint32_t R, double* sums);
+int fbls_count_rows(fbls_ctx* ctx, const double* time, uint32_t n, const uint8_t* excluded, const double* rows,
+                    uint32_t R, uint32_t* counts);
 
 /* Proposal network kernels. Every pointer is device memory; `stream` is a
  * cudaStream_t (NULL: the legacy stream). Activations are f32 laid out

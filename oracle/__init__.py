@@ -61,6 +61,9 @@ def _load():
                                             _dp, _dp]),
         "orc_transit_mask": (C.c_int64, [_dp, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double,
                                          C.POINTER(C.c_uint8)]),
+        "orc_rescore_rows": (None, [_dp, _dp, _dp, C.POINTER(C.c_uint8), C.c_int64, _dp, C.c_int64, C.c_double,
+                                    _dp]),
+        "orc_count_rows": (None, [_dp, C.POINTER(C.c_uint8), C.c_int64, _dp, C.c_int64, C.POINTER(C.c_uint32)]),
         "orc_scan_bank": (C.c_int64, [_dp, _dp, _dp, C.c_int64, C.c_double, _dp, C.c_int64, C.c_int, _dp, _dp,
                                       C.c_int, _dp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp,
                                       C.POINTER(C.c_uint32)]),
@@ -176,6 +179,28 @@ def transit_mask(time, period, epoch, duration, margin) -> np.ndarray:
     _load().orc_transit_mask(_p(t), t.shape[0], period, epoch, duration, margin,
                              m.ctypes.data_as(C.POINTER(C.c_uint8)))
     return m.astype(bool)
+
+
+def rescore_rows(time, v, w, excluded, rows, origin: float) -> np.ndarray:
+    """(R, 3) box sums a, hp, norm per row (kernels.rs:936-990)."""
+    t, vv, ww = _f(time), _f(v), _f(w)
+    ex = np.ascontiguousarray(excluded, dtype=np.uint8)
+    r = _f(rows).reshape(-1, 3)
+    out = np.zeros((r.shape[0], 3))
+    _load().orc_rescore_rows(_p(t), _p(vv), _p(ww), ex.ctypes.data_as(C.POINTER(C.c_uint8)), t.shape[0], _p(r),
+                             r.shape[0], float(origin), _p(out))
+    return out
+
+
+def count_rows(time, excluded, rows) -> np.ndarray:
+    """(R, 2) in-transit and not-excluded in-transit counts per row (kernels.rs:993-1042)."""
+    t = _f(time)
+    ex = np.ascontiguousarray(excluded, dtype=np.uint8)
+    r = _f(rows).reshape(-1, 3)
+    out = np.zeros((r.shape[0], 2), dtype=np.uint32)
+    _load().orc_count_rows(_p(t), ex.ctypes.data_as(C.POINTER(C.c_uint8)), t.shape[0], _p(r), r.shape[0],
+                           out.ctypes.data_as(C.POINTER(C.c_uint32)))
+    return out
 
 
 # -- scan path ------------------------------------------------------------------

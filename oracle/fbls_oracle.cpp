@@ -436,6 +436,75 @@ extern "C" int64_t orc_transit_mask(const double* time, int64_t n, double period
     return count;
 }
 
+// Peak-selection rescoring, kernels.rs:936-1042 (RESCORE_BLOCK = 256, :41):
+// per row, lane l of 256 sums the observations i = l (mod 256) in increasing
+// i, then the lanes' partial sums meet in the tree red[l] += red[l + s] for
+// s = 128, 64, ..., 1. Every observation is visited, as in the reference.
+namespace {
+constexpr int RESCORE_LANES = 256;
+
+template <typename T>
+T lane_tree(std::vector<T>& red) {
+    for (int stride = RESCORE_LANES / 2; stride > 0; stride /= 2)
+        for (int l = 0; l < stride; l++) red[l] = red[l] + red[l + stride];
+    return red[0];
+}
+}  // namespace
+
+extern "C" void orc_rescore_rows(const double* time, const double* v, const double* w, const uint8_t* excluded,
+                                 int64_t n, const double* rows, int64_t R, double origin, double* sums) {
+    std::vector<double> ra(RESCORE_LANES), rh(RESCORE_LANES), rn(RESCORE_LANES);
+    for (int64_t r = 0; r < R; r++) {
+        const double period = rows[3 * r], epoch = rows[3 * r + 1], duration = rows[3 * r + 2];
+        const double inverse = 1.0 / period;
+        const double half = duration / 2.0;
+        for (int l = 0; l < RESCORE_LANES; l++) {
+            double a = 0.0, hp = 0.0, norm = 0.0;
+            for (int64_t i = l; i < n; i += RESCORE_LANES) {
+                if (excluded[i] != 0) continue;
+                const double x = (time[i] + origin - epoch) * inverse + 0.5;
+                const double phase = (x - std::floor(x) - 0.5) * period;
+                if (std::fabs(phase) <= half) {
+                    a += v[i];
+                    hp += w[i];
+                    norm += w[i];
+                }
+            }
+            ra[l] = a;
+            rh[l] = hp;
+            rn[l] = norm;
+        }
+        sums[3 * r] = lane_tree(ra);
+        sums[3 * r + 1] = lane_tree(rh);
+        sums[3 * r + 2] = lane_tree(rn);
+    }
+}
+
+extern "C" void orc_count_rows(const double* time, const uint8_t* excluded, int64_t n, const double* rows, int64_t R,
+                               uint32_t* counts) {
+    std::vector<uint32_t> rt(RESCORE_LANES), ru(RESCORE_LANES);
+    for (int64_t r = 0; r < R; r++) {
+        const double period = rows[3 * r], epoch = rows[3 * r + 1], duration = rows[3 * r + 2];
+        const double inverse = 1.0 / period;
+        const double half = duration / 2.0;
+        for (int l = 0; l < RESCORE_LANES; l++) {
+            uint32_t total = 0, unshared = 0;
+            for (int64_t i = l; i < n; i += RESCORE_LANES) {
+                const double x = (time[i] - epoch) * inverse + 0.5;
+                const double phase = (x - std::floor(x) - 0.5) * period;
+                if (std::fabs(phase) <= half) {
+                    total += 1;
+                    unshared += excluded[i] == 0 ? 1u : 0u;
+                }
+            }
+            rt[l] = total;
+            ru[l] = unshared;
+        }
+        counts[2 * r] = lane_tree(rt);
+        counts[2 * r + 1] = lane_tree(ru);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Scan path: fold (kernels.rs:465-553), doubled prefix sums (:237-309),
 // tile scan (:610-845, helpers :51-146, :389-455), merge (:1115-1155).
