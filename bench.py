@@ -582,6 +582,66 @@ def run_rescore(args):
     gpu.close()
 
 
+def run_single_event(args):
+    """Single-event scan (SURVEY's next row 2): a step is one
+    single_event_search of the 13-sector star (one trial period of 357 d, nb
+    68,544, 20 durations x 3 shapes), through the C ABI with the family
+    resident. value: templates per second of kernel time (fold + scan_all,
+    CUDA events around the launches on the context's stream); e2e: of the
+    whole call."""
+    import torch
+    import oracle
+    from fbls_b200 import api, synth
+    torch.cuda.set_device(0)
+    c, cfg = synth.multi_sector(), synth.multi_sector_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    gpu = api.Gpu(0)
+    dev = gpu.upload(st)
+    for _ in range(args.warmup):
+        rows, stats = gpu.single_event_search(st, cfg, dev=dev)
+    gpu.set_kernel_timing(True)
+    gpu.counters(reset=True)
+    clocks = Clocks(0)
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rows, stats = gpu.single_event_search(st, cfg, dev=dev)
+        times.append((time.perf_counter() - t0) * 1e3)
+    clk = clocks.stop()
+    ctr = gpu.counters(reset=True)
+    tm = stats["templates_scanned"]
+    ms = (ctr["fold_ms"] + ctr["scan_ms"]) / args.steps
+    wall = sum(times) / len(times)
+    out = {
+        "metric": "single-event templates/s", "value": tm / (ms * 1e-3), "unit": "templates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "single_event: the 13-sector star (247,104 observations), trial period "
+                               "baseline + 2 x 15 h, 20 durations 0.5-15 h, 3 shapes x 4 layers",
+                   "templates": tm, "survivors": stats["threshold_survivors"]},
+        "step_ms": [round(t, 3) for t in times],
+        "kernel_ms": {"fold": ctr["fold_ms"] / args.steps, "scan_all": ctr["scan_ms"] / args.steps},
+        "gpu_launches": int(ctr["launches"]) // args.steps,
+        "e2e": {"value": tm / (wall * 1e-3), "unit": "templates/s", "ms_per_step": wall,
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 40 * int(rows.shape[0])},
+        "clocks": clk,
+    }
+    if not args.no_cpu:
+        ost = oracle.family_state(c.time, c.flux, c.flux_err, cfg.durations_days())
+        t0 = time.perf_counter()
+        want, wst = oracle.single_event_search(ost, cfg)
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": wst["templates_scanned"] / sec, "unit": "templates/s", "cores": 1,
+                               "kind": "port", "sample": f"the whole search on the oracle (fold, prefix, every "
+                                                         f"template), single thread, {sec:.2f} s"}
+        out["parity"] = bool(np.array_equal(rows, want))
+    print(json.dumps(out))
+    dev.free()
+    gpu.close()
+
+
 def run_precision_report(args):
     """The reference's mixed mode (f32 pre-rank from (hi, lo) pairs, f64
     winner) against f64 ranking throughout, on every period of every band at
@@ -656,7 +716,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fbls_b200", choices=["fbls_b200", "reference"])
     ap.add_argument("--workload", default="multi_sector",
-                    choices=["multi_sector", "single_sector", "survey", "proposal", "rescore"])
+                    choices=["multi_sector", "single_sector", "survey", "proposal", "rescore", "single_event"])
     ap.add_argument("--rows", type=int, default=8192, help="rescore workload: rows per step")
     ap.add_argument("--stars", type=int, default=512, help="survey workload: stars per GPU")
     ap.add_argument("--batch-workers", type=int, default=0,
@@ -678,6 +738,8 @@ def main():
         run_proposal(args)
     elif args.workload == "rescore":
         run_rescore(args)
+    elif args.workload == "single_event":
+        run_single_event(args)
     else:
         run_gpu(args)
 

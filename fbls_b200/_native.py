@@ -135,6 +135,14 @@ class EvidenceRow(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class EventStats(C.Structure):
+    _fields_ = [("templates_scanned", C.c_uint64), ("threshold_survivors", C.c_uint64), ("overflow", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {"templates_scanned": int(self.templates_scanned),
+                "threshold_survivors": int(self.threshold_survivors), "overflow": bool(self.overflow)}
+
+
 class Counters(C.Structure):
     _fields_ = [
         ("launches", C.c_uint64),
@@ -194,6 +202,9 @@ SIGNATURES = {
     "fbls_coarse_map_batch": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, C.c_uint32]),
     "fbls_coarse_features": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, c_uint32_p, C.c_uint32,
                                        C.c_uint32, C.POINTER(C.c_float)]),
+    "fbls_single_event_search": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, c_double_p, C.c_uint32,
+                                           C.POINTER(Config), C.c_uint32, C.POINTER(Row), c_uint32_p,
+                                           C.POINTER(EventStats)]),
     "fbls_rescore_rows": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint8), c_double_p, C.c_uint32,
                                     c_double_p]),
     "fbls_count_rows": (C.c_int, [C.c_void_p, c_double_p, C.c_uint32, C.POINTER(C.c_uint8), c_double_p, C.c_uint32,

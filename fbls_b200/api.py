@@ -264,6 +264,29 @@ class Gpu:
         self._check(self.lib.fbls_coarse_map_batch(self.ctx, jobs, count, int(workers)))
         return outs
 
+    def single_event_search(self, state: FamilyState, cfg: SearchConfig, capacity: int = 131072,
+                            dev: Optional[DeviceReady] = None):
+        """single_event_search (events.rs:18-153): rows (period inf, epoch,
+        duration, score, depth) of every template above threshold at one
+        trial period longer than the baseline, and the EventStats dict."""
+        own = dev is None
+        if own:
+            dev = self.upload(state)
+        try:
+            c, keep = _config(cfg)
+            d, r = _f64(state.durations), _f64(state.rho)
+            out = np.empty((max(int(capacity), 1), 5))  # the pipeline's capacity (pipeline.rs:14)
+            n = C.c_uint32(0)
+            st = N.EventStats()
+            self._check(self.lib.fbls_single_event_search(self.ctx, dev.handle, _dptr(d), _dptr(r), len(d),
+                                                          C.byref(c), int(capacity),
+                                                          out.ctypes.data_as(C.POINTER(N.Row)), C.byref(n),
+                                                          C.byref(st)))
+            return out[: n.value].copy(), st.as_dict()
+        finally:
+            if own:
+                dev.free()
+
     def rescore_rows(self, dev: DeviceReady, excluded, rows) -> np.ndarray:
         """(R, 3) box sums a, hp, norm of rows (R x 3: period, epoch, duration)
         over the family's observations with excluded == 0 (rescore_rows,

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "../../include/fbls_b200.h"
@@ -1963,6 +1964,159 @@ int fbls_search_batch(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbl
     }
     for (uint32_t i = 0; i < count; i++)
         if (stars[i].status) return fail(ctx, stars[i].status, "star " + std::to_string(i) + ": " + errors[i]);
+    return FBLS_OK;
+}
+
+// single_event_search (events.rs:18-153): the durations sorted with their
+// rho, one trial period baseline + 2 (longest duration) + 1e-6 d (longer than
+// the data, so nothing wraps), nb = max(8, ceil(phase_oversample * trial /
+// shortest duration)); the family folded at that period by the fold kernels,
+// then k_scan_all keeps every template whose exact score reaches the
+// threshold. Rows (period +inf, epoch, duration, score, depth) come out
+// ordered by (phase, duration, shape); past `capacity` survivors the rows are
+// dropped and `overflow` set, as the reference does.
+int fbls_single_event_search(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
+                             uint32_t nd, const fbls_config* cfg, uint32_t capacity, fbls_row* rows_out,
+                             uint32_t* n_rows, fbls_event_stats* stats) {
+    if (!ctx || !ready || !durations || !rho || !cfg || !n_rows || (capacity && !rows_out))
+        return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (nd == 0 || nd > (uint32_t)MAX_DURATIONS) return fail(ctx, FBLS_ERR_ARGUMENT, "1 to 64 durations");
+    if (cfg->n_ingress < 1 || cfg->n_ingress > (uint32_t)MAX_SHAPES || cfg->shape_layers < 1 ||
+        cfg->shape_layers > (uint32_t)MAX_LAYERS)
+        return fail(ctx, FBLS_ERR_ARGUMENT, "bank size outside the supported range");
+    *n_rows = 0;
+    CK(cudaSetDevice(ctx->device), "set device");
+    std::vector<std::pair<double, double>> ds(nd);
+    for (uint32_t i = 0; i < nd; i++) ds[i] = {durations[i], rho[i]};
+    std::stable_sort(ds.begin(), ds.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    if (!(ds[0].first > 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "durations must be positive");
+    const double trial = ready->t_last + 2.0 * ds[nd - 1].first + 1e-6;
+    const uint64_t nb64 = std::max<uint64_t>(8, as_u64(std::ceil((double)cfg->phase_oversample * trial / ds[0].first)));
+    if (nb64 > (1u << 24)) return fail(ctx, FBLS_ERR_ARGUMENT, "phase grid too large");
+    const int nb = (int)nb64;
+    const double scale = (double)nb / trial;
+    const uint32_t ns = cfg->n_ingress, layers = cfg->shape_layers;
+    std::vector<double> bank;  // durations | rho | ingress | factors (scan.rs:157-171)
+    for (auto& d : ds) bank.push_back(d.first);
+    for (auto& d : ds) bank.push_back(d.second);
+    bank.insert(bank.end(), cfg->ingress_fractions, cfg->ingress_fractions + ns);
+    for (uint32_t si = 0; si < ns; si++)
+        for (uint32_t l = 0; l < layers; l++)
+            bank.push_back(1.0 - 2.0 * cfg->ingress_fractions[si] *
+                                     (layers > 1 ? (double)l / (double)(layers - 1) : 0.0));
+    const FoldShape shape = fold_group_shape(nb, 1, ctx->sm_count);
+    std::vector<int> chunks((size_t)ready->n + 2);
+    const int count = fold_chunks(ready->time_host.data(), (int)ready->n, scale, nb, shape.span_cap,
+                                  shape.chunk_cap, chunks.data(), (int)chunks.size());
+    if (count < 1) return fail(ctx, FBLS_ERR_ARGUMENT, "fold chunking failed");
+    chunks.resize((size_t)count + 1);
+    const size_t stride = 2 * (size_t)nb + 1;
+    const size_t o_scale = 0, o_bank = 256, o_chunks = o_bank + align256(bank.size() * sizeof(double)),
+                 in_total = o_chunks + align256(chunks.size() * sizeof(int));
+    const size_t o_counter = 0, o_rec = 256, out_total = o_rec + align256((size_t)capacity * EVENT_RECORD * 8 + 8);
+    CK(ensure(ctx->pass_in, in_total), "workspace");
+    CK(ensure(ctx->pass_out, out_total), "workspace");
+    CK(ensure(ctx->cum, NF * stride * sizeof(double)), "workspace");
+    CK(ensure(ctx->cum32, NF * stride * sizeof(float2)), "workspace");
+    if (!shape.hist_in_smem) CK(ensure(ctx->hist, (size_t)shape.group * NF * shape.row_stride * sizeof(double)),
+                                "workspace");
+    CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
+    CK(ensure_pinned(ctx->pin_up, in_total), "pinned workspace");
+    unsigned char* up = static_cast<unsigned char*>(ctx->pin_up.ptr);
+    std::memcpy(up + o_scale, &scale, sizeof(double));
+    std::memcpy(up + o_bank, bank.data(), bank.size() * sizeof(double));
+    std::memcpy(up + o_chunks, chunks.data(), chunks.size() * sizeof(int));
+    unsigned char* din = static_cast<unsigned char*>(ctx->pass_in.ptr);
+    unsigned char* dout = static_cast<unsigned char*>(ctx->pass_out.ptr);
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
+    CK(cudaMemsetAsync(dout + o_counter, 0, sizeof(uint32_t), s), "workspace");
+    CK(cudaMemcpyAsync(din, up, in_total, cudaMemcpyHostToDevice, s), "upload");
+    FoldArgs fa{};
+    fa.time = ready->time;
+    fa.v = ready->v;
+    fa.w = ready->w;
+    fa.scales = reinterpret_cast<const double*>(din + o_scale);
+    fa.n = (int)ready->n;
+    fa.nb = nb;
+    fa.periods = 1;
+    fa.group = shape.group;
+    fa.cum = as<double>(ctx->cum);
+    fa.cum32 = as<float2>(ctx->cum32);
+    fa.hist_global = shape.hist_in_smem ? nullptr : as<double>(ctx->hist);
+    fa.chunks = reinterpret_cast<const int*>(din + o_chunks);
+    fa.nchunks = count;
+    fa.stage_field = shape.stage_field;
+    fa.window = shape.window;
+    fa.row_stride = shape.row_stride;
+    fa.fault = as<uint32_t>(ctx->fault);
+    const bool timing = ctx->profile || ctx->kernel_timing;
+    if (timing) CK(cudaEventRecord(ctx->ev[0], s), "event");
+    CK(launch_fold(fa, shape, s), "fold");
+    if (timing) CK(cudaEventRecord(ctx->ev[1], s), "event");
+    const double* d_bank = reinterpret_cast<const double*>(din + o_bank);
+    EventArgs ea{};
+    ea.cum = fa.cum;
+    ea.durations = d_bank;
+    ea.rho = d_bank + nd;
+    ea.ingress = d_bank + 2 * nd;
+    ea.factors = d_bank + 2 * nd + ns;
+    ea.scale = scale;
+    ea.baseline = ready->baseline_norm;
+    ea.threshold = cfg->threshold;
+    ea.n = (double)ready->n;
+    ea.nb = nb;
+    ea.nd = (int)nd;
+    ea.ns = (int)ns;
+    ea.layers = (int)layers;
+    ea.capacity = capacity;
+    ea.counter = reinterpret_cast<uint32_t*>(dout + o_counter);
+    ea.records = reinterpret_cast<double*>(dout + o_rec);
+    CK(launch_scan_all(ea, s), "scan_all");
+    if (timing) CK(cudaEventRecord(ctx->ev[2], s), "event");
+    ctx->counters.launches += 2;
+    ctx->counters.fold_launches += 1;
+    ctx->counters.scan_launches += 1;
+    uint32_t found = 0, fault = 0;
+    CK(cudaMemcpyAsync(&found, dout + o_counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaMemcpyAsync(&fault, ctx->fault.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaStreamSynchronize(s), "single_event_search");
+    if (fault) return fail(ctx, FBLS_ERR_CUDA, "fold: staging copies did not complete");
+    if (timing) {
+        float f_ms = 0.f, s_ms = 0.f;
+        CK(cudaEventElapsedTime(&f_ms, ctx->ev[0], ctx->ev[1]), "event");
+        CK(cudaEventElapsedTime(&s_ms, ctx->ev[1], ctx->ev[2]), "event");
+        ctx->counters.fold_ms += f_ms;
+        ctx->counters.scan_ms += s_ms;
+    }
+    ctx->counters.fold_updates += ready->n;
+    if (stats) {
+        stats->templates_scanned = (uint64_t)nb * nd * ns;
+        stats->threshold_survivors = found;
+        stats->overflow = found > capacity ? 1 : 0;
+    }
+    if (found > capacity || found == 0) return FBLS_OK;
+    std::vector<double> rec((size_t)found * EVENT_RECORD);
+    CK(cudaMemcpyAsync(rec.data(), dout + o_rec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, s),
+       "download");
+    CK(cudaStreamSynchronize(s), "single_event_search");
+    std::vector<uint32_t> order(found);
+    for (uint32_t i = 0; i < found; i++) order[i] = i;
+    auto key = [&](uint32_t i) {
+        const double* r = &rec[(size_t)i * EVENT_RECORD];
+        return std::make_tuple(r[0], r[4], r[5]);
+    };
+    std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
+    for (uint32_t m = 0; m < found; m++) {
+        const double* r = &rec[(size_t)order[m] * EVENT_RECORD];
+        fbls_row& row = rows_out[m];
+        row.period = __builtin_huge_val();
+        row.epoch = (r[0] + r[1] / 2.0) / scale + ready->origin;
+        row.duration = r[1] / scale;
+        row.score = r[2];
+        row.depth = r[3];
+    }
+    *n_rows = found;
     return FBLS_OK;
 }
 

@@ -105,6 +105,26 @@ struct MergeArgs {
     uint32_t* flags_out;
 };
 
+// Single-event scan (scan_all, kernels.rs:851-921): every template of one
+// trial period whose exact f64 score reaches the threshold, appended through
+// a counter as (j, k, score, depth, duration index, shape index).
+constexpr int EVENT_RECORD = 6;
+struct EventArgs {
+    const double* cum;        // NF x (2nb+1)
+    const double* durations;  // nd, ascending
+    const double* rho;        // nd
+    const double* ingress;    // ns
+    const double* factors;    // ns x layers
+    double scale;
+    double baseline;          // baseline_norm c
+    double threshold;
+    double n;                 // observation count
+    int nb, nd, ns, layers;
+    uint32_t capacity;        // records
+    uint32_t* counter;        // templates above threshold (may exceed capacity)
+    double* records;          // capacity x EVENT_RECORD
+};
+
 // Coarse periodogram of the proposal path (proposal.cu).
 constexpr int MAP_MAX_DURATIONS = 8;
 struct MapArgs {
@@ -171,6 +191,7 @@ cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, i
 cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, cudaStream_t stream);
 cudaError_t launch_merge_jobs(const MergeArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream);
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream);
+cudaError_t launch_scan_all(const EventArgs& a, cudaStream_t stream);
 cudaError_t launch_merge(const MergeArgs& a, cudaStream_t stream);
 cudaError_t launch_box_map(const MapArgs& a, int periods, cudaStream_t stream);
 cudaError_t launch_bin_fields(const double* v, const double* w, const int* starts, int nbins, double* vb, double* wb,

@@ -392,6 +392,59 @@ __device__ __forceinline__ void merge_period(const MergeArgs& a, const int f) {
 // Launchers.
 // ---------------------------------------------------------------------------
 
+// Single-event scan (kernels.rs:851-921): one thread per phase j of the
+// single trial period; for every duration whose box is usable (width below
+// nb / 2, 3 .. n - 3 observations) and every shape, the exact f64 score
+// (a / rho) / sqrt(norm - hp^2 / c); a template reaching the threshold takes
+// a slot from the counter. The host orders the records by (j, duration,
+// shape), so the output does not depend on the order of the appends.
+__global__ void __launch_bounds__(TILE) k_scan_all(EventArgs a) {
+    const uint32_t nb = (uint32_t)a.nb;
+    const uint32_t j = blockIdx.x * TILE + threadIdx.x;
+    if (j >= nb) return;
+    const size_t stride = 2 * (size_t)nb + 1;
+    const double* rv = a.cum + F_V * stride;
+    const double* rw = a.cum + F_W * stride;
+    const double* rn = a.cum + F_N * stride;
+    const uint32_t half = nb / 2;
+    for (int di = 0; di < a.nd; di++) {
+        const uint32_t raw = template_width(a.durations[di], a.scale);
+        const uint32_t k = raw < half ? raw : half;
+        const double r = a.rho[di];
+        const double count = interval64(rn, j, k);
+        const double w = interval64(rw, j, k);
+        const double av = interval64(rv, j, k);
+        if (!(raw < half && count >= 3.0 && count <= a.n - 3.0)) continue;
+        for (int si = 0; si < a.ns; si++) {
+            double aa, hp, norm;
+            shape_sums64(rv, rw, j, k, av, w, w, a.ingress[si], a.factors, si, a.layers, aa, hp, norm);
+            const double q = __dsub_rn(norm, __ddiv_rn(__dmul_rn(hp, hp), a.baseline));
+            if (!(aa > 0.0 && q > 0.0)) continue;
+            const double score = __ddiv_rn(__ddiv_rn(aa, r), __dsqrt_rn(q));
+            if (score >= a.threshold) {
+                const uint32_t slot = atomicAdd(a.counter, 1u);
+                if (slot < a.capacity) {
+                    double* rec = a.records + (size_t)slot * EVENT_RECORD;
+                    rec[0] = (double)j;
+                    rec[1] = (double)k;
+                    rec[2] = score;
+                    rec[3] = __ddiv_rn(aa, q);
+                    rec[4] = (double)di;
+                    rec[5] = (double)si;
+                }
+            }
+        }
+    }
+}
+
+cudaError_t launch_scan_all(const EventArgs& a, cudaStream_t stream) {
+    if (a.nb < 2 || a.nd < 1 || a.nd > MAX_DURATIONS || a.ns < 1 || a.ns > MAX_SHAPES || a.layers < 1 ||
+        a.layers > MAX_LAYERS || !a.cum || !a.counter || (a.capacity && !a.records))
+        return cudaErrorInvalidValue;
+    k_scan_all<<<(a.nb + TILE - 1) / TILE, TILE, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream) {
     dim3 grid((a.nb + TILE - 1) / TILE, periods);
     k_scan_tiles<<<grid, TILE, 0, stream>>>(a);

@@ -308,6 +308,25 @@ int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uin
 int fbls_coarse_features(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, const uint32_t* offsets,
                          uint32_t channels, uint32_t T, float* x);
 
+/* EventStats, src/search/events.rs:10-15. */
+typedef struct {
+    uint64_t templates_scanned;   /* nb x nd x shapes */
+    uint64_t threshold_survivors; /* templates at or above threshold */
+    int overflow;                 /* survivors exceeded capacity: no rows */
+} fbls_event_stats;
+
+/* single_event_search (src/search/events.rs:18-153): every template (phase,
+ * duration, shape) above cfg->threshold at one trial period longer than the
+ * observing baseline (baseline + 2 x longest duration + 1e-6 d), so nothing
+ * folds; nb = max(8, ceil(phase_oversample x trial / shortest duration)).
+ * Rows: period +inf, epoch, duration, score (the exact f64 score), depth
+ * (a / q), ordered by (phase, duration, shape) — the reference appends them
+ * in an arbitrary order. More than `capacity` survivors: no rows, overflow
+ * set, status 0. */
+int fbls_single_event_search(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
+                             uint32_t nd, const fbls_config* cfg, uint32_t capacity, fbls_row* rows_out,
+                             uint32_t* n_rows, fbls_event_stats* stats);
+
 /* Peak-selection rescoring, replacing the kernels rescore_rows and
  * count_rows (src/search/kernels.rs:936-1042) that Rescorer::evaluate
  * (src/select/peaks.rs:148-252) launches. rows: R x 3 (period, epoch,

@@ -64,6 +64,8 @@ def _load():
         "orc_rescore_rows": (None, [_dp, _dp, _dp, C.POINTER(C.c_uint8), C.c_int64, _dp, C.c_int64, C.c_double,
                                     _dp]),
         "orc_count_rows": (None, [_dp, C.POINTER(C.c_uint8), C.c_int64, _dp, C.c_int64, C.POINTER(C.c_uint32)]),
+        "orc_single_event_scan": (C.c_int64, [_dp, _dp, _dp, C.c_int64, C.c_double, C.c_double, C.c_int, _dp, _dp,
+                                              C.c_int, _dp, C.c_int, C.c_int, C.c_double, C.c_int64, _dp]),
         "orc_scan_bank": (C.c_int64, [_dp, _dp, _dp, C.c_int64, C.c_double, _dp, C.c_int64, C.c_int, _dp, _dp,
                                       C.c_int, _dp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp,
                                       C.POINTER(C.c_uint32)]),
@@ -305,6 +307,33 @@ def fold_prefix(state: State, scale: float, nb: int):
     lib.orc_fold_prefix(_p(state.time), _p(state.v), _p(state.w), state.n, scale, nb, _p(folded), _p(cum),
                         cum32.ctypes.data_as(C.POINTER(C.c_float)))
     return folded, cum, cum32
+
+
+def single_event_search(state: State, cfg, capacity: int = 131072):
+    """events.rs:18-153: rows (period inf, epoch, duration, score, depth) of
+    every template above threshold at one trial period longer than the
+    baseline, in (phase, duration, shape) order, and the stats
+    (templates_scanned, threshold_survivors, overflow)."""
+    order = np.argsort(np.asarray(state.durations), kind="stable")
+    d = _f(np.asarray(state.durations)[order])
+    r = _f(np.asarray(state.rho)[order])
+    baseline = float(state.time[-1])
+    trial = baseline + 2.0 * float(d[-1]) + 1e-6
+    nb = max(8, int(math.ceil(cfg.phase_oversample * trial / float(d[0]))))
+    scale = nb / trial
+    ing = _f(cfg.ingress_fractions)
+    rec = np.empty((capacity, 4))
+    count = _load().orc_single_event_scan(_p(state.time), _p(state.v), _p(state.w), state.n, state.baseline_norm,
+                                          scale, nb, _p(d), _p(r), d.shape[0], _p(ing), ing.shape[0],
+                                          cfg.shape_layers, cfg.threshold, capacity, _p(rec))
+    stats = {"templates_scanned": nb * d.shape[0] * ing.shape[0], "threshold_survivors": int(count),
+             "overflow": bool(count > capacity)}
+    if count > capacity:
+        return np.empty((0, 5)), stats
+    rec = rec[:count]
+    rows = np.column_stack([np.full(count, np.inf), (rec[:, 0] + rec[:, 1] / 2.0) / scale + state.origin,
+                            rec[:, 1] / scale, rec[:, 2], rec[:, 3]])
+    return rows, stats
 
 
 def box_direct(state: State, scale: float, nb: int, j: int, k: int):

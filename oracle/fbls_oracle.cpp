@@ -970,6 +970,59 @@ extern "C" void orc_box_direct(const double* time, const double* v, const double
     out3[2] = c;
 }
 
+// Single-event scan, events.rs:18-153 with scan_all (kernels.rs:851-921):
+// the fold and doubled prefix of one trial period at `scale` with nb bins,
+// then every template (phase j, duration, shape) whose exact f64 score
+// reaches the threshold, in (j, duration, shape) order: records of (j, k,
+// score, depth = a / q). Returns the count; records beyond `capacity` are
+// not written.
+extern "C" int64_t orc_single_event_scan(const double* time, const double* v, const double* w, int64_t n,
+                                         double baseline_norm, double scale, int nb, const double* durations,
+                                         const double* rho, int nd, const double* ingress, int ns, int layers,
+                                         double threshold, int64_t capacity, double* records) {
+    std::vector<double> folded, cum;
+    std::vector<float> cum32;
+    fold_and_prefix(time, v, w, n, scale, nb, folded, cum, cum32);
+    const PeriodView P{cum.data(), cum32.data(), nb, 2 * nb + 1};
+    std::vector<double> factors;
+    for (int s = 0; s < ns; s++)
+        for (int l = 0; l < layers; l++)
+            factors.push_back(1.0 - 2.0 * ingress[s] * (layers > 1 ? (double)l / (double)(layers - 1) : 0.0));
+    const Bank B{durations, rho, nd, ingress, ns, layers, factors.data(), 0.0, baseline_norm, (double)n};
+    const size_t half = (size_t)nb / 2;
+    int64_t count = 0;
+    for (size_t j = 0; j < (size_t)nb; j++) {
+        for (int di = 0; di < nd; di++) {
+            size_t raw = as_usize(std::floor(durations[di] * scale + 0.5));
+            if (raw < 1) raw = 1;
+            const size_t k = raw < half ? raw : half;
+            const double r = rho[di];
+            const double cnt = interval(P, F_N, j, k);
+            const double ww = interval(P, F_W, j, k);
+            const double oa = interval(P, F_V, j, k);
+            if (!(raw < half && cnt >= 3.0 && cnt <= (double)n - 3.0)) continue;
+            for (int si = 0; si < ns; si++) {
+                double a, hp, norm;
+                shape_sums(P, j, k, oa, ww, ww, ingress[si], B, si, a, hp, norm);
+                const double q = norm - hp * hp / baseline_norm;
+                if (!(a > 0.0 && q > 0.0)) continue;
+                const double score = (a / r) / std::sqrt(q);
+                if (score >= threshold) {
+                    if (count < capacity) {
+                        double* rec = records + 4 * count;
+                        rec[0] = (double)j;
+                        rec[1] = (double)k;
+                        rec[2] = score;
+                        rec[3] = a / q;
+                    }
+                    count++;
+                }
+            }
+        }
+    }
+    return count;
+}
+
 // ---------------------------------------------------------------------------
 // Evidence: src/search/evidence.rs:37-67 (helpers), :75-144 (fold, prefix),
 // :151-273 (screen), :280-632 (joint tiles), :655-1003 (host).
