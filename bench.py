@@ -292,7 +292,7 @@ def run_gpu(args):
                              "served from shared memory, and the kernel is bound by the shared-memory pipe "
                              "(profiles/k_fold_walk_multi_sector.md)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h),
-                "ms_per_step": e2e_total / args.steps},
+                "ms_per_step": e2e_total / args.steps, "step_ms": [round(t, 2) for t in e2e_ms]},
         "clocks": clk,
     }
     if world == 1 and not args.no_cpu:
@@ -642,6 +642,60 @@ def run_single_event(args):
     gpu.close()
 
 
+def run_detrend(args):
+    """Biweight detrending (SURVEY's next row 3): a step is one
+    fbls_biweight_flatten of the 13-sector curve (247,104 observations at
+    120 s) with a 0.75 d window, c 5, 10 iterations, gap 0.5 d. value:
+    observations per second of kernel time; e2e: of the whole call (window
+    bounds on the host, upload, download)."""
+    import torch
+    import oracle
+    from fbls_b200 import api, synth
+    torch.cuda.set_device(0)
+    c = synth.multi_sector()
+    t = c.time - c.time[0]
+    gpu = api.Gpu(0)
+    for _ in range(args.warmup):
+        out = gpu.biweight_flatten(t, c.flux, 0.75)
+    gpu.set_kernel_timing(True)
+    gpu.counters(reset=True)
+    clocks = Clocks(0)
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = gpu.biweight_flatten(t, c.flux, 0.75)
+        times.append((time.perf_counter() - t0) * 1e3)
+    clk = clocks.stop()
+    ctr = gpu.counters(reset=True)
+    ms = ctr["detrend_ms"] / args.steps
+    wall = sum(times) / len(times)
+    n = t.shape[0]
+    res = {
+        "metric": "detrended observations/s (biweight, 0.75 d window)", "value": n / (ms * 1e-3),
+        "unit": "observations/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "detrend: the 13-sector curve (247,104 observations at 120 s, 1 d gaps), biweight "
+                               "window 0.75 d (about 540 observations), c 5, 10 iterations, gap 0.5 d"},
+        "step_ms": [round(x, 2) for x in times], "gpu_launches": int(ctr["launches"]) // args.steps,
+        "e2e": {"value": n / (wall * 1e-3), "unit": "observations/s", "ms_per_step": wall,
+                "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
+        "clocks": clk,
+    }
+    if not args.no_cpu:
+        k = 2000
+        t0 = time.perf_counter()
+        want = oracle.biweight_flatten(t[:k], c.flux[:k], 0.75)
+        sec = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": k / sec, "unit": "observations/s", "cores": 1, "kind": "port",
+                               "sample": f"the first {k} observations through the oracle's form of the reference "
+                                         f"kernel (single thread), {sec:.2f} s"}
+        res["parity_sample"] = bool(np.array_equal(gpu.biweight_flatten(t[:k], c.flux[:k], 0.75), want))
+    print(json.dumps(res))
+    gpu.close()
+
+
 def run_precision_report(args):
     """The reference's mixed mode (f32 pre-rank from (hi, lo) pairs, f64
     winner) against f64 ranking throughout, on every period of every band at
@@ -716,7 +770,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fbls_b200", choices=["fbls_b200", "reference"])
     ap.add_argument("--workload", default="multi_sector",
-                    choices=["multi_sector", "single_sector", "survey", "proposal", "rescore", "single_event"])
+                    choices=["multi_sector", "single_sector", "survey", "proposal", "rescore", "single_event",
+                             "detrend"])
     ap.add_argument("--rows", type=int, default=8192, help="rescore workload: rows per step")
     ap.add_argument("--stars", type=int, default=512, help="survey workload: stars per GPU")
     ap.add_argument("--batch-workers", type=int, default=0,
@@ -740,6 +795,8 @@ def main():
         run_rescore(args)
     elif args.workload == "single_event":
         run_single_event(args)
+    elif args.workload == "detrend":
+        run_detrend(args)
     else:
         run_gpu(args)
 

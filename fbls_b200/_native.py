@@ -155,6 +155,7 @@ class Counters(C.Structure):
         ("fold_updates", C.c_uint64),
         ("rescore_launches", C.c_uint64),
         ("rescore_ms", C.c_double),
+        ("detrend_ms", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -202,6 +203,8 @@ SIGNATURES = {
     "fbls_coarse_map_batch": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, C.c_uint32]),
     "fbls_coarse_features": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, c_uint32_p, C.c_uint32,
                                        C.c_uint32, C.POINTER(C.c_float)]),
+    "fbls_biweight_flatten": (C.c_int, [C.c_void_p, c_double_p, c_double_p, C.c_uint32, C.c_double, C.c_double,
+                                        C.c_double, C.c_uint32, c_double_p]),
     "fbls_single_event_search": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, c_double_p, C.c_uint32,
                                            C.POINTER(Config), C.c_uint32, C.POINTER(Row), c_uint32_p,
                                            C.POINTER(EventStats)]),

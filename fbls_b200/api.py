@@ -264,6 +264,16 @@ class Gpu:
         self._check(self.lib.fbls_coarse_map_batch(self.ctx, jobs, count, int(workers)))
         return outs
 
+    def biweight_flatten(self, time, relative_flux, window: float, gap: float = 0.5, c: float = 5.0,
+                         iterations: int = 10) -> np.ndarray:
+        """biweight_flatten_gpu (curve.rs:256-329): (1 + relative_flux) over
+        its biweight location in a sliding window, minus 1."""
+        t, f = _f64(time), _f64(relative_flux)
+        out = np.empty_like(t)
+        self._check(self.lib.fbls_biweight_flatten(self.ctx, _dptr(t), _dptr(f), t.shape[0], float(window),
+                                                   float(gap), float(c), int(iterations), _dptr(out)))
+        return out
+
     def single_event_search(self, state: FamilyState, cfg: SearchConfig, capacity: int = 131072,
                             dev: Optional[DeviceReady] = None):
         """single_event_search (events.rs:18-153): rows (period inf, epoch,

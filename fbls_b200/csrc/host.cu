@@ -2120,6 +2120,87 @@ int fbls_single_event_search(fbls_ctx* ctx, const fbls_ready* ready, const doubl
     return FBLS_OK;
 }
 
+// biweight_flatten_gpu (src/prep/curve.rs:256-329): window bounds per
+// observation from the sorted times (segments split where the time step
+// exceeds `gap`), blocks of up to 128 observations whose windows' union fits
+// the shared-memory stage, one k_biweight launch. A window wider than the
+// stage is read from global memory by a block of its own, so every window
+// runs on the GPU (the reference sends a curve with one such window to its
+// CPU implementation, which gives the same values).
+int fbls_biweight_flatten(fbls_ctx* ctx, const double* time, const double* relative_flux, uint32_t n, double window,
+                          double gap, double c, uint32_t iterations, double* out) {
+    if (!ctx || (n && (!time || !relative_flux || !out))) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (n == 0) return FBLS_OK;
+    if (!(window >= 0.0) || !(gap >= 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "window and gap must not be negative");
+    for (uint32_t i = 1; i < n; i++)
+        if (!(time[i] >= time[i - 1])) return fail(ctx, FBLS_ERR_ARGUMENT, "times must be ascending");
+    CK(cudaSetDevice(ctx->device), "set device");
+    std::vector<uint32_t> lo(n), hi(n);
+    std::vector<std::pair<uint32_t, uint32_t>> segs;
+    for (uint32_t start = 0, i = 1; i <= n; i++)
+        if (i == n || time[i] - time[i - 1] > gap) {
+            segs.push_back({start, i});
+            start = i;
+        }
+    parallel_for(segs.size(), [&](size_t sgi) {
+        const uint32_t a = segs[sgi].first, b = segs[sgi].second;
+        const double* t0 = time + a;
+        const double* t1 = time + b;
+        for (uint32_t j = a; j < b; j++) {
+            lo[j] = a + (uint32_t)(std::lower_bound(t0, t1, time[j] - window / 2.0) - t0);
+            hi[j] = a + (uint32_t)(std::upper_bound(t0, t1, time[j] + window / 2.0) - t0);
+        }
+    });
+    std::vector<uint32_t> blocks;
+    size_t smem = 0;
+    for (uint32_t first = 0; first < n;) {
+        uint32_t count = 1;
+        while (count < (uint32_t)BIWEIGHT_THREADS && first + count < n &&
+               hi[first + count] - lo[first] <= (uint32_t)BIWEIGHT_STAGE)
+            count++;
+        const uint32_t ulo = lo[first], uhi = hi[first + count - 1];
+        if (uhi - ulo <= (uint32_t)BIWEIGHT_STAGE) smem = std::max(smem, (size_t)(uhi - ulo) * sizeof(double));
+        blocks.insert(blocks.end(), {first, count, ulo, uhi});
+        first += count;
+    }
+    const size_t nblocks = blocks.size() / 4;
+    const size_t o_flux = 0, o_lo = align256((size_t)n * 8), o_hi = o_lo + align256((size_t)n * 4),
+                 o_blk = o_hi + align256((size_t)n * 4), o_out = o_blk + align256(blocks.size() * 4),
+                 total = o_out + align256((size_t)n * 8);
+    CK(ensure(ctx->pass_in, total), "workspace");
+    CK(ensure_pinned(ctx->pin_up, o_out), "pinned workspace");
+    unsigned char* up = static_cast<unsigned char*>(ctx->pin_up.ptr);
+    double* fl = reinterpret_cast<double*>(up + o_flux);
+    for (uint32_t i = 0; i < n; i++) fl[i] = 1.0 + relative_flux[i];
+    std::memcpy(up + o_lo, lo.data(), (size_t)n * 4);
+    std::memcpy(up + o_hi, hi.data(), (size_t)n * 4);
+    std::memcpy(up + o_blk, blocks.data(), blocks.size() * 4);
+    unsigned char* d = static_cast<unsigned char*>(ctx->pass_in.ptr);
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(d, up, o_out, cudaMemcpyHostToDevice, s), "upload");
+    BiweightArgs a{};
+    a.flux = reinterpret_cast<const double*>(d + o_flux);
+    a.lo = reinterpret_cast<const uint32_t*>(d + o_lo);
+    a.hi = reinterpret_cast<const uint32_t*>(d + o_hi);
+    a.blocks = reinterpret_cast<const uint32_t*>(d + o_blk);
+    a.c = c;
+    a.iterations = (int)iterations;
+    a.out = reinterpret_cast<double*>(d + o_out);
+    const bool timing = ctx->profile || ctx->kernel_timing;
+    if (timing) CK(cudaEventRecord(ctx->ev[0], s), "event");
+    CK(launch_biweight(a, (int)nblocks, smem, s), "biweight");
+    if (timing) CK(cudaEventRecord(ctx->ev[1], s), "event");
+    ctx->counters.launches += 1;
+    CK(cudaMemcpyAsync(out, d + o_out, (size_t)n * 8, cudaMemcpyDeviceToHost, s), "download");
+    CK(cudaStreamSynchronize(s), "biweight");
+    if (timing) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]), "event");
+        ctx->counters.detrend_ms += ms;
+    }
+    return FBLS_OK;
+}
+
 // Peak-selection rescoring (src/select/peaks.rs:148-252 calls these): the
 // rows' box sums over an uploaded family's observations outside `excluded`,
 // and their in-transit counts over a time vector. Host arrays in and out;

@@ -176,6 +176,21 @@ struct RescoreArgs {
     uint32_t* counts;          // R x 2: in transit, of which not excluded (count)
 };
 
+// Biweight detrending (biweight.cu): blocks of up to BIWEIGHT_THREADS
+// consecutive observations; a block's window union is staged in shared
+// memory when it holds at most BIWEIGHT_STAGE values.
+constexpr int BIWEIGHT_THREADS = 128;
+constexpr int BIWEIGHT_STAGE = 25600;  // doubles (200 KB)
+struct BiweightArgs {
+    const double* flux;      // n: 1 + relative flux
+    const uint32_t* lo;      // n: first index of each window
+    const uint32_t* hi;      // n: one past the last
+    const uint32_t* blocks;  // 4 per block: first, count, union start, union end
+    double c;                // tuning constant
+    int iterations;
+    double* out;             // n: flux / location - 1
+};
+
 FoldShape fold_group_shape(int nb, int periods, int sm_count);
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
 // spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.
@@ -199,6 +214,7 @@ cudaError_t launch_bin_fields(const double* v, const double* w, const int* start
 // Job launches of the maps: jobs and offsets (njobs + 1) in device memory.
 cudaError_t launch_box_map_jobs(const MapArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream);
 cudaError_t launch_bin_fields_jobs(const BinJob* jobs, const int* b0, int njobs, int total, cudaStream_t stream);
+cudaError_t launch_biweight(const BiweightArgs& a, int nblocks, size_t smem, cudaStream_t stream);
 cudaError_t launch_rescore_rows(const RescoreArgs& a, cudaStream_t stream);
 cudaError_t launch_count_rows(const RescoreArgs& a, cudaStream_t stream);
 cudaError_t launch_map_features(const FeatJob* jobs, int njobs, int channels, int B, int T, float* x,

@@ -225,6 +225,7 @@ typedef struct {
     uint64_t fold_updates;    /* observation x period bin updates */
     uint64_t rescore_launches; /* rescore_rows + count_rows launches */
     double rescore_ms;        /* their summed device time (timing enabled) */
+    double detrend_ms;        /* biweight launches' device time (timing enabled) */
 } fbls_counters;
 
 /* Enables per-launch event timing of the fold, scan and rescoring kernels
@@ -307,6 +308,17 @@ int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uin
  * message). */
 int fbls_coarse_features(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, const uint32_t* offsets,
                          uint32_t channels, uint32_t T, float* x);
+
+/* biweight_flatten_gpu (src/prep/curve.rs:256-329, kernel biweight
+ * kernels.rs:1051-1110): for every observation of the ascending `time`, the
+ * Tukey biweight location (tuning constant c, `iterations` reweightings from
+ * the lower median) of 1 + relative_flux over the observations within
+ * window / 2 of it in its gap-separated segment; out = (1 + relative_flux) /
+ * location - 1. Medians are the windows' exact lower medians (bisection as
+ * the reference). Device time adds to the counters' detrend_ms when timing is
+ * on. Returns 0, FBLS_ERR_ARGUMENT or FBLS_ERR_CUDA. */
+int fbls_biweight_flatten(fbls_ctx* ctx, const double* time, const double* relative_flux, uint32_t n, double window,
+                          double gap, double c, uint32_t iterations, double* out);
 
 /* EventStats, src/search/events.rs:10-15. */
 typedef struct {

@@ -64,6 +64,8 @@ def _load():
         "orc_rescore_rows": (None, [_dp, _dp, _dp, C.POINTER(C.c_uint8), C.c_int64, _dp, C.c_int64, C.c_double,
                                     _dp]),
         "orc_count_rows": (None, [_dp, C.POINTER(C.c_uint8), C.c_int64, _dp, C.c_int64, C.POINTER(C.c_uint32)]),
+        "orc_biweight_flatten": (None, [_dp, _dp, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                        _dp]),
         "orc_single_event_scan": (C.c_int64, [_dp, _dp, _dp, C.c_int64, C.c_double, C.c_double, C.c_int, _dp, _dp,
                                               C.c_int, _dp, C.c_int, C.c_int, C.c_double, C.c_int64, _dp]),
         "orc_scan_bank": (C.c_int64, [_dp, _dp, _dp, C.c_int64, C.c_double, _dp, C.c_int64, C.c_int, _dp, _dp,
@@ -181,6 +183,18 @@ def transit_mask(time, period, epoch, duration, margin) -> np.ndarray:
     _load().orc_transit_mask(_p(t), t.shape[0], period, epoch, duration, margin,
                              m.ctypes.data_as(C.POINTER(C.c_uint8)))
     return m.astype(bool)
+
+
+def biweight_flatten(time, relative_flux, window: float, gap: float = 0.5, c: float = 5.0, iterations: int = 10,
+                     sorted_medians: bool = False) -> np.ndarray:
+    """Biweight detrend: the reference's GPU form (bisection medians,
+    kernels.rs:1051-1110) or, with sorted_medians, its CPU form
+    (curve.rs:202-250)."""
+    t, f = _f(time), _f(relative_flux)
+    out = np.empty_like(t)
+    _load().orc_biweight_flatten(_p(t), _p(f), t.shape[0], float(window), float(gap), float(c), int(iterations),
+                                 int(sorted_medians), _p(out))
+    return out
 
 
 def rescore_rows(time, v, w, excluded, rows, origin: float) -> np.ndarray:

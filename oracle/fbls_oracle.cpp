@@ -420,6 +420,79 @@ extern "C" int orc_fit_segment_noise(const double* time, const double* flux, con
     return 0;
 }
 
+// Biweight detrending, both of the reference's forms: the GPU kernel's
+// (kernels.rs:1051-1110: lower medians by bisection on the value range,
+// window_median :333-377) and the CPU function's (curve.rs:202-250: lower
+// medians by sorting). Windows [t - window/2, t + window/2] within
+// gap-separated segments; out = (1 + f) / location - 1.
+namespace {
+double bisect_median(const double* x, size_t a, size_t e, size_t k, double center, bool absolute) {
+    auto value = [&](size_t j) { return absolute ? std::fabs(x[j] - center) : x[j]; };
+    double vlo = INFINITY, vhi = -INFINITY;
+    for (size_t j = a; j < e; j++) {
+        vlo = std::fmin(vlo, value(j));
+        vhi = std::fmax(vhi, value(j));
+    }
+    for (int it = 0; it < 64 && vhi > vlo; it++) {
+        const double mid = 0.5 * (vlo + vhi);
+        if (mid <= vlo || mid >= vhi) break;
+        size_t below = 0;
+        for (size_t j = a; j < e; j++) below += value(j) < mid ? 1 : 0;
+        if (below <= k)
+            vlo = mid;
+        else
+            vhi = mid;
+    }
+    double best = INFINITY;
+    for (size_t j = a; j < e; j++)
+        if (value(j) >= vlo && value(j) < best) best = value(j);
+    return best;
+}
+}  // namespace
+
+extern "C" void orc_biweight_flatten(const double* time, const double* relative, int64_t n, double window, double gap,
+                                     double c, int iterations, int sorted_medians, double* out) {
+    std::vector<double> flux(n);
+    for (int64_t i = 0; i < n; i++) flux[i] = 1.0 + relative[i];
+    int64_t start = 0;
+    for (int64_t i = 1; i <= n; i++) {
+        if (i < n && !(time[i] - time[i - 1] > gap)) continue;
+        const double* t0 = time + start;
+        const double* t1 = time + i;
+        for (int64_t p = start; p < i; p++) {
+            const size_t a = (size_t)(std::lower_bound(t0, t1, time[p] - window / 2.0) - time);
+            const size_t e = (size_t)(std::upper_bound(t0, t1, time[p] + window / 2.0) - time);
+            const size_t k = (e - a - 1) / 2;
+            std::vector<double> vals(flux.begin() + a, flux.begin() + e);
+            double location = sorted_medians ? median_lower(vals) : bisect_median(flux.data(), a, e, k, 0.0, false);
+            for (int it = 0; it < iterations; it++) {
+                double med;
+                if (sorted_medians) {
+                    std::vector<double> dev(vals.size());
+                    for (size_t j = 0; j < vals.size(); j++) dev[j] = std::fabs(vals[j] - location);
+                    med = median_lower(dev);
+                } else {
+                    med = bisect_median(flux.data(), a, e, k, location, true);
+                }
+                const double scale = std::fmax(c * med, 1e-12);
+                double total = 0.0, acc = 0.0;
+                for (size_t j = a; j < e; j++) {
+                    const double v = flux[j];
+                    const double u = (v - location) / scale;
+                    if (std::fabs(u) < 1.0) {
+                        const double wt = (1.0 - u * u) * (1.0 - u * u);
+                        total += wt;
+                        acc += wt * v;
+                    }
+                }
+                if (total > 0.0) location = acc / total;
+            }
+            out[p] = flux[p] / location - 1.0;
+        }
+        start = i;
+    }
+}
+
 // transit_mask, curve.rs:572-585: count of masked observations and the mask.
 extern "C" int64_t orc_transit_mask(const double* time, int64_t n, double period, double epoch, double duration,
                                     double margin, uint8_t* mask) {
