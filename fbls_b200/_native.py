@@ -135,6 +135,17 @@ class EvidenceRow(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class PrepConfig(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("bin_minutes", "window_min", "window_factor", "window_max", "clip_sigma",
+                                           "edge_trim")]
+
+
+class FamilyOut(C.Structure):
+    _fields_ = [("time", C.POINTER(C.c_double)), ("flux", C.POINTER(C.c_double)), ("sigma", C.POINTER(C.c_double)),
+                ("n", C.c_uint32), ("window_days", C.c_double), ("clipped", C.c_uint32),
+                ("indices", C.POINTER(C.c_uint32)), ("n_indices", C.c_uint32)]
+
+
 class EventStats(C.Structure):
     _fields_ = [("templates_scanned", C.c_uint64), ("threshold_survivors", C.c_uint64), ("overflow", C.c_int)]
 
@@ -203,6 +214,15 @@ SIGNATURES = {
     "fbls_coarse_map_batch": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, C.c_uint32]),
     "fbls_coarse_features": (C.c_int, [C.c_void_p, C.POINTER(MapJob), C.c_uint32, c_uint32_p, C.c_uint32,
                                        C.c_uint32, C.POINTER(C.c_float)]),
+    "fbls_fit_segment_noise": (C.c_int, [c_double_p, c_double_p, c_double_p, C.POINTER(C.c_int64), C.c_uint32,
+                                         C.c_double, C.c_double, c_uint32_p, c_double_p, c_double_p, c_double_p,
+                                         C.POINTER(C.c_int64), c_double_p, C.c_char_p, C.c_uint32]),
+    "fbls_segment_edges": (C.c_int, [c_double_p, C.c_uint32, C.c_double, c_double_p]),
+    "fbls_detrending_windows": (C.c_int, [c_double_p, C.c_uint32, C.c_double, C.c_double, C.c_double, c_double_p,
+                                          c_uint32_p, c_uint32_p]),
+    "fbls_prepare_families": (C.c_int, [C.c_void_p, c_double_p, c_double_p, c_double_p, C.POINTER(C.c_int64),
+                                        C.c_uint32, c_double_p, C.c_uint32, C.POINTER(PrepConfig),
+                                        C.POINTER(FamilyOut), c_uint32_p]),
     "fbls_biweight_flatten": (C.c_int, [C.c_void_p, c_double_p, c_double_p, C.c_uint32, C.c_double, C.c_double,
                                         C.c_double, C.c_uint32, c_double_p]),
     "fbls_single_event_search": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, c_double_p, C.c_uint32,

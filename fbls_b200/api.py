@@ -127,6 +127,82 @@ def family_state(time, flux, sigma, durations_days: Sequence[float], correlated:
                        d.copy(), rho[:len(d)].copy(), float(scal[3]), int(scal[4]))
 
 
+def _opt_f64(a):
+    return None if a is None else _f64(a)
+
+
+def _opt_i64(a):
+    return None if a is None else np.ascontiguousarray(np.asarray(a, dtype=np.int64))
+
+
+@dataclasses.dataclass
+class NoiseModel:
+    """DiagonalNoise (curve.rs:89-198): relative times, deficit, variance,
+    group per observation, origin, inflation, segments."""
+    time: np.ndarray
+    deficit: np.ndarray
+    variance: np.ndarray
+    group: np.ndarray
+    origin: float
+    inflation: float
+    segments: int
+
+
+def fit_segment_noise(time, flux, err=None, group=None, bin_minutes: float = 0.0, gap_days: float = 0.75) -> NoiseModel:
+    """The diagonal noise model of raw mission flux (host only)."""
+    lib = N.load()
+    t, f, e, g = _f64(time), _f64(flux), _opt_f64(err), _opt_i64(group)
+    n_in = t.shape[0]
+    to, do, vo = (np.empty(max(n_in, 1)) for _ in range(3))
+    go = np.empty(max(n_in, 1), dtype=np.int64)
+    scal = np.empty(3)
+    n_out = C.c_uint32(0)
+    msg = C.create_string_buffer(256)
+    rc = lib.fbls_fit_segment_noise(_dptr(t), _dptr(f), None if e is None else _dptr(e),
+                                    None if g is None else g.ctypes.data_as(C.POINTER(C.c_int64)), n_in,
+                                    float(bin_minutes), float(gap_days), C.byref(n_out), _dptr(to), _dptr(do),
+                                    _dptr(vo), go.ctypes.data_as(C.POINTER(C.c_int64)), _dptr(scal), msg, 256)
+    if rc:
+        raise FblsError(rc, msg.value.decode())
+    n = n_out.value
+    return NoiseModel(to[:n].copy(), do[:n].copy(), vo[:n].copy(), go[:n].copy(), float(scal[0]), float(scal[1]),
+                      int(scal[2]))
+
+
+def segment_edges(time, gap: float) -> np.ndarray:
+    """Distance to the nearer edge of each gap-separated segment (curve.rs:332-345)."""
+    t = _f64(time)
+    out = np.empty_like(t)
+    rc = N.load().fbls_segment_edges(_dptr(t), t.shape[0], float(gap), _dptr(out))
+    if rc:
+        raise FblsError(rc, "segment_edges")
+    return out
+
+
+def detrending_windows(durations, minimum: float, factor: float, maximum: float) -> List[Tuple[float, List[int]]]:
+    """(window, duration indices) sorted by window (curve.rs:349-370)."""
+    d = _f64(durations)
+    w = np.empty(max(len(d), 1))
+    fam = np.empty(max(len(d), 1), dtype=np.uint32)
+    k = C.c_uint32(0)
+    rc = N.load().fbls_detrending_windows(_dptr(d), len(d), float(minimum), float(factor), float(maximum), _dptr(w),
+                                          fam.ctypes.data_as(N.c_uint32_p), C.byref(k))
+    if rc:
+        raise FblsError(rc, "detrending_windows")
+    return [(float(w[j]), [i for i in range(len(d)) if fam[i] == j]) for j in range(k.value)]
+
+
+@dataclasses.dataclass
+class PreparedCurve:
+    """One detrended curve of prepare_families (curve.rs:384-425)."""
+    time: np.ndarray      # absolute
+    flux: np.ndarray      # detrended relative flux
+    sigma: np.ndarray
+    window_days: float
+    clipped: int
+    indices: np.ndarray   # durations searched on this curve
+
+
 def prepared_family(time, flux, flux_err, cfg: SearchConfig) -> FamilyState:
     """search_prepared's single family holding every duration (pipeline.rs:41-68)."""
     return family_state(time, flux, flux_err, cfg.durations_days(), cfg.correlated_noise)
@@ -263,6 +339,34 @@ class Gpu:
             j.out = o.ctypes.data_as(C.POINTER(C.c_float))
         self._check(self.lib.fbls_coarse_map_batch(self.ctx, jobs, count, int(workers)))
         return outs
+
+    def prepare_families(self, time, flux, err, group, cfg: SearchConfig) -> List[PreparedCurve]:
+        """prepare_families (curve.rs:384-425): raw flux to one detrended
+        curve per detrending window of cfg's durations (raw mode,
+        pipeline.rs:27-37); the biweight detrend runs on the GPU."""
+        t, f, e, g = _f64(time), _f64(flux), _opt_f64(err), _opt_i64(group)
+        n = t.shape[0]
+        d = _f64(cfg.durations_days())
+        pc = N.PrepConfig(cfg.bin_minutes, cfg.window_days, cfg.window_factor, cfg.window_max_days, cfg.clip_sigma,
+                          cfg.edge_trim_windows)
+        outs = (N.FamilyOut * max(len(d), 1))()
+        bufs = []
+        for k in range(len(d)):
+            arr = [np.empty(max(n, 1)) for _ in range(3)] + [np.empty(max(len(d), 1), dtype=np.uint32)]
+            bufs.append(arr)
+            outs[k].time, outs[k].flux, outs[k].sigma = (_dptr(a) for a in arr[:3])
+            outs[k].indices = arr[3].ctypes.data_as(N.c_uint32_p)
+        nf = C.c_uint32(0)
+        self._check(self.lib.fbls_prepare_families(self.ctx, _dptr(t), _dptr(f), None if e is None else _dptr(e),
+                                                   None if g is None else g.ctypes.data_as(C.POINTER(C.c_int64)), n,
+                                                   _dptr(d), len(d), C.byref(pc), outs, C.byref(nf)))
+        res = []
+        for k in range(nf.value):
+            o, arr = outs[k], bufs[k]
+            m = o.n
+            res.append(PreparedCurve(arr[0][:m].copy(), arr[1][:m].copy(), arr[2][:m].copy(), float(o.window_days),
+                                     int(o.clipped), arr[3][:o.n_indices].copy()))
+        return res
 
     def biweight_flatten(self, time, relative_flux, window: float, gap: float = 0.5, c: float = 5.0,
                          iterations: int = 10) -> np.ndarray:

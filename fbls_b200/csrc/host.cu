@@ -2201,6 +2201,107 @@ int fbls_biweight_flatten(fbls_ctx* ctx, const double* time, const double* relat
     return FBLS_OK;
 }
 
+// fit_segment_noise (src/prep/curve.rs:89-198) on the host: the diagonal
+// noise model of raw flux. Outputs hold up to n_in values.
+int fbls_fit_segment_noise(const double* time, const double* flux, const double* err, const int64_t* group,
+                           uint32_t n_in, double bin_minutes, double gap_days, uint32_t* n_out, double* time_out,
+                           double* deficit_out, double* variance_out, int64_t* group_out, double* scalars_out,
+                           char* error, uint32_t error_len) {
+    auto fail_msg = [&](int status, const std::string& message) {
+        if (error && error_len) {
+            std::strncpy(error, message.c_str(), error_len - 1);
+            error[error_len - 1] = '\0';
+        }
+        return status;
+    };
+    if (!time || !flux || !n_out || !time_out || !deficit_out || !variance_out || !scalars_out)
+        return fail_msg(FBLS_ERR_ARGUMENT, "null argument");
+    DiagonalNoise d;
+    std::string message;
+    if (fit_segment_noise(time, flux, err, group, n_in, bin_minutes, gap_days, d, message))
+        return fail_msg(FBLS_ERR_DATA, message);
+    const size_t n = d.time.size();
+    *n_out = (uint32_t)n;
+    std::memcpy(time_out, d.time.data(), n * sizeof(double));
+    std::memcpy(deficit_out, d.deficit.data(), n * sizeof(double));
+    std::memcpy(variance_out, d.variance.data(), n * sizeof(double));
+    if (group_out) std::memcpy(group_out, d.group.data(), n * sizeof(int64_t));
+    scalars_out[0] = d.origin;
+    scalars_out[1] = d.inflation;
+    scalars_out[2] = (double)d.segments;
+    return FBLS_OK;
+}
+
+// segment_edges and detrending_windows (curve.rs:332-370), host only.
+int fbls_segment_edges(const double* time, uint32_t n, double gap, double* out) {
+    if (n && (!time || !out)) return FBLS_ERR_ARGUMENT;
+    const std::vector<double> e = segment_edges(std::vector<double>(time, time + n), gap);
+    std::memcpy(out, e.data(), (size_t)n * sizeof(double));
+    return FBLS_OK;
+}
+
+int fbls_detrending_windows(const double* durations, uint32_t nd, double minimum, double factor, double maximum,
+                            double* windows_out, uint32_t* family_out, uint32_t* n_windows) {
+    if (!n_windows || (nd && (!durations || !windows_out || !family_out))) return FBLS_ERR_ARGUMENT;
+    const auto w = detrending_windows(durations, nd, minimum, factor, maximum);
+    for (size_t k = 0; k < w.size(); k++) {
+        windows_out[k] = w[k].first;
+        for (uint32_t i : w[k].second) family_out[i] = (uint32_t)k;
+    }
+    *n_windows = (uint32_t)w.size();
+    return FBLS_OK;
+}
+
+// prepare_families (src/prep/curve.rs:384-425): the noise model of the raw
+// flux (groups, bins of cfg->bin_minutes, gap 0.75 d), then per detrending
+// window the biweight detrend on the GPU (gap 0.5 d, c 5, 10 iterations) and
+// the curve kept where the detrended flux is finite, at most clip_sigma
+// robust scales above zero and at least edge_trim windows from a segment
+// edge.
+int fbls_prepare_families(fbls_ctx* ctx, const double* time, const double* flux, const double* err,
+                          const int64_t* group, uint32_t n, const double* durations, uint32_t nd,
+                          const fbls_prep_config* cfg, fbls_family_out* out, uint32_t* n_families) {
+    if (!ctx || !time || !flux || !durations || !cfg || !out || !n_families)
+        return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    *n_families = 0;
+    DiagonalNoise d;
+    std::string message;
+    if (fit_segment_noise(time, flux, err, group, n, cfg->bin_minutes, 0.75, d, message))
+        return fail(ctx, FBLS_ERR_DATA, message);
+    const size_t m = d.time.size();
+    std::vector<double> sigma(m), relative(m), flat(m);
+    for (size_t i = 0; i < m; i++) {
+        sigma[i] = std::sqrt(d.variance[i]);
+        relative[i] = -d.deficit[i];
+    }
+    const std::vector<double> edge = segment_edges(d.time, 0.5);
+    const auto windows = detrending_windows(durations, nd, cfg->window_min, cfg->window_factor, cfg->window_max);
+    for (size_t k = 0; k < windows.size(); k++) {
+        const double window = windows[k].first;
+        const int rc = fbls_biweight_flatten(ctx, d.time.data(), relative.data(), (uint32_t)m, window, 0.5, 5.0, 10,
+                                             flat.data());
+        if (rc) return rc;
+        const double scale = robust_scale(flat);
+        fbls_family_out& f = out[k];
+        if (!f.time || !f.flux || !f.sigma || !f.indices) return fail(ctx, FBLS_ERR_ARGUMENT, "null family buffer");
+        uint32_t kept = 0;
+        for (size_t i = 0; i < m; i++)
+            if (std::isfinite(flat[i]) && flat[i] <= cfg->clip_sigma * scale && edge[i] >= cfg->edge_trim * window) {
+                f.time[kept] = d.time[i] + d.origin;
+                f.flux[kept] = flat[i];
+                f.sigma[kept] = sigma[i];
+                kept++;
+            }
+        f.n = kept;
+        f.window_days = window;
+        f.clipped = (uint32_t)(m - kept);
+        f.n_indices = (uint32_t)windows[k].second.size();
+        std::memcpy(f.indices, windows[k].second.data(), windows[k].second.size() * sizeof(uint32_t));
+    }
+    *n_families = (uint32_t)windows.size();
+    return FBLS_OK;
+}
+
 // Peak-selection rescoring (src/select/peaks.rs:148-252 calls these): the
 // rows' box sums over an uploaded family's observations outside `excluded`,
 // and their in-transit counts over a time vector. Host arrays in and out;

@@ -2,7 +2,9 @@
 // path): the diagonal noise model, the precision-weighted fields and the
 // correlated-noise factors. C++ restatement of the reference's host code:
 //   family_state              src/prep/curve.rs:541-569
-//   fit_segment_noise (bin 0) src/prep/curve.rs:89-198
+//   fit_segment_noise         src/prep/curve.rs:89-198 (prepared mode: bin 0,
+//                             one group; raw mode: fit_segment_noise below)
+//   segment_edges, detrending_windows  src/prep/curve.rs:332-370
 //   prepare_ready             src/prep/curve.rs:427-450
 //   correlated_noise_factors  src/prep/curve.rs:456-539
 //   median_lower, mad_scale   src/prep/stats.rs:4-18
@@ -203,6 +205,166 @@ int prepare_family(const double* time, const double* flux, const double* sigma, 
     }
     return 0;
 }
+
+int fit_segment_noise(const double* time, const double* flux, const double* err, const int64_t* group, size_t n_in,
+                      double bin_minutes, double gap_days, DiagonalNoise& out, std::string& error) {
+    auto e_in = [&](size_t i) { return err ? err[i] : 1.0; };
+    auto g_in = [&](size_t i) { return group ? group[i] : (int64_t)0; };
+    std::vector<size_t> keep;
+    for (size_t i = 0; i < n_in; i++)
+        if (std::isfinite(time[i]) && std::isfinite(flux[i]) && std::isfinite(e_in(i)) && e_in(i) > 0.0)
+            keep.push_back(i);
+    std::stable_sort(keep.begin(), keep.end(), [&](size_t a, size_t b) { return time[a] < time[b]; });
+    size_t n = keep.size();
+    std::vector<double> t(n), f(n), e(n);
+    std::vector<int64_t> sec(n);
+    for (size_t i = 0; i < n; i++) {
+        t[i] = time[keep[i]];
+        f[i] = flux[keep[i]];
+        e[i] = e_in(keep[i]);
+        sec[i] = g_in(keep[i]);
+    }
+    if (n < 6) {
+        error = "insufficient usable observations";
+        return 1;
+    }
+    std::vector<int64_t> labels = sec;
+    std::sort(labels.begin(), labels.end());
+    labels.erase(std::unique(labels.begin(), labels.end()), labels.end());
+    for (int64_t label : labels) {
+        std::vector<double> vals;
+        for (size_t i = 0; i < n; i++)
+            if (sec[i] == label) vals.push_back(f[i]);
+        const double m = median_lower(vals);
+        if (!(m > 0.0)) {
+            error = "mission flux must have a positive median";
+            return 1;
+        }
+        for (size_t i = 0; i < n; i++)
+            if (sec[i] == label) {
+                f[i] = f[i] / m - 1.0;
+                e[i] /= m;
+            }
+    }
+    const double origin = t[0];
+    for (size_t i = 0; i < n; i++) t[i] -= origin;
+    if (bin_minutes > 0.0) {
+        // Inverse-variance means per (bin, group), keys in sorted order.
+        const double width = bin_minutes / 1440.0;
+        std::vector<std::pair<int64_t, int64_t>> keys(n);
+        for (size_t i = 0; i < n; i++) keys[i] = {(int64_t)std::floor(t[i] / width), sec[i]};
+        std::vector<std::pair<int64_t, int64_t>> unique = keys;
+        std::sort(unique.begin(), unique.end());
+        unique.erase(std::unique(unique.begin(), unique.end()), unique.end());
+        const size_t m = unique.size();
+        std::vector<double> den(m, 0.0), st(m, 0.0), sf(m, 0.0);
+        for (size_t i = 0; i < n; i++) {
+            const size_t k = (size_t)(std::lower_bound(unique.begin(), unique.end(), keys[i]) - unique.begin());
+            const double w = 1.0 / (e[i] * e[i]);
+            den[k] += w;
+            st[k] += t[i] * w;
+            sf[k] += f[i] * w;
+        }
+        std::vector<double> tb(m), fb(m), eb(m);
+        std::vector<int64_t> sb(m);
+        for (size_t k = 0; k < m; k++) {
+            tb[k] = st[k] / den[k];
+            fb[k] = sf[k] / den[k];
+            eb[k] = 1.0 / std::sqrt(den[k]);
+            sb[k] = unique[k].second;
+        }
+        std::vector<size_t> order(m);
+        for (size_t k = 0; k < m; k++) order[k] = k;
+        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return tb[a] < tb[b]; });
+        t.resize(m);
+        f.resize(m);
+        e.resize(m);
+        sec.resize(m);
+        for (size_t k = 0; k < m; k++) {
+            t[k] = tb[order[k]];
+            f[k] = fb[order[k]];
+            e[k] = eb[order[k]];
+            sec[k] = sb[order[k]];
+        }
+        n = m;
+    }
+    std::vector<double> standardized, deltas;
+    for (size_t i = 1; i < n; i++)
+        if (t[i] - t[i - 1] < gap_days && sec[i] == sec[i - 1]) {
+            const double d = f[i] - f[i - 1];
+            deltas.push_back(d);
+            standardized.push_back(d / std::sqrt(e[i] * e[i] + e[i - 1] * e[i - 1]));
+        }
+    if (deltas.empty()) {
+        error = "no adjacent observations available for noise estimation";
+        return 1;
+    }
+    const double inflation = fmax_rust(mad_scale(standardized), 1.0);
+    out.variance.resize(n);
+    if (err) {
+        for (size_t i = 0; i < n; i++) {
+            const double x = e[i] * inflation;
+            out.variance[i] = x * x;
+        }
+    } else {
+        const double m = median_lower(deltas);
+        std::vector<double> dev(deltas.size());
+        for (size_t i = 0; i < deltas.size(); i++) dev[i] = std::fabs(deltas[i] - m);
+        const double white = fmax_rust(1.4826 / std::sqrt(2.0) * median_lower(dev), 1e-12);
+        for (size_t i = 0; i < n; i++) out.variance[i] = white * white;
+    }
+    size_t segments = 1;
+    for (size_t i = 1; i < n; i++)
+        if (t[i] - t[i - 1] > gap_days || sec[i] != sec[i - 1]) segments++;
+    out.time = t;
+    out.deficit.resize(n);
+    for (size_t i = 0; i < n; i++) out.deficit[i] = -f[i];
+    out.group = sec;
+    out.origin = origin;
+    out.inflation = inflation;
+    out.segments = segments;
+    return 0;
+}
+
+std::vector<double> segment_edges(const std::vector<double>& time, double gap) {
+    const size_t n = time.size();
+    std::vector<double> out(n, 0.0);
+    size_t start = 0;
+    for (size_t i = 1; i <= n; i++)
+        if (i == n || time[i] - time[i - 1] > gap) {
+            for (size_t j = start; j < i; j++) {
+                const double a = time[j] - time[start], b = time[i - 1] - time[j];
+                out[j] = std::isnan(a) ? b : (std::isnan(b) ? a : (a < b ? a : b));
+            }
+            start = i;
+        }
+    return out;
+}
+
+std::vector<std::pair<double, std::vector<uint32_t>>> detrending_windows(const double* durations, size_t nd,
+                                                                          double minimum, double factor,
+                                                                          double maximum) {
+    std::vector<double> windows(nd);
+    for (size_t i = 0; i < nd; i++) {
+        double x = factor * durations[i];
+        if (x < minimum) x = minimum;  // f64::clamp
+        if (x > maximum) x = maximum;
+        windows[i] = std::round(x * 1e6) / 1e6;  // f64::round: halves away from zero
+    }
+    std::vector<double> uniq = windows;
+    std::sort(uniq.begin(), uniq.end());
+    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+    std::vector<std::pair<double, std::vector<uint32_t>>> out;
+    for (double w : uniq) {
+        std::vector<uint32_t> idx;
+        for (size_t i = 0; i < nd; i++)
+            if (windows[i] == w) idx.push_back((uint32_t)i);
+        out.push_back({w, idx});
+    }
+    return out;
+}
+
+double robust_scale(const std::vector<double>& values) { return mad_scale(values); }
 
 int64_t period_grid(double minimum, double maximum, double baseline, double minimum_duration, double oversample,
                     double* out, int64_t capacity) {

@@ -320,6 +320,64 @@ int fbls_coarse_features(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, cons
 int fbls_biweight_flatten(fbls_ctx* ctx, const double* time, const double* relative_flux, uint32_t n, double window,
                           double gap, double c, uint32_t iterations, double* out);
 
+/* fit_segment_noise (src/prep/curve.rs:89-198), host only: the diagonal noise
+ * model of raw mission flux. Usable observations (finite, err > 0) in time
+ * order; each group (sector label) divided by its lower median (flux / m - 1,
+ * err / m); times relative to the first; with bin_minutes > 0,
+ * inverse-variance means per (floor(t / width), group); the adjacent
+ * differences within gap_days and one group give the error inflation (with
+ * `err`) or a white level (err null). err and group may be null. Outputs hold
+ * up to n_in values; scalars_out: origin, inflation, segments. Returns 0,
+ * FBLS_ERR_ARGUMENT, or FBLS_ERR_DATA with the reference's message. */
+int fbls_fit_segment_noise(const double* time, const double* flux, const double* err, const int64_t* group,
+                           uint32_t n_in, double bin_minutes, double gap_days, uint32_t* n_out, double* time_out,
+                           double* deficit_out, double* variance_out, int64_t* group_out, double* scalars_out,
+                           char* error, uint32_t error_len);
+
+/* segment_edges (curve.rs:332-345): each observation's distance to the
+ * nearer edge of its segment (segments split where the time step exceeds
+ * gap). detrending_windows (curve.rs:349-370): the distinct windows
+ * round(clamp(factor x D, minimum, maximum) x 1e6) / 1e6 in increasing order
+ * (windows_out, room for nd) and each duration's window index (family_out).
+ * Host only; return 0 or FBLS_ERR_ARGUMENT. */
+int fbls_segment_edges(const double* time, uint32_t n, double gap, double* out);
+int fbls_detrending_windows(const double* durations, uint32_t nd, double minimum, double factor, double maximum,
+                            double* windows_out, uint32_t* family_out, uint32_t* n_windows);
+
+/* PrepConfig (src/prep/curve.rs:372-379, from SearchConfig, src/main.rs:134-143). */
+typedef struct {
+    double bin_minutes;
+    double window_min;     /* days */
+    double window_factor;  /* window = clamp(factor x duration, min, max) */
+    double window_max;     /* days */
+    double clip_sigma;     /* positive outliers above clip_sigma robust scales are dropped */
+    double edge_trim;      /* observations within edge_trim windows of a segment edge are dropped */
+} fbls_prep_config;
+
+/* One detrended curve of prepare_families: caller-owned arrays (time, flux,
+ * sigma: room for n observations; indices: room for nd), filled with the kept
+ * observations (absolute times), the window, the count dropped and the
+ * indices of the durations searched on it. */
+typedef struct {
+    double* time;
+    double* flux;
+    double* sigma;
+    uint32_t n;
+    double window_days;
+    uint32_t clipped;
+    uint32_t* indices;
+    uint32_t n_indices;
+} fbls_family_out;
+
+/* prepare_families (src/prep/curve.rs:384-425): raw flux to one detrended
+ * curve per detrending window (durations grouped by clamp(window_factor x D,
+ * window_min, window_max) rounded to 1e-6 d), the biweight detrend on the
+ * GPU. `out` has room for nd families; *n_families is the number filled, in
+ * increasing window. */
+int fbls_prepare_families(fbls_ctx* ctx, const double* time, const double* flux, const double* err,
+                          const int64_t* group, uint32_t n, const double* durations, uint32_t nd,
+                          const fbls_prep_config* cfg, fbls_family_out* out, uint32_t* n_families);
+
 /* EventStats, src/search/events.rs:10-15. */
 typedef struct {
     uint64_t templates_scanned;   /* nb x nd x shapes */

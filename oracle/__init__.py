@@ -197,6 +197,112 @@ def biweight_flatten(time, relative_flux, window: float, gap: float = 0.5, c: fl
     return out
 
 
+# -- raw-mode preparation (curve.rs:89-198, :332-425), restated in Python ------
+
+def _median_lower_py(v) -> float:
+    v = np.sort(np.asarray(v, dtype=np.float64)[np.isfinite(v)])
+    return float(v[(v.shape[0] - 1) // 2]) if v.shape[0] else math.nan
+
+
+def _mad_scale_py(v) -> float:
+    v = np.asarray(v, dtype=np.float64)
+    m = _median_lower_py(v)
+    return 1.4826 * _median_lower_py(np.abs(v - m))
+
+
+def _round_half_away(y: float) -> float:
+    r = math.trunc(y)
+    return r + math.copysign(1.0, y) if abs(y - r) >= 0.5 else float(r)
+
+
+def fit_segment_noise_raw(time, flux, err=None, group=None, bin_minutes: float = 0.0, gap_days: float = 0.75):
+    """fit_segment_noise (curve.rs:89-198) with groups and bins: (time,
+    deficit, variance, group, origin, inflation, segments)."""
+    t_in, f_in = _f(time), _f(flux)
+    n = t_in.shape[0]
+    e_in = np.ones(n) if err is None else _f(err)
+    g_in = np.zeros(n, dtype=np.int64) if group is None else np.asarray(group, dtype=np.int64)
+    keep = np.flatnonzero(np.isfinite(t_in) & np.isfinite(f_in) & np.isfinite(e_in) & (e_in > 0.0))
+    keep = keep[np.argsort(t_in[keep], kind="stable")]
+    t, f, e, sec = t_in[keep].copy(), f_in[keep].copy(), e_in[keep].copy(), g_in[keep].copy()
+    if t.shape[0] < 6:
+        raise ValueError("insufficient usable observations")
+    for label in np.unique(sec):
+        idx = np.flatnonzero(sec == label)
+        m = _median_lower_py(f[idx])
+        if not m > 0.0:
+            raise ValueError("mission flux must have a positive median")
+        f[idx] = f[idx] / m - 1.0
+        e[idx] = e[idx] / m
+    origin = float(t[0])
+    t = t - origin
+    if bin_minutes > 0.0:
+        width = bin_minutes / 1440.0
+        keys = list(zip(np.floor(t / width).astype(np.int64).tolist(), sec.tolist()))
+        uniq = sorted(set(keys))
+        at = {k: i for i, k in enumerate(uniq)}
+        m = len(uniq)
+        den, st, sf = [0.0] * m, [0.0] * m, [0.0] * m
+        for i, k in enumerate(keys):  # in observation order, as the reference
+            j = at[k]
+            w = 1.0 / (e[i] * e[i])
+            den[j] += w
+            st[j] += t[i] * w
+            sf[j] += f[i] * w
+        den, st, sf = np.array(den), np.array(st), np.array(sf)
+        tb, fb, eb = st / den, sf / den, 1.0 / np.sqrt(den)
+        sb = np.array([k[1] for k in uniq], dtype=np.int64)
+        o = np.argsort(tb, kind="stable")
+        t, f, e, sec = tb[o], fb[o], eb[o], sb[o]
+    adj = (np.diff(t) < gap_days) & (sec[1:] == sec[:-1])
+    deltas = (f[1:] - f[:-1])[adj]
+    if deltas.shape[0] == 0:
+        raise ValueError("no adjacent observations available for noise estimation")
+    standardized = deltas / np.sqrt(e[1:][adj] * e[1:][adj] + e[:-1][adj] * e[:-1][adj])
+    ms = _mad_scale_py(standardized)
+    inflation = ms if ms > 1.0 else 1.0
+    if err is not None:
+        variance = (e * inflation) ** 2
+    else:
+        md = _median_lower_py(deltas)
+        white = max(1.4826 / math.sqrt(2.0) * _median_lower_py(np.abs(deltas - md)), 1e-12)
+        variance = np.full(t.shape[0], white * white)
+    segments = 1 + int(np.count_nonzero((np.diff(t) > gap_days) | (sec[1:] != sec[:-1])))
+    return t, -f, variance, sec, origin, inflation, segments
+
+
+def segment_edges_py(t, gap: float) -> np.ndarray:
+    out = np.zeros(len(t))
+    start = 0
+    for i in range(1, len(t) + 1):
+        if i == len(t) or t[i] - t[i - 1] > gap:
+            for j in range(start, i):
+                out[j] = min(t[j] - t[start], t[i - 1] - t[j])
+            start = i
+    return out
+
+
+def prepare_families(time, flux, err, group, durations, cfg):
+    """prepare_families (curve.rs:384-425) on the oracle: [(time absolute,
+    flux, sigma, window, clipped, indices)] per detrending window."""
+    t, deficit, variance, _, origin, _, _ = fit_segment_noise_raw(time, flux, err, group, cfg.bin_minutes, 0.75)
+    sigma = np.sqrt(variance)
+    edge = segment_edges_py(t, 0.5)
+    relative = -deficit
+    win = []
+    for d in durations:
+        x = min(max(cfg.window_factor * d, cfg.window_days), cfg.window_max_days)
+        win.append(_round_half_away(x * 1e6) / 1e6)
+    out = []
+    for w in sorted(set(win)):
+        flat = biweight_flatten(t, relative, w, 0.5, 5.0, 10)
+        scale = _mad_scale_py(flat)
+        keep = np.isfinite(flat) & (flat <= cfg.clip_sigma * scale) & (edge >= cfg.edge_trim_windows * w)
+        out.append((t[keep] + origin, flat[keep], sigma[keep], w, int(flat.shape[0] - keep.sum()),
+                    [i for i, x in enumerate(win) if x == w]))
+    return out
+
+
 def rescore_rows(time, v, w, excluded, rows, origin: float) -> np.ndarray:
     """(R, 3) box sums a, hp, norm per row (kernels.rs:936-990)."""
     t, vv, ww = _f(time), _f(v), _f(w)

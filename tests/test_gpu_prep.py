@@ -30,3 +30,31 @@ def test_biweight_on_a_sector(gpu):
     got = gpu.biweight_flatten(t, c.flux, 0.75)
     want = oracle.biweight_flatten(t, c.flux, 0.75)
     assert np.array_equal(got, want)
+
+
+def test_biweight_removes_a_smooth_trend(gpu):
+    # the reference's known-answer test, curve.rs:624-634
+    t = np.arange(2000) * 0.01
+    flat = gpu.biweight_flatten(t, 0.01 * np.sin(t / 5.0), 0.5, 0.5, 5.0, 10)
+    assert np.abs(flat[100:1900]).max() < 5e-5
+
+
+def test_prepare_families_matches_the_oracle(gpu):
+    """Raw flux of two sectors with their own levels, NaNs and a sector label
+    each, binned to 30 minutes: every detrended family equal to the oracle's."""
+    from fbls_b200.config import SearchConfig
+    rng = np.random.default_rng(2)
+    t = synth.sector_times(2, 600.0)
+    sec = np.floor((t - t[0]) / synth.SECTOR_DAYS).astype(np.int64) + 17
+    level = 1.2e4 * (1.0 + 0.05 * (sec - 17))
+    flux = level * (1.0 + 2e-3 * np.sin(t / 1.7) + rng.normal(0.0, 8e-4, t.shape[0]))
+    flux[rng.integers(0, t.shape[0], 40)] *= 1.02  # positive outliers to clip
+    err = np.full(t.shape[0], 8e-4) * level
+    cfg = SearchConfig(bin_minutes=30.0, durations_hours=[0.5, 1.0, 2.0, 6.0, 14.0])
+    got = gpu.prepare_families(t, flux, err, sec, cfg)
+    want = oracle.prepare_families(t, flux, err, sec, cfg.durations_days(), cfg)
+    assert len(got) == len(want) >= 3
+    for g, w in zip(got, want):
+        assert np.array_equal(g.time, w[0]) and np.array_equal(g.flux, w[1]) and np.array_equal(g.sigma, w[2])
+        assert (g.window_days, g.clipped, g.indices.tolist()) == (w[3], w[4], w[5])
+    assert any(g.clipped > 0 for g in got)
