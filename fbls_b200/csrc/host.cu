@@ -256,10 +256,14 @@ struct Pass {
 };
 
 // Runs f(i) for i in [0, n) on up to 16 host threads, the caller's included.
+// Fewer than PARALLEL_MIN items run on the caller's thread: a single star's
+// few passes plan in milliseconds, and starting threads for them only adds
+// the risk of waiting on a descheduled one when the host's cores are busy.
+constexpr size_t PARALLEL_MIN = 32;
 template <typename F>
 void parallel_for(size_t n, F f) {
     const size_t threads = std::min<size_t>(n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
-    if (threads <= 1) {
+    if (threads <= 1 || n < PARALLEL_MIN) {
         for (size_t i = 0; i < n; i++) f(i);
         return;
     }

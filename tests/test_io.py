@@ -1,0 +1,89 @@
+"""Input formats (src/io/npz.rs, src/io/fits.rs, read_inputs src/main.rs:50-132)
+on the CPU: NPZ members of every supported dtype and byte order, the
+reference's FITS binary-table and TAN-projection known-answer tests, and
+the grouping of several inputs."""
+import math
+import struct
+
+import numpy as np
+import pytest
+
+from fbls_b200 import io
+
+BLOCK = io.BLOCK
+
+
+def test_npz_dtypes_and_byte_orders(tmp_path):
+    arrays = {
+        "f8": np.array([1.5, -2.25, math.pi]), "f4": np.array([0.5, 3.25], dtype=np.float32),
+        "i8": np.array([[1, -2], [3, 4]], dtype=np.int64), "i4": np.array([7, -9], dtype=np.int32),
+        "i2": np.array([-3], dtype=np.int16), "u1": np.array([200, 1], dtype=np.uint8),
+        "b1": np.array([True, False, True]), "be": np.array([1.25, -8.5], dtype=">f8"),
+        "scalar": np.float64(17.0),
+    }
+    path = tmp_path / "a.npz"
+    np.savez(path, **arrays)
+    got = io.read_npz(str(path))
+    for k, v in arrays.items():
+        a = np.asarray(v)
+        assert got[k].shape == a.shape
+        assert np.array_equal(got[k].data, a.astype(np.float64).reshape(-1))
+    bad = tmp_path / "b.npz"
+    np.savez(bad, c=np.array([1 + 2j]))
+    with pytest.raises(ValueError, match="unsupported NPY dtype"):
+        io.read_npz(str(bad))
+
+
+def _card(key, value):
+    s = f"{key:<8}= {value:>20}"[:80]
+    return s.ljust(80).encode()
+
+
+def _pad(b, fill):
+    return b + fill * ((-len(b)) % BLOCK)
+
+
+def test_fits_binary_table_round_trip(tmp_path):
+    # fits.rs:354-402
+    primary = b"".join(_card(k, v) for k, v in [("SIMPLE", "T"), ("BITPIX", "8"), ("NAXIS", "0")])
+    primary = _pad(primary + b"END".ljust(80), b" ")
+    ext = b"".join(_card(k, v) for k, v in [
+        ("XTENSION", "'BINTABLE'"), ("BITPIX", "8"), ("NAXIS", "2"), ("NAXIS1", "16"), ("NAXIS2", "3"),
+        ("PCOUNT", "0"), ("GCOUNT", "1"), ("TFIELDS", "3"), ("TTYPE1", "'TIME'"), ("TFORM1", "'D'"),
+        ("TTYPE2", "'FLUX'"), ("TFORM2", "'E'"), ("TTYPE3", "'QUALITY'"), ("TFORM3", "'J'"),
+        ("EXTNAME", "'LIGHTCURVE'")])
+    ext = _pad(ext + b"END".ljust(80), b" ")
+    data = b"".join(struct.pack(">d", 1.5 + r) + struct.pack(">f", 2.0 * r) + struct.pack(">i", 7 * r)
+                    for r in range(3))
+    path = tmp_path / "t.fits"
+    path.write_bytes(primary + ext + _pad(data, b"\0"))
+    hdus = io.read_fits(str(path))
+    assert len(hdus) == 2
+    t = hdus[1]
+    assert t.name == "LIGHTCURVE"
+    assert t.column_f64("TIME").tolist() == [1.5, 2.5, 3.5]
+    assert t.column_f64("FLUX").tolist() == [0.0, 2.0, 4.0]
+    assert t.column_f64("QUALITY").tolist() == [0.0, 7.0, 14.0]
+
+
+def test_tan_projection_inverse_at_reference_point():
+    # fits.rs:404-423
+    h = io.Header([("CRPIX1", "6.635"), ("CRPIX2", "6.366"), ("CRVAL1", "26.2247"), ("CRVAL2", "-67.9748"),
+                   ("CDELT1", "-0.00584"), ("CDELT2", "0.00584"), ("PC1_1", "-0.2788"), ("PC1_2", "0.9622"),
+                   ("PC2_1", "0.9573"), ("PC2_2", "0.2828")])
+    x, y = io.tan_world_to_pixel(h, 26.2247, -67.9748)
+    assert abs(x - 5.635) < 1e-9 and abs(y - 5.366) < 1e-9
+
+
+def test_read_inputs_groups_files_and_sectors(tmp_path):
+    a, b, c = tmp_path / "a.npz", tmp_path / "b.npz", tmp_path / "c.npz"
+    np.savez(a, time_bjd=np.arange(4.0), flux=np.ones(4), flux_err=np.full(4, 0.1), sector=np.array([3, 3, 4, 4]))
+    np.savez(b, time_bjd=np.arange(10.0, 13.0), flux=np.ones(3), flux_err=np.full(3, 0.2), sector=np.array(3))
+    np.savez(c, time_bjd=np.arange(3.0), flux=np.ones(3))
+    obs = io.read_inputs([str(a), str(b)])
+    assert obs.time.tolist() == [0.0, 1.0, 2.0, 3.0, 10.0, 11.0, 12.0]
+    assert obs.group.tolist() == [0, 0, 1, 1, 2, 2, 2]  # per (file, sector)
+    assert obs.err.tolist() == [0.1] * 4 + [0.2] * 3
+    with pytest.raises(ValueError, match="either provide flux_err or omit it"):
+        io.read_inputs([str(a), str(c)])
+    assert io.read_inputs([str(c)]).err is None
