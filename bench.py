@@ -290,7 +290,7 @@ def run_gpu(args):
                      "algorithmic_bytes_per_launch": fold_bytes_per, "launch_ms": fold_ms_per,
                      "note": "algorithmic bytes count the observation stream once per period (24 n B); it is "
                              "served from shared memory, and the kernel is bound by the shared-memory pipe "
-                             "(profiles/k_fold_walk_multi_sector.md)"},
+                             "(76 % of its wavefront peak in an ncu capture; 1.7 % of DRAM peak)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": e2e_total / args.steps, "step_ms": [round(t, 2) for t in e2e_ms]},
         "clocks": clk,
@@ -504,7 +504,7 @@ def _rescore_bytes(time_rel, origin, rows, n_all):
 
 
 def run_rescore(args):
-    """Peak-selection rescoring (SURVEY's next row 1): a step is one refresh
+    """Peak-selection rescoring: a step is one refresh
     block of select_peaks on the 13-sector star, 8192 rows rescored, i.e.
     fbls_rescore_rows over the family outside the excluded set plus
     fbls_count_rows over the merged times, through the C ABI with host
@@ -583,7 +583,7 @@ def run_rescore(args):
 
 
 def run_single_event(args):
-    """Single-event scan (SURVEY's next row 2): a step is one
+    """Single-event scan: a step is one
     single_event_search of the 13-sector star (one trial period of 357 d, nb
     68,544, 20 durations x 3 shapes), through the C ABI with the family
     resident. value: templates per second of kernel time (fold + scan_all,
@@ -643,7 +643,7 @@ def run_single_event(args):
 
 
 def run_detrend(args):
-    """Biweight detrending (SURVEY's next row 3): a step is one
+    """Biweight detrending: a step is one
     fbls_biweight_flatten of the 13-sector curve (247,104 observations at
     120 s) with a 0.75 d window, c 5, 10 iterations, gap 0.5 d. value:
     observations per second of kernel time; e2e: of the whole call (window

@@ -1,4 +1,4 @@
-// Kernels of the proposal network (north_star's learned form): a small 1D
+// Kernels of the proposal network (the learned pruning of the search): a small 1D
 // CNN over the coarse periodogram, trained and run on the GPU.
 //
 // Activations are laid out channel-major, [C][B][T] (channel, curve, position),

@@ -1,4 +1,4 @@
-// Kernels of the proposal path (north_star's learned form): the coarse
+// Kernels of the proposal path (the learned pruning of the search): the coarse
 // periodogram that feeds the proposal network.
 //
 // k_box_map: for each period of a launch and each duration of a small bank,

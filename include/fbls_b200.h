@@ -259,7 +259,7 @@ int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* dur
                        uint32_t nd, const fbls_config* cfg, fbls_row* rows_out, uint32_t capacity,
                        uint32_t* n_rows, uint64_t* grid_len, fbls_scan_stats* stats_out, uint32_t* n_bands);
 
-/* ---- proposal path (north_star's learned form; no counterpart in the
+/* ---- proposal path (learned pruning of the search; no counterpart in the
  * reference) ------------------------------------------------------------- */
 
 /* Coarse periodogram of an uploaded family, the proposal network's input:
