@@ -128,6 +128,31 @@ def _dist():
     return world, rank, local
 
 
+def _barrier(world: int) -> None:
+    """Every rank meets here (no-op on one rank)."""
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _over_ranks(maxes, sums, world: int, device: str = "cpu"):
+    """(max over ranks of each of `maxes`, sum over ranks of each of `sums`):
+    step times take the slowest rank, work adds up (the whole job's
+    throughput); identity on one rank. Every rank calls it, in the same order."""
+    maxes, sums = [float(x) for x in maxes], [float(x) for x in sums]
+    if world <= 1:
+        return maxes, sums
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(maxes + sums, dtype=torch.float64, device=device)
+    mx, sm = t[:len(maxes)].clone(), t[len(maxes):].clone()
+    if len(maxes):
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    if len(sums):
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return mx.tolist(), sm.tolist()
+
+
 def _oracle_sample(state, cfg, every: int, threads: int):
     """The reference algorithm on every `every`-th period of each band: (trials, seconds)."""
     import oracle
@@ -222,16 +247,12 @@ def run_gpu(args):
         rows, glen, stats = step()
         times.append(gpu.timer_stop())
         trials += sum(s["templates_scanned"] for s in stats)
+    torch.cuda.synchronize()
+    _barrier(world)
     clk = clocks.stop()
     gpu.set_kernel_timing(False)
     ctr = gpu.counters(reset=True)
-    total_ms = sum(times)
-    if world > 1:
-        t = torch.tensor([total_ms, float(trials)], dtype=torch.float64, device=f"cuda:{local}")
-        mx = t.clone()
-        torch.distributed.all_reduce(mx[:1], op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
-        total_ms, trials = float(mx[0]), float(t[1])
+    (total_ms,), (trials,) = _over_ranks([sum(times)], [trials], world, f"cuda:{local}")
     value = trials / (total_ms * 1e-3)
 
     # End to end through the C ABI with host buffers: upload, scan, download.
@@ -246,11 +267,9 @@ def run_gpu(args):
         rows_e, glen_e, stats_e = gpu.signal_search(sub, cfg)
         e2e_ms.append(gpu.timer_stop())
     gc.enable()
-    e2e_total = sum(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_total = float(t[0])
+    torch.cuda.synchronize()
+    _barrier(world)
+    (e2e_total,), _ = _over_ranks([sum(e2e_ms)], [], world, f"cuda:{local}")
     e2e_value = trials / (e2e_total * 1e-3)
     h2d = 3 * 8 * state.n
     d2h = sum((s["periods"] + s["prescan_survivors"]) * (9 * 8 + 8 + 8 + 4) for s in stats_e) + 40 * len(rows_e)
@@ -361,6 +380,8 @@ def run_survey(args):
         out = step()
         times.append((time.perf_counter() - t0) * 1e3)
         trials += sum(t for _, _, t in out)
+    torch.cuda.synchronize()
+    _barrier(world)
     clk = clocks.stop()
     ctr = gpu.counters(reset=True)
     e2e_ms = []
@@ -371,13 +392,9 @@ def run_survey(args):
         out_e = step(resident=False)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     gc.enable()
-    total_ms, e2e_total = sum(times), sum(e2e_ms)
-    if world > 1:
-        t = torch.tensor([total_ms, e2e_total, float(trials)], dtype=torch.float64, device=f"cuda:{local}")
-        mx = t.clone()
-        torch.distributed.all_reduce(mx[:2], op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(t[2:], op=torch.distributed.ReduceOp.SUM)
-        total_ms, e2e_total, trials = float(mx[0]), float(mx[1]), float(t[2])
+    torch.cuda.synchronize()
+    _barrier(world)
+    (total_ms, e2e_total), (trials,) = _over_ranks([sum(times), sum(e2e_ms)], [trials], world, f"cuda:{local}")
     if rank != 0:
         return
     value = trials / (total_ms * 1e-3)
