@@ -5,17 +5,21 @@ import this package, and only to check or time against it. The product
 (fbls_b200) never calls it.
 
 The arithmetic lives in fbls_oracle.cpp (a C++ restatement of the
-reference's src/search/{grid,scan,kernels,evidence,math}.rs and the
-prepared-mode preparation in src/prep/{curve,stats}.rs); this module binds
-it with ctypes and restates the small host orchestration of
-scan_periods (src/search/scan.rs:363-408) and signal_search
-(src/search/scan.rs:413-473) in Python.
+reference's src/search/{grid,scan,kernels,evidence,math}.rs, the
+prepared-mode preparation in src/prep/{curve,stats}.rs, the rescoring and
+single-event kernels and both forms of the biweight detrend); this module
+binds it with ctypes and restates in Python the host orchestration of
+scan_periods (src/search/scan.rs:363-408), signal_search
+(src/search/scan.rs:413-473), single_event_search (src/search/events.rs) and
+the raw-mode preparation (src/prep/curve.rs:89-198, :332-425).
 
 Parity status: pinned by the reference's erfc table (math.rs:183-210), grid
-property (grid.rs:34-42) and noise-model / transit-mask tests
-(curve.rs:636-673). The reference has no golden vectors for the fold,
-prefix, tile-scan or evidence outputs; those are checked here by brute-force
-identities only (parity unpinned against reference output).
+property (grid.rs:34-42), noise-model / transit-mask tests
+(curve.rs:636-673) and biweight trend test (curve.rs:624-634). The reference
+has no golden vectors for the fold, prefix, tile-scan, evidence, rescoring,
+single-event or detrend outputs; those are checked here by brute-force
+identities and literal loop restatements only (parity unpinned against
+reference output).
 """
 from __future__ import annotations
 
