@@ -29,7 +29,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-
               "-Xptxas", "-O3"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall"]
 
-CU_SOURCES = ["fold.cu", "scan_kernels.cu", "evidence.cu", "proposal.cu", "rescore.cu", "biweight.cu", "cnn.cu", "host.cu",
+CU_SOURCES = ["fold.cu", "scan_kernels.cu", "evidence.cu", "proposal.cu", "rescore.cu", "biweight.cu", "cnn.cu", "host.cu", "host_maps.cu", "host_next.cu",
               "static_entry.cu"]
 CPP_SOURCES = ["prep.cpp"]
 

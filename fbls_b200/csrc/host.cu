@@ -1,4 +1,8 @@
-// Host driver of the FBLS search path on one B200 and the library's C ABI.
+// Host driver of the FBLS search path on one B200 and the search's C ABI
+// (context, families, scan_bank / scan_periods / signal_search, evidence, the
+// batch runner). The coarse maps are in host_maps.cu, the steps either side
+// of the search in host_next.cu, the shared context and helpers in
+// host_internal.h.
 //
 // Restates the reference's host logic around the kernels:
 //   scan_bank      src/search/scan.rs:144-357 (bank factors, fold budget,
@@ -11,20 +15,11 @@
 // two sessions (every band's first pass, then every band's survivor pass),
 // each with one upload from page-locked memory, all launches back to back on
 // one stream, one download and one synchronisation.
-#include <algorithm>
-#include <atomic>
-#include <cmath>
-#include <cstdio>
-#include <cstdlib>
-#include <cstring>
-#include <string>
-#include <thread>
 #include <tuple>
-#include <vector>
 
-#include "../../include/fbls_b200.h"
 #include "common.cuh"
 #include "evidence.h"
+#include "host_internal.h"
 #include "kernels.h"
 #include "prep.h"
 
@@ -32,104 +27,6 @@ using namespace fbls;
 
 namespace {
 
-struct DevBuf {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-};
-
-struct PinBuf {  // page-locked host memory
-    void* ptr = nullptr;
-    size_t bytes = 0;
-};
-
-}  // namespace
-
-struct fbls_ctx {
-    int device = 0;
-    int sm_count = 148;
-    cudaStream_t stream = nullptr;
-    std::string error;
-    bool profile = false;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    bool kernel_timing = false;
-    cudaEvent_t timer[2] = {nullptr, nullptr};
-    std::vector<cudaEvent_t> pool;  // per-launch timing events
-    fbls_counters counters{};
-    // Workspace, grown on demand and reused across bands and calls.
-    DevBuf cum, cum32, hist, parts, keys, tflags;  // per launch
-    DevBuf pass_in, pass_out;  // per session: every pass's inputs and outputs
-    DevBuf evidence, fault;
-    DevBuf family;  // observations of the star a batch worker is searching
-    DevBuf mapbin;  // time-binned observations of a coarse map
-    DevBuf feat;    // the proposal network's input made from coarse maps
-    DevBuf rescore; // peak-selection rescoring: rows, masks, times and results
-    PinBuf pin_up, pin_down, pin_down2;  // staging of a session's upload and download (two sessions in flight)
-    std::vector<fbls_ctx*> workers;  // fbls_search_batch worker contexts, kept for reuse
-};
-
-struct fbls_ready {
-    fbls_ctx* ctx = nullptr;
-    double* time = nullptr;  // n
-    double* v = nullptr;     // n
-    double* w = nullptr;     // n
-    uint32_t n = 0;
-    double baseline_norm = 0.0;
-    double origin = 0.0;
-    double residual_energy = 0.0;
-    double t_last = 0.0;
-    std::vector<double> time_host;  // for the fold's chunk boundaries
-    bool owned = true;              // time/v/w allocated for this handle (else a context's buffer)
-};
-
-namespace {
-
-int fail(fbls_ctx* ctx, int status, const std::string& message) {
-    if (ctx) ctx->error = message;
-    return status;
-}
-
-int cuda_fail(fbls_ctx* ctx, cudaError_t e, const char* where) {
-    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
-    return fail(ctx, FBLS_ERR_CUDA, m);
-}
-
-#define CK(call, where)                                   \
-    do {                                                  \
-        cudaError_t e_ = (call);                          \
-        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
-    } while (0)
-
-cudaError_t ensure(DevBuf& b, size_t bytes) {
-    if (bytes == 0) bytes = 16;
-    if (b.bytes >= bytes) return cudaSuccess;
-    if (b.ptr) {
-        cudaError_t e = cudaFree(b.ptr);
-        if (e != cudaSuccess) return e;
-        b.ptr = nullptr;
-        b.bytes = 0;
-    }
-    size_t want = bytes + bytes / 4;
-    cudaError_t e = cudaMalloc(&b.ptr, want);
-    if (e != cudaSuccess) return e;
-    b.bytes = want;
-    return cudaSuccess;
-}
-
-void release(DevBuf& b) {
-    if (b.ptr) cudaFree(b.ptr);
-    b.ptr = nullptr;
-    b.bytes = 0;
-}
-
-template <typename T>
-T* as(DevBuf& b) {
-    return reinterpret_cast<T*>(b.ptr);
-}
-
-// Checks and uploads a prepared family into `r` (DeviceReady::upload,
-// scan.rs:110-124): into a fresh allocation owned by `r` when `buf` is null,
-// else into the reusable context buffer `buf` (no allocation once it is
-// large enough, so a batch worker never synchronises the device on cudaFree).
 // Checks a family's host arrays; a rejection's message goes to `err`.
 int check_family(std::string& err, const double* time, const double* v, const double* w, uint32_t n) {
     auto bad = [&](int status, const char* message) {
@@ -144,6 +41,10 @@ int check_family(std::string& err, const double* time, const double* v, const do
     return FBLS_OK;
 }
 
+// Checks and uploads a prepared family into `r` (DeviceReady::upload,
+// scan.rs:110-124): into a fresh allocation owned by `r` when `buf` is null,
+// else into the reusable context buffer `buf` (no allocation once it is
+// large enough, so a batch worker never synchronises the device on cudaFree).
 int upload_family(fbls_ctx* ctx, DevBuf* buf, const double* time, const double* v, const double* w, uint32_t n,
                   double baseline_norm, double origin, double residual_energy, fbls_ready* r) {
     std::string err;
@@ -186,15 +87,6 @@ int upload_family(fbls_ctx* ctx, DevBuf* buf, const double* time, const double* 
     return FBLS_OK;
 }
 
-// Fold budget in MiB: the configured value capped at half of the free device
-// memory (Gpu::fold_budget_mib, scan.rs:93-98).
-double fold_budget_mib(double configured) {
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return configured;
-    double cap = (double)free_b / 1048576.0 / 2.0;
-    return configured < cap ? configured : cap;
-}
-
 // A pass's outputs, read in place from its session's page-locked download
 // buffer (valid until that buffer serves another session).
 struct BandOut {
@@ -203,30 +95,6 @@ struct BandOut {
     const double* depth = nullptr;
     const uint32_t* flags = nullptr;
 };
-
-double now_seconds() {
-    timespec ts;
-    clock_gettime(CLOCK_MONOTONIC, &ts);
-    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
-}
-
-size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
-
-cudaError_t ensure_pinned(PinBuf& b, size_t bytes) {
-    if (bytes == 0) bytes = 256;
-    if (b.bytes >= bytes) return cudaSuccess;
-    if (b.ptr) {
-        cudaError_t e = cudaFreeHost(b.ptr);
-        if (e != cudaSuccess) return e;
-        b.ptr = nullptr;
-        b.bytes = 0;
-    }
-    size_t want = bytes + bytes / 4;
-    cudaError_t e = cudaHostAlloc(&b.ptr, want, cudaHostAllocDefault);
-    if (e != cudaSuccess) return e;
-    b.bytes = want;
-    return cudaSuccess;
-}
 
 // One scan_bank pass (scan.rs:144-357): every period's best template at nb
 // bins. Planned on the host, then enqueued with the other passes of a session.
@@ -254,28 +122,6 @@ struct Pass {
         return status;
     }
 };
-
-// Runs f(i) for i in [0, n) on up to 16 host threads, the caller's included.
-// Fewer than PARALLEL_MIN items run on the caller's thread: a single star's
-// few passes plan in milliseconds, and starting threads for them only adds
-// the risk of waiting on a descheduled one when the host's cores are busy.
-constexpr size_t PARALLEL_MIN = 32;
-template <typename F>
-void parallel_for(size_t n, F f) {
-    const size_t threads = std::min<size_t>(n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
-    if (threads <= 1 || n < PARALLEL_MIN) {
-        for (size_t i = 0; i < n; i++) f(i);
-        return;
-    }
-    std::atomic<size_t> next{0};
-    auto work = [&]() {
-        for (size_t i; (i = next.fetch_add(1)) < n;) f(i);
-    };
-    std::vector<std::thread> pool;
-    for (size_t k = 1; k < threads; k++) pool.emplace_back(work);
-    work();
-    for (std::thread& t : pool) t.join();
-}
 
 // plan_pass over every pass (in parallel: the passes are independent);
 // returns the first failure in pass order, its message in ctx.
@@ -1235,422 +1081,6 @@ int search_batch_fused(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fb
     return FBLS_OK;
 }
 
-
-// A coarse map (fbls_coarse_map) planned on the host: its time bins when
-// bin_days > 0 (observations whose floor((t - t0) / bin_days) agree, summed at
-// their mean time) and its octave groups [lo, 2 lo), each folded at nb =
-// max(8, ceil(oversample * (group's longest period) / shortest duration)) in
-// launches of at most per_launch periods. plan_map writes only the plan, so
-// the plans of a batch are made in parallel.
-struct MapPlan {
-    fbls_map_job* job = nullptr;
-    int star = 0;             // index of the job in its batch
-    bool need_out = true;     // job->out must be given (else only features are made)
-    bool use_bins = false;
-    fbls_ready bins;          // the binned family (use_bins); device fields set by run_maps
-    std::vector<int> starts;  // nbins + 1 observation offsets of the bins
-    struct Group {
-        uint32_t i0 = 0, count = 0, nb = 0, per_launch = 0;
-        FoldShape shape{};
-        std::vector<int> chunks;
-        size_t off_scales = 0, off_chunks = 0;
-    };
-    std::vector<Group> groups;
-    size_t off_time = 0, off_starts = 0, in_bytes = 0;  // within the plan's upload region (bank at 0)
-    size_t in_off = 0, out_off = 0, bin_off = 0;          // the plan's regions in its run
-    std::string err;
-    const fbls_ready* ready() const { return use_bins ? &bins : job->ready; }
-};
-
-int plan_map(const fbls_ctx* ctx, MapPlan& m) {
-    const fbls_map_job& j = *m.job;
-    auto bad = [&](int status, const char* message) {
-        m.err = message;
-        return status;
-    };
-    if (!j.ready || (j.P && !j.periods) || !j.durations || !j.rho || (m.need_out && !j.out))
-        return bad(FBLS_ERR_ARGUMENT, "null argument");
-    if (!(j.bin_days >= 0.0)) return bad(FBLS_ERR_ARGUMENT, "bin_days must not be negative");
-    if (j.nd < 1 || j.nd > (uint32_t)MAP_MAX_DURATIONS) return bad(FBLS_ERR_ARGUMENT, "1 to 8 map durations");
-    if (j.P == 0) return FBLS_OK;
-    if (!(j.oversample > 0.0)) return bad(FBLS_ERR_ARGUMENT, "oversample must be positive");
-    for (uint32_t i = 0; i < j.P; i++)
-        if (!(j.periods[i] > 0.0) || !std::isfinite(j.periods[i]) || (i && !(j.periods[i] > j.periods[i - 1])))
-            return bad(FBLS_ERR_ARGUMENT, "periods must be positive, finite and ascending");
-    double dmin = __builtin_huge_val();
-    for (uint32_t i = 0; i < j.nd; i++) {
-        if (!(j.durations[i] > 0.0) || !(j.rho[i] > 0.0)) return bad(FBLS_ERR_ARGUMENT, "bad map duration");
-        dmin = rmin(dmin, j.durations[i]);
-    }
-    const fbls_ready* family = j.ready;
-    if (j.bin_days > 0.0) {
-        const std::vector<double>& t = family->time_host;
-        std::vector<double>& tb = m.bins.time_host;
-        tb.clear();
-        m.starts.clear();
-        for (uint32_t i = 0; i < family->n;) {
-            const double b = std::floor((t[i] - t[0]) / j.bin_days);
-            uint32_t k = i;
-            double sum = 0.0;
-            while (k < family->n && std::floor((t[k] - t[0]) / j.bin_days) == b) sum += t[k++];
-            m.starts.push_back((int)i);
-            tb.push_back(sum / (double)(k - i));
-            i = k;
-        }
-        m.starts.push_back((int)family->n);
-        m.use_bins = true;
-        m.bins.n = (uint32_t)tb.size();
-        m.bins.baseline_norm = family->baseline_norm;
-        m.bins.origin = family->origin;
-        m.bins.residual_energy = family->residual_energy;
-        m.bins.t_last = tb.back();
-        m.bins.owned = false;
-    }
-    const fbls_ready* ready = m.ready();
-    size_t in_bytes = align256(2 * j.nd * sizeof(double));
-    if (m.use_bins) {
-        m.off_time = in_bytes;
-        in_bytes += align256(fold_field_stride(m.bins.n) * sizeof(double));
-        m.off_starts = in_bytes;
-        in_bytes += align256(m.starts.size() * sizeof(int));
-    }
-    m.groups.clear();
-    for (uint32_t i0 = 0; i0 < j.P;) {
-        uint32_t i1 = i0 + 1;
-        while (i1 < j.P && j.periods[i1] < 2.0 * j.periods[i0]) i1++;
-        MapPlan::Group g;
-        g.i0 = i0;
-        g.count = i1 - i0;
-        const uint64_t nb = std::max<uint64_t>(8, as_u64(std::ceil(j.oversample * j.periods[i1 - 1] / dmin)));
-        if (nb > (1u << 24)) return bad(FBLS_ERR_ARGUMENT, "phase grid too large");
-        g.nb = (uint32_t)nb;
-        const double scale_max = (double)nb / j.periods[i0];
-        if (std::floor(ready->t_last * scale_max) >= 4294967295.0 - 2.0 * (double)nb - 2.0)
-            return bad(FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
-        const size_t stride = 2 * (size_t)nb + 1;
-        g.per_launch = (uint32_t)std::max<size_t>(1, std::min<size_t>(16384, (512ull << 20) / (NF * stride * 12)));
-        g.shape = fold_group_shape((int)nb, (int)std::min(g.count, g.per_launch), ctx->sm_count);
-        g.chunks.resize((size_t)ready->n + 2);
-        const int c = fold_chunks(ready->time_host.data(), (int)ready->n, scale_max, (int)nb, g.shape.span_cap,
-                                  g.shape.chunk_cap, g.chunks.data(), (int)g.chunks.size());
-        if (c < 1) return bad(FBLS_ERR_ARGUMENT, "fold chunking failed");
-        g.chunks.resize((size_t)c + 1);
-        g.off_scales = in_bytes;
-        in_bytes += align256(g.count * sizeof(double));
-        g.off_chunks = in_bytes;
-        in_bytes += align256(g.chunks.size() * sizeof(int));
-        m.groups.push_back(std::move(g));
-        i0 = i1;
-    }
-    m.in_bytes = in_bytes;
-    return FBLS_OK;
-}
-
-// Runs planned maps on ctx->stream: one upload, one launch for every star's
-// bins, then waves of fold units (a group's launch of at most per_launch
-// periods), each wave one fold launch of the walking folds as jobs, whose
-// epilogue computes the box maps from the prefix rows in shared memory, and
-// for any other fold (too many bins for the walking fold) its own launch,
-// prefix rows in HBM (the wave's share under MAP_WAVE_BYTES) and a box-map
-// launch;
-// with `feat`, one k_map_features launch writing the maps' network input into
-// feat->x (device); one download and one synchronisation; each map is copied
-// to its job's out when there is one.
-constexpr size_t MAP_WAVE_BYTES = 1536ull << 20;
-
-struct MapFeatures {
-    float* x = nullptr;  // device, channels x B x T, zeroed
-    int channels = 0, B = 0, T = 0;
-    const uint32_t* offsets = nullptr;  // per star
-};
-
-int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeatures* feat) {
-    if (plans.empty()) return FBLS_OK;
-    struct Unit {
-        MapPlan* m;
-        const MapPlan::Group* g;
-        uint32_t c0;
-        int n;
-        size_t cum_off, hist_off;
-        bool walk;
-    };
-    struct Wave {
-        std::vector<Unit> units;
-        size_t cum = 0, hist = 0, smem = 0;
-        int fold_jobs = 0, fold_ctas = 0, map_jobs = 0, map_total = 0;
-        size_t off_fold = 0, off_fcta = 0, off_map = 0, off_mp = 0;
-    };
-    size_t in_total = 0, out_total = 0, bin_total = 0;
-    int nbinned = 0, bin_total_bins = 0;
-    std::vector<Wave> waves(1);
-    for (MapPlan* m : plans) {
-        m->in_off = in_total;
-        in_total += m->in_bytes;
-        m->out_off = out_total;
-        out_total += align256((size_t)m->job->P * m->job->nd * sizeof(float));
-        if (m->use_bins) {
-            m->bin_off = bin_total;
-            bin_total += align256(2 * fold_field_stride(m->bins.n) * sizeof(double));
-            nbinned++;
-            bin_total_bins += (int)m->bins.n;
-        }
-        for (const MapPlan::Group& g : m->groups) {
-            const size_t stride = 2 * (size_t)g.nb + 1;
-            for (uint32_t c0 = 0; c0 < g.count; c0 += g.per_launch) {
-                const int n = (int)std::min(g.count - c0, g.per_launch);
-                const bool walk = g.shape.kind == FOLD_WALK;  // box maps in the fold's epilogue: no prefix rows
-                const size_t cum = walk ? 0 : (size_t)n * NF * stride;
-                const size_t hist = walk ? 0 : ((n + g.shape.group - 1) / g.shape.group) * (size_t)g.shape.group *
-                                                   NF * (size_t)g.shape.row_stride;
-                if (!waves.back().units.empty() &&
-                    (waves.back().cum + cum) * (sizeof(double) + sizeof(float2)) > MAP_WAVE_BYTES)
-                    waves.emplace_back();
-                Wave& w = waves.back();
-                w.units.push_back({m, &g, c0, n, w.cum, w.hist, walk});
-                w.cum += cum;
-                w.hist += hist;
-                if (walk) {
-                    w.fold_jobs++;
-                    w.fold_ctas += (n + g.shape.group - 1) / g.shape.group;
-                    w.smem = std::max(w.smem, g.shape.smem);
-                } else {
-                    w.map_jobs++;
-                    w.map_total += n;
-                }
-            }
-        }
-    }
-    size_t blob = in_total;
-    auto take = [&](size_t bytes) {
-        const size_t at = blob;
-        blob += align256(bytes);
-        return at;
-    };
-    const size_t off_bins = take(std::max(1, nbinned) * sizeof(BinJob)), off_b0 = take((nbinned + 1) * sizeof(int));
-    const size_t off_feat = take(plans.size() * sizeof(FeatJob));
-    size_t cum_max = 0, hist_max = 0;
-    for (Wave& w : waves) {
-        cum_max = std::max(cum_max, w.cum);
-        hist_max = std::max(hist_max, w.hist);
-        w.off_fold = take(std::max(1, w.fold_jobs) * sizeof(FoldArgs));
-        w.off_fcta = take((w.fold_jobs + 1) * sizeof(int));
-        w.off_map = take(std::max(1, w.map_jobs) * sizeof(MapArgs));
-        w.off_mp = take((w.map_jobs + 1) * sizeof(int));
-    }
-    CK(ensure(ctx->pass_in, blob), "workspace");
-    CK(ensure(ctx->pass_out, out_total), "workspace");
-    if (cum_max) {
-        CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
-        CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
-    }
-    if (hist_max) CK(ensure(ctx->hist, hist_max * sizeof(double)), "workspace");
-    if (bin_total) CK(ensure(ctx->mapbin, bin_total), "workspace");
-    CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
-    CK(ensure_pinned(ctx->pin_up, blob), "pinned workspace");
-    CK(ensure_pinned(ctx->pin_down, out_total + 256), "pinned workspace");
-    unsigned char* up = static_cast<unsigned char*>(ctx->pin_up.ptr);
-    unsigned char* din = static_cast<unsigned char*>(ctx->pass_in.ptr);
-    unsigned char* dout = static_cast<unsigned char*>(ctx->pass_out.ptr);
-    unsigned char* dbin = static_cast<unsigned char*>(ctx->mapbin.ptr);
-    BinJob* bj = reinterpret_cast<BinJob*>(up + off_bins);
-    int* b0 = reinterpret_cast<int*>(up + off_b0);
-    int nb_jobs = 0, nb_bins = 0;
-    for (MapPlan* m : plans) {
-        const fbls_map_job& j = *m->job;
-        unsigned char* b = up + m->in_off;
-        std::memcpy(b, j.durations, j.nd * sizeof(double));
-        std::memcpy(b + j.nd * sizeof(double), j.rho, j.nd * sizeof(double));
-        if (m->use_bins) {
-            const size_t stride = fold_field_stride(m->bins.n);
-            double* t = reinterpret_cast<double*>(b + m->off_time);
-            std::memcpy(t, m->bins.time_host.data(), m->bins.n * sizeof(double));
-            std::memset(t + m->bins.n, 0, (stride - m->bins.n) * sizeof(double));
-            std::memcpy(b + m->off_starts, m->starts.data(), m->starts.size() * sizeof(int));
-            m->bins.time = reinterpret_cast<double*>(din + m->in_off + m->off_time);
-            m->bins.v = reinterpret_cast<double*>(dbin + m->bin_off);
-            m->bins.w = m->bins.v + stride;
-            bj[nb_jobs] = {j.ready->v, j.ready->w, reinterpret_cast<const int*>(din + m->in_off + m->off_starts),
-                           (int)m->bins.n, m->bins.v, m->bins.w};
-            b0[nb_jobs++] = nb_bins;
-            nb_bins += (int)m->bins.n;
-        }
-        for (const MapPlan::Group& g : m->groups) {
-            double* sc = reinterpret_cast<double*>(b + g.off_scales);
-            for (uint32_t i = 0; i < g.count; i++) sc[i] = (double)g.nb / j.periods[g.i0 + i];
-            std::memcpy(b + g.off_chunks, g.chunks.data(), g.chunks.size() * sizeof(int));
-        }
-    }
-    b0[nb_jobs] = nb_bins;
-    FeatJob* fjobs = reinterpret_cast<FeatJob*>(up + off_feat);
-    bool any_out = false;
-    for (size_t k = 0; k < plans.size(); k++) {
-        const MapPlan* m = plans[k];
-        any_out = any_out || m->job->out;
-        fjobs[k] = {reinterpret_cast<const float*>(dout + m->out_off), (int)m->job->P, (int)m->job->nd, m->star,
-                    feat ? (int)feat->offsets[m->star] : 0};
-    }
-    std::vector<FoldArgs> own;  // folds that are not walking folds: their own launches
-    std::vector<const FoldShape*> own_shape;
-    std::vector<size_t> own_wave;
-    for (size_t wi = 0; wi < waves.size(); wi++) {
-        Wave& w = waves[wi];
-        FoldArgs* fj = reinterpret_cast<FoldArgs*>(up + w.off_fold);
-        int* fc = reinterpret_cast<int*>(up + w.off_fcta);
-        MapArgs* mj = reinterpret_cast<MapArgs*>(up + w.off_map);
-        int* mp = reinterpret_cast<int*>(up + w.off_mp);
-        int nf = 0, fcta = 0, nm = 0, mtot = 0;
-        for (size_t u = 0; u < w.units.size(); u++) {
-            const Unit& un = w.units[u];
-            const MapPlan& m = *un.m;
-            const MapPlan::Group& g = *un.g;
-            const fbls_ready* r = m.ready();
-            const unsigned char* b = din + m.in_off;
-            FoldArgs fa{};
-            fa.time = r->time;
-            fa.v = r->v;
-            fa.w = r->w;
-            fa.scales = reinterpret_cast<const double*>(b + g.off_scales) + un.c0;
-            fa.n = (int)r->n;
-            fa.nb = (int)g.nb;
-            fa.periods = un.n;
-            fa.group = g.shape.group;
-            fa.cum = un.walk ? nullptr : as<double>(ctx->cum) + un.cum_off;
-            fa.cum32 = un.walk ? nullptr : as<float2>(ctx->cum32) + un.cum_off;
-            fa.hist_global = un.walk ? nullptr : as<double>(ctx->hist) + un.hist_off;
-            fa.hist_out = nullptr;
-            fa.chunks = reinterpret_cast<const int*>(b + g.off_chunks);
-            fa.nchunks = (int)g.chunks.size() - 1;
-            fa.stage_field = g.shape.stage_field;
-            fa.window = g.shape.window;
-            fa.row_stride = g.shape.row_stride;
-            fa.fault = as<uint32_t>(ctx->fault);
-            float* out = reinterpret_cast<float*>(dout + m.out_off) + (size_t)(g.i0 + un.c0) * m.job->nd;
-            if (un.walk) {
-                fa.map_out = out;
-                fa.map_durations = reinterpret_cast<const double*>(b);
-                fa.map_rho = reinterpret_cast<const double*>(b) + m.job->nd;
-                fa.map_nd = (int)m.job->nd;
-                fa.map_baseline = r->baseline_norm;
-                if (!fold_job_ok(fa, g.shape)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
-                fj[nf] = fa;
-                fc[nf++] = fcta;
-                fcta += (un.n + g.shape.group - 1) / g.shape.group;
-            } else {
-                own.push_back(fa);
-                own_shape.push_back(&g.shape);
-                own_wave.push_back(wi);
-            }
-            if (!un.walk) {
-                MapArgs ma{};
-                ma.cum = fa.cum;
-                ma.scales = fa.scales;
-                ma.durations = reinterpret_cast<const double*>(b);
-                ma.rho = reinterpret_cast<const double*>(b) + m.job->nd;
-                ma.nd = (int)m.job->nd;
-                ma.nb = (int)g.nb;
-                ma.baseline = r->baseline_norm;
-                ma.n = (double)r->n;
-                ma.out = out;
-                mj[nm] = ma;
-                mp[nm++] = mtot;
-                mtot += un.n;
-            }
-            ctx->counters.fold_updates += (uint64_t)un.n * r->n;
-        }
-        fc[nf] = fcta;
-        mp[nm] = mtot;
-    }
-    cudaStream_t s = ctx->stream;
-    CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
-    if (bin_total) CK(cudaMemsetAsync(ctx->mapbin.ptr, 0, bin_total, s), "workspace");
-    CK(cudaMemcpyAsync(din, up, blob, cudaMemcpyHostToDevice, s), "upload");
-    if (nb_jobs) {
-        CK(launch_bin_fields_jobs(reinterpret_cast<const BinJob*>(din + off_bins),
-                                  reinterpret_cast<const int*>(din + off_b0), nb_jobs, nb_bins, s),
-           "bins");
-        ctx->counters.launches += 1;
-    }
-    size_t oi = 0;
-    for (size_t wi = 0; wi < waves.size(); wi++) {
-        const Wave& w = waves[wi];
-        if (w.fold_jobs) {
-            CK(launch_fold_jobs(reinterpret_cast<const FoldArgs*>(din + w.off_fold),
-                                reinterpret_cast<const int*>(din + w.off_fcta), w.fold_jobs, w.fold_ctas, w.smem, s),
-               "fold");
-            ctx->counters.launches += 1;
-        }
-        for (; oi < own.size() && own_wave[oi] == wi; oi++) {
-            CK(launch_fold(own[oi], *own_shape[oi], s), "fold");
-            ctx->counters.launches += 1;
-        }
-        if (w.map_jobs) {
-            CK(launch_box_map_jobs(reinterpret_cast<const MapArgs*>(din + w.off_map),
-                                   reinterpret_cast<const int*>(din + w.off_mp), w.map_jobs, w.map_total, s),
-               "box map");
-            ctx->counters.launches += 1;
-        }
-    }
-    if (feat) {
-        CK(launch_map_features(reinterpret_cast<const FeatJob*>(din + off_feat), (int)plans.size(), feat->channels,
-                               feat->B, feat->T, feat->x, s),
-           "map features");
-        ctx->counters.launches += 1;
-    }
-    unsigned char* down = static_cast<unsigned char*>(ctx->pin_down.ptr);
-    if (any_out) CK(cudaMemcpyAsync(down, dout, out_total, cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaMemcpyAsync(down + out_total, ctx->fault.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaStreamSynchronize(s), "coarse map");
-    uint32_t fault = 0;
-    std::memcpy(&fault, down + out_total, sizeof(uint32_t));
-    if (fault) return fail(ctx, FBLS_ERR_CUDA, "fold: staging copies did not complete");
-    for (MapPlan* m : plans)
-        if (m->job->out) std::memcpy(m->job->out, down + m->out_off, (size_t)m->job->P * m->job->nd * sizeof(float));
-    return FBLS_OK;
-}
-
-// Plans (in parallel) and runs the maps of `jobs` on ctx, in runs of at most
-// MAP_RUN_PERIODS periods; every job's status is set, a failing job's message
-// goes to errors[i]. Returns a failure of the device work itself, else 0.
-constexpr uint64_t MAP_RUN_PERIODS = 1u << 22;
-
-int coarse_maps(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, std::vector<std::string>& errors,
-                const MapFeatures* feat = nullptr) {
-    std::vector<MapPlan> plans(count);
-    std::vector<int> rc(count, FBLS_OK);
-    for (uint32_t i = 0; i < count; i++) {
-        plans[i].job = &jobs[i];
-        plans[i].star = (int)i;
-        plans[i].need_out = feat == nullptr;
-    }
-    parallel_for(count, [&](size_t i) { rc[i] = plan_map(ctx, plans[i]); });
-    std::vector<MapPlan*> run;
-    uint64_t periods = 0;
-    for (uint32_t i = 0; i <= count; i++) {
-        if (i == count || (!run.empty() && periods + jobs[i].P > MAP_RUN_PERIODS)) {
-            const int e = run_maps(ctx, run, feat);
-            if (e) {
-                for (MapPlan* m : run) {
-                    m->job->status = e;
-                    errors[m->job - jobs] = ctx->error;
-                }
-                return e;
-            }
-            run.clear();
-            periods = 0;
-            if (i == count) break;
-        }
-        jobs[i].status = rc[i];
-        if (rc[i]) {
-            errors[i] = plans[i].err;
-            continue;
-        }
-        if (plans[i].groups.empty()) continue;
-        run.push_back(&plans[i]);
-        periods += jobs[i].P;
-    }
-    return FBLS_OK;
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1878,21 +1308,6 @@ int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* du
     return FBLS_OK;
 }
 
-// Coarse periodogram of a family for the proposal network (plan_map, then
-// run_maps: the octave groups' folds and box maps as job launches).
-int fbls_coarse_map(fbls_ctx* ctx, const fbls_ready* family, const double* periods, uint32_t P,
-                    const double* durations, const double* rho, uint32_t nd, double oversample, double bin_days,
-                    float* out) {
-    if (!ctx) return FBLS_ERR_ARGUMENT;
-    CK(cudaSetDevice(ctx->device), "set device");
-    fbls_map_job job{family, periods, P, durations, rho, nd, oversample, bin_days, out, FBLS_OK};
-    std::vector<std::string> errors(1);
-    const int rc = coarse_maps(ctx, &job, 1, errors);
-    if (rc) return rc;
-    if (job.status) return fail(ctx, job.status, errors[0]);
-    return FBLS_OK;
-}
-
 // Many stars on one device: `workers` host threads (the caller's included),
 // each with its own context (stream, workspace and a reusable buffer for the
 // star's observations), take stars from a shared counter and run
@@ -1970,508 +1385,4 @@ int fbls_search_batch(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbl
         if (stars[i].status) return fail(ctx, stars[i].status, "star " + std::to_string(i) + ": " + errors[i]);
     return FBLS_OK;
 }
-
-// single_event_search (events.rs:18-153): the durations sorted with their
-// rho, one trial period baseline + 2 (longest duration) + 1e-6 d (longer than
-// the data, so nothing wraps), nb = max(8, ceil(phase_oversample * trial /
-// shortest duration)); the family folded at that period by the fold kernels,
-// then k_scan_all keeps every template whose exact score reaches the
-// threshold. Rows (period +inf, epoch, duration, score, depth) come out
-// ordered by (phase, duration, shape); past `capacity` survivors the rows are
-// dropped and `overflow` set, as the reference does.
-int fbls_single_event_search(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
-                             uint32_t nd, const fbls_config* cfg, uint32_t capacity, fbls_row* rows_out,
-                             uint32_t* n_rows, fbls_event_stats* stats) {
-    if (!ctx || !ready || !durations || !rho || !cfg || !n_rows || (capacity && !rows_out))
-        return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    if (nd == 0 || nd > (uint32_t)MAX_DURATIONS) return fail(ctx, FBLS_ERR_ARGUMENT, "1 to 64 durations");
-    if (cfg->n_ingress < 1 || cfg->n_ingress > (uint32_t)MAX_SHAPES || cfg->shape_layers < 1 ||
-        cfg->shape_layers > (uint32_t)MAX_LAYERS)
-        return fail(ctx, FBLS_ERR_ARGUMENT, "bank size outside the supported range");
-    *n_rows = 0;
-    CK(cudaSetDevice(ctx->device), "set device");
-    std::vector<std::pair<double, double>> ds(nd);
-    for (uint32_t i = 0; i < nd; i++) ds[i] = {durations[i], rho[i]};
-    std::stable_sort(ds.begin(), ds.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    if (!(ds[0].first > 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "durations must be positive");
-    const double trial = ready->t_last + 2.0 * ds[nd - 1].first + 1e-6;
-    const uint64_t nb64 = std::max<uint64_t>(8, as_u64(std::ceil((double)cfg->phase_oversample * trial / ds[0].first)));
-    if (nb64 > (1u << 24)) return fail(ctx, FBLS_ERR_ARGUMENT, "phase grid too large");
-    const int nb = (int)nb64;
-    const double scale = (double)nb / trial;
-    const uint32_t ns = cfg->n_ingress, layers = cfg->shape_layers;
-    std::vector<double> bank;  // durations | rho | ingress | factors (scan.rs:157-171)
-    for (auto& d : ds) bank.push_back(d.first);
-    for (auto& d : ds) bank.push_back(d.second);
-    bank.insert(bank.end(), cfg->ingress_fractions, cfg->ingress_fractions + ns);
-    for (uint32_t si = 0; si < ns; si++)
-        for (uint32_t l = 0; l < layers; l++)
-            bank.push_back(1.0 - 2.0 * cfg->ingress_fractions[si] *
-                                     (layers > 1 ? (double)l / (double)(layers - 1) : 0.0));
-    const FoldShape shape = fold_group_shape(nb, 1, ctx->sm_count);
-    std::vector<int> chunks((size_t)ready->n + 2);
-    const int count = fold_chunks(ready->time_host.data(), (int)ready->n, scale, nb, shape.span_cap,
-                                  shape.chunk_cap, chunks.data(), (int)chunks.size());
-    if (count < 1) return fail(ctx, FBLS_ERR_ARGUMENT, "fold chunking failed");
-    chunks.resize((size_t)count + 1);
-    const size_t stride = 2 * (size_t)nb + 1;
-    const size_t o_scale = 0, o_bank = 256, o_chunks = o_bank + align256(bank.size() * sizeof(double)),
-                 in_total = o_chunks + align256(chunks.size() * sizeof(int));
-    const size_t o_counter = 0, o_rec = 256, out_total = o_rec + align256((size_t)capacity * EVENT_RECORD * 8 + 8);
-    CK(ensure(ctx->pass_in, in_total), "workspace");
-    CK(ensure(ctx->pass_out, out_total), "workspace");
-    CK(ensure(ctx->cum, NF * stride * sizeof(double)), "workspace");
-    CK(ensure(ctx->cum32, NF * stride * sizeof(float2)), "workspace");
-    if (!shape.hist_in_smem) CK(ensure(ctx->hist, (size_t)shape.group * NF * shape.row_stride * sizeof(double)),
-                                "workspace");
-    CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
-    CK(ensure_pinned(ctx->pin_up, in_total), "pinned workspace");
-    unsigned char* up = static_cast<unsigned char*>(ctx->pin_up.ptr);
-    std::memcpy(up + o_scale, &scale, sizeof(double));
-    std::memcpy(up + o_bank, bank.data(), bank.size() * sizeof(double));
-    std::memcpy(up + o_chunks, chunks.data(), chunks.size() * sizeof(int));
-    unsigned char* din = static_cast<unsigned char*>(ctx->pass_in.ptr);
-    unsigned char* dout = static_cast<unsigned char*>(ctx->pass_out.ptr);
-    cudaStream_t s = ctx->stream;
-    CK(cudaMemsetAsync(ctx->fault.ptr, 0, sizeof(uint32_t), s), "workspace");
-    CK(cudaMemsetAsync(dout + o_counter, 0, sizeof(uint32_t), s), "workspace");
-    CK(cudaMemcpyAsync(din, up, in_total, cudaMemcpyHostToDevice, s), "upload");
-    FoldArgs fa{};
-    fa.time = ready->time;
-    fa.v = ready->v;
-    fa.w = ready->w;
-    fa.scales = reinterpret_cast<const double*>(din + o_scale);
-    fa.n = (int)ready->n;
-    fa.nb = nb;
-    fa.periods = 1;
-    fa.group = shape.group;
-    fa.cum = as<double>(ctx->cum);
-    fa.cum32 = as<float2>(ctx->cum32);
-    fa.hist_global = shape.hist_in_smem ? nullptr : as<double>(ctx->hist);
-    fa.chunks = reinterpret_cast<const int*>(din + o_chunks);
-    fa.nchunks = count;
-    fa.stage_field = shape.stage_field;
-    fa.window = shape.window;
-    fa.row_stride = shape.row_stride;
-    fa.fault = as<uint32_t>(ctx->fault);
-    const bool timing = ctx->profile || ctx->kernel_timing;
-    if (timing) CK(cudaEventRecord(ctx->ev[0], s), "event");
-    CK(launch_fold(fa, shape, s), "fold");
-    if (timing) CK(cudaEventRecord(ctx->ev[1], s), "event");
-    const double* d_bank = reinterpret_cast<const double*>(din + o_bank);
-    EventArgs ea{};
-    ea.cum = fa.cum;
-    ea.durations = d_bank;
-    ea.rho = d_bank + nd;
-    ea.ingress = d_bank + 2 * nd;
-    ea.factors = d_bank + 2 * nd + ns;
-    ea.scale = scale;
-    ea.baseline = ready->baseline_norm;
-    ea.threshold = cfg->threshold;
-    ea.n = (double)ready->n;
-    ea.nb = nb;
-    ea.nd = (int)nd;
-    ea.ns = (int)ns;
-    ea.layers = (int)layers;
-    ea.capacity = capacity;
-    ea.counter = reinterpret_cast<uint32_t*>(dout + o_counter);
-    ea.records = reinterpret_cast<double*>(dout + o_rec);
-    CK(launch_scan_all(ea, s), "scan_all");
-    if (timing) CK(cudaEventRecord(ctx->ev[2], s), "event");
-    ctx->counters.launches += 2;
-    ctx->counters.fold_launches += 1;
-    ctx->counters.scan_launches += 1;
-    uint32_t found = 0, fault = 0;
-    CK(cudaMemcpyAsync(&found, dout + o_counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaMemcpyAsync(&fault, ctx->fault.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaStreamSynchronize(s), "single_event_search");
-    if (fault) return fail(ctx, FBLS_ERR_CUDA, "fold: staging copies did not complete");
-    if (timing) {
-        float f_ms = 0.f, s_ms = 0.f;
-        CK(cudaEventElapsedTime(&f_ms, ctx->ev[0], ctx->ev[1]), "event");
-        CK(cudaEventElapsedTime(&s_ms, ctx->ev[1], ctx->ev[2]), "event");
-        ctx->counters.fold_ms += f_ms;
-        ctx->counters.scan_ms += s_ms;
-    }
-    ctx->counters.fold_updates += ready->n;
-    if (stats) {
-        stats->templates_scanned = (uint64_t)nb * nd * ns;
-        stats->threshold_survivors = found;
-        stats->overflow = found > capacity ? 1 : 0;
-    }
-    if (found > capacity || found == 0) return FBLS_OK;
-    std::vector<double> rec((size_t)found * EVENT_RECORD);
-    CK(cudaMemcpyAsync(rec.data(), dout + o_rec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, s),
-       "download");
-    CK(cudaStreamSynchronize(s), "single_event_search");
-    std::vector<uint32_t> order(found);
-    for (uint32_t i = 0; i < found; i++) order[i] = i;
-    auto key = [&](uint32_t i) {
-        const double* r = &rec[(size_t)i * EVENT_RECORD];
-        return std::make_tuple(r[0], r[4], r[5]);
-    };
-    std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
-    for (uint32_t m = 0; m < found; m++) {
-        const double* r = &rec[(size_t)order[m] * EVENT_RECORD];
-        fbls_row& row = rows_out[m];
-        row.period = __builtin_huge_val();
-        row.epoch = (r[0] + r[1] / 2.0) / scale + ready->origin;
-        row.duration = r[1] / scale;
-        row.score = r[2];
-        row.depth = r[3];
-    }
-    *n_rows = found;
-    return FBLS_OK;
-}
-
-// biweight_flatten_gpu (src/prep/curve.rs:256-329): window bounds per
-// observation from the sorted times (segments split where the time step
-// exceeds `gap`), blocks of up to 128 observations whose windows' union fits
-// the shared-memory stage, one k_biweight launch. A window wider than the
-// stage is read from global memory by a block of its own, so every window
-// runs on the GPU (the reference sends a curve with one such window to its
-// CPU implementation, which gives the same values).
-int fbls_biweight_flatten(fbls_ctx* ctx, const double* time, const double* relative_flux, uint32_t n, double window,
-                          double gap, double c, uint32_t iterations, double* out) {
-    if (!ctx || (n && (!time || !relative_flux || !out))) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    if (n == 0) return FBLS_OK;
-    if (!(window >= 0.0) || !(gap >= 0.0)) return fail(ctx, FBLS_ERR_ARGUMENT, "window and gap must not be negative");
-    for (uint32_t i = 1; i < n; i++)
-        if (!(time[i] >= time[i - 1])) return fail(ctx, FBLS_ERR_ARGUMENT, "times must be ascending");
-    CK(cudaSetDevice(ctx->device), "set device");
-    std::vector<uint32_t> lo(n), hi(n);
-    std::vector<std::pair<uint32_t, uint32_t>> segs;
-    for (uint32_t start = 0, i = 1; i <= n; i++)
-        if (i == n || time[i] - time[i - 1] > gap) {
-            segs.push_back({start, i});
-            start = i;
-        }
-    parallel_for(segs.size(), [&](size_t sgi) {
-        const uint32_t a = segs[sgi].first, b = segs[sgi].second;
-        const double* t0 = time + a;
-        const double* t1 = time + b;
-        for (uint32_t j = a; j < b; j++) {
-            lo[j] = a + (uint32_t)(std::lower_bound(t0, t1, time[j] - window / 2.0) - t0);
-            hi[j] = a + (uint32_t)(std::upper_bound(t0, t1, time[j] + window / 2.0) - t0);
-        }
-    });
-    std::vector<uint32_t> blocks;
-    size_t smem = 0;
-    for (uint32_t first = 0; first < n;) {
-        uint32_t count = 1;
-        while (count < (uint32_t)BIWEIGHT_THREADS && first + count < n &&
-               hi[first + count] - lo[first] <= (uint32_t)BIWEIGHT_STAGE)
-            count++;
-        const uint32_t ulo = lo[first], uhi = hi[first + count - 1];
-        if (uhi - ulo <= (uint32_t)BIWEIGHT_STAGE) smem = std::max(smem, (size_t)(uhi - ulo) * sizeof(double));
-        blocks.insert(blocks.end(), {first, count, ulo, uhi});
-        first += count;
-    }
-    const size_t nblocks = blocks.size() / 4;
-    const size_t o_flux = 0, o_lo = align256((size_t)n * 8), o_hi = o_lo + align256((size_t)n * 4),
-                 o_blk = o_hi + align256((size_t)n * 4), o_out = o_blk + align256(blocks.size() * 4),
-                 total = o_out + align256((size_t)n * 8);
-    CK(ensure(ctx->pass_in, total), "workspace");
-    CK(ensure_pinned(ctx->pin_up, o_out), "pinned workspace");
-    unsigned char* up = static_cast<unsigned char*>(ctx->pin_up.ptr);
-    double* fl = reinterpret_cast<double*>(up + o_flux);
-    for (uint32_t i = 0; i < n; i++) fl[i] = 1.0 + relative_flux[i];
-    std::memcpy(up + o_lo, lo.data(), (size_t)n * 4);
-    std::memcpy(up + o_hi, hi.data(), (size_t)n * 4);
-    std::memcpy(up + o_blk, blocks.data(), blocks.size() * 4);
-    unsigned char* d = static_cast<unsigned char*>(ctx->pass_in.ptr);
-    cudaStream_t s = ctx->stream;
-    CK(cudaMemcpyAsync(d, up, o_out, cudaMemcpyHostToDevice, s), "upload");
-    BiweightArgs a{};
-    a.flux = reinterpret_cast<const double*>(d + o_flux);
-    a.lo = reinterpret_cast<const uint32_t*>(d + o_lo);
-    a.hi = reinterpret_cast<const uint32_t*>(d + o_hi);
-    a.blocks = reinterpret_cast<const uint32_t*>(d + o_blk);
-    a.c = c;
-    a.iterations = (int)iterations;
-    a.out = reinterpret_cast<double*>(d + o_out);
-    const bool timing = ctx->profile || ctx->kernel_timing;
-    if (timing) CK(cudaEventRecord(ctx->ev[0], s), "event");
-    CK(launch_biweight(a, (int)nblocks, smem, s), "biweight");
-    if (timing) CK(cudaEventRecord(ctx->ev[1], s), "event");
-    ctx->counters.launches += 1;
-    CK(cudaMemcpyAsync(out, d + o_out, (size_t)n * 8, cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaStreamSynchronize(s), "biweight");
-    if (timing) {
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]), "event");
-        ctx->counters.detrend_ms += ms;
-    }
-    return FBLS_OK;
-}
-
-// fit_segment_noise (src/prep/curve.rs:89-198) on the host: the diagonal
-// noise model of raw flux. Outputs hold up to n_in values.
-int fbls_fit_segment_noise(const double* time, const double* flux, const double* err, const int64_t* group,
-                           uint32_t n_in, double bin_minutes, double gap_days, uint32_t* n_out, double* time_out,
-                           double* deficit_out, double* variance_out, int64_t* group_out, double* scalars_out,
-                           char* error, uint32_t error_len) {
-    auto fail_msg = [&](int status, const std::string& message) {
-        if (error && error_len) {
-            std::strncpy(error, message.c_str(), error_len - 1);
-            error[error_len - 1] = '\0';
-        }
-        return status;
-    };
-    if (!time || !flux || !n_out || !time_out || !deficit_out || !variance_out || !scalars_out)
-        return fail_msg(FBLS_ERR_ARGUMENT, "null argument");
-    DiagonalNoise d;
-    std::string message;
-    if (fit_segment_noise(time, flux, err, group, n_in, bin_minutes, gap_days, d, message))
-        return fail_msg(FBLS_ERR_DATA, message);
-    const size_t n = d.time.size();
-    *n_out = (uint32_t)n;
-    std::memcpy(time_out, d.time.data(), n * sizeof(double));
-    std::memcpy(deficit_out, d.deficit.data(), n * sizeof(double));
-    std::memcpy(variance_out, d.variance.data(), n * sizeof(double));
-    if (group_out) std::memcpy(group_out, d.group.data(), n * sizeof(int64_t));
-    scalars_out[0] = d.origin;
-    scalars_out[1] = d.inflation;
-    scalars_out[2] = (double)d.segments;
-    return FBLS_OK;
-}
-
-// segment_edges and detrending_windows (curve.rs:332-370), host only.
-int fbls_segment_edges(const double* time, uint32_t n, double gap, double* out) {
-    if (n && (!time || !out)) return FBLS_ERR_ARGUMENT;
-    const std::vector<double> e = segment_edges(std::vector<double>(time, time + n), gap);
-    std::memcpy(out, e.data(), (size_t)n * sizeof(double));
-    return FBLS_OK;
-}
-
-int fbls_detrending_windows(const double* durations, uint32_t nd, double minimum, double factor, double maximum,
-                            double* windows_out, uint32_t* family_out, uint32_t* n_windows) {
-    if (!n_windows || (nd && (!durations || !windows_out || !family_out))) return FBLS_ERR_ARGUMENT;
-    const auto w = detrending_windows(durations, nd, minimum, factor, maximum);
-    for (size_t k = 0; k < w.size(); k++) {
-        windows_out[k] = w[k].first;
-        for (uint32_t i : w[k].second) family_out[i] = (uint32_t)k;
-    }
-    *n_windows = (uint32_t)w.size();
-    return FBLS_OK;
-}
-
-// prepare_families (src/prep/curve.rs:384-425): the noise model of the raw
-// flux (groups, bins of cfg->bin_minutes, gap 0.75 d), then per detrending
-// window the biweight detrend on the GPU (gap 0.5 d, c 5, 10 iterations) and
-// the curve kept where the detrended flux is finite, at most clip_sigma
-// robust scales above zero and at least edge_trim windows from a segment
-// edge.
-int fbls_prepare_families(fbls_ctx* ctx, const double* time, const double* flux, const double* err,
-                          const int64_t* group, uint32_t n, const double* durations, uint32_t nd,
-                          const fbls_prep_config* cfg, fbls_family_out* out, uint32_t* n_families) {
-    if (!ctx || !time || !flux || !durations || !cfg || !out || !n_families)
-        return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    *n_families = 0;
-    DiagonalNoise d;
-    std::string message;
-    if (fit_segment_noise(time, flux, err, group, n, cfg->bin_minutes, 0.75, d, message))
-        return fail(ctx, FBLS_ERR_DATA, message);
-    const size_t m = d.time.size();
-    std::vector<double> sigma(m), relative(m), flat(m);
-    for (size_t i = 0; i < m; i++) {
-        sigma[i] = std::sqrt(d.variance[i]);
-        relative[i] = -d.deficit[i];
-    }
-    const std::vector<double> edge = segment_edges(d.time, 0.5);
-    const auto windows = detrending_windows(durations, nd, cfg->window_min, cfg->window_factor, cfg->window_max);
-    for (size_t k = 0; k < windows.size(); k++) {
-        const double window = windows[k].first;
-        const int rc = fbls_biweight_flatten(ctx, d.time.data(), relative.data(), (uint32_t)m, window, 0.5, 5.0, 10,
-                                             flat.data());
-        if (rc) return rc;
-        const double scale = robust_scale(flat);
-        fbls_family_out& f = out[k];
-        if (!f.time || !f.flux || !f.sigma || !f.indices) return fail(ctx, FBLS_ERR_ARGUMENT, "null family buffer");
-        uint32_t kept = 0;
-        for (size_t i = 0; i < m; i++)
-            if (std::isfinite(flat[i]) && flat[i] <= cfg->clip_sigma * scale && edge[i] >= cfg->edge_trim * window) {
-                f.time[kept] = d.time[i] + d.origin;
-                f.flux[kept] = flat[i];
-                f.sigma[kept] = sigma[i];
-                kept++;
-            }
-        f.n = kept;
-        f.window_days = window;
-        f.clipped = (uint32_t)(m - kept);
-        f.n_indices = (uint32_t)windows[k].second.size();
-        std::memcpy(f.indices, windows[k].second.data(), windows[k].second.size() * sizeof(uint32_t));
-    }
-    *n_families = (uint32_t)windows.size();
-    return FBLS_OK;
-}
-
-// Peak-selection rescoring (src/select/peaks.rs:148-252 calls these): the
-// rows' box sums over an uploaded family's observations outside `excluded`,
-// and their in-transit counts over a time vector. Host arrays in and out;
-// one upload, one launch, one download each.
-int fbls_rescore_rows(fbls_ctx* ctx, const fbls_ready* family, const uint8_t* excluded, const double* rows,
-                      uint32_t R, double* sums) {
-    if (!ctx || !family || (family->n && !excluded) || (R && (!rows || !sums)))
-        return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    if (R == 0) return FBLS_OK;
-    CK(cudaSetDevice(ctx->device), "set device");
-    const size_t o_rows = 0, o_sums = align256((size_t)R * 3 * sizeof(double)),
-                 o_ex = o_sums + align256((size_t)R * 3 * sizeof(double)),
-                 total = o_ex + align256((size_t)family->n + 1);
-    CK(ensure(ctx->rescore, total), "workspace");
-    unsigned char* d = static_cast<unsigned char*>(ctx->rescore.ptr);
-    cudaStream_t s = ctx->stream;
-    CK(cudaMemcpyAsync(d + o_rows, rows, (size_t)R * 3 * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
-    if (family->n) CK(cudaMemcpyAsync(d + o_ex, excluded, family->n, cudaMemcpyHostToDevice, s), "upload");
-    RescoreArgs a{};
-    a.time = family->time;
-    a.v = family->v;
-    a.w = family->w;
-    a.excluded = d + o_ex;
-    a.rows = reinterpret_cast<const double*>(d + o_rows);
-    a.origin = family->origin;
-    a.n = (int)family->n;
-    a.R = (int)R;
-    a.sums = reinterpret_cast<double*>(d + o_sums);
-    const bool timing = ctx->profile || ctx->kernel_timing;
-    if (timing) CK(cudaEventRecord(ctx->ev[0], s), "event");
-    CK(launch_rescore_rows(a, s), "rescore_rows");
-    if (timing) CK(cudaEventRecord(ctx->ev[1], s), "event");
-    ctx->counters.launches += 1;
-    ctx->counters.rescore_launches += 1;
-    CK(cudaMemcpyAsync(sums, d + o_sums, (size_t)R * 3 * sizeof(double), cudaMemcpyDeviceToHost, s), "download");
-    CK(cudaStreamSynchronize(s), "rescore_rows");
-    if (timing) {
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]), "event");
-        ctx->counters.rescore_ms += ms;
-    }
-    return FBLS_OK;
-}
-
-int fbls_count_rows(fbls_ctx* ctx, const double* time, uint32_t n, const uint8_t* excluded, const double* rows,
-                    uint32_t R, uint32_t* counts) {
-    if (!ctx || (n && (!time || !excluded)) || (R && (!rows || !counts)))
-        return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    for (uint32_t i = 1; i < n; i++)
-        if (!(time[i] >= time[i - 1])) return fail(ctx, FBLS_ERR_ARGUMENT, "times must be ascending");
-    if (R == 0) return FBLS_OK;
-    CK(cudaSetDevice(ctx->device), "set device");
-    const size_t o_rows = 0, o_counts = align256((size_t)R * 3 * sizeof(double)),
-                 o_time = o_counts + align256((size_t)R * 2 * sizeof(uint32_t)),
-                 o_ex = o_time + align256((size_t)n * sizeof(double) + 8), total = o_ex + align256((size_t)n + 1);
-    CK(ensure(ctx->rescore, total), "workspace");
-    unsigned char* d = static_cast<unsigned char*>(ctx->rescore.ptr);
-    cudaStream_t s = ctx->stream;
-    CK(cudaMemcpyAsync(d + o_rows, rows, (size_t)R * 3 * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
-    if (n) {
-        CK(cudaMemcpyAsync(d + o_time, time, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
-        CK(cudaMemcpyAsync(d + o_ex, excluded, n, cudaMemcpyHostToDevice, s), "upload");
-    }
-    RescoreArgs a{};
-    a.time = reinterpret_cast<const double*>(d + o_time);
-    a.excluded = d + o_ex;
-    a.rows = reinterpret_cast<const double*>(d + o_rows);
-    a.n = (int)n;
-    a.R = (int)R;
-    a.counts = reinterpret_cast<uint32_t*>(d + o_counts);
-    const bool timing = ctx->profile || ctx->kernel_timing;
-    if (timing) CK(cudaEventRecord(ctx->ev[0], s), "event");
-    CK(launch_count_rows(a, s), "count_rows");
-    if (timing) CK(cudaEventRecord(ctx->ev[1], s), "event");
-    ctx->counters.launches += 1;
-    ctx->counters.rescore_launches += 1;
-    CK(cudaMemcpyAsync(counts, d + o_counts, (size_t)R * 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
-       "download");
-    CK(cudaStreamSynchronize(s), "count_rows");
-    if (timing) {
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]), "event");
-        ctx->counters.rescore_ms += ms;
-    }
-    return FBLS_OK;
-}
-
-}  // extern "C"
-
-extern "C" {
-
-// Coarse maps of many uploaded families (the proposal path's first step for a
-// batch of stars): on the batch worker contexts, or with workers == 0 planned
-// in parallel and run together as job launches on ctx (coarse_maps).
-int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uint32_t workers) {
-    if (!ctx || (count && !jobs)) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    if (count == 0) return FBLS_OK;
-    CK(cudaSetDevice(ctx->device), "set device");
-    if (workers == 0) {
-        std::vector<std::string> errors(count);
-        const int rc = coarse_maps(ctx, jobs, count, errors);
-        if (rc) return rc;
-        for (uint32_t i = 0; i < count; i++)
-            if (jobs[i].status) return fail(ctx, jobs[i].status, "map " + std::to_string(i) + ": " + errors[i]);
-        return FBLS_OK;
-    }
-    workers = std::min({workers, count, 64u});
-    while (ctx->workers.size() < workers) {
-        int status = FBLS_OK;
-        fbls_ctx* w = fbls_create(ctx->device, &status);
-        if (!w) return fail(ctx, status ? status : FBLS_ERR_CUDA, "batch worker context");
-        ctx->workers.push_back(w);
-    }
-    std::atomic<uint32_t> next{0};
-    std::vector<std::string> errors(count);
-    auto work = [&](fbls_ctx* wc) {
-        if (cudaSetDevice(wc->device) != cudaSuccess) return;
-        for (;;) {
-            const uint32_t i = next.fetch_add(1);
-            if (i >= count) break;
-            fbls_map_job& j = jobs[i];
-            j.status = fbls_coarse_map(wc, j.ready, j.periods, j.P, j.durations, j.rho, j.nd, j.oversample,
-                                       j.bin_days, j.out);
-            if (j.status) errors[i] = wc->error;
-        }
-    };
-    std::vector<std::thread> threads;
-    for (uint32_t k = 1; k < workers; k++) threads.emplace_back(work, ctx->workers[k]);
-    work(ctx->workers[0]);
-    for (std::thread& t : threads) t.join();
-    for (uint32_t i = 0; i < count; i++)
-        if (jobs[i].status) return fail(ctx, jobs[i].status, "map " + std::to_string(i) + ": " + errors[i]);
-    return FBLS_OK;
-}
-
-
-// The proposal network's input for a batch of stars (coarse_maps with
-// k_map_features): rows of x (channels x count x T) hold each map's
-// standardised log1p channels at [offsets[i], offsets[i] + P_i).
-int fbls_coarse_features(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, const uint32_t* offsets,
-                         uint32_t channels, uint32_t T, float* x) {
-    if (!ctx || (count && (!jobs || !offsets || !x))) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    if (channels < 1 || channels > (uint32_t)MAP_MAX_DURATIONS || T < 1)
-        return fail(ctx, FBLS_ERR_ARGUMENT, "1 to 8 channels and T >= 1");
-    if (count == 0) return FBLS_OK;
-    for (uint32_t i = 0; i < count; i++)
-        if (jobs[i].nd != channels || (uint64_t)offsets[i] + jobs[i].P > T)
-            return fail(ctx, FBLS_ERR_ARGUMENT, "map " + std::to_string(i) + ": does not fit its feature row");
-    CK(cudaSetDevice(ctx->device), "set device");
-    const size_t bytes = (size_t)channels * count * T * sizeof(float);
-    CK(ensure(ctx->feat, bytes), "workspace");
-    CK(cudaMemsetAsync(ctx->feat.ptr, 0, bytes, ctx->stream), "workspace");
-    MapFeatures feat;
-    feat.x = as<float>(ctx->feat);
-    feat.channels = (int)channels;
-    feat.B = (int)count;
-    feat.T = (int)T;
-    feat.offsets = offsets;
-    std::vector<std::string> errors(count);
-    const int rc = coarse_maps(ctx, jobs, count, errors, &feat);
-    if (rc) return rc;
-    for (uint32_t i = 0; i < count; i++)
-        if (jobs[i].status) return fail(ctx, jobs[i].status, "map " + std::to_string(i) + ": " + errors[i]);
-    CK(cudaMemcpyAsync(x, ctx->feat.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download");
-    CK(cudaStreamSynchronize(ctx->stream), "map features");
-    return FBLS_OK;
-}
-
 }  // extern "C"
