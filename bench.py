@@ -97,17 +97,23 @@ def _l2_copy_peak(device: str, copies: int = 32, reps: int = 10):
     return best, best_mib
 
 
-def _workload(name):
+def _workload(name, period_oversample=None):
+    """(curve, config, description) of a single-star workload; a
+    `period_oversample` other than the configuration's 3 gives the denser-grid
+    variants (6.9 on single_sector: ~30k periods; 19 on multi_sector: ~1.2M)."""
     from fbls_b200 import synth
     if name == "single_sector":
         c, cfg = synth.single_sector(), synth.single_sector_config()
         desc = ("single_sector: 1 x 27.4 d sector at 120 s with a 1 d gap (19,008 points), 12 durations 0.5-12 h, "
-                "periods 0.5-13.7 d at period_oversample 3")
+                "periods 0.5-13.7 d at period_oversample {os:g}")
     else:
         c, cfg = synth.multi_sector(), synth.multi_sector_config()
         desc = ("multi_sector: 13 x 27.4 d sectors at 120 s with a 1 d gap each (247,104 points), white 8e-4 + AR(1) "
-                "(0.95, 3e-4), 400 ppm box at 17.3 d; 20 durations 0.5-15 h, periods 0.5-20 d at period_oversample 3")
-    return c, cfg, desc
+                "(0.95, 3e-4), 400 ppm box at 17.3 d; 20 durations 0.5-15 h, periods 0.5-20 d at "
+                "period_oversample {os:g}")
+    if period_oversample is not None:
+        cfg.period_oversample = float(period_oversample)
+    return c, cfg, desc.format(os=cfg.period_oversample)
 
 
 class Clocks:
@@ -220,7 +226,7 @@ def run_reference(args):
     world, rank, local = _dist()
     if rank != 0:
         return
-    curve, cfg, desc = _workload(args.workload)
+    curve, cfg, desc = _workload(args.workload, args.period_oversample)
     st, every, threads, trials, sec = _cpu_sample(curve, cfg, args.cpu_seconds / 2)
     for _ in range(args.warmup):
         _oracle_sample(st, cfg, every, threads)
@@ -255,7 +261,7 @@ def run_gpu(args):
     torch.cuda.set_device(local)
     from fbls_b200 import api
 
-    curve, cfg, desc = _workload(args.workload)
+    curve, cfg, desc = _workload(args.workload, args.period_oversample)
     state = api.prepared_family(curve.time, curve.flux, curve.flux_err, cfg)
     gpu = api.Gpu(local)
     dev = gpu.upload(state)
@@ -321,7 +327,7 @@ def run_gpu(args):
     # workload (measured once, not in this run).
     traffic = None
     prof = ROOT / "profiles" / "fold_traffic.json"
-    if prof.exists():
+    if prof.exists() and args.period_oversample is None:  # captured on the default grid
         try:
             traffic = json.loads(prof.read_text()).get(args.workload)
         except (OSError, ValueError):
@@ -335,11 +341,13 @@ def run_gpu(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": desc, "stars": world, "periods": int(glen), "bands": len(bands),
-                   "observations": state.n, "l2": "flushed between steps (256 MiB write)",
+                   "observations": state.n, "period_oversample": cfg.period_oversample,
+                   "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "stars_per_s": world * args.steps / (total_ms * 1e-3),
         "step_ms": [round(t, 2) for t in times],
         "trials_per_step": trials / args.steps / world,
+        "box_trials_per_s": value / len(cfg.ingress_fractions),
         "rows_per_step": int(len(rows)),
         "gpu_launches": int(ctr["launches"]),
         "kernel_ms": {"fold_prefix": ctr["fold_ms"] / args.steps, "scan_tiles+merge": ctr["scan_ms"] / args.steps},
@@ -760,7 +768,7 @@ def run_precision_report(args):
     the coarse and the full nb: how often the winning template differs, and
     the relative error of the reported power (score) and depth."""
     from fbls_b200 import api
-    curve, cfg, desc = _workload(args.workload)
+    curve, cfg, desc = _workload(args.workload, args.period_oversample)
     state = api.prepared_family(curve.time, curve.flux, curve.flux_err, cfg)
     grid, bands = api.band_plan(state, cfg)
     out = {"report": "precision", "workload": desc, "passes": []}
@@ -836,6 +844,9 @@ def main():
                     help="survey / proposal workloads: search_batch host worker threads (0: stars fused into "
                          "job launches)")
     ap.add_argument("--bands", type=int, default=1, help="proposal workload: log-period bands searched per star")
+    ap.add_argument("--period-oversample", type=float, default=None,
+                    help="single-star workloads: period grid density (default 3; 19 gives multi_sector's ~1.2M "
+                         "periods, 6.9 single_sector's ~30k)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
