@@ -19,7 +19,9 @@ property (grid.rs:34-42), noise-model / transit-mask tests
 has no golden vectors for the fold, prefix, tile-scan, evidence, rescoring,
 single-event or detrend outputs; those are checked here by brute-force
 identities and literal loop restatements only (parity unpinned against
-reference output).
+reference output). The oracle's own outputs on seeded small inputs are frozen
+in tests/golden/ (tests/golden/make_golden.py), where the CPU tests pin the
+oracle and the GPU tests hold the CUDA path to the same files.
 """
 from __future__ import annotations
 
