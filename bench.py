@@ -59,6 +59,30 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _bf16_peak():
+    """Dense bf16 tensor peak (TFLOP/s): the burst figure of MEASURED_PEAKS.json,
+    else this pool's earlier measurement."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def _network_flops(curves: int) -> int:
+    """Forward FLOPs of the proposal network over `curves` coarse maps: the
+    convolutions' GEMMs, 2 x CH x (ci x KW) x T per layer (bias, ReLU, pooling
+    and the head are not counted)."""
+    from fbls_b200 import proposal as pr
+    flops, t, ci = 0, pr.T_IN, pr.MAP_CHANNELS
+    for pool in pr.POOLS:
+        flops += 2 * pr.CH * ci * pr.KW * t
+        t //= pool
+        ci = pr.CH
+    return flops * curves
+
+
 def _l2_copy_peak(device: str, copies: int = 32, reps: int = 10):
     """The copy rate (read + write bytes per second, GB/s) of a buffer pair
     that stays in L2, measured here: the same STREAM-style copy as the HBM
@@ -544,6 +568,15 @@ def run_proposal(args):
         "step_ms": {"exhaustive": [round(1e3 * t, 1) for t in t_ex], "proposal": [round(1e3 * t, 1) for t in t_pr]},
         "proposal_ms_last_step": {k: round(v, 1) for k, v in parts.items()},
     }
+    tpeak, tkind = _bf16_peak()
+    net_s = parts.get("network", 0.0) * 1e-3
+    if net_s > 0:
+        achieved = _network_flops(args.stars) / net_s / 1e12
+        out["network_roofline"] = {
+            "kernel": "k_gemm_bf16 (the network's convolutions, forward)", "bound": "tensor",
+            "achieved": achieved, "peak": tpeak, "peak_kind": tkind, "unit": "TFLOP/s", "frac": achieved / tpeak,
+            "flops_per_curve": _network_flops(1),
+            "note": "host clock around the band scores of the last step (feature upload, forward, logits download)"}
     print(json.dumps(out))
     for d in devs:
         d.free()
