@@ -101,6 +101,8 @@ def period_grid(minimum: float, maximum: float, baseline: float, minimum_duratio
                 oversample: float) -> np.ndarray:
     lib = N.load()
     count = lib.fbls_period_grid(minimum, maximum, baseline, minimum_duration, oversample, None, 0)
+    if count < 0:
+        raise FblsError(1, "the period grid is infinite or too large")
     out = np.empty(count, dtype=np.float64)
     lib.fbls_period_grid(minimum, maximum, baseline, minimum_duration, oversample, _dptr(out), count)
     return out

@@ -865,6 +865,15 @@ int plan_star_bands(std::string& err, const fbls_ready* ready, const double* dur
         err = "no durations";
         return FBLS_ERR_ARGUMENT;
     }
+    if (!durations || !rho || !cfg) {
+        err = "null argument";
+        return FBLS_ERR_ARGUMENT;
+    }
+    for (uint32_t i = 0; i < nd; i++)
+        if (!(durations[i] > 0.0) || !std::isfinite(durations[i])) {
+            err = "durations must be positive and finite";
+            return FBLS_ERR_ARGUMENT;
+        }
     auto kept = [&](double p) {
         if (!n_ranges) return true;
         for (uint32_t i = 0; i < n_ranges; i++)
@@ -880,6 +889,10 @@ int plan_star_bands(std::string& err, const fbls_ready* ready, const double* dur
     const double minimum = rmax(cfg->period_min, 4.0 * ds[0].first * (1.0 + 1e-9));
     if (maximum <= minimum) return FBLS_OK;
     const int64_t count = period_grid(minimum, maximum, baseline, ds[0].first, cfg->period_oversample, nullptr, 0);
+    if (count < 1) {
+        err = "the period grid is infinite or too large";
+        return FBLS_ERR_ARGUMENT;
+    }
     std::vector<double> grid((size_t)count);
     period_grid(minimum, maximum, baseline, ds[0].first, cfg->period_oversample, grid.data(), count);
     sb.grid_len = (uint64_t)count;
@@ -1230,6 +1243,14 @@ int fbls_family_state(const double* time, const double* flux, const double* sigm
                       const double* durations, uint32_t nd, int correlated, uint32_t* n_out, double* time_out,
                       double* v_out, double* w_out, double* scalars_out, double* rho_out, char* error,
                       uint32_t error_len) {
+    if (!time || !flux || !sigma || (nd && !durations) || !n_out || !time_out || !v_out || !w_out || !scalars_out ||
+        (nd && !rho_out)) {
+        if (error && error_len) {
+            std::strncpy(error, "null argument", error_len - 1);
+            error[error_len - 1] = '\0';
+        }
+        return FBLS_ERR_ARGUMENT;
+    }
     PreparedFamily fam;
     std::string message;
     int rc = prepare_family(time, flux, sigma, n_in, durations, nd, correlated != 0, fam, message);

@@ -370,6 +370,11 @@ int64_t period_grid(double minimum, double maximum, double baseline, double mini
                     double* out, int64_t capacity) {
     const double log_step = std::log1p(minimum_duration / (oversample * baseline));
     const double c = std::ceil(std::log(maximum / minimum) / log_step);
+    // An infinite quotient (a zero minimum or a zero step) saturates the
+    // reference's count (grid.rs:12), which then fails to allocate or index
+    // the grid; such grids, and any above 2^53 periods, are refused here.
+    // A NaN or negative quotient gives one period, as there.
+    if (c >= 9007199254740992.0) return -1;
     const int64_t count = (c > 0.0 ? (int64_t)c : 0) + 1;
     if (out == nullptr || capacity < count) return count;
     const double a = std::log(minimum), b = std::log(maximum);

@@ -237,7 +237,9 @@ int fbls_read_counters(fbls_ctx* ctx, fbls_counters* out, int reset);
 /* ---- host-side mirror ------------------------------------------------- */
 
 /* period_grid (grid.rs:5-28). Returns the count; writes it when capacity
- * suffices (out may be NULL to query the count). */
+ * suffices (out may be NULL to query the count). Returns -1 when the count
+ * is infinite (a zero minimum period or a zero step) or above 2^53, grids the
+ * reference cannot allocate either. */
 int64_t fbls_period_grid(double minimum, double maximum, double baseline, double minimum_duration,
                          double oversample, double* out, int64_t capacity);
 
@@ -245,7 +247,8 @@ int64_t fbls_period_grid(double minimum, double maximum, double baseline, double
  * fit_segment_noise at bin 0, prepare_ready, correlated_noise_factors).
  * out arrays hold n_in entries; *n_out is the usable count. scalars_out:
  * baseline_norm, origin, residual_energy, inflation, segments. Status
- * FBLS_ERR_DATA with the reference's message on bad input. */
+ * FBLS_ERR_DATA with the reference's message on bad input, FBLS_ERR_ARGUMENT
+ * ("null argument") for a null array. */
 int fbls_family_state(const double* time, const double* flux, const double* sigma, uint32_t n_in,
                       const double* durations, uint32_t nd, int correlated, uint32_t* n_out, double* time_out,
                       double* v_out, double* w_out, double* scalars_out, double* rho_out, char* error,
@@ -254,7 +257,9 @@ int fbls_family_state(const double* time, const double* flux, const double* sigm
 /* signal_search (scan.rs:413-473) for one family: octave bands over the
  * family's grid. At most `capacity` rows are written to rows_out and
  * *n_rows is the number found (more than capacity: ask again with room for
- * all; the grid length always suffices); stats_out holds up to 64 bands. */
+ * all; the grid length always suffices); stats_out holds up to 64 bands.
+ * Durations must be positive and finite (FBLS_ERR_ARGUMENT otherwise, as for
+ * a period grid that is infinite or too large). */
 int fbls_signal_search(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
                        uint32_t nd, const fbls_config* cfg, fbls_row* rows_out, uint32_t capacity,
                        uint32_t* n_rows, uint64_t* grid_len, fbls_scan_stats* stats_out, uint32_t* n_bands);

@@ -5,7 +5,8 @@
  * short buffer), the segment edges and detrending windows of the
  * reference's own test cases (src/prep/curve.rs:609-622), the prepared
  * family state of the noise-model test's series (curve.rs:636-661) and its
- * error path with the reference's message, and context creation, which
+ * error paths (the reference's message; a null array), the refusal of an
+ * infinite period grid, and context creation, which
  * without a visible CUDA device must fail with FBLS_ERR_CUDA and a NULL
  * context rather than abort. Prints one JSON object; exits nonzero when a
  * check failed. */
@@ -85,6 +86,11 @@ int main(void) {
                                         sizeof error);
     CHECK(data_status == FBLS_ERR_DATA);
     CHECK(strcmp(error, "insufficient usable observations") == 0);
+    char null_error[32] = "";
+    CHECK(fbls_family_state(NULL, f, e, N, durations, 2, 1, &n_out, to, vo, wo, scalars, rho, null_error,
+                            sizeof null_error) == FBLS_ERR_ARGUMENT);
+    CHECK(strcmp(null_error, "null argument") == 0);
+    CHECK(fbls_period_grid(0.0, 20.0, 50.0, 0.02, 3.0, NULL, 0) == -1); /* infinite grid */
 
     /* context creation */
     int status = -1;

@@ -2,6 +2,7 @@
 declares, and its host-side code (period grid, prepared-mode family state,
 configuration) matches the oracle exactly. No GPU calls."""
 import ctypes
+import math
 import re
 from pathlib import Path
 
@@ -103,3 +104,24 @@ def test_band_plan_matches_oracle():
     # The reference's rule at this configuration: 13,065 periods, nb 192 ... 2631.
     assert grid.shape[0] == 13065
     assert [b["nb"] for b in bands] == [192, 384, 768, 1536, 2631]
+
+
+def test_period_grid_refuses_infinite_grids_and_keeps_the_reference_edge_cases():
+    lib = _native.load()
+    # infinite counts: a zero minimum period, a zero minimum duration (zero step), an infinite maximum
+    for args in [(0.0, 20.0, 50.0, 0.02, 3.0), (0.5, 20.0, 50.0, 0.0, 3.0), (0.5, math.inf, 50.0, 0.02, 3.0),
+                 (1e-9, 1e9, 1e9, 1e-12, 1e6)]:
+        assert lib.fbls_period_grid(*args, None, 0) == -1, args
+        with pytest.raises(api.FblsError, match="infinite or too large"):
+            api.period_grid(*args)
+    # a reversed range or a NaN bound gives one period (the reference's saturating count), the maximum
+    for args in [(20.0, 0.5, 50.0, 0.02, 3.0), (math.nan, 20.0, 50.0, 0.02, 3.0)]:
+        g = api.period_grid(*args)
+        assert g.shape == (1,) and g[0] == args[1]
+
+
+def test_family_state_rejects_null_arrays():
+    lib = _native.load()
+    err = ctypes.create_string_buffer(64)
+    rc = lib.fbls_family_state(None, None, None, 10, None, 0, 1, None, None, None, None, None, None, err, 64)
+    assert rc == 1 and err.value == b"null argument"
