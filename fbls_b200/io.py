@@ -29,6 +29,29 @@ class Array:
 _NPY_KINDS = {"f8": "f8", "f4": "f4", "i8": "i8", "i4": "i4", "i2": "i2", "u1": "u1", "b1": "u1"}
 
 
+def _usize(text: str) -> int:
+    """A non-negative integer as the reference's usize parse reads it: an
+    optional '+' and ASCII digits, below 2^64; its error texts otherwise."""
+    digits = text[1:] if text.startswith("+") else text
+    if not digits:
+        raise ValueError("cannot parse integer from empty string")
+    if not (digits.isascii() and digits.isdigit()):
+        raise ValueError("invalid digit found in string")
+    value = int(digits)
+    if value >= 1 << 64:
+        raise ValueError("number too large to fit in target type")
+    return value
+
+
+def _i64(text: str) -> Optional[int]:
+    """A signed integer as the reference's i64 parse reads it (None where it fails)."""
+    sign, digits = (-1, text[1:]) if text.startswith("-") else (1, text[1:] if text.startswith("+") else text)
+    if not digits or not (digits.isascii() and digits.isdigit()):
+        return None
+    value = sign * int(digits)
+    return value if -(1 << 63) <= value < (1 << 63) else None
+
+
 def _header_value(header: str, key: str) -> Optional[str]:
     """The text after `key` up to the next comma (npz.rs:92-96)."""
     parts = header.split(key, 1)
@@ -44,6 +67,8 @@ def parse_npy(data: bytes) -> Array:
     i2, u1 and b1 in either byte order; C order only."""
     if len(data) < 10 or data[:6] != b"\x93NUMPY":
         raise ValueError("not an NPY file")
+    if data[6] != 1 and len(data) < 12:
+        raise ValueError("truncated NPY header")
     if data[6] == 1:
         header_len, offset = struct.unpack("<H", data[8:10])[0], 10
     else:
@@ -59,8 +84,8 @@ def parse_npy(data: bytes) -> Array:
     if len(parts) < 2 or "(" not in parts[1] or ")" not in parts[1]:
         raise ValueError("NPY header without shape")
     inner = parts[1].split("(", 1)[1].split(")", 1)[0]
-    shape = tuple(int(s) for s in (x.strip() for x in inner.split(",")) if s)
-    count = 1 if not shape else int(np.prod(shape))
+    shape = tuple(_usize(s) for s in (x.strip() for x in inner.split(",")) if s)
+    count = math.prod(shape)  # exact; 1 for a scalar
     descr = descr.strip("'\"")
     little = not descr.startswith(">")
     kind = descr[1:]
@@ -106,17 +131,16 @@ class Header:
 
     def f64(self, key: str) -> Optional[float]:
         v = self.get(key)
+        if v is None or "_" in v:  # the reference's f64 parse takes no digit separators
+            return None
         try:
-            return float(v.strip()) if v is not None else None
+            return float(v.strip())
         except ValueError:
             return None
 
     def i64(self, key: str) -> Optional[int]:
         v = self.get(key)
-        try:
-            return int(v.strip()) if v is not None else None
-        except ValueError:
-            return None
+        return None if v is None else _i64(v.strip())
 
     def text(self, key: str) -> Optional[str]:
         v = self.get(key)
@@ -221,12 +245,19 @@ def read_fits(path: str) -> List[Hdu]:
         bitpix = header.i64("BITPIX")
         bitpix = 8 if bitpix is None else bitpix
         naxis = header.i64("NAXIS") or 0
+        if not 0 <= naxis <= 999:
+            raise ValueError(f"{path}: invalid NAXIS {naxis}")
         naxes = [header.i64(f"NAXIS{i}") or 0 for i in range(1, naxis + 1)]
-        size = 0 if naxis == 0 else int(np.prod(naxes)) * (abs(bitpix) // 8)
-        size += header.i64("PCOUNT") or 0
+        pcount = header.i64("PCOUNT") or 0
         name = header.text("EXTNAME")
         if name is None:
             name = "PRIMARY" if not hdus else ""
+        if any(n < 0 for n in naxes) or pcount < 0:
+            # the reference reads these as usize: a negative value wraps to a
+            # unit larger than any file
+            raise ValueError(f"{path}: truncated data unit {name}")
+        size = 0 if naxis == 0 else math.prod(naxes) * (abs(bitpix) // 8)
+        size += pcount
         columns, rows, row_bytes = [], 0, 0
         if header.text("XTENSION") == "BINTABLE":
             row_bytes = naxes[0] if naxes else 0
@@ -240,9 +271,9 @@ def read_fits(path: str) -> List[Hdu]:
                     raise ValueError("empty TFORM")
                 code = form[-1]
                 try:
-                    repeat = int(form[:-1]) if form[:-1] else 1
+                    repeat = _usize(form[:-1])
                 except ValueError:
-                    repeat = 1
+                    repeat = 1  # parse().unwrap_or(1), fits.rs
                 if code not in _WIDTH:
                     raise ValueError(f"unsupported FITS column type {code}")
                 columns.append(Column(header.text(f"TTYPE{i}") or "", code, repeat, offset, _WIDTH[code]))

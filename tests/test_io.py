@@ -1,7 +1,9 @@
 """Input formats (src/io/npz.rs, src/io/fits.rs, read_inputs src/main.rs:50-132)
 on the CPU: NPZ members of every supported dtype and byte order, the
-reference's FITS binary-table and TAN-projection known-answer tests, and
-the grouping of several inputs."""
+reference's FITS binary-table and TAN-projection known-answer tests, the
+grouping of several inputs, and malformed files (negative or oversized units,
+axis counts, shapes; integers, repeats and headers the reference's parses
+refuse), which must raise ValueError promptly instead of looping or wrapping."""
 import math
 import struct
 
@@ -87,3 +89,70 @@ def test_read_inputs_groups_files_and_sectors(tmp_path):
     with pytest.raises(ValueError, match="either provide flux_err or omit it"):
         io.read_inputs([str(a), str(c)])
     assert io.read_inputs([str(c)]).err is None
+
+
+def _table(cards, data=b""):
+    primary = _pad(b"".join(_card(k, v) for k, v in [("SIMPLE", "T"), ("BITPIX", "8"), ("NAXIS", "0")])
+                   + b"END".ljust(80), b" ")
+    ext = _pad(b"".join(_card(k, v) for k, v in cards) + b"END".ljust(80), b" ")
+    return primary + ext + _pad(data, b"\0")
+
+
+@pytest.mark.timeout(20)
+@pytest.mark.parametrize("cards,message", [
+    ([("XTENSION", "'BINTABLE'"), ("BITPIX", "8"), ("NAXIS", "2"), ("NAXIS1", "8"), ("NAXIS2", "1"),
+      ("PCOUNT", "-5760")], "truncated data unit"),       # would move the next header backwards
+    ([("XTENSION", "'BINTABLE'"), ("BITPIX", "8"), ("NAXIS", "2"), ("NAXIS1", "8"), ("NAXIS2", "-1")],
+     "truncated data unit"),
+    ([("XTENSION", "'BINTABLE'"), ("BITPIX", "8"), ("NAXIS", "2"), ("NAXIS1", "4294967296"),
+      ("NAXIS2", "4294967296")], "truncated data unit"),   # 2^64 bytes: no integer wrap
+    ([("XTENSION", "'IMAGE'"), ("BITPIX", "8"), ("NAXIS", "1000000000")], "invalid NAXIS"),
+    ([("XTENSION", "'IMAGE'"), ("BITPIX", "8"), ("NAXIS", "-3")], "invalid NAXIS"),
+])
+def test_fits_malformed_sizes_fail_cleanly(tmp_path, cards, message):
+    path = tmp_path / "bad.fits"
+    path.write_bytes(_table(cards, b"\0" * 8))
+    with pytest.raises(ValueError, match=message):
+        io.read_fits(str(path))
+
+
+def test_fits_integers_and_repeats_parse_as_the_reference():
+    h = io.Header([("A", "1_0"), ("B", "+7"), ("C", "-7"), ("D", "9223372036854775808"), ("E", "1_0.5"),
+                   ("F", "2.5E3"), ("G", "٣")])
+    assert h.i64("A") is None and h.i64("B") == 7 and h.i64("C") == -7 and h.i64("D") is None
+    assert h.i64("G") is None
+    assert h.f64("E") is None and h.f64("F") == 2500.0
+
+
+def test_fits_tform_repeat_falls_back_to_one(tmp_path):
+    cards = [("XTENSION", "'BINTABLE'"), ("BITPIX", "8"), ("NAXIS", "2"), ("NAXIS1", "8"), ("NAXIS2", "1"),
+             ("PCOUNT", "0"), ("TFIELDS", "2"), ("TTYPE1", "'A'"), ("TFORM1", "'1_0E'"), ("TTYPE2", "'B'"),
+             ("TFORM2", "'-2E'")]
+    path = tmp_path / "r.fits"
+    path.write_bytes(_table(cards, struct.pack(">ff", 1.5, 2.5)))
+    t = io.read_fits(str(path))[1]
+    assert [c.repeat for c in t.columns] == [1, 1]
+    assert t.column_f64("A").tolist() == [1.5] and t.column_f64("B").tolist() == [2.5]
+
+
+def _npy(header: str, body: bytes, version: int = 1) -> bytes:
+    h = header.encode()
+    if version == 1:
+        return b"\x93NUMPY\x01\x00" + struct.pack("<H", len(h)) + h + body
+    return b"\x93NUMPY\x02\x00" + struct.pack("<I", len(h)) + h + body
+
+
+def test_npy_malformed_shapes_and_headers_fail_cleanly():
+    body = struct.pack("<3d", 1.0, 2.0, 3.0)
+    with pytest.raises(ValueError, match="invalid digit found in string"):
+        io.parse_npy(_npy("{'descr': '<f8', 'fortran_order': False, 'shape': (-1,), }", body))
+    with pytest.raises(ValueError, match="truncated NPY body"):
+        io.parse_npy(_npy("{'descr': '<f8', 'fortran_order': False, 'shape': (4294967296, 4294967296), }", body))
+    with pytest.raises(ValueError, match="number too large"):
+        io.parse_npy(_npy("{'descr': '<f8', 'fortran_order': False, 'shape': (18446744073709551616,), }", body))
+    with pytest.raises(ValueError, match="truncated NPY header"):
+        io.parse_npy(b"\x93NUMPY\x02\x00\x10\x00")
+    a = io.parse_npy(_npy("{'descr': '<f8', 'fortran_order': False, 'shape': (3,), }", body, version=2))
+    assert a.shape == (3,) and a.data.tolist() == [1.0, 2.0, 3.0]
+    s = io.parse_npy(_npy("{'descr': '<f8', 'fortran_order': False, 'shape': (), }", body))
+    assert s.shape == () and s.data.tolist() == [1.0]
