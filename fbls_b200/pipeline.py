@@ -275,6 +275,8 @@ def run_search(argv: Sequence[str]) -> int:
         if a == "--prepared":
             prepared = True
         elif a in ("--output", "--save-table", "--device", "--pmin", "--pmax", "--prescan", "--threshold"):
+            if i + 1 >= len(argv):
+                raise ValueError(f"{a} needs a value")  # the reference indexes past the end and panics
             v = argv[i + 1]
             i += 1
             if a == "--output":

@@ -7,6 +7,7 @@ import json
 import types
 
 import numpy as np
+import pytest
 
 import oracle
 from fbls_b200 import io, pipeline, synth
@@ -74,3 +75,18 @@ def test_raw_search_on_the_oracle():
     report = pipeline.search_transits(_OracleGpu(), obs, cfg)
     _check(report, c, "raw")
     assert report["statistics"]["passes"][0]["families"][0]["window_days"] == 0.4
+
+
+@pytest.mark.parametrize("argv,message", [
+    ([], "usage: python -m fbls_b200 search"),
+    (["search"], "--input is required"),
+    (["search", "--input", "a.npz", "--output"], "--output needs a value"),
+    (["search", "--input", "a.npz", "--pmin", "x"], "could not convert"),
+    (["search", "--input", "a.npz", "--bogus"], "unknown argument --bogus"),
+    (["search", "--input", "missing.npz"], "missing.npz"),
+])
+def test_search_command_errors_exit_1_with_a_message(argv, message, capsys, tmp_path, monkeypatch):
+    from fbls_b200 import pipeline
+    monkeypatch.chdir(tmp_path)
+    assert pipeline.main(argv) == 1
+    assert message in capsys.readouterr().err
