@@ -110,3 +110,30 @@ def test_npy_round_trip(dtype, shape, seed):
 def test_detrending_window_halves_round_away_from_zero():
     # 1.03125 x 0.25 d = 0.2578125 d: 257812.5 micro-days rounds to 257813, as Rust's f64::round does
     assert api.detrending_windows([0.25], 0.25, 1.03125, 1.25)[0][0] == 0.257813
+
+
+@SETTINGS
+@given(seed=st.integers(0, 2**31 - 1), n=st.integers(2, 600), sectors=st.integers(1, 3),
+       bin_minutes=st.sampled_from([0.0, 0.0, 2.0, 10.0, 30.0]), with_err=st.booleans(),
+       nan_frac=st.floats(0.0, 0.2), gap=st.floats(0.1, 1.5))
+def test_noise_fit_matches_the_oracle_on_random_raw_curves(seed, n, sectors, bin_minutes, with_err, nan_frac, gap):
+    rng = np.random.default_rng(seed)
+    t = 1000.0 + np.cumsum(rng.uniform(0.2, 1.8, n) * (2.0 / 1440.0))
+    sec = np.sort(rng.integers(0, sectors, n)).astype(np.int64) + 5
+    t += (sec - 5) * 30.0
+    level = 1e4 * (1.0 + 0.1 * (sec - 5))
+    flux = level * (1.0 + rng.normal(0.0, 1e-3, n))
+    flux[rng.uniform(size=n) < nan_frac] = np.nan
+    err = level * rng.uniform(5e-4, 2e-3, n) if with_err else None
+    try:
+        want = oracle.fit_segment_noise_raw(t, flux, err, sec, bin_minutes, gap)
+    except ValueError as e:
+        with pytest.raises(api.FblsError, match=str(e)):
+            api.fit_segment_noise(t, flux, err, sec, bin_minutes, gap)
+        return
+    got = api.fit_segment_noise(t, flux, err, sec, bin_minutes, gap)
+    assert np.array_equal(got.time, want[0])
+    assert np.array_equal(got.deficit, want[1])
+    assert np.array_equal(got.variance, want[2])
+    assert np.array_equal(got.group, want[3])
+    assert (got.origin, got.inflation, got.segments) == want[4:]
