@@ -6,8 +6,9 @@ prototype's parameter and return types."""
 import re
 from pathlib import Path
 
+import _header as _hdr
+
 ROOT = Path(__file__).resolve().parent.parent
-HEADER = ROOT / "include" / "fbls_b200.h"
 DOC = ROOT / "INTEGRATION.md"
 
 _RUST_SCALARS = {"f64": "double", "f32": "float", "u32": "uint32_t", "u64": "uint64_t", "i64": "int64_t",
@@ -16,12 +17,6 @@ _RUST_SCALARS = {"f64": "double", "f32": "float", "u32": "uint32_t", "u64": "uin
 
 def _snake(name: str) -> str:
     return re.sub(r"(?<!^)([A-Z])", r"_\1", name).lower()
-
-
-def _c_type(text: str) -> str:
-    """Canonical form of a C type: 'const double*' -> 'const double *'."""
-    t = text.replace("*", " * ").split()
-    return " ".join(t)
 
 
 def _rust_type(text: str) -> str:
@@ -39,23 +34,7 @@ def _rust_type(text: str) -> str:
 
 
 def _header():
-    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
-    structs = {}
-    for body, name in re.findall(r"typedef struct\s*\{(.*?)\}\s*(fbls_\w+)\s*;", text, flags=re.S):
-        fields = []
-        for decl in body.split(";"):
-            decl = decl.strip()
-            if not decl:
-                continue
-            m = re.fullmatch(r"(.+?)\s*\b(\w+)", decl, flags=re.S)
-            fields.append((m.group(2), _c_type(m.group(1))))
-        structs[name] = fields
-    protos = {}
-    for ret, name, params in re.findall(r"([A-Za-z_][\w\s\*]*?)\b(fbls_\w+)\s*\(([^)]*)\)\s*;", text, flags=re.S):
-        ps = [] if params.strip() in ("", "void") else [p.strip() for p in params.split(",")]
-        types = [_c_type(re.fullmatch(r"(.+?)\s*\b(\w+)", p, flags=re.S).group(1)) for p in ps]
-        protos[name] = (_c_type(ret.strip()), types)
-    return structs, protos
+    return _hdr.structs(), _hdr.prototypes()
 
 
 def _rust_blocks():
