@@ -85,11 +85,12 @@ def _fmax(a: float, b: float) -> float:
 
 
 def round_half_away(x):
-    """f64::round (halves away from zero), exactly, elementwise."""
+    """f64::round (halves away from zero), exactly, elementwise; the sign of
+    a zero result is the input's, as there (-0.4 rounds to -0.0)."""
     x = np.asarray(x, dtype=np.float64)
     r = np.trunc(x)
     frac = x - r  # exact
-    return r + np.where(np.abs(frac) >= 0.5, np.sign(x), 0.0)
+    return np.copysign(r + np.where(np.abs(frac) >= 0.5, np.sign(x), 0.0), x)
 
 
 def rem_euclid(x, m: float):
