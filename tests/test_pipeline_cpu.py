@@ -90,3 +90,35 @@ def test_search_command_errors_exit_1_with_a_message(argv, message, capsys, tmp_
     monkeypatch.chdir(tmp_path)
     assert pipeline.main(argv) == 1
     assert message in capsys.readouterr().err
+
+
+def test_a_search_that_finds_nothing_still_writes_a_schema_3_report():
+    """Pure noise under a threshold no row reaches: no candidates, every key
+    of the report present, and the JSON writable as run_search writes it."""
+    rng = np.random.default_rng(12)
+    c, cfg = synth.small_curve(), synth.small_config()
+    cfg = dataclasses.replace(cfg, threshold=50.0)
+    flux = rng.normal(0.0, 1e-3, c.time.shape[0])
+    obs = io.Observations(c.time, flux, c.flux_err, np.zeros(c.time.shape[0], dtype=np.int64))
+    report = pipeline.search_prepared(_OracleGpu(), obs, cfg)
+    for key in ("schema_version", "software_version", "config", "statistics", "candidates", "signal_candidates",
+                "single_events"):
+        assert key in report, key
+    assert report["schema_version"] == 3
+    assert report["signal_candidates"] == [] and report["candidates"] == []
+    assert report["statistics"]["periods_tested"] > 0
+    text = json.dumps(pipeline._clean(report), default=pipeline._json_default)
+    assert json.loads(text)["signal_candidates"] == []
+
+
+def test_band_plan_of_a_baseline_shorter_than_the_minimum_period_is_empty():
+    from fbls_b200 import api
+    c, cfg = synth.small_curve(), synth.small_config()
+    st = oracle.family_state(c.time[:40], c.flux[:40], c.flux_err[:40], cfg.durations_days())
+    assert float(st.time[-1]) < cfg.period_min * 4
+    cfg = dataclasses.replace(cfg, period_min=float(st.time[-1]) * 2.0, period_max=float(st.time[-1]) * 4.0,
+                              durations_hours=[0.5])
+    grid, bands = api.band_plan(st, cfg)
+    assert len(grid) == 0 and bands == []
+    rows, ogrid, stats = oracle.signal_search(st, cfg)
+    assert rows.shape == (0, 5) and len(ogrid) == 0 and stats == []
