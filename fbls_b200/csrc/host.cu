@@ -51,6 +51,7 @@ int upload_family(fbls_ctx* ctx, DevBuf* buf, const double* time, const double* 
     const int rc = check_family(err, time, v, w, n);
     if (rc) return fail(ctx, rc, err);
     r->ctx = ctx;
+    r->device = ctx->device;
     r->n = n;
     r->baseline_norm = baseline_norm;
     r->origin = origin;
@@ -1006,6 +1007,7 @@ int search_batch_fused(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fb
                 if (rc == FBLS_OK) {
                     fbls_ready& f = local[k];
                     f.ctx = ctx;
+                    f.device = ctx->device;
                     f.n = s.n;
                     f.baseline_norm = s.baseline_norm;
                     f.origin = s.origin;
@@ -1190,7 +1192,7 @@ int fbls_upload_ready(fbls_ctx* ctx, const double* time, const double* v, const 
 void fbls_free_ready(fbls_ready* r) {
     if (!r) return;
     if (r->owned) {
-        if (r->ctx) cudaSetDevice(r->ctx->device);
+        cudaSetDevice(r->device);
         cudaFree(r->time);
     }
     delete r;

@@ -58,6 +58,7 @@ struct fbls_ctx {
 
 struct fbls_ready {
     fbls_ctx* ctx = nullptr;
+    int device = 0;          // the device holding time/v/w; fbls_free_ready reads it, not ctx, which may be gone
     double* time = nullptr;  // n
     double* v = nullptr;     // n
     double* w = nullptr;     // n

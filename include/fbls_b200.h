@@ -160,6 +160,7 @@ const char* fbls_version(void);
  * observations. residual_energy is Ready::residual_energy (curve.rs:440). */
 int fbls_upload_ready(fbls_ctx* ctx, const double* time, const double* v, const double* w, uint32_t n,
                       double baseline_norm, double origin, double residual_energy, fbls_ready** out);
+/* Frees an uploaded family; before or after fbls_destroy of its context. */
 void fbls_free_ready(fbls_ready* ready);
 
 /* Replaces scan_periods (scan.rs:363-408): best template per period over
