@@ -122,3 +122,45 @@ def test_band_plan_of_a_baseline_shorter_than_the_minimum_period_is_empty():
     assert len(grid) == 0 and bands == []
     rows, ogrid, stats = oracle.signal_search(st, cfg)
     assert rows.shape == (0, 5) and len(ogrid) == 0 and stats == []
+
+
+class _OracleContext(_OracleGpu):
+    """api.Gpu's place in run_search: the oracle behind a context manager."""
+
+    def __init__(self, device=0):
+        self.device = device
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+@pytest.mark.parametrize("mode", ["raw", "prepared"])
+def test_search_command_on_npz_files_with_the_oracle(tmp_path, monkeypatch, mode):
+    """run_search end to end on the CPU: NPZ files written by numpy, the
+    options, the report and the CSV table; the GPU steps answered by the
+    oracle."""
+    rng = np.random.default_rng(9)
+    t = synth.sector_times(1, 1200.0)
+    rel = synth.inject_box(t, rng.normal(0.0, 8e-4, t.shape[0]), 3.3, t[0] + 1.1, 0.15, 4e-3)
+    flux = 5.0e3 * (1.0 + 0.002 * np.sin(t / 2.3)) * (1.0 + rel)
+    raw, prepared = tmp_path / "star.npz", tmp_path / "prepared.npz"
+    np.savez(raw, time_bjd=t, flux=flux, flux_err=np.full(t.shape[0], 4.0), sector=np.full(t.shape[0], 31))
+    np.savez(prepared, time_bjd=t, flux=rel, flux_err=np.full(t.shape[0], 8e-4))
+    monkeypatch.setattr(pipeline.api, "Gpu", _OracleContext)
+    out, table = tmp_path / "report.json", tmp_path / "table.csv"
+    args = ["search", "--input", str(raw if mode == "raw" else prepared), "--output", str(out),
+            "--save-table", str(table), "--pmax", "6"]
+    if mode == "prepared":
+        args.append("--prepared")
+    assert pipeline.main(args) == 0
+    report = json.loads(out.read_text())
+    assert report["schema_version"] == 3 and report["input_mode"] == mode
+    assert report["input_files"] == [str(raw if mode == "raw" else prepared)]
+    assert "period_table" not in report
+    best = report["signal_candidates"][0]
+    assert abs(best["period_days"] - 3.3) / 3.3 < 0.01
+    lines = table.read_text().splitlines()
+    assert lines[0] == "period_days,epoch_bjd,duration_days,snr,depth" and len(lines) > 1
