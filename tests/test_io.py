@@ -156,3 +156,37 @@ def test_npy_malformed_shapes_and_headers_fail_cleanly():
     assert a.shape == (3,) and a.data.tolist() == [1.0, 2.0, 3.0]
     s = io.parse_npy(_npy("{'descr': '<f8', 'fortran_order': False, 'shape': (), }", body))
     assert s.shape == () and s.data.tolist() == [1.0]
+
+
+def _spoc(path, sector, rows):
+    """A SPOC-like light-curve product: rows of (time, flux, err, quality)."""
+    primary = _pad(b"".join(_card(k, v) for k, v in [
+        ("SIMPLE", "T"), ("BITPIX", "8"), ("NAXIS", "0"), ("TICID", "123456789"), ("SECTOR", str(sector)),
+        ("TESSMAG", "9.5"), ("TEFF", "5700.0"), ("RADIUS", "1.02"), ("LOGG", "4.4")]) + b"END".ljust(80), b" ")
+    cols = [("TIME", "D"), ("PDCSAP_FLUX", "E"), ("PDCSAP_FLUX_ERR", "E"), ("MOM_CENTR1", "D"), ("MOM_CENTR2", "D"),
+            ("QUALITY", "J")]
+    cards = [("XTENSION", "'BINTABLE'"), ("BITPIX", "8"), ("NAXIS", "2"), ("NAXIS1", "36"),
+             ("NAXIS2", str(len(rows))), ("PCOUNT", "0"), ("GCOUNT", "1"), ("TFIELDS", str(len(cols)))]
+    for i, (name, form) in enumerate(cols, 1):
+        cards += [(f"TTYPE{i}", f"'{name}'"), (f"TFORM{i}", f"'{form}'")]
+    cards += [("EXTNAME", "'LIGHTCURVE'"), ("BJDREFI", "2457000"), ("BJDREFF", "0.5"), ("CROWDSAP", "0.99")]
+    ext = _pad(b"".join(_card(k, v) for k, v in cards) + b"END".ljust(80), b" ")
+    data = b"".join(struct.pack(">dffddi", t, f, e, 10.0, 20.0, q) for t, f, e, q in rows)
+    path.write_bytes(primary + ext + _pad(data, b"\0"))
+
+
+def test_read_light_curve_applies_the_quality_mask_and_bjd_reference(tmp_path):
+    # fits.rs:284-333 with the default bitmask 17087 (fits.rs:214-217)
+    rows = [(1.0, 100.0, 1.0, 0), (2.0, 101.0, 1.0, 1), (3.0, 102.0, 1.0, 2048), (4.0, math.nan, 1.0, 0),
+            (math.nan, 103.0, 1.0, 0), (6.0, 104.0, 1.0, 16384), (7.0, 105.0, 1.5, 4096), (8.0, 106.0, 1.0, 512)]
+    path = tmp_path / "lc.fits"
+    _spoc(path, 14, rows)
+    lc = io.read_light_curve(str(path))
+    assert lc.tic == 123456789 and lc.sector == 14 and lc.points_total == 8
+    # kept: quality 0, 2048 (bit 11) and 4096 (bit 12); dropped: bits 0, 14 and 9, NaN flux, NaN time
+    assert (lc.time_bjd - 2457000.5).tolist() == [1.0, 3.0, 7.0]
+    assert lc.flux.tolist() == [100.0, 102.0, 105.0] and lc.flux_err.tolist() == [1.0, 1.0, 1.5]
+    assert lc.star.tmag == 9.5 and lc.star.teff == 5700.0 and lc.crowdsap == 0.99
+    assert lc.target_pixel is None  # no APERTURE extension
+    obs = io.read_inputs([str(path)])
+    assert obs.time.tolist() == lc.time_bjd.tolist() and obs.err is not None and obs.group.tolist() == [0, 0, 0]
