@@ -125,3 +125,22 @@ def test_family_state_rejects_null_arrays():
     err = ctypes.create_string_buffer(64)
     rc = lib.fbls_family_state(None, None, None, 10, None, 0, 1, None, None, None, None, None, None, err, 64)
     assert rc == 1 and err.value == b"null argument"
+
+
+def test_multi_sector_workload_sizes():
+    """The 13-sector benchmark workload under the reference's rules: 247,104
+    points, 189,216 periods in 6 octave bands of 11, 14, 18, 20, 20, 20
+    durations at nb 192 ... 3840; the dense-grid variants' counts."""
+    c, cfg = synth.multi_sector(), synth.multi_sector_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    grid, bands = api.band_plan(st, cfg)
+    assert st.n == 247104 and grid.shape[0] == 189216
+    assert [len(b["durations"]) for b in bands] == [11, 14, 18, 20, 20, 20]
+    assert [b["nb"] for b in bands] == [192, 384, 768, 1536, 3072, 3840]
+    assert sum(len(b["periods"]) for b in bands) == grid.shape[0]
+    dense = SearchConfig(**{**cfg.__dict__, "period_oversample": 19.0})
+    assert api.band_plan(st, dense)[0].shape[0] == 1198347
+    s1, c1 = synth.single_sector(), synth.single_sector_config()
+    st1 = api.prepared_family(s1.time, s1.flux, s1.flux_err, c1)
+    assert st1.n == 19008
+    assert api.band_plan(st1, SearchConfig(**{**c1.__dict__, "period_oversample": 6.9}))[0].shape[0] == 30044
