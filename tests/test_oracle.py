@@ -127,3 +127,28 @@ def test_mixed_and_f64_modes_agree_on_winners(small_state):
     assert same.mean() > 0.99
     ok = np.isfinite(r0[1])
     assert np.allclose(r0[1][ok & same], r1[1][ok & same], rtol=1e-12)
+
+
+def test_erfc_against_arbitrary_precision():
+    """Beyond the reference's 16-value table: Cody's approximation as the
+    reference evaluates it stays within 2e-15 of the exact value (mpmath at
+    50 digits) on [-6, XBIG), is exactly 0 from XBIG = 26.543 on (the
+    reference returns 0 there; the exact value is subnormal), and keeps
+    erfc(-x) = 2 - erfc(x)."""
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.dps = 50
+    xs = np.concatenate([np.linspace(-6.0, 26.54, 4001), [0.46875, 0.46876, 4.0, 4.0000001, 26.5429]])
+    worst = max(abs(oracle.erfc(x) - float(mpmath.erfc(x))) / float(mpmath.erfc(x)) for x in xs)
+    assert worst < 2e-15, worst
+    assert all(oracle.erfc(x) == 0.0 for x in (26.543, 26.6, 30.0, 1e300))
+    assert all(oracle.erfc(-x) == 2.0 - oracle.erfc(x) for x in (0.5, 1.0, 3.0, 10.0))
+
+
+def test_log_add_against_arbitrary_precision():
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.dps = 50
+    vals = [-700.0, -50.0, -3.5, -1e-3, 0.0, 2.0, 40.0, 700.0]
+    for a in vals:
+        for b in vals:
+            exact = float(mpmath.log(mpmath.exp(a) + mpmath.exp(b)))
+            assert abs(oracle.log_add(a, b) - exact) <= 4e-16 * max(1.0, abs(exact)), (a, b)
