@@ -152,3 +152,44 @@ def test_log_add_against_arbitrary_precision():
         for b in vals:
             exact = float(mpmath.log(mpmath.exp(a) + mpmath.exp(b)))
             assert abs(oracle.log_add(a, b) - exact) <= 4e-16 * max(1.0, abs(exact)), (a, b)
+
+
+def test_positive_amplitude_evidence_is_the_half_normal_integral():
+    """math.rs:112-139: log of the integral over depths x >= 0 of a
+    half-normal prior of scale tau times exp(a x - q x^2 / 2), in closed form
+    -ln(1 + tau^2 q) / 2 + z^2 / 2 + ln erfc(-z / sqrt 2); the reference's
+    asymptotic series below z = -26 included."""
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.dps = 60
+    rng = np.random.default_rng(6)
+    cases = [(a, q, tau) for a, q, tau in zip(rng.normal(0.0, 30.0, 300), np.exp(rng.uniform(-3, 8, 300)),
+                                              np.exp(rng.uniform(-6, 1, 300)))]
+    cases += [(-2000.0, 100.0, 1.0), (-5000.0, 1e4, 0.5), (-30.0, 0.0, 1.0), (0.0, 1.0, 0.1), (5.0, -3.0, 0.2)]
+    seen_series = False
+    for a, q, tau in cases:
+        qq = max(q, 0.0)
+        precision = 1 + mpmath.mpf(tau) ** 2 * qq
+        z = mpmath.mpf(tau) * a / mpmath.sqrt(precision)
+        seen_series |= z < -26
+        exact = -mpmath.log(precision) / 2 + z * z / 2 + mpmath.log(mpmath.erfc(-z / mpmath.sqrt(2)))
+        got = oracle.positive_amplitude_evidence(a, q, tau)
+        assert abs(got - float(exact)) <= 1e-11 * max(1.0, abs(float(exact))), (a, q, tau, got, float(exact))
+    assert seen_series
+
+
+def test_subspace_upper_bounds_every_positive_mixture():
+    """math.rs:141-177: an upper bound of (a x + b y - [x y] M [x y]^T / 2) / rho^2
+    over depths x, y >= 0 (M = [[q, c], [c, r]]), within its 1e-6 margins."""
+    rng = np.random.default_rng(7)
+    for _ in range(300):
+        q, r = np.exp(rng.uniform(-2, 3, 2))
+        c = rng.uniform(-0.95, 0.95) * math.sqrt(q * r)
+        a, b = rng.normal(0.0, 5.0, 2)
+        rho2 = rng.uniform(1.0, 3.0)
+        upper = oracle.subspace_upper(a, b, q, r, c, rho2)
+        xs = np.abs(rng.normal(0.0, 3.0, (400, 2)))
+        grid = np.stack(np.meshgrid(np.linspace(0, 6, 61), np.linspace(0, 6, 61)), -1).reshape(-1, 2)
+        x, y = np.vstack([xs, grid]).T
+        value = (a * x + b * y - 0.5 * (q * x * x + 2 * c * x * y + r * y * y)) / rho2
+        assert value.max() <= upper + 1e-9, (a, b, q, r, c, rho2, value.max(), upper)
+    assert oracle.subspace_upper(-1.0, -2.0, 1.0, 1.0, 0.0, 1.0) == pytest.approx(1e-6)  # no positive gain
