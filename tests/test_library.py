@@ -144,3 +144,33 @@ def test_multi_sector_workload_sizes():
     st1 = api.prepared_family(s1.time, s1.flux, s1.flux_err, c1)
     assert st1.n == 19008
     assert api.band_plan(st1, SearchConfig(**{**c1.__dict__, "period_oversample": 6.9}))[0].shape[0] == 30044
+
+
+def test_host_entry_points_are_safe_to_call_from_many_threads():
+    """ctypes releases the GIL, so these calls overlap in the library: family
+    state, period grids and noise fits from 8 threads equal the sequential
+    results (the host code keeps no shared state)."""
+    from concurrent.futures import ThreadPoolExecutor
+    curves = [synth.small_curve(seed=s) for s in range(8)]
+    cfg = synth.small_config()
+
+    def work(c):
+        st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+        g = api.period_grid(0.3, 9.0, float(st.time[-1]), 0.02, 3.0)
+        m = api.fit_segment_noise(c.time, 1e4 * (1.0 + c.flux), None, None, 10.0, 0.75)
+        return st.v, g, m.deficit
+
+    want = [work(c) for c in curves]
+    with ThreadPoolExecutor(8) as pool:
+        for _ in range(3):
+            got = list(pool.map(work, curves))
+            for (v, g, d), (wv, wg, wd) in zip(got, want):
+                assert np.array_equal(v, wv) and np.array_equal(g, wg) and np.array_equal(d, wd)
+
+
+def test_oracle_search_does_not_depend_on_its_thread_count():
+    c, cfg = synth.small_curve(), synth.small_config()
+    st = oracle.family_state(c.time, c.flux, c.flux_err, cfg.durations_days())
+    one = oracle.signal_search(st, cfg, threads=1)
+    many = oracle.signal_search(st, cfg, threads=8)
+    assert np.array_equal(one[0], many[0]) and np.array_equal(one[1], many[1])
