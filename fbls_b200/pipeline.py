@@ -94,10 +94,9 @@ def _finite(x: float) -> Optional[float]:
 
 
 def _peak_json(p: select.Peak) -> dict:
-    out = dataclasses.asdict(p)
-    out["pass"] = out.pop("pass_")
-    out.pop("row")  # not serialised by the reference (peaks.rs:30-31)
-    return out
+    """The fields in the reference's order (Peak, peaks.rs:18-45), `pass_`
+    written as "pass" in its place and `row` left out (not serialised there)."""
+    return {("pass" if k == "pass_" else k): v for k, v in dataclasses.asdict(p).items() if k != "row"}
 
 
 def search_families(gpu: api.Gpu, fams: List[Tuple[Curve, List[int]]], durations: Sequence[float],
@@ -310,7 +309,9 @@ def run_search(argv: Sequence[str]) -> int:
             for r in report["period_table"]:
                 fh.write(f"{r['period']},{r['epoch']},{r['duration']},{r['score']},{r['depth']}\n")
     report.pop("period_table")
-    text = json.dumps(_clean(report), indent=2, default=_json_default)
+    # serde_json without preserve_order keeps every object in a BTreeMap, so the
+    # reference writes all keys sorted (main.rs:221, to_string_pretty).
+    text = json.dumps(_clean(report), indent=2, sort_keys=True, default=_json_default)
     if output == "-":
         print(text)
     else:

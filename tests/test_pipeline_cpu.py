@@ -164,3 +164,33 @@ def test_search_command_on_npz_files_with_the_oracle(tmp_path, monkeypatch, mode
     assert abs(best["period_days"] - 3.3) / 3.3 < 0.01
     lines = table.read_text().splitlines()
     assert lines[0] == "period_days,epoch_bjd,duration_days,snr,depth" and len(lines) > 1
+
+
+def test_candidate_fields_are_the_references():
+    # Peak, src/select/peaks.rs:18-45 (`row` is not serialised)
+    want = ["period_days", "epoch_bjd", "duration_hours", "snr", "snr_folded", "snr_without_strongest_event",
+            "depth", "depth_ppm", "events", "family", "pass", "planet_log_odds", "log_bf_planet_noise",
+            "log_bf_binary_noise", "binary_secondary_ratio", "binary_secondary_phase", "binary_odd_even_ratio",
+            "binary_period_days", "ingress_fraction", "evidence_epoch_bjd", "evidence_duration_hours",
+            "model_preferred", "binary_diagnostics_complete"]
+    c, cfg = synth.small_curve(), synth.small_config()
+    obs = io.Observations(c.time, c.flux, c.flux_err, np.zeros(c.time.shape[0], dtype=np.int64))
+    report = pipeline.search_prepared(_OracleGpu(), obs, cfg)
+    assert list(report["signal_candidates"][0].keys()) == want
+
+
+def test_written_report_keys_are_sorted_at_every_level(tmp_path, monkeypatch):
+    """The reference builds the report as a serde_json Value without
+    preserve_order (BTreeMap objects), so its file has every object's keys
+    in sorted order; run_search writes the same order."""
+    c = synth.small_curve()
+    path = tmp_path / "p.npz"
+    np.savez(path, time_bjd=c.time, flux=c.flux, flux_err=c.flux_err)
+    monkeypatch.setattr(pipeline.api, "Gpu", _OracleContext)
+    out = tmp_path / "r.json"
+    cfg_args = ["--pmin", "0.4", "--pmax", "2.9"]
+    assert pipeline.main(["search", "--prepared", "--input", str(path), "--output", str(out)] + cfg_args) == 0
+    orders = []
+    json.loads(out.read_text(), object_pairs_hook=lambda pairs: orders.append([k for k, _ in pairs]) or dict(pairs))
+    assert len(orders) > 5
+    assert all(keys == sorted(keys) for keys in orders)
