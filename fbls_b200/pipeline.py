@@ -93,6 +93,16 @@ def _finite(x: float) -> Optional[float]:
     return float(x) if math.isfinite(x) else None
 
 
+def _config_json(cfg: SearchConfig) -> dict:
+    """SearchConfig as the reference serialises it (config.rs:5-88): its
+    fields only; this library's precision_mode appears only when a run asks
+    for f64 ranking, which the reference does not have."""
+    out = dataclasses.asdict(cfg)
+    if out.get("precision_mode", 0) == 0:
+        out.pop("precision_mode", None)
+    return out
+
+
 def _peak_json(p: select.Peak) -> dict:
     """The fields in the reference's order (Peak, peaks.rs:18-45), `pass_`
     written as "pass" in its place and `row` left out (not serialised there)."""
@@ -218,7 +228,7 @@ def search_families(gpu: api.Gpu, fams: List[Tuple[Curve, List[int]]], durations
     return {
         "schema_version": SCHEMA_VERSION,
         "software_version": "fbls_b200 0.1",
-        "config": dataclasses.asdict(cfg),
+        "config": _config_json(cfg),
         "statistics": {
             "device": f"cuda:{device}", "observations": int(time_all.shape[0]), "baseline_days": baseline,
             "periodic_period_max_days": min(cfg.period_max, baseline), "periods_tested": periods_tested,

@@ -194,3 +194,15 @@ def test_written_report_keys_are_sorted_at_every_level(tmp_path, monkeypatch):
     json.loads(out.read_text(), object_pairs_hook=lambda pairs: orders.append([k for k, _ in pairs]) or dict(pairs))
     assert len(orders) > 5
     assert all(keys == sorted(keys) for keys in orders)
+
+
+def test_report_config_has_the_reference_fields():
+    fields = ["period_min", "period_max", "durations_hours", "threshold"]  # a few, and the whole set below
+    c, cfg = synth.small_curve(), synth.small_config()
+    obs = io.Observations(c.time, c.flux, c.flux_err, np.zeros(c.time.shape[0], dtype=np.int64))
+    report = pipeline.search_prepared(_OracleGpu(), obs, cfg)
+    assert all(f in report["config"] for f in fields)
+    assert "precision_mode" not in report["config"]  # not a field of the reference's SearchConfig
+    assert len(report["config"]) == 36  # config.rs:6-88
+    f64 = pipeline.search_prepared(_OracleGpu(), obs, dataclasses.replace(cfg, precision_mode=1))
+    assert f64["config"]["precision_mode"] == 1
