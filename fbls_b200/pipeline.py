@@ -93,6 +93,16 @@ def _finite(x: float) -> Optional[float]:
     return float(x) if math.isfinite(x) else None
 
 
+# ScanStats as the reference serialises it (scan.rs:24-37); the library's
+# fbls_scan_stats adds tile_rescans, which the schema-3 report leaves out.
+SCAN_STATS_FIELDS = ("periods", "prescan_survivors", "phase_bins", "batches", "templates_scanned",
+                     "exact_tile_retries", "seconds", "seconds_fold", "seconds_cumulative", "seconds_scan")
+
+
+def _scan_stats_json(stats: dict) -> dict:
+    return {k: stats[k] for k in SCAN_STATS_FIELDS if k in stats}
+
+
 def _config_json(cfg: SearchConfig) -> dict:
     """SearchConfig as the reference serialises it (config.rs:5-88): its
     fields only; this library's precision_mode appears only when a run asks
@@ -138,7 +148,7 @@ def search_families(gpu: api.Gpu, fams: List[Tuple[Curve, List[int]]], durations
                 "family": k, "window_days": _finite(fam.curve.window_days), "observations": int(fam.curve.time.shape[0]),
                 "clipped": fam.curve.clipped, "error_inflation": fam.state.inflation, "segments": fam.state.segments,
                 "durations_hours": (fam.durations * 24.0).tolist(), "periods": grid_len,
-                "rho": fam.state.rho.tolist(), "bands": stats})
+                "rho": fam.state.rho.tolist(), "bands": [_scan_stats_json(b) for b in stats]})
             family += [k] * rows.shape[0]
             tables.append(rows)
         table = np.vstack(tables) if tables else np.empty((0, 5))

@@ -206,3 +206,11 @@ def test_report_config_has_the_reference_fields():
     assert len(report["config"]) == 36  # config.rs:6-88
     f64 = pipeline.search_prepared(_OracleGpu(), obs, dataclasses.replace(cfg, precision_mode=1))
     assert f64["config"]["precision_mode"] == 1
+
+
+def test_band_stats_in_the_report_are_the_references_scan_stats():
+    from fbls_b200 import _native
+    full = _native.ScanStats().as_dict()  # every field the C ABI reports
+    assert "tile_rescans" in full
+    got = pipeline._scan_stats_json(full)
+    assert list(got) == list(pipeline.SCAN_STATS_FIELDS) and "tile_rescans" not in got
