@@ -193,3 +193,49 @@ def test_subspace_upper_bounds_every_positive_mixture():
         value = (a * x + b * y - 0.5 * (q * x * x + 2 * c * x * y + r * y * y)) / rho2
         assert value.max() <= upper + 1e-9, (a, b, q, r, c, rho2, value.max(), upper)
     assert oracle.subspace_upper(-1.0, -2.0, 1.0, 1.0, 0.0, 1.0) == pytest.approx(1e-6)  # no positive gain
+
+
+def test_single_event_rows_are_every_box_template_over_the_threshold():
+    """The oracle's single-event scan (events.rs:18-153, scan_all
+    kernels.rs:851-921) with the box shape only, against a brute-force
+    enumeration: one trial period baseline + 2 x longest duration + 1e-6 d,
+    nb = max(8, ceil(phase_oversample x trial / shortest duration)), every
+    (phase, duration) window from direct per-observation sums that is usable
+    (raw width below nb / 2, 3 ... n - 3 observations, a > 0, q > 0) and
+    reaches the threshold."""
+    import dataclasses as dc
+    c = synth.small_curve()
+    cfg = dc.replace(synth.small_config(), ingress_fractions=[0.0], threshold=4.0)
+    st = oracle.family_state(c.time, c.flux, c.flux_err, cfg.durations_days())
+    rows, stats = oracle.single_event_search(st, cfg)
+    order = np.argsort(st.durations, kind="stable")
+    d, rho = st.durations[order], st.rho[order]
+    trial = float(st.time[-1]) + 2.0 * d[-1] + 1e-6
+    nb = max(8, math.ceil(cfg.phase_oversample * trial / d[0]))
+    scale = nb / trial
+    want = {}
+    for di in range(len(d)):
+        raw_k = max(1, math.floor(d[di] * scale + 0.5))
+        if raw_k >= nb // 2:
+            continue
+        k = raw_k
+        for j in range(nb):
+            a, hp, cnt = oracle.box_direct(st, scale, nb, j, k)
+            q = hp - hp * hp / st.baseline_norm
+            if not (3 <= cnt <= st.n - 3 and a > 0 and q > 0):
+                continue
+            score = (a / rho[di]) / math.sqrt(q)
+            if score >= cfg.threshold:
+                want[(j, k, di)] = (score, a / q)
+    got = {}
+    for r in rows:
+        j = round((r[1] - st.origin) * scale - (r[2] * scale) / 2.0)
+        k = round(r[2] * scale)
+        di = next(i for i in range(len(d)) if max(1, math.floor(d[i] * scale + 0.5)) == k and (j, k, i) not in got)
+        got[(j, k, di)] = (r[3], r[4])
+    assert len(want) > 20 and stats["threshold_survivors"] == len(rows)
+    near = {key for key, (s, _) in want.items() if abs(s - cfg.threshold) <= 1e-9 * cfg.threshold}
+    assert set(got) ^ set(want) <= near
+    for key in set(got) & set(want):
+        assert got[key][0] == pytest.approx(want[key][0], rel=1e-9)
+        assert got[key][1] == pytest.approx(want[key][1], rel=1e-9)
