@@ -13,7 +13,6 @@
 // (at most 64 halvings), then the smallest value at or above the bound; the
 // weighted sums run over the window in order. All arithmetic rounds as the
 // reference's (no contraction), so the output is the reference's bit for bit.
-#include <mutex>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -105,20 +104,12 @@ __global__ void __launch_bounds__(BIWEIGHT_THREADS) k_biweight(BiweightArgs args
 cudaError_t launch_biweight(const BiweightArgs& a, int nblocks, size_t smem, cudaStream_t stream) {
     if (nblocks < 1 || smem > BIWEIGHT_STAGE * sizeof(double) || !a.flux || !a.lo || !a.hi || !a.blocks || !a.out)
         return cudaErrorInvalidValue;
-    {
-        static std::mutex mu;
-        static bool configured[64] = {};
-        int dev = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        if (e != cudaSuccess) return e;
-        std::lock_guard<std::mutex> lock(mu);
-        if (dev < 64 && !configured[dev]) {
-            e = cudaFuncSetAttribute(k_biweight, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(BIWEIGHT_STAGE * sizeof(double)));
-            if (e != cudaSuccess) return e;
-            configured[dev] = true;
-        }
-    }
+    // The limit belongs to the module loaded in the current context; a context
+    // made again after cudaDeviceReset reloads the module without it, so it is
+    // set at every launch (a host-side attribute write, no device work).
+    cudaError_t e = cudaFuncSetAttribute(k_biweight, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(BIWEIGHT_STAGE * sizeof(double)));
+    if (e != cudaSuccess) return e;
     k_biweight<<<nblocks, BIWEIGHT_THREADS, smem, stream>>>(a);
     return cudaGetLastError();
 }

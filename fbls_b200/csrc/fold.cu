@@ -25,7 +25,6 @@
 // The doubled prefix sums then follow the association of the reference's
 // prefix_block (kernels.rs:237-309), one warp per (period, field) row, and
 // are written as f64 and (hi, lo) f32 pairs.
-#include <mutex>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -569,7 +568,17 @@ __device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) 
         const int buf = blk & 1;
         const bool landed = mbar_wait_bounded(bar0 + 8 * buf, (uint32_t)(blk >> 1) & 1u);
         if (!__syncthreads_and(landed)) {
-            if (tid == 0) atomicOr(a.fault, 1u);
+            // Give up on this fold, but not while the block's bulk copies may
+            // still write into this CTA's shared memory: thread 0 (which
+            // issued them; the next block's copies are not issued yet) waits
+            // again with a longer bound. If that also runs out the copies may
+            // still be pending when the CTA ends; the fault word is set either
+            // way and the host discards the pass.
+            if (tid == 0) {
+                for (int again = 0; again < 16; again++)
+                    if (mbar_wait_bounded(bar0 + 8 * buf, (uint32_t)(blk >> 1) & 1u)) break;
+                atomicOr(a.fault, 1u);
+            }
             return;
         }
         const int next_lo = blk_hi, next_hi = next_lo < nch ? block_end(next_lo) : next_lo;
@@ -893,21 +902,11 @@ int fold_chunks(const double* time, int n, double scale_max, int nb, int span_ca
 cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, size_t smem,
                              cudaStream_t stream) {
     if (njobs < 1 || ctas < 1 || smem > MAX_FOLD_SMEM) return cudaErrorInvalidValue;
-    {
-        static std::mutex mu;
-        static bool configured[64] = {};
-        int dev = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        if (e != cudaSuccess) return e;
-        if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-        std::lock_guard<std::mutex> lock(mu);
-        if (!configured[dev]) {
-            e = cudaFuncSetAttribute(k_fold_walk_jobs<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)MAX_FOLD_SMEM);
-            if (e != cudaSuccess) return e;
-            configured[dev] = true;
-        }
-    }
+    // Set at every launch: the attribute belongs to the module loaded in the
+    // current context, which a cudaDeviceReset replaces.
+    const cudaError_t e = cudaFuncSetAttribute(k_fold_walk_jobs<WALK_CAP>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
+    if (e != cudaSuccess) return e;
     k_fold_walk_jobs<WALK_CAP><<<ctas, 1024, smem, stream>>>(jobs, cta0, njobs);
     return cudaGetLastError();
 }
@@ -924,24 +923,15 @@ bool fold_job_ok(const FoldArgs& a, const FoldShape& shape) {
 }
 
 cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream) {
-    // The shared-memory limit is a per-device attribute of each kernel; set it
-    // once per device (contexts of several host threads may launch).
+    // The shared-memory limit is an attribute of each kernel in the module
+    // loaded in the current context; it is set at every launch, so a context
+    // made again after cudaDeviceReset (which reloads the module) gets it too.
     {
-        static std::mutex mu;
-        static bool configured[64] = {};
-        int dev = 0;
-        cudaError_t e = cudaGetDevice(&dev);
+        cudaError_t e = cudaFuncSetAttribute(k_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_fold_walk<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)MAX_FOLD_SMEM);
         if (e != cudaSuccess) return e;
-        if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-        std::lock_guard<std::mutex> lock(mu);
-        if (!configured[dev]) {
-            e = cudaFuncSetAttribute(k_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(k_fold_walk<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)MAX_FOLD_SMEM);
-            if (e != cudaSuccess) return e;
-            configured[dev] = true;
-        }
     }
     if (!a.time || !a.v || !a.w || !a.scales || !a.chunks || (!a.hist_out && !a.map_out && (!a.cum || !a.cum32)))
         return cudaErrorInvalidValue;

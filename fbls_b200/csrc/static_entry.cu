@@ -11,10 +11,13 @@
 // and scanned in batches of periods that fit it, and the results are copied
 // back.
 //
-// Set-up: the first call on a device, with that device current, resolves the
-// array's device address (cudaGetSymbolAddress) and caches it per device; that
-// first call should come before any stream capture. In host code the array's
-// name is only a host-side stand-in, never a device address.
+// Set-up: every call, with its device current, resolves the array's device
+// address (cudaGetSymbolAddress) and checks the result. The address is not
+// kept between calls: after cudaDeviceReset the module is loaded again and
+// the array may sit elsewhere. The first call on a device also loads the
+// library's module there, so make that call before any stream capture. In
+// host code the array's name is only a host-side stand-in, never a device
+// address.
 //
 // Every call shares the one array and overwrites it: calls that overlap on
 // the GPU (from several host threads, or on several streams) race. Nothing in
@@ -24,7 +27,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -39,9 +41,6 @@ static __device__ __align__(256) unsigned char g_fbls_scratch[FBLS_STATIC_SCRATC
 namespace {
 
 constexpr int MAX_DEVICES = 64;
-std::mutex g_static_mutex;
-unsigned char* g_static_ptr[MAX_DEVICES] = {nullptr};
-int g_static_sms[MAX_DEVICES] = {0};
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -72,6 +71,11 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
     if (nd == 0 || nd > (uint32_t)MAX_DURATIONS || ns == 0 || ns > (uint32_t)MAX_SHAPES || layers == 0 ||
         layers > (uint32_t)MAX_LAYERS || nb < 8)
         return report(error, error_len, FBLS_ERR_ARGUMENT, "bank size outside the supported range");
+    if (!bank->durations || !bank->rho || !bank->ingress)
+        return report(error, error_len, FBLS_ERR_ARGUMENT, "null argument");
+    for (uint32_t i = 0; i < nd; i++)
+        if (!(bank->durations[i] > 0.0) || !std::isfinite(bank->durations[i]) || !std::isfinite(bank->rho[i]))
+            return report(error, error_len, FBLS_ERR_ARGUMENT, "durations must be positive and finite");
     for (uint32_t i = 1; i < n; i++)
         if (!(time[i] >= time[i - 1])) return report(error, error_len, FBLS_ERR_ARGUMENT, "times must be ascending");
     if (!(time[0] >= 0.0))
@@ -89,25 +93,14 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
 
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return report(error, error_len, FBLS_ERR_CUDA, cudaGetErrorString(e));
-    unsigned char* base = nullptr;
+    void* symbol = nullptr;
+    e = cudaGetSymbolAddress(&symbol, g_fbls_scratch);
+    if (e != cudaSuccess)
+        return report(error, error_len, FBLS_ERR_CUDA, std::string("static scratch address: ") + cudaGetErrorString(e));
+    unsigned char* const base = static_cast<unsigned char*>(symbol);
     int sms = 0;
-    {
-        std::lock_guard<std::mutex> lock(g_static_mutex);
-        if (!g_static_ptr[device]) {
-            void* ptr = nullptr;
-            e = cudaGetSymbolAddress(&ptr, g_fbls_scratch);
-            if (e != cudaSuccess)
-                return report(error, error_len, FBLS_ERR_CUDA,
-                              std::string("static scratch address: ") + cudaGetErrorString(e));
-            int count = 0;
-            e = cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, device);
-            if (e != cudaSuccess) return report(error, error_len, FBLS_ERR_CUDA, cudaGetErrorString(e));
-            g_static_ptr[device] = static_cast<unsigned char*>(ptr);
-            g_static_sms[device] = count;
-        }
-        base = g_static_ptr[device];
-        sms = g_static_sms[device];
-    }
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return report(error, error_len, FBLS_ERR_CUDA, cudaGetErrorString(e));
 
     // Fixed part of the array: fields, bank constants, fold chunks.
     std::vector<double> host_bank;
@@ -125,25 +118,39 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
     const uint32_t tiles = (nb + TILE - 1) / TILE;
     const size_t stride = 2 * (size_t)nb + 1;
     // Per period of a batch: scales, periods, cum, cum32, parts, keys, tile
-    // flags, records, score, depth, flags, plus 3 rs doubles of fold scratch
-    // when the histogram does not fit shared memory; 256 bytes of alignment
-    // slack per region.
-    const FoldShape probe = fold_group_shape((int)nb, (int)P, sms);
-    const size_t per_period = 2 * sizeof(double) + NF * stride * (sizeof(double) + sizeof(float2)) +
-                              tiles * (PART_STRIDE * sizeof(double) + sizeof(uint64_t) + sizeof(uint32_t)) +
-                              RECORD_STRIDE * sizeof(double) + 2 * sizeof(double) + sizeof(uint32_t) +
-                              (probe.hist_in_smem ? 0 : (size_t)NF * probe.row_stride * sizeof(double));
+    // flags, records, score, depth, flags, plus 3 row_stride doubles of fold
+    // scratch when the histogram does not fit shared memory (the fold's CTAs
+    // take `group` periods each, so the scratch covers group x ceil(batch /
+    // group) periods: group - 1 more are budgeted); 256 bytes of alignment
+    // slack per region. The batch is the largest that fits with the fold
+    // shape it is launched with.
     const size_t slack = 12 * 256;
-    if (fixed + slack + per_period > FBLS_STATIC_SCRATCH_BYTES)
-        return report(error, error_len, FBLS_ERR_ARGUMENT,
-                      "input exceeds the static scratch of fbls_scan_bank_static (" +
-                          std::to_string((unsigned long long)FBLS_STATIC_SCRATCH_BYTES) + " bytes)");
-    size_t batch = (FBLS_STATIC_SCRATCH_BYTES - fixed - slack) / per_period;
-    if (batch > P) batch = P;
-
-    FoldShape shape = fold_group_shape((int)nb, (int)batch, sms);
-    if (shape.hist_in_smem != probe.hist_in_smem)  // keep the budget above valid
-        shape = probe;
+    auto per_period_of = [&](const FoldShape& sh) {
+        return 2 * sizeof(double) + NF * stride * (sizeof(double) + sizeof(float2)) +
+               tiles * (PART_STRIDE * sizeof(double) + sizeof(uint64_t) + sizeof(uint32_t)) +
+               RECORD_STRIDE * sizeof(double) + 2 * sizeof(double) + sizeof(uint32_t) +
+               (sh.hist_in_smem ? 0 : (size_t)NF * sh.row_stride * sizeof(double));
+    };
+    auto hist_extra_of = [&](const FoldShape& sh) {
+        return sh.hist_in_smem ? (size_t)0 : (size_t)(sh.group - 1) * NF * sh.row_stride * sizeof(double);
+    };
+    size_t batch = P;
+    FoldShape shape{};
+    for (;;) {
+        shape = fold_group_shape((int)nb, (int)batch, sms);
+        const size_t need = fixed + slack + hist_extra_of(shape);
+        const size_t per_period = per_period_of(shape);
+        const size_t fit = need + per_period > FBLS_STATIC_SCRATCH_BYTES
+                               ? 0
+                               : (FBLS_STATIC_SCRATCH_BYTES - need) / per_period;
+        if (fit == 0)
+            return report(error, error_len, FBLS_ERR_ARGUMENT,
+                          "input exceeds the static scratch of fbls_scan_bank_static (" +
+                              std::to_string((unsigned long long)FBLS_STATIC_SCRATCH_BYTES) + " bytes)");
+        if (batch <= fit) break;
+        batch = fit;  // strictly smaller: the loop ends
+    }
+    const size_t hist_periods = ((batch + shape.group - 1) / shape.group) * (size_t)shape.group;
     std::vector<int> chunks((size_t)n + 2);
     const int nchunks = fold_chunks(time, (int)n, scale_max, (int)nb, shape.span_cap, shape.chunk_cap, chunks.data(),
                                     (int)chunks.size());
@@ -172,9 +179,9 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
     double* d_score = reinterpret_cast<double*>(take(sizeof(double) * batch));
     double* d_depth = reinterpret_cast<double*>(take(sizeof(double) * batch));
     uint32_t* d_rflags = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * batch));
-    double* d_hist = shape.hist_in_smem
-                         ? nullptr
-                         : reinterpret_cast<double*>(take((size_t)NF * shape.row_stride * sizeof(double) * batch));
+    double* d_hist = shape.hist_in_smem ? nullptr
+                                        : reinterpret_cast<double*>(
+                                              take((size_t)NF * shape.row_stride * sizeof(double) * hist_periods));
     if ((size_t)(at - base) > FBLS_STATIC_SCRATCH_BYTES)
         return report(error, error_len, FBLS_ERR_ARGUMENT, "input exceeds the static scratch");
 

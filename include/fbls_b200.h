@@ -196,9 +196,10 @@ int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* du
  * relative times ascending), periods (P), outputs as in fbls_scan_bank.
  * Inputs whose fields, chunk table and one period's intermediates do not fit
  * the array are rejected (FBLS_ERR_ARGUMENT with the message in error);
- * larger P is processed in batches that fit. The first call on a device
- * resolves the array's address on that device; make that call before any
- * stream capture. Calls share the array: calls that overlap on the GPU race.
+ * larger P is processed in batches that fit. Every call resolves the
+ * array's address on its device (again after a cudaDeviceReset); the first
+ * call on a device also loads the module there, so make it before any stream
+ * capture. Calls share the array: calls that overlap on the GPU race.
  * Runs on the legacy default stream and returns after the results are on
  * the host. */
 #define FBLS_STATIC_SCRATCH_BYTES (64u * 1024u * 1024u)
