@@ -741,6 +741,90 @@ def run_single_event(args):
     gpu.close()
 
 
+def _evidence_candidates(gpu, st, cfg, count: int):
+    """The `count` strongest distinct periods of the star's signal_search
+    rows (the candidates the pipeline's evidence step would see)."""
+    rows, _, _ = gpu.signal_search(st, cfg)
+    periods = []
+    for i in np.argsort(-rows[:, 3]):
+        p = float(rows[i, 0])
+        if all(abs(p - q) > 1e-3 * q for q in periods):
+            periods.append(p)
+        if len(periods) == count:
+            break
+    return periods
+
+
+def run_evidence(args):
+    """Evidence (model comparison): a step is one fbls_compare_batch of
+    --candidates trial periods of the 13-sector star (its strongest distinct
+    signal_search periods; the family resident). value: candidates per second
+    of device time (CUDA events around the batch on the context's stream);
+    e2e: of the whole call with the rows back on the host."""
+    import torch
+    import oracle
+    from fbls_b200 import api, synth
+    torch.cuda.set_device(0)
+    c, cfg = synth.multi_sector(), synth.multi_sector_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    gpu = api.Gpu(0)
+    dev = gpu.upload(st)
+    periods = _evidence_candidates(gpu, st, cfg, args.candidates)
+    cands = [(st, p) for p in periods]
+    devs = [dev] * len(cands)
+    for _ in range(args.warmup):
+        got = gpu.compare_batch(cands, cfg, devs=devs)
+    gpu.counters(reset=True)
+    clocks = Clocks(0)
+    clocks.start()
+    walls, dev_ms = [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gpu.timer_start()
+        got = gpu.compare_batch(cands, cfg, devs=devs)
+        dev_ms.append(gpu.timer_stop())
+        walls.append((time.perf_counter() - t0) * 1e3)
+    clk = clocks.stop()
+    ctr = gpu.counters(reset=True)
+    ms = sum(dev_ms) / len(dev_ms)
+    wall = sum(walls) / len(walls)
+    nrows = sum(len(g) for g in got)
+    out = {
+        "metric": "evidence candidates/s", "value": len(cands) / (ms * 1e-3), "unit": "candidates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"evidence: {len(cands)} candidates of the 13-sector star (247,104 observations, "
+                               f"20 durations 0.5-15 h, periods {min(periods):.3f}-{max(periods):.3f} d), "
+                               "planet / binary / noise comparison per candidate",
+                   "candidates": len(cands), "rows": nrows},
+        "step_ms": [round(t, 3) for t in dev_ms],
+        "gpu_launches": int(ctr["launches"]) // args.steps,
+        "e2e": {"value": len(cands) / (wall * 1e-3), "unit": "candidates/s", "ms_per_step": wall,
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 2 * 13 * 8 * len(cands)},
+        "clocks": clk,
+    }
+    if not args.no_cpu:
+        ost = oracle.family_state(c.time, c.flux, c.flux_err, cfg.durations_days())
+        sample = periods[:4]
+        t0 = time.perf_counter()
+        want = [oracle.compare_search(ost, p, cfg) for p in sample]
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": len(sample) / sec, "unit": "candidates/s", "cores": 1, "kind": "port",
+                               "sample": f"the first {len(sample)} candidates on the oracle, single thread, "
+                                         f"{sec:.2f} s"}
+        ok = True
+        for g, w in zip(got[:len(sample)], want):
+            ok = ok and len(g) == len(w) and all(
+                a["selection_flags"] == b["selection_flags"] and a["epoch"] == b["epoch"] and
+                abs(a["log_bf_planet_noise"] - b["log_bf_planet_noise"]) <= 1e-9 * max(1.0, abs(b["log_bf_planet_noise"]))
+                for a, b in zip(g, w))
+        out["parity"] = bool(ok)
+    print(json.dumps(out))
+    dev.free()
+    gpu.close()
+
+
 def run_detrend(args):
     """Biweight detrending: a step is one
     fbls_biweight_flatten of the 13-sector curve (247,104 observations at
@@ -870,7 +954,8 @@ def main():
     ap.add_argument("--impl", default="fbls_b200", choices=["fbls_b200", "reference"])
     ap.add_argument("--workload", default="multi_sector",
                     choices=["multi_sector", "single_sector", "survey", "proposal", "rescore", "single_event",
-                             "detrend"])
+                             "detrend", "evidence"])
+    ap.add_argument("--candidates", type=int, default=32, help="evidence workload: candidates per batch")
     ap.add_argument("--rows", type=int, default=8192, help="rescore workload: rows per step")
     ap.add_argument("--stars", type=int, default=512, help="survey workload: stars per GPU")
     ap.add_argument("--batch-workers", type=int, default=0,
@@ -899,6 +984,8 @@ def main():
         run_single_event(args)
     elif args.workload == "detrend":
         run_detrend(args)
+    elif args.workload == "evidence":
+        run_evidence(args)
     else:
         run_gpu(args)
 

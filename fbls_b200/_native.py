@@ -135,6 +135,12 @@ class EvidenceRow(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class EvidenceJob(C.Structure):
+    _fields_ = [("ready", C.c_void_p), ("period", C.c_double), ("durations", C.POINTER(C.c_double)),
+                ("rho", C.POINTER(C.c_double)), ("nd", C.c_uint32), ("rows", EvidenceRow * 2),
+                ("n_rows", C.c_uint32), ("status", C.c_int)]
+
+
 class PrepConfig(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("bin_minutes", "window_min", "window_factor", "window_max", "clip_sigma",
                                            "edge_trim")]
@@ -189,6 +195,7 @@ SIGNATURES = {
                                  C.POINTER(ScanStats)]),
     "fbls_compare_search": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, c_double_p, C.c_uint32, C.c_double,
                                       C.POINTER(Config), C.POINTER(EvidenceRow), c_uint32_p]),
+    "fbls_compare_batch": (C.c_int, [C.c_void_p, C.POINTER(EvidenceJob), C.c_uint32, C.POINTER(Config)]),
     "fbls_scan_bank_static": (C.c_int, [C.c_int, c_double_p, c_double_p, c_double_p, C.c_uint32, C.c_double,
                                         c_double_p, C.c_uint32, C.POINTER(Bank), C.c_uint32, C.c_uint32,
                                         c_double_p, c_double_p, c_double_p, c_uint32_p, C.c_char_p,

@@ -549,6 +549,40 @@ class Gpu:
                 dev.free()
 
 
+    def compare_batch(self, candidates: Sequence[Tuple[FamilyState, float]], cfg: SearchConfig,
+                      devs: Optional[Sequence[DeviceReady]] = None) -> List[List[dict]]:
+        """Evidence rows of many (family, period) candidates in one batch
+        (fbls_compare_batch): for each candidate the rows compare_search gives.
+        devs: the families already uploaded (one per candidate), else each
+        distinct family is uploaded for the call."""
+        uploaded: List[DeviceReady] = []
+        try:
+            if devs is None:
+                seen = {}
+                devs = []
+                for st, _ in candidates:
+                    if id(st) not in seen:
+                        seen[id(st)] = self.upload(st)
+                        uploaded.append(seen[id(st)])
+                    devs.append(seen[id(st)])
+            c, keep = _config(cfg)
+            jobs = (N.EvidenceJob * max(1, len(candidates)))()
+            arrays = []
+            for i, ((st, period), dev) in enumerate(zip(candidates, devs)):
+                d, r = _f64(st.durations), _f64(st.rho)
+                arrays.append((d, r))
+                jobs[i].ready = dev.handle
+                jobs[i].period = float(period)
+                jobs[i].durations = _dptr(d)
+                jobs[i].rho = _dptr(r)
+                jobs[i].nd = len(d)
+            self._check(self.lib.fbls_compare_batch(self.ctx, jobs, len(candidates), C.byref(c)))
+            return [[jobs[i].rows[k].as_dict() for k in range(jobs[i].n_rows)] for i in range(len(candidates))]
+        finally:
+            for dev in uploaded:
+                dev.free()
+
+
 def _grid_count(state: FamilyState, cfg: SearchConfig) -> int:
     """Length of the period grid signal_search scans (an upper bound on its rows)."""
     dmin = float(np.min(state.durations))

@@ -26,6 +26,7 @@
 // prefix_block (kernels.rs:237-309), one warp per (period, field) row, and
 // are written as f64 and (hi, lo) f32 pairs.
 
+#include "bulk.cuh"
 #include "common.cuh"
 #include "kernels.h"
 
@@ -199,7 +200,8 @@ __device__ __forceinline__ double prefix_segment(const HistRow& r, int nb, int s
     return total;
 }
 
-__global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
+// The staged-by-threads fold of CTA `cta` (periods cta * G ..) of one fold.
+__device__ __forceinline__ void fold_smem_cta(const FoldArgs& a, int cta) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ double s_scale[MAX_GROUP];
 
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
     const int G = a.group;          // periods per CTA, a power of two
     const int wpp = (T / 32) / G;   // warps per period (>= 1)
     const int NS = wpp * 32;        // segments per period
-    const int g0 = blockIdx.x * G;
+    const int g0 = cta * G;
     const int g = min(G, a.periods - g0);
     const int q = warp / wpp;
     const int seg = (warp - q * wpp) * 32 + lane;
@@ -229,7 +231,7 @@ __global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
     double* hw = hv + (size_t)G * rs;
     uint32_t* hc = reinterpret_cast<uint32_t*>(hw + (size_t)G * rs);
     if (a.hist_global) {
-        hv = a.hist_global + (size_t)blockIdx.x * G * rs * 3;
+        hv = a.hist_global + (size_t)cta * G * rs * 3;
         hw = hv + (size_t)G * rs;
         hc = reinterpret_cast<uint32_t*>(hw + (size_t)G * rs);
     }
@@ -343,56 +345,31 @@ __global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) {
     }
 }
 
+__global__ void __launch_bounds__(1024, 1) k_fold(FoldArgs a) { fold_smem_cta(a, blockIdx.x); }
+
+// Many staged-by-threads folds in one launch: CTA c runs CTA c - cta0[j] of
+// job j, where cta0[j] <= c < cta0[j + 1] (every job with the same CTA size).
+__global__ void __launch_bounds__(1024, 1) k_fold_jobs(const FoldArgs* __restrict__ jobs, const int* __restrict__ cta0,
+                                                       int njobs) {
+    int lo = 0, hi = njobs - 1;
+    const int c = blockIdx.x;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (cta0[mid] <= c)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    fold_smem_cta(jobs[lo], c - cta0[lo]);
+}
+
 // ---------------------------------------------------------------------------
 // TMA staging: mbarrier helpers and the bulk copies of one chunk.
 
 namespace {
 
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-
-// Waits for the barrier phase with a bounded number of polls; false when the
-// copies did not land in time.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-    for (uint32_t i = 0; i < (1u << 20); ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
 // Issues the three bulk copies of chunk [i0, i1), rounded out to whole
 // 16-byte pieces, into one staging buffer (fields at `field` doubles apart).
-// Named barrier `id` over `threads` threads of the CTA.
-__device__ __forceinline__ void group_sync(uint32_t id, uint32_t threads) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
-}
-
 __device__ __forceinline__ void stage_chunk(const FoldArgs& a, int i0, int i1, double* buf, int field, uint32_t bar) {
     const int a0 = i0 & ~1, a1 = (i1 + 1) & ~1;
     const uint32_t bytes = (uint32_t)(a1 - a0) * (uint32_t)sizeof(double);
@@ -915,11 +892,33 @@ bool fold_job_ok(const FoldArgs& a, const FoldShape& shape) {
     return shape.kind == FOLD_WALK && shape.smem <= MAX_FOLD_SMEM && a.group == shape.group && a.group >= 1 &&
            a.group <= MAX_GROUP && (a.group & (a.group - 1)) == 0 && shape.threads == 1024 && a.nchunks >= 1 &&
            a.nb >= 2 && a.stage_field == WALK_CAP + 2 && shape.chunk_cap == WALK_CAP &&
-           a.row_stride == shape.row_stride && a.row_stride >= a.nb && a.fault != nullptr && a.hist_out == nullptr &&
-           a.time && a.v && a.w && a.scales && a.chunks && (a.map_out || (a.cum && a.cum32)) &&
+           a.row_stride == shape.row_stride && a.row_stride >= a.nb && a.fault != nullptr &&
+           (a.hist_out == nullptr || (a.group == 1 && a.periods == 1 && a.map_out == nullptr)) &&
+           a.time && a.v && a.w && a.scales && a.chunks && (a.map_out || a.hist_out || (a.cum && a.cum32)) &&
            (!a.map_out || (a.map_nd >= 1 && a.map_nd <= MAP_MAX_DURATIONS && a.map_durations && a.map_rho)) &&
            !(reinterpret_cast<uintptr_t>(a.time) & 15) && !(reinterpret_cast<uintptr_t>(a.v) & 15) &&
            !(reinterpret_cast<uintptr_t>(a.w) & 15);
+}
+
+bool fold_smem_job_ok(const FoldArgs& a, const FoldShape& shape) {
+    return shape.kind == FOLD_SMEM && shape.smem <= MAX_FOLD_SMEM && a.group == shape.group && a.group >= 1 &&
+           a.group <= MAX_GROUP && (a.group & (a.group - 1)) == 0 && a.nchunks >= 1 &&
+           (shape.threads == 1024 || shape.threads == 512) && a.group <= shape.threads / 32 &&
+           a.stage_field == shape.stage_field && a.row_stride == shape.row_stride &&
+           (shape.hist_in_smem || a.hist_global != nullptr) && a.map_out == nullptr && a.time && a.v && a.w &&
+           a.scales && a.chunks && (a.hist_out ? (a.group == 1 && a.periods == 1) : (a.cum && a.cum32));
+}
+
+cudaError_t launch_fold_smem_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads, size_t smem,
+                                  cudaStream_t stream) {
+    if (njobs < 1 || ctas < 1 || smem > MAX_FOLD_SMEM || (threads != 1024 && threads != 512))
+        return cudaErrorInvalidValue;
+    // Set at every launch, as for the other fold kernels.
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_fold_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
+    if (e != cudaSuccess) return e;
+    k_fold_jobs<<<ctas, threads, smem, stream>>>(jobs, cta0, njobs);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream) {

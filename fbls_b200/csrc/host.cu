@@ -1318,17 +1318,66 @@ int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* du
                         uint32_t* n_rows) {
     if (!ctx || !ready || !durations || !rho || !cfg || !rows_out || !n_rows)
         return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
-    CK(cudaSetDevice(ctx->device), "set device");
-    EvidenceReady er{ready->time, ready->v, ready->w, ready->n, ready->baseline_norm, ready->origin,
-                     ready->residual_energy, ready->t_last, ready->time_host.data()};
-    std::string message;
-    int rc = compare_search(ctx->stream, ctx->evidence.ptr, ctx->evidence.bytes, er, durations, rho, nd, period, *cfg,
-                            rows_out, n_rows, message, [&](size_t bytes) -> void* {
-                                if (ensure(ctx->evidence, bytes) != cudaSuccess) return nullptr;
-                                return ctx->evidence.ptr;
-                            });
-    if (rc) return fail(ctx, rc, message);
+    *n_rows = 0;
+    fbls_evidence_job job{};
+    job.ready = ready;
+    job.period = period;
+    job.durations = durations;
+    job.rho = rho;
+    job.nd = nd;
+    const int rc = fbls_compare_batch(ctx, &job, 1, cfg);
+    if (rc) return rc;
+    for (uint32_t i = 0; i < job.n_rows; i++) rows_out[i] = job.rows[i];
+    *n_rows = job.n_rows;
     return FBLS_OK;
+}
+
+int fbls_compare_batch(fbls_ctx* ctx, fbls_evidence_job* jobs, uint32_t count, const fbls_config* cfg) {
+    if (!ctx || !cfg || (count && !jobs)) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (count == 0) return FBLS_OK;
+    CK(cudaSetDevice(ctx->device), "set device");
+    std::vector<EvidenceCandidate> cands(count);
+    for (uint32_t i = 0; i < count; i++) {
+        fbls_evidence_job& J = jobs[i];
+        J.n_rows = 0;
+        J.status = FBLS_OK;
+        EvidenceCandidate& E = cands[i];
+        E.durations = J.durations;
+        E.rho = J.rho;
+        E.nd = J.nd;
+        E.period = J.period;
+        const fbls_ready* r = J.ready;
+        if (r && r->device != ctx->device) {
+            J.status = FBLS_ERR_ARGUMENT;
+            return fail(ctx, FBLS_ERR_ARGUMENT,
+                        "candidate " + std::to_string(i) + ": family uploaded to another device");
+        }
+        E.r = r ? EvidenceReady{r->time, r->v, r->w, r->n, r->baseline_norm, r->origin, r->residual_energy,
+                                r->t_last, r->time_host.data()}
+                : EvidenceReady{};
+    }
+    std::string message;
+    uint64_t launched = 0;
+    const int rc = compare_batch(ctx->stream, cands.data(), count, *cfg, message,
+                                 [&](size_t bytes) -> void* {
+                                     if (ensure(ctx->evidence, bytes) != cudaSuccess) return nullptr;
+                                     return ctx->evidence.ptr;
+                                 },
+                                 ctx->sm_count, &launched);
+    ctx->counters.launches += launched;
+    if (rc) return fail(ctx, rc, message);
+    int first = FBLS_OK;
+    for (uint32_t i = 0; i < count; i++) {
+        fbls_evidence_job& J = jobs[i];
+        J.status = cands[i].status;
+        J.n_rows = cands[i].n_rows;
+        for (uint32_t k = 0; k < J.n_rows; k++) J.rows[k] = cands[i].rows[k];
+        if (J.status && first == FBLS_OK) {
+            first = J.status;
+            fail(ctx, J.status, "candidate " + std::to_string(i) + ": " + cands[i].message);
+        }
+    }
+    return first;
 }
 
 // Many stars on one device: `workers` host threads (the caller's included),

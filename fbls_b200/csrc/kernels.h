@@ -200,7 +200,14 @@ int fold_chunks(const double* time, int n, double scale_max, int nb, int span_ca
 cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream);
 // Job launches (the batched search): jobs and their first CTA / period
 // offsets (njobs + 1 entries, the last = total) live in device memory.
-bool fold_job_ok(const FoldArgs& a, const FoldShape& shape);  // a walking-fold job within limits
+// A walking-fold job within limits. A job may write one period's raw
+// histogram (hist_out, group 1) instead of prefix rows.
+bool fold_job_ok(const FoldArgs& a, const FoldShape& shape);
+// A staged-by-threads (FOLD_SMEM) fold job within limits, and the launch of
+// many of them with one CTA size.
+bool fold_smem_job_ok(const FoldArgs& a, const FoldShape& shape);
+cudaError_t launch_fold_smem_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads, size_t smem,
+                                  cudaStream_t stream);
 cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, size_t smem,
                              cudaStream_t stream);
 cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, cudaStream_t stream);

@@ -180,6 +180,10 @@ def search_families(gpu: api.Gpu, fams: List[Tuple[Curve, List[int]]], durations
     if cfg.model_comparison and peaks:
         ev_start = _time.perf_counter()
         order = sorted(range(len(peaks)), key=lambda i: -peaks[i].snr)
+        # Every candidate's family (the others' transits masked), then one
+        # batched evidence call for all of them (fbls_compare_batch); the rows
+        # are those of one compare_search per peak (pipeline.rs:169-192).
+        chosen, cands = [], []
         for index in order[:cfg.evidence_candidates]:
             peak = peaks[index]
             base = original[peak.family]
@@ -190,7 +194,10 @@ def search_families(gpu: api.Gpu, fams: List[Tuple[Curve, List[int]]], durations
             if curve.time.shape[0] < 6:
                 continue
             state = family_state(curve, base.durations, base.indices, cfg.correlated_noise)
-            rows = gpu.compare_search(state.state, peak.period_days, cfg)
+            chosen.append(peak)
+            cands.append((state.state, peak.period_days))
+        results = gpu.compare_batch(cands, cfg) if cands else []
+        for peak, rows in zip(chosen, results):
             row = next((r for r in rows if int(r["selection_flags"]) & 1), rows[0] if rows else None)
             if row is None:
                 continue

@@ -14,6 +14,8 @@
  *   fbls_scan_bank               <- scan_bank (every period's   src/search/scan.rs:144-357
  *                                   winner at one nb)
  *   fbls_compare_search          <- compare_search              src/search/evidence.rs:693-1003
+ *   fbls_compare_batch           <- the pipeline's evidence loop src/pipeline.rs:169-192
+ *                                   (compare_search per peak)
  *
  * Host-side mirror (C++ restatements of the Rust host functions around the
  * path, for callers that do not have the Rust host):
@@ -184,6 +186,31 @@ int fbls_scan_bank(fbls_ctx* ctx, const fbls_ready* ready, const double* periods
 int fbls_compare_search(fbls_ctx* ctx, const fbls_ready* ready, const double* durations, const double* rho,
                         uint32_t nd, double period, const fbls_config* cfg, fbls_evidence_row* rows_out,
                         uint32_t* n_rows);
+
+/* One candidate of fbls_compare_batch: an uploaded family, one trial
+ * period and the family's nd durations (days) and correlated-noise factors
+ * (host arrays, any order). Outputs: rows[0 .. n_rows) (0, 1 or 2 rows, as
+ * fbls_compare_search writes them) and the candidate's status. */
+typedef struct {
+    const fbls_ready* ready;
+    double period;
+    const double* durations;
+    const double* rho;
+    uint32_t nd;
+    fbls_evidence_row rows[2];
+    uint32_t n_rows;
+    int status;
+} fbls_evidence_job;
+
+/* compare_search (evidence.rs:693-1003) for many candidates at once: the
+ * pipeline's evidence loop (src/pipeline.rs:169-192, one compare_search per
+ * peak, up to evidence_candidates of them) or several stars' peaks. Every
+ * candidate's fold, prefix sums, screen, pilot and joint tiles run as shared
+ * launches on the context's stream with one synchronisation; the rows are
+ * those of one fbls_compare_search per candidate. Returns 0, or the first
+ * failing candidate's status ("candidate i: " message); every candidate's
+ * own status is in its record. */
+int fbls_compare_batch(fbls_ctx* ctx, fbls_evidence_job* jobs, uint32_t count, const fbls_config* cfg);
 
 /* ---- no device allocation ----------------------------------------------
  * No counterpart in the reference. For callers that cannot call cudaMalloc

@@ -64,6 +64,9 @@ class OracleGpu:
     def compare_search(self, state, period, cfg):
         return oracle.compare_search(state, period, cfg)
 
+    def compare_batch(self, candidates, cfg, devs=None):
+        return [oracle.compare_search(state, period, cfg) for state, period in candidates]
+
     def rescore_rows(self, dev, excluded, rows):
         s = dev.state
         return oracle.rescore_rows(s.time, s.v, s.w, excluded, rows, s.origin)

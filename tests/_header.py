@@ -23,8 +23,10 @@ def structs() -> dict:
         for decl in body.split(";"):
             decl = decl.strip()
             if decl:
-                m = re.fullmatch(r"(.+?)\s*\b(\w+)", decl, flags=re.S)
-                fields.append((m.group(2), c_type(m.group(1))))
+                # an array field keeps its extent in the type: 'fbls_evidence_row[2]'
+                m = re.fullmatch(r"(.+?)\s*\b(\w+)\s*(\[\s*\d+\s*\])?", decl, flags=re.S)
+                extent = m.group(3).replace(" ", "") if m.group(3) else ""
+                fields.append((m.group(2), c_type(m.group(1)) + extent))
         out[name] = fields
     return out
 

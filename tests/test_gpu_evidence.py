@@ -35,6 +35,14 @@ def _check_rows(g, o):
                 assert gr[k] == orr[k], k
 
 
+def _same_rows(a, b):
+    """Bit-identical rows (NaN fields equal to NaN)."""
+    assert len(a) == len(b)
+    for x, y in zip(a, b):
+        assert x.keys() == y.keys()
+        assert np.array_equal(np.array([float(x[k]) for k in x]), np.array([float(y[k]) for k in y]), equal_nan=True)
+
+
 @pytest.fixture(scope="module")
 def small():
     c = synth.small_curve()
@@ -69,6 +77,75 @@ def test_compare_search_single_sector(gpu):
     ost = oracle.family_state(c.time, c.flux, c.flux_err, cfg.durations_days())
     for period in (c.period, 2.0 * c.period, 5.123):
         _check_rows(gpu.compare_search(st, period, cfg), oracle.compare_search(ost, period, cfg))
+
+
+@pytest.fixture(scope="module")
+def multi():
+    c = synth.multi_sector()
+    cfg = synth.multi_sector_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    ost = oracle.family_state(c.time, c.flux, c.flux_err, cfg.durations_days())
+    return c, cfg, st, ost
+
+
+@pytest.mark.parametrize("factor", [1.0, 2.0, 0.5])
+def test_compare_search_parity_thirteen_sectors(gpu, multi, factor):
+    # The 13-sector star at its injected 17.3 d period (nb 3,324, 2 nb 6,648,
+    # 52 tiles: prefix rows read from global memory), and at 2x and 1/2x.
+    c, cfg, st, ost = multi
+    period = c.period * factor
+    g = gpu.compare_search(st, period, cfg)
+    o, diag = oracle.compare_search(ost, period, cfg, diag=True)
+    _check_rows(g, o)
+    if factor == 1.0:
+        assert int(diag["nb"]) == 3324 and int(diag["tiles"]) == 52
+        assert g, "the injected box must pass the evidence screen"
+
+
+def test_compare_batch_equals_one_call_per_candidate(gpu, multi, small):
+    # Candidates of three families in one batch (every launch class: staged
+    # rows of a few KB, of ~160 KB and rows left in global memory) against one
+    # compare_search each and against the oracle.
+    c, cfg, st, ost = multi
+    cs, cfgs, sst, sost = small
+    rows, _, _ = gpu.signal_search(st, cfg)
+    order = np.argsort(-rows[:, 3])
+    periods = []
+    for i in order:
+        p = float(rows[i, 0])
+        if all(abs(p - q) > 1e-3 * q for q in periods):
+            periods.append(p)
+        if len(periods) == 12:
+            break
+    periods += [c.period, 1.7, 3.1]
+    cands = [(st, p) for p in periods]
+    got = gpu.compare_batch(cands, cfg)
+    for (s_, p), g in zip(cands, got):
+        _same_rows(g, gpu.compare_search(s_, p, cfg))
+        _check_rows(g, oracle.compare_search(ost, p, cfg))
+    # the small star has its own config: a second batch with both stars' bands
+    got_small = gpu.compare_batch([(sst, 1.3), (sst, 0.9), (sst, 2.6)], cfgs)
+    for p, g in zip((1.3, 0.9, 2.6), got_small):
+        _check_rows(g, oracle.compare_search(sost, p, cfgs))
+
+
+def test_compare_batch_on_masked_families(gpu, multi):
+    # The pipeline masks the other peaks out of each candidate's family, so a
+    # batch holds several families of different lengths.
+    c, cfg, st, ost = multi
+    rng = np.random.default_rng(11)
+    cands, ocands = [], []
+    for k in range(4):
+        centre = c.time[0] + rng.uniform(0.0, c.time[-1] - c.time[0])
+        keep = np.abs(c.time - centre) > 0.5 + 0.5 * k
+        s_ = api.prepared_family(c.time[keep], c.flux[keep], c.flux_err[keep], cfg)
+        o_ = oracle.family_state(c.time[keep], c.flux[keep], c.flux_err[keep], cfg.durations_days())
+        p = c.period * (1.0 + 0.01 * k)
+        cands.append((s_, p))
+        ocands.append((o_, p))
+    got = gpu.compare_batch(cands, cfg)
+    for g, (o_, p) in zip(got, ocands):
+        _check_rows(g, oracle.compare_search(o_, p, cfg))
 
 
 def test_compare_search_below_threshold_returns_nothing(gpu, small):

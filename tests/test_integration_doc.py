@@ -22,6 +22,9 @@ def _snake(name: str) -> str:
 def _rust_type(text: str) -> str:
     """The C spelling of a Rust FFI type."""
     t = text.strip()
+    a = re.fullmatch(r"\[\s*(.+?)\s*;\s*(\d+)\s*\]", t)
+    if a:  # [T; N] -> T[N]
+        return f"{_rust_type(a.group(1))}[{a.group(2)}]"
     m = re.fullmatch(r"\*(const|mut)\s+(.+)", t)
     if m:
         inner = _rust_type(m.group(2))

@@ -41,6 +41,9 @@ class _OracleGpu:
     def compare_search(self, state, period, cfg):
         return oracle.compare_search(state, period, cfg)
 
+    def compare_batch(self, candidates, cfg, devs=None):
+        return [oracle.compare_search(state, period, cfg) for state, period in candidates]
+
     def single_event_search(self, state, cfg, capacity=131072, dev=None):
         return oracle.single_event_search(state, cfg, capacity)
 
