@@ -391,11 +391,66 @@ def run_gpu(args):
         st, every, threads, tr, sec = _cpu_sample(curve, cfg, args.cpu_seconds)
         out["cpu_baseline"] = {"value": tr / sec, "unit": UNIT, "cores": threads, "kind": "port",
                                "sample": f"every {every}th period of each band, {tr} trials, {sec:.1f} s"}
-    print(json.dumps(out))
     dev.free()
+    if world == 1 and args.extras_stars > 0:
+        out.update(_metric_second_half(gpu, args.extras_stars))
+    print(json.dumps(out))
     gpu.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def _metric_second_half(gpu, count: int) -> dict:
+    """The metric's other parts on `count` seeded survey stars (held out from
+    the proposal network's training seeds): the batched exhaustive search's
+    stars/s (resident families, and end to end with host families), and the
+    proposal-pruned search against it (stars/s, speed-up, top-1 recall: the
+    pruned search's best row is the exhaustive best row). Host clock around
+    each device-synchronised batch; one warm-up, two timed steps each."""
+    import torch
+    from fbls_b200 import proposal as pr
+    stars, cfg = _survey(count, 1000)
+    pstars = [(s, p) for _, s, p in stars]
+    states, pmax = [s for s, _ in pstars], [p for _, p in pstars]
+    devs = [gpu.upload(s) for s in states]
+    net = pr.load_net(0)
+
+    def timed(fn, steps=2):
+        fn()
+        out, ts = None, []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            ts.append(time.perf_counter() - t0)
+        return out, sum(ts) / len(ts), ts
+
+    full, t_ex, ts_ex = timed(lambda: gpu.search_batch(states, cfg, period_max=pmax, devs=devs, workers=0))
+    _, t_e2e, _ = timed(lambda: gpu.search_batch(states, cfg, period_max=pmax, workers=0), steps=1)
+    (pruned, _), t_pr, ts_pr = timed(lambda: pr.search_proposed(gpu, net, pstars, devs, cfg, k=1, workers=0))
+    hits = labelled = 0
+    for (fr, _, _), (pr_rows, _, _) in zip(full, pruned):
+        if fr.shape[0] == 0:
+            continue
+        labelled += 1
+        best = fr[int(np.argmax(fr[:, 3]))]
+        hits += int(pr_rows.shape[0] > 0 and np.array_equal(pr_rows[int(np.argmax(pr_rows[:, 3]))], best))
+    trials = sum(t for _, _, t in full)
+    for d in devs:
+        d.free()
+    desc = (f"{count} seeded survey stars (1-13 sectors ~ Geometric(0.4), cadence 120/200/600 s, white + AR(1) "
+            "noise, 30 % with a box), 20 durations 0.5-15 h, periods 0.5-min(20, baseline/2) d")
+    return {
+        "survey": {"stars": count, "workload": desc, "stars_per_s": count / t_ex, "trials_per_s": trials / t_ex,
+                   "step_ms": [round(1e3 * t, 1) for t in ts_ex],
+                   "e2e_stars_per_s": count / t_e2e, "e2e_h2d_bytes": 24 * sum(s.n for s in states),
+                   "timing": "host clock around the device-synchronised fbls_search_batch (stars fused)"},
+        "proposal": {"stars": count, "exhaustive_stars_per_s": count / t_ex, "proposal_stars_per_s": count / t_pr,
+                     "speedup": t_ex / t_pr, "top1_recall": hits / max(labelled, 1),
+                     "stars_with_detection": labelled, "bands_searched": 1, "bands": pr.BANDS,
+                     "step_ms": [round(1e3 * t, 1) for t in ts_pr],
+                     "timing": "host clock around coarse maps + network + pruned fbls_search_batch"},
+    }
 
 
 def _survey(count: int, seed: int):
@@ -577,6 +632,128 @@ def run_proposal(args):
             "achieved": achieved, "peak": tpeak, "peak_kind": tkind, "unit": "TFLOP/s", "frac": achieved / tpeak,
             "flops_per_curve": _network_flops(1),
             "note": "host clock around the band scores of the last step (feature upload, forward, logits download)"}
+    print(json.dumps(out))
+    for d in devs:
+        d.free()
+    gpu.close()
+
+
+def _full_chunk(seed: int, start: int, count: int):
+    """Stars [start, start + count) of the survey-scale batch (one seeded
+    stream per star): prepared families and what was injected."""
+    from fbls_b200 import api, synth
+    out = []
+    for i in range(start, start + count):
+        c = synth.survey_star_full(np.random.default_rng([seed, i]))
+        cfg = synth.survey_config(c)
+        st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+        out.append((st, cfg.period_max, c.label, c.period))
+    return out
+
+
+def run_full(args):
+    """Survey-scale full form: --stars seeded stars (8 % boxes, 2 %
+    eclipsing-binary-like pairs); a step is the proposal-pruned search of all
+    of them followed by the evidence comparison (null, box, box plus
+    secondary) of each star's best candidate, in batches. Also timed once:
+    the exhaustive batched search, the reference for top-1 recall. Host clock
+    around device-synchronised calls."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    import torch
+    chunk = 250
+    with cf.ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1), mp_context=mp.get_context("spawn")) as ex:
+        parts = list(ex.map(_full_chunk, [2000] * ((args.stars + chunk - 1) // chunk),
+                            range(0, args.stars, chunk), [min(chunk, args.stars - s) for s in range(0, args.stars, chunk)]))
+    stars = [x for p in parts for x in p]
+    from fbls_b200 import api, synth
+    from fbls_b200 import proposal as pr
+    torch.cuda.set_device(0)
+    cfg = synth.survey_config(synth.survey_star(np.random.default_rng(0)))
+    gpu = api.Gpu(0)
+    states, pmax = [s for s, _, _, _ in stars], [p for _, p, _, _ in stars]
+    devs = [gpu.upload(s) for s in states]
+    net = pr.load_net(0)
+    pstars = list(zip(states, pmax))
+
+    def full_form():
+        t0 = time.perf_counter()
+        pruned, _ = pr.search_proposed(gpu, net, pstars, devs, cfg, k=1, workers=0)
+        t1 = time.perf_counter()
+        idx, cands, cdevs = [], [], []
+        for i, (rows, _, _) in enumerate(pruned):
+            if rows.shape[0]:
+                idx.append(i)
+                cands.append((states[i], float(rows[int(np.argmax(rows[:, 3])), 0])))
+                cdevs.append(devs[i])
+        ev = []
+        for s in range(0, len(cands), 1024):
+            ev += gpu.compare_batch(cands[s:s + 1024], cfg, devs=cdevs[s:s + 1024])
+        t2 = time.perf_counter()
+        return pruned, idx, ev, (t1 - t0, t2 - t1)
+
+    # warm-up on a slice, then the timed full form
+    sub = slice(0, min(256, len(states)))
+    pr.search_proposed(gpu, net, pstars[sub], devs[sub], cfg, k=1, workers=0)
+    gpu.compare_batch([(states[0], 1.0)], cfg, devs=[devs[0]])
+    gpu.set_kernel_timing(True)
+    gpu.counters(reset=True)
+    clocks = Clocks(0)
+    clocks.start()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pruned, idx, ev, (t_search, t_ev) = full_form()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    ctr = gpu.counters(reset=True)
+    gpu.set_kernel_timing(False)
+    parts_ms = dict(pr.search_proposed.last_ms)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    full = gpu.search_batch(states, cfg, period_max=pmax, devs=devs, workers=0)
+    t_ex = time.perf_counter() - t0
+    hits = labelled = 0
+    pairs = pair_binary = 0
+    evmap = dict(zip(idx, ev))
+    for i, ((fr, _, _), (prr, _, _)) in enumerate(zip(full, pruned)):
+        if fr.shape[0]:
+            labelled += 1
+            best = fr[int(np.argmax(fr[:, 3]))]
+            hits += int(prr.shape[0] > 0 and np.array_equal(prr[int(np.argmax(prr[:, 3]))], best))
+        if "pair" in stars[i][2] and i in evmap and evmap[i]:
+            pairs += 1
+            row = next((r for r in evmap[i] if r["selection_flags"] & 1), evmap[i][0])
+            pair_binary += int(row["log_bf_binary_noise"] > row["log_bf_planet_noise"])
+    peak, peak_kind = _peaks()
+    tpeak, tkind = _bf16_peak()
+    fold_launches = max(ctr["fold_launches"], 1)
+    fold_ms = ctr["fold_ms"] / fold_launches
+    hbm = ctr["fold_bytes"] / fold_launches / (fold_ms * 1e-3) / 1e9 if fold_ms > 0 else 0.0
+    net_s = parts_ms.get("network", 0.0) * 1e-3
+    tflops = _network_flops(len(states)) / net_s / 1e12 if net_s > 0 else 0.0
+    n_obs = sum(s.n for s in states)
+    out = {
+        "metric": METRIC, "value": len(states) / wall, "unit": "stars/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 search and evidence, bf16 network", "data": "synthetic",
+        "config": {"workload": f"full: {len(states)} seeded survey stars (1-13 sectors ~ Geometric(0.4), cadence "
+                               "120/200/600 s, white + AR(1) noise; 8 % boxes, 2 % eclipsing-binary-like pairs "
+                               "with unequal depths 1-20 %); proposal (1 of 32 bands) -> pruned search -> "
+                               "evidence of each star's best candidate",
+                   "stars": len(states), "observations": n_obs,
+                   "boxes": sum("box" in x[2] for x in stars), "pairs": sum("pair" in x[2] for x in stars)},
+        "seconds": {"proposal_and_pruned_search": t_search, "evidence": t_ev, **{k: v / 1e3 for k, v in parts_ms.items()}},
+        "evidence_candidates": len(ev), "evidence_candidates_per_s": len(ev) / t_ev if t_ev > 0 else None,
+        "exhaustive_stars_per_s": len(states) / t_ex, "speedup_vs_exhaustive_search": t_ex / wall,
+        "top1_recall": hits / max(labelled, 1), "stars_with_detection": labelled,
+        "pairs_with_evidence": pairs, "pairs_binary_preferred": pair_binary,
+        "roofline": {"hbm": {"kernel": "fold + prefix", "achieved": hbm, "peak": peak, "peak_kind": peak_kind,
+                             "unit": "GB/s", "frac": hbm / peak},
+                     "tensor": {"kernel": "proposal network forward", "achieved": tflops, "peak": tpeak,
+                                "peak_kind": tkind, "unit": "TFLOP/s", "frac": tflops / tpeak}},
+        "gpu_launches": int(ctr["launches"]),
+        "clocks": clk,
+    }
     print(json.dumps(out))
     for d in devs:
         d.free()
@@ -880,42 +1057,78 @@ def run_detrend(args):
 
 
 def run_precision_report(args):
-    """The reference's mixed mode (f32 pre-rank from (hi, lo) pairs, f64
-    winner) against f64 ranking throughout, on every period of every band at
-    the coarse and the full nb: how often the winning template differs, and
-    the relative error of the reported power (score) and depth."""
+    """The precision forms against the FP64 reference on every period of every
+    band at the coarse and the full nb. Modes of the scan: 0, the reference's
+    mixed ranking (f32 pre-rank from compensated (hi, lo) f32 prefix pairs,
+    f64 rescans and winner); 1, f64 ranking throughout (the FP64 oracle's
+    arithmetic); 2, the f32 form (f32 ranking and winner from the (hi, lo)
+    pairs only, no f64 prefix rows written or read). Per mode against mode 1:
+    the share of periods with the same winning template (bin = phase, width,
+    shape, duration) and the relative errors of the reported power (score^2),
+    SNR (score) and depth, with the device time of the pass. And the bin
+    index: for every observation at every 8th period of each band, the fold's
+    f64 bin against an f32 product, a double-single product, and the
+    double-single product with its exact f64 fallback near integers."""
+    import torch
     from fbls_b200 import api
     curve, cfg, desc = _workload(args.workload, args.period_oversample)
     state = api.prepared_family(curve.time, curve.flux, curve.flux_err, cfg)
     grid, bands = api.band_plan(state, cfg)
-    out = {"report": "precision", "workload": desc, "passes": []}
+    out = {"report": "precision", "workload": desc, "reference": "mode 1 (f64 ranking, the FP64 oracle's arithmetic)",
+           "passes": [], "bins": []}
+    key = [2, 3, 7, 8]  # phase, width, ingress (shape), rho (duration)
     with api.Gpu(0) as gpu:
         dev = gpu.upload(state)
         for band in bands:
             bank = api.bank_for(band, cfg)
             for nb in (band["nb"] // 2, band["nb"]):
-                mixed = gpu.scan_bank(dev, band["periods"], bank, nb, precision_mode=0)
-                exact = gpu.scan_bank(dev, band["periods"], bank, nb, precision_mode=1)
-                key = [2, 3, 7, 8]  # phase, width, ingress, rho
-                same = (mixed[0][:, key] == exact[0][:, key]).all(axis=1)
-                ok = np.isfinite(exact[1]) & (exact[1] != 0)
-                rel = np.abs(mixed[1][ok] - exact[1][ok]) / np.abs(exact[1][ok])
-                rdep = np.abs(mixed[2][ok] - exact[2][ok]) / np.maximum(np.abs(exact[2][ok]), 1e-300)
-                top = ok & (exact[1] >= bank.threshold * bank.prescan_fraction)
-                reltop = np.abs(mixed[1][top] - exact[1][top]) / np.abs(exact[1][top])
-                out["passes"].append({
-                    "nb": int(nb), "periods": int(len(band["periods"])),
-                    "same_template": float(same.mean()),
-                    "max_rel_score": float(rel.max(initial=0.0)), "max_rel_depth": float(rdep.max(initial=0.0)),
-                    "periods_over_prescan_cut": int(top.sum()),
-                    "max_rel_score_over_cut": float(reltop.max(initial=0.0)),
-                    "rescanned_tiles_mixed": int(mixed[4]["tile_rescans"]),
-                })
+                res, ms = {}, {}
+                for mode in (1, 0, 2):
+                    gpu.scan_bank(dev, band["periods"], bank, nb, precision_mode=mode)  # warm
+                    torch.cuda.synchronize()
+                    gpu.timer_start()
+                    res[mode] = gpu.scan_bank(dev, band["periods"], bank, nb, precision_mode=mode)
+                    ms[mode] = gpu.timer_stop()
+                ref = res[1]
+                ok = np.isfinite(ref[1]) & (ref[1] > 0)
+                top = ok & (ref[1] >= bank.threshold)
+                rec = {"nb": int(nb), "periods": int(len(band["periods"])), "periods_over_threshold": int(top.sum()),
+                       "ms": {f"mode{m}": round(ms[m], 3) for m in ms}}
+                for mode in (0, 2):
+                    got = res[mode]
+                    same = (got[0][:, key] == ref[0][:, key]).all(axis=1)
+                    both = ok & same
+                    rs = np.abs(got[1][both] - ref[1][both]) / ref[1][both]
+                    rp = np.abs(got[1][both] ** 2 - ref[1][both] ** 2) / ref[1][both] ** 2
+                    rd = np.abs(got[2][both] - ref[2][both]) / np.maximum(np.abs(ref[2][both]), 1e-300)
+                    tb = top & same
+                    rec[f"mode{mode}"] = {
+                        "same_template": float(same[ok].mean()) if ok.any() else 1.0,
+                        "same_template_over_threshold": float(same[top].mean()) if top.any() else 1.0,
+                        "max_rel_snr": float(rs.max(initial=0.0)), "max_rel_power": float(rp.max(initial=0.0)),
+                        "max_rel_depth": float(rd.max(initial=0.0)),
+                        "p99_rel_snr": float(np.percentile(rs, 99)) if rs.size else 0.0,
+                        "max_rel_snr_over_threshold": float(
+                            (np.abs(got[1][tb] - ref[1][tb]) / ref[1][tb]).max(initial=0.0))}
+                out["passes"].append(rec)
+            scales = band["nb"] / np.asarray(band["periods"][::8], dtype=np.float64)
+            b = gpu.precision_bins(dev, scales, band["nb"])
+            b["nb"] = int(band["nb"])
+            out["bins"].append(b)
         dev.free()
     p = out["passes"]
-    out["same_template"] = float(np.average([x["same_template"] for x in p], weights=[x["periods"] for x in p]))
-    out["max_rel_score"] = max(x["max_rel_score"] for x in p)
-    out["max_rel_score_over_cut"] = max(x["max_rel_score_over_cut"] for x in p)
+    w = [x["periods"] for x in p]
+    for mode in (0, 2):
+        out[f"mode{mode}"] = {
+            "same_template": float(np.average([x[f"mode{mode}"]["same_template"] for x in p], weights=w)),
+            "max_rel_snr": max(x[f"mode{mode}"]["max_rel_snr"] for x in p),
+            "max_rel_power": max(x[f"mode{mode}"]["max_rel_power"] for x in p),
+            "max_rel_depth": max(x[f"mode{mode}"]["max_rel_depth"] for x in p),
+            "max_rel_snr_over_threshold": max(x[f"mode{mode}"]["max_rel_snr_over_threshold"] for x in p),
+            "ms": sum(x["ms"][f"mode{mode}"] for x in p)}
+    out["mode1_ms"] = sum(x["ms"]["mode1"] for x in p)
+    tot = {k: sum(b[k] for b in out["bins"]) for k in out["bins"][0] if k != "nb"}
+    out["bins_total"] = tot
     print(json.dumps(out))
 
 
@@ -954,10 +1167,11 @@ def main():
     ap.add_argument("--impl", default="fbls_b200", choices=["fbls_b200", "reference"])
     ap.add_argument("--workload", default="multi_sector",
                     choices=["multi_sector", "single_sector", "survey", "proposal", "rescore", "single_event",
-                             "detrend", "evidence"])
+                             "detrend", "evidence", "full"])
     ap.add_argument("--candidates", type=int, default=32, help="evidence workload: candidates per batch")
     ap.add_argument("--rows", type=int, default=8192, help="rescore workload: rows per step")
-    ap.add_argument("--stars", type=int, default=512, help="survey workload: stars per GPU")
+    ap.add_argument("--stars", type=int, default=None,
+                    help="survey / proposal workloads: stars per GPU (default 512); full: stars (default 10000)")
     ap.add_argument("--batch-workers", type=int, default=0,
                     help="survey / proposal workloads: search_batch host worker threads (0: stars fused into "
                          "job launches)")
@@ -965,9 +1179,13 @@ def main():
     ap.add_argument("--period-oversample", type=float, default=None,
                     help="single-star workloads: period grid density (default 3; 19 gives multi_sector's ~1.2M "
                          "periods, 6.9 single_sector's ~30k)")
+    ap.add_argument("--extras-stars", type=int, default=128,
+                    help="default workload, 1 GPU: survey stars for the metric's survey and proposal keys (0: none)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
+    if args.stars is None:
+        args.stars = 10000 if args.workload == "full" else 512
     if args.precision_report:
         run_precision_report(args)
     elif args.profile_case:
@@ -986,6 +1204,8 @@ def main():
         run_detrend(args)
     elif args.workload == "evidence":
         run_evidence(args)
+    elif args.workload == "full":
+        run_full(args)
     else:
         run_gpu(args)
 

@@ -200,6 +200,8 @@ SIGNATURES = {
                                         c_double_p, C.c_uint32, C.POINTER(Bank), C.c_uint32, C.c_uint32,
                                         c_double_p, c_double_p, c_double_p, c_uint32_p, C.c_char_p,
                                         C.c_uint32]),
+    "fbls_precision_bins": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, C.c_uint32, C.c_uint32,
+                                      C.POINTER(C.c_uint64)]),
     "fbls_timer_start": (C.c_int, [C.c_void_p]),
     "fbls_timer_stop": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "fbls_set_kernel_timing": (C.c_int, [C.c_void_p, C.c_int]),

@@ -549,6 +549,16 @@ class Gpu:
                 dev.free()
 
 
+    def precision_bins(self, dev: DeviceReady, scales, nb: int) -> dict:
+        """Bin forms of the precision study (fbls_precision_bins): mismatches
+        of the f32 and double-single bin products against the fold's f64
+        product, and of the double-single form with its exact fallback."""
+        sc = _f64(scales)
+        out = (C.c_uint64 * 5)()
+        self._check(self.lib.fbls_precision_bins(self.ctx, dev.handle, _dptr(sc), sc.shape[0], int(nb), out))
+        keys = ("pairs", "f32_mismatches", "double_single_mismatches", "fallbacks", "fallback_mismatches")
+        return {k: int(v) for k, v in zip(keys, out)}
+
     def compare_batch(self, candidates: Sequence[Tuple[FamilyState, float]], cfg: SearchConfig,
                       devs: Optional[Sequence[DeviceReady]] = None) -> List[List[dict]]:
         """Evidence rows of many (family, period) candidates in one batch

@@ -30,7 +30,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall"]
 
 CU_SOURCES = ["fold.cu", "scan_kernels.cu", "evidence.cu", "proposal.cu", "rescore.cu", "biweight.cu", "cnn.cu", "host.cu", "host_maps.cu", "host_next.cu",
-              "static_entry.cu"]
+              "static_entry.cu", "precision.cu"]
 CPP_SOURCES = ["prep.cpp"]
 
 

@@ -133,7 +133,7 @@ __device__ __forceinline__ double prefix_row_smem(const HistRow& r, int nb, bool
                                                   float2* __restrict__ out32) {
     const int lane = threadIdx.x & 31;
     if (global && lane == 0) {
-        out64[0] = 0.0;
+        if (out64) out64[0] = 0.0;
         out32[0] = make_float2(0.f, 0.f);
     }
     double carry = 0.0;
@@ -148,7 +148,7 @@ __device__ __forceinline__ double prefix_row_smem(const HistRow& r, int nb, bool
             if (b < nb) {
                 const double val = __dadd_rn(x, offset);
                 if (global) {
-                    out64[b + 1] = val;
+                    if (out64) out64[b + 1] = val;
                     out32[b + 1] = split_pair(val);
                 }
                 r.store(b, val);
@@ -161,7 +161,7 @@ __device__ __forceinline__ double prefix_row_smem(const HistRow& r, int nb, bool
     if (global)
         for (int b = lane; b < nb; b += 32) {  // bins this lane stored above
             const double val = __dadd_rn(r.load(b), carry);
-            out64[nb + b + 1] = val;
+            if (out64) out64[nb + b + 1] = val;
             out32[nb + b + 1] = split_pair(val);
         }
     return carry;
@@ -186,10 +186,12 @@ __device__ __forceinline__ double prefix_segment(const HistRow& r, int nb, int s
         const double wt = __shfl_sync(0xffffffffu, x, 31);
         if (mode == SEG_GLOBAL && b < nb) {
             const double val = __dadd_rn(x, offset);
-            out64[b + 1] = val;
-            out32[b + 1] = split_pair(val);
             const double val2 = __dadd_rn(val, final);
-            out64[nb + b + 1] = val2;
+            if (out64) {
+                out64[b + 1] = val;
+                out64[nb + b + 1] = val2;
+            }
+            out32[b + 1] = split_pair(val);
             out32[nb + b + 1] = split_pair(val2);
         } else if (mode == SEG_IN_PLACE && b < nb) {
             r.store(b, __dadd_rn(x, offset));
@@ -695,7 +697,7 @@ __device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) 
     const int S = (nb + 255) >> 8;
     auto row_of = [&](int row, double*& out64, float2*& out32) {
         const int qq = row / NF, f = row - qq * NF;
-        out64 = a.cum + ((size_t)(g0 + qq) * NF + f) * stride;
+        out64 = a.rows32_only ? nullptr : a.cum + ((size_t)(g0 + qq) * NF + f) * stride;
         out32 = a.cum32 + ((size_t)(g0 + qq) * NF + f) * stride;
         const size_t o = (size_t)qq * rs;
         HistRow r;
@@ -734,7 +736,7 @@ __device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) 
             float2* o32;
             const HistRow r = row_of(row, o64, o32);
             if (!map && sg == 0 && lane == 0) {
-                o64[0] = 0.0;
+                if (o64) o64[0] = 0.0;
                 o32[0] = make_float2(0.f, 0.f);
             }
             prefix_segment(r, nb, sg * 256, seg_carry[it], row_final[row], map ? SEG_IN_PLACE : SEG_GLOBAL, o64,

@@ -105,7 +105,7 @@ struct Pass {
     uint32_t P = 0;
     const fbls_bank* bank = nullptr;
     uint32_t nb = 0;
-    bool mixed = true;
+    int mode = 1;  // ScanArgs::mixed: 1 the reference's mixed ranking, 0 f64, 2 the f32 form
     // plan
     uint64_t batch = 0, launch = 0;
     FoldShape shape{};
@@ -305,6 +305,7 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
             fa.window = p.shape.window;
             fa.row_stride = p.shape.row_stride;
             fa.fault = as<uint32_t>(ctx->fault);
+            fa.rows32_only = p.mode == 2 ? 1 : 0;
             if (timing) CK(cudaEventRecord(ctx->pool[3 * li], s), "event");
             CK(launch_fold(fa, p.shape, s), "fold");
             if (timing) CK(cudaEventRecord(ctx->pool[3 * li + 1], s), "event");
@@ -323,7 +324,7 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
             sa.nd = (int)nd;
             sa.ns = (int)ns;
             sa.layers = (int)layers;
-            sa.mixed = p.mixed ? 1 : 0;
+            sa.mixed = p.mode;
             sa.parts = as<double>(ctx->parts);
             sa.keys = as<uint64_t>(ctx->keys);
             sa.flags = as<uint32_t>(ctx->tflags);
@@ -535,6 +536,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             fa.window = p.shape.window;
             fa.row_stride = p.shape.row_stride;
             fa.fault = as<uint32_t>(ctx->fault);
+            fa.rows32_only = p.mode == 2 ? 1 : 0;
             if (un.walk) {
                 if (!fold_job_ok(fa, p.shape)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
                 fj[nf] = fa;
@@ -556,7 +558,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             sa.nd = (int)nd;
             sa.ns = (int)ns;
             sa.layers = (int)layers;
-            sa.mixed = p.mixed ? 1 : 0;
+            sa.mixed = p.mode;
             sa.parts = as<double>(ctx->parts) + un.parts_off * PART_STRIDE;
             sa.keys = as<uint64_t>(ctx->keys) + un.parts_off;
             sa.flags = as<uint32_t>(ctx->tflags) + un.parts_off;
@@ -632,6 +634,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             fa.window = p.shape.window;
             fa.row_stride = p.shape.row_stride;
             fa.fault = as<uint32_t>(ctx->fault);
+            fa.rows32_only = p.mode == 2 ? 1 : 0;
             CK(launch_fold(fa, p.shape, s), "fold");
         }
         if (timing) CK(cudaEventRecord(ctx->pool[3 * wi + 1], s), "event");
@@ -689,14 +692,14 @@ void add_pass_stats(fbls_scan_stats& st, const Pass& p) {
 
 // One scan_bank pass on its own (fbls_scan_bank).
 int scan_bank(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_t P, const fbls_bank* bank, uint32_t nb,
-              bool mixed, BandOut& out, fbls_scan_stats* stats) {
+              int mode, BandOut& out, fbls_scan_stats* stats) {
     std::vector<Pass> passes(1);
     Pass& p = passes[0];
     p.periods = periods;
     p.P = P;
     p.bank = bank;
     p.nb = nb;
-    p.mixed = mixed;
+    p.mode = mode;
     int rc = plan_pass(ctx, r, p);
     if (rc) return fail(ctx, rc, p.err);
     rc = run_session(ctx, passes, ctx->pin_down);
@@ -727,7 +730,7 @@ struct BandJob {
     int status = FBLS_OK;         // fused sessions: FBLS_ERR_PRECISION when a pass of this band was marked bad
 };
 
-int scan_bands(fbls_ctx* ctx, std::vector<BandJob>& jobs, bool mixed, bool fused) {
+int scan_bands(fbls_ctx* ctx, std::vector<BandJob>& jobs, int mode, bool fused) {
     std::vector<Pass> first, second;
     auto session = [&](std::vector<Pass>& passes, PinBuf& down) {
         return fused ? run_session_fused(ctx, passes, down) : run_session(ctx, passes, down);
@@ -749,7 +752,7 @@ int scan_bands(fbls_ctx* ctx, std::vector<BandJob>& jobs, bool mixed, bool fused
         p.P = j.P;
         p.bank = j.bank;
         p.nb = (uint32_t)(j.coarse ? j.nb / j.bank->prescan_factor : j.nb);
-        p.mixed = mixed;
+        p.mode = mode;
         j.first = (int)first.size();
         first.push_back(std::move(p));
     }
@@ -781,7 +784,7 @@ int scan_bands(fbls_ctx* ctx, std::vector<BandJob>& jobs, bool mixed, bool fused
         p.P = (uint32_t)j.survivors.size();
         p.bank = j.bank;
         p.nb = (uint32_t)j.nb;
-        p.mixed = mixed;
+        p.mode = mode;
         j.second = (int)second.size();
         second.push_back(std::move(p));
     }
@@ -827,14 +830,14 @@ int scan_bands(fbls_ctx* ctx, std::vector<BandJob>& jobs, bool mixed, bool fused
 
 // scan_periods (scan.rs:363-408). Rows are appended to `rows`.
 int scan_periods(fbls_ctx* ctx, const fbls_ready* r, const double* periods, uint32_t P, const fbls_bank* bank,
-                 bool mixed, std::vector<fbls_row>& rows, fbls_scan_stats* stats) {
+                 int mode, std::vector<fbls_row>& rows, fbls_scan_stats* stats) {
     std::vector<BandJob> jobs(1);
     jobs[0].r = r;
     jobs[0].rows = &rows;
     jobs[0].periods = periods;
     jobs[0].P = P;
     jobs[0].bank = bank;
-    int rc = scan_bands(ctx, jobs, mixed, false);
+    int rc = scan_bands(ctx, jobs, mode, false);
     if (stats) *stats = jobs[0].st;
     return rc;
 }
@@ -966,7 +969,8 @@ constexpr uint64_t FUSED_GROUP_PERIODS = 1u << 21;
 int search_batch_fused(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fbls_config* cfg,
                        std::vector<std::string>& errors) {
     const double budget_mib = fold_budget_mib(cfg->max_fold_mib);
-    const bool mixed = cfg->precision_mode == 0;
+    if (cfg->precision_mode > 2) return fail(ctx, FBLS_ERR_ARGUMENT, "precision_mode must be 0, 1 or 2");
+    const int mode = scan_mode(cfg->precision_mode);
     // A star's grid length, from the sizes alone (0 when its inputs are bad):
     // what the groups are cut by.
     auto grid_estimate = [&](const fbls_star& s) -> uint64_t {
@@ -1067,7 +1071,7 @@ int search_batch_fused(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fb
             CK(cudaMemcpyAsync(ctx->family.ptr, host, total, cudaMemcpyHostToDevice, ctx->stream), "upload_ready");
             CK(cudaStreamSynchronize(ctx->stream), "upload_ready");  // the sessions reuse the staging buffer
         }
-        const int rc = scan_bands(ctx, jobs, mixed, true);
+        const int rc = scan_bands(ctx, jobs, mode, true);
         for (size_t j = 0; j < jobs.size(); j++) {
             fbls_star& s = stars[job_star[j]];
             if (s.status) continue;
@@ -1202,6 +1206,7 @@ int fbls_scan_bank(fbls_ctx* ctx, const fbls_ready* ready, const double* periods
                    uint32_t nb, uint32_t precision_mode, double* records, double* score, double* depth,
                    uint32_t* flags, fbls_scan_stats* stats) {
     if (!ctx || !ready || !bank || (P && !periods)) return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (precision_mode > 2) return fail(ctx, FBLS_ERR_ARGUMENT, "precision_mode must be 0, 1 or 2");
     CK(cudaSetDevice(ctx->device), "set device");
     fbls_scan_stats st;
     std::memset(&st, 0, sizeof(st));
@@ -1211,7 +1216,7 @@ int fbls_scan_bank(fbls_ctx* ctx, const fbls_ready* ready, const double* periods
         return FBLS_OK;
     }
     BandOut band;
-    int rc = scan_bank(ctx, ready, periods, P, bank, nb, precision_mode == 0, band, &st);
+    int rc = scan_bank(ctx, ready, periods, P, bank, nb, scan_mode(precision_mode), band, &st);
     if (stats) *stats = st;
     if (rc && rc != FBLS_ERR_PRECISION) return rc;
     if (!band.records) return rc;
@@ -1227,9 +1232,10 @@ int fbls_scan_periods(fbls_ctx* ctx, const fbls_ready* ready, const double* peri
                       fbls_scan_stats* stats) {
     if (!ctx || !ready || !bank || !n_rows || (P && (!periods || !rows_out)))
         return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (precision_mode > 2) return fail(ctx, FBLS_ERR_ARGUMENT, "precision_mode must be 0, 1 or 2");
     CK(cudaSetDevice(ctx->device), "set device");
     std::vector<fbls_row> rows;
-    int rc = scan_periods(ctx, ready, periods, P, bank, precision_mode == 0, rows, stats);
+    int rc = scan_periods(ctx, ready, periods, P, bank, scan_mode(precision_mode), rows, stats);
     if (rc) return rc;
     std::memcpy(rows_out, rows.data(), rows.size() * sizeof(fbls_row));
     *n_rows = (uint32_t)rows.size();
@@ -1290,6 +1296,7 @@ int fbls_signal_search_ranges(fbls_ctx* ctx, const fbls_ready* ready, const doub
                               fbls_scan_stats* stats_out, uint32_t* n_bands) {
     if (!ctx || !ready || !durations || !rho || !cfg || !n_rows || (n_ranges && !ranges))
         return fail(ctx, FBLS_ERR_ARGUMENT, "null argument");
+    if (cfg->precision_mode > 2) return fail(ctx, FBLS_ERR_ARGUMENT, "precision_mode must be 0, 1 or 2");
     CK(cudaSetDevice(ctx->device), "set device");
     StarBands sb;
     std::vector<BandJob> jobs;
@@ -1301,7 +1308,7 @@ int fbls_signal_search_ranges(fbls_ctx* ctx, const fbls_ready* ready, const doub
     if (grid_len) *grid_len = sb.grid_len;
     if (n_bands) *n_bands = 0;
     if (rc) return fail(ctx, rc, err);
-    rc = scan_bands(ctx, jobs, cfg->precision_mode == 0, false);
+    rc = scan_bands(ctx, jobs, scan_mode(cfg->precision_mode), false);
     if (rc) return rc;
     for (size_t i = 0; i < jobs.size() && stats_out && i < 64; i++) stats_out[i] = jobs[i].st;
     const uint32_t n_scanned = (uint32_t)jobs.size();

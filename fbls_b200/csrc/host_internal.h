@@ -73,6 +73,11 @@ struct fbls_ready {
 
 namespace fbls {
 
+// The tile scan's mode for a precision_mode of the C ABI: 0 (the reference's
+// f32 pre-rank, f64 rescans and winner) -> 1, 1 (f64 ranking) -> 0, 2 (the
+// f32 form: f32 ranking and winner, no f64 rows) -> 2.
+inline int scan_mode(uint32_t precision_mode) { return precision_mode == 0 ? 1 : precision_mode == 1 ? 0 : 2; }
+
 inline int fail(fbls_ctx* ctx, int status, const std::string& message) {
     if (ctx) ctx->error = message;
     return status;

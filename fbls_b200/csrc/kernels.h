@@ -47,6 +47,7 @@ struct FoldArgs {
     int window;            // 0: whole histogram in shared memory; else window rows
     int row_stride;        // FoldShape::row_stride
     uint32_t* fault;       // FOLD_WALK: set nonzero when a staging wait gives up
+    int rows32_only;       // FOLD_WALK: write only the (hi, lo) f32 rows (the f32 form reads no f64 rows)
     // Coarse-map epilogue (FOLD_WALK only): when map_out is set, the prefix
     // rows stay in shared memory (cum / cum32 unused) and each period's best
     // box score per map duration, as k_box_map computes it, goes to
@@ -84,7 +85,7 @@ struct ScanArgs {
     double gate;              // shape gate (score units)
     double n;                 // observation count
     int nb, nd, ns, layers;
-    int mixed;                // 1 = f32 pre-rank + f64 rescans, 0 = f64 only
+    int mixed;                // 1 = f32 pre-rank + f64 rescans, 0 = f64 only, 2 = f32 only (no f64 rows read)
     double* parts;            // periods x tiles x 9
     uint64_t* keys;           // periods x tiles
     uint32_t* flags;          // periods x tiles

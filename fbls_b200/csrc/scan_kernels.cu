@@ -188,6 +188,9 @@ __device__ __forceinline__ void scan_tile_cta(const ScanArgs& a, const int tile,
 
     LaneState st;
     st.reset();
+    // mixed: 1 = the reference's f32 pre-rank with f64 rescans and winner,
+    // 0 = f64 ranking, 2 = the f32 form (f32 ranking and winner, no rescan).
+    const bool f32_only = a.mixed == 2;
     bool fast = a.mixed != 0;
     bool retry = false;
     uint64_t winner_key = KEY_MAX;
@@ -296,12 +299,43 @@ __device__ __forceinline__ void scan_tile_cta(const ScanArgs& a, const int tile,
         winner_key = bk;
         winner_value = bv;
         winner_di = s_di;
-        retry = fast && (unsafe_any || near_count > 1 || near_sensitive);
+        retry = fast && !f32_only && (unsafe_any || near_count > 1 || near_sensitive);
         bad_any = bad_any || bad;
         __syncthreads();
     }
 
-    if (lane == 0) {
+    if (lane == 0 && f32_only) {
+        // The f32 form: the winner's statistics from the (hi, lo) pairs in
+        // f32, as the pre-rank reads them; no f64 rows are read.
+        const uint32_t phase = (uint32_t)(winner_key % nb1);
+        const uint32_t width = (uint32_t)((winner_key / nb1) % nb1);
+        const uint32_t si = (uint32_t)(winner_key / (nb1 * nb1));
+        const int sic = min((int)si, ns - 1);
+        const double ing = s_ing[sic];
+        const float rf = (float)s_rho[winner_di];
+        const float w = interval32(rw32, phase, width);
+        const float av = interval32(rv32, phase, width);
+        float a0, hp, norm;
+        shape_sums32(rv32, rw32, phase, width, av, w, w, ing, s_fac, sic, layers, a0, hp, norm);
+        const float aa = __fdiv_rn(a0, rf);
+        const float d = __fdiv_rn(__fmul_rn(hp, hp), basef);
+        const float q = rmaxf(__fsub_rn(norm, d), 1e-30f);
+        const double value = winner_value > neg_inf() ? (double)__fdiv_rn(aa, __fsqrt_rn(q)) : neg_inf();
+        const double depth = (double)__fmul_rn(__fdiv_rn(aa, q), rf);
+        const size_t idx = (size_t)f * tiles + tile;
+        double* out = a.parts + idx * PART_STRIDE;
+        out[0] = (double)phase;
+        out[1] = (double)width;
+        out[2] = (double)aa;
+        out[3] = (double)norm;
+        out[4] = (double)d;
+        out[5] = ing;
+        out[6] = s_rho[winner_di];
+        out[7] = value;
+        out[8] = depth;
+        a.keys[idx] = winner_key;
+        a.flags[idx] = 0u;
+    } else if (lane == 0) {
         // The winner recomputed in f64 (kernels.rs:800-843).
         const uint32_t phase = (uint32_t)(winner_key % nb1);
         const uint32_t width = (uint32_t)((winner_key / nb1) % nb1);

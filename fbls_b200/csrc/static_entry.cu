@@ -65,6 +65,7 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
     if (!time || !v || !w || !bank || (P && (!periods || !records || !score || !depth || !flags)))
         return report(error, error_len, FBLS_ERR_ARGUMENT, "null argument");
     if (device < 0 || device >= MAX_DEVICES) return report(error, error_len, FBLS_ERR_ARGUMENT, "bad device");
+    if (precision_mode > 2) return report(error, error_len, FBLS_ERR_ARGUMENT, "precision_mode must be 0, 1 or 2");
     if (P == 0) return FBLS_OK;
     if (n < 6) return report(error, error_len, FBLS_ERR_DATA, "at least six observations are required");
     const uint32_t nd = bank->nd, ns = bank->ns, layers = bank->layers;
@@ -227,6 +228,7 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
         fa.window = shape.window;
         fa.row_stride = shape.row_stride;
         fa.fault = d_fault;
+        fa.rows32_only = precision_mode == 2 ? 1 : 0;
         if (!ok(launch_fold(fa, shape, s), "fold")) return FBLS_ERR_CUDA;
         ScanArgs sa{};
         sa.cum = d_cum;
@@ -243,7 +245,7 @@ extern "C" int fbls_scan_bank_static(int device, const double* time, const doubl
         sa.nd = (int)nd;
         sa.ns = (int)ns;
         sa.layers = (int)layers;
-        sa.mixed = precision_mode == 0 ? 1 : 0;
+        sa.mixed = precision_mode == 0 ? 1 : precision_mode == 1 ? 0 : 2;
         sa.parts = d_parts;
         sa.keys = d_keys;
         sa.flags = d_tflags;

@@ -15,6 +15,9 @@ distributions of the configurations the path is specified on:
   survey_star    one star of the batched population: geometric(0.4) sectors
                  capped at 13, cadence in {120, 200, 600} s, white noise
                  log-uniform 2e-4-5e-3 plus AR(1) (rho 0.9), a box on 30%.
+  survey_star_full  the survey-scale batch's star: the same population with
+                 a box on 8% and an eclipsing-binary-like pair (primary and
+                 secondary at phase 0.5, unequal depths 1-20%) on 2%.
 
 Flux is returned as relative flux (transits negative) with flux_err, the
 prepared-mode input of the reference (pipeline.rs:41-68).
@@ -125,6 +128,43 @@ def survey_star(rng: np.random.Generator, inject_fraction: float = 0.3) -> Curve
         epoch = t[0] + rng.uniform(0.0, period)
         c.flux = inject_box(t, flux, period, epoch, duration, depth)
         c.period, c.epoch, c.depth, c.duration = period, epoch, depth, duration
+    return c
+
+
+def inject_pair(time: np.ndarray, flux: np.ndarray, period: float, epoch: float, duration: float,
+                primary: float, secondary: float) -> np.ndarray:
+    """An eclipsing-binary-like pair: a primary box at epoch and a secondary
+    box half a period later, of depths `primary` and `secondary`."""
+    out = inject_box(time, flux, period, epoch, duration, primary)
+    return inject_box(time, out, period, epoch + 0.5 * period, duration, secondary)
+
+
+def survey_star_full(rng: np.random.Generator, box_fraction: float = 0.08, pair_fraction: float = 0.02) -> Curve:
+    """One star of the survey-scale batch: the batching population (as
+    survey_star) with a box on `box_fraction` of the stars and an
+    eclipsing-binary-like pair on `pair_fraction`: primary and secondary boxes
+    at phases 0 and 0.5 with unequal depths, each log-uniform in 1-20 %
+    (redrawn until they differ by at least 10 %), period log-uniform 0.5 d to
+    min(20 d, baseline / 2), duration as for the boxes."""
+    c = survey_star(rng, inject_fraction=0.0)
+    u = rng.uniform()
+    baseline = c.time[-1] - c.time[0]
+    pmax = min(20.0, baseline / 2.0)
+    period = math.exp(rng.uniform(math.log(0.5), math.log(pmax)))
+    duration = 13.0 / 24.0 * (period / 365.25) ** (1.0 / 3.0) * rng.uniform(0.5, 2.0)
+    epoch = c.time[0] + rng.uniform(0.0, period)
+    if u < box_fraction:
+        depth = math.exp(rng.uniform(math.log(100e-6), math.log(1e-2)))
+        c.flux = inject_box(c.time, c.flux, period, epoch, duration, depth)
+        c.period, c.epoch, c.depth, c.duration, c.label = period, epoch, depth, duration, c.label + " box"
+    elif u < box_fraction + pair_fraction:
+        while True:
+            d1, d2 = (math.exp(rng.uniform(math.log(0.01), math.log(0.2))) for _ in range(2))
+            if abs(d1 - d2) >= 0.1 * max(d1, d2):
+                break
+        c.flux = inject_pair(c.time, c.flux, period, epoch, duration, d1, d2)
+        c.period, c.epoch, c.depth, c.duration = period, epoch, max(d1, d2), duration
+        c.label += f" pair {d1:.3f}/{d2:.3f}"
     return c
 
 

@@ -123,7 +123,10 @@ typedef struct {
     double planet_radius_scale_rj;
     double target_flux_fraction;
     /* Scan precision: 0 = the reference's mixed mode (f32 pre-rank from
-     * (hi, lo) pairs, f64 winner and rescans); 1 = f64 ranking throughout. */
+     * (hi, lo) pairs, f64 winner and rescans); 1 = f64 ranking throughout;
+     * 2 = the f32 form (f32 ranking from the (hi, lo) pairs, no rescans, the
+     * winner's score, depth and sums in f32: values within ~1e-6 of mode 1,
+     * winners equal except at near ties). */
     uint32_t precision_mode;
 } fbls_config;
 
@@ -242,6 +245,16 @@ int fbls_scan_bank_static(int device, const double* time, const double* v, const
  * recorded on that stream (stop synchronises on its event). */
 int fbls_timer_start(fbls_ctx* ctx);
 int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
+
+/* The precision study's bin forms (no counterpart in the reference): for
+ * every observation of an uploaded family and every scale (nb / period), the
+ * bin floor(t * scale) mod nb of the fold (one rounded f64 product,
+ * kernels.rs:314-327) against a plain f32 product, a double-single product,
+ * and the double-single product with an exact f64 fallback near integers.
+ * counts (5): pairs, f32 mismatches, double-single mismatches, fallbacks
+ * taken, mismatches after the fallback. Needs t * scale below 2^24. */
+int fbls_precision_bins(fbls_ctx* ctx, const fbls_ready* ready, const double* scales, uint32_t P, uint32_t nb,
+                        uint64_t* counts);
 
 typedef struct {
     uint64_t launches;        /* every kernel this context launched */

@@ -4,7 +4,9 @@ kernels.rs (tests/_scan_literal.py, no shared code). On seeded small curves
 built to reach every branch of scan_tiles' f32 pre-ranking (exact near ties,
 an unsafe merit, the sensitivity flag, the tile shape gate open and closed,
 the invalid key nb + 1 + j, the f64 rescan) both give the same records,
-scores, depths and flags bit for bit, and the GPU gives them too.
+scores, depths and flags bit for bit, and the GPU gives them too. A literal
+reading of the evidence screen (tests/_screen_literal.py) picks the oracle's
+screen maximum and pilot template.
 """
 import math
 from collections import Counter
@@ -13,6 +15,7 @@ import numpy as np
 import pytest
 
 import _scan_literal as L
+import _screen_literal as S
 import oracle
 from fbls_b200 import synth
 
@@ -124,3 +127,20 @@ def test_gpu_scan_equals_the_literal_restatement(gpu, name):
     assert np.array_equal(score, lit[1])
     assert np.array_equal(depth, lit[2])
     assert np.array_equal(flags, lit[3])
+
+
+# -- the evidence screen ------------------------------------------------------
+
+@pytest.mark.parametrize("period", [1.3, 0.9, 1.95, 2.6])
+def test_literal_screen_picks_the_oracles_pilot(period):
+    # The screen's maximum (the threshold test) and the pilot key (the
+    # template the floors come from) of a literal reading of evidence.rs
+    # against the oracle's compare_search diagnostics on the small curve.
+    c, cfg = synth.small_curve(), synth.small_config()
+    st = oracle.family_state(c.time, c.flux, c.flux_err, cfg.durations_days())
+    maximum, key, s = S.pilot(st, period, cfg)
+    _, diag = oracle.compare_search(st, period, cfg, diag=True)
+    assert int(diag["nb"]) == s["nb"]
+    assert maximum == diag["screen_max"]
+    if maximum >= cfg.threshold * (1.0 - 1e-12):
+        assert key == diag["pilot_key"]
