@@ -141,6 +141,10 @@ class EvidenceJob(C.Structure):
                 ("n_rows", C.c_uint32), ("status", C.c_int)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("fold_group_max", C.c_uint32 * 32), ("launch_periods", C.c_uint32)]
+
+
 class PrepConfig(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("bin_minutes", "window_min", "window_factor", "window_max", "clip_sigma",
                                            "edge_trim")]
@@ -200,6 +204,8 @@ SIGNATURES = {
                                         c_double_p, C.c_uint32, C.POINTER(Bank), C.c_uint32, C.c_uint32,
                                         c_double_p, c_double_p, c_double_p, c_uint32_p, C.c_char_p,
                                         C.c_uint32]),
+    "fbls_set_tuning": (C.c_int, [C.POINTER(Tuning)]),
+    "fbls_get_tuning": (C.c_int, [C.POINTER(Tuning)]),
     "fbls_precision_bins": (C.c_int, [C.c_void_p, C.c_void_p, c_double_p, C.c_uint32, C.c_uint32,
                                       C.POINTER(C.c_uint64)]),
     "fbls_timer_start": (C.c_int, [C.c_void_p]),

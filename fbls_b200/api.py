@@ -235,13 +235,24 @@ class DeviceReady:
 class Gpu:
     """One device context and stream (Gpu, scan.rs:39-99)."""
 
-    def __init__(self, device: int = 0):
+    _tuning_loaded = False
+
+    def __init__(self, device: int = 0, tuned: bool = True):
         self.lib = N.load()
         status = C.c_int(0)
         self.ctx = self.lib.fbls_create(device, C.byref(status))
         if not self.ctx:
             raise FblsError(status.value, f"cannot create a context on device {device}")
         self.device = device
+        if tuned and not Gpu._tuning_loaded:
+            # The measured launch-shape table (fbls_b200.autotune), when it was
+            # measured on this device model; the rules apply otherwise.
+            Gpu._tuning_loaded = True
+            try:
+                from . import autotune
+                autotune.load_for(autotune.device_name(device))
+            except (ImportError, RuntimeError):
+                pass
 
     def close(self) -> None:
         if self.ctx:

@@ -1,0 +1,142 @@
+"""Autotuner of the fold's launch shape, measured on the GPU.
+
+The fold's period group (periods per 1024-thread CTA, sharing each staged
+observation chunk) trades shared memory for histograms against CTAs per
+launch; the built-in rule takes the largest group whose histograms fit while
+every SM still gets a CTA. This sweep measures, per nb class floor(log2(nb)),
+the fold's device time (CUDA events on the context's stream, the library's
+kernel-timing counters) of one scan_bank pass over 4096 periods of the
+13-sector synthetic star at every allowed group cap, and the periods per
+launch on a whole signal_search, and writes the fastest as a table:
+
+    python -m fbls_b200.autotune --out fbls_b200/data/tuning.json
+
+`Gpu` loads the table (fbls_set_tuning) when the device name matches. The
+results of the search do not depend on it, only the launch shapes do.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import _native as N
+
+TABLE = Path(__file__).resolve().parent / "data" / "tuning.json"
+GROUPS = (1, 2, 4, 8, 16, 32)
+LAUNCHES = (4096, 8192, 16384, 32768)
+
+
+def device_name(device: int = 0) -> str:
+    import torch
+    return torch.cuda.get_device_name(device)
+
+
+def apply(table: dict) -> None:
+    """Sets the process-wide tuning from a table (fbls_set_tuning)."""
+    t = N.Tuning()
+    for cls, g in table.get("fold_group_max", {}).items():
+        t.fold_group_max[int(cls)] = int(g)
+    t.launch_periods = int(table.get("launch_periods", 0))
+    rc = N.load().fbls_set_tuning(C.byref(t))
+    if rc:
+        raise ValueError(f"tuning table rejected (status {rc})")
+
+
+def current() -> dict:
+    t = N.Tuning()
+    N.load().fbls_get_tuning(C.byref(t))
+    return {"fold_group_max": {str(c): int(g) for c, g in enumerate(t.fold_group_max) if g},
+            "launch_periods": int(t.launch_periods)}
+
+
+def reset() -> None:
+    apply({})
+
+
+def load_for(device_name_: str, path: Path = TABLE) -> bool:
+    """Applies the committed table when it was measured on this device model."""
+    if not path.exists():
+        return False
+    table = json.loads(path.read_text())
+    if table.get("device") != device_name_:
+        return False
+    apply(table)
+    return True
+
+
+def _fold_ms(gpu, dev, periods, bank, nb, reps: int) -> float:
+    gpu.scan_bank(dev, periods, bank, nb)  # warm
+    gpu.counters(reset=True)
+    for _ in range(reps):
+        gpu.scan_bank(dev, periods, bank, nb)
+    return gpu.counters(reset=True)["fold_ms"] / reps
+
+
+def sweep(reps: int = 3, log=print) -> dict:
+    from . import api, synth
+    c, cfg = synth.multi_sector(), synth.multi_sector_config()
+    st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
+    grid, bands = api.band_plan(st, cfg)
+    out = {"device": device_name(0),
+           "workload": "13-sector synthetic star (247,104 observations), 4096 periods of each octave band at its "
+                       "coarse and full nb; fold device time per pass (ms) by period-group cap, 0 = the rule",
+           "fold_ms": {}, "fold_group_max": {}, "command": "python -m fbls_b200.autotune"}
+    with api.Gpu(0, tuned=False) as gpu:
+        dev = gpu.upload(st)
+        gpu.set_kernel_timing(True)
+        cases = {}
+        for band in bands:
+            for nb in (band["nb"] // 2, band["nb"]):
+                cases.setdefault(int(np.floor(np.log2(nb))), (nb, band))
+        for cls, (nb, band) in sorted(cases.items()):
+            bank = api.bank_for(band, cfg)
+            periods = band["periods"][:4096]
+            reset()
+            times = {0: _fold_ms(gpu, dev, periods, bank, nb, reps)}  # the built-in rule
+            for g in GROUPS:
+                apply({"fold_group_max": {str(cls): g}})
+                times[g] = _fold_ms(gpu, dev, periods, bank, nb, reps)
+            reset()
+            best = min(times, key=times.get)
+            out["fold_ms"][str(cls)] = {"nb": int(nb), **{str(k): round(v, 4) for k, v in times.items()}}
+            if best != 0 and times[best] < 0.98 * times[0]:
+                out["fold_group_max"][str(cls)] = int(best)
+            log(f"nb {nb} (class {cls}): " + ", ".join(f"G<={k or 'rule'}: {v:.3f} ms" for k, v in times.items())
+                + f" -> {best or 'rule'}")
+        launches = {}
+        for lp in LAUNCHES:
+            apply({"fold_group_max": out["fold_group_max"], "launch_periods": lp})
+            gpu.signal_search(st, cfg, dev=dev)
+            ms = []
+            for _ in range(reps):
+                gpu.timer_start()
+                gpu.signal_search(st, cfg, dev=dev)
+                ms.append(gpu.timer_stop())
+            launches[lp] = sum(ms) / len(ms)
+            log(f"launch {lp}: {launches[lp]:.2f} ms per signal_search")
+        best = min(launches, key=launches.get)
+        out["signal_search_ms"] = {str(k): round(v, 3) for k, v in launches.items()}
+        out["launch_periods"] = int(best) if launches[best] < 0.99 * launches[16384] else 0
+        dev.free()
+    reset()
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--out", default=str(TABLE))
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args(argv)
+    t0 = time.time()
+    table = sweep(args.reps, log=lambda m: print(f"[{time.time() - t0:6.1f} s] {m}", flush=True))
+    Path(args.out).write_text(json.dumps(table, indent=1) + "\n")
+    print(json.dumps({"fold_group_max": table["fold_group_max"], "launch_periods": table["launch_periods"]}))
+
+
+if __name__ == "__main__":
+    main()

@@ -26,6 +26,8 @@
 // prefix_block (kernels.rs:237-309), one warp per (period, field) row, and
 // are written as f64 and (hi, lo) f32 pairs.
 
+#include <atomic>
+
 #include "bulk.cuh"
 #include "common.cuh"
 #include "kernels.h"
@@ -790,6 +792,16 @@ constexpr int WALK_CAP = 2048;
 
 // Walking-fold shape: 1024 threads, chunks of up to WALK_CAP observations,
 // the largest power-of-two group whose histograms fit beside the staging.
+// Tuning (process-wide, set by fbls_set_tuning from a measured table): the
+// largest period group per nb class floor(log2(nb)), 0 = the built-in rule.
+std::atomic<uint32_t> g_group_cap[32];
+std::atomic<uint32_t> g_launch_periods{16384};
+
+uint32_t group_cap(int nb) {
+    const int cls = nb > 0 ? 31 - __builtin_clz((unsigned)nb) : 0;
+    return g_group_cap[cls].load(std::memory_order_relaxed);
+}
+
 bool walk_shape(int nb, int periods, int sm_count, FoldShape* out) {
     FoldShape s{};
     s.kind = FOLD_WALK;
@@ -802,6 +814,8 @@ bool walk_shape(int nb, int periods, int sm_count, FoldShape* out) {
     int g = 1;
     while (2 * g <= MAX_GROUP && stage + starts(2 * g) + (size_t)(2 * g) * hist_per <= MAX_FOLD_SMEM) g *= 2;
     while (g > 1 && (g / 2 >= periods || (periods + g - 1) / g < sm_count)) g /= 2;
+    const uint32_t gcap = group_cap(nb);
+    while (gcap && g > 1 && (uint32_t)g > gcap) g /= 2;
     s.group = g;
     s.hist_in_smem = true;
     s.window = 0;
@@ -833,6 +847,8 @@ FoldShape fold_group_shape(int nb, int periods, int sm_count) {
     while (g < MAX_GROUP && (size_t)(2 * g) * hist_per + stage_min <= MAX_FOLD_SMEM) g *= 2;
     const int fill = (periods + sm_count - 1) / sm_count;
     while (g > 1 && g / 2 >= fill) g /= 2;
+    const uint32_t gcap = group_cap(nb);
+    while (gcap && g > 1 && (uint32_t)g > gcap) g /= 2;
     s.group = g;
     s.hist_in_smem = (size_t)g * hist_per + stage_min <= MAX_FOLD_SMEM;
     const size_t room = MAX_FOLD_SMEM - (s.hist_in_smem ? (size_t)g * hist_per : 0) - 4 * (1024 + 32);
@@ -849,6 +865,18 @@ FoldShape fold_group_shape(int nb, int periods, int sm_count) {
     s.smem = SLOT_BYTES * (size_t)s.stage_field + starts_bytes + (s.hist_in_smem ? (size_t)g * hist_per : 0);
     return s;
 }
+
+void set_fold_tuning(const uint32_t* group_caps, uint32_t launch_periods) {
+    for (int c = 0; c < 32; c++) g_group_cap[c].store(group_caps ? group_caps[c] : 0u, std::memory_order_relaxed);
+    g_launch_periods.store(launch_periods ? launch_periods : 16384u, std::memory_order_relaxed);
+}
+
+void get_fold_tuning(uint32_t* group_caps, uint32_t* launch_periods) {
+    for (int c = 0; c < 32; c++) group_caps[c] = g_group_cap[c].load(std::memory_order_relaxed);
+    *launch_periods = g_launch_periods.load(std::memory_order_relaxed);
+}
+
+uint32_t tuned_launch_periods() { return g_launch_periods.load(std::memory_order_relaxed); }
 
 int fold_chunks(const double* time, int n, double scale_max, int nb, int span_cap, int chunk_cap, int* out,
                 int capacity) {

@@ -172,7 +172,8 @@ int plan_pass(const fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
         return p.fail(FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
     // Periods per launch: whole batches of the reference's size, as many as
     // the fold budget holds in this path's buffers (cum, cum32 and tile parts;
-    // the histograms never reach device memory), up to 16,384, so bands with
+    // the histograms never reach device memory), up to 16,384 (or the tuned
+    // cap), so bands with
     // few bins fill the GPU with larger period groups. Statistics still count
     // the reference's batches.
     const size_t stride = 2 * (size_t)nb + 1;
@@ -180,7 +181,7 @@ int plan_pass(const fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
         (double)(NF * stride * (sizeof(double) + sizeof(float2)) +
                  tiles * (PART_STRIDE * sizeof(double) + sizeof(uint64_t) + sizeof(uint32_t)));
     uint64_t launch = (uint64_t)std::floor(bank->max_fold_mib * 1048576.0 / launch_period_bytes);
-    launch = std::min<uint64_t>(launch, 16384);
+    launch = std::min<uint64_t>(launch, tuned_launch_periods());
     launch = std::max<uint64_t>(launch / batch, 1) * batch;
     if (launch > p.P) launch = p.P;
     p.batch = batch;

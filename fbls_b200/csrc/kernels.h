@@ -193,6 +193,12 @@ struct BiweightArgs {
 };
 
 FoldShape fold_group_shape(int nb, int periods, int sm_count);
+// Measured tuning of the fold's launch shape (process-wide): per nb class
+// floor(log2(nb)) the largest period group (0 = the built-in rule), and the
+// periods per launch (0 = 16,384).
+void set_fold_tuning(const uint32_t* group_caps, uint32_t launch_periods);
+void get_fold_tuning(uint32_t* group_caps, uint32_t* launch_periods);
+uint32_t tuned_launch_periods();
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
 // spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.
 // Writes count + 1 offsets; returns count, or -1 when capacity is too small.

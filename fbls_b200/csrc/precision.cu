@@ -1,4 +1,5 @@
-// Bin-index forms of the precision study on sm_100a: the fold's bin
+// Bin-index forms of the precision study on sm_100a (and, at the end, the C
+// entry points of the launch-shape tuning table): the fold's bin
 // floor(t * scale) mod nb (src/search/kernels.rs:314-327, one rounded f64
 // product) against two cheaper forms, on the device, for every observation
 // of an uploaded family at a sample of scales:
@@ -19,10 +20,6 @@
 namespace fbls {
 
 namespace {
-
-struct BinCounts {
-    unsigned long long pairs, f32_miss, ds_miss, fallbacks, ds_fallback_miss;
-};
 
 __device__ __forceinline__ uint32_t bin_f64(double t, double scale, uint32_t nb) {
     return (uint32_t)((uint64_t)floor(__dmul_rn(t, scale)) % nb);
@@ -111,5 +108,21 @@ extern "C" int fbls_precision_bins(fbls_ctx* ctx, const fbls_ready* ready, const
     CK(cudaMemcpyAsync(host, d_counts, sizeof(host), cudaMemcpyDeviceToHost, s), "download counts");
     CK(cudaStreamSynchronize(s), "bin forms");
     for (int k = 0; k < 5; k++) counts[k] = host[k];
+    return FBLS_OK;
+}
+
+extern "C" int fbls_set_tuning(const fbls_tuning* tuning) {
+    if (!tuning) return FBLS_ERR_ARGUMENT;
+    for (int c = 0; c < 32; c++) {
+        const uint32_t g = tuning->fold_group_max[c];
+        if (g > (uint32_t)MAX_GROUP || (g & (g - 1)) != 0) return FBLS_ERR_ARGUMENT;
+    }
+    set_fold_tuning(tuning->fold_group_max, tuning->launch_periods);
+    return FBLS_OK;
+}
+
+extern "C" int fbls_get_tuning(fbls_tuning* tuning) {
+    if (!tuning) return FBLS_ERR_ARGUMENT;
+    get_fold_tuning(tuning->fold_group_max, &tuning->launch_periods);
     return FBLS_OK;
 }

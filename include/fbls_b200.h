@@ -246,6 +246,19 @@ int fbls_scan_bank_static(int device, const double* time, const double* v, const
 int fbls_timer_start(fbls_ctx* ctx);
 int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
 
+/* Measured launch-shape tuning (no counterpart in the reference; written by
+ * the autotuner, python -m fbls_b200.autotune, and read back from its table):
+ * per nb class floor(log2(nb)) the largest fold period group (a power of two;
+ * 0 = the built-in rule: the largest group whose histograms fit shared memory
+ * while every SM gets a CTA), and the periods per launch (0 = 16,384).
+ * Process-wide; results do not depend on it, only the launch shapes do. */
+typedef struct {
+    uint32_t fold_group_max[32];
+    uint32_t launch_periods;
+} fbls_tuning;
+int fbls_set_tuning(const fbls_tuning* tuning);
+int fbls_get_tuning(fbls_tuning* tuning);
+
 /* The precision study's bin forms (no counterpart in the reference): for
  * every observation of an uploaded family and every scale (nb / period), the
  * bin floor(t * scale) mod nb of the fold (one rounded f64 product,

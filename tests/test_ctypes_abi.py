@@ -22,7 +22,7 @@ for _ct, _names in ((C.c_double, {"double"}), (C.c_float, {"float"}), (C.c_int, 
 _STRUCTS = {N.Bank: "fbls_bank", N.Row: "fbls_row", N.ScanStats: "fbls_scan_stats", N.Config: "fbls_config",
             N.EvidenceRow: "fbls_evidence_row", N.Counters: "fbls_counters", N.Star: "fbls_star",
             N.MapJob: "fbls_map_job", N.PrepConfig: "fbls_prep_config", N.FamilyOut: "fbls_family_out",
-            N.EventStats: "fbls_event_stats", N.EvidenceJob: "fbls_evidence_job"}
+            N.EventStats: "fbls_event_stats", N.EvidenceJob: "fbls_evidence_job", N.Tuning: "fbls_tuning"}
 
 
 def _base(c_type: str) -> str:

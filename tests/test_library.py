@@ -174,3 +174,17 @@ def test_oracle_search_does_not_depend_on_its_thread_count():
     one = oracle.signal_search(st, cfg, threads=1)
     many = oracle.signal_search(st, cfg, threads=8)
     assert np.array_equal(one[0], many[0]) and np.array_equal(one[1], many[1])
+
+
+def test_tuning_table_round_trip_and_limits():
+    from fbls_b200 import autotune
+    try:
+        autotune.apply({"fold_group_max": {"10": 4, "11": 2}, "launch_periods": 8192})
+        assert autotune.current() == {"fold_group_max": {"10": 4, "11": 2}, "launch_periods": 8192}
+        with pytest.raises(ValueError):
+            autotune.apply({"fold_group_max": {"10": 3}})  # not a power of two
+        with pytest.raises(ValueError):
+            autotune.apply({"fold_group_max": {"10": 64}})  # above the largest group
+    finally:
+        autotune.reset()
+    assert autotune.current() == {"fold_group_max": {}, "launch_periods": 16384}
