@@ -89,7 +89,7 @@ struct EvCand {
     const double* hist;  // 3 x nb2, the two-period fold
     double* cum;         // 3 rows of rs = nb2 + 2 doubles: exclusive prefix (v, w, count) over 2 nb bins
     double* screen;      // tiles x EV_SCREEN
-    double* rec;         // tiles x EV_REC
+    double* rec;         // tiles x parts x EV_REC
     double* pilot;       // EV_PILOT
     const EvDur* dur;    // nd
     const EvLayer* lay;  // nd x ns x L: the template at width k
@@ -100,7 +100,10 @@ struct EvCand {
     double n;            // observations
     double threshold;
     double margin;       // log(rtol) - log((NORB + 1) nb nd ns)
-    int nb, nd, ns, L, tiles, stage, cta0, pad;
+    int nb, nd, ns, L, tiles, stage;
+    int cta0;            // first CTA of the candidate in its screen launch
+    int cta0j;           // first CTA of the candidate in its joint launch
+    int parts;           // the joint pass splits the durations into this many parts, one CTA each
 };
 
 // Batch-wide constants of the evidence model (evidence.rs:665-689 and the
@@ -388,12 +391,13 @@ __device__ __forceinline__ bool usable_at(const EvCand& C, const double* cum, in
     return jv && D.raw_ok && count >= 3.0 && count <= C.n - 3.0;
 }
 
-// First CTA of a candidate: the last candidate whose cta0 is <= blockIdx.x.
-__device__ __forceinline__ int candidate_of(const EvCand* __restrict__ cands, int ncand, int cta) {
+// The candidate of a CTA: the last candidate whose first CTA (cta0 in the
+// screen launch, cta0j in the joint launch) is at or before it.
+__device__ __forceinline__ int candidate_of(const EvCand* __restrict__ cands, int ncand, int cta, bool joint) {
     int lo = 0, hi = ncand - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) / 2;
-        if (cands[mid].cta0 <= cta)
+        if ((joint ? cands[mid].cta0j : cands[mid].cta0) <= cta)
             lo = mid;
         else
             hi = mid - 1;
@@ -479,7 +483,7 @@ __global__ void __launch_bounds__(EV_THREADS, 1) k_ev_screen(const EvCand* __res
     extern __shared__ __align__(128) double ev_rows[];
     __shared__ double slot[2][EV_CTA_TILES][2][4];
     __shared__ __align__(8) uint64_t bar;
-    const EvCand& C = cands[candidate_of(cands, ncand, blockIdx.x)];
+    const EvCand& C = cands[candidate_of(cands, ncand, blockIdx.x, false)];
     bool ok;
     const double* cum = stage_rows(C, ev_rows, &bar, fault, ok);
     if (!ok) return;
@@ -623,15 +627,19 @@ __global__ void __launch_bounds__(EV_THREADS, 1) k_ev_joint(const EvCand* __rest
     __shared__ double slot[2][EV_CTA_TILES][2][4];
     __shared__ uint8_t decisions[EV_CTA_TILES][MAX_DURATIONS * MAX_SHAPES];
     __shared__ __align__(8) uint64_t bar;
-    const EvCand& C = cands[candidate_of(cands, ncand, blockIdx.x)];
+    const EvCand& C = cands[candidate_of(cands, ncand, blockIdx.x, true)];
     if (C.pilot[3] == 0.0) return;  // inactive candidate (uniform over the CTA)
     const double floor_p = C.pilot[0], floor_b = C.pilot[1];
     bool ok;
     const double* cum = stage_rows(C, ev_rows, &bar, fault, ok);
     if (!ok) return;
     const int tl = threadIdx.x >> 6, lane = threadIdx.x & 63;
-    const int tile = ((int)blockIdx.x - C.cta0) * EV_CTA_TILES + tl;
+    // CTA (tile group, part): the part's durations of the group's tiles.
+    const int local = (int)blockIdx.x - C.cta0j;
+    const int part = local % C.parts;
+    const int tile = (local / C.parts) * EV_CTA_TILES + tl;
     if (tile >= C.tiles) return;
+    const int di0 = part * C.nd / C.parts, di1 = (part + 1) * C.nd / C.parts;
     TileRed red{slot, tl, (int)((threadIdx.x >> 5) & 1), 1 + tl, 0};
     const int nb = C.nb, rs = 2 * nb + 2;
     const int j = tile * EV_TILE + lane;
@@ -641,7 +649,7 @@ __global__ void __launch_bounds__(EV_THREADS, 1) k_ev_joint(const EvCand* __rest
     Lane S;
     lane_init(S);
     const TileDecide decide{&red, decisions[tl], lane};
-    for (int di = 0; di < C.nd; di++) {
+    for (int di = di0; di < di1; di++) {
         if (!C.dur[di].raw_ok) continue;  // uniform: no template of this duration enters the sums
         const bool usable = usable_at(C, cum, rs, jj, jv, di);
         for (int si = 0; si < C.ns; si++) {
@@ -650,7 +658,10 @@ __global__ void __launch_bounds__(EV_THREADS, 1) k_ev_joint(const EvCand* __rest
         }
     }
 
-    double* rec = C.rec + (size_t)tile * EV_REC;
+    // One record per (tile, part): the winners and log sums of the part's
+    // templates. The host takes the best record by (value, lowest key) and
+    // log-sum-exps all records, which is the whole tile's result.
+    double* rec = C.rec + ((size_t)tile * C.parts + part) * EV_REC;
     for (int sel = 0; sel < 2; sel++) {
         const double m = sel ? S.best_signal : S.best_joint;
         const unsigned long long key = sel ? S.signal_key : S.joint_key;
@@ -725,7 +736,7 @@ double host_logsumexp(const std::vector<double>& v) {
 // Everything the device needs about one candidate, in host memory.
 struct Plan {
     bool run = false;  // false: no rows (no duration below period / 4) or rejected (status set)
-    int nb = 0, nd = 0, ns = 0, L = 0, tiles = 0, cls = 0;
+    int nb = 0, nd = 0, ns = 0, L = 0, tiles = 0, cls = 0, parts = 1;
     double scale = 0.0, margin = 0.0, log_mass = 0.0;
     std::vector<double> durations, priors;
     std::vector<EvDur> dur;
@@ -974,6 +985,14 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
             if (plans[i].run && plans[i].cls == cls) order.push_back(i);
     if (order.empty()) return 0;
     const size_t R = order.size();
+    // Parts of the joint pass: enough (tile group, part) CTAs for about two
+    // per SM, at most 8 parts and one duration per part.
+    {
+        size_t groups = 0;
+        for (size_t i : order) groups += (size_t)(plans[i].tiles + EV_CTA_TILES - 1) / EV_CTA_TILES;
+        const int target = (int)std::min<size_t>(8, (2 * (size_t)std::max(sm_count, 1) + groups - 1) / groups);
+        for (size_t i : order) plans[i].parts = std::max(1, std::min(target, plans[i].nd));
+    }
 
     // Workspace layout: [EvCand x R | fold jobs | cta0 | per-candidate tables,
     // scale, chunks] uploaded; then hist, fold scratch, cum, screen, rec,
@@ -1010,7 +1029,7 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
     const size_t o_first = at;
     for (size_t r = 0; r < R; r++) {
         Plan& P = plans[order[r]];
-        P.o_rec = take((size_t)P.tiles * EV_REC * sizeof(double));
+        P.o_rec = take((size_t)P.tiles * P.parts * EV_REC * sizeof(double));
         P.o_pilot = take(EV_PILOT * sizeof(double));
     }
     const size_t o_fault = take(sizeof(uint32_t));
@@ -1032,16 +1051,19 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
     // CTA numbering of the screen and joint launches restarts in each class.
     int cls_first[5] = {0, 0, 0, 0, 0};
     {
-        int cls_prev = -1, cta = 0;
+        int cls_prev = -1, cta = 0, ctaj = 0;
         for (size_t r = 0; r < R; r++) {
             const Plan& P = plans[order[r]];
             if (P.cls != cls_prev) {
                 for (int k = cls_prev + 1; k <= P.cls; k++) cls_first[k] = (int)r;
                 cls_prev = P.cls;
-                cta = 0;
+                cta = ctaj = 0;
             }
             hc[r].cta0 = cta;
+            hc[r].cta0j = ctaj;
+            hc[r].parts = P.parts;
             cta += (P.tiles + EV_CTA_TILES - 1) / EV_CTA_TILES;
+            ctaj += (P.tiles + EV_CTA_TILES - 1) / EV_CTA_TILES * P.parts;
         }
         for (int k = cls_prev + 1; k <= 4; k++) cls_first[k] = (int)R;
     }
@@ -1155,7 +1177,7 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
             size_t smem = 0;
             for (int r = r0; r < r1; r++) {
                 const Plan& P = plans[order[r]];
-                ctas += (P.tiles + EV_CTA_TILES - 1) / EV_CTA_TILES;
+                ctas += (P.tiles + EV_CTA_TILES - 1) / EV_CTA_TILES * (joint ? P.parts : 1);
                 if (cls < 3) smem = std::max(smem, 3 * (2 * (size_t)P.nb + 2) * sizeof(double));
             }
             const auto kernel = joint ? k_ev_joint : k_ev_screen;
@@ -1193,7 +1215,7 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
         const double* pil = reinterpret_cast<const double*>(host.data() + (P.o_pilot - o_first));
         if (pil[3] == 0.0) continue;  // below the threshold: no rows
         const double* rec = reinterpret_cast<const double*>(host.data() + (P.o_rec - o_first));
-        const int tiles = P.tiles;
+        const int tiles = P.tiles * P.parts;  // records: (tile, part)
         const uint64_t nb = (uint64_t)P.nb;
         fbls_evidence_row rows[2];
         std::vector<double> sp(tiles), sb(tiles);

@@ -126,7 +126,9 @@ def test_gpu_scan_equals_the_literal_restatement(gpu, name):
     assert np.array_equal(rec, lit[0])
     assert np.array_equal(score, lit[1])
     assert np.array_equal(depth, lit[2])
-    assert np.array_equal(flags, lit[3])
+    # The device's flag word adds bit 2 (this tile ran its f64 rescan), which
+    # the library counts as tile_rescans; bits 0 and 1 are the reference's.
+    assert np.array_equal(flags & 3, lit[3])
 
 
 # -- the evidence screen ------------------------------------------------------
