@@ -427,7 +427,8 @@ def _metric_second_half(gpu, count: int) -> dict:
 
     full, t_ex, ts_ex = timed(lambda: gpu.search_batch(states, cfg, period_max=pmax, devs=devs, workers=0))
     _, t_e2e, _ = timed(lambda: gpu.search_batch(states, cfg, period_max=pmax, workers=0), steps=1)
-    (pruned, _), t_pr, ts_pr = timed(lambda: pr.search_proposed(gpu, net, pstars, devs, cfg, k=1, workers=0))
+    (pruned, _), t_pr, ts_pr = timed(lambda: pr.search_proposed(gpu, net, pstars, devs, cfg, k=pr.TOP_BANDS,
+                                                                workers=0))
     hits = labelled = 0
     for (fr, _, _), (pr_rows, _, _) in zip(full, pruned):
         if fr.shape[0] == 0:
@@ -447,7 +448,7 @@ def _metric_second_half(gpu, count: int) -> dict:
                    "timing": "host clock around the device-synchronised fbls_search_batch (stars fused)"},
         "proposal": {"stars": count, "exhaustive_stars_per_s": count / t_ex, "proposal_stars_per_s": count / t_pr,
                      "speedup": t_ex / t_pr, "top1_recall": hits / max(labelled, 1),
-                     "stars_with_detection": labelled, "bands_searched": 1, "bands": pr.BANDS,
+                     "stars_with_detection": labelled, "bands_searched": pr.TOP_BANDS, "bands": pr.BANDS,
                      "step_ms": [round(1e3 * t, 1) for t in ts_pr],
                      "timing": "host clock around coarse maps + network + pruned fbls_search_batch"},
     }
@@ -678,7 +679,7 @@ def run_full(args):
 
     def full_form():
         t0 = time.perf_counter()
-        pruned, _ = pr.search_proposed(gpu, net, pstars, devs, cfg, k=1, workers=0)
+        pruned, _ = pr.search_proposed(gpu, net, pstars, devs, cfg, k=pr.TOP_BANDS, workers=0)
         t1 = time.perf_counter()
         idx, cands, cdevs = [], [], []
         for i, (rows, _, _) in enumerate(pruned):
@@ -694,7 +695,7 @@ def run_full(args):
 
     # warm-up on a slice, then the timed full form
     sub = slice(0, min(256, len(states)))
-    pr.search_proposed(gpu, net, pstars[sub], devs[sub], cfg, k=1, workers=0)
+    pr.search_proposed(gpu, net, pstars[sub], devs[sub], cfg, k=pr.TOP_BANDS, workers=0)
     gpu.compare_batch([(states[0], 1.0)], cfg, devs=[devs[0]])
     gpu.set_kernel_timing(True)
     gpu.counters(reset=True)
@@ -738,7 +739,7 @@ def run_full(args):
         "dtype": "f64 search and evidence, bf16 network", "data": "synthetic",
         "config": {"workload": f"full: {len(states)} seeded survey stars (1-13 sectors ~ Geometric(0.4), cadence "
                                "120/200/600 s, white + AR(1) noise; 8 % boxes, 2 % eclipsing-binary-like pairs "
-                               "with unequal depths 1-20 %); proposal (1 of 32 bands) -> pruned search -> "
+                               "with unequal depths 1-20 %); proposal (32 of 1024 bands) -> pruned search -> "
                                "evidence of each star's best candidate",
                    "stars": len(states), "observations": n_obs,
                    "boxes": sum("box" in x[2] for x in stars), "pairs": sum("pair" in x[2] for x in stars)},
@@ -1181,7 +1182,8 @@ def main():
     ap.add_argument("--batch-workers", type=int, default=0,
                     help="survey / proposal workloads: search_batch host worker threads (0: stars fused into "
                          "job launches)")
-    ap.add_argument("--bands", type=int, default=1, help="proposal workload: log-period bands searched per star")
+    ap.add_argument("--bands", type=int, default=32,
+                    help="proposal workload: log-period bands (of 1024) searched per star")
     ap.add_argument("--period-oversample", type=float, default=None,
                     help="single-star workloads: period grid density (default 3; 19 gives multi_sector's ~1.2M "
                          "periods, 6.9 single_sector's ~30k)")

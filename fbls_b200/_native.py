@@ -254,10 +254,14 @@ SIGNATURES = {
     "fbls_nn_col2im": (C.c_int, [C.c_void_p, C.c_void_p] + [C.c_int] * 5 + [C.c_void_p]),
     "fbls_nn_bias_relu_pool": (C.c_int, [C.c_void_p] * 4 + [C.c_int] * 4 + [C.c_void_p]),
     "fbls_nn_bias_relu_pool_bwd": (C.c_int, [C.c_void_p] * 5 + [C.c_int] * 4 + [C.c_void_p]),
+    "fbls_nn_bias_gelu_pool": (C.c_int, [C.c_void_p] * 4 + [C.c_int] * 4 + [C.c_void_p]),
+    "fbls_nn_bias_gelu_pool_bwd": (C.c_int, [C.c_void_p] * 6 + [C.c_int] * 4 + [C.c_void_p]),
     "fbls_nn_head": (C.c_int, [C.c_void_p] * 7 + [C.c_int] * 4 + [C.c_void_p]),
     "fbls_nn_head_bwd": (C.c_int, [C.c_void_p] * 6 + [C.c_int] * 4 + [C.c_void_p]),
     "fbls_nn_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_float,
                                C.c_float, C.c_float, C.c_int, C.c_void_p]),
+    "fbls_nn_adamw": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_float,
+                                C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p]),
 }
 
 _lib = None

@@ -12,6 +12,7 @@
 // with mma.sync m16n8k16 (bf16 inputs, f32 accumulation) and written as f32.
 // The network is a few MFLOP per curve, so these tiles are sized for
 // simplicity, not for peak throughput.
+#include <atomic>
 #include <cstdint>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -197,6 +198,58 @@ __global__ void k_bias_relu_pool_bwd(const float* dZ, const float* Z, const uint
     }
 }
 
+// GELU, x Phi(x) with the normal CDF Phi from CUDA's erff, and its
+// derivative Phi(x) + x phi(x).
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float x) {
+    return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+// Z[c][b][u] = max over t in [u*P, u*P + P) of gelu(Y[c][b][t] + bias[c]);
+// idx keeps the window offset of the maximum (first one). P = 1 is GELU alone.
+__global__ void k_bias_gelu_pool(const float* Y, const float* bias, float* Z, uint8_t* idx, int B, int C, int T,
+                                 int P) {
+    const int U = T / P;
+    const long long total = (long long)B * C * U;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int u = (int)(e % U);
+        const long long bc = e / U;  // c * B + b
+        const int c = (int)(bc / B);
+        const float* y = Y + bc * T + (long long)u * P;
+        float best = gelu(y[0] + bias[c]);
+        int at = 0;
+        for (int i = 1; i < P; i++) {
+            const float v = gelu(y[i] + bias[c]);
+            if (v > best) {
+                best = v;
+                at = i;
+            }
+        }
+        Z[e] = best;
+        idx[e] = (uint8_t)at;
+    }
+}
+
+// dY[c][b][t] = dZ gelu'(Y + bias) at the window's maximum, else 0; dbias[c]
+// += sum of dY (one atomic per thread and element with a nonzero gradient).
+__global__ void k_bias_gelu_pool_bwd(const float* dZ, const float* Y, const uint8_t* idx, const float* bias, float* dY,
+                                     float* dbias, int B, int C, int T, int P) {
+    const int U = T / P;
+    const long long total = (long long)B * C * U;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int u = (int)(e % U);
+        const long long bc = e / U;  // c * B + b
+        const int c = (int)(bc / B);
+        const long long base = bc * T + (long long)u * P;
+        const int at = idx[e];
+        const float g = dZ[e] * gelu_grad(Y[base + at] + bias[c]);
+        for (int i = 0; i < P; i++) dY[base + i] = (i == at) ? g : 0.f;
+        if (g != 0.f) atomicAdd(&dbias[c], g);
+    }
+}
+
 // Head: h[b][t] = sum_c wh[c] Z[c][b][t] + bh; logits[b][j] = mean of h over
 // t in [j*G, j*G + G); softmax cross-entropy with label[b] (or no loss when
 // labels is null): loss[b], dlogits[b][j] = (softmax - onehot) / B.
@@ -260,9 +313,37 @@ __global__ void k_adam(float* w, const float* g, float* m, float* v, long long n
     }
 }
 
+// AdamW (Loshchilov & Hutter 2019): Adam with bias correction and the weight
+// decay decoupled from the gradient, w -= lr (m_hat / (sqrt(v_hat) + eps) +
+// wd w); step t >= 1.
+__global__ void k_adamw(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
+                        float eps, float wd, int t) {
+    const float c1 = 1.f - powf(b1, (float)t), c2 = 1.f - powf(b2, (float)t);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        m[i] = b1 * m[i] + (1.f - b1) * g[i];
+        v[i] = b2 * v[i] + (1.f - b2) * g[i] * g[i];
+        w[i] -= lr * ((m[i] / c1) / (sqrtf(v[i] / c2) + eps) + wd * w[i]);
+    }
+}
+
+// Grid of a grid-stride elementwise kernel: one CTA of 256 threads per 256
+// elements, at most 64 CTAs per SM of the current device (its SM count read
+// once per device, so that launches being captured into a graph make no
+// device queries).
 int grid_for(long long total) {
+    static std::atomic<int> sm_count[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = -1;
+    int sms = dev >= 0 ? sm_count[dev].load(std::memory_order_relaxed) : 0;
+    if (sms < 1) {
+        if (dev < 0 || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+            sms = 1;
+        else
+            sm_count[dev].store(sms, std::memory_order_relaxed);
+    }
+    const long long cap = 64LL * sms;
     long long b = (total + 255) / 256;
-    return (int)(b < 1 ? 1 : (b > 148 * 64 ? 148 * 64 : b));
+    return (int)(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
 int status(cudaError_t e) { return e == cudaSuccess ? FBLS_OK : FBLS_ERR_CUDA; }
@@ -309,6 +390,29 @@ int fbls_nn_bias_relu_pool_bwd(const float* dZ, const float* Z, const uint8_t* i
     if (B < 1 || C < 1 || P < 1 || P > 255 || T % P) return FBLS_ERR_ARGUMENT;
     k_bias_relu_pool_bwd<<<grid_for((long long)B * C * (T / P)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         dZ, Z, idx, dY, dbias, B, C, T, P);
+    return status(cudaGetLastError());
+}
+
+int fbls_nn_bias_gelu_pool(const float* Y, const float* bias, float* Z, uint8_t* idx, int B, int C, int T, int P,
+                           void* stream) {
+    if (B < 1 || C < 1 || P < 1 || P > 255 || T % P) return FBLS_ERR_ARGUMENT;
+    k_bias_gelu_pool<<<grid_for((long long)B * C * (T / P)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        Y, bias, Z, idx, B, C, T, P);
+    return status(cudaGetLastError());
+}
+
+int fbls_nn_bias_gelu_pool_bwd(const float* dZ, const float* Y, const uint8_t* idx, const float* bias, float* dY,
+                               float* dbias, int B, int C, int T, int P, void* stream) {
+    if (B < 1 || C < 1 || P < 1 || P > 255 || T % P) return FBLS_ERR_ARGUMENT;
+    k_bias_gelu_pool_bwd<<<grid_for((long long)B * C * (T / P)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        dZ, Y, idx, bias, dY, dbias, B, C, T, P);
+    return status(cudaGetLastError());
+}
+
+int fbls_nn_adamw(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+                  float wd, int t, void* stream) {
+    if (n < 1 || t < 1) return FBLS_ERR_ARGUMENT;
+    k_adamw<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(w, g, m, v, n, lr, b1, b2, eps, wd, t);
     return status(cudaGetLastError());
 }
 

@@ -1,14 +1,14 @@
-"""Proposal network of the learned form: a small 1D CNN that reads a star's
-coarse periodogram (best box score per period and duration, from
-fbls_coarse_map) and scores log-period bands, so that only the best bands get
-the exhaustive scan.
+"""Proposal network of the learned form: a 1D CNN that reads a star's coarse
+periodogram (best box score per period and duration, from fbls_coarse_map)
+and scores log-period bands, so that only the best bands get the exhaustive
+scan.
 
-Input: 4 durations x 4096 log-spaced periods over [0.5, 20] d. Four
-convolution layers (kernel 7, 32 channels, ReLU, max-pool 2, 2, 2, 4), then a
-1x1 head averaged over groups of 4 positions: 32 band logits. Every layer runs
-on this library's kernels (fbls_nn_*): convolutions as bf16 tensor-core GEMMs
-with f32 accumulation, trained by softmax cross-entropy and Adam. torch is
-used for device buffers only.
+Input: 4 durations x 8192 log-spaced periods over [0.5, 20] d. Six
+convolution layers (kernel 7, 64 channels, GELU; max-pool 2 after each of the
+first three), then a 1x1 head: 1024 band logits, one per position; the top 32
+bands are searched. Every layer runs on this library's kernels (fbls_nn_*):
+convolutions as bf16 tensor-core GEMMs with f32 accumulation, trained by
+softmax cross-entropy and AdamW. torch is used for device buffers only.
 """
 from __future__ import annotations
 
@@ -21,13 +21,16 @@ import numpy as np
 from . import _native as N
 
 PMIN, PMAX = 0.5, 20.0
-T_IN = 4096
-BANDS = 32
-CH = 32
+T_IN = 8192
+BANDS = 1024
+CH = 64
 KW = 7
-POOLS = (2, 2, 2, 4)
-HEAD_G = 4
+POOLS = (2, 2, 2, 1, 1, 1)
+HEAD_G = 1
 MAP_CHANNELS = 4
+ACTIVATION = "gelu"
+TOP_BANDS = 32       # bands searched per star
+WEIGHT_DECAY = 1e-4  # AdamW, on the convolution and head weights (not the biases)
 
 
 _MAP_PERIODS = np.geomspace(PMIN, PMAX, T_IN)
@@ -136,6 +139,7 @@ class Net:
             self.views.append((self.w[o:o + k].view(*s), self.grad[o:o + k].view(*s)))
             o += k
         self._ws: Dict[int, dict] = {}
+        self._graphs: Dict[int, tuple] = {}  # captured inference graphs by batch size
         self.ones = torch.ones(4096, dtype=torch.float32, device=self.dev)
 
     # -- workspace -------------------------------------------------------
@@ -169,10 +173,15 @@ class Net:
         if rc != 0:
             raise RuntimeError(f"{what} failed with status {rc}")
 
+    def _stream(self):
+        """torch's current stream: the library's kernels run on it, so a
+        forward pass can be captured into a CUDA graph."""
+        return self.torch.cuda.current_stream(self.dev).cuda_stream
+
     def _gemm(self, A, B, Cm, M, Nn, K, sa, sb, sc, alpha=1.0, beta=0.0, batch=1, bs=(0, 0, 0)):
         self._check(self.lib.fbls_nn_gemm(self._p(A), self._p(B), self._p(Cm), M, Nn, K, sa[0], sa[1], bs[0],
-                                          sb[0], sb[1], bs[1], sc[0], sc[1], bs[2], batch, alpha, beta, None),
-                    "gemm")
+                                          sb[0], sb[1], bs[1], sc[0], sc[1], bs[2], batch, alpha, beta,
+                                          self._stream()), "gemm")
 
     # -- forward / backward ------------------------------------------------
     def forward(self, x, labels=None):
@@ -189,12 +198,12 @@ class Net:
             W, _ = self.views[2 * l]
             b, _ = self.views[2 * l + 1]
             Xc, Y, Z, idx = ws["Xc"][l], ws["Y"][l], ws["Z"][l], ws["idx"][l]
-            self._check(lib.fbls_nn_im2col(self._p(X), self._p(Xc), B, ci, T, KW, KW // 2, None), "im2col")
+            self._check(lib.fbls_nn_im2col(self._p(X), self._p(Xc), B, ci, T, KW, KW // 2, self._stream()), "im2col")
             n = B * T
             # Y (CH x n) = W (CH x ci*KW) . Xc (ci*KW x n)
             self._gemm(W, Xc, Y, CH, n, ci * KW, (ci * KW, 1), (n, 1), (n, 1))
-            self._check(lib.fbls_nn_bias_relu_pool(self._p(Y), self._p(b), self._p(Z), self._p(idx), B, CH, T, P,
-                                                   None), "pool")
+            self._check(lib.fbls_nn_bias_gelu_pool(self._p(Y), self._p(b), self._p(Z), self._p(idx), B, CH, T, P,
+                                                   self._stream()), "activation and pool")
             X = Z
             ws["X"].append(Z)
             T //= P
@@ -207,7 +216,7 @@ class Net:
             lab = ws["labels"]
         self._check(lib.fbls_nn_head(self._p(X), self._p(wh), self._p(bh), self._p(lab) if lab is not None else None,
                                      self._p(ws["logits"]), self._p(ws["loss"]), self._p(ws["dlogits"]), B, CH, T,
-                                     HEAD_G, None), "head")
+                                     HEAD_G, self._stream()), "head")
         loss = ws["loss"].mean() if labels is not None else None
         return ws["logits"], loss
 
@@ -223,7 +232,7 @@ class Net:
         Zl = ws["X"][-1]
         dZ = torch.empty_like(Zl)
         self._check(lib.fbls_nn_head_bwd(self._p(Zl), self._p(wh), self._p(ws["dlogits"]), self._p(dZ), self._p(dwh),
-                                         self._p(dbh), B, CH, T, HEAD_G, None), "head backward")
+                                         self._p(dbh), B, CH, T, HEAD_G, self._stream()), "head backward")
         Ts = [T_IN]
         for P in POOLS:
             Ts.append(Ts[-1] // P)
@@ -232,10 +241,11 @@ class Net:
             Tl = Ts[l]
             ci = MAP_CHANNELS if l == 0 else CH
             W, dW = self.views[2 * l]
-            _, db = self.views[2 * l + 1]
+            b, db = self.views[2 * l + 1]
             dY = torch.empty(CH, B * Tl, device=self.dev)
-            self._check(lib.fbls_nn_bias_relu_pool_bwd(self._p(dZ), self._p(ws["Z"][l]), self._p(ws["idx"][l]),
-                                                       self._p(dY), self._p(db), B, CH, Tl, P, None), "pool backward")
+            self._check(lib.fbls_nn_bias_gelu_pool_bwd(self._p(dZ), self._p(ws["Y"][l]), self._p(ws["idx"][l]),
+                                                       self._p(b), self._p(dY), self._p(db), B, CH, Tl, P,
+                                                       self._stream()), "activation and pool backward")
             n = B * Tl
             Xc = ws["Xc"][l]
             kdim = ci * KW
@@ -254,12 +264,22 @@ class Net:
             dXc = torch.empty(kdim, n, device=self.dev)
             self._gemm(W, dY, dXc, kdim, n, CH, (1, kdim), (n, 1), (n, 1))
             dZ = torch.empty(ci, B * Tl, device=self.dev)
-            self._check(lib.fbls_nn_col2im(self._p(dXc), self._p(dZ), B, ci, Tl, KW, KW // 2, None), "col2im")
+            self._check(lib.fbls_nn_col2im(self._p(dXc), self._p(dZ), B, ci, Tl, KW, KW // 2, self._stream()),
+                        "col2im")
 
-    def adam(self, lr: float = 1e-3):
+    def adam(self, lr: float = 1e-3, weight_decay: float = WEIGHT_DECAY):
+        """One AdamW step: weights decay, biases do not (one launch per
+        parameter tensor)."""
         self.t += 1
-        self._check(self.lib.fbls_nn_adam(self._p(self.w), self._p(self.grad), self._p(self.m), self._p(self.v),
-                                          self.w.numel(), lr, 0.9, 0.999, 1e-8, self.t, None), "adam")
+        o = 0
+        for kind, shape in self.shapes:
+            k = int(np.prod(shape))
+            wd = weight_decay if kind in ("W", "wh") else 0.0
+            off = 4 * o
+            self._check(self.lib.fbls_nn_adamw(self._p(self.w) + off, self._p(self.grad) + off, self._p(self.m) + off,
+                                               self._p(self.v) + off, k, lr, 0.9, 0.999, 1e-8, wd, self.t,
+                                               self._stream()), "adamw")
+            o += k
 
     def state_dict(self) -> np.ndarray:
         return self.w.detach().cpu().numpy().copy()
@@ -270,18 +290,41 @@ class Net:
 
 # ---- data, training, proposal ------------------------------------------------
 
-def survey_stars(count: int, seed: int, max_sectors: int = 13, inject_fraction: float = 1.0):
-    """Seeded survey stars (the survey generator of synth), prepared:
-    [(FamilyState, period_max)] and the base SearchConfig."""
+def _survey_chunk(seed: int, start: int, count: int, max_sectors: int, inject_fraction: float):
     from . import api, synth
-    rng = np.random.default_rng(seed)
     out = []
-    while len(out) < count:
-        c = synth.survey_star(rng, inject_fraction=inject_fraction)
-        if c.time[-1] - c.time[0] > 27.4 * max_sectors + 1.0:
-            continue
+    for i in range(start, start + count):
+        attempt = 0
+        while True:
+            c = synth.survey_star(np.random.default_rng([seed, i, attempt]), inject_fraction=inject_fraction)
+            attempt += 1
+            if c.time[-1] - c.time[0] <= 27.4 * max_sectors + 1.0:
+                break
         cfg = synth.survey_config(c)
         out.append((api.prepared_family(c.time, c.flux, c.flux_err, cfg), cfg.period_max))
+    return out
+
+
+def survey_stars(count: int, seed: int, max_sectors: int = 13, inject_fraction: float = 1.0):
+    """Seeded survey stars (the survey generator of synth, one seeded stream
+    per star, redrawn above max_sectors), prepared: [(FamilyState,
+    period_max)] and the base SearchConfig. Large sets are generated on a
+    pool of spawned processes."""
+    from . import synth
+    chunk = 500
+    starts = list(range(0, count, chunk))
+    sizes = [min(chunk, count - s) for s in starts]
+    if count <= 2 * chunk:
+        out = _survey_chunk(seed, 0, count, max_sectors, inject_fraction)
+    else:
+        import concurrent.futures as cf
+        import multiprocessing as mp
+        import os
+        with cf.ProcessPoolExecutor(max_workers=min(32, os.cpu_count() or 1),
+                                    mp_context=mp.get_context("spawn")) as ex:
+            parts = ex.map(_survey_chunk, [seed] * len(starts), starts, sizes, [max_sectors] * len(starts),
+                           [inject_fraction] * len(starts))
+            out = [x for p in parts for x in p]
     return out, synth.survey_config(synth.survey_star(np.random.default_rng(0)))
 
 
@@ -313,7 +356,8 @@ def features(gpu, stars, devs, bin_days: float = 0.0) -> np.ndarray:
 
 def train(net: Net, x: np.ndarray, y: np.ndarray, epochs: int = 30, batch: int = 128, lr: float = 2e-3,
           seed: int = 0, log=None):
-    """Adam on the softmax cross-entropy of the band labels y (>= 0)."""
+    """AdamW (cosine learning rate) on the softmax cross-entropy of the band
+    labels y (>= 0)."""
     torch = net.torch
     keep = np.nonzero(y >= 0)[0]
     xs = torch.from_numpy(x[:, keep, :]).to(net.dev)
@@ -333,14 +377,45 @@ def train(net: Net, x: np.ndarray, y: np.ndarray, epochs: int = 30, batch: int =
             log(f"epoch {ep} loss {total / max(1, n // batch):.4f}")
 
 
-def scores(net: Net, x: np.ndarray, batch: int = 256) -> np.ndarray:
-    """Band logits (count, BANDS)."""
+def _inference_graph(net: Net, batch: int):
+    """The forward pass of `batch` maps captured once into a CUDA graph (a
+    static input buffer and logits), replayed for every batch: 12 kernel
+    launches become one graph launch."""
+    torch = net.torch
+    if batch in net._graphs:
+        return net._graphs[batch]
+    xin = torch.zeros(MAP_CHANNELS, batch, T_IN, device=net.dev)
+    side = torch.cuda.Stream(net.dev)
+    side.wait_stream(torch.cuda.current_stream(net.dev))
+    with torch.cuda.stream(side):
+        net.forward(xin)  # workspace allocated before the capture
+    torch.cuda.current_stream(net.dev).wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        logits, _ = net.forward(xin)
+    net._graphs[batch] = (graph, xin, logits)
+    return net._graphs[batch]
+
+
+def scores(net: Net, x: np.ndarray, batch: int = 256, graph: bool = True) -> np.ndarray:
+    """Band logits (count, BANDS): the forward pass in batches, replayed from
+    a captured CUDA graph (graph=False launches the kernels one by one)."""
     torch = net.torch
     out = []
+    if graph:
+        g, xin, logits = _inference_graph(net, batch)
     for s in range(0, x.shape[1], batch):
         xb = torch.from_numpy(np.ascontiguousarray(x[:, s:s + batch, :])).to(net.dev)
-        logits, _ = net.forward(xb)
-        out.append(logits[:xb.shape[1]].detach().cpu().numpy().copy())
+        n = xb.shape[1]
+        if graph:
+            xin[:, :n].copy_(xb)
+            if n < batch:
+                xin[:, n:].zero_()
+            g.replay()
+            out.append(logits[:n].detach().cpu().numpy().copy())
+        else:
+            lg, _ = net.forward(xb)
+            out.append(lg[:n].detach().cpu().numpy().copy())
     return np.concatenate(out, axis=0)
 
 
@@ -382,7 +457,7 @@ def load_net(device: int = 0, path=None) -> Net:
     return net
 
 
-def search_proposed(gpu, net: Net, stars, devs, cfg, k: int = 3, workers: int = 0):
+def search_proposed(gpu, net: Net, stars, devs, cfg, k: int = TOP_BANDS, workers: int = 0):
     """The proposal-pruned search of many stars: coarse maps and their
     features in one call, band scores, then the exhaustive search of each
     star's k best bands only (its rows are the full search's rows in those
@@ -406,17 +481,17 @@ def main(argv=None):
     """Trains the proposal network on exhaustive-search labels of seeded survey
     stars and writes its weights and held-out recall:
 
-        python -m fbls_b200.proposal --train 6000 --test 1500 --out weights.npz
+        python -m fbls_b200.proposal --train 50000 --test 5000 --out weights.npz
     """
     import argparse
     import json
     import time
     from . import api
     ap = argparse.ArgumentParser(description=main.__doc__)
-    ap.add_argument("--train", type=int, default=6000)
-    ap.add_argument("--test", type=int, default=1500)
+    ap.add_argument("--train", type=int, default=50000)
+    ap.add_argument("--test", type=int, default=5000)
     ap.add_argument("--max-sectors", type=int, default=4)
-    ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--workers", type=int, default=0, help="search_batch workers of the labelling search")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--bin-minutes", type=float, default=10.0, help="time bins of the coarse map (0: none)")
@@ -440,7 +515,7 @@ def main(argv=None):
         train(net, x[:, :ntr], y[:ntr], epochs=args.epochs, log=log)
         lt = scores(net, x[:, ntr:])
         rec = recall_at(lt, y[ntr:])
-        log("held-out recall@k " + " ".join(f"{k + 1}:{r:.4f}" for k, r in enumerate(rec[:12])))
+        log("held-out recall@k " + " ".join(f"{k}:{rec[k - 1]:.4f}" for k in (1, 2, 4, 8, 16, 32, 64)))
         np.savez(args.out, weights=net.state_dict(), recall=rec, train=ntr, test=args.test, seed=args.seed,
                  max_sectors=args.max_sectors, epochs=args.epochs, bin_days=bin_days)
         print(json.dumps({"recall": rec.tolist(), "labelled_test": int((y[ntr:] >= 0).sum())}))

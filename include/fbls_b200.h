@@ -493,6 +493,12 @@ int fbls_nn_bias_relu_pool(const float* Y, const float* bias, float* Z, uint8_t*
                            void* stream);
 int fbls_nn_bias_relu_pool_bwd(const float* dZ, const float* Z, const uint8_t* idx, float* dY, float* dbias, int B,
                                int C, int T, int P, void* stream);
+/* The same with GELU (x Phi(x)) in place of ReLU; the backward pass reads
+ * the pre-activation Y and the bias. P = 1 is GELU without pooling. */
+int fbls_nn_bias_gelu_pool(const float* Y, const float* bias, float* Z, uint8_t* idx, int B, int C, int T, int P,
+                           void* stream);
+int fbls_nn_bias_gelu_pool_bwd(const float* dZ, const float* Y, const uint8_t* idx, const float* bias, float* dY,
+                               float* dbias, int B, int C, int T, int P, void* stream);
 /* Head: logits[b][j] = mean over a group of G positions of (wh . Z[:, b, t] +
  * bh); with labels, the softmax cross-entropy per curve and d loss_mean /
  * d logits; and its backward pass (dwh, dbh accumulate). */
@@ -503,6 +509,10 @@ int fbls_nn_head_bwd(const float* Z, const float* wh, const float* dlogits, floa
 /* Adam step t (>= 1) with bias correction over n parameters. */
 int fbls_nn_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
                  int t, void* stream);
+/* AdamW step t (>= 1): Adam with the weight decay wd decoupled from the
+ * gradient (w -= lr (m_hat / (sqrt(v_hat) + eps) + wd w)). */
+int fbls_nn_adamw(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+                  float wd, int t, void* stream);
 
 /* signal_search restricted to period ranges [lo, hi) given as n_ranges
  * pairs (no counterpart in the reference; the proposal path's pruned search):

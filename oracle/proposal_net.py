@@ -8,7 +8,8 @@ at tap k, then its bias b (CH,); then the head's wh (CH,) and bh (1,).
 
 Input x is channel-major (C, B, T). A layer computes
 y[o, b, t] = b[o] + sum_{c,k} W[o, c*KW + k] * x[c, b, t + k - KW//2]
-(zero outside [0, T)), then ReLU, then the maximum over P consecutive t. The
+(zero outside [0, T)), then the activation (ReLU, or GELU y Phi(y) with the
+normal CDF Phi), then the maximum over P consecutive t. The
 head computes h[b, t] = sum_c wh[c] * z[c, b, t] + bh and the band logits
 logits[b, g] = mean(h[b, g*G : (g+1)*G]) with G = T_out / bands. The loss is
 the batch mean of the softmax cross-entropy of the band labels.
@@ -26,6 +27,15 @@ from __future__ import annotations
 from typing import List, Sequence, Tuple
 
 import numpy as np
+from scipy.special import erf
+
+
+def _gelu(y):
+    return 0.5 * y * (1.0 + erf(y / np.sqrt(2.0)))
+
+
+def _gelu_grad(y):
+    return 0.5 * (1.0 + erf(y / np.sqrt(2.0))) + y * np.exp(-0.5 * y * y) / np.sqrt(2.0 * np.pi)
 
 
 def shapes(in_channels: int, channels: int, kw: int, pools: Sequence[int]) -> List[Tuple[str, Tuple[int, ...]]]:
@@ -83,9 +93,12 @@ class ProposalNet:
     """Forward and backward of the network for one batch, in f64."""
 
     def __init__(self, in_channels: int, channels: int, kw: int, pools: Sequence[int], bands: int,
-                 operands: str = "f64"):
+                 operands: str = "f64", activation: str = "relu"):
         if operands not in ("f64", "bf16"):
             raise ValueError("operands must be 'f64' or 'bf16'")
+        if activation not in ("relu", "gelu"):
+            raise ValueError("activation must be 'relu' or 'gelu'")
+        self.activation = activation
         self.in_channels, self.channels, self.kw = in_channels, channels, kw
         self.pools, self.bands = tuple(pools), bands
         self._op = bf16_round if operands == "bf16" else (lambda a: a)
@@ -105,7 +118,7 @@ class ProposalNet:
             ci, Tl = h.shape[0], h.shape[2]
             cols = _im2col(h, self.kw)
             y = (self._op(W) @ self._op(cols)).reshape(self.channels, B, Tl) + b[:, None, None]
-            r = np.maximum(y, 0.0)
+            r = np.maximum(y, 0.0) if self.activation == "relu" else _gelu(y)
             win = r.reshape(self.channels, B, Tl // P, P)
             arg = np.argmax(win, axis=3)  # first maximum of each window
             z = np.take_along_axis(win, arg[..., None], axis=3)[..., 0]
@@ -149,7 +162,7 @@ class ProposalNet:
             ci, _, Tl = h.shape
             dr = np.zeros((self.channels, B, Tl // P, P))
             np.put_along_axis(dr, arg[..., None], dz[..., None], axis=3)
-            dy = dr.reshape(self.channels, B, Tl) * (y > 0.0)
+            dy = dr.reshape(self.channels, B, Tl) * ((y > 0.0) if self.activation == "relu" else _gelu_grad(y))
             grads[2 * l + 1] = dy.sum(axis=(1, 2))
             dy2 = dy.reshape(self.channels, B * Tl)
             grads[2 * l] = self._op(dy2) @ self._op(cols).T

@@ -5,11 +5,12 @@ from fbls_b200 import proposal as pr
 
 
 def test_network_flops_counts_the_convolution_gemms():
-    # 4 -> 32 channels at T 4096, then 32 -> 32 at 2048, 1024, 512; kernel 7
-    want = 2 * 32 * 7 * (4 * 4096 + 32 * 2048 + 32 * 1024 + 32 * 512)
-    assert bench._network_flops(1) == want == 58_720_256
+    # 4 -> 64 channels at T 8192, then 64 -> 64 at 4096, 2048 and three times
+    # at 1024 (pools 2, 2, 2, 1, 1, 1); kernel 7
+    want = 2 * 64 * 7 * (4 * 8192 + 64 * 4096 + 64 * 2048 + 3 * 64 * 1024)
+    assert bench._network_flops(1) == want == 557_842_432
     assert bench._network_flops(512) == 512 * want
-    assert pr.T_IN == 4096 and pr.POOLS == (2, 2, 2, 4)
+    assert pr.T_IN == 8192 and pr.POOLS == (2, 2, 2, 1, 1, 1)
 
 
 def test_peaks_fall_back_without_the_measured_file(tmp_path, monkeypatch):

@@ -53,7 +53,8 @@ def _torch_net(net, x, labels):
     ci = pr.MAP_CHANNELS
     for l, P in enumerate(pr.POOLS):
         W = params[2 * l].view(pr.CH, ci, pr.KW)
-        h = F.max_pool1d(F.relu(F.conv1d(h, W, params[2 * l + 1], padding=pr.KW // 2)), P)
+        y = F.conv1d(h, W, params[2 * l + 1], padding=pr.KW // 2)
+        h = F.max_pool1d(F.gelu(y) if pr.ACTIVATION == "gelu" else F.relu(y), P)
         ci = pr.CH
     hh = torch.einsum("bct,c->bt", h, params[-2]) + params[-1]
     logits = hh.view(hh.shape[0], -1, pr.HEAD_G).mean(dim=2)
@@ -226,3 +227,17 @@ def test_binned_coarse_map_is_the_map_of_the_binned_family(gpu):
     assert np.array_equal(got, want)
     dev.free()
     devb.free()
+
+
+def test_graph_captured_inference_equals_launched_inference(gpu):
+    # The inference graph (one capture of the 12 launches of a forward pass,
+    # replayed per batch) gives the logits of the kernels launched one by one.
+    import torch
+    from fbls_b200 import proposal as pr
+    net = pr.Net(0, seed=7)
+    g = torch.Generator().manual_seed(9)
+    x = torch.randn(pr.MAP_CHANNELS, 40, pr.T_IN, generator=g).numpy()
+    a = pr.scores(net, x, batch=16, graph=True)
+    b = pr.scores(net, x, batch=16, graph=False)
+    assert a.shape == (40, pr.BANDS)
+    assert np.array_equal(a, b)

@@ -15,8 +15,8 @@ from fbls_b200 import proposal as pr
 B = 5
 
 
-def _net():
-    return ProposalNet(pr.MAP_CHANNELS, pr.CH, pr.KW, pr.POOLS, pr.BANDS)
+def _net(operands="f64"):
+    return ProposalNet(pr.MAP_CHANNELS, pr.CH, pr.KW, pr.POOLS, pr.BANDS, operands=operands, activation=pr.ACTIVATION)
 
 
 def _weights(net, seed):
@@ -56,7 +56,8 @@ def _torch(net, w, x, labels):
     ci = pr.MAP_CHANNELS
     for l, P in enumerate(pr.POOLS):
         W = views[2 * l].view(pr.CH, ci, pr.KW)
-        h = F.max_pool1d(F.relu(F.conv1d(h, W, views[2 * l + 1], padding=pr.KW // 2)), P)
+        y = F.conv1d(h, W, views[2 * l + 1], padding=pr.KW // 2)
+        h = F.max_pool1d(F.gelu(y) if pr.ACTIVATION == "gelu" else F.relu(y), P)
         ci = pr.CH
     head = torch.einsum("bct,c->bt", h, views[-2]) + views[-1]
     logits = head.view(head.shape[0], pr.BANDS, -1).mean(dim=2)
@@ -130,7 +131,7 @@ def test_bf16_rounding_is_torch_round_to_nearest_even():
 def test_bf16_operand_mode_stays_near_the_f64_mode():
     w = _weights(_net(), 5)
     x, labels = _inputs(15)
-    exact, rounded = _net(), ProposalNet(pr.MAP_CHANNELS, pr.CH, pr.KW, pr.POOLS, pr.BANDS, operands="bf16")
+    exact, rounded = _net(), _net("bf16")
     l64, loss64 = exact.forward(w, x, labels)
     g64 = exact.backward()
     l16, loss16 = rounded.forward(w, x, labels)
@@ -140,3 +141,5 @@ def test_bf16_operand_mode_stays_near_the_f64_mode():
     assert g16 @ g64 / (np.linalg.norm(g16) * np.linalg.norm(g64)) > 0.95
     with pytest.raises(ValueError):
         ProposalNet(pr.MAP_CHANNELS, pr.CH, pr.KW, pr.POOLS, pr.BANDS, operands="f16")
+    with pytest.raises(ValueError):
+        ProposalNet(pr.MAP_CHANNELS, pr.CH, pr.KW, pr.POOLS, pr.BANDS, activation="tanh")
