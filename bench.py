@@ -380,6 +380,10 @@ def run_gpu(args):
                      "algorithmic_bytes_per_launch": fold_bytes_per, "launch_ms": fold_ms_per,
                      "l2": {"peak": l2_peak, "frac": achieved / l2_peak if l2_peak > 0 else None,
                             "peak_kind": f"measured here: copy of a {l2_mib} MiB buffer pair that stays in L2"},
+                     "limiter": {"pipe": "shared memory", "wavefronts_frac_of_peak": 0.763,
+                                 "wavefronts_per_update": 0.90, "dram_frac_of_peak": 0.017,
+                                 "source": "ncu --set full of one nb-1536 launch of this workload "
+                                           "(profiles/k_fold_walk_multi_sector.md)"},
                      "note": "algorithmic bytes count the observation stream once per period (24 n B); it is "
                              "served from L2 and shared memory, and the kernel is bound by the shared-memory "
                              "pipe (76 % of its wavefront peak in an ncu capture; 1.7 % of DRAM peak)"},

@@ -94,7 +94,7 @@ struct EvCand {
     const EvDur* dur;    // nd
     const EvLayer* lay;  // nd x ns x L: the template at width k
     const EvOrbit* orb;  // nd x NORB
-    const EvLayer* olay; // nd x NORB x ns x L: the secondary at its width
+    double* mom;         // (nd x ns) x 3 x nb2: the moment table (see k_ev_screen)
     const double* priors;  // ns x 2: shape log priors (planet, binary)
     double c;            // baseline_norm
     double n;            // observations
@@ -253,16 +253,29 @@ __device__ __forceinline__ void lane_init(Lane& S) {
     S.sum_p = S.sum_b = neg_inf();
 }
 
-// Secondary moments of orbit entry `o` at duration di, shape si: the v sum
-// (ass), the w sum (ps) and the norm (nsum) over both cycles.
-__device__ __forceinline__ void secondary(const EvCand& C, const double* cum, int rs, int nb2, int jj, int di, int o,
-                                          int si, double& ass, double& ps, double& nsum) {
-    const EvOrbit& O = C.orb[di * NORB + o];
-    const int s0 = jj + O.shift;
-    const Sums m = staircase(cum, rs, nb2, s0, s0 + C.nb, C.olay + (((size_t)di * NORB + o) * C.ns + si) * C.L, C.L);
-    ass = m.a0 + m.a1;
-    ps = m.w0 + m.w1;
-    nsum = m.q0 + m.q1;
+// Row p (taken mod 2 nb) of step `step`'s moment table: the staircase's
+// v sum, w sum and norm of the template starting at bin p.
+__device__ __forceinline__ void moment(const EvCand& C, int step, int p, double& a, double& w, double& q) {
+    const int nb2 = 2 * C.nb;
+    if (p >= nb2) p -= nb2;
+    const double* t = C.mom + (size_t)step * 3 * nb2;
+    a = t[p];
+    w = t[nb2 + p];
+    q = t[2 * (size_t)nb2 + p];
+}
+
+// The secondary of orbit entry `o` (a template of the same width, the
+// reference's bank having duration ratio 1, at the primary's start plus the
+// entry's shift) over both cycles: its v sum, w sum and norm.
+__device__ __forceinline__ void secondary(const EvCand& C, int step, int jj, int di, int o, double& ass, double& ps,
+                                          double& nsum) {
+    const int s0 = jj + C.orb[di * NORB + o].shift;
+    double a0, w0, q0, a1, w1, q1;
+    moment(C, step, s0, a0, w0, q0);
+    moment(C, step, (s0 >= 2 * C.nb ? s0 - 2 * C.nb : s0) + C.nb, a1, w1, q1);
+    ass = a0 + a1;
+    ps = w0 + w1;
+    nsum = q0 + q1;
 }
 
 // One template (phase jj, duration di, shape si) of the joint pass: its
@@ -278,8 +291,10 @@ __device__ __forceinline__ Eval joint_template(const EvCand& C, const EvConst& K
     const double c = C.c;
     const EvDur D = C.dur[di];
     const double rho2 = D.rho2, dlm = D.dlm;
-    const Sums m = staircase(cum, rs, nb2, jj, jj + nb, C.lay + ((size_t)di * C.ns + si) * C.L, C.L);
-    const double ae = m.a0, ao = m.a1, pe = m.w0, po = m.w1, ne = m.q0, no = m.q1;
+    const int step = di * C.ns + si;
+    double ae, ao, pe, po, ne, no;
+    moment(C, step, jj, ae, pe, ne);
+    moment(C, step, jj + nb, ao, po, no);
     const double qe = ne - pe * pe / c, qo = no - po * po / c, qeo = -pe * po / c;
     const double ap = ae + ao, qp = qe + qo + 2.0 * qeo;
     const double snr = ap / sqrt(rmax(qp * rho2, 1e-300));
@@ -291,7 +306,7 @@ __device__ __forceinline__ Eval joint_template(const EvCand& C, const EvConst& K
     for (int o = 0; o < NORB; o++) {
         const EvOrbit& O = C.orb[di * NORB + o];
         double ass, ps, nsum;
-        secondary(C, cum, rs, nb2, jj, di, o, si, ass, ps, nsum);
+        secondary(C, step, jj, di, o, ass, ps, nsum);
         const double qs = nsum - ps * ps / c;
         const double qps = -(pe + po) * ps / c;
         const double su = subspace_upper(ap / rho2, ass / rho2, qp / rho2, qs / rho2, qps / rho2, 1.0);
@@ -306,7 +321,7 @@ __device__ __forceinline__ Eval joint_template(const EvCand& C, const EvConst& K
     const double alias_mass = D.k < nb2 / 8 ? 0.0 : neg_inf();
     raw[3] = subspace_upper(ba, bb, bq, br, bx, 1.0) + 1e-6 + alias_mass;
     up[3] = jv ? raw[3] + dlm : neg_inf();
-    const uint32_t keep = decide(up, floor_b, di * C.ns + si);
+    const uint32_t keep = decide(up, floor_b, step);
 
     double lp = neg_inf(), lb = neg_inf(), component_best = neg_inf(), omitted_upper = neg_inf();
     double sec_ratio = 0.0, sec_phase = 0.5, odd_ratio = 1.0, binary_multiple = 1.0;
@@ -314,7 +329,7 @@ __device__ __forceinline__ Eval joint_template(const EvCand& C, const EvConst& K
         if (keep & (1u << o)) {
             const EvOrbit& O = C.orb[di * NORB + o];
             double ass, ps, nsum;
-            secondary(C, cum, rs, nb2, jj, di, o, si, ass, ps, nsum);
+            secondary(C, step, jj, di, o, ass, ps, nsum);
             const double qs = nsum - ps * ps / c;
             const double qps = -(pe + po) * ps / c;
             const double pa = ap / rho2, pb = ass / rho2, pq = qp / rho2, pr = qs / rho2, px = qps / rho2;
@@ -473,11 +488,15 @@ __global__ void __launch_bounds__(256) k_ev_prefix(const EvCand* __restrict__ ca
     }
 }
 
-// Screen (evidence.rs:151-273): per tile the maximum score over its usable
-// templates, and for the tile's best template by merit (0.5 score^2 + log
-// masses; the first lane and first template on ties) the planet and binary
-// evidence lower bounds and its key. A tile without a usable template
-// records zeros.
+// Screen (evidence.rs:151-273), which also writes the moment table: for
+// every step (duration, shape) whose raw width is in range, the staircase's
+// v sum, w sum and norm of the template starting at each of the 2 nb bins
+// (lane j writes bins j and j + nb). The joint pass reads its templates and
+// their quarter-phase secondaries (the same width, shifted) from it. Then
+// per tile the maximum score over its usable templates, and for the tile's
+// best template by merit (0.5 score^2 + log masses; the first lane and first
+// template on ties) the planet and binary evidence lower bounds and its key.
+// A tile without a usable template records zeros.
 __global__ void __launch_bounds__(EV_THREADS, 1) k_ev_screen(const EvCand* __restrict__ cands, int ncand, EvConst K,
                                                              uint32_t* fault) {
     extern __shared__ __align__(128) double ev_rows[];
@@ -506,6 +525,15 @@ __global__ void __launch_bounds__(EV_THREADS, 1) k_ev_screen(const EvCand* __res
         const bool usable = usable_at(C, cum, rs, jj, jv, di);
         for (int si = 0; si < C.ns; si++) {
             const Sums m = staircase(cum, rs, nb2, jj, jj + nb, C.lay + ((size_t)di * C.ns + si) * C.L, C.L);
+            if (jv) {  // the moment table: this template's sums at bins j and j + nb
+                double* t = C.mom + (size_t)(di * C.ns + si) * 3 * nb2;
+                t[j] = m.a0;
+                t[j + nb] = m.a1;
+                t[nb2 + j] = m.w0;
+                t[nb2 + j + nb] = m.w1;
+                t[2 * (size_t)nb2 + j] = m.q0;
+                t[2 * (size_t)nb2 + j + nb] = m.q1;
+            }
             const double a = m.a0 + m.a1;
             const double qe = m.q0 - m.w0 * m.w0 / c, qo = m.q1 - m.w1 * m.w1 / c, qeo = -m.w0 * m.w1 / c;
             const double q = qe + qo + 2.0 * qeo;
@@ -621,18 +649,13 @@ __global__ void __launch_bounds__(128) k_ev_pilot(const EvCand* __restrict__ can
 // pruned against the pilot's floors; per tile the winners by joint evidence
 // and by amplitude (largest value, lowest key) with their values, and the
 // tile's log sums of planet and binary evidence.
-__global__ void __launch_bounds__(EV_THREADS, 1) k_ev_joint(const EvCand* __restrict__ cands, int ncand, EvConst K,
-                                                            uint32_t* fault) {
-    extern __shared__ __align__(128) double ev_rows[];
+__global__ void __launch_bounds__(EV_THREADS, 1) k_ev_joint(const EvCand* __restrict__ cands, int ncand, EvConst K) {
     __shared__ double slot[2][EV_CTA_TILES][2][4];
     __shared__ uint8_t decisions[EV_CTA_TILES][MAX_DURATIONS * MAX_SHAPES];
-    __shared__ __align__(8) uint64_t bar;
     const EvCand& C = cands[candidate_of(cands, ncand, blockIdx.x, true)];
     if (C.pilot[3] == 0.0) return;  // inactive candidate (uniform over the CTA)
     const double floor_p = C.pilot[0], floor_b = C.pilot[1];
-    bool ok;
-    const double* cum = stage_rows(C, ev_rows, &bar, fault, ok);
-    if (!ok) return;
+    const double* cum = C.cum;  // the count row only (the sums come from the moment table)
     const int tl = threadIdx.x >> 6, lane = threadIdx.x & 63;
     // CTA (tile group, part): the part's durations of the group's tiles.
     const int local = (int)blockIdx.x - C.cta0j;
@@ -740,13 +763,13 @@ struct Plan {
     double scale = 0.0, margin = 0.0, log_mass = 0.0;
     std::vector<double> durations, priors;
     std::vector<EvDur> dur;
-    std::vector<EvLayer> lay, olay;
+    std::vector<EvLayer> lay;
     std::vector<EvOrbit> orb;
     FoldShape shape{};
     std::vector<int> chunks;
     int nchunks = 0;
     // workspace offsets (bytes)
-    size_t o_dur = 0, o_lay = 0, o_orb = 0, o_olay = 0, o_pri = 0, o_scale = 0, o_chunks = 0, o_hist = 0,
+    size_t o_dur = 0, o_lay = 0, o_orb = 0, o_mom = 0, o_pri = 0, o_scale = 0, o_chunks = 0, o_hist = 0,
            o_fscratch = 0, o_cum = 0, o_screen = 0, o_rec = 0, o_pilot = 0;
 };
 
@@ -862,13 +885,14 @@ int plan_candidate(const EvidenceCandidate& E, const fbls_config& cfg, int sm_co
             int64_t sk = (int64_t)std::floor((double)k * duration_ratio + 0.5);
             sk = std::min<int64_t>(std::max<int64_t>(sk, 1), (int64_t)nb - 1);
             const int64_t shift = offset + (int64_t)std::floor(((double)k - (double)sk) / 2.0);
-            if (shift < 0) {
+            // The secondary has the primary's width (ratio 1), so its sums are
+            // rows of the primary's moment table, shift bins further on.
+            if (shift < 0 || sk != (int64_t)k || shift >= (int64_t)nb2) {
                 message = "evidence orbit bank outside the cycle";
                 return FBLS_ERR_ARGUMENT;
             }
             P.orb.push_back({(int)shift, 0, phases[o], lp_bank[(size_t)di * NORB + o] + norm_p,
                              lb_bank[(size_t)di * NORB + o] + norm_b});
-            layers_at((uint64_t)sk, P.olay);
             max_start = std::max<int64_t>(max_start, shift + (int64_t)sk);
         }
         max_start = std::max<int64_t>(max_start, (int64_t)k);
@@ -1011,7 +1035,6 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
         P.o_dur = take(P.dur.size() * sizeof(EvDur));
         P.o_lay = take(P.lay.size() * sizeof(EvLayer));
         P.o_orb = take(P.orb.size() * sizeof(EvOrbit));
-        P.o_olay = take(P.olay.size() * sizeof(EvLayer));
         P.o_pri = take(P.priors.size() * sizeof(double));
         P.o_scale = take(sizeof(double));
         P.o_chunks = take(((size_t)P.nchunks + 1) * sizeof(int));
@@ -1023,6 +1046,7 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
         P.o_hist = take(3 * nb2 * sizeof(double));
         P.o_fscratch = P.shape.hist_in_smem ? 0 : take(3 * (size_t)P.shape.row_stride * sizeof(double));
         P.o_cum = take(3 * (nb2 + 2) * sizeof(double));
+        P.o_mom = take((size_t)P.nd * P.ns * 3 * nb2 * sizeof(double));
         P.o_screen = take((size_t)P.tiles * EV_SCREEN * sizeof(double));
     }
     // What comes back to the host, in one contiguous region.
@@ -1074,7 +1098,6 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
         put(P.o_dur, P.dur.data(), P.dur.size() * sizeof(EvDur));
         put(P.o_lay, P.lay.data(), P.lay.size() * sizeof(EvLayer));
         put(P.o_orb, P.orb.data(), P.orb.size() * sizeof(EvOrbit));
-        put(P.o_olay, P.olay.data(), P.olay.size() * sizeof(EvLayer));
         put(P.o_pri, P.priors.data(), P.priors.size() * sizeof(double));
         put(P.o_scale, &P.scale, sizeof(double));
         put(P.o_chunks, P.chunks.data(), ((size_t)P.nchunks + 1) * sizeof(int));
@@ -1087,7 +1110,7 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
         c.dur = reinterpret_cast<const EvDur*>(ws + P.o_dur);
         c.lay = reinterpret_cast<const EvLayer*>(ws + P.o_lay);
         c.orb = reinterpret_cast<const EvOrbit*>(ws + P.o_orb);
-        c.olay = reinterpret_cast<const EvLayer*>(ws + P.o_olay);
+        c.mom = reinterpret_cast<double*>(ws + P.o_mom);
         c.priors = reinterpret_cast<const double*>(ws + P.o_pri);
         c.c = E.r.baseline_norm;
         c.n = (double)E.r.n;
@@ -1180,11 +1203,15 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
                 ctas += (P.tiles + EV_CTA_TILES - 1) / EV_CTA_TILES * (joint ? P.parts : 1);
                 if (cls < 3) smem = std::max(smem, 3 * (2 * (size_t)P.nb + 2) * sizeof(double));
             }
-            const auto kernel = joint ? k_ev_joint : k_ev_screen;
-            if (!check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)EV_STAGE_MAX),
-                       "evidence shared memory"))
-                return false;
-            kernel<<<ctas, EV_THREADS, smem, stream>>>(d_cands + r0, r1 - r0, K, d_fault);
+            if (joint) {
+                k_ev_joint<<<ctas, EV_THREADS, 0, stream>>>(d_cands + r0, r1 - r0, K);
+            } else {
+                if (!check(cudaFuncSetAttribute(k_ev_screen, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)EV_STAGE_MAX),
+                           "evidence shared memory"))
+                    return false;
+                k_ev_screen<<<ctas, EV_THREADS, smem, stream>>>(d_cands + r0, r1 - r0, K, d_fault);
+            }
             if (!counted(cudaGetLastError(), joint ? "evidence joint" : "evidence screen")) return false;
         }
         return true;
