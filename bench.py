@@ -246,12 +246,24 @@ def _cpu_sample(curve, cfg, target_seconds: float):
     return st, every, threads, trials, sec
 
 
+def _workload_config(state, cfg, desc: str, world: int) -> dict:
+    """The `config` of a single-star workload's line, the same for both arms."""
+    from fbls_b200 import api
+    grid, bands = api.band_plan(state, cfg)
+    return {"workload": desc, "stars": world, "periods": int(len(grid)), "bands": len(bands),
+            "observations": state.n, "period_oversample": cfg.period_oversample,
+            "l2": "flushed between steps (256 MiB write)",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"}
+
+
 def run_reference(args):
     world, rank, local = _dist()
     if rank != 0:
         return
+    from fbls_b200 import api
     curve, cfg, desc = _workload(args.workload, args.period_oversample)
-    st, every, threads, trials, sec = _cpu_sample(curve, cfg, args.cpu_seconds / 2)
+    state = api.prepared_family(curve.time, curve.flux, curve.flux_err, cfg)
+    st, every, threads, trials, sec = _cpu_sample(curve, cfg, args.cpu_seconds)
     for _ in range(args.warmup):
         _oracle_sample(st, cfg, every, threads)
     times, tr = [], 0
@@ -266,7 +278,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc, "stars": 1, "parallelism": "host threads"},
+        "config": _workload_config(state, cfg, desc, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference (Rust + cuda-oxide) not buildable offline; its CPU restatement (oracle/) is timed",
@@ -364,10 +376,7 @@ def run_gpu(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc, "stars": world, "periods": int(glen), "bands": len(bands),
-                   "observations": state.n, "period_oversample": cfg.period_oversample,
-                   "l2": "flushed between steps (256 MiB write)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "config": _workload_config(state, cfg, desc, world),
         "stars_per_s": world * args.steps / (total_ms * 1e-3),
         "step_ms": [round(t, 2) for t in times],
         "trials_per_step": trials / args.steps / world,

@@ -2,7 +2,7 @@
 """Writes the golden fixtures of this directory. Run it from the repository
 root where the reference's sources are present:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <path to the reference's source tree>
 
 reference_kats.json
     The known-answer values of the reference's own unit tests, read from its
@@ -206,7 +206,7 @@ def oracle_fixtures():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="the reference's source tree (read as text)")
     args = ap.parse_args()
     ref = Path(args.reference)
     if ref.exists():
