@@ -6,8 +6,10 @@ launch; the built-in rule takes the largest group whose histograms fit while
 every SM still gets a CTA. This sweep measures, per nb class floor(log2(nb)),
 the fold's device time (CUDA events on the context's stream, the library's
 kernel-timing counters) of one scan_bank pass over 4096 periods of the
-13-sector synthetic star at every allowed group cap, and the periods per
-launch on a whole signal_search, and writes the fastest as a table:
+13-sector synthetic star at every allowed group cap, the periods per launch
+on a whole signal_search, and, on a batch of seeded survey stars searched
+together, a CTA per fold unit against the persistent work-stealing fold
+grid; it writes the fastest as a table:
 
     python -m fbls_b200.autotune --out fbls_b200/data/tuning.json
 
@@ -42,6 +44,7 @@ def apply(table: dict) -> None:
     for cls, g in table.get("fold_group_max", {}).items():
         t.fold_group_max[int(cls)] = int(g)
     t.launch_periods = int(table.get("launch_periods", 0))
+    t.fold_steal = int(table.get("fold_steal", 0))
     rc = N.load().fbls_set_tuning(C.byref(t))
     if rc:
         raise ValueError(f"tuning table rejected (status {rc})")
@@ -51,7 +54,7 @@ def current() -> dict:
     t = N.Tuning()
     N.load().fbls_get_tuning(C.byref(t))
     return {"fold_group_max": {str(c): int(g) for c, g in enumerate(t.fold_group_max) if g},
-            "launch_periods": int(t.launch_periods)}
+            "launch_periods": int(t.launch_periods), "fold_steal": int(t.fold_steal)}
 
 
 def reset() -> None:
@@ -77,7 +80,7 @@ def _fold_ms(gpu, dev, periods, bank, nb, reps: int) -> float:
     return gpu.counters(reset=True)["fold_ms"] / reps
 
 
-def sweep(reps: int = 3, log=print) -> dict:
+def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
     from . import api, synth
     c, cfg = synth.multi_sector(), synth.multi_sector_config()
     st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
@@ -123,6 +126,32 @@ def sweep(reps: int = 3, log=print) -> dict:
         out["signal_search_ms"] = {str(k): round(v, 3) for k, v in launches.items()}
         out["launch_periods"] = int(best) if launches[best] < 0.99 * launches[16384] else 0
         dev.free()
+        # The batch's fold jobs: a CTA per unit against the persistent
+        # work-stealing grid, on seeded survey stars searched together.
+        rng = np.random.default_rng(77)
+        stars = []
+        for _ in range(survey_stars):
+            cs = synth.survey_star(rng)
+            cc = synth.survey_config(cs)
+            stars.append((api.prepared_family(cs.time, cs.flux, cs.flux_err, cc), cc.period_max))
+        devs = [gpu.upload(s_) for s_, _ in stars]
+        steal = {}
+        for flag in (0, 1):
+            apply({"fold_group_max": out["fold_group_max"], "launch_periods": out["launch_periods"],
+                   "fold_steal": flag})
+            gpu.search_batch([s_ for s_, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs, workers=0)
+            ts = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                gpu.search_batch([s_ for s_, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs,
+                                 workers=0)
+                ts.append(time.perf_counter() - t0)
+            steal[flag] = sum(ts) / len(ts)
+            log(f"survey of {survey_stars} stars, fold_steal {flag}: {1e3 * steal[flag]:.1f} ms")
+        out["survey_ms"] = {"stars": survey_stars, **{str(k): round(1e3 * v, 2) for k, v in steal.items()}}
+        out["fold_steal"] = 1 if steal[1] < 0.99 * steal[0] else 0
+        for d in devs:
+            d.free()
     reset()
     return out
 
@@ -135,7 +164,8 @@ def main(argv=None):
     t0 = time.time()
     table = sweep(args.reps, log=lambda m: print(f"[{time.time() - t0:6.1f} s] {m}", flush=True))
     Path(args.out).write_text(json.dumps(table, indent=1) + "\n")
-    print(json.dumps({"fold_group_max": table["fold_group_max"], "launch_periods": table["launch_periods"]}))
+    print(json.dumps({"fold_group_max": table["fold_group_max"], "launch_periods": table["launch_periods"],
+                      "fold_steal": table["fold_steal"]}))
 
 
 if __name__ == "__main__":

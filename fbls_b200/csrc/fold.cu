@@ -478,8 +478,12 @@ __device__ __noinline__ void fold_map_epilogue(float* map_out, const double* map
 
 // One CTA of the walking fold: CTA `cta` of the launch described by `a`
 // folds periods [cta * G, cta * G + G).
+// One CTA of the walking fold: CTA `cta` of the launch described by `a`
+// folds periods [cta * G, cta * G + G). `reuse`: this CTA ran an earlier
+// fold (a persistent CTA), whose barriers are invalidated before the new
+// ones. Returns false (uniformly over the CTA) when a staging wait gave up.
 template <int CAP>
-__device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) {
+__device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, const bool reuse) {
     constexpr int F = CAP + 2;  // doubles per staged field
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ double s_scale[MAX_GROUP];
@@ -517,6 +521,10 @@ __device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) 
     }
     const uint32_t bar0 = smem_addr(&s_bar[0]);
     if (tid == 0) {
+        if (reuse) {  // a persistent CTA's earlier fold left its barriers valid (every phase completed)
+            mbar_inval(bar0);
+            mbar_inval(bar0 + 8);
+        }
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -560,7 +568,7 @@ __device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) 
                     if (mbar_wait_bounded(bar0 + 8 * buf, (uint32_t)(blk >> 1) & 1u)) break;
                 atomicOr(a.fault, 1u);
             }
-            return;
+            return false;
         }
         const int next_lo = blk_hi, next_hi = next_lo < nch ? block_end(next_lo) : next_lo;
         if (tid == 0 && next_lo < nch)
@@ -686,7 +694,7 @@ __device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) 
             a.hist_out[nb + p] = hvw[p].y;
             a.hist_out[2 * (size_t)nb + p] = (double)hc[p];
         }
-        return;
+        return true;
     }
     // Doubled prefix rows. A row has S segments of 256 bins whose carries
     // chain; with few rows (large nb, small G) the rows' segments are spread
@@ -753,16 +761,17 @@ __device__ __forceinline__ void fold_walk_cta(const FoldArgs& a, const int cta) 
             if (map && lane == 0) row_final[row] = carry;
         }
     }
-    if (!map) return;
+    if (!map) return true;
 
     __syncthreads();
     fold_map_epilogue(a.map_out, a.map_durations, a.map_rho, a.map_nd, a.map_baseline, a.n, hvw, hc, s_scale,
                       row_final, stage + 6 * F - W, nb, rs, g, g0, W);
+    return true;
 }
 
 template <int CAP>
 __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
-    fold_walk_cta<CAP>(a, blockIdx.x);
+    fold_walk_cta<CAP>(a, blockIdx.x, false);
 }
 
 // Many folds in one launch (the batched search): CTA c runs CTA
@@ -781,7 +790,35 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk_jobs(const FoldArgs* __re
         else
             hi = mid - 1;
     }
-    fold_walk_cta<CAP>(jobs[lo], c - cta0[lo]);
+    fold_walk_cta<CAP>(jobs[lo], c - cta0[lo], false);
+}
+
+// The same jobs as k_fold_walk_jobs, by a persistent grid (one CTA per SM)
+// that steals work: each CTA takes the next unit (one walking-fold CTA's
+// periods of one job) from a global counter until none is left. A CTA whose
+// staging wait gave up stops taking units (its copies may still be pending).
+template <int CAP>
+__global__ void __launch_bounds__(1024, 1) k_fold_walk_steal(const FoldArgs* __restrict__ jobs,
+                                                             const int* __restrict__ cta0, int njobs, int units,
+                                                             unsigned int* __restrict__ next) {
+    __shared__ int s_unit;
+    for (bool reuse = false;; reuse = true) {
+        if (threadIdx.x == 0) s_unit = (int)atomicAdd(next, 1u);
+        __syncthreads();
+        const int u = s_unit;
+        __syncthreads();  // every thread has read s_unit before it is taken again
+        if (u >= units) return;
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {  // last job with cta0[j] <= u
+            const int mid = (lo + hi + 1) / 2;
+            if (cta0[mid] <= u)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        if (!fold_walk_cta<CAP>(jobs[lo], u - cta0[lo], reuse)) return;
+        __syncthreads();  // the unit's shared memory is free before the next one
+    }
 }
 
 namespace {
@@ -796,6 +833,7 @@ constexpr int WALK_CAP = 2048;
 // largest period group per nb class floor(log2(nb)), 0 = the built-in rule.
 std::atomic<uint32_t> g_group_cap[32];
 std::atomic<uint32_t> g_launch_periods{16384};
+std::atomic<uint32_t> g_fold_steal{0};
 
 uint32_t group_cap(int nb) {
     const int cls = nb > 0 ? 31 - __builtin_clz((unsigned)nb) : 0;
@@ -866,15 +904,19 @@ FoldShape fold_group_shape(int nb, int periods, int sm_count) {
     return s;
 }
 
-void set_fold_tuning(const uint32_t* group_caps, uint32_t launch_periods) {
+void set_fold_tuning(const uint32_t* group_caps, uint32_t launch_periods, uint32_t steal) {
     for (int c = 0; c < 32; c++) g_group_cap[c].store(group_caps ? group_caps[c] : 0u, std::memory_order_relaxed);
     g_launch_periods.store(launch_periods ? launch_periods : 16384u, std::memory_order_relaxed);
+    g_fold_steal.store(steal ? 1u : 0u, std::memory_order_relaxed);
 }
 
-void get_fold_tuning(uint32_t* group_caps, uint32_t* launch_periods) {
+void get_fold_tuning(uint32_t* group_caps, uint32_t* launch_periods, uint32_t* steal) {
     for (int c = 0; c < 32; c++) group_caps[c] = g_group_cap[c].load(std::memory_order_relaxed);
     *launch_periods = g_launch_periods.load(std::memory_order_relaxed);
+    *steal = g_fold_steal.load(std::memory_order_relaxed);
 }
+
+bool tuned_fold_steal() { return g_fold_steal.load(std::memory_order_relaxed) != 0; }
 
 uint32_t tuned_launch_periods() { return g_launch_periods.load(std::memory_order_relaxed); }
 
@@ -915,6 +957,19 @@ cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, i
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
     if (e != cudaSuccess) return e;
     k_fold_walk_jobs<WALK_CAP><<<ctas, 1024, smem, stream>>>(jobs, cta0, njobs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, size_t smem,
+                              unsigned int* counter, int sm_count, cudaStream_t stream) {
+    if (njobs < 1 || units < 1 || smem > MAX_FOLD_SMEM || !counter || sm_count < 1) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_fold_walk_steal<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)MAX_FOLD_SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream);
+    if (e != cudaSuccess) return e;
+    const int grid = units < sm_count ? units : sm_count;
+    k_fold_walk_steal<WALK_CAP><<<grid, 1024, smem, stream>>>(jobs, cta0, njobs, units, counter);
     return cudaGetLastError();
 }
 

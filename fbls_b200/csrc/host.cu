@@ -606,11 +606,18 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
     for (size_t wi = 0; wi < waves.size(); wi++) {
         Wave& w = waves[wi];
         if (timing) CK(cudaEventRecord(ctx->pool[3 * wi], s), "event");
-        if (w.fold_jobs)
+        if (w.fold_jobs && tuned_fold_steal()) {
+            CK(ensure(ctx->steal, sizeof(unsigned int)), "workspace");
+            CK(launch_fold_steal(reinterpret_cast<const FoldArgs*>(din + in_total + w.off_fold),
+                                 reinterpret_cast<const int*>(din + in_total + w.off_fcta), w.fold_jobs, w.fold_ctas,
+                                 w.smem, as<unsigned int>(ctx->steal), ctx->sm_count, s),
+               "fold");
+        } else if (w.fold_jobs) {
             CK(launch_fold_jobs(reinterpret_cast<const FoldArgs*>(din + in_total + w.off_fold),
                                 reinterpret_cast<const int*>(din + in_total + w.off_fcta), w.fold_jobs, w.fold_ctas,
                                 w.smem, s),
                "fold");
+        }
         for (const Unit& un : w.units) {
             if (un.walk) continue;
             Pass& p = passes[un.pass];
@@ -1135,7 +1142,7 @@ void fbls_destroy(fbls_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf* bufs[] = {&ctx->cum,     &ctx->cum32,    &ctx->hist,     &ctx->parts, &ctx->keys,  &ctx->tflags,
                       &ctx->pass_in, &ctx->pass_out, &ctx->evidence, &ctx->fault, &ctx->family, &ctx->mapbin, &ctx->feat,
-                      &ctx->rescore};
+                      &ctx->rescore, &ctx->steal};
     for (DevBuf* b : bufs) release(*b);
     for (PinBuf* b : {&ctx->pin_up, &ctx->pin_down, &ctx->pin_down2})
         if (b->ptr) cudaFreeHost(b->ptr);

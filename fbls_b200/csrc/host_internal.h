@@ -48,6 +48,7 @@ struct fbls_ctx {
     fbls::DevBuf cum, cum32, hist, parts, keys, tflags;  // per launch
     fbls::DevBuf pass_in, pass_out;  // per session: every pass's inputs and outputs
     fbls::DevBuf evidence, fault;
+    fbls::DevBuf steal;   // the work counter of a persistent fold grid
     fbls::DevBuf family;  // observations of the star a batch worker is searching
     fbls::DevBuf mapbin;  // time-binned observations of a coarse map
     fbls::DevBuf feat;    // the proposal network's input made from coarse maps

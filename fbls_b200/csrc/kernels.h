@@ -194,11 +194,13 @@ struct BiweightArgs {
 
 FoldShape fold_group_shape(int nb, int periods, int sm_count);
 // Measured tuning of the fold's launch shape (process-wide): per nb class
-// floor(log2(nb)) the largest period group (0 = the built-in rule), and the
-// periods per launch (0 = 16,384).
-void set_fold_tuning(const uint32_t* group_caps, uint32_t launch_periods);
-void get_fold_tuning(uint32_t* group_caps, uint32_t* launch_periods);
+// floor(log2(nb)) the largest period group (0 = the built-in rule), the
+// periods per launch (0 = 16,384), and whether a batch's walking-fold jobs
+// run as a persistent work-stealing grid (launch_fold_steal).
+void set_fold_tuning(const uint32_t* group_caps, uint32_t launch_periods, uint32_t steal);
+void get_fold_tuning(uint32_t* group_caps, uint32_t* launch_periods, uint32_t* steal);
 uint32_t tuned_launch_periods();
+bool tuned_fold_steal();
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
 // spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.
 // Writes count + 1 offsets; returns count, or -1 when capacity is too small.
@@ -217,6 +219,10 @@ cudaError_t launch_fold_smem_jobs(const FoldArgs* jobs, const int* cta0, int njo
                                   cudaStream_t stream);
 cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, size_t smem,
                              cudaStream_t stream);
+// The same fold jobs by a persistent grid of one CTA per SM taking units
+// from `counter` (device memory, zeroed by the launch).
+cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, size_t smem,
+                              unsigned int* counter, int sm_count, cudaStream_t stream);
 cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, cudaStream_t stream);
 cudaError_t launch_merge_jobs(const MergeArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream);
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream);

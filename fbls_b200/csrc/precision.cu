@@ -117,12 +117,12 @@ extern "C" int fbls_set_tuning(const fbls_tuning* tuning) {
         const uint32_t g = tuning->fold_group_max[c];
         if (g > (uint32_t)MAX_GROUP || (g & (g - 1)) != 0) return FBLS_ERR_ARGUMENT;
     }
-    set_fold_tuning(tuning->fold_group_max, tuning->launch_periods);
+    set_fold_tuning(tuning->fold_group_max, tuning->launch_periods, tuning->fold_steal);
     return FBLS_OK;
 }
 
 extern "C" int fbls_get_tuning(fbls_tuning* tuning) {
     if (!tuning) return FBLS_ERR_ARGUMENT;
-    get_fold_tuning(tuning->fold_group_max, &tuning->launch_periods);
+    get_fold_tuning(tuning->fold_group_max, &tuning->launch_periods, &tuning->fold_steal);
     return FBLS_OK;
 }

@@ -250,11 +250,15 @@ int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
  * the autotuner, python -m fbls_b200.autotune, and read back from its table):
  * per nb class floor(log2(nb)) the largest fold period group (a power of two;
  * 0 = the built-in rule: the largest group whose histograms fit shared memory
- * while every SM gets a CTA), and the periods per launch (0 = 16,384).
+ * while every SM gets a CTA), the periods per launch (0 = 16,384), and
+ * fold_steal: nonzero runs a batch's walking-fold jobs (fbls_search_batch
+ * with workers 0) as one persistent grid of a CTA per SM that takes the next
+ * (star, pass, period-group) unit from a counter, instead of a CTA per unit.
  * Process-wide; results do not depend on it, only the launch shapes do. */
 typedef struct {
     uint32_t fold_group_max[32];
     uint32_t launch_periods;
+    uint32_t fold_steal;
 } fbls_tuning;
 int fbls_set_tuning(const fbls_tuning* tuning);
 int fbls_get_tuning(fbls_tuning* tuning);

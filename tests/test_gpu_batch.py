@@ -106,3 +106,26 @@ def test_fused_batch_uploads_every_star(gpu):
         assert np.array_equal(rows, wrows)
     for d in devs:
         d.free()
+
+
+def test_work_stealing_fold_gives_the_same_rows(gpu):
+    # The batch's walking-fold jobs by a persistent grid that takes units from
+    # a counter (fold_steal) against a CTA per unit: the same rows bit for bit.
+    from fbls_b200 import autotune
+    rng = np.random.default_rng(31)
+    stars = []
+    for _ in range(24):
+        c = synth.survey_star(rng)
+        cfg = synth.survey_config(c)
+        stars.append((api.prepared_family(c.time, c.flux, c.flux_err, cfg), cfg.period_max))
+    base = synth.survey_config(synth.survey_star(np.random.default_rng(0)))
+    saved = autotune.current()
+    try:
+        autotune.apply({**saved, "fold_steal": 0})
+        want = gpu.search_batch([s for s, _ in stars], base, period_max=[p for _, p in stars], workers=0)
+        autotune.apply({**saved, "fold_steal": 1})
+        got = gpu.search_batch([s for s, _ in stars], base, period_max=[p for _, p in stars], workers=0)
+    finally:
+        autotune.apply(saved)
+    for (r1, g1, t1), (r2, g2, t2) in zip(got, want):
+        assert np.array_equal(r1, r2) and g1 == g2 and t1 == t2

@@ -179,12 +179,12 @@ def test_oracle_search_does_not_depend_on_its_thread_count():
 def test_tuning_table_round_trip_and_limits():
     from fbls_b200 import autotune
     try:
-        autotune.apply({"fold_group_max": {"10": 4, "11": 2}, "launch_periods": 8192})
-        assert autotune.current() == {"fold_group_max": {"10": 4, "11": 2}, "launch_periods": 8192}
+        autotune.apply({"fold_group_max": {"10": 4, "11": 2}, "launch_periods": 8192, "fold_steal": 1})
+        assert autotune.current() == {"fold_group_max": {"10": 4, "11": 2}, "launch_periods": 8192, "fold_steal": 1}
         with pytest.raises(ValueError):
             autotune.apply({"fold_group_max": {"10": 3}})  # not a power of two
         with pytest.raises(ValueError):
             autotune.apply({"fold_group_max": {"10": 64}})  # above the largest group
     finally:
         autotune.reset()
-    assert autotune.current() == {"fold_group_max": {}, "launch_periods": 16384}
+    assert autotune.current() == {"fold_group_max": {}, "launch_periods": 16384, "fold_steal": 0}
