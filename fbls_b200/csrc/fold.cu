@@ -603,36 +603,38 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
                 const uint32_t base = cur - s0;
                 uint32_t slot = s0;
                 double2 acc = lvw[slot];
-                uint32_t cnt = lc[slot];
+                uint32_t cnt = 0;  // the run's observations, added to the bin's count at its end
                 for (int j = k; j < end; j++) {
                     const uint32_t cj = cell_of(tt[j], scale);
                     if (cj != cur) {
                         lvw[slot] = acc;
-                        lc[slot] = cnt;
+                        atomicAdd(&lc[slot], cnt);
+                        cnt = 0;
                         const uint32_t b = cj - base;
                         slot = b >= unb ? b - unb : b;
                         cur = cj;
                         acc = lvw[slot];
-                        cnt = lc[slot];
                     }
                     acc.x = __dadd_rn(acc.x, tt[j + F]);
                     acc.y = __dadd_rn(acc.y, tt[j + 2 * F]);
                     cnt += 1u;
                 }
                 lvw[slot] = acc;
-                lc[slot] = cnt;
+                atomicAdd(&lc[slot], cnt);
             }
         } else {
         // Lockstep walk: at step i every lane reads observation seg * R + i
         // (R odd, so the lanes' reads fall in distinct banks) and folds it when
         // it lies in the lane's window [k, end). Entering a cell takes the
         // bin's sums prefetched at the previous cell change (the next cell's
-        // bin), and prefetches the bin after it.
+        // bin), and prefetches the bin after it. Counts are integers, so a
+        // run's count is added to its bin with one shared-memory atomic add
+        // when the run ends (no load of the bin's count).
         const int b0 = seg * R;
         const bool has = live && k < end;
         const int steps = __reduce_max_sync(0xffffffffu, has ? end - b0 : 0);
         if (steps > 0) {
-            uint32_t cur = 0, base = 0, slot = 0, nslot = 0, cnt = 0, pcnt = 0;
+            uint32_t cur = 0, base = 0, slot = 0, nslot = 0, cnt = 0;
             double2 acc = make_double2(0.0, 0.0), pre = acc;
             if (has) {
                 cur = cell_of(tt[k], scale);
@@ -641,9 +643,7 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
                 slot = s0;
                 nslot = s0 + 1u == unb ? 0u : s0 + 1u;
                 acc = lvw[slot];
-                cnt = lc[slot];
                 pre = lvw[nslot];
-                pcnt = lc[nslot];
             }
             for (int i = 0; i < steps; i++) {
                 const int o = b0 + i;
@@ -653,21 +653,19 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
                 const uint32_t cj = cell_of(tj, scale);
                 if (in && cj != cur) {
                     lvw[slot] = acc;
-                    lc[slot] = cnt;
+                    atomicAdd(&lc[slot], cnt);
+                    cnt = 0;
                     if (cj == cur + 1u) {
                         acc = pre;
-                        cnt = pcnt;
                         slot = nslot;
                     } else {  // empty cells skipped
                         const uint32_t b = cj - base;
                         slot = b >= unb ? b - unb : b;
                         acc = lvw[slot];
-                        cnt = lc[slot];
                     }
                     cur = cj;
                     nslot = slot + 1u == unb ? 0u : slot + 1u;
                     pre = lvw[nslot];
-                    pcnt = lc[nslot];
                 }
                 if (in) {
                     acc.x = __dadd_rn(acc.x, vj);
@@ -677,7 +675,7 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
             }
             if (has) {
                 lvw[slot] = acc;
-                lc[slot] = cnt;
+                atomicAdd(&lc[slot], cnt);
             }
         }
         }
