@@ -1,15 +1,19 @@
 """Autotuner of the fold's launch shape, measured on the GPU.
 
-The fold's period group (periods per 1024-thread CTA, sharing each staged
-observation chunk) trades shared memory for histograms against CTAs per
-launch; the built-in rule takes the largest group whose histograms fit while
-every SM still gets a CTA. This sweep measures, per nb class floor(log2(nb)),
+The fold's period group (periods per CTA, sharing each staged observation
+chunk) trades shared memory for histograms against CTAs per launch; the
+built-in rule takes the largest group whose histograms fit while every SM
+still gets a CTA. The CTA size sets how many lanes split a staged chunk per
+period, hence the segment each lane walks, and the lockstep threshold picks
+between lanes stepping together (conflict-free reads, idle steps) and each
+walking its own window. This sweep measures, per nb class floor(log2(nb)),
 the fold's device time (CUDA events on the context's stream, the library's
 kernel-timing counters) of one scan_bank pass over 4096 periods of the
-13-sector synthetic star at every allowed group cap, the periods per launch
-on a whole signal_search, and, on a batch of seeded survey stars searched
-together, a CTA per fold unit against the persistent work-stealing fold
-grid; it writes the fastest as a table:
+13-sector synthetic star at every allowed group cap, then at every CTA size
+and lockstep threshold, the periods per launch on a whole signal_search,
+and, on a batch of seeded survey stars searched together, a CTA per fold
+unit against the persistent work-stealing fold grid; it writes the fastest
+as a table:
 
     python -m fbls_b200.autotune --out fbls_b200/data/tuning.json
 
@@ -31,6 +35,8 @@ from . import _native as N
 TABLE = Path(__file__).resolve().parent / "data" / "tuning.json"
 GROUPS = (1, 2, 4, 8, 16, 32)
 LAUNCHES = (4096, 8192, 16384, 32768)
+THREADS = (1024, 512, 256, 128)
+LOCKSTEP = (0, 3, 7, 15, 4096)  # 0: the built-in 11; 4096: never in lockstep
 
 
 def device_name(device: int = 0) -> str:
@@ -43,6 +49,10 @@ def apply(table: dict) -> None:
     t = N.Tuning()
     for cls, g in table.get("fold_group_max", {}).items():
         t.fold_group_max[int(cls)] = int(g)
+    for cls, th in table.get("fold_threads", {}).items():
+        t.fold_threads[int(cls)] = int(th)
+    for cls, lm in table.get("lockstep_min", {}).items():
+        t.lockstep_min[int(cls)] = int(lm)
     t.launch_periods = int(table.get("launch_periods", 0))
     t.fold_steal = int(table.get("fold_steal", 0))
     rc = N.load().fbls_set_tuning(C.byref(t))
@@ -54,6 +64,8 @@ def current() -> dict:
     t = N.Tuning()
     N.load().fbls_get_tuning(C.byref(t))
     return {"fold_group_max": {str(c): int(g) for c, g in enumerate(t.fold_group_max) if g},
+            "fold_threads": {str(c): int(v) for c, v in enumerate(t.fold_threads) if v},
+            "lockstep_min": {str(c): int(v) for c, v in enumerate(t.lockstep_min) if v},
             "launch_periods": int(t.launch_periods), "fold_steal": int(t.fold_steal)}
 
 
@@ -96,6 +108,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
         for band in bands:
             for nb in (band["nb"] // 2, band["nb"]):
                 cases.setdefault(int(np.floor(np.log2(nb))), (nb, band))
+        out["fold_threads"], out["lockstep_min"], out["shape_ms"] = {}, {}, {}
         for cls, (nb, band) in sorted(cases.items()):
             bank = api.bank_for(band, cfg)
             periods = band["periods"][:4096]
@@ -111,9 +124,30 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
                 out["fold_group_max"][str(cls)] = int(best)
             log(f"nb {nb} (class {cls}): " + ", ".join(f"G<={k or 'rule'}: {v:.3f} ms" for k, v in times.items())
                 + f" -> {best or 'rule'}")
+            # CTA size and lockstep threshold at the chosen group cap.
+            caps = {str(cls): out["fold_group_max"][str(cls)]} if str(cls) in out["fold_group_max"] else {}
+            shapes = {}
+            for th in THREADS:
+                for lm in LOCKSTEP:
+                    apply({"fold_group_max": caps, "fold_threads": {str(cls): th}, "lockstep_min": {str(cls): lm}})
+                    shapes[(th, lm)] = _fold_ms(gpu, dev, periods, bank, nb, reps)
+            reset()
+            base = shapes[(1024, 0)]
+            bth, blm = min(shapes, key=shapes.get)
+            out["shape_ms"][str(cls)] = {f"{th}/{lm or 'rule'}": round(v, 4) for (th, lm), v in shapes.items()}
+            if shapes[(bth, blm)] < 0.98 * base:
+                if bth != 1024:
+                    out["fold_threads"][str(cls)] = int(bth)
+                if blm:
+                    out["lockstep_min"][str(cls)] = int(blm)
+            log(f"nb {nb} (class {cls}): threads/lockstep " +
+                ", ".join(f"{th}/{lm or 'rule'}: {v:.3f}" for (th, lm), v in shapes.items()) +
+                f" -> {bth}/{blm or 'rule'}")
+        tuned = {"fold_group_max": out["fold_group_max"], "fold_threads": out["fold_threads"],
+                 "lockstep_min": out["lockstep_min"]}
         launches = {}
         for lp in LAUNCHES:
-            apply({"fold_group_max": out["fold_group_max"], "launch_periods": lp})
+            apply({**tuned, "launch_periods": lp})
             gpu.signal_search(st, cfg, dev=dev)
             ms = []
             for _ in range(reps):
@@ -137,8 +171,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
         devs = [gpu.upload(s_) for s_, _ in stars]
         steal = {}
         for flag in (0, 1):
-            apply({"fold_group_max": out["fold_group_max"], "launch_periods": out["launch_periods"],
-                   "fold_steal": flag})
+            apply({**tuned, "launch_periods": out["launch_periods"], "fold_steal": flag})
             gpu.search_batch([s_ for s_, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs, workers=0)
             ts = []
             for _ in range(reps):
@@ -164,8 +197,8 @@ def main(argv=None):
     t0 = time.time()
     table = sweep(args.reps, log=lambda m: print(f"[{time.time() - t0:6.1f} s] {m}", flush=True))
     Path(args.out).write_text(json.dumps(table, indent=1) + "\n")
-    print(json.dumps({"fold_group_max": table["fold_group_max"], "launch_periods": table["launch_periods"],
-                      "fold_steal": table["fold_steal"]}))
+    print(json.dumps({k: table[k] for k in ("fold_group_max", "fold_threads", "lockstep_min", "launch_periods",
+                                             "fold_steal")}))
 
 
 if __name__ == "__main__":

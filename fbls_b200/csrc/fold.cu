@@ -535,6 +535,7 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
     uint32_t* lc = hc + (size_t)(live ? q : 0) * rs;
     int* lstart = starts + (live ? q : 0) * (NS + 1);
     const float inv_ns = 1.0f / (float)NS;
+    const int lmin = a.lockstep_min > 0 ? a.lockstep_min : LOCKSTEP_MIN_SEGMENT;
     const int nch = a.nchunks;
     // Staging blocks: runs of consecutive chunks of at most CAP observations
     // in all, one bulk copy per field. Between the chunks of a block only the
@@ -595,7 +596,7 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
         if (live && seg == 0) lstart[NS] = len;
         group_sync(gbar, gthreads);
         const int end = live ? lstart[seg + 1] : 0;
-        if (R < LOCKSTEP_MIN_SEGMENT) {
+        if (R < lmin) {
             // Short segments: each lane walks its own window.
             if (live && k < end) {
                 uint32_t cur = cell_of(tt[k], scale);
@@ -825,30 +826,43 @@ constexpr size_t SLOT_BYTES = 3 * sizeof(double);
 constexpr int STAGE_MAX = 4096;
 constexpr int WALK_CAP = 2048;
 
-// Walking-fold shape: 1024 threads, chunks of up to WALK_CAP observations,
-// the largest power-of-two group whose histograms fit beside the staging.
-// Tuning (process-wide, set by fbls_set_tuning from a measured table): the
-// largest period group per nb class floor(log2(nb)), 0 = the built-in rule.
+// Walking-fold shape: chunks of up to WALK_CAP observations, the largest
+// power-of-two group whose histograms fit beside the staging, 1024 threads.
+// Tuning (process-wide, set by fbls_set_tuning from a measured table), per nb
+// class floor(log2(nb)): the largest period group (0 = the built-in rule),
+// and for the callers that ask for it the CTA size (a power of two from 128
+// to 1024, 0 = 1024; a CTA has at least one warp per period) and the lockstep
+// threshold (0 = built-in).
 std::atomic<uint32_t> g_group_cap[32];
+std::atomic<uint32_t> g_threads[32];
+std::atomic<uint32_t> g_lockstep[32];
 std::atomic<uint32_t> g_launch_periods{16384};
 std::atomic<uint32_t> g_fold_steal{0};
 
-uint32_t group_cap(int nb) {
-    const int cls = nb > 0 ? 31 - __builtin_clz((unsigned)nb) : 0;
-    return g_group_cap[cls].load(std::memory_order_relaxed);
-}
+int nb_class(int nb) { return nb > 0 ? 31 - __builtin_clz((unsigned)nb) : 0; }
 
-bool walk_shape(int nb, int periods, int sm_count, FoldShape* out) {
+uint32_t group_cap(int nb) { return g_group_cap[nb_class(nb)].load(std::memory_order_relaxed); }
+
+bool walk_threads_ok(int t) { return t == 128 || t == 256 || t == 512 || t == 1024; }
+
+bool walk_shape(int nb, int periods, int sm_count, bool tuned, FoldShape* out) {
     FoldShape s{};
     s.kind = FOLD_WALK;
     s.threads = 1024;
+    if (tuned) {
+        const uint32_t t = g_threads[nb_class(nb)].load(std::memory_order_relaxed);
+        if (t) s.threads = (int)t;
+        s.lockstep_min = (int)g_lockstep[nb_class(nb)].load(std::memory_order_relaxed);
+    }
+    const int T = s.threads;
     s.row_stride = nb | 1;
     const size_t stage = 6 * sizeof(double) * (size_t)(WALK_CAP + 2);
     const size_t hist_per = (size_t)s.row_stride * BIN_BYTES;
-    auto starts = [&](int g) { return ((size_t)g * (1024 / g + 1) * sizeof(int) + 15) & ~(size_t)15; };
+    auto starts = [&](int g) { return ((size_t)g * (T / g + 1) * sizeof(int) + 15) & ~(size_t)15; };
     if (stage + starts(1) + hist_per > MAX_FOLD_SMEM) return false;
     int g = 1;
-    while (2 * g <= MAX_GROUP && stage + starts(2 * g) + (size_t)(2 * g) * hist_per <= MAX_FOLD_SMEM) g *= 2;
+    while (2 * g <= MAX_GROUP && 2 * g <= T / 32 && stage + starts(2 * g) + (size_t)(2 * g) * hist_per <= MAX_FOLD_SMEM)
+        g *= 2;
     while (g > 1 && (g / 2 >= periods || (periods + g - 1) / g < sm_count)) g /= 2;
     const uint32_t gcap = group_cap(nb);
     while (gcap && g > 1 && (uint32_t)g > gcap) g /= 2;
@@ -871,9 +885,9 @@ bool walk_shape(int nb, int periods, int sm_count, FoldShape* out) {
 // STAGE_MAX); the CTA has 1024 threads, or 512 when segments would
 // otherwise be shorter than 16 observations. A single period whose
 // histogram does not fit folds into global scratch.
-FoldShape fold_group_shape(int nb, int periods, int sm_count) {
+FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned) {
     FoldShape w;
-    if (walk_shape(nb, periods, sm_count, &w)) return w;
+    if (walk_shape(nb, periods, sm_count, tuned, &w)) return w;
     FoldShape s{};
     s.kind = FOLD_SMEM;
     s.row_stride = nb | 1;
@@ -902,16 +916,24 @@ FoldShape fold_group_shape(int nb, int periods, int sm_count) {
     return s;
 }
 
-void set_fold_tuning(const uint32_t* group_caps, uint32_t launch_periods, uint32_t steal) {
-    for (int c = 0; c < 32; c++) g_group_cap[c].store(group_caps ? group_caps[c] : 0u, std::memory_order_relaxed);
-    g_launch_periods.store(launch_periods ? launch_periods : 16384u, std::memory_order_relaxed);
-    g_fold_steal.store(steal ? 1u : 0u, std::memory_order_relaxed);
+void set_fold_tuning(const FoldTuning& t) {
+    for (int c = 0; c < 32; c++) {
+        g_group_cap[c].store(t.group_cap[c], std::memory_order_relaxed);
+        g_threads[c].store(t.threads[c], std::memory_order_relaxed);
+        g_lockstep[c].store(t.lockstep_min[c], std::memory_order_relaxed);
+    }
+    g_launch_periods.store(t.launch_periods ? t.launch_periods : 16384u, std::memory_order_relaxed);
+    g_fold_steal.store(t.steal ? 1u : 0u, std::memory_order_relaxed);
 }
 
-void get_fold_tuning(uint32_t* group_caps, uint32_t* launch_periods, uint32_t* steal) {
-    for (int c = 0; c < 32; c++) group_caps[c] = g_group_cap[c].load(std::memory_order_relaxed);
-    *launch_periods = g_launch_periods.load(std::memory_order_relaxed);
-    *steal = g_fold_steal.load(std::memory_order_relaxed);
+void get_fold_tuning(FoldTuning* t) {
+    for (int c = 0; c < 32; c++) {
+        t->group_cap[c] = g_group_cap[c].load(std::memory_order_relaxed);
+        t->threads[c] = g_threads[c].load(std::memory_order_relaxed);
+        t->lockstep_min[c] = g_lockstep[c].load(std::memory_order_relaxed);
+    }
+    t->launch_periods = g_launch_periods.load(std::memory_order_relaxed);
+    t->steal = g_fold_steal.load(std::memory_order_relaxed);
 }
 
 bool tuned_fold_steal() { return g_fold_steal.load(std::memory_order_relaxed) != 0; }
@@ -946,34 +968,36 @@ int fold_chunks(const double* time, int n, double scale_max, int nb, int span_ca
     return count;
 }
 
-cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, size_t smem,
+cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads, size_t smem,
                              cudaStream_t stream) {
-    if (njobs < 1 || ctas < 1 || smem > MAX_FOLD_SMEM) return cudaErrorInvalidValue;
+    if (njobs < 1 || ctas < 1 || smem > MAX_FOLD_SMEM || !walk_threads_ok(threads)) return cudaErrorInvalidValue;
     // Set at every launch: the attribute belongs to the module loaded in the
     // current context, which a cudaDeviceReset replaces.
     const cudaError_t e = cudaFuncSetAttribute(k_fold_walk_jobs<WALK_CAP>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
     if (e != cudaSuccess) return e;
-    k_fold_walk_jobs<WALK_CAP><<<ctas, 1024, smem, stream>>>(jobs, cta0, njobs);
+    k_fold_walk_jobs<WALK_CAP><<<ctas, threads, smem, stream>>>(jobs, cta0, njobs);
     return cudaGetLastError();
 }
 
-cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, size_t smem,
+cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, int threads, size_t smem,
                               unsigned int* counter, int sm_count, cudaStream_t stream) {
-    if (njobs < 1 || units < 1 || smem > MAX_FOLD_SMEM || !counter || sm_count < 1) return cudaErrorInvalidValue;
+    if (njobs < 1 || units < 1 || smem > MAX_FOLD_SMEM || !counter || sm_count < 1 || !walk_threads_ok(threads))
+        return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(k_fold_walk_steal<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)MAX_FOLD_SMEM);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
     const int grid = units < sm_count ? units : sm_count;
-    k_fold_walk_steal<WALK_CAP><<<grid, 1024, smem, stream>>>(jobs, cta0, njobs, units, counter);
+    k_fold_walk_steal<WALK_CAP><<<grid, threads, smem, stream>>>(jobs, cta0, njobs, units, counter);
     return cudaGetLastError();
 }
 
 bool fold_job_ok(const FoldArgs& a, const FoldShape& shape) {
     return shape.kind == FOLD_WALK && shape.smem <= MAX_FOLD_SMEM && a.group == shape.group && a.group >= 1 &&
-           a.group <= MAX_GROUP && (a.group & (a.group - 1)) == 0 && shape.threads == 1024 && a.nchunks >= 1 &&
+           a.group <= MAX_GROUP && (a.group & (a.group - 1)) == 0 && walk_threads_ok(shape.threads) &&
+           a.group <= shape.threads / 32 && a.lockstep_min >= 0 && a.nchunks >= 1 &&
            a.nb >= 2 && a.stage_field == WALK_CAP + 2 && shape.chunk_cap == WALK_CAP &&
            a.row_stride == shape.row_stride && a.row_stride >= a.nb && a.fault != nullptr &&
            (a.hist_out == nullptr || (a.group == 1 && a.periods == 1 && a.map_out == nullptr)) &&
@@ -1022,7 +1046,8 @@ cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t 
         return cudaErrorInvalidValue;
     if (shape.kind == FOLD_WALK) {
         if (shape.smem > MAX_FOLD_SMEM || a.group != shape.group || a.group < 1 || a.group > MAX_GROUP ||
-            (a.group & (a.group - 1)) != 0 || shape.threads != 1024 || a.nchunks < 1 || a.nb < 2 ||
+            (a.group & (a.group - 1)) != 0 || !walk_threads_ok(shape.threads) || a.group > shape.threads / 32 ||
+            a.lockstep_min < 0 || a.nchunks < 1 || a.nb < 2 ||
             a.stage_field != WALK_CAP + 2 || shape.chunk_cap != WALK_CAP || a.row_stride != shape.row_stride ||
             a.row_stride < a.nb || a.fault == nullptr || (a.hist_out != nullptr && a.group != 1) ||
             (reinterpret_cast<uintptr_t>(a.time) & 15) || (reinterpret_cast<uintptr_t>(a.v) & 15) ||

@@ -186,7 +186,7 @@ int plan_pass(const fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
     if (launch > p.P) launch = p.P;
     p.batch = batch;
     p.launch = launch;
-    p.shape = fold_group_shape((int)nb, (int)launch, ctx->sm_count);
+    p.shape = fold_group_shape((int)nb, (int)launch, ctx->sm_count, true);
     p.chunks.resize((size_t)r->n + 2);
     const int count = fold_chunks(r->time_host.data(), (int)r->n, scale_max, (int)nb, p.shape.span_cap,
                                   p.shape.chunk_cap, p.chunks.data(), (int)p.chunks.size());
@@ -307,6 +307,7 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
             fa.row_stride = p.shape.row_stride;
             fa.fault = as<uint32_t>(ctx->fault);
             fa.rows32_only = p.mode == 2 ? 1 : 0;
+            fa.lockstep_min = p.shape.lockstep_min;
             if (timing) CK(cudaEventRecord(ctx->pool[3 * li], s), "event");
             CK(launch_fold(fa, p.shape, s), "fold");
             if (timing) CK(cudaEventRecord(ctx->pool[3 * li + 1], s), "event");
@@ -413,11 +414,17 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         size_t cum_off, parts_off, hist_off;  // elements within the wave's workspace
         bool walk;
     };
+    // A wave's walking-fold jobs run as one launch per CTA size: job range
+    // [j0, j0 + njobs) with its CTA offsets at fc0 (njobs + 1 entries).
+    struct FoldLaunch {
+        int threads, j0, njobs, fc0, ctas;
+        size_t smem;
+    };
     struct Wave {
         std::vector<Unit> units;
+        std::vector<FoldLaunch> folds;
         size_t cum = 0, parts = 0, hist = 0;
-        int fold_jobs = 0, fold_ctas = 0, scan_ctas = 0, merge_total = 0;
-        size_t smem = 0;
+        int fold_jobs = 0, scan_ctas = 0, merge_total = 0;
         size_t off_fold = 0, off_fcta = 0, off_scan = 0, off_scta = 0, off_merge = 0, off_mp = 0;  // in the job blob
     };
     size_t in_total = 0, out_total = 0;
@@ -448,8 +455,16 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             w.hist += hist;
             if (walk) {
                 w.fold_jobs++;
-                w.fold_ctas += (n + p.shape.group - 1) / p.shape.group;
-                w.smem = std::max(w.smem, p.shape.smem);
+                FoldLaunch* fl = nullptr;
+                for (FoldLaunch& f : w.folds)
+                    if (f.threads == p.shape.threads) fl = &f;
+                if (!fl) {
+                    w.folds.push_back({p.shape.threads, 0, 0, 0, 0, 0});
+                    fl = &w.folds.back();
+                }
+                fl->njobs++;
+                fl->ctas += (n + p.shape.group - 1) / p.shape.group;
+                fl->smem = std::max(fl->smem, p.shape.smem);
             }
             w.scan_ctas += n * (int)tiles;
             w.merge_total += n;
@@ -471,7 +486,14 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         hist_max = std::max(hist_max, w.hist);
         const size_t nu = w.units.size();
         w.off_fold = take(std::max(1, w.fold_jobs) * sizeof(FoldArgs));
-        w.off_fcta = take((w.fold_jobs + 1) * sizeof(int));
+        int j0 = 0, fc0 = 0;
+        for (FoldLaunch& f : w.folds) {
+            f.j0 = j0;
+            f.fc0 = fc0;
+            j0 += f.njobs;
+            fc0 += f.njobs + 1;
+        }
+        w.off_fcta = take((w.fold_jobs + w.folds.size() + 1) * sizeof(int));
         w.off_scan = take(nu * sizeof(ScanArgs));
         w.off_scta = take((nu + 1) * sizeof(int));
         w.off_merge = take(nu * sizeof(MergeArgs));
@@ -507,7 +529,8 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         int* sc = reinterpret_cast<int*>(up + in_total + w.off_scta);
         MergeArgs* mj = reinterpret_cast<MergeArgs*>(up + in_total + w.off_merge);
         int* mp = reinterpret_cast<int*>(up + in_total + w.off_mp);
-        int nf = 0, fcta = 0, scta = 0, mtot = 0;
+        int scta = 0, mtot = 0;
+        std::vector<int> nf(w.folds.size(), 0), fcta(w.folds.size(), 0);  // per CTA size: jobs and CTAs so far
         for (size_t u = 0; u < w.units.size(); u++) {
             const Unit& un = w.units[u];
             Pass& p = passes[un.pass];
@@ -538,11 +561,15 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             fa.row_stride = p.shape.row_stride;
             fa.fault = as<uint32_t>(ctx->fault);
             fa.rows32_only = p.mode == 2 ? 1 : 0;
+            fa.lockstep_min = p.shape.lockstep_min;
             if (un.walk) {
                 if (!fold_job_ok(fa, p.shape)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
-                fj[nf] = fa;
-                fc[nf++] = fcta;
-                fcta += (un.n + p.shape.group - 1) / p.shape.group;
+                size_t g = 0;
+                while (w.folds[g].threads != p.shape.threads) g++;
+                const FoldLaunch& fl = w.folds[g];
+                fj[fl.j0 + nf[g]] = fa;
+                fc[fl.fc0 + nf[g]++] = fcta[g];
+                fcta[g] += (un.n + p.shape.group - 1) / p.shape.group;
             }
             ScanArgs sa{};
             sa.cum = fa.cum;
@@ -588,7 +615,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             ctx->counters.fold_updates += (uint64_t)un.n * r->n;
             ctx->counters.scan_bytes += (double)un.n * (24.0 * (2.0 * nb + 1.0) + 84.0 * tiles);
         }
-        fc[nf] = fcta;
+        for (size_t g = 0; g < w.folds.size(); g++) fc[w.folds[g].fc0 + nf[g]] = fcta[g];
         sc[w.units.size()] = scta;
         mp[w.units.size()] = mtot;
     }
@@ -606,17 +633,18 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
     for (size_t wi = 0; wi < waves.size(); wi++) {
         Wave& w = waves[wi];
         if (timing) CK(cudaEventRecord(ctx->pool[3 * wi], s), "event");
-        if (w.fold_jobs && tuned_fold_steal()) {
-            CK(ensure(ctx->steal, sizeof(unsigned int)), "workspace");
-            CK(launch_fold_steal(reinterpret_cast<const FoldArgs*>(din + in_total + w.off_fold),
-                                 reinterpret_cast<const int*>(din + in_total + w.off_fcta), w.fold_jobs, w.fold_ctas,
-                                 w.smem, as<unsigned int>(ctx->steal), ctx->sm_count, s),
-               "fold");
-        } else if (w.fold_jobs) {
-            CK(launch_fold_jobs(reinterpret_cast<const FoldArgs*>(din + in_total + w.off_fold),
-                                reinterpret_cast<const int*>(din + in_total + w.off_fcta), w.fold_jobs, w.fold_ctas,
-                                w.smem, s),
-               "fold");
+        for (const FoldLaunch& fl : w.folds) {
+            const FoldArgs* jobs = reinterpret_cast<const FoldArgs*>(din + in_total + w.off_fold) + fl.j0;
+            const int* cta0 = reinterpret_cast<const int*>(din + in_total + w.off_fcta) + fl.fc0;
+            if (tuned_fold_steal()) {
+                CK(ensure(ctx->steal, sizeof(unsigned int)), "workspace");
+                CK(launch_fold_steal(jobs, cta0, fl.njobs, fl.ctas, fl.threads, fl.smem, as<unsigned int>(ctx->steal),
+                                     ctx->sm_count, s),
+                   "fold");
+            } else {
+                CK(launch_fold_jobs(jobs, cta0, fl.njobs, fl.ctas, fl.threads, fl.smem, s), "fold");
+            }
+            ctx->counters.launches += 1;
         }
         for (const Unit& un : w.units) {
             if (un.walk) continue;
@@ -644,6 +672,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             fa.fault = as<uint32_t>(ctx->fault);
             fa.rows32_only = p.mode == 2 ? 1 : 0;
             CK(launch_fold(fa, p.shape, s), "fold");
+            ctx->counters.launches += 1;
         }
         if (timing) CK(cudaEventRecord(ctx->pool[3 * wi + 1], s), "event");
         CK(launch_scan_jobs(reinterpret_cast<const ScanArgs*>(din + in_total + w.off_scan),
@@ -655,7 +684,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
                              w.merge_total, s),
            "merge");
         if (timing) CK(cudaEventRecord(ctx->pool[3 * wi + 2], s), "event");
-        ctx->counters.launches += 3;
+        ctx->counters.launches += 2;
     }
     unsigned char* down = static_cast<unsigned char*>(down_buf.ptr);
     CK(cudaMemcpyAsync(down, dout, out_total, cudaMemcpyDeviceToHost, s), "download");

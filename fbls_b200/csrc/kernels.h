@@ -48,6 +48,7 @@ struct FoldArgs {
     int row_stride;        // FoldShape::row_stride
     uint32_t* fault;       // FOLD_WALK: set nonzero when a staging wait gives up
     int rows32_only;       // FOLD_WALK: write only the (hi, lo) f32 rows (the f32 form reads no f64 rows)
+    int lockstep_min;      // FOLD_WALK: segments at least this long are walked in lockstep (0: the built-in 11)
     // Coarse-map epilogue (FOLD_WALK only): when map_out is set, the prefix
     // rows stay in shared memory (cum / cum32 unused) and each period's best
     // box score per map duration, as k_box_map computes it, goes to
@@ -71,6 +72,20 @@ struct FoldShape {
     int threads;        // CTA size
     int stage_field;    // staged slots per field: chunk_cap + segments
     size_t smem;        // dynamic shared memory bytes
+    int lockstep_min;   // FOLD_WALK: FoldArgs::lockstep_min for this shape (0: built-in)
+};
+
+// Measured tuning of the fold's launch shape (process-wide): per nb class
+// floor(log2(nb)) the largest period group (0 = the built-in rule), the
+// walking fold's CTA size (128, 256, 512 or 1024; 0 = 1024) and its lockstep
+// threshold (0 = the built-in 11); the periods per launch (0 = 16,384), and
+// whether a batch's walking-fold jobs run as a persistent work-stealing grid.
+struct FoldTuning {
+    uint32_t group_cap[32];
+    uint32_t threads[32];
+    uint32_t lockstep_min[32];
+    uint32_t launch_periods;
+    uint32_t steal;
 };
 
 struct ScanArgs {
@@ -192,13 +207,12 @@ struct BiweightArgs {
     double* out;             // n: flux / location - 1
 };
 
-FoldShape fold_group_shape(int nb, int periods, int sm_count);
-// Measured tuning of the fold's launch shape (process-wide): per nb class
-// floor(log2(nb)) the largest period group (0 = the built-in rule), the
-// periods per launch (0 = 16,384), and whether a batch's walking-fold jobs
-// run as a persistent work-stealing grid (launch_fold_steal).
-void set_fold_tuning(const uint32_t* group_caps, uint32_t launch_periods, uint32_t steal);
-void get_fold_tuning(uint32_t* group_caps, uint32_t* launch_periods, uint32_t* steal);
+// Launch shape of a fold of `periods` periods at nb bins. `tuned`: the
+// walking fold takes its CTA size and lockstep threshold from the tuning
+// table (callers whose job launches mix shapes keep 1024 threads).
+FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned = false);
+void set_fold_tuning(const FoldTuning& t);
+void get_fold_tuning(FoldTuning* t);
 uint32_t tuned_launch_periods();
 bool tuned_fold_steal();
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
@@ -217,11 +231,12 @@ bool fold_job_ok(const FoldArgs& a, const FoldShape& shape);
 bool fold_smem_job_ok(const FoldArgs& a, const FoldShape& shape);
 cudaError_t launch_fold_smem_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads, size_t smem,
                                   cudaStream_t stream);
-cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, size_t smem,
+// Walking-fold jobs of one CTA size (`threads`, of their shapes).
+cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads, size_t smem,
                              cudaStream_t stream);
 // The same fold jobs by a persistent grid of one CTA per SM taking units
 // from `counter` (device memory, zeroed by the launch).
-cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, size_t smem,
+cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, int threads, size_t smem,
                               unsigned int* counter, int sm_count, cudaStream_t stream);
 cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, cudaStream_t stream);
 cudaError_t launch_merge_jobs(const MergeArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream);

@@ -113,16 +113,32 @@ extern "C" int fbls_precision_bins(fbls_ctx* ctx, const fbls_ready* ready, const
 
 extern "C" int fbls_set_tuning(const fbls_tuning* tuning) {
     if (!tuning) return FBLS_ERR_ARGUMENT;
+    FoldTuning t{};
     for (int c = 0; c < 32; c++) {
-        const uint32_t g = tuning->fold_group_max[c];
+        const uint32_t g = tuning->fold_group_max[c], th = tuning->fold_threads[c], l = tuning->lockstep_min[c];
         if (g > (uint32_t)MAX_GROUP || (g & (g - 1)) != 0) return FBLS_ERR_ARGUMENT;
+        if (th != 0 && th != 128 && th != 256 && th != 512 && th != 1024) return FBLS_ERR_ARGUMENT;
+        if (l > 4096) return FBLS_ERR_ARGUMENT;
+        t.group_cap[c] = g;
+        t.threads[c] = th;
+        t.lockstep_min[c] = l;
     }
-    set_fold_tuning(tuning->fold_group_max, tuning->launch_periods, tuning->fold_steal);
+    t.launch_periods = tuning->launch_periods;
+    t.steal = tuning->fold_steal;
+    set_fold_tuning(t);
     return FBLS_OK;
 }
 
 extern "C" int fbls_get_tuning(fbls_tuning* tuning) {
     if (!tuning) return FBLS_ERR_ARGUMENT;
-    get_fold_tuning(tuning->fold_group_max, &tuning->launch_periods, &tuning->fold_steal);
+    FoldTuning t{};
+    get_fold_tuning(&t);
+    for (int c = 0; c < 32; c++) {
+        tuning->fold_group_max[c] = t.group_cap[c];
+        tuning->fold_threads[c] = t.threads[c];
+        tuning->lockstep_min[c] = t.lockstep_min[c];
+    }
+    tuning->launch_periods = t.launch_periods;
+    tuning->fold_steal = t.steal;
     return FBLS_OK;
 }

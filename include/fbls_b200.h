@@ -254,11 +254,18 @@ int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
  * fold_steal: nonzero runs a batch's walking-fold jobs (fbls_search_batch
  * with workers 0) as one persistent grid of a CTA per SM that takes the next
  * (star, pass, period-group) unit from a counter, instead of a CTA per unit.
+ * Per nb class, for the signal-search folds: fold_threads, the walking
+ * fold's CTA size (128, 256, 512 or 1024; 0 = 1024; the period group is cut
+ * to at most one period per warp), and lockstep_min, the segment length from
+ * which a CTA's lanes walk their observations in lockstep rather than each
+ * its own window (0 = 11; at most 4096).
  * Process-wide; results do not depend on it, only the launch shapes do. */
 typedef struct {
     uint32_t fold_group_max[32];
     uint32_t launch_periods;
     uint32_t fold_steal;
+    uint32_t fold_threads[32];
+    uint32_t lockstep_min[32];
 } fbls_tuning;
 int fbls_set_tuning(const fbls_tuning* tuning);
 int fbls_get_tuning(fbls_tuning* tuning);

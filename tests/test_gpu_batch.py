@@ -129,3 +129,39 @@ def test_work_stealing_fold_gives_the_same_rows(gpu):
         autotune.apply(saved)
     for (r1, g1, t1), (r2, g2, t2) in zip(got, want):
         assert np.array_equal(r1, r2) and g1 == g2 and t1 == t2
+
+
+@pytest.mark.parametrize("threads,lockstep", [(128, 0), (256, 3), (512, 4096), (1024, 3)])
+def test_fold_cta_size_and_lockstep_give_the_same_rows(gpu, threads, lockstep):
+    # The walking fold at every CTA size and lockstep threshold the tuning
+    # table allows, in both the per-star search and the batch's job launches
+    # (where shapes of several CTA sizes share a wave), with and without work
+    # stealing: the same rows bit for bit as the built-in shape.
+    from fbls_b200 import autotune
+    rng = np.random.default_rng(37)
+    stars = []
+    for _ in range(12):
+        c = synth.survey_star(rng)
+        cfg = synth.survey_config(c)
+        stars.append((api.prepared_family(c.time, c.flux, c.flux_err, cfg), cfg.period_max))
+    base = synth.survey_config(synth.survey_star(np.random.default_rng(0)))
+    one = synth.single_sector()
+    one_cfg = synth.single_sector_config()
+    one_st = api.prepared_family(one.time, one.flux, one.flux_err, one_cfg)
+    saved = autotune.current()
+    try:
+        autotune.reset()
+        want = gpu.search_batch([s for s, _ in stars], base, period_max=[p for _, p in stars], workers=0)
+        want_one = gpu.signal_search(one_st, one_cfg)
+        # every class but the smallest at the CTA size under test, so a wave mixes sizes
+        classes = {str(c): threads for c in range(7, 16)}
+        for steal in (0, 1):
+            autotune.apply({"fold_threads": classes, "lockstep_min": {str(c): lockstep for c in range(32)} if lockstep
+                            else {}, "fold_steal": steal})
+            got = gpu.search_batch([s for s, _ in stars], base, period_max=[p for _, p in stars], workers=0)
+            for (r1, g1, t1), (r2, g2, t2) in zip(got, want):
+                assert np.array_equal(r1, r2) and g1 == g2 and t1 == t2
+        got_one = gpu.signal_search(one_st, one_cfg)
+        assert np.array_equal(got_one[0], want_one[0]) and got_one[1] == want_one[1]
+    finally:
+        autotune.apply(saved)

@@ -179,12 +179,19 @@ def test_oracle_search_does_not_depend_on_its_thread_count():
 def test_tuning_table_round_trip_and_limits():
     from fbls_b200 import autotune
     try:
-        autotune.apply({"fold_group_max": {"10": 4, "11": 2}, "launch_periods": 8192, "fold_steal": 1})
-        assert autotune.current() == {"fold_group_max": {"10": 4, "11": 2}, "launch_periods": 8192, "fold_steal": 1}
+        table = {"fold_group_max": {"10": 4, "11": 2}, "fold_threads": {"10": 512, "11": 256},
+                 "lockstep_min": {"10": 7}, "launch_periods": 8192, "fold_steal": 1}
+        autotune.apply(table)
+        assert autotune.current() == table
         with pytest.raises(ValueError):
             autotune.apply({"fold_group_max": {"10": 3}})  # not a power of two
         with pytest.raises(ValueError):
             autotune.apply({"fold_group_max": {"10": 64}})  # above the largest group
+        with pytest.raises(ValueError):
+            autotune.apply({"fold_threads": {"10": 384}})  # not a walking-fold CTA size
+        with pytest.raises(ValueError):
+            autotune.apply({"lockstep_min": {"10": 5000}})
     finally:
         autotune.reset()
-    assert autotune.current() == {"fold_group_max": {}, "launch_periods": 16384, "fold_steal": 0}
+    assert autotune.current() == {"fold_group_max": {}, "fold_threads": {}, "lockstep_min": {}, "launch_periods": 16384,
+                                  "fold_steal": 0}
