@@ -55,6 +55,7 @@ def apply(table: dict) -> None:
         t.lockstep_min[int(cls)] = int(lm)
     t.launch_periods = int(table.get("launch_periods", 0))
     t.fold_steal = int(table.get("fold_steal", 0))
+    t.separate_scan = int(table.get("separate_scan", 0))
     rc = N.load().fbls_set_tuning(C.byref(t))
     if rc:
         raise ValueError(f"tuning table rejected (status {rc})")
@@ -66,7 +67,8 @@ def current() -> dict:
     return {"fold_group_max": {str(c): int(g) for c, g in enumerate(t.fold_group_max) if g},
             "fold_threads": {str(c): int(v) for c, v in enumerate(t.fold_threads) if v},
             "lockstep_min": {str(c): int(v) for c, v in enumerate(t.lockstep_min) if v},
-            "launch_periods": int(t.launch_periods), "fold_steal": int(t.fold_steal)}
+            "launch_periods": int(t.launch_periods), "fold_steal": int(t.fold_steal),
+            "separate_scan": int(t.separate_scan)}
 
 
 def reset() -> None:

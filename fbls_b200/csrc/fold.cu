@@ -31,6 +31,7 @@
 #include "bulk.cuh"
 #include "common.cuh"
 #include "kernels.h"
+#include "scan_tile.cuh"
 
 namespace fbls {
 
@@ -49,12 +50,6 @@ __device__ __forceinline__ uint32_t mod_nb(uint32_t v, uint32_t nb, double inv_n
 
 __device__ __forceinline__ uint32_t cell_of(double t, double scale) {
     return (uint32_t)floor(__dmul_rn(t, scale));
-}
-
-__device__ __forceinline__ float2 split_pair(double value) {
-    float hi = __double2float_rn(value);
-    float lo = __double2float_rn(__dsub_rn(value, (double)hi));
-    return make_float2(hi, lo);
 }
 
 // Doubled exclusive prefix of one row by one warp, in the order of the
@@ -476,14 +471,37 @@ __device__ __noinline__ void fold_map_epilogue(float* map_out, const double* map
 }
 
 
-// One CTA of the walking fold: CTA `cta` of the launch described by `a`
-// folds periods [cta * G, cta * G + G).
+// The fused tile scan of a walking-fold CTA (after the in-place prefix rows
+// and a barrier), out of line like the map epilogue, so the fold's loop keeps
+// its registers: groups of TILE threads take the (period, tile) units of the
+// CTA's periods in turn and scan them from the in-place rows, each group with
+// its own scratch.
+__device__ __noinline__ void fold_scan_epilogue(const ScanArgs& scan, const double2* hvw, const uint32_t* hc,
+                                                const double* row_final, const double* s_scale, TileScratch* scratch,
+                                                int nb, int rs, int g, int g0) {
+    const int tiles = (nb + TILE - 1) / TILE;
+    const int ngroups = (int)blockDim.x / TILE;
+    const int gi = (int)threadIdx.x / TILE;
+    const NamedGroup grp{1u + (uint32_t)gi, gi * TILE};
+    for (int u = gi; u < g * tiles; u += ngroups) {
+        const int qq = u / tiles, t = u - qq * tiles;
+        SmemRows rows;
+        rows.vw = hvw + (size_t)qq * rs;
+        rows.c = hc + (size_t)qq * rs;
+        rows.fin = row_final + qq * NF;
+        rows.nb = (uint32_t)nb;
+        grp.sync();  // the group's scratch is free: its previous unit is done with it
+        scan_tile(scan, rows, grp, scratch[gi], t, g0 + qq, tiles, s_scale[qq]);
+    }
+}
+
 // One CTA of the walking fold: CTA `cta` of the launch described by `a`
 // folds periods [cta * G, cta * G + G). `reuse`: this CTA ran an earlier
 // fold (a persistent CTA), whose barriers are invalidated before the new
 // ones. Returns false (uniformly over the CTA) when a staging wait gave up.
 template <int CAP>
-__device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, const bool reuse) {
+__device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, const bool reuse,
+                                              const ScanArgs* scan) {
     constexpr int F = CAP + 2;  // doubles per staged field
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ double s_scale[MAX_GROUP];
@@ -704,10 +722,12 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
     const int W = T / 32;
     const int rows = g * NF;
     const int S = (nb + 255) >> 8;
+    const bool map = a.map_out != nullptr;
+    const bool in_place = map || scan != nullptr;  // the rows stay in shared memory
     auto row_of = [&](int row, double*& out64, float2*& out32) {
         const int qq = row / NF, f = row - qq * NF;
-        out64 = a.rows32_only ? nullptr : a.cum + ((size_t)(g0 + qq) * NF + f) * stride;
-        out32 = a.cum32 + ((size_t)(g0 + qq) * NF + f) * stride;
+        out64 = (a.rows32_only || in_place) ? nullptr : a.cum + ((size_t)(g0 + qq) * NF + f) * stride;
+        out32 = in_place ? nullptr : a.cum32 + ((size_t)(g0 + qq) * NF + f) * stride;
         const size_t o = (size_t)qq * rs;
         HistRow r;
         r.d = f == F_V ? &hvw[o].x : f == F_W ? &hvw[o].y : nullptr;
@@ -715,9 +735,12 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
         return r;
     };
     const int items = rows * S;
-    const bool map = a.map_out != nullptr;
-    double* row_final = stage;  // rows: each row's final carry (map epilogue)
-    if (2 * ((items + W - 1) / W) < ((rows + W - 1) / W) * S && 2 * items + rows + W <= 6 * F) {
+    double* row_final = stage;  // rows: each row's final carry (map epilogue, fused scan)
+    // The tail of the staging buffers is kept for the epilogue: the map's
+    // per-warp partial maxima, or the fused scan's per-group scratch.
+    const int ngroups = T / TILE;
+    const int scratch_doubles = scan ? ngroups * (int)((sizeof(TileScratch) + 7) / 8) : W;
+    if (2 * ((items + W - 1) / W) < ((rows + W - 1) / W) * S && 2 * items + rows + scratch_doubles <= 6 * F) {
         double* seg_total = stage;             // rows x S (the staging buffers are idle now)
         double* seg_carry = stage + items;     // rows x S
         row_final = stage + 2 * items;         // rows
@@ -744,11 +767,11 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
             double* o64;
             float2* o32;
             const HistRow r = row_of(row, o64, o32);
-            if (!map && sg == 0 && lane == 0) {
+            if (!in_place && sg == 0 && lane == 0) {
                 if (o64) o64[0] = 0.0;
                 o32[0] = make_float2(0.f, 0.f);
             }
-            prefix_segment(r, nb, sg * 256, seg_carry[it], row_final[row], map ? SEG_IN_PLACE : SEG_GLOBAL, o64,
+            prefix_segment(r, nb, sg * 256, seg_carry[it], row_final[row], in_place ? SEG_IN_PLACE : SEG_GLOBAL, o64,
                            o32);
         }
     } else {
@@ -756,13 +779,18 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
             double* o64;
             float2* o32;
             const HistRow r = row_of(row, o64, o32);
-            const double carry = prefix_row_smem(r, nb, !map, o64, o32);
-            if (map && lane == 0) row_final[row] = carry;
+            const double carry = prefix_row_smem(r, nb, !in_place, o64, o32);
+            if (in_place && lane == 0) row_final[row] = carry;
         }
     }
-    if (!map) return true;
+    if (!in_place) return true;
 
     __syncthreads();
+    if (scan) {
+        fold_scan_epilogue(*scan, hvw, hc, row_final, s_scale,
+                           reinterpret_cast<TileScratch*>(stage + 6 * F - scratch_doubles), nb, rs, g, g0);
+        return true;
+    }
     fold_map_epilogue(a.map_out, a.map_durations, a.map_rho, a.map_nd, a.map_baseline, a.n, hvw, hc, s_scale,
                       row_final, stage + 6 * F - W, nb, rs, g, g0, W);
     return true;
@@ -770,7 +798,13 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
 
 template <int CAP>
 __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
-    fold_walk_cta<CAP>(a, blockIdx.x, false);
+    fold_walk_cta<CAP>(a, blockIdx.x, false, nullptr);
+}
+
+// The walking fold with the tile scan fused (launch_fold_scan).
+template <int CAP>
+__global__ void __launch_bounds__(1024, 1) k_fold_scan(FoldArgs a, const __grid_constant__ ScanArgs s) {
+    fold_walk_cta<CAP>(a, blockIdx.x, false, &s);
 }
 
 // Many folds in one launch (the batched search): CTA c runs CTA
@@ -789,7 +823,7 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk_jobs(const FoldArgs* __re
         else
             hi = mid - 1;
     }
-    fold_walk_cta<CAP>(jobs[lo], c - cta0[lo], false);
+    fold_walk_cta<CAP>(jobs[lo], c - cta0[lo], false, jobs[lo].scan);
 }
 
 // The same jobs as k_fold_walk_jobs, by a persistent grid (one CTA per SM)
@@ -815,7 +849,7 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk_steal(const FoldArgs* __r
             else
                 hi = mid - 1;
         }
-        if (!fold_walk_cta<CAP>(jobs[lo], u - cta0[lo], reuse)) return;
+        if (!fold_walk_cta<CAP>(jobs[lo], u - cta0[lo], reuse, jobs[lo].scan)) return;
         __syncthreads();  // the unit's shared memory is free before the next one
     }
 }
@@ -838,6 +872,7 @@ std::atomic<uint32_t> g_threads[32];
 std::atomic<uint32_t> g_lockstep[32];
 std::atomic<uint32_t> g_launch_periods{16384};
 std::atomic<uint32_t> g_fold_steal{0};
+std::atomic<uint32_t> g_separate_scan{0};
 
 int nb_class(int nb) { return nb > 0 ? 31 - __builtin_clz((unsigned)nb) : 0; }
 
@@ -924,6 +959,7 @@ void set_fold_tuning(const FoldTuning& t) {
     }
     g_launch_periods.store(t.launch_periods ? t.launch_periods : 16384u, std::memory_order_relaxed);
     g_fold_steal.store(t.steal ? 1u : 0u, std::memory_order_relaxed);
+    g_separate_scan.store(t.separate_scan ? 1u : 0u, std::memory_order_relaxed);
 }
 
 void get_fold_tuning(FoldTuning* t) {
@@ -934,7 +970,10 @@ void get_fold_tuning(FoldTuning* t) {
     }
     t->launch_periods = g_launch_periods.load(std::memory_order_relaxed);
     t->steal = g_fold_steal.load(std::memory_order_relaxed);
+    t->separate_scan = g_separate_scan.load(std::memory_order_relaxed);
 }
+
+bool tuned_separate_scan() { return g_separate_scan.load(std::memory_order_relaxed) != 0; }
 
 bool tuned_fold_steal() { return g_fold_steal.load(std::memory_order_relaxed) != 0; }
 
@@ -994,6 +1033,17 @@ cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, 
     return cudaGetLastError();
 }
 
+// The walking-fold limits on everything but the outputs.
+static bool fold_job_ok_rows(const FoldArgs& a, const FoldShape& shape) {
+    return shape.kind == FOLD_WALK && shape.smem <= MAX_FOLD_SMEM && a.group == shape.group && a.group >= 1 &&
+           a.group <= MAX_GROUP && (a.group & (a.group - 1)) == 0 && walk_threads_ok(shape.threads) &&
+           a.group <= shape.threads / 32 && a.lockstep_min >= 0 && a.nchunks >= 1 && a.nb >= 2 &&
+           a.stage_field == WALK_CAP + 2 && shape.chunk_cap == WALK_CAP && a.row_stride == shape.row_stride &&
+           a.row_stride >= a.nb && a.fault != nullptr && a.time && a.v && a.w && a.scales && a.chunks &&
+           !(reinterpret_cast<uintptr_t>(a.time) & 15) && !(reinterpret_cast<uintptr_t>(a.v) & 15) &&
+           !(reinterpret_cast<uintptr_t>(a.w) & 15);
+}
+
 bool fold_job_ok(const FoldArgs& a, const FoldShape& shape) {
     return shape.kind == FOLD_WALK && shape.smem <= MAX_FOLD_SMEM && a.group == shape.group && a.group >= 1 &&
            a.group <= MAX_GROUP && (a.group & (a.group - 1)) == 0 && walk_threads_ok(shape.threads) &&
@@ -1001,7 +1051,9 @@ bool fold_job_ok(const FoldArgs& a, const FoldShape& shape) {
            a.nb >= 2 && a.stage_field == WALK_CAP + 2 && shape.chunk_cap == WALK_CAP &&
            a.row_stride == shape.row_stride && a.row_stride >= a.nb && a.fault != nullptr &&
            (a.hist_out == nullptr || (a.group == 1 && a.periods == 1 && a.map_out == nullptr)) &&
-           a.time && a.v && a.w && a.scales && a.chunks && (a.map_out || a.hist_out || (a.cum && a.cum32)) &&
+           a.time && a.v && a.w && a.scales && a.chunks &&
+           (a.map_out || a.hist_out || a.scan || (a.cum && a.cum32)) &&
+           (!a.scan || (!a.map_out && !a.hist_out)) &&
            (!a.map_out || (a.map_nd >= 1 && a.map_nd <= MAP_MAX_DURATIONS && a.map_durations && a.map_rho)) &&
            !(reinterpret_cast<uintptr_t>(a.time) & 15) && !(reinterpret_cast<uintptr_t>(a.v) & 15) &&
            !(reinterpret_cast<uintptr_t>(a.w) & 15);
@@ -1025,6 +1077,23 @@ cudaError_t launch_fold_smem_jobs(const FoldArgs* jobs, const int* cta0, int njo
         cudaFuncSetAttribute(k_fold_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
     if (e != cudaSuccess) return e;
     k_fold_jobs<<<ctas, threads, smem, stream>>>(jobs, cta0, njobs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_scan(const FoldArgs& a, const FoldShape& shape, const ScanArgs& s, cudaStream_t stream) {
+    if (shape.kind != FOLD_WALK || a.map_out || a.hist_out || a.scan || !s.parts || !s.keys || !s.flags ||
+        !s.scales || !s.durations || !s.rho || !s.ingress || !s.factors || s.nb != a.nb || s.nd < 1 ||
+        s.nd > MAX_DURATIONS || s.ns < 1 || s.ns > MAX_SHAPES || s.layers < 1 || s.layers > MAX_LAYERS)
+        return cudaErrorInvalidValue;
+    FoldArgs f = a;
+    f.cum = nullptr;
+    f.cum32 = nullptr;
+    if (!fold_job_ok_rows(f, shape)) return cudaErrorInvalidValue;
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_fold_scan<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
+    if (e != cudaSuccess) return e;
+    const int blocks = (a.periods + a.group - 1) / a.group;
+    k_fold_scan<WALK_CAP><<<blocks, shape.threads, shape.smem, stream>>>(f, s);
     return cudaGetLastError();
 }
 

@@ -215,6 +215,25 @@ int plan_passes(fbls_ctx* ctx, std::vector<Pass>& passes) {
     return FBLS_OK;
 }
 
+// A pass whose fold also scans: walking-fold shapes, unless the tuning
+// table asks for the separate scan kernels.
+bool fused_scan(const Pass& p) { return p.shape.kind == FOLD_WALK && !tuned_separate_scan(); }
+
+// Kernel counters of one fold launch of n periods: algorithmic bytes are the
+// observation stream once per period (24 B per observation) plus the prefix
+// rows written and read back (unfused) or the tile parts written (fused).
+void count_fold(fbls_ctx* ctx, int n, uint32_t nobs, uint32_t nb, bool fused) {
+    const double stride = 2.0 * nb + 1.0, tiles = (double)((nb + TILE - 1) / TILE);
+    ctx->counters.fold_updates += (uint64_t)n * nobs;
+    if (fused) {
+        ctx->counters.fold_bytes += (double)n * (24.0 * nobs + 84.0 * tiles);
+        ctx->counters.scan_bytes += (double)n * 84.0 * tiles;
+    } else {
+        ctx->counters.fold_bytes += (double)n * (24.0 * nobs + 48.0 * stride);
+        ctx->counters.scan_bytes += (double)n * (24.0 * stride + 84.0 * tiles);
+    }
+}
+
 // Runs a session of planned passes on ctx->stream: one upload of every
 // pass's inputs from page-locked memory, the fold / scan / merge launches of
 // all passes back to back, one download of all outputs into `down` and a
@@ -232,7 +251,7 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
         launches += p.nlaunch;
         const size_t stride = 2 * (size_t)p.nb + 1;
         const size_t tiles = (p.nb + TILE - 1) / TILE;
-        cum_max = std::max(cum_max, (size_t)p.launch * NF * stride);
+        if (!fused_scan(p)) cum_max = std::max(cum_max, (size_t)p.launch * NF * stride);
         parts_max = std::max(parts_max, (size_t)p.launch * tiles);
         if (!p.shape.hist_in_smem) {
             const size_t blocks = (p.launch + p.shape.group - 1) / p.shape.group;
@@ -241,8 +260,10 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
     }
     CK(ensure(ctx->pass_in, in_total), "workspace");
     CK(ensure(ctx->pass_out, out_total), "workspace");
-    CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
-    CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
+    if (cum_max) {
+        CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
+        CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
+    }
     CK(ensure(ctx->parts, parts_max * PART_STRIDE * sizeof(double)), "workspace");
     CK(ensure(ctx->keys, parts_max * sizeof(uint64_t)), "workspace");
     CK(ensure(ctx->tflags, parts_max * sizeof(uint32_t)), "workspace");
@@ -308,9 +329,6 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
             fa.fault = as<uint32_t>(ctx->fault);
             fa.rows32_only = p.mode == 2 ? 1 : 0;
             fa.lockstep_min = p.shape.lockstep_min;
-            if (timing) CK(cudaEventRecord(ctx->pool[3 * li], s), "event");
-            CK(launch_fold(fa, p.shape, s), "fold");
-            if (timing) CK(cudaEventRecord(ctx->pool[3 * li + 1], s), "event");
             ScanArgs sa{};
             sa.cum = fa.cum;
             sa.cum32 = fa.cum32;
@@ -330,7 +348,19 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
             sa.parts = as<double>(ctx->parts);
             sa.keys = as<uint64_t>(ctx->keys);
             sa.flags = as<uint32_t>(ctx->tflags);
-            CK(launch_scan_tiles(sa, n, s), "scan_tiles");
+            const bool fused = fused_scan(p);
+            if (timing) CK(cudaEventRecord(ctx->pool[3 * li], s), "event");
+            if (fused) {
+                fa.cum = nullptr;
+                fa.cum32 = nullptr;
+                sa.cum = nullptr;
+                sa.cum32 = nullptr;
+                CK(launch_fold_scan(fa, p.shape, sa, s), "fold_scan");
+            } else {
+                CK(launch_fold(fa, p.shape, s), "fold");
+            }
+            if (timing) CK(cudaEventRecord(ctx->pool[3 * li + 1], s), "event");
+            if (!fused) CK(launch_scan_tiles(sa, n, s), "scan_tiles");
             MergeArgs ma{};
             ma.parts = sa.parts;
             ma.keys = sa.keys;
@@ -346,12 +376,10 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
             ma.flags_out = d_flags;
             CK(launch_merge(ma, s), "merge");
             if (timing) CK(cudaEventRecord(ctx->pool[3 * li + 2], s), "event");
-            ctx->counters.launches += 3;
+            ctx->counters.launches += fused ? 2 : 3;
             ctx->counters.fold_launches += 1;
             ctx->counters.scan_launches += 1;
-            ctx->counters.fold_bytes += (double)n * (24.0 * r->n + 48.0 * (double)stride);
-            ctx->counters.fold_updates += (uint64_t)n * r->n;
-            ctx->counters.scan_bytes += (double)n * (24.0 * (double)stride + 84.0 * tiles);
+            count_fold(ctx, n, r->n, nb, fused);
             p.st.templates_scanned += (uint64_t)n * nd * ns * nb;
             p.st.batches += ((uint64_t)n + p.batch - 1) / p.batch;
         }
@@ -413,6 +441,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         int n;
         size_t cum_off, parts_off, hist_off;  // elements within the wave's workspace
         bool walk;
+        bool fused;  // a walking fold that scans its own tiles (no rows in device memory)
     };
     // A wave's walking-fold jobs run as one launch per CTA size: job range
     // [j0, j0 + njobs) with its CTA offsets at fc0 (njobs + 1 entries).
@@ -424,8 +453,9 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         std::vector<Unit> units;
         std::vector<FoldLaunch> folds;
         size_t cum = 0, parts = 0, hist = 0;
-        int fold_jobs = 0, scan_ctas = 0, merge_total = 0;
-        size_t off_fold = 0, off_fcta = 0, off_scan = 0, off_scta = 0, off_merge = 0, off_mp = 0;  // in the job blob
+        int fold_jobs = 0, scan_units = 0, scan_ctas = 0, merge_total = 0;
+        // in the job blob; fold jobs' fused scans at off_fscan, in fold-job order
+        size_t off_fold = 0, off_fcta = 0, off_fscan = 0, off_scan = 0, off_scta = 0, off_merge = 0, off_mp = 0;
     };
     size_t in_total = 0, out_total = 0;
     for (Pass& p : passes) {
@@ -442,14 +472,18 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         const size_t tiles = (p.nb + TILE - 1) / TILE;
         for (uint64_t cursor = 0; cursor < p.P; cursor += p.launch) {
             const int n = (int)std::min<uint64_t>(p.P - cursor, p.launch);
-            const size_t cum = (size_t)n * NF * stride, parts = (size_t)n * tiles;
-            const bool walk = p.shape.kind == FOLD_WALK;
+            const bool walk = p.shape.kind == FOLD_WALK, fused = fused_scan(p);
+            const size_t cum = fused ? 0 : (size_t)n * NF * stride, parts = (size_t)n * tiles;
             const size_t hist = walk ? 0 : ((n + p.shape.group - 1) / p.shape.group) * (size_t)p.shape.group * NF *
                                                (size_t)p.shape.row_stride;
-            if (!waves.back().units.empty() && (waves.back().cum + cum) * (sizeof(double) + sizeof(float2)) > WAVE_BYTES)
+            // A wave's device workspace (prefix rows and tile parts) stays within WAVE_BYTES.
+            auto bytes = [](size_t c, size_t t) {
+                return c * (sizeof(double) + sizeof(float2)) + t * (PART_STRIDE * sizeof(double) + 12);
+            };
+            if (!waves.back().units.empty() && bytes(waves.back().cum + cum, waves.back().parts + parts) > WAVE_BYTES)
                 waves.emplace_back();
             Wave& w = waves.back();
-            w.units.push_back({(int)pi, cursor, n, w.cum, w.parts, w.hist, walk});
+            w.units.push_back({(int)pi, cursor, n, w.cum, w.parts, w.hist, walk, fused});
             w.cum += cum;
             w.parts += parts;
             w.hist += hist;
@@ -466,7 +500,10 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
                 fl->ctas += (n + p.shape.group - 1) / p.shape.group;
                 fl->smem = std::max(fl->smem, p.shape.smem);
             }
-            w.scan_ctas += n * (int)tiles;
+            if (!fused) {
+                w.scan_units++;
+                w.scan_ctas += n * (int)tiles;
+            }
             w.merge_total += n;
             p.st.templates_scanned += (uint64_t)n * p.bank->nd * p.bank->ns * p.nb;
             p.st.batches += ((uint64_t)n + p.batch - 1) / p.batch;
@@ -494,16 +531,19 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             fc0 += f.njobs + 1;
         }
         w.off_fcta = take((w.fold_jobs + w.folds.size() + 1) * sizeof(int));
-        w.off_scan = take(nu * sizeof(ScanArgs));
-        w.off_scta = take((nu + 1) * sizeof(int));
+        w.off_fscan = take(std::max(1, w.fold_jobs) * sizeof(ScanArgs));
+        w.off_scan = take(std::max(1, w.scan_units) * sizeof(ScanArgs));
+        w.off_scta = take((w.scan_units + 1) * sizeof(int));
         w.off_merge = take(nu * sizeof(MergeArgs));
         w.off_mp = take((nu + 1) * sizeof(int));
     }
     const size_t up_total = in_total + blob;
     CK(ensure(ctx->pass_in, up_total), "workspace");
     CK(ensure(ctx->pass_out, out_total), "workspace");
-    CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
-    CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
+    if (cum_max) {
+        CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
+        CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
+    }
     CK(ensure(ctx->parts, parts_max * PART_STRIDE * sizeof(double)), "workspace");
     CK(ensure(ctx->keys, parts_max * sizeof(uint64_t)), "workspace");
     CK(ensure(ctx->tflags, parts_max * sizeof(uint32_t)), "workspace");
@@ -525,11 +565,13 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
     for (Wave& w : waves) {
         FoldArgs* fj = reinterpret_cast<FoldArgs*>(up + in_total + w.off_fold);
         int* fc = reinterpret_cast<int*>(up + in_total + w.off_fcta);
+        ScanArgs* fs = reinterpret_cast<ScanArgs*>(up + in_total + w.off_fscan);
+        const ScanArgs* d_fs = reinterpret_cast<const ScanArgs*>(din + in_total + w.off_fscan);
         ScanArgs* sj = reinterpret_cast<ScanArgs*>(up + in_total + w.off_scan);
         int* sc = reinterpret_cast<int*>(up + in_total + w.off_scta);
         MergeArgs* mj = reinterpret_cast<MergeArgs*>(up + in_total + w.off_merge);
         int* mp = reinterpret_cast<int*>(up + in_total + w.off_mp);
-        int scta = 0, mtot = 0;
+        int scta = 0, mtot = 0, su = 0;
         std::vector<int> nf(w.folds.size(), 0), fcta(w.folds.size(), 0);  // per CTA size: jobs and CTAs so far
         for (size_t u = 0; u < w.units.size(); u++) {
             const Unit& un = w.units[u];
@@ -550,8 +592,8 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             fa.nb = (int)nb;
             fa.periods = un.n;
             fa.group = p.shape.group;
-            fa.cum = as<double>(ctx->cum) + un.cum_off;
-            fa.cum32 = as<float2>(ctx->cum32) + un.cum_off;
+            fa.cum = un.fused ? nullptr : as<double>(ctx->cum) + un.cum_off;
+            fa.cum32 = un.fused ? nullptr : as<float2>(ctx->cum32) + un.cum_off;
             fa.hist_global = un.walk ? nullptr : as<double>(ctx->hist) + un.hist_off;
             fa.hist_out = nullptr;
             fa.chunks = d_chunks;
@@ -562,15 +604,6 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             fa.fault = as<uint32_t>(ctx->fault);
             fa.rows32_only = p.mode == 2 ? 1 : 0;
             fa.lockstep_min = p.shape.lockstep_min;
-            if (un.walk) {
-                if (!fold_job_ok(fa, p.shape)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
-                size_t g = 0;
-                while (w.folds[g].threads != p.shape.threads) g++;
-                const FoldLaunch& fl = w.folds[g];
-                fj[fl.j0 + nf[g]] = fa;
-                fc[fl.fc0 + nf[g]++] = fcta[g];
-                fcta[g] += (un.n + p.shape.group - 1) / p.shape.group;
-            }
             ScanArgs sa{};
             sa.cum = fa.cum;
             sa.cum32 = fa.cum32;
@@ -590,9 +623,25 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             sa.parts = as<double>(ctx->parts) + un.parts_off * PART_STRIDE;
             sa.keys = as<uint64_t>(ctx->keys) + un.parts_off;
             sa.flags = as<uint32_t>(ctx->tflags) + un.parts_off;
-            sj[u] = sa;
-            sc[u] = scta;
-            scta += un.n * tiles;
+            if (un.walk) {
+                size_t g = 0;
+                while (w.folds[g].threads != p.shape.threads) g++;
+                const FoldLaunch& fl = w.folds[g];
+                const int j = fl.j0 + nf[g];
+                if (un.fused) {
+                    fs[j] = sa;
+                    fa.scan = d_fs + j;
+                }
+                if (!fold_job_ok(fa, p.shape)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
+                fj[j] = fa;
+                fc[fl.fc0 + nf[g]++] = fcta[g];
+                fcta[g] += (un.n + p.shape.group - 1) / p.shape.group;
+            }
+            if (!un.fused) {
+                sj[su] = sa;
+                sc[su++] = scta;
+                scta += un.n * tiles;
+            }
             MergeArgs ma{};
             ma.parts = sa.parts;
             ma.keys = sa.keys;
@@ -611,12 +660,10 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             mtot += un.n;
             ctx->counters.fold_launches += 1;
             ctx->counters.scan_launches += 1;
-            ctx->counters.fold_bytes += (double)un.n * (24.0 * r->n + 48.0 * (2.0 * nb + 1.0));
-            ctx->counters.fold_updates += (uint64_t)un.n * r->n;
-            ctx->counters.scan_bytes += (double)un.n * (24.0 * (2.0 * nb + 1.0) + 84.0 * tiles);
+            count_fold(ctx, un.n, r->n, nb, un.fused);
         }
         for (size_t g = 0; g < w.folds.size(); g++) fc[w.folds[g].fc0 + nf[g]] = fcta[g];
-        sc[w.units.size()] = scta;
+        sc[su] = scta;
         mp[w.units.size()] = mtot;
     }
     cudaStream_t s = ctx->stream;
@@ -675,16 +722,19 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             ctx->counters.launches += 1;
         }
         if (timing) CK(cudaEventRecord(ctx->pool[3 * wi + 1], s), "event");
-        CK(launch_scan_jobs(reinterpret_cast<const ScanArgs*>(din + in_total + w.off_scan),
-                            reinterpret_cast<const int*>(din + in_total + w.off_scta), (int)w.units.size(),
-                            w.scan_ctas, s),
-           "scan_tiles");
+        if (w.scan_units) {
+            CK(launch_scan_jobs(reinterpret_cast<const ScanArgs*>(din + in_total + w.off_scan),
+                                reinterpret_cast<const int*>(din + in_total + w.off_scta), w.scan_units, w.scan_ctas,
+                                s),
+               "scan_tiles");
+            ctx->counters.launches += 1;
+        }
         CK(launch_merge_jobs(reinterpret_cast<const MergeArgs*>(din + in_total + w.off_merge),
                              reinterpret_cast<const int*>(din + in_total + w.off_mp), (int)w.units.size(),
                              w.merge_total, s),
            "merge");
         if (timing) CK(cudaEventRecord(ctx->pool[3 * wi + 2], s), "event");
-        ctx->counters.launches += 2;
+        ctx->counters.launches += 1;
     }
     unsigned char* down = static_cast<unsigned char*>(down_buf.ptr);
     CK(cudaMemcpyAsync(down, dout, out_total, cudaMemcpyDeviceToHost, s), "download");

@@ -28,6 +28,8 @@ constexpr int FOLD_WALK = 2;
 // chunk out to whole 16-byte pieces).
 inline size_t fold_field_stride(size_t n) { return (n + 2) & ~(size_t)1; }
 
+struct ScanArgs;
+
 struct FoldArgs {
     const double* time;    // n, relative days, ascending
     const double* v;       // n
@@ -49,6 +51,11 @@ struct FoldArgs {
     uint32_t* fault;       // FOLD_WALK: set nonzero when a staging wait gives up
     int rows32_only;       // FOLD_WALK: write only the (hi, lo) f32 rows (the f32 form reads no f64 rows)
     int lockstep_min;      // FOLD_WALK: segments at least this long are walked in lockstep (0: the built-in 11)
+    // Fused tile scan (FOLD_WALK job launches): when set (device memory),
+    // the prefix rows stay in shared memory (cum / cum32 unused) and the
+    // CTA scans its periods' tiles itself, writing the scan's parts, keys
+    // and flags as k_scan_tiles does.
+    const ScanArgs* scan;
     // Coarse-map epilogue (FOLD_WALK only): when map_out is set, the prefix
     // rows stay in shared memory (cum / cum32 unused) and each period's best
     // box score per map duration, as k_box_map computes it, goes to
@@ -86,6 +93,7 @@ struct FoldTuning {
     uint32_t lockstep_min[32];
     uint32_t launch_periods;
     uint32_t steal;
+    uint32_t separate_scan;  // nonzero: fold and tile scan as separate kernels (else fused)
 };
 
 struct ScanArgs {
@@ -214,6 +222,7 @@ FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned = false
 void set_fold_tuning(const FoldTuning& t);
 void get_fold_tuning(FoldTuning* t);
 uint32_t tuned_launch_periods();
+bool tuned_separate_scan();
 bool tuned_fold_steal();
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
 // spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.
@@ -221,6 +230,12 @@ bool tuned_fold_steal();
 int fold_chunks(const double* time, int n, double scale_max, int nb, int span_cap, int chunk_cap, int* out,
                 int capacity);
 cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream);
+// The walking fold with the tile scan fused (FOLD_WALK shapes, no map or
+// histogram output): the prefix rows stay in shared memory and every CTA
+// scans its periods' tiles with groups of TILE threads, writing s.parts,
+// s.keys and s.flags (s.cum, s.cum32 unused). The same records as
+// launch_fold + launch_scan_tiles.
+cudaError_t launch_fold_scan(const FoldArgs& a, const FoldShape& shape, const ScanArgs& s, cudaStream_t stream);
 // Job launches (the batched search): jobs and their first CTA / period
 // offsets (njobs + 1 entries, the last = total) live in device memory.
 // A walking-fold job within limits. A job may write one period's raw

@@ -125,6 +125,7 @@ extern "C" int fbls_set_tuning(const fbls_tuning* tuning) {
     }
     t.launch_periods = tuning->launch_periods;
     t.steal = tuning->fold_steal;
+    t.separate_scan = tuning->separate_scan;
     set_fold_tuning(t);
     return FBLS_OK;
 }
@@ -140,5 +141,6 @@ extern "C" int fbls_get_tuning(fbls_tuning* tuning) {
     }
     tuning->launch_periods = t.launch_periods;
     tuning->fold_steal = t.steal;
+    tuning->separate_scan = t.separate_scan;
     return FBLS_OK;
 }

@@ -258,7 +258,10 @@ int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
  * fold's CTA size (128, 256, 512 or 1024; 0 = 1024; the period group is cut
  * to at most one period per warp), and lockstep_min, the segment length from
  * which a CTA's lanes walk their observations in lockstep rather than each
- * its own window (0 = 11; at most 4096).
+ * its own window (0 = 11; at most 4096). separate_scan: nonzero runs the
+ * tile scan as its own kernel over prefix rows the fold writes to device
+ * memory, instead of in the walking fold's CTAs from the rows they keep in
+ * shared memory (the default).
  * Process-wide; results do not depend on it, only the launch shapes do. */
 typedef struct {
     uint32_t fold_group_max[32];
@@ -266,6 +269,7 @@ typedef struct {
     uint32_t fold_steal;
     uint32_t fold_threads[32];
     uint32_t lockstep_min[32];
+    uint32_t separate_scan;
 } fbls_tuning;
 int fbls_set_tuning(const fbls_tuning* tuning);
 int fbls_get_tuning(fbls_tuning* tuning);

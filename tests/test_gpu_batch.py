@@ -165,3 +165,47 @@ def test_fold_cta_size_and_lockstep_give_the_same_rows(gpu, threads, lockstep):
         assert np.array_equal(got_one[0], want_one[0]) and got_one[1] == want_one[1]
     finally:
         autotune.apply(saved)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_fused_tile_scan_equals_the_separate_kernels(gpu, mode):
+    # The walking fold scanning its own tiles from the prefix rows it keeps
+    # in shared memory (the default) against the fold writing the rows to
+    # device memory and k_scan_tiles reading them back: the same records,
+    # scores, depths and flags bit for bit, in each precision mode, for a
+    # multi-band star (nb from 96 to 1,920, several period groups per CTA)
+    # and a batch of survey stars (the job launches).
+    import dataclasses
+    from fbls_b200 import autotune
+    one = synth.single_sector()
+    cfg = dataclasses.replace(synth.single_sector_config(), precision_mode=mode)
+    st = api.prepared_family(one.time, one.flux, one.flux_err, cfg)
+    grid, bands = api.band_plan(st, cfg)
+    rng = np.random.default_rng(41)
+    stars = []
+    for _ in range(8):
+        c = synth.survey_star(rng)
+        sc = synth.survey_config(c)
+        stars.append((api.prepared_family(c.time, c.flux, c.flux_err, sc), sc.period_max))
+    base = dataclasses.replace(synth.survey_config(synth.survey_star(np.random.default_rng(0))), precision_mode=mode)
+    saved = autotune.current()
+    out = {}
+    try:
+        dev = gpu.upload(st)
+        for sep in (1, 0):
+            autotune.apply({**saved, "separate_scan": sep})
+            banks = [gpu.scan_bank(dev, b["periods"][:3000], api.bank_for(b, cfg), nb, precision_mode=mode)
+                     for b in bands for nb in (b["nb"] // 2, b["nb"])]
+            rows = gpu.signal_search(st, cfg, dev=dev)
+            batch = gpu.search_batch([s for s, _ in stars], base, period_max=[p for _, p in stars], workers=0)
+            out[sep] = (banks, rows, batch)
+        dev.free()
+    finally:
+        autotune.apply(saved)
+    (b1, r1, s1), (b0, r0, s0) = out[1], out[0]
+    for x, y in zip(b1, b0):
+        for u, v in zip(x[:4], y[:4]):
+            assert np.array_equal(u, v, equal_nan=True)
+    assert np.array_equal(r1[0], r0[0]) and r1[1] == r0[1]
+    for (x, gx, tx), (y, gy, ty) in zip(s1, s0):
+        assert np.array_equal(x, y) and gx == gy and tx == ty
