@@ -471,14 +471,19 @@ __device__ __noinline__ void fold_map_epilogue(float* map_out, const double* map
 }
 
 
-// The fused tile scan of a walking-fold CTA (after the in-place prefix rows
-// and a barrier), out of line like the map epilogue, so the fold's loop keeps
-// its registers: groups of TILE threads take the (period, tile) units of the
-// CTA's periods in turn and scan them from the in-place rows, each group with
-// its own scratch.
-__device__ __noinline__ void fold_scan_epilogue(const ScanArgs& scan, const double2* hvw, const uint32_t* hc,
-                                                const double* row_final, const double* s_scale, TileScratch* scratch,
-                                                int nb, int rs, int g, int g0) {
+// Shared memory of the fused scan's tile winners: PART_STRIDE doubles, the
+// key and the flags (in a double's slot) per (period, tile) of the CTA.
+constexpr int FUSED_PART_DOUBLES = PART_STRIDE + 2;
+
+// The fused tile scan and merge of a walking-fold CTA (after the in-place
+// prefix rows and a barrier), out of line like the map epilogue, so the
+// fold's loop keeps its registers: groups of TILE threads take the (period,
+// tile) units of the CTA's periods in turn and scan them from the in-place
+// rows, each group with its own scratch, into `parts`; then one thread per
+// period merges its tiles into the records.
+__device__ __noinline__ void fold_scan_epilogue(const ScanArgs& scan, const MergeArgs& merge, const double2* hvw,
+                                                const uint32_t* hc, const double* row_final, const double* s_scale,
+                                                TileScratch* scratch, double* parts, int nb, int rs, int g, int g0) {
     const int tiles = (nb + TILE - 1) / TILE;
     const int ngroups = (int)blockDim.x / TILE;
     const int gi = (int)threadIdx.x / TILE;
@@ -490,8 +495,32 @@ __device__ __noinline__ void fold_scan_epilogue(const ScanArgs& scan, const doub
         rows.c = hc + (size_t)qq * rs;
         rows.fin = row_final + qq * NF;
         rows.nb = (uint32_t)nb;
+        double* slot = parts + (size_t)u * FUSED_PART_DOUBLES;
         grp.sync();  // the group's scratch is free: its previous unit is done with it
-        scan_tile(scan, rows, grp, scratch[gi], t, g0 + qq, tiles, s_scale[qq]);
+        scan_tile(scan, rows, grp, scratch[gi], t, s_scale[qq], slot, reinterpret_cast<uint64_t*>(slot + PART_STRIDE),
+                  reinterpret_cast<uint32_t*>(slot + PART_STRIDE + 1));
+    }
+    __syncthreads();
+    for (int qq = (int)threadIdx.x; qq < g; qq += (int)blockDim.x) {
+        // The unit of tile t of period qq is qq * tiles + t: its tiles' slots
+        // follow one another at FUSED_PART_DOUBLES doubles.
+        const double* p0 = parts + (size_t)qq * tiles * FUSED_PART_DOUBLES;
+        double best = neg_inf();
+        uint64_t key = KEY_MAX;
+        int chosen = 0;
+        uint32_t fl = 0;
+        for (int t = 0; t < tiles; t++) {
+            const double* sl = p0 + (size_t)t * FUSED_PART_DOUBLES;
+            const double v = sl[7];
+            const uint64_t k = *reinterpret_cast<const uint64_t*>(sl + PART_STRIDE);
+            fl |= *reinterpret_cast<const uint32_t*>(sl + PART_STRIDE + 1);
+            if (v > best || (v == best && k < key)) {
+                best = v;
+                key = k;
+                chosen = t;
+            }
+        }
+        merge_record(merge, g0 + qq, p0 + (size_t)chosen * FUSED_PART_DOUBLES, best, fl);
     }
 }
 
@@ -501,7 +530,7 @@ __device__ __noinline__ void fold_scan_epilogue(const ScanArgs& scan, const doub
 // ones. Returns false (uniformly over the CTA) when a staging wait gave up.
 template <int CAP>
 __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, const bool reuse,
-                                              const ScanArgs* scan) {
+                                              const ScanArgs* scan, const MergeArgs* merge) {
     constexpr int F = CAP + 2;  // doubles per staged field
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ double s_scale[MAX_GROUP];
@@ -738,9 +767,11 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
     double* row_final = stage;  // rows: each row's final carry (map epilogue, fused scan)
     // The tail of the staging buffers is kept for the epilogue: the map's
     // per-warp partial maxima, or the fused scan's per-group scratch.
+    // Fused scan: the groups' scratch, below it the tile winners.
     const int ngroups = T / TILE;
     const int scratch_doubles = scan ? ngroups * (int)((sizeof(TileScratch) + 7) / 8) : W;
-    if (2 * ((items + W - 1) / W) < ((rows + W - 1) / W) * S && 2 * items + rows + scratch_doubles <= 6 * F) {
+    const int reserve = scratch_doubles + (scan ? G * ((nb + TILE - 1) / TILE) * FUSED_PART_DOUBLES : 0);
+    if (2 * ((items + W - 1) / W) < ((rows + W - 1) / W) * S && 2 * items + rows + reserve <= 6 * F) {
         double* seg_total = stage;             // rows x S (the staging buffers are idle now)
         double* seg_carry = stage + items;     // rows x S
         row_final = stage + 2 * items;         // rows
@@ -787,8 +818,9 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
 
     __syncthreads();
     if (scan) {
-        fold_scan_epilogue(*scan, hvw, hc, row_final, s_scale,
-                           reinterpret_cast<TileScratch*>(stage + 6 * F - scratch_doubles), nb, rs, g, g0);
+        fold_scan_epilogue(*scan, *merge, hvw, hc, row_final, s_scale,
+                           reinterpret_cast<TileScratch*>(stage + 6 * F - scratch_doubles),
+                           stage + 6 * F - reserve, nb, rs, g, g0);
         return true;
     }
     fold_map_epilogue(a.map_out, a.map_durations, a.map_rho, a.map_nd, a.map_baseline, a.n, hvw, hc, s_scale,
@@ -798,13 +830,14 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
 
 template <int CAP>
 __global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
-    fold_walk_cta<CAP>(a, blockIdx.x, false, nullptr);
+    fold_walk_cta<CAP>(a, blockIdx.x, false, nullptr, nullptr);
 }
 
-// The walking fold with the tile scan fused (launch_fold_scan).
+// The walking fold with the tile scan and merge fused (launch_fold_scan).
 template <int CAP>
-__global__ void __launch_bounds__(1024, 1) k_fold_scan(FoldArgs a, const __grid_constant__ ScanArgs s) {
-    fold_walk_cta<CAP>(a, blockIdx.x, false, &s);
+__global__ void __launch_bounds__(1024, 1) k_fold_scan(FoldArgs a, const __grid_constant__ ScanArgs s,
+                                                       const __grid_constant__ MergeArgs m) {
+    fold_walk_cta<CAP>(a, blockIdx.x, false, &s, &m);
 }
 
 // Many folds in one launch (the batched search): CTA c runs CTA
@@ -823,7 +856,7 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk_jobs(const FoldArgs* __re
         else
             hi = mid - 1;
     }
-    fold_walk_cta<CAP>(jobs[lo], c - cta0[lo], false, jobs[lo].scan);
+    fold_walk_cta<CAP>(jobs[lo], c - cta0[lo], false, jobs[lo].scan, jobs[lo].merge);
 }
 
 // The same jobs as k_fold_walk_jobs, by a persistent grid (one CTA per SM)
@@ -849,7 +882,7 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk_steal(const FoldArgs* __r
             else
                 hi = mid - 1;
         }
-        if (!fold_walk_cta<CAP>(jobs[lo], u - cta0[lo], reuse, jobs[lo].scan)) return;
+        if (!fold_walk_cta<CAP>(jobs[lo], u - cta0[lo], reuse, jobs[lo].scan, jobs[lo].merge)) return;
         __syncthreads();  // the unit's shared memory is free before the next one
     }
 }
@@ -1052,7 +1085,7 @@ bool fold_job_ok(const FoldArgs& a, const FoldShape& shape) {
            a.row_stride == shape.row_stride && a.row_stride >= a.nb && a.fault != nullptr &&
            (a.hist_out == nullptr || (a.group == 1 && a.periods == 1 && a.map_out == nullptr)) &&
            a.time && a.v && a.w && a.scales && a.chunks &&
-           (a.map_out || a.hist_out || a.scan || (a.cum && a.cum32)) &&
+           (a.map_out || a.hist_out || a.scan || (a.cum && a.cum32)) && (!a.scan == !a.merge) &&
            (!a.scan || (!a.map_out && !a.hist_out)) &&
            (!a.map_out || (a.map_nd >= 1 && a.map_nd <= MAP_MAX_DURATIONS && a.map_durations && a.map_rho)) &&
            !(reinterpret_cast<uintptr_t>(a.time) & 15) && !(reinterpret_cast<uintptr_t>(a.v) & 15) &&
@@ -1080,11 +1113,16 @@ cudaError_t launch_fold_smem_jobs(const FoldArgs* jobs, const int* cta0, int njo
     return cudaGetLastError();
 }
 
-cudaError_t launch_fold_scan(const FoldArgs& a, const FoldShape& shape, const ScanArgs& s, cudaStream_t stream) {
-    if (shape.kind != FOLD_WALK || a.map_out || a.hist_out || a.scan || !s.parts || !s.keys || !s.flags ||
-        !s.scales || !s.durations || !s.rho || !s.ingress || !s.factors || s.nb != a.nb || s.nd < 1 ||
-        s.nd > MAX_DURATIONS || s.ns < 1 || s.ns > MAX_SHAPES || s.layers < 1 || s.layers > MAX_LAYERS)
-        return cudaErrorInvalidValue;
+bool fused_scan_ok(const FoldArgs& a, const ScanArgs& s, const MergeArgs& m) {
+    return !a.map_out && !a.hist_out && s.scales && s.durations && s.rho && s.ingress && s.factors &&
+           s.nb == a.nb && s.nd >= 1 && s.nd <= MAX_DURATIONS && s.ns >= 1 && s.ns <= MAX_SHAPES && s.layers >= 1 &&
+           s.layers <= MAX_LAYERS && m.periods_in && m.scales && m.records && m.score && m.depth && m.flags_out &&
+           m.periods == a.periods && m.offset >= 0;
+}
+
+cudaError_t launch_fold_scan(const FoldArgs& a, const FoldShape& shape, const ScanArgs& s, const MergeArgs& m,
+                             cudaStream_t stream) {
+    if (shape.kind != FOLD_WALK || a.scan || a.merge || !fused_scan_ok(a, s, m)) return cudaErrorInvalidValue;
     FoldArgs f = a;
     f.cum = nullptr;
     f.cum32 = nullptr;
@@ -1093,7 +1131,7 @@ cudaError_t launch_fold_scan(const FoldArgs& a, const FoldShape& shape, const Sc
         cudaFuncSetAttribute(k_fold_scan<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
     if (e != cudaSuccess) return e;
     const int blocks = (a.periods + a.group - 1) / a.group;
-    k_fold_scan<WALK_CAP><<<blocks, shape.threads, shape.smem, stream>>>(f, s);
+    k_fold_scan<WALK_CAP><<<blocks, shape.threads, shape.smem, stream>>>(f, s, m);
     return cudaGetLastError();
 }
 

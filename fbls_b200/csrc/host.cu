@@ -251,8 +251,10 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
         launches += p.nlaunch;
         const size_t stride = 2 * (size_t)p.nb + 1;
         const size_t tiles = (p.nb + TILE - 1) / TILE;
-        if (!fused_scan(p)) cum_max = std::max(cum_max, (size_t)p.launch * NF * stride);
-        parts_max = std::max(parts_max, (size_t)p.launch * tiles);
+        if (!fused_scan(p)) {  // a fused pass keeps its rows and tile winners in shared memory
+            cum_max = std::max(cum_max, (size_t)p.launch * NF * stride);
+            parts_max = std::max(parts_max, (size_t)p.launch * tiles);
+        }
         if (!p.shape.hist_in_smem) {
             const size_t blocks = (p.launch + p.shape.group - 1) / p.shape.group;
             hist_max = std::max(hist_max, blocks * p.shape.group * NF * (size_t)p.shape.row_stride);
@@ -264,9 +266,11 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
         CK(ensure(ctx->cum, cum_max * sizeof(double)), "workspace");
         CK(ensure(ctx->cum32, cum_max * sizeof(float2)), "workspace");
     }
-    CK(ensure(ctx->parts, parts_max * PART_STRIDE * sizeof(double)), "workspace");
-    CK(ensure(ctx->keys, parts_max * sizeof(uint64_t)), "workspace");
-    CK(ensure(ctx->tflags, parts_max * sizeof(uint32_t)), "workspace");
+    if (parts_max) {
+        CK(ensure(ctx->parts, parts_max * PART_STRIDE * sizeof(double)), "workspace");
+        CK(ensure(ctx->keys, parts_max * sizeof(uint64_t)), "workspace");
+        CK(ensure(ctx->tflags, parts_max * sizeof(uint32_t)), "workspace");
+    }
     if (hist_max) CK(ensure(ctx->hist, hist_max * sizeof(double)), "workspace");
     CK(ensure(ctx->fault, sizeof(uint32_t)), "workspace");
     CK(ensure_pinned(ctx->pin_up, in_total), "pinned workspace");
@@ -348,19 +352,6 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
             sa.parts = as<double>(ctx->parts);
             sa.keys = as<uint64_t>(ctx->keys);
             sa.flags = as<uint32_t>(ctx->tflags);
-            const bool fused = fused_scan(p);
-            if (timing) CK(cudaEventRecord(ctx->pool[3 * li], s), "event");
-            if (fused) {
-                fa.cum = nullptr;
-                fa.cum32 = nullptr;
-                sa.cum = nullptr;
-                sa.cum32 = nullptr;
-                CK(launch_fold_scan(fa, p.shape, sa, s), "fold_scan");
-            } else {
-                CK(launch_fold(fa, p.shape, s), "fold");
-            }
-            if (timing) CK(cudaEventRecord(ctx->pool[3 * li + 1], s), "event");
-            if (!fused) CK(launch_scan_tiles(sa, n, s), "scan_tiles");
             MergeArgs ma{};
             ma.parts = sa.parts;
             ma.keys = sa.keys;
@@ -374,9 +365,22 @@ int run_session(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf) {
             ma.score = d_score;
             ma.depth = d_depth;
             ma.flags_out = d_flags;
-            CK(launch_merge(ma, s), "merge");
+            const bool fused = fused_scan(p);
+            if (timing) CK(cudaEventRecord(ctx->pool[3 * li], s), "event");
+            if (fused) {
+                fa.cum = nullptr;
+                fa.cum32 = nullptr;
+                CK(launch_fold_scan(fa, p.shape, sa, ma, s), "fold_scan");
+            } else {
+                CK(launch_fold(fa, p.shape, s), "fold");
+            }
+            if (timing) CK(cudaEventRecord(ctx->pool[3 * li + 1], s), "event");
+            if (!fused) {
+                CK(launch_scan_tiles(sa, n, s), "scan_tiles");
+                CK(launch_merge(ma, s), "merge");
+            }
             if (timing) CK(cudaEventRecord(ctx->pool[3 * li + 2], s), "event");
-            ctx->counters.launches += fused ? 2 : 3;
+            ctx->counters.launches += fused ? 1 : 3;
             ctx->counters.fold_launches += 1;
             ctx->counters.scan_launches += 1;
             count_fold(ctx, n, r->n, nb, fused);
@@ -454,8 +458,11 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         std::vector<FoldLaunch> folds;
         size_t cum = 0, parts = 0, hist = 0;
         int fold_jobs = 0, scan_units = 0, scan_ctas = 0, merge_total = 0;
-        // in the job blob; fold jobs' fused scans at off_fscan, in fold-job order
-        size_t off_fold = 0, off_fcta = 0, off_fscan = 0, off_scan = 0, off_scta = 0, off_merge = 0, off_mp = 0;
+        // in the job blob; the fold jobs' fused scans and merges at off_fscan
+        // and off_fmerge, in fold-job order; the other units' scans and
+        // merges at off_scan and off_merge
+        size_t off_fold = 0, off_fcta = 0, off_fscan = 0, off_fmerge = 0, off_scan = 0, off_scta = 0, off_merge = 0,
+               off_mp = 0;
     };
     size_t in_total = 0, out_total = 0;
     for (Pass& p : passes) {
@@ -473,7 +480,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         for (uint64_t cursor = 0; cursor < p.P; cursor += p.launch) {
             const int n = (int)std::min<uint64_t>(p.P - cursor, p.launch);
             const bool walk = p.shape.kind == FOLD_WALK, fused = fused_scan(p);
-            const size_t cum = fused ? 0 : (size_t)n * NF * stride, parts = (size_t)n * tiles;
+            const size_t cum = fused ? 0 : (size_t)n * NF * stride, parts = fused ? 0 : (size_t)n * tiles;
             const size_t hist = walk ? 0 : ((n + p.shape.group - 1) / p.shape.group) * (size_t)p.shape.group * NF *
                                                (size_t)p.shape.row_stride;
             // A wave's device workspace (prefix rows and tile parts) stays within WAVE_BYTES.
@@ -503,8 +510,8 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             if (!fused) {
                 w.scan_units++;
                 w.scan_ctas += n * (int)tiles;
+                w.merge_total += n;
             }
-            w.merge_total += n;
             p.st.templates_scanned += (uint64_t)n * p.bank->nd * p.bank->ns * p.nb;
             p.st.batches += ((uint64_t)n + p.batch - 1) / p.batch;
         }
@@ -532,10 +539,11 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         }
         w.off_fcta = take((w.fold_jobs + w.folds.size() + 1) * sizeof(int));
         w.off_fscan = take(std::max(1, w.fold_jobs) * sizeof(ScanArgs));
+        w.off_fmerge = take(std::max(1, w.fold_jobs) * sizeof(MergeArgs));
         w.off_scan = take(std::max(1, w.scan_units) * sizeof(ScanArgs));
         w.off_scta = take((w.scan_units + 1) * sizeof(int));
-        w.off_merge = take(nu * sizeof(MergeArgs));
-        w.off_mp = take((nu + 1) * sizeof(int));
+        w.off_merge = take(std::max(1, w.scan_units) * sizeof(MergeArgs));
+        w.off_mp = take((w.scan_units + 1) * sizeof(int));
     }
     const size_t up_total = in_total + blob;
     CK(ensure(ctx->pass_in, up_total), "workspace");
@@ -567,6 +575,8 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         int* fc = reinterpret_cast<int*>(up + in_total + w.off_fcta);
         ScanArgs* fs = reinterpret_cast<ScanArgs*>(up + in_total + w.off_fscan);
         const ScanArgs* d_fs = reinterpret_cast<const ScanArgs*>(din + in_total + w.off_fscan);
+        MergeArgs* fm = reinterpret_cast<MergeArgs*>(up + in_total + w.off_fmerge);
+        const MergeArgs* d_fm = reinterpret_cast<const MergeArgs*>(din + in_total + w.off_fmerge);
         ScanArgs* sj = reinterpret_cast<ScanArgs*>(up + in_total + w.off_scan);
         int* sc = reinterpret_cast<int*>(up + in_total + w.off_scta);
         MergeArgs* mj = reinterpret_cast<MergeArgs*>(up + in_total + w.off_merge);
@@ -623,25 +633,6 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             sa.parts = as<double>(ctx->parts) + un.parts_off * PART_STRIDE;
             sa.keys = as<uint64_t>(ctx->keys) + un.parts_off;
             sa.flags = as<uint32_t>(ctx->tflags) + un.parts_off;
-            if (un.walk) {
-                size_t g = 0;
-                while (w.folds[g].threads != p.shape.threads) g++;
-                const FoldLaunch& fl = w.folds[g];
-                const int j = fl.j0 + nf[g];
-                if (un.fused) {
-                    fs[j] = sa;
-                    fa.scan = d_fs + j;
-                }
-                if (!fold_job_ok(fa, p.shape)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
-                fj[j] = fa;
-                fc[fl.fc0 + nf[g]++] = fcta[g];
-                fcta[g] += (un.n + p.shape.group - 1) / p.shape.group;
-            }
-            if (!un.fused) {
-                sj[su] = sa;
-                sc[su++] = scta;
-                scta += un.n * tiles;
-            }
             MergeArgs ma{};
             ma.parts = sa.parts;
             ma.keys = sa.keys;
@@ -655,16 +646,38 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             ma.score = reinterpret_cast<double*>(dout + p.out_off + p.out_score);
             ma.depth = reinterpret_cast<double*>(dout + p.out_off + p.out_depth);
             ma.flags_out = reinterpret_cast<uint32_t*>(dout + p.out_off + p.out_flags);
-            mj[u] = ma;
-            mp[u] = mtot;
-            mtot += un.n;
+            if (un.walk) {
+                size_t g = 0;
+                while (w.folds[g].threads != p.shape.threads) g++;
+                const FoldLaunch& fl = w.folds[g];
+                const int j = fl.j0 + nf[g];
+                if (un.fused) {
+                    if (!fused_scan_ok(fa, sa, ma)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
+                    fs[j] = sa;
+                    fm[j] = ma;
+                    fa.scan = d_fs + j;
+                    fa.merge = d_fm + j;
+                }
+                if (!fold_job_ok(fa, p.shape)) return fail(ctx, FBLS_ERR_ARGUMENT, "fold job outside limits");
+                fj[j] = fa;
+                fc[fl.fc0 + nf[g]++] = fcta[g];
+                fcta[g] += (un.n + p.shape.group - 1) / p.shape.group;
+            }
+            if (!un.fused) {
+                sj[su] = sa;
+                mj[su] = ma;
+                mp[su] = mtot;
+                mtot += un.n;
+                sc[su++] = scta;
+                scta += un.n * tiles;
+            }
             ctx->counters.fold_launches += 1;
             ctx->counters.scan_launches += 1;
             count_fold(ctx, un.n, r->n, nb, un.fused);
         }
         for (size_t g = 0; g < w.folds.size(); g++) fc[w.folds[g].fc0 + nf[g]] = fcta[g];
         sc[su] = scta;
-        mp[w.units.size()] = mtot;
+        mp[su] = mtot;
     }
     cudaStream_t s = ctx->stream;
     const bool timing = ctx->profile || ctx->kernel_timing;
@@ -729,12 +742,14 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
                "scan_tiles");
             ctx->counters.launches += 1;
         }
-        CK(launch_merge_jobs(reinterpret_cast<const MergeArgs*>(din + in_total + w.off_merge),
-                             reinterpret_cast<const int*>(din + in_total + w.off_mp), (int)w.units.size(),
-                             w.merge_total, s),
-           "merge");
+        if (w.scan_units) {
+            CK(launch_merge_jobs(reinterpret_cast<const MergeArgs*>(din + in_total + w.off_merge),
+                                 reinterpret_cast<const int*>(din + in_total + w.off_mp), w.scan_units, w.merge_total,
+                                 s),
+               "merge");
+            ctx->counters.launches += 1;
+        }
         if (timing) CK(cudaEventRecord(ctx->pool[3 * wi + 2], s), "event");
-        ctx->counters.launches += 1;
     }
     unsigned char* down = static_cast<unsigned char*>(down_buf.ptr);
     CK(cudaMemcpyAsync(down, dout, out_total, cudaMemcpyDeviceToHost, s), "download");

@@ -29,6 +29,7 @@ constexpr int FOLD_WALK = 2;
 inline size_t fold_field_stride(size_t n) { return (n + 2) & ~(size_t)1; }
 
 struct ScanArgs;
+struct MergeArgs;
 
 struct FoldArgs {
     const double* time;    // n, relative days, ascending
@@ -51,11 +52,13 @@ struct FoldArgs {
     uint32_t* fault;       // FOLD_WALK: set nonzero when a staging wait gives up
     int rows32_only;       // FOLD_WALK: write only the (hi, lo) f32 rows (the f32 form reads no f64 rows)
     int lockstep_min;      // FOLD_WALK: segments at least this long are walked in lockstep (0: the built-in 11)
-    // Fused tile scan (FOLD_WALK job launches): when set (device memory),
-    // the prefix rows stay in shared memory (cum / cum32 unused) and the
-    // CTA scans its periods' tiles itself, writing the scan's parts, keys
-    // and flags as k_scan_tiles does.
+    // Fused tile scan and merge (FOLD_WALK job launches): when set (device
+    // memory, both), the prefix rows stay in shared memory (cum / cum32
+    // unused), the CTA scans its periods' tiles into shared memory and
+    // merges them into the records as k_merge does (the scan's parts, keys
+    // and flags unused).
     const ScanArgs* scan;
+    const MergeArgs* merge;
     // Coarse-map epilogue (FOLD_WALK only): when map_out is set, the prefix
     // rows stay in shared memory (cum / cum32 unused) and each period's best
     // box score per map duration, as k_box_map computes it, goes to
@@ -230,17 +233,21 @@ bool tuned_fold_steal();
 int fold_chunks(const double* time, int n, double scale_max, int nb, int span_cap, int chunk_cap, int* out,
                 int capacity);
 cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream);
-// The walking fold with the tile scan fused (FOLD_WALK shapes, no map or
-// histogram output): the prefix rows stay in shared memory and every CTA
-// scans its periods' tiles with groups of TILE threads, writing s.parts,
-// s.keys and s.flags (s.cum, s.cum32 unused). The same records as
-// launch_fold + launch_scan_tiles.
-cudaError_t launch_fold_scan(const FoldArgs& a, const FoldShape& shape, const ScanArgs& s, cudaStream_t stream);
+// The walking fold with the tile scan and merge fused (FOLD_WALK shapes, no
+// map or histogram output): the prefix rows stay in shared memory, every CTA
+// scans its periods' tiles with groups of TILE threads into shared memory
+// and merges them into m's records (s.cum, s.cum32, s.parts, s.keys,
+// s.flags and m.parts, m.keys, m.flags unused). The same records as
+// launch_fold + launch_scan_tiles + launch_merge.
+cudaError_t launch_fold_scan(const FoldArgs& a, const FoldShape& shape, const ScanArgs& s, const MergeArgs& m,
+                             cudaStream_t stream);
 // Job launches (the batched search): jobs and their first CTA / period
 // offsets (njobs + 1 entries, the last = total) live in device memory.
 // A walking-fold job within limits. A job may write one period's raw
 // histogram (hist_out, group 1) instead of prefix rows.
 bool fold_job_ok(const FoldArgs& a, const FoldShape& shape);
+// The scan and merge of a fused walking-fold job within limits.
+bool fused_scan_ok(const FoldArgs& a, const ScanArgs& s, const MergeArgs& m);
 // A staged-by-threads (FOLD_SMEM) fold job within limits, and the launch of
 // many of them with one CTA size.
 bool fold_smem_job_ok(const FoldArgs& a, const FoldShape& shape);

@@ -23,7 +23,8 @@ __device__ __forceinline__ void scan_tile_cta(const ScanArgs& a, const int tile,
     rows.stride = 2 * (size_t)a.nb + 1;
     rows.r64 = a.cum ? a.cum + (size_t)f * NF * rows.stride : nullptr;
     rows.r32 = a.cum32 + (size_t)f * NF * rows.stride;
-    scan_tile(a, rows, CtaGroup{}, sc, tile, f, tiles, a.scales[f]);
+    const size_t idx = (size_t)f * tiles + tile;
+    scan_tile(a, rows, CtaGroup{}, sc, tile, a.scales[f], a.parts + idx * PART_STRIDE, a.keys + idx, a.flags + idx);
 }
 
 // Eight CTAs per SM (64 registers): the f32 pass keeps its state in registers;
@@ -54,30 +55,8 @@ __global__ void __launch_bounds__(TILE, 8) k_scan_jobs(const ScanArgs* __restric
 // Best tile per period by (score, lowest key) (kernels.rs:1115-1155). Writes
 // records at `offset` so one buffer collects a whole band; flags are ORed.
 __device__ __forceinline__ void merge_period(const MergeArgs& a, const int f) {
-    double best = neg_inf();
-    uint64_t key = KEY_MAX;
-    int chosen = 0;
-    uint32_t fl = 0;
-    for (int t = 0; t < a.tiles; t++) {
-        const size_t idx = (size_t)f * a.tiles + t;
-        double v = a.parts[idx * PART_STRIDE + 7];
-        uint64_t k = a.keys[idx];
-        fl |= a.flags[idx];
-        if (v > best || (v == best && k < key)) {
-            best = v;
-            key = k;
-            chosen = t;
-        }
-    }
-    const double* part = a.parts + ((size_t)f * a.tiles + chosen) * PART_STRIDE;
-    const size_t g = (size_t)a.offset + f;
-    double* rec = a.records + g * RECORD_STRIDE;
-    rec[0] = a.periods_in[f];
-    rec[1] = a.scales[f];
-    for (int i = 0; i < 7; i++) rec[2 + i] = part[i];
-    a.score[g] = best;
-    a.depth[g] = part[8];
-    a.flags_out[g] = fl;
+    const size_t idx = (size_t)f * a.tiles;
+    merge_tiles(a.parts + idx * PART_STRIDE, a.keys + idx, a.flags + idx, a.tiles, a, f);
 }
 
 // ---------------------------------------------------------------------------

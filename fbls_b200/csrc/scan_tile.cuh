@@ -232,13 +232,15 @@ __device__ __forceinline__ void shape_sums32(const Rows& rows, uint32_t j, uint3
     }
 }
 
-// Tile `tile` (of `tiles`) of period `f` of scan `a` (scale nb / period) by
-// group `grp`, with its shared memory `sc`. Every thread of the group calls
-// it; the group's threads must not touch `sc` from an earlier call when it
-// starts (it begins by filling it).
+// Tile `tile` of one period of scan `a` (scale nb / period) by group `grp`,
+// with its shared memory `sc`; the tile's winner goes to out[PART_STRIDE],
+// *key_out and *flag_out. Every thread of the group calls it; the group's
+// threads must not touch `sc` from an earlier call when it starts (it begins
+// by filling it).
 template <typename Rows, typename Group>
 __device__ __forceinline__ void scan_tile(const ScanArgs& a, const Rows& rows, const Group& grp, TileScratch& sc,
-                                          const int tile, const int f, const int tiles, const double scale) {
+                                          const int tile, const double scale, double* out, uint64_t* key_out,
+                                          uint32_t* flag_out) {
     const int lane = grp.lane();
     const int nb = a.nb;
     const int nd = a.nd, ns = a.ns, layers = a.layers;
@@ -401,8 +403,6 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const Rows& rows, c
         const float q = rmaxf(__fsub_rn(norm, d), 1e-30f);
         const double value = winner_value > neg_inf() ? (double)__fdiv_rn(aa, __fsqrt_rn(q)) : neg_inf();
         const double depth = (double)__fmul_rn(__fdiv_rn(aa, q), rf);
-        const size_t idx = (size_t)f * tiles + tile;
-        double* out = a.parts + idx * PART_STRIDE;
         out[0] = (double)phase;
         out[1] = (double)width;
         out[2] = (double)aa;
@@ -412,8 +412,8 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const Rows& rows, c
         out[6] = sc.rho[winner_di];
         out[7] = value;
         out[8] = depth;
-        a.keys[idx] = winner_key;
-        a.flags[idx] = 0u;
+        *key_out = winner_key;
+        *flag_out = 0u;
     } else if (lane == 0) {
         // The winner recomputed in f64 (kernels.rs:800-843).
         const uint32_t phase = (uint32_t)(winner_key % nb1);
@@ -431,8 +431,6 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const Rows& rows, c
         const double q = rmax(__dsub_rn(norm, d), 1e-300);
         const double value = winner_value > neg_inf() ? __ddiv_rn(aa, __dsqrt_rn(q)) : neg_inf();
         const double depth = __dmul_rn(__ddiv_rn(aa, q), r);
-        const size_t idx = (size_t)f * tiles + tile;
-        double* out = a.parts + idx * PART_STRIDE;
         out[0] = (double)phase;
         out[1] = (double)width;
         out[2] = aa;
@@ -442,9 +440,44 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const Rows& rows, c
         out[6] = r;
         out[7] = value;
         out[8] = depth;
-        a.keys[idx] = winner_key;
-        a.flags[idx] = (uint32_t)retry | ((uint32_t)bad_any << 1) | ((uint32_t)rescanned << 2);
+        *key_out = winner_key;
+        *flag_out = (uint32_t)retry | ((uint32_t)bad_any << 1) | ((uint32_t)rescanned << 2);
     }
+}
+
+// Period f's record from its best tile's part (PART_STRIDE doubles), its
+// score and its ORed tile flags (kernels.rs:1115-1155).
+__device__ __forceinline__ void merge_record(const MergeArgs& a, const int f, const double* part, double best,
+                                             uint32_t fl) {
+    const size_t g = (size_t)a.offset + f;
+    double* rec = a.records + g * RECORD_STRIDE;
+    rec[0] = a.periods_in[f];
+    rec[1] = a.scales[f];
+    for (int i = 0; i < 7; i++) rec[2 + i] = part[i];
+    a.score[g] = best;
+    a.depth[g] = part[8];
+    a.flags_out[g] = fl;
+}
+
+// Best tile of period f by (score, lowest key), flags ORed, into the merge's
+// record; parts, keys and flags are the period's `tiles` tile winners.
+__device__ __forceinline__ void merge_tiles(const double* parts, const uint64_t* keys, const uint32_t* flags,
+                                            int tiles, const MergeArgs& a, const int f) {
+    double best = neg_inf();
+    uint64_t key = KEY_MAX;
+    int chosen = 0;
+    uint32_t fl = 0;
+    for (int t = 0; t < tiles; t++) {
+        double v = parts[(size_t)t * PART_STRIDE + 7];
+        uint64_t k = keys[t];
+        fl |= flags[t];
+        if (v > best || (v == best && k < key)) {
+            best = v;
+            key = k;
+            chosen = t;
+        }
+    }
+    merge_record(a, f, parts + (size_t)chosen * PART_STRIDE, best, fl);
 }
 
 }  // namespace fbls
