@@ -357,6 +357,9 @@ def run_gpu(args):
     d2h = sum((s["periods"] + s["prescan_survivors"]) * (9 * 8 + 8 + 8 + 4) for s in stats) + 40 * len(rows_e)
 
     peak, peak_kind = _peaks()
+    from fbls_b200 import autotune
+    fused = not autotune.current().get("separate_scan", 0)
+    kernel = ("k_fold_scan (fold + prefix + tile scan + merge, fused)" if fused else "k_fold_walk (fold + prefix)")
     fold_launches = max(ctr["fold_launches"], 1)
     fold_ms_per = ctr["fold_ms"] / fold_launches
     fold_bytes_per = ctr["fold_bytes"] / fold_launches
@@ -385,8 +388,9 @@ def run_gpu(args):
         "box_trials_per_s": value / len(cfg.ingress_fractions),
         "rows_per_step": int(len(rows)),
         "gpu_launches": int(ctr["launches"]),
-        "kernel_ms": {"fold_prefix": ctr["fold_ms"] / args.steps, "scan_tiles+merge": ctr["scan_ms"] / args.steps},
-        "roofline": {"kernel": "k_fold_walk (fold + prefix)", "bound": "hbm", "achieved": achieved, "peak": peak,
+        "kernel_ms": ({"fold_scan_merge": ctr["fold_ms"] / args.steps} if fused else
+                      {"fold_prefix": ctr["fold_ms"] / args.steps, "scan_tiles+merge": ctr["scan_ms"] / args.steps}),
+        "roofline": {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": fold_bytes_per, "launch_ms": fold_ms_per,
                      "l2": {"peak": l2_peak, "frac": achieved / l2_peak if l2_peak > 0 else None,

@@ -10,10 +10,10 @@ walking its own window. This sweep measures, per nb class floor(log2(nb)),
 the fold's device time (CUDA events on the context's stream, the library's
 kernel-timing counters) of one scan_bank pass over 4096 periods of the
 13-sector synthetic star at every allowed group cap, then at every CTA size
-and lockstep threshold, the periods per launch on a whole signal_search,
-and, on a batch of seeded survey stars searched together, a CTA per fold
-unit against the persistent work-stealing fold grid; it writes the fastest
-as a table:
+and lockstep threshold, the periods per launch and the fused against the
+separate tile scan on a whole signal_search, and, on a batch of seeded
+survey stars searched together, a CTA per fold unit against the persistent
+work-stealing fold grid; it writes the fastest as a table:
 
     python -m fbls_b200.autotune --out fbls_b200/data/tuning.json
 
@@ -161,6 +161,22 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
         best = min(launches, key=launches.get)
         out["signal_search_ms"] = {str(k): round(v, 3) for k, v in launches.items()}
         out["launch_periods"] = int(best) if launches[best] < 0.99 * launches[16384] else 0
+        # The tile scan fused into the fold's CTAs against the separate scan
+        # and merge kernels over prefix rows in device memory.
+        sep = {}
+        for flag in (0, 1):
+            apply({**tuned, "launch_periods": out["launch_periods"], "separate_scan": flag})
+            gpu.signal_search(st, cfg, dev=dev)
+            ms = []
+            for _ in range(reps):
+                gpu.timer_start()
+                gpu.signal_search(st, cfg, dev=dev)
+                ms.append(gpu.timer_stop())
+            sep[flag] = sum(ms) / len(ms)
+            log(f"separate_scan {flag}: {sep[flag]:.2f} ms per signal_search")
+        out["separate_scan_ms"] = {str(k): round(v, 3) for k, v in sep.items()}
+        out["separate_scan"] = 1 if sep[1] < 0.99 * sep[0] else 0
+        tuned["separate_scan"] = out["separate_scan"]
         dev.free()
         # The batch's fold jobs: a CTA per unit against the persistent
         # work-stealing grid, on seeded survey stars searched together.
@@ -200,7 +216,7 @@ def main(argv=None):
     table = sweep(args.reps, log=lambda m: print(f"[{time.time() - t0:6.1f} s] {m}", flush=True))
     Path(args.out).write_text(json.dumps(table, indent=1) + "\n")
     print(json.dumps({k: table[k] for k in ("fold_group_max", "fold_threads", "lockstep_min", "launch_periods",
-                                             "fold_steal")}))
+                                             "separate_scan", "fold_steal")}))
 
 
 if __name__ == "__main__":
