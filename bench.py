@@ -358,7 +358,7 @@ def run_gpu(args):
 
     peak, peak_kind = _peaks()
     from fbls_b200 import autotune
-    fused = not autotune.current().get("separate_scan", 0)
+    fused = bool(autotune.current().get("fused_scan", 0))
     kernel = ("k_fold_scan (fold + prefix + tile scan + merge, fused)" if fused else "k_fold_walk (fold + prefix)")
     fold_launches = max(ctr["fold_launches"], 1)
     fold_ms_per = ctr["fold_ms"] / fold_launches

@@ -13,7 +13,8 @@ kernel-timing counters) of one scan_bank pass over 4096 periods of the
 and lockstep threshold, the periods per launch and the fused against the
 separate tile scan on a whole signal_search, and, on a batch of seeded
 survey stars searched together, a CTA per fold unit against the persistent
-work-stealing fold grid; it writes the fastest as a table:
+work-stealing fold grid and the coarse maps' lockstep threshold; it writes
+the fastest as a table:
 
     python -m fbls_b200.autotune --out fbls_b200/data/tuning.json
 
@@ -37,6 +38,7 @@ GROUPS = (1, 2, 4, 8, 16, 32)
 LAUNCHES = (4096, 8192, 16384, 32768)
 THREADS = (1024, 512, 256, 128)
 LOCKSTEP = (0, 3, 7, 15, 4096)  # 0: the built-in 11; 4096: never in lockstep
+MAP_LOCKSTEP = (0, 3, 5, 7, 4096)
 
 
 def device_name(device: int = 0) -> str:
@@ -55,7 +57,8 @@ def apply(table: dict) -> None:
         t.lockstep_min[int(cls)] = int(lm)
     t.launch_periods = int(table.get("launch_periods", 0))
     t.fold_steal = int(table.get("fold_steal", 0))
-    t.separate_scan = int(table.get("separate_scan", 0))
+    t.fused_scan = int(table.get("fused_scan", 0))
+    t.map_lockstep_min = int(table.get("map_lockstep_min", 0))
     rc = N.load().fbls_set_tuning(C.byref(t))
     if rc:
         raise ValueError(f"tuning table rejected (status {rc})")
@@ -68,7 +71,7 @@ def current() -> dict:
             "fold_threads": {str(c): int(v) for c, v in enumerate(t.fold_threads) if v},
             "lockstep_min": {str(c): int(v) for c, v in enumerate(t.lockstep_min) if v},
             "launch_periods": int(t.launch_periods), "fold_steal": int(t.fold_steal),
-            "separate_scan": int(t.separate_scan)}
+            "fused_scan": int(t.fused_scan), "map_lockstep_min": int(t.map_lockstep_min)}
 
 
 def reset() -> None:
@@ -165,7 +168,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
         # and merge kernels over prefix rows in device memory.
         sep = {}
         for flag in (0, 1):
-            apply({**tuned, "launch_periods": out["launch_periods"], "separate_scan": flag})
+            apply({**tuned, "launch_periods": out["launch_periods"], "fused_scan": flag})
             gpu.signal_search(st, cfg, dev=dev)
             ms = []
             for _ in range(reps):
@@ -173,10 +176,10 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
                 gpu.signal_search(st, cfg, dev=dev)
                 ms.append(gpu.timer_stop())
             sep[flag] = sum(ms) / len(ms)
-            log(f"separate_scan {flag}: {sep[flag]:.2f} ms per signal_search")
-        out["separate_scan_ms"] = {str(k): round(v, 3) for k, v in sep.items()}
-        out["separate_scan"] = 1 if sep[1] < 0.99 * sep[0] else 0
-        tuned["separate_scan"] = out["separate_scan"]
+            log(f"fused_scan {flag}: {sep[flag]:.2f} ms per signal_search")
+        out["fused_scan_ms"] = {str(k): round(v, 3) for k, v in sep.items()}
+        out["fused_scan"] = 1 if sep[1] < 0.99 * sep[0] else 0
+        tuned["fused_scan"] = out["fused_scan"]
         dev.free()
         # The batch's fold jobs: a CTA per unit against the persistent
         # work-stealing grid, on seeded survey stars searched together.
@@ -201,6 +204,26 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
             log(f"survey of {survey_stars} stars, fold_steal {flag}: {1e3 * steal[flag]:.1f} ms")
         out["survey_ms"] = {"stars": survey_stars, **{str(k): round(1e3 * v, 2) for k, v in steal.items()}}
         out["fold_steal"] = 1 if steal[1] < 0.99 * steal[0] else 0
+        # The coarse maps' folds (the proposal network's input, binned
+        # families) by lockstep threshold, on the same stars.
+        from . import proposal as pr
+        pstars = [(s_, p) for s_, p in stars]
+        bin_days = float(np.load(pr.WEIGHTS)["bin_days"])
+        maps = {}
+        for lm in MAP_LOCKSTEP:
+            apply({**tuned, "launch_periods": out["launch_periods"], "fold_steal": out["fold_steal"],
+                   "map_lockstep_min": lm})
+            pr.features(gpu, pstars, devs, bin_days)
+            ts = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                pr.features(gpu, pstars, devs, bin_days)
+                ts.append(time.perf_counter() - t0)
+            maps[lm] = sum(ts) / len(ts)
+            log(f"coarse maps of {survey_stars} stars, map lockstep {lm or 'rule'}: {1e3 * maps[lm]:.1f} ms")
+        best = min(maps, key=maps.get)
+        out["maps_ms"] = {str(k): round(1e3 * v, 2) for k, v in maps.items()}
+        out["map_lockstep_min"] = int(best) if maps[best] < 0.98 * maps[0] else 0
         for d in devs:
             d.free()
     reset()
@@ -216,7 +239,7 @@ def main(argv=None):
     table = sweep(args.reps, log=lambda m: print(f"[{time.time() - t0:6.1f} s] {m}", flush=True))
     Path(args.out).write_text(json.dumps(table, indent=1) + "\n")
     print(json.dumps({k: table[k] for k in ("fold_group_max", "fold_threads", "lockstep_min", "launch_periods",
-                                             "separate_scan", "fold_steal")}))
+                                             "fused_scan", "fold_steal", "map_lockstep_min")}))
 
 
 if __name__ == "__main__":

@@ -905,7 +905,8 @@ std::atomic<uint32_t> g_threads[32];
 std::atomic<uint32_t> g_lockstep[32];
 std::atomic<uint32_t> g_launch_periods{16384};
 std::atomic<uint32_t> g_fold_steal{0};
-std::atomic<uint32_t> g_separate_scan{0};
+std::atomic<uint32_t> g_fused_scan{0};
+std::atomic<uint32_t> g_map_lockstep{0};
 
 int nb_class(int nb) { return nb > 0 ? 31 - __builtin_clz((unsigned)nb) : 0; }
 
@@ -992,7 +993,8 @@ void set_fold_tuning(const FoldTuning& t) {
     }
     g_launch_periods.store(t.launch_periods ? t.launch_periods : 16384u, std::memory_order_relaxed);
     g_fold_steal.store(t.steal ? 1u : 0u, std::memory_order_relaxed);
-    g_separate_scan.store(t.separate_scan ? 1u : 0u, std::memory_order_relaxed);
+    g_fused_scan.store(t.fused_scan ? 1u : 0u, std::memory_order_relaxed);
+    g_map_lockstep.store(t.map_lockstep_min, std::memory_order_relaxed);
 }
 
 void get_fold_tuning(FoldTuning* t) {
@@ -1003,10 +1005,13 @@ void get_fold_tuning(FoldTuning* t) {
     }
     t->launch_periods = g_launch_periods.load(std::memory_order_relaxed);
     t->steal = g_fold_steal.load(std::memory_order_relaxed);
-    t->separate_scan = g_separate_scan.load(std::memory_order_relaxed);
+    t->fused_scan = g_fused_scan.load(std::memory_order_relaxed);
+    t->map_lockstep_min = g_map_lockstep.load(std::memory_order_relaxed);
 }
 
-bool tuned_separate_scan() { return g_separate_scan.load(std::memory_order_relaxed) != 0; }
+int tuned_map_lockstep() { return (int)g_map_lockstep.load(std::memory_order_relaxed); }
+
+bool tuned_fused_scan() { return g_fused_scan.load(std::memory_order_relaxed) != 0; }
 
 bool tuned_fold_steal() { return g_fold_steal.load(std::memory_order_relaxed) != 0; }
 

@@ -215,9 +215,10 @@ int plan_passes(fbls_ctx* ctx, std::vector<Pass>& passes) {
     return FBLS_OK;
 }
 
-// A pass whose fold also scans: walking-fold shapes, unless the tuning
-// table asks for the separate scan kernels.
-bool fused_scan(const Pass& p) { return p.shape.kind == FOLD_WALK && !tuned_separate_scan(); }
+// A pass whose fold also scans and merges: walking-fold shapes, when the
+// tuning table asks for it (measured slower than the separate kernels on
+// B200; it keeps no prefix rows or tile parts in device memory).
+bool fused_scan(const Pass& p) { return p.shape.kind == FOLD_WALK && tuned_fused_scan(); }
 
 // Kernel counters of one fold launch of n periods: algorithmic bytes are the
 // observation stream once per period (24 B per observation) plus the prefix

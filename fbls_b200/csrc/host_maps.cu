@@ -298,6 +298,7 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
             fa.window = g.shape.window;
             fa.row_stride = g.shape.row_stride;
             fa.fault = as<uint32_t>(ctx->fault);
+            fa.lockstep_min = tuned_map_lockstep();
             float* out = reinterpret_cast<float*>(dout + m.out_off) + (size_t)(g.i0 + un.c0) * m.job->nd;
             if (un.walk) {
                 fa.map_out = out;

@@ -96,7 +96,8 @@ struct FoldTuning {
     uint32_t lockstep_min[32];
     uint32_t launch_periods;
     uint32_t steal;
-    uint32_t separate_scan;  // nonzero: fold and tile scan as separate kernels (else fused)
+    uint32_t fused_scan;  // nonzero: the walking fold scans and merges its own tiles (else separate kernels)
+    uint32_t map_lockstep_min;  // the coarse maps' folds: lockstep threshold (0: built-in)
 };
 
 struct ScanArgs {
@@ -225,7 +226,8 @@ FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned = false
 void set_fold_tuning(const FoldTuning& t);
 void get_fold_tuning(FoldTuning* t);
 uint32_t tuned_launch_periods();
-bool tuned_separate_scan();
+bool tuned_fused_scan();
+int tuned_map_lockstep();
 bool tuned_fold_steal();
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
 // spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.

@@ -125,7 +125,9 @@ extern "C" int fbls_set_tuning(const fbls_tuning* tuning) {
     }
     t.launch_periods = tuning->launch_periods;
     t.steal = tuning->fold_steal;
-    t.separate_scan = tuning->separate_scan;
+    t.fused_scan = tuning->fused_scan;
+    if (tuning->map_lockstep_min > 4096) return FBLS_ERR_ARGUMENT;
+    t.map_lockstep_min = tuning->map_lockstep_min;
     set_fold_tuning(t);
     return FBLS_OK;
 }
@@ -141,6 +143,7 @@ extern "C" int fbls_get_tuning(fbls_tuning* tuning) {
     }
     tuning->launch_periods = t.launch_periods;
     tuning->fold_steal = t.steal;
-    tuning->separate_scan = t.separate_scan;
+    tuning->fused_scan = t.fused_scan;
+    tuning->map_lockstep_min = t.map_lockstep_min;
     return FBLS_OK;
 }

@@ -258,10 +258,13 @@ int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
  * fold's CTA size (128, 256, 512 or 1024; 0 = 1024; the period group is cut
  * to at most one period per warp), and lockstep_min, the segment length from
  * which a CTA's lanes walk their observations in lockstep rather than each
- * its own window (0 = 11; at most 4096). separate_scan: nonzero runs the
- * tile scan as its own kernel over prefix rows the fold writes to device
- * memory, instead of in the walking fold's CTAs from the rows they keep in
- * shared memory (the default).
+ * its own window (0 = 11; at most 4096). fused_scan: nonzero has the
+ * walking fold's CTAs scan and merge their own periods' tiles from the prefix
+ * sums they keep in shared memory (no prefix rows or tile parts in device
+ * memory), instead of the separate scan and merge kernels over prefix rows
+ * the fold writes to device memory (the default, faster on B200).
+ * map_lockstep_min: lockstep_min of the coarse maps' folds (their binned
+ * families walk short segments), one value for every nb.
  * Process-wide; results do not depend on it, only the launch shapes do. */
 typedef struct {
     uint32_t fold_group_max[32];
@@ -269,7 +272,8 @@ typedef struct {
     uint32_t fold_steal;
     uint32_t fold_threads[32];
     uint32_t lockstep_min[32];
-    uint32_t separate_scan;
+    uint32_t fused_scan;
+    uint32_t map_lockstep_min;
 } fbls_tuning;
 int fbls_set_tuning(const fbls_tuning* tuning);
 int fbls_get_tuning(fbls_tuning* tuning);

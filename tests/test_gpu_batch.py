@@ -169,9 +169,10 @@ def test_fold_cta_size_and_lockstep_give_the_same_rows(gpu, threads, lockstep):
 
 @pytest.mark.parametrize("mode", [0, 1, 2])
 def test_fused_tile_scan_equals_the_separate_kernels(gpu, mode):
-    # The walking fold scanning its own tiles from the prefix rows it keeps
-    # in shared memory (the default) against the fold writing the rows to
-    # device memory and k_scan_tiles reading them back: the same records,
+    # The walking fold scanning and merging its own tiles from the prefix
+    # rows it keeps in shared memory (fused_scan) against the fold writing
+    # the rows to device memory and k_scan_tiles and k_merge reading them
+    # back (the default): the same records,
     # scores, depths and flags bit for bit, in each precision mode, for a
     # multi-band star (nb from 96 to 1,920, several period groups per CTA)
     # and a batch of survey stars (the job launches).
@@ -193,7 +194,7 @@ def test_fused_tile_scan_equals_the_separate_kernels(gpu, mode):
     try:
         dev = gpu.upload(st)
         for sep in (1, 0):
-            autotune.apply({**saved, "separate_scan": sep})
+            autotune.apply({**saved, "fused_scan": sep})
             banks = [gpu.scan_bank(dev, b["periods"][:3000], api.bank_for(b, cfg), nb, precision_mode=mode)
                      for b in bands for nb in (b["nb"] // 2, b["nb"])]
             rows = gpu.signal_search(st, cfg, dev=dev)

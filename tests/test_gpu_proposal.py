@@ -160,6 +160,26 @@ def test_coarse_map_batch_matches_single_maps(gpu, bin_days):
         d.free()
 
 
+def test_map_lockstep_threshold_does_not_change_the_maps(gpu):
+    """The coarse maps' folds at every lockstep threshold the tuning table
+    allows give the same network input bit for bit."""
+    from fbls_b200 import autotune
+    from fbls_b200 import proposal as pr
+    stars, cfg = pr.survey_stars(6, seed=9, max_sectors=3)
+    devs = [gpu.upload(s) for s, _ in stars]
+    saved = autotune.current()
+    try:
+        autotune.apply({**saved, "map_lockstep_min": 0})
+        want = pr.features(gpu, stars, devs, bin_days=600.0 / 86400.0)
+        for lm in (3, 5, 4096):
+            autotune.apply({**saved, "map_lockstep_min": lm})
+            assert np.array_equal(pr.features(gpu, stars, devs, bin_days=600.0 / 86400.0), want)
+    finally:
+        autotune.apply(saved)
+    for d in devs:
+        d.free()
+
+
 @pytest.mark.parametrize("bin_days", [0.0, 600.0 / 86400.0])
 def test_features_are_the_standardised_maps(gpu, bin_days):
     """fbls_coarse_features: the batch's network input equals, star for star,
