@@ -8,8 +8,9 @@ period, hence the segment each lane walks, and the lockstep threshold picks
 between lanes stepping together (conflict-free reads, idle steps) and each
 walking its own window. This sweep measures, per nb class floor(log2(nb)),
 the fold's device time (CUDA events on the context's stream, the library's
-kernel-timing counters) of one scan_bank pass over 4096 periods of the
-13-sector synthetic star at every allowed group cap, then at every CTA size
+kernel-timing counters) of one scan_bank pass over every period of an
+octave band of the 13-sector synthetic star (the launches and period groups
+of a search) at every allowed group cap, then at every CTA size
 and lockstep threshold, the periods per launch and the fused against the
 separate tile scan on a whole signal_search, and, on a batch of seeded
 survey stars searched together, a CTA per fold unit against the persistent
@@ -103,7 +104,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
     st = api.prepared_family(c.time, c.flux, c.flux_err, cfg)
     grid, bands = api.band_plan(st, cfg)
     out = {"device": device_name(0),
-           "workload": "13-sector synthetic star (247,104 observations), 4096 periods of each octave band at its "
+           "workload": "13-sector synthetic star (247,104 observations), every period of an octave band at its "
                        "coarse and full nb; fold device time per pass (ms) by period-group cap, 0 = the rule",
            "fold_ms": {}, "fold_group_max": {}, "command": "python -m fbls_b200.autotune"}
     with api.Gpu(0, tuned=False) as gpu:
@@ -116,7 +117,8 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
         out["fold_threads"], out["lockstep_min"], out["shape_ms"] = {}, {}, {}
         for cls, (nb, band) in sorted(cases.items()):
             bank = api.bank_for(band, cfg)
-            periods = band["periods"][:4096]
+            # the whole band, so the launches have the period groups of a search
+            periods = band["periods"]
             reset()
             times = {0: _fold_ms(gpu, dev, periods, bank, nb, reps)}  # the built-in rule
             for g in GROUPS:
@@ -180,6 +182,33 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
         out["fused_scan_ms"] = {str(k): round(v, 3) for k, v in sep.items()}
         out["fused_scan"] = 1 if sep[1] < 0.99 * sep[0] else 0
         tuned["fused_scan"] = out["fused_scan"]
+
+        # The per-class choices together, on the whole search: kept only
+        # where they beat the built-in shapes end to end.
+        def search_ms(table):
+            apply(table)
+            gpu.signal_search(st, cfg, dev=dev)
+            ms = []
+            for _ in range(reps):
+                gpu.timer_start()
+                gpu.signal_search(st, cfg, dev=dev)
+                ms.append(gpu.timer_stop())
+            return sum(ms) / len(ms)
+
+        rest = {"launch_periods": out["launch_periods"], "fused_scan": out["fused_scan"]}
+        variants = {"built-in shapes": {}, "tuned groups": {"fold_group_max": out["fold_group_max"]},
+                    "tuned groups and lockstep": {"fold_group_max": out["fold_group_max"],
+                                                  "lockstep_min": out["lockstep_min"]},
+                    "tuned groups, lockstep and CTA sizes": {k: tuned[k] for k in
+                                                             ("fold_group_max", "fold_threads", "lockstep_min")}}
+        whole = {name: search_ms({**v, **rest}) for name, v in variants.items()}
+        for name, v in whole.items():
+            log(f"signal_search with {name}: {v:.2f} ms")
+        pick = min(whole, key=whole.get)
+        out["whole_search_ms"] = {k: round(v, 3) for k, v in whole.items()}
+        for k in ("fold_group_max", "fold_threads", "lockstep_min"):
+            out[k] = variants[pick].get(k, {})
+            tuned[k] = out[k]
         dev.free()
         # The batch's fold jobs: a CTA per unit against the persistent
         # work-stealing grid, on seeded survey stars searched together.
