@@ -671,9 +671,9 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
                 atomicAdd(&lc[slot], cnt);
             }
         } else {
-        // Lockstep walk: at step i every lane reads observation seg * R + i
-        // (R odd, so the lanes' reads fall in distinct banks) and folds it when
-        // it lies in the lane's window [k, end). Entering a cell takes the
+        // Lockstep walk: at step i every lane whose window [k, end) holds
+        // observation seg * R + i reads and folds it (R odd, so the lanes'
+        // reads fall in distinct banks). Entering a cell takes the
         // bin's sums prefetched at the previous cell change (the next cell's
         // bin), and prefetches the bin after it. Counts are integers, so a
         // run's count is added to its bin with one shared-memory atomic add
@@ -695,27 +695,27 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
             }
             for (int i = 0; i < steps; i++) {
                 const int o = b0 + i;
-                const int j = min(o, len);  // staged slot (or slack) for every step
-                const double tj = tt[j], vj = tt[j + F], wj = tt[j + 2 * F];
-                const bool in = o >= k && o < end;
-                const uint32_t cj = cell_of(tj, scale);
-                if (in && cj != cur) {
-                    lvw[slot] = acc;
-                    atomicAdd(&lc[slot], cnt);
-                    cnt = 0;
-                    if (cj == cur + 1u) {
-                        acc = pre;
-                        slot = nslot;
-                    } else {  // empty cells skipped
-                        const uint32_t b = cj - base;
-                        slot = b >= unb ? b - unb : b;
-                        acc = lvw[slot];
+                // Only the lanes whose window holds o read it, so a step's
+                // reads take fewer wavefronts as lanes run out of window.
+                if (o >= k && o < end) {
+                    const double tj = tt[o], vj = tt[o + F], wj = tt[o + 2 * F];
+                    const uint32_t cj = cell_of(tj, scale);
+                    if (cj != cur) {
+                        lvw[slot] = acc;
+                        atomicAdd(&lc[slot], cnt);
+                        cnt = 0;
+                        if (cj == cur + 1u) {
+                            acc = pre;
+                            slot = nslot;
+                        } else {  // empty cells skipped
+                            const uint32_t b = cj - base;
+                            slot = b >= unb ? b - unb : b;
+                            acc = lvw[slot];
+                        }
+                        cur = cj;
+                        nslot = slot + 1u == unb ? 0u : slot + 1u;
+                        pre = lvw[nslot];
                     }
-                    cur = cj;
-                    nslot = slot + 1u == unb ? 0u : slot + 1u;
-                    pre = lvw[nslot];
-                }
-                if (in) {
                     acc.x = __dadd_rn(acc.x, vj);
                     acc.y = __dadd_rn(acc.y, wj);
                     cnt += 1u;
