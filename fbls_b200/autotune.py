@@ -90,6 +90,12 @@ def load_for(device_name_: str, path: Path = TABLE) -> bool:
     return True
 
 
+def _median(xs) -> float:
+    """The median of repeated timings (one slow step of a shared host does
+    not move it)."""
+    return float(np.median(np.asarray(xs, dtype=np.float64)))
+
+
 def _fold_ms(gpu, dev, periods, bank, nb, reps: int) -> float:
     gpu.scan_bank(dev, periods, bank, nb)  # warm
     gpu.counters(reset=True)
@@ -161,7 +167,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
                 gpu.timer_start()
                 gpu.signal_search(st, cfg, dev=dev)
                 ms.append(gpu.timer_stop())
-            launches[lp] = sum(ms) / len(ms)
+            launches[lp] = _median(ms)
             log(f"launch {lp}: {launches[lp]:.2f} ms per signal_search")
         best = min(launches, key=launches.get)
         out["signal_search_ms"] = {str(k): round(v, 3) for k, v in launches.items()}
@@ -177,7 +183,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
                 gpu.timer_start()
                 gpu.signal_search(st, cfg, dev=dev)
                 ms.append(gpu.timer_stop())
-            sep[flag] = sum(ms) / len(ms)
+            sep[flag] = _median(ms)
             log(f"fused_scan {flag}: {sep[flag]:.2f} ms per signal_search")
         out["fused_scan_ms"] = {str(k): round(v, 3) for k, v in sep.items()}
         out["fused_scan"] = 1 if sep[1] < 0.99 * sep[0] else 0
@@ -193,7 +199,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
                 gpu.timer_start()
                 gpu.signal_search(st, cfg, dev=dev)
                 ms.append(gpu.timer_stop())
-            return sum(ms) / len(ms)
+            return _median(ms)
 
         rest = {"launch_periods": out["launch_periods"], "fused_scan": out["fused_scan"]}
         variants = {"built-in shapes": {}, "tuned groups": {"fold_group_max": out["fold_group_max"]},
@@ -229,7 +235,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
                 gpu.search_batch([s_ for s_, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs,
                                  workers=0)
                 ts.append(time.perf_counter() - t0)
-            steal[flag] = sum(ts) / len(ts)
+            steal[flag] = _median(ts)
             log(f"survey of {survey_stars} stars, fold_steal {flag}: {1e3 * steal[flag]:.1f} ms")
         out["survey_ms"] = {"stars": survey_stars, **{str(k): round(1e3 * v, 2) for k, v in steal.items()}}
         out["fold_steal"] = 1 if steal[1] < 0.99 * steal[0] else 0
@@ -248,7 +254,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
                 t0 = time.perf_counter()
                 pr.features(gpu, pstars, devs, bin_days)
                 ts.append(time.perf_counter() - t0)
-            maps[lm] = sum(ts) / len(ts)
+            maps[lm] = _median(ts)
             log(f"coarse maps of {survey_stars} stars, map lockstep {lm or 'rule'}: {1e3 * maps[lm]:.1f} ms")
         best = min(maps, key=maps.get)
         out["maps_ms"] = {str(k): round(1e3 * v, 2) for k, v in maps.items()}
@@ -262,7 +268,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--out", default=str(TABLE))
-    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--reps", type=int, default=5)
     args = ap.parse_args(argv)
     t0 = time.time()
     table = sweep(args.reps, log=lambda m: print(f"[{time.time() - t0:6.1f} s] {m}", flush=True))
