@@ -38,6 +38,7 @@ TABLE = Path(__file__).resolve().parent / "data" / "tuning.json"
 GROUPS = (1, 2, 4, 8, 16, 32)
 LAUNCHES = (4096, 8192, 16384, 32768)
 THREADS = (1024, 512, 256, 128)
+PAIR_THREADS = (512, 256)
 LOCKSTEP = (0, 3, 7, 15, 4096)  # 0: the built-in 11; 4096: never in lockstep
 MAP_LOCKSTEP = (0, 3, 5, 7, 4096)
 
@@ -56,6 +57,8 @@ def apply(table: dict) -> None:
         t.fold_threads[int(cls)] = int(th)
     for cls, lm in table.get("lockstep_min", {}).items():
         t.lockstep_min[int(cls)] = int(lm)
+    for cls, pv in table.get("fold_pair", {}).items():
+        t.fold_pair[int(cls)] = int(pv)
     t.launch_periods = int(table.get("launch_periods", 0))
     t.fold_steal = int(table.get("fold_steal", 0))
     t.fused_scan = int(table.get("fused_scan", 0))
@@ -71,6 +74,7 @@ def current() -> dict:
     return {"fold_group_max": {str(c): int(g) for c, g in enumerate(t.fold_group_max) if g},
             "fold_threads": {str(c): int(v) for c, v in enumerate(t.fold_threads) if v},
             "lockstep_min": {str(c): int(v) for c, v in enumerate(t.lockstep_min) if v},
+            "fold_pair": {str(c): int(v) for c, v in enumerate(t.fold_pair) if v},
             "launch_periods": int(t.launch_periods), "fold_steal": int(t.fold_steal),
             "fused_scan": int(t.fused_scan), "map_lockstep_min": int(t.map_lockstep_min)}
 
@@ -120,7 +124,7 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
         for band in bands:
             for nb in (band["nb"] // 2, band["nb"]):
                 cases.setdefault(int(np.floor(np.log2(nb))), (nb, band))
-        out["fold_threads"], out["lockstep_min"], out["shape_ms"] = {}, {}, {}
+        out["fold_threads"], out["lockstep_min"], out["fold_pair"], out["shape_ms"] = {}, {}, {}, {}
         for cls, (nb, band) in sorted(cases.items()):
             bank = api.bank_for(band, cfg)
             # the whole band, so the launches have the period groups of a search
@@ -140,24 +144,29 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
             # CTA size and lockstep threshold at the chosen group cap.
             caps = {str(cls): out["fold_group_max"][str(cls)]} if str(cls) in out["fold_group_max"] else {}
             shapes = {}
-            for th in THREADS:
-                for lm in LOCKSTEP:
-                    apply({"fold_group_max": caps, "fold_threads": {str(cls): th}, "lockstep_min": {str(cls): lm}})
-                    shapes[(th, lm)] = _fold_ms(gpu, dev, periods, bank, nb, reps)
+            for pair, ths in ((0, THREADS), (1, PAIR_THREADS)):
+                for th in ths:
+                    for lm in LOCKSTEP:
+                        apply({"fold_group_max": caps, "fold_threads": {str(cls): th},
+                               "lockstep_min": {str(cls): lm}, "fold_pair": {str(cls): pair}})
+                        shapes[(pair, th, lm)] = _fold_ms(gpu, dev, periods, bank, nb, reps)
             reset()
-            base = shapes[(1024, 0)]
-            bth, blm = min(shapes, key=shapes.get)
-            out["shape_ms"][str(cls)] = {f"{th}/{lm or 'rule'}": round(v, 4) for (th, lm), v in shapes.items()}
-            if shapes[(bth, blm)] < 0.98 * base:
+            base = shapes[(0, 1024, 0)]
+            bp, bth, blm = min(shapes, key=shapes.get)
+            out["shape_ms"][str(cls)] = {f"{'pair ' if p else ''}{th}/{lm or 'rule'}": round(v, 4)
+                                         for (p, th, lm), v in shapes.items()}
+            if shapes[(bp, bth, blm)] < 0.98 * base:
                 if bth != 1024:
                     out["fold_threads"][str(cls)] = int(bth)
                 if blm:
                     out["lockstep_min"][str(cls)] = int(blm)
-            log(f"nb {nb} (class {cls}): threads/lockstep " +
-                ", ".join(f"{th}/{lm or 'rule'}: {v:.3f}" for (th, lm), v in shapes.items()) +
-                f" -> {bth}/{blm or 'rule'}")
+                if bp:
+                    out["fold_pair"][str(cls)] = 1
+            log(f"nb {nb} (class {cls}): form/threads/lockstep " +
+                ", ".join(f"{'pair ' if p else ''}{th}/{lm or 'rule'}: {v:.3f}" for (p, th, lm), v in shapes.items())
+                + f" -> {'pair ' if bp else ''}{bth}/{blm or 'rule'}")
         tuned = {"fold_group_max": out["fold_group_max"], "fold_threads": out["fold_threads"],
-                 "lockstep_min": out["lockstep_min"]}
+                 "lockstep_min": out["lockstep_min"], "fold_pair": out["fold_pair"]}
         launches = {}
         for lp in LAUNCHES:
             apply({**tuned, "launch_periods": lp})
@@ -206,13 +215,15 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
                     "tuned groups and lockstep": {"fold_group_max": out["fold_group_max"],
                                                   "lockstep_min": out["lockstep_min"]},
                     "tuned groups, lockstep and CTA sizes": {k: tuned[k] for k in
-                                                             ("fold_group_max", "fold_threads", "lockstep_min")}}
+                                                             ("fold_group_max", "fold_threads", "lockstep_min")},
+                    "tuned groups, lockstep, CTA sizes and paired walks": {
+                        k: tuned[k] for k in ("fold_group_max", "fold_threads", "lockstep_min", "fold_pair")}}
         whole = {name: search_ms({**v, **rest}) for name, v in variants.items()}
         for name, v in whole.items():
             log(f"signal_search with {name}: {v:.2f} ms")
         pick = min(whole, key=whole.get)
         out["whole_search_ms"] = {k: round(v, 3) for k, v in whole.items()}
-        for k in ("fold_group_max", "fold_threads", "lockstep_min"):
+        for k in ("fold_group_max", "fold_threads", "lockstep_min", "fold_pair"):
             out[k] = variants[pick].get(k, {})
             tuned[k] = out[k]
         dev.free()
@@ -273,7 +284,8 @@ def main(argv=None):
     t0 = time.time()
     table = sweep(args.reps, log=lambda m: print(f"[{time.time() - t0:6.1f} s] {m}", flush=True))
     Path(args.out).write_text(json.dumps(table, indent=1) + "\n")
-    print(json.dumps({k: table[k] for k in ("fold_group_max", "fold_threads", "lockstep_min", "launch_periods",
+    print(json.dumps({k: table[k] for k in ("fold_group_max", "fold_threads", "lockstep_min", "fold_pair",
+                                             "launch_periods",
                                              "fused_scan", "fold_steal", "map_lockstep_min")}))
 
 

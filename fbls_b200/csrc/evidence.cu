@@ -1181,7 +1181,7 @@ int compare_batch(cudaStream_t stream, EvidenceCandidate* cands, size_t count, c
             const int njobs = (int)(e - r);
             cudaError_t err;
             if (s0.kind == FOLD_WALK)
-                err = launch_fold_jobs(d_jobs + r, d_cta0, njobs, njobs, s0.threads, smem, stream);
+                err = launch_fold_jobs(d_jobs + r, d_cta0, njobs, njobs, s0.threads, false, smem, stream);
             else
                 err = launch_fold_smem_jobs(d_jobs + r, d_cta0, njobs, njobs, s0.threads, smem, stream);
             if (!counted(err, "evidence fold")) return FBLS_ERR_CUDA;

@@ -398,6 +398,96 @@ __device__ __forceinline__ void stage_chunk(const FoldArgs& a, int i0, int i1, d
 // lose more to idle steps than the conflict-free reads gain).
 constexpr int LOCKSTEP_MIN_SEGMENT = 11;
 
+// The first observation of a lane's window in a chunk: its segment's start
+// seg * R moved forward to the period's next cell boundary (so every run
+// belongs to exactly one lane), at most len.
+__device__ __forceinline__ int window_start(const double* tt, int len, int R, int seg, double scale) {
+    int k = seg * R;
+    if (k < len && k > 0) {
+        const uint32_t prev = cell_of(tt[k - 1], scale);
+        while (k < len) {
+            if (cell_of(tt[k], scale) != prev) break;
+            ++k;
+        }
+    }
+    return k > len ? len : k;
+}
+
+// Short segments: one lane walks its window [k, end) of one period, loading
+// a bin's sums when its run starts and storing them when it ends; a run's
+// count goes to its bin by one shared-memory atomic add (no load).
+__device__ __forceinline__ void walk_window(const double* tt, int F, int k, int end, double scale, uint32_t unb,
+                                            double inv_nb, double2* lvw, uint32_t* lc) {
+    uint32_t cur = cell_of(tt[k], scale);
+    const uint32_t s0 = mod_nb(cur, unb, inv_nb);
+    const uint32_t base = cur - s0;
+    uint32_t slot = s0;
+    double2 acc = lvw[slot];
+    uint32_t cnt = 0;
+    for (int j = k; j < end; j++) {
+        const uint32_t cj = cell_of(tt[j], scale);
+        if (cj != cur) {
+            lvw[slot] = acc;
+            atomicAdd(&lc[slot], cnt);
+            cnt = 0;
+            const uint32_t b = cj - base;
+            slot = b >= unb ? b - unb : b;
+            cur = cj;
+            acc = lvw[slot];
+        }
+        acc.x = __dadd_rn(acc.x, tt[j + F]);
+        acc.y = __dadd_rn(acc.y, tt[j + 2 * F]);
+        cnt += 1u;
+    }
+    lvw[slot] = acc;
+    atomicAdd(&lc[slot], cnt);
+}
+
+// A lane's run state for one period in the lockstep walk: the current
+// cell's sums, and the next cell's bin prefetched at each cell change.
+struct RunWalker {
+    double2* lvw;
+    uint32_t* lc;
+    uint32_t cur, base, slot, nslot, cnt;
+    double2 acc, pre;
+    __device__ __forceinline__ void open(double t, double scale, uint32_t unb, double inv_nb) {
+        cur = cell_of(t, scale);
+        const uint32_t s0 = mod_nb(cur, unb, inv_nb);
+        base = cur - s0;  // bin = cell - base (- nb past the wrap)
+        slot = s0;
+        nslot = s0 + 1u == unb ? 0u : s0 + 1u;
+        acc = lvw[slot];
+        pre = lvw[nslot];
+        cnt = 0;
+    }
+    __device__ __forceinline__ void add(double t, double v, double w, double scale, uint32_t unb) {
+        const uint32_t cj = cell_of(t, scale);
+        if (cj != cur) {
+            lvw[slot] = acc;
+            atomicAdd(&lc[slot], cnt);
+            cnt = 0;
+            if (cj == cur + 1u) {
+                acc = pre;
+                slot = nslot;
+            } else {  // empty cells skipped
+                const uint32_t b = cj - base;
+                slot = b >= unb ? b - unb : b;
+                acc = lvw[slot];
+            }
+            cur = cj;
+            nslot = slot + 1u == unb ? 0u : slot + 1u;
+            pre = lvw[nslot];
+        }
+        acc.x = __dadd_rn(acc.x, v);
+        acc.y = __dadd_rn(acc.y, w);
+        cnt += 1u;
+    }
+    __device__ __forceinline__ void close() {
+        lvw[slot] = acc;
+        atomicAdd(&lc[slot], cnt);
+    }
+};
+
 // The coarse-map epilogue of the walking fold (after the in-place prefix rows
 // and a barrier), out of line: it runs once per CTA.
 __device__ __noinline__ void fold_map_epilogue(float* map_out, const double* map_durations, const double* map_rho,
@@ -528,7 +618,7 @@ __device__ __noinline__ void fold_scan_epilogue(const ScanArgs& scan, const Merg
 // folds periods [cta * G, cta * G + G). `reuse`: this CTA ran an earlier
 // fold (a persistent CTA), whose barriers are invalidated before the new
 // ones. Returns false (uniformly over the CTA) when a staging wait gave up.
-template <int CAP>
+template <int CAP, bool PAIR>
 __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, const bool reuse,
                                               const ScanArgs* scan, const MergeArgs* merge) {
     constexpr int F = CAP + 2;  // doubles per staged field
@@ -544,13 +634,17 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
     const uint32_t unb = (uint32_t)nb;
     const double inv_nb = 1.0 / (double)nb;
     const int G = a.group;
-    const int wpp = (T / 32) / G;
-    const int NS = wpp * 32;
+    // Paired walk: each lane walks two periods, q and q + G / 2, over the
+    // same staged observations (one read of t, v, w serves both).
+    const int GV = PAIR ? G / 2 : G;  // lane sets
+    const int wpp = (T / 32) / GV;    // warps per lane set (>= 1)
+    const int NS = wpp * 32;          // segments per period
     const int g0 = cta * G;
     const int g = min(G, a.periods - g0);
     const int q = warp / wpp;
     const int seg = (warp - q * wpp) * 32 + lane;
     const bool live = q < g;
+    const bool live_b = PAIR && q + GV < g;
     const int rs = a.row_stride;
 
     // Shared memory: staging [2][t | v | w][F] | run starts [G][NS + 1]
@@ -581,6 +675,11 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
     double2* lvw = hvw + (size_t)(live ? q : 0) * rs;
     uint32_t* lc = hc + (size_t)(live ? q : 0) * rs;
     int* lstart = starts + (live ? q : 0) * (NS + 1);
+    const int qb = live_b ? q + GV : 0;
+    const double scale_b = live_b ? s_scale[qb] : 0.0;
+    double2* lvw_b = hvw + (size_t)qb * rs;
+    uint32_t* lc_b = hc + (size_t)qb * rs;
+    int* lstart_b = starts + qb * (NS + 1);
     const float inv_ns = 1.0f / (float)NS;
     const int lmin = a.lockstep_min > 0 ? a.lockstep_min : LOCKSTEP_MIN_SEGMENT;
     const int nch = a.nchunks;
@@ -629,101 +728,78 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
         const double* tt = sb + (i0 - base_i);
         // Segment length: at least ceil(len / NS), odd.
         const int R = ((int)((float)len * inv_ns) + 1) | 1;
-        int k = seg * R;
-        if (live && k < len && k > 0) {
-            uint32_t prev = cell_of(tt[k - 1], scale);
-            while (k < len) {
-                const uint32_t v = cell_of(tt[k], scale);
-                if (v != prev) break;
-                ++k;
+        const int k = live ? window_start(tt, len, R, seg, scale) : 0;
+        int kb = 0;
+        if constexpr (PAIR) kb = live_b ? window_start(tt, len, R, seg, scale_b) : 0;
+        if (live) {
+            lstart[seg] = k;
+            if (seg == 0) lstart[NS] = len;
+        }
+        if constexpr (PAIR) {
+            if (live_b) {
+                lstart_b[seg] = kb;
+                if (seg == 0) lstart_b[NS] = len;
             }
         }
-        if (k > len) k = len;
-        if (live) lstart[seg] = k;
-        if (live && seg == 0) lstart[NS] = len;
         group_sync(gbar, gthreads);
         const int end = live ? lstart[seg + 1] : 0;
+        int end_b = 0;
+        if constexpr (PAIR) end_b = live_b ? lstart_b[seg + 1] : 0;
         if (R < lmin) {
-            // Short segments: each lane walks its own window.
-            if (live && k < end) {
-                uint32_t cur = cell_of(tt[k], scale);
-                const uint32_t s0 = mod_nb(cur, unb, inv_nb);
-                const uint32_t base = cur - s0;
-                uint32_t slot = s0;
-                double2 acc = lvw[slot];
-                uint32_t cnt = 0;  // the run's observations, added to the bin's count at its end
-                for (int j = k; j < end; j++) {
-                    const uint32_t cj = cell_of(tt[j], scale);
-                    if (cj != cur) {
-                        lvw[slot] = acc;
-                        atomicAdd(&lc[slot], cnt);
-                        cnt = 0;
-                        const uint32_t b = cj - base;
-                        slot = b >= unb ? b - unb : b;
-                        cur = cj;
-                        acc = lvw[slot];
-                    }
-                    acc.x = __dadd_rn(acc.x, tt[j + F]);
-                    acc.y = __dadd_rn(acc.y, tt[j + 2 * F]);
-                    cnt += 1u;
-                }
-                lvw[slot] = acc;
-                atomicAdd(&lc[slot], cnt);
-            }
+            // Short segments: each lane walks its own window(s).
+            if (live && k < end) walk_window(tt, F, k, end, scale, unb, inv_nb, lvw, lc);
+            if constexpr (PAIR)
+                if (live_b && kb < end_b) walk_window(tt, F, kb, end_b, scale_b, unb, inv_nb, lvw_b, lc_b);
         } else {
         // Lockstep walk: at step i every lane whose window [k, end) holds
         // observation seg * R + i reads and folds it (R odd, so the lanes'
-        // reads fall in distinct banks). Entering a cell takes the
-        // bin's sums prefetched at the previous cell change (the next cell's
-        // bin), and prefetches the bin after it. Counts are integers, so a
-        // run's count is added to its bin with one shared-memory atomic add
-        // when the run ends (no load of the bin's count).
+        // reads fall in distinct banks). Entering a cell takes the bin's sums
+        // prefetched at the previous cell change (the next cell's bin), and
+        // prefetches the bin after it. Counts are integers, so a run's count
+        // is added to its bin with one shared-memory atomic add when the run
+        // ends (no load of the bin's count). A paired lane folds each read
+        // observation into both its periods' windows that hold it.
         const int b0 = seg * R;
         const bool has = live && k < end;
-        const int steps = __reduce_max_sync(0xffffffffu, has ? end - b0 : 0);
-        if (steps > 0) {
-            uint32_t cur = 0, base = 0, slot = 0, nslot = 0, cnt = 0;
-            double2 acc = make_double2(0.0, 0.0), pre = acc;
-            if (has) {
-                cur = cell_of(tt[k], scale);
-                const uint32_t s0 = mod_nb(cur, unb, inv_nb);
-                base = cur - s0;  // bin = cell - base (- nb past the wrap)
-                slot = s0;
-                nslot = s0 + 1u == unb ? 0u : s0 + 1u;
-                acc = lvw[slot];
-                pre = lvw[nslot];
-            }
-            for (int i = 0; i < steps; i++) {
-                const int o = b0 + i;
-                // Only the lanes whose window holds o read it, so a step's
-                // reads take fewer wavefronts as lanes run out of window.
-                if (o >= k && o < end) {
-                    const double tj = tt[o], vj = tt[o + F], wj = tt[o + 2 * F];
-                    const uint32_t cj = cell_of(tj, scale);
-                    if (cj != cur) {
-                        lvw[slot] = acc;
-                        atomicAdd(&lc[slot], cnt);
-                        cnt = 0;
-                        if (cj == cur + 1u) {
-                            acc = pre;
-                            slot = nslot;
-                        } else {  // empty cells skipped
-                            const uint32_t b = cj - base;
-                            slot = b >= unb ? b - unb : b;
-                            acc = lvw[slot];
-                        }
-                        cur = cj;
-                        nslot = slot + 1u == unb ? 0u : slot + 1u;
-                        pre = lvw[nslot];
-                    }
-                    acc.x = __dadd_rn(acc.x, vj);
-                    acc.y = __dadd_rn(acc.y, wj);
-                    cnt += 1u;
+        if constexpr (!PAIR) {
+            const int steps = __reduce_max_sync(0xffffffffu, has ? end - b0 : 0);
+            if (steps > 0) {
+                RunWalker wa;
+                wa.lvw = lvw;
+                wa.lc = lc;
+                if (has) wa.open(tt[k], scale, unb, inv_nb);
+                for (int i = 0; i < steps; i++) {
+                    const int o = b0 + i;
+                    // Only the lanes whose windows hold o read it, so a step's
+                    // reads take fewer wavefronts as lanes run out of window.
+                    if (o >= k && o < end) wa.add(tt[o], tt[o + F], tt[o + 2 * F], scale, unb);
                 }
+                if (has) wa.close();
             }
-            if (has) {
-                lvw[slot] = acc;
-                atomicAdd(&lc[slot], cnt);
+        } else {
+            const bool has_b = live_b && kb < end_b;
+            const int steps =
+                __reduce_max_sync(0xffffffffu, max(has ? end - b0 : 0, has_b ? end_b - b0 : 0));
+            if (steps > 0) {
+                RunWalker wa, wb;
+                wa.lvw = lvw;
+                wa.lc = lc;
+                wb.lvw = lvw_b;
+                wb.lc = lc_b;
+                if (has) wa.open(tt[k], scale, unb, inv_nb);
+                if (has_b) wb.open(tt[kb], scale_b, unb, inv_nb);
+                for (int i = 0; i < steps; i++) {
+                    const int o = b0 + i;
+                    const bool in = o >= k && o < end;
+                    const bool in_b = o >= kb && o < end_b;
+                    if (in || in_b) {
+                        const double tj = tt[o], vj = tt[o + F], wj = tt[o + 2 * F];
+                        if (in) wa.add(tj, vj, wj, scale, unb);
+                        if (in_b) wb.add(tj, vj, wj, scale_b, unb);
+                    }
+                }
+                if (has) wa.close();
+                if (has_b) wb.close();
             }
         }
         }
@@ -828,25 +904,28 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
     return true;
 }
 
-template <int CAP>
-__global__ void __launch_bounds__(1024, 1) k_fold_walk(FoldArgs a) {
-    fold_walk_cta<CAP>(a, blockIdx.x, false, nullptr, nullptr);
+// The kernels come in two forms: one period per lane (CTAs of up to 1024
+// threads, 64 registers) and the paired walk (two periods per lane, CTAs of
+// up to 512 threads, 128 registers).
+template <int CAP, bool PAIR>
+__global__ void __launch_bounds__(PAIR ? 512 : 1024, 1) k_fold_walk(FoldArgs a) {
+    fold_walk_cta<CAP, PAIR>(a, blockIdx.x, false, nullptr, nullptr);
 }
 
 // The walking fold with the tile scan and merge fused (launch_fold_scan).
-template <int CAP>
-__global__ void __launch_bounds__(1024, 1) k_fold_scan(FoldArgs a, const __grid_constant__ ScanArgs s,
-                                                       const __grid_constant__ MergeArgs m) {
-    fold_walk_cta<CAP>(a, blockIdx.x, false, &s, &m);
+template <int CAP, bool PAIR>
+__global__ void __launch_bounds__(PAIR ? 512 : 1024, 1) k_fold_scan(FoldArgs a, const __grid_constant__ ScanArgs s,
+                                                                    const __grid_constant__ MergeArgs m) {
+    fold_walk_cta<CAP, PAIR>(a, blockIdx.x, false, &s, &m);
 }
 
 // Many folds in one launch (the batched search): CTA c runs CTA
 // c - cta0[j] of job j, where cta0[j] <= c < cta0[j + 1]. Every job uses the
 // walking fold with TMA staging; the launch's shared memory is the largest
 // job's.
-template <int CAP>
-__global__ void __launch_bounds__(1024, 1) k_fold_walk_jobs(const FoldArgs* __restrict__ jobs,
-                                                            const int* __restrict__ cta0, int njobs) {
+template <int CAP, bool PAIR>
+__global__ void __launch_bounds__(PAIR ? 512 : 1024, 1) k_fold_walk_jobs(const FoldArgs* __restrict__ jobs,
+                                                                         const int* __restrict__ cta0, int njobs) {
     int lo = 0, hi = njobs - 1;
     const int c = blockIdx.x;
     while (lo < hi) {  // last job with cta0[j] <= c
@@ -856,17 +935,24 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk_jobs(const FoldArgs* __re
         else
             hi = mid - 1;
     }
-    fold_walk_cta<CAP>(jobs[lo], c - cta0[lo], false, jobs[lo].scan, jobs[lo].merge);
+    fold_walk_cta<CAP, PAIR>(jobs[lo], c - cta0[lo], false, jobs[lo].scan, jobs[lo].merge);
+}
+
+// One unit of the persistent grid, out of line so the fold's registers are
+// allocated as in a CTA per unit rather than around the grid's unit loop.
+template <int CAP, bool PAIR>
+__device__ __noinline__ bool fold_walk_unit(const FoldArgs& a, int cta, bool reuse) {
+    return fold_walk_cta<CAP, PAIR>(a, cta, reuse, a.scan, a.merge);
 }
 
 // The same jobs as k_fold_walk_jobs, by a persistent grid (one CTA per SM)
 // that steals work: each CTA takes the next unit (one walking-fold CTA's
 // periods of one job) from a global counter until none is left. A CTA whose
 // staging wait gave up stops taking units (its copies may still be pending).
-template <int CAP>
-__global__ void __launch_bounds__(1024, 1) k_fold_walk_steal(const FoldArgs* __restrict__ jobs,
-                                                             const int* __restrict__ cta0, int njobs, int units,
-                                                             unsigned int* __restrict__ next) {
+template <int CAP, bool PAIR>
+__global__ void __launch_bounds__(PAIR ? 512 : 1024, 1) k_fold_walk_steal(const FoldArgs* __restrict__ jobs,
+                                                                          const int* __restrict__ cta0, int njobs,
+                                                                          int units, unsigned int* __restrict__ next) {
     __shared__ int s_unit;
     for (bool reuse = false;; reuse = true) {
         if (threadIdx.x == 0) s_unit = (int)atomicAdd(next, 1u);
@@ -882,7 +968,7 @@ __global__ void __launch_bounds__(1024, 1) k_fold_walk_steal(const FoldArgs* __r
             else
                 hi = mid - 1;
         }
-        if (!fold_walk_cta<CAP>(jobs[lo], u - cta0[lo], reuse, jobs[lo].scan, jobs[lo].merge)) return;
+        if (!fold_walk_unit<CAP, PAIR>(jobs[lo], u - cta0[lo], reuse)) return;
         __syncthreads();  // the unit's shared memory is free before the next one
     }
 }
@@ -897,12 +983,14 @@ constexpr int WALK_CAP = 2048;
 // power-of-two group whose histograms fit beside the staging, 1024 threads.
 // Tuning (process-wide, set by fbls_set_tuning from a measured table), per nb
 // class floor(log2(nb)): the largest period group (0 = the built-in rule),
-// and for the callers that ask for it the CTA size (a power of two from 128
-// to 1024, 0 = 1024; a CTA has at least one warp per period) and the lockstep
-// threshold (0 = built-in).
+// and for the callers that ask for it the paired walk (two periods per lane,
+// CTAs of at most 512 threads, groups of at least 2), the CTA size (a power of
+// two from 128 to 1024, 0 = 1024, or 512 paired; a CTA has at least one warp
+// per lane set) and the lockstep threshold (0 = built-in).
 std::atomic<uint32_t> g_group_cap[32];
 std::atomic<uint32_t> g_threads[32];
 std::atomic<uint32_t> g_lockstep[32];
+std::atomic<uint32_t> g_pair[32];
 std::atomic<uint32_t> g_launch_periods{16384};
 std::atomic<uint32_t> g_fold_steal{0};
 std::atomic<uint32_t> g_fused_scan{0};
@@ -914,27 +1002,39 @@ uint32_t group_cap(int nb) { return g_group_cap[nb_class(nb)].load(std::memory_o
 
 bool walk_threads_ok(int t) { return t == 128 || t == 256 || t == 512 || t == 1024; }
 
-bool walk_shape(int nb, int periods, int sm_count, bool tuned, FoldShape* out) {
+bool walk_shape(int nb, int periods, int sm_count, bool tuned, FoldShape* out, bool pair_ok = true) {
     FoldShape s{};
     s.kind = FOLD_WALK;
     s.threads = 1024;
+    const int cls = nb_class(nb);
     if (tuned) {
-        const uint32_t t = g_threads[nb_class(nb)].load(std::memory_order_relaxed);
+        s.pair = pair_ok && periods >= 2 && g_pair[cls].load(std::memory_order_relaxed) != 0;
+        const uint32_t t = g_threads[cls].load(std::memory_order_relaxed);
         if (t) s.threads = (int)t;
-        s.lockstep_min = (int)g_lockstep[nb_class(nb)].load(std::memory_order_relaxed);
+        if (s.pair && s.threads > 512) s.threads = 512;
+        s.lockstep_min = (int)g_lockstep[cls].load(std::memory_order_relaxed);
     }
     const int T = s.threads;
+    const int PV = s.pair ? 2 : 1;  // periods per lane
     s.row_stride = nb | 1;
     const size_t stage = 6 * sizeof(double) * (size_t)(WALK_CAP + 2);
     const size_t hist_per = (size_t)s.row_stride * BIN_BYTES;
-    auto starts = [&](int g) { return ((size_t)g * (T / g + 1) * sizeof(int) + 15) & ~(size_t)15; };
-    if (stage + starts(1) + hist_per > MAX_FOLD_SMEM) return false;
-    int g = 1;
-    while (2 * g <= MAX_GROUP && 2 * g <= T / 32 && stage + starts(2 * g) + (size_t)(2 * g) * hist_per <= MAX_FOLD_SMEM)
+    // run starts [g][NS + 1], NS = the segments of a period: 32 x (warps per lane set)
+    auto starts = [&](int g) {
+        const int sets = g / PV > 0 ? g / PV : 1;
+        return ((size_t)g * ((T / 32) / sets * 32 + 1) * sizeof(int) + 15) & ~(size_t)15;
+    };
+    if (stage + starts(PV) + (size_t)PV * hist_per > MAX_FOLD_SMEM) {
+        if (s.pair) return walk_shape(nb, periods, sm_count, tuned, out, false);
+        return false;
+    }
+    int g = PV;
+    while (2 * g <= MAX_GROUP && 2 * g <= PV * (T / 32) &&
+           stage + starts(2 * g) + (size_t)(2 * g) * hist_per <= MAX_FOLD_SMEM)
         g *= 2;
-    while (g > 1 && (g / 2 >= periods || (periods + g - 1) / g < sm_count)) g /= 2;
+    while (g > PV && (g / 2 >= periods || (periods + g - 1) / g < sm_count)) g /= 2;
     const uint32_t gcap = group_cap(nb);
-    while (gcap && g > 1 && (uint32_t)g > gcap) g /= 2;
+    while (gcap && g > PV && (uint32_t)g > gcap) g /= 2;
     s.group = g;
     s.hist_in_smem = true;
     s.window = 0;
@@ -990,6 +1090,7 @@ void set_fold_tuning(const FoldTuning& t) {
         g_group_cap[c].store(t.group_cap[c], std::memory_order_relaxed);
         g_threads[c].store(t.threads[c], std::memory_order_relaxed);
         g_lockstep[c].store(t.lockstep_min[c], std::memory_order_relaxed);
+        g_pair[c].store(t.pair[c] ? 1u : 0u, std::memory_order_relaxed);
     }
     g_launch_periods.store(t.launch_periods ? t.launch_periods : 16384u, std::memory_order_relaxed);
     g_fold_steal.store(t.steal ? 1u : 0u, std::memory_order_relaxed);
@@ -1002,6 +1103,7 @@ void get_fold_tuning(FoldTuning* t) {
         t->group_cap[c] = g_group_cap[c].load(std::memory_order_relaxed);
         t->threads[c] = g_threads[c].load(std::memory_order_relaxed);
         t->lockstep_min[c] = g_lockstep[c].load(std::memory_order_relaxed);
+        t->pair[c] = g_pair[c].load(std::memory_order_relaxed);
     }
     t->launch_periods = g_launch_periods.load(std::memory_order_relaxed);
     t->steal = g_fold_steal.load(std::memory_order_relaxed);
@@ -1045,37 +1147,61 @@ int fold_chunks(const double* time, int n, double scale_max, int nb, int span_ca
     return count;
 }
 
-cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads, size_t smem,
-                             cudaStream_t stream) {
-    if (njobs < 1 || ctas < 1 || smem > MAX_FOLD_SMEM || !walk_threads_ok(threads)) return cudaErrorInvalidValue;
+// A CTA size and form of the walking fold: a power of two from 128 to 1024
+// threads, at most 512 paired.
+static bool walk_form_ok(int threads, bool pair) { return walk_threads_ok(threads) && (!pair || threads <= 512); }
+
+// A group within a walking-fold shape's CTA: a power of two up to MAX_GROUP,
+// at least one warp per lane set (a period, or a pair of periods).
+static bool walk_group_ok(int group, const FoldShape& shape) {
+    return shape.kind == FOLD_WALK && walk_form_ok(shape.threads, shape.pair) && group == shape.group &&
+           group >= (shape.pair ? 2 : 1) && group <= MAX_GROUP && (group & (group - 1)) == 0 &&
+           (shape.pair ? group / 2 : group) <= shape.threads / 32 && shape.smem <= MAX_FOLD_SMEM;
+}
+
+template <bool PAIR>
+static cudaError_t launch_fold_jobs_t(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads,
+                                      size_t smem, cudaStream_t stream) {
     // Set at every launch: the attribute belongs to the module loaded in the
     // current context, which a cudaDeviceReset replaces.
-    const cudaError_t e = cudaFuncSetAttribute(k_fold_walk_jobs<WALK_CAP>,
+    const cudaError_t e = cudaFuncSetAttribute(k_fold_walk_jobs<WALK_CAP, PAIR>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
     if (e != cudaSuccess) return e;
-    k_fold_walk_jobs<WALK_CAP><<<ctas, threads, smem, stream>>>(jobs, cta0, njobs);
+    k_fold_walk_jobs<WALK_CAP, PAIR><<<ctas, threads, smem, stream>>>(jobs, cta0, njobs);
     return cudaGetLastError();
 }
 
-cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, int threads, size_t smem,
-                              unsigned int* counter, int sm_count, cudaStream_t stream) {
-    if (njobs < 1 || units < 1 || smem > MAX_FOLD_SMEM || !counter || sm_count < 1 || !walk_threads_ok(threads))
-        return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(k_fold_walk_steal<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)MAX_FOLD_SMEM);
+cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads, bool pair,
+                             size_t smem, cudaStream_t stream) {
+    if (njobs < 1 || ctas < 1 || smem > MAX_FOLD_SMEM || !walk_form_ok(threads, pair)) return cudaErrorInvalidValue;
+    return pair ? launch_fold_jobs_t<true>(jobs, cta0, njobs, ctas, threads, smem, stream)
+                : launch_fold_jobs_t<false>(jobs, cta0, njobs, ctas, threads, smem, stream);
+}
+
+template <bool PAIR>
+static cudaError_t launch_fold_steal_t(const FoldArgs* jobs, const int* cta0, int njobs, int units, int threads,
+                                       size_t smem, unsigned int* counter, int sm_count, cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(k_fold_walk_steal<WALK_CAP, PAIR>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream);
     if (e != cudaSuccess) return e;
     const int grid = units < sm_count ? units : sm_count;
-    k_fold_walk_steal<WALK_CAP><<<grid, threads, smem, stream>>>(jobs, cta0, njobs, units, counter);
+    k_fold_walk_steal<WALK_CAP, PAIR><<<grid, threads, smem, stream>>>(jobs, cta0, njobs, units, counter);
     return cudaGetLastError();
+}
+
+cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, int threads, bool pair,
+                              size_t smem, unsigned int* counter, int sm_count, cudaStream_t stream) {
+    if (njobs < 1 || units < 1 || smem > MAX_FOLD_SMEM || !counter || sm_count < 1 || !walk_form_ok(threads, pair))
+        return cudaErrorInvalidValue;
+    return pair ? launch_fold_steal_t<true>(jobs, cta0, njobs, units, threads, smem, counter, sm_count, stream)
+                : launch_fold_steal_t<false>(jobs, cta0, njobs, units, threads, smem, counter, sm_count, stream);
 }
 
 // The walking-fold limits on everything but the outputs.
 static bool fold_job_ok_rows(const FoldArgs& a, const FoldShape& shape) {
-    return shape.kind == FOLD_WALK && shape.smem <= MAX_FOLD_SMEM && a.group == shape.group && a.group >= 1 &&
-           a.group <= MAX_GROUP && (a.group & (a.group - 1)) == 0 && walk_threads_ok(shape.threads) &&
-           a.group <= shape.threads / 32 && a.lockstep_min >= 0 && a.nchunks >= 1 && a.nb >= 2 &&
+    return walk_group_ok(a.group, shape) && a.lockstep_min >= 0 && a.nchunks >= 1 && a.nb >= 2 &&
            a.stage_field == WALK_CAP + 2 && shape.chunk_cap == WALK_CAP && a.row_stride == shape.row_stride &&
            a.row_stride >= a.nb && a.fault != nullptr && a.time && a.v && a.w && a.scales && a.chunks &&
            !(reinterpret_cast<uintptr_t>(a.time) & 15) && !(reinterpret_cast<uintptr_t>(a.v) & 15) &&
@@ -1083,9 +1209,7 @@ static bool fold_job_ok_rows(const FoldArgs& a, const FoldShape& shape) {
 }
 
 bool fold_job_ok(const FoldArgs& a, const FoldShape& shape) {
-    return shape.kind == FOLD_WALK && shape.smem <= MAX_FOLD_SMEM && a.group == shape.group && a.group >= 1 &&
-           a.group <= MAX_GROUP && (a.group & (a.group - 1)) == 0 && walk_threads_ok(shape.threads) &&
-           a.group <= shape.threads / 32 && a.lockstep_min >= 0 && a.nchunks >= 1 &&
+    return walk_group_ok(a.group, shape) && a.lockstep_min >= 0 && a.nchunks >= 1 &&
            a.nb >= 2 && a.stage_field == WALK_CAP + 2 && shape.chunk_cap == WALK_CAP &&
            a.row_stride == shape.row_stride && a.row_stride >= a.nb && a.fault != nullptr &&
            (a.hist_out == nullptr || (a.group == 1 && a.periods == 1 && a.map_out == nullptr)) &&
@@ -1132,11 +1256,18 @@ cudaError_t launch_fold_scan(const FoldArgs& a, const FoldShape& shape, const Sc
     f.cum = nullptr;
     f.cum32 = nullptr;
     if (!fold_job_ok_rows(f, shape)) return cudaErrorInvalidValue;
-    const cudaError_t e =
-        cudaFuncSetAttribute(k_fold_scan<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
-    if (e != cudaSuccess) return e;
     const int blocks = (a.periods + a.group - 1) / a.group;
-    k_fold_scan<WALK_CAP><<<blocks, shape.threads, shape.smem, stream>>>(f, s, m);
+    if (shape.pair) {
+        const cudaError_t e = cudaFuncSetAttribute(k_fold_scan<WALK_CAP, true>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
+        if (e != cudaSuccess) return e;
+        k_fold_scan<WALK_CAP, true><<<blocks, shape.threads, shape.smem, stream>>>(f, s, m);
+    } else {
+        const cudaError_t e = cudaFuncSetAttribute(k_fold_scan<WALK_CAP, false>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
+        if (e != cudaSuccess) return e;
+        k_fold_scan<WALK_CAP, false><<<blocks, shape.threads, shape.smem, stream>>>(f, s, m);
+    }
     return cudaGetLastError();
 }
 
@@ -1147,7 +1278,10 @@ cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t 
     {
         cudaError_t e = cudaFuncSetAttribute(k_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MAX_FOLD_SMEM);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_fold_walk<WALK_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            e = cudaFuncSetAttribute(k_fold_walk<WALK_CAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)MAX_FOLD_SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_fold_walk<WALK_CAP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)MAX_FOLD_SMEM);
         if (e != cudaSuccess) return e;
     }
@@ -1157,16 +1291,17 @@ cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t 
                       !a.map_durations || !a.map_rho))
         return cudaErrorInvalidValue;
     if (shape.kind == FOLD_WALK) {
-        if (shape.smem > MAX_FOLD_SMEM || a.group != shape.group || a.group < 1 || a.group > MAX_GROUP ||
-            (a.group & (a.group - 1)) != 0 || !walk_threads_ok(shape.threads) || a.group > shape.threads / 32 ||
-            a.lockstep_min < 0 || a.nchunks < 1 || a.nb < 2 ||
+        if (!walk_group_ok(a.group, shape) || a.lockstep_min < 0 || a.nchunks < 1 || a.nb < 2 ||
             a.stage_field != WALK_CAP + 2 || shape.chunk_cap != WALK_CAP || a.row_stride != shape.row_stride ||
             a.row_stride < a.nb || a.fault == nullptr || (a.hist_out != nullptr && a.group != 1) ||
             (reinterpret_cast<uintptr_t>(a.time) & 15) || (reinterpret_cast<uintptr_t>(a.v) & 15) ||
             (reinterpret_cast<uintptr_t>(a.w) & 15))
             return cudaErrorInvalidValue;
         const int blocks = (a.periods + a.group - 1) / a.group;
-        k_fold_walk<WALK_CAP><<<blocks, shape.threads, shape.smem, stream>>>(a);
+        if (shape.pair)
+            k_fold_walk<WALK_CAP, true><<<blocks, shape.threads, shape.smem, stream>>>(a);
+        else
+            k_fold_walk<WALK_CAP, false><<<blocks, shape.threads, shape.smem, stream>>>(a);
         return cudaGetLastError();
     }
     if (shape.smem > MAX_FOLD_SMEM || a.group != shape.group || a.group > MAX_GROUP || a.group < 1 ||

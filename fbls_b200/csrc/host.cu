@@ -448,10 +448,12 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         bool walk;
         bool fused;  // a walking fold that scans its own tiles (no rows in device memory)
     };
-    // A wave's walking-fold jobs run as one launch per CTA size: job range
+    // A wave's walking-fold jobs run as one launch per CTA size and form: job range
     // [j0, j0 + njobs) with its CTA offsets at fc0 (njobs + 1 entries).
     struct FoldLaunch {
-        int threads, j0, njobs, fc0, ctas;
+        int threads;
+        bool pair;
+        int j0, njobs, fc0, ctas;
         size_t smem;
     };
     struct Wave {
@@ -499,9 +501,9 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
                 w.fold_jobs++;
                 FoldLaunch* fl = nullptr;
                 for (FoldLaunch& f : w.folds)
-                    if (f.threads == p.shape.threads) fl = &f;
+                    if (f.threads == p.shape.threads && f.pair == p.shape.pair) fl = &f;
                 if (!fl) {
-                    w.folds.push_back({p.shape.threads, 0, 0, 0, 0, 0});
+                    w.folds.push_back({p.shape.threads, p.shape.pair, 0, 0, 0, 0, 0});
                     fl = &w.folds.back();
                 }
                 fl->njobs++;
@@ -649,7 +651,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             ma.flags_out = reinterpret_cast<uint32_t*>(dout + p.out_off + p.out_flags);
             if (un.walk) {
                 size_t g = 0;
-                while (w.folds[g].threads != p.shape.threads) g++;
+                while (w.folds[g].threads != p.shape.threads || w.folds[g].pair != p.shape.pair) g++;
                 const FoldLaunch& fl = w.folds[g];
                 const int j = fl.j0 + nf[g];
                 if (un.fused) {
@@ -699,11 +701,11 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             const int* cta0 = reinterpret_cast<const int*>(din + in_total + w.off_fcta) + fl.fc0;
             if (tuned_fold_steal()) {
                 CK(ensure(ctx->steal, sizeof(unsigned int)), "workspace");
-                CK(launch_fold_steal(jobs, cta0, fl.njobs, fl.ctas, fl.threads, fl.smem, as<unsigned int>(ctx->steal),
-                                     ctx->sm_count, s),
+                CK(launch_fold_steal(jobs, cta0, fl.njobs, fl.ctas, fl.threads, fl.pair, fl.smem,
+                                     as<unsigned int>(ctx->steal), ctx->sm_count, s),
                    "fold");
             } else {
-                CK(launch_fold_jobs(jobs, cta0, fl.njobs, fl.ctas, fl.threads, fl.smem, s), "fold");
+                CK(launch_fold_jobs(jobs, cta0, fl.njobs, fl.ctas, fl.threads, fl.pair, fl.smem, s), "fold");
             }
             ctx->counters.launches += 1;
         }

@@ -351,7 +351,7 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
         if (w.fold_jobs) {
             CK(launch_fold_jobs(reinterpret_cast<const FoldArgs*>(din + w.off_fold),
                                 reinterpret_cast<const int*>(din + w.off_fcta), w.fold_jobs, w.fold_ctas, 1024,
-                                w.smem, s),
+                                false, w.smem, s),
                "fold");
             ctx->counters.launches += 1;
         }

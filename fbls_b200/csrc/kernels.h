@@ -83,6 +83,7 @@ struct FoldShape {
     int stage_field;    // staged slots per field: chunk_cap + segments
     size_t smem;        // dynamic shared memory bytes
     int lockstep_min;   // FOLD_WALK: FoldArgs::lockstep_min for this shape (0: built-in)
+    bool pair;          // FOLD_WALK: the paired walk (two periods per lane; group >= 2, <= 512 threads)
 };
 
 // Measured tuning of the fold's launch shape (process-wide): per nb class
@@ -94,6 +95,7 @@ struct FoldTuning {
     uint32_t group_cap[32];
     uint32_t threads[32];
     uint32_t lockstep_min[32];
+    uint32_t pair[32];
     uint32_t launch_periods;
     uint32_t steal;
     uint32_t fused_scan;  // nonzero: the walking fold scans and merges its own tiles (else separate kernels)
@@ -255,13 +257,14 @@ bool fused_scan_ok(const FoldArgs& a, const ScanArgs& s, const MergeArgs& m);
 bool fold_smem_job_ok(const FoldArgs& a, const FoldShape& shape);
 cudaError_t launch_fold_smem_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads, size_t smem,
                                   cudaStream_t stream);
-// Walking-fold jobs of one CTA size (`threads`, of their shapes).
-cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads, size_t smem,
-                             cudaStream_t stream);
+// Walking-fold jobs of one CTA size and form (`threads`, `pair`, of their
+// shapes).
+cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, int ctas, int threads, bool pair,
+                             size_t smem, cudaStream_t stream);
 // The same fold jobs by a persistent grid of one CTA per SM taking units
 // from `counter` (device memory, zeroed by the launch).
-cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, int threads, size_t smem,
-                              unsigned int* counter, int sm_count, cudaStream_t stream);
+cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, int threads, bool pair,
+                              size_t smem, unsigned int* counter, int sm_count, cudaStream_t stream);
 cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, cudaStream_t stream);
 cudaError_t launch_merge_jobs(const MergeArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream);
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream);

@@ -122,6 +122,8 @@ extern "C" int fbls_set_tuning(const fbls_tuning* tuning) {
         t.group_cap[c] = g;
         t.threads[c] = th;
         t.lockstep_min[c] = l;
+        if (tuning->fold_pair[c] > 1) return FBLS_ERR_ARGUMENT;
+        t.pair[c] = tuning->fold_pair[c];
     }
     t.launch_periods = tuning->launch_periods;
     t.steal = tuning->fold_steal;
@@ -140,6 +142,7 @@ extern "C" int fbls_get_tuning(fbls_tuning* tuning) {
         tuning->fold_group_max[c] = t.group_cap[c];
         tuning->fold_threads[c] = t.threads[c];
         tuning->lockstep_min[c] = t.lockstep_min[c];
+        tuning->fold_pair[c] = t.pair[c];
     }
     tuning->launch_periods = t.launch_periods;
     tuning->fold_steal = t.steal;

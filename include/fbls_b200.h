@@ -264,7 +264,10 @@ int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
  * memory), instead of the separate scan and merge kernels over prefix rows
  * the fold writes to device memory (the default, faster on B200).
  * map_lockstep_min: lockstep_min of the coarse maps' folds (their binned
- * families walk short segments), one value for every nb.
+ * families walk short segments), one value for every nb. fold_pair, per nb
+ * class of the signal-search folds: nonzero walks two periods per lane, one
+ * read of each staged observation serving both (CTAs of at most 512
+ * threads; 512 when fold_threads is 0).
  * Process-wide; results do not depend on it, only the launch shapes do. */
 typedef struct {
     uint32_t fold_group_max[32];
@@ -274,6 +277,7 @@ typedef struct {
     uint32_t lockstep_min[32];
     uint32_t fused_scan;
     uint32_t map_lockstep_min;
+    uint32_t fold_pair[32];
 } fbls_tuning;
 int fbls_set_tuning(const fbls_tuning* tuning);
 int fbls_get_tuning(fbls_tuning* tuning);

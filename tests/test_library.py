@@ -180,7 +180,8 @@ def test_tuning_table_round_trip_and_limits():
     from fbls_b200 import autotune
     try:
         table = {"fold_group_max": {"10": 4, "11": 2}, "fold_threads": {"10": 512, "11": 256},
-                 "lockstep_min": {"10": 7}, "launch_periods": 8192, "fold_steal": 1, "fused_scan": 1,
+                 "lockstep_min": {"10": 7}, "fold_pair": {"9": 1}, "launch_periods": 8192, "fold_steal": 1,
+                 "fused_scan": 1,
                  "map_lockstep_min": 3}
         autotune.apply(table)
         assert autotune.current() == table
@@ -194,5 +195,6 @@ def test_tuning_table_round_trip_and_limits():
             autotune.apply({"lockstep_min": {"10": 5000}})
     finally:
         autotune.reset()
-    assert autotune.current() == {"fold_group_max": {}, "fold_threads": {}, "lockstep_min": {}, "launch_periods": 16384,
+    assert autotune.current() == {"fold_group_max": {}, "fold_threads": {}, "lockstep_min": {}, "fold_pair": {},
+                                  "launch_periods": 16384,
                                   "fold_steal": 0, "fused_scan": 0, "map_lockstep_min": 0}
