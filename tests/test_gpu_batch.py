@@ -195,20 +195,24 @@ def test_fused_tile_scan_equals_the_separate_kernels(gpu, mode):
     out = {}
     try:
         dev = gpu.upload(st)
-        for sep in (1, 0):
-            autotune.apply({**saved, "fused_scan": sep})
+        # (fused, steal): fused scans in a CTA per unit and in the persistent
+        # work-stealing grid (one launch covering fold, scan and merge).
+        for fused, steal in ((0, 0), (1, 0), (1, 1)):
+            autotune.apply({**saved, "fused_scan": fused, "fold_steal": steal})
             banks = [gpu.scan_bank(dev, b["periods"][:3000], api.bank_for(b, cfg), nb, precision_mode=mode)
                      for b in bands for nb in (b["nb"] // 2, b["nb"])]
             rows = gpu.signal_search(st, cfg, dev=dev)
             batch = gpu.search_batch([s for s, _ in stars], base, period_max=[p for _, p in stars], workers=0)
-            out[sep] = (banks, rows, batch)
+            out[(fused, steal)] = (banks, rows, batch)
         dev.free()
     finally:
         autotune.apply(saved)
-    (b1, r1, s1), (b0, r0, s0) = out[1], out[0]
-    for x, y in zip(b1, b0):
-        for u, v in zip(x[:4], y[:4]):
-            assert np.array_equal(u, v, equal_nan=True)
-    assert np.array_equal(r1[0], r0[0]) and r1[1] == r0[1]
-    for (x, gx, tx), (y, gy, ty) in zip(s1, s0):
-        assert np.array_equal(x, y) and gx == gy and tx == ty
+    b0, r0, s0 = out[(0, 0)]
+    for key in ((1, 0), (1, 1)):
+        b1, r1, s1 = out[key]
+        for x, y in zip(b1, b0):
+            for u, v in zip(x[:4], y[:4]):
+                assert np.array_equal(u, v, equal_nan=True)
+        assert np.array_equal(r1[0], r0[0]) and r1[1] == r0[1]
+        for (x, gx, tx), (y, gy, ty) in zip(s1, s0):
+            assert np.array_equal(x, y) and gx == gy and tx == ty
