@@ -441,10 +441,13 @@ class Gpu:
         return out
 
     def coarse_features(self, devs: Sequence[DeviceReady], periods: Sequence, durations: Sequence, rho: Sequence,
-                        offsets: Sequence[int], T: int, oversample: float = 2.0, bin_days: float = 0.0) -> np.ndarray:
+                        offsets: Sequence[int], T: int, oversample: float = 2.0, bin_days: float = 0.0,
+                        device: bool = False):
         """The proposal network's input (channels, len(devs), T) float32: each
         star's coarse map (channels = its durations), log1p'd and standardised
-        per channel, at positions [offset, offset + len(periods)) of its row."""
+        per channel, at positions [offset, offset + len(periods)) of its row.
+        device=True returns it as a torch tensor on the context's GPU (copied
+        there device to device), else as a numpy array."""
         count = len(devs)
         channels = len(durations[0]) if count else 1
         jobs = (N.MapJob * max(count, 1))()
@@ -458,9 +461,15 @@ class Gpu:
             j.oversample = float(oversample)
             j.bin_days = float(bin_days)
         offs = np.ascontiguousarray(offsets, dtype=np.uint32)
-        x = np.empty((channels, count, T), dtype=np.float32)
+        if device:
+            import torch
+            x = torch.empty((channels, count, T), dtype=torch.float32, device=f"cuda:{self.device}")
+            ptr = C.cast(C.c_void_p(x.data_ptr()), C.POINTER(C.c_float))
+        else:
+            x = np.empty((channels, count, T), dtype=np.float32)
+            ptr = x.ctypes.data_as(C.POINTER(C.c_float))
         self._check(self.lib.fbls_coarse_features(self.ctx, jobs, count, offs.ctypes.data_as(N.c_uint32_p),
-                                                  channels, T, x.ctypes.data_as(C.POINTER(C.c_float))))
+                                                  channels, T, ptr))
         return x
 
     def search_batch(self, states: Sequence[FamilyState], cfg: SearchConfig, period_max: Optional[Sequence[float]] = None,

@@ -519,7 +519,8 @@ int fbls_coarse_features(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, cons
     if (rc) return rc;
     for (uint32_t i = 0; i < count; i++)
         if (jobs[i].status) return fail(ctx, jobs[i].status, "map " + std::to_string(i) + ": " + errors[i]);
-    CK(cudaMemcpyAsync(x, ctx->feat.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream), "download");
+    // x is host or device memory (unified addressing tells the copy which).
+    CK(cudaMemcpyAsync(x, ctx->feat.ptr, bytes, cudaMemcpyDefault, ctx->stream), "copy features");
     CK(cudaStreamSynchronize(ctx->stream), "map features");
     return FBLS_OK;
 }

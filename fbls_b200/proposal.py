@@ -335,10 +335,11 @@ def top_band(rows: np.ndarray) -> int:
     return band_of(float(rows[int(np.argmax(rows[:, 3])), 0]))
 
 
-def features(gpu, stars, devs, bin_days: float = 0.0) -> np.ndarray:
+def features(gpu, stars, devs, bin_days: float = 0.0, device: bool = False):
     """(4, count, T_IN) float32, channel-major: every star's coarse map and
     its features in one fbls_coarse_features call (map_features on the
-    device)."""
+    device); a numpy array, or with device=True a torch tensor left on the
+    GPU for the network."""
     periods, ds, rs, offsets = [], [], [], []
     banks = {}
     for st, pmax in stars:
@@ -351,7 +352,7 @@ def features(gpu, stars, devs, bin_days: float = 0.0) -> np.ndarray:
         ds.append(d)
         rs.append(r)
         offsets.append(i0)
-    return gpu.coarse_features(devs, periods, ds, rs, offsets, T_IN, 2.0, bin_days)
+    return gpu.coarse_features(devs, periods, ds, rs, offsets, T_IN, 2.0, bin_days, device=device)
 
 
 def train(net: Net, x: np.ndarray, y: np.ndarray, epochs: int = 30, batch: int = 128, lr: float = 2e-3,
@@ -397,15 +398,21 @@ def _inference_graph(net: Net, batch: int):
     return net._graphs[batch]
 
 
-def scores(net: Net, x: np.ndarray, batch: int = 256, graph: bool = True) -> np.ndarray:
+def scores(net: Net, x, batch: int = 256, graph: bool = True) -> np.ndarray:
     """Band logits (count, BANDS): the forward pass in batches, replayed from
-    a captured CUDA graph (graph=False launches the kernels one by one)."""
+    a captured CUDA graph (graph=False launches the kernels one by one). x is
+    a numpy array or a torch tensor on the network's GPU (features(...,
+    device=True)), which is read there without a copy through the host."""
     torch = net.torch
     out = []
     if graph:
         g, xin, logits = _inference_graph(net, batch)
+    on_device = isinstance(x, torch.Tensor)
     for s in range(0, x.shape[1], batch):
-        xb = torch.from_numpy(np.ascontiguousarray(x[:, s:s + batch, :])).to(net.dev)
+        if on_device:
+            xb = x[:, s:s + batch, :]
+        else:
+            xb = torch.from_numpy(np.ascontiguousarray(x[:, s:s + batch, :])).to(net.dev)
         n = xb.shape[1]
         if graph:
             xin[:, :n].copy_(xb)
@@ -465,7 +472,7 @@ def search_proposed(gpu, net: Net, stars, devs, cfg, k: int = TOP_BANDS, workers
     job launches). Returns the batch results and logits."""
     import time
     t0 = time.perf_counter()
-    x = features(gpu, stars, devs, getattr(net, "bin_days", 0.0))
+    x = features(gpu, stars, devs, getattr(net, "bin_days", 0.0), device=True)
     t1 = time.perf_counter()
     logits = scores(net, x)
     ranges = [ranges_for(l, k) for l in logits]

@@ -382,7 +382,9 @@ int fbls_coarse_map_batch(fbls_ctx* ctx, fbls_map_job* jobs, uint32_t count, uin
 
 /* The proposal network's input for a batch of stars: every job's coarse map
  * (as fbls_coarse_map_batch with workers == 0; a job's `out` may be null) and
- * x (host, channels x count x T floats, channel-major): row i of channel c
+ * x (channels x count x T floats, channel-major; host memory, or device
+ * memory of the context's device, which the features are copied to without
+ * leaving the GPU; ready when the call returns): row i of channel c
  * holds (log1p(max(map, 0)) - mean) / (std + 1e-3) of the job's P map values
  * of duration c at positions [offsets[i], offsets[i] + P), with mean and
  * (population) std over those P values, and zeros elsewhere and for maps of

@@ -190,6 +190,9 @@ def test_features_are_the_standardised_maps(gpu, bin_days):
     devs = [gpu.upload(s) for s, _ in stars]
     x = pr.features(gpu, stars, devs, bin_days=bin_days)
     assert x.shape == (pr.MAP_CHANNELS, len(stars), pr.T_IN)
+    # the same features copied device to device into a torch tensor
+    xd = pr.features(gpu, stars, devs, bin_days=bin_days, device=True)
+    assert xd.is_cuda and np.array_equal(xd.cpu().numpy(), x)
     p = pr.map_periods()
     for i, ((st, pmax), dev) in enumerate(zip(stars, devs)):
         assert np.array_equal(x[:, i, :], pr.star_map(gpu, dev, st, pmax, bin_days))
@@ -261,3 +264,6 @@ def test_graph_captured_inference_equals_launched_inference(gpu):
     b = pr.scores(net, x, batch=16, graph=False)
     assert a.shape == (40, pr.BANDS)
     assert np.array_equal(a, b)
+    # the input as a device tensor: the same logits
+    c = pr.scores(net, torch.from_numpy(x).to(net.dev), batch=16, graph=True)
+    assert np.array_equal(a, c)
