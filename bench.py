@@ -371,14 +371,19 @@ def run_gpu(args):
     fold_ms_per = ctr["fold_ms"] / fold_launches
     fold_bytes_per = ctr["fold_bytes"] / fold_launches
     achieved = fold_bytes_per / (fold_ms_per * 1e-3) / 1e9 if fold_ms_per > 0 else 0.0
-    # DRAM bytes per fold launch, from the committed ncu launch list of this
-    # workload (measured once, not in this run).
+    # DRAM bytes per fold launch: one committed ncu capture of a smaller
+    # launch of this kernel (measured once, not in this run) scaled to this
+    # run's mean launch by what grows with it: the prefix rows written and
+    # the periods folded.
     traffic = None
     prof = ROOT / "profiles" / "fold_traffic.json"
-    if prof.exists() and args.period_oversample is None:  # captured on the default grid
+    if prof.exists() and not fused:
         try:
-            traffic = json.loads(prof.read_text()).get(args.workload)
-        except (OSError, ValueError):
+            rates = json.loads(prof.read_text())
+            rows_per_launch = (ctr["fold_bytes"] - 24.0 * ctr["fold_updates"]) / fold_launches
+            periods_per_launch = ctr["fold_updates"] / state.n / fold_launches
+            traffic = int(rates["write_per_row_byte"] * rows_per_launch + rates["read_per_period"] * periods_per_launch)
+        except (OSError, ValueError, KeyError):
             traffic = None
 
     if rank != 0:
@@ -402,13 +407,17 @@ def run_gpu(args):
                      "algorithmic_bytes_per_launch": fold_bytes_per, "launch_ms": fold_ms_per,
                      "l2": {"peak": l2_peak, "frac": achieved / l2_peak if l2_peak > 0 else None,
                             "peak_kind": f"measured here: copy of a {l2_mib} MiB buffer pair that stays in L2"},
-                     "limiter": {"pipe": "shared memory", "wavefronts_frac_of_peak": 0.763,
-                                 "wavefronts_per_update": 0.90, "dram_frac_of_peak": 0.017,
+                     "traffic_source": "one ncu capture of an nb-1536 launch scaled to this run's mean launch "
+                                       "(profiles/fold_traffic.json)",
+                     "limiter": {"pipe": "shared memory and issue", "wavefronts_frac_of_peak": 0.639,
+                                 "wavefronts_per_update": 0.61, "issue_active_frac": 0.697,
+                                 "dram_frac_of_peak": 0.021,
                                  "source": "ncu --set full of one nb-1536 launch of this workload "
                                            "(profiles/k_fold_walk_multi_sector.md)"},
                      "note": "algorithmic bytes count the observation stream once per period (24 n B); it is "
                              "served from L2 and shared memory, and the kernel is bound by the shared-memory "
-                             "pipe (76 % of its wavefront peak in an ncu capture; 1.7 % of DRAM peak)"},
+                             "pipe (64 % of its wavefront peak) and instruction issue (70 %) in an ncu capture; "
+                             "2 % of DRAM peak"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": e2e_total / args.steps, "step_ms": [round(t, 2) for t in e2e_ms],
                 "rows_equal_resident": bool(np.array_equal(rows_e, rows))},
