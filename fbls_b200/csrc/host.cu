@@ -1076,8 +1076,9 @@ int search_batch_fused(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fb
     const double budget_mib = fold_budget_mib(cfg->max_fold_mib);
     if (cfg->precision_mode > 2) return fail(ctx, FBLS_ERR_ARGUMENT, "precision_mode must be 0, 1 or 2");
     const int mode = scan_mode(cfg->precision_mode);
-    // A star's grid length, from the sizes alone (0 when its inputs are bad):
-    // what the groups are cut by.
+    // A star's grid length, from the sizes alone (0 when its inputs are bad),
+    // or with period ranges the grid lengths of the ranges: what the groups
+    // are cut by.
     auto grid_estimate = [&](const fbls_star& s) -> uint64_t {
         if (!s.durations || !s.nd) return 0;
         const double t_last = s.ready ? s.ready->t_last : (s.time && s.n ? s.time[s.n - 1] : 0.0);
@@ -1086,8 +1087,15 @@ int search_batch_fused(fbls_ctx* ctx, fbls_star* stars, uint32_t count, const fb
         const double maximum = rmin(std::isfinite(s.period_max) ? s.period_max : cfg->period_max, t_last);
         const double minimum = rmax(cfg->period_min, 4.0 * dmin * (1.0 + 1e-9));
         if (!(maximum > minimum) || !(dmin > 0.0)) return 0;
-        return (uint64_t)std::max<int64_t>(0, period_grid(minimum, maximum, t_last, dmin, cfg->period_oversample,
-                                                          nullptr, 0));
+        auto count = [&](double lo, double hi) -> uint64_t {
+            if (!(hi > lo)) return 0;
+            return (uint64_t)std::max<int64_t>(0, period_grid(lo, hi, t_last, dmin, cfg->period_oversample, nullptr, 0));
+        };
+        if (!s.n_ranges || !s.ranges) return count(minimum, maximum);
+        uint64_t est = 0;
+        for (uint32_t r = 0; r < s.n_ranges; r++)
+            est += count(rmax(minimum, s.ranges[2 * r]), rmin(maximum, s.ranges[2 * r + 1]));
+        return est;
     };
     uint32_t i0 = 0;
     while (i0 < count) {
