@@ -254,16 +254,18 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
         # families) by lockstep threshold, on the same stars.
         from . import proposal as pr
         pstars = [(s_, p) for s_, p in stars]
-        bin_days = float(np.load(pr.WEIGHTS)["bin_days"])
+        saved = np.load(pr.WEIGHTS)
+        bin_days = float(saved["bin_days"])
+        oversample = float(saved["map_oversample"]) if "map_oversample" in saved.files else 2.0
         maps = {}
         for lm in MAP_LOCKSTEP:
             apply({**tuned, "launch_periods": out["launch_periods"], "fold_steal": out["fold_steal"],
                    "map_lockstep_min": lm})
-            pr.features(gpu, pstars, devs, bin_days)
+            pr.features(gpu, pstars, devs, bin_days, oversample=oversample)
             ts = []
             for _ in range(reps):
                 t0 = time.perf_counter()
-                pr.features(gpu, pstars, devs, bin_days)
+                pr.features(gpu, pstars, devs, bin_days, oversample=oversample)
                 ts.append(time.perf_counter() - t0)
             maps[lm] = _median(ts)
             log(f"coarse maps of {survey_stars} stars, map lockstep {lm or 'rule'}: {1e3 * maps[lm]:.1f} ms")

@@ -335,11 +335,12 @@ def top_band(rows: np.ndarray) -> int:
     return band_of(float(rows[int(np.argmax(rows[:, 3])), 0]))
 
 
-def features(gpu, stars, devs, bin_days: float = 0.0, device: bool = False):
-    """(4, count, T_IN) float32, channel-major: every star's coarse map and
-    its features in one fbls_coarse_features call (map_features on the
-    device); a numpy array, or with device=True a torch tensor left on the
-    GPU for the network."""
+def features(gpu, stars, devs, bin_days: float = 0.0, device: bool = False, oversample: float = 2.0):
+    """(4, count, T_IN) float32, channel-major: every star's coarse map
+    (phase cells of dmin / oversample over time bins of bin_days) and its
+    features in one fbls_coarse_features call (map_features on the device);
+    a numpy array, or with device=True a torch tensor left on the GPU for
+    the network."""
     periods, ds, rs, offsets = [], [], [], []
     banks = {}
     for st, pmax in stars:
@@ -352,7 +353,7 @@ def features(gpu, stars, devs, bin_days: float = 0.0, device: bool = False):
         ds.append(d)
         rs.append(r)
         offsets.append(i0)
-    return gpu.coarse_features(devs, periods, ds, rs, offsets, T_IN, 2.0, bin_days, device=device)
+    return gpu.coarse_features(devs, periods, ds, rs, offsets, T_IN, oversample, bin_days, device=device)
 
 
 def train(net: Net, x: np.ndarray, y: np.ndarray, epochs: int = 30, batch: int = 128, lr: float = 2e-3,
@@ -461,6 +462,7 @@ def load_net(device: int = 0, path=None) -> Net:
     saved = np.load(path or WEIGHTS)
     net.load(saved["weights"])
     net.bin_days = float(saved["bin_days"]) if "bin_days" in saved.files else 0.0
+    net.map_oversample = float(saved["map_oversample"]) if "map_oversample" in saved.files else 2.0
     return net
 
 
@@ -472,7 +474,8 @@ def search_proposed(gpu, net: Net, stars, devs, cfg, k: int = TOP_BANDS, workers
     job launches). Returns the batch results and logits."""
     import time
     t0 = time.perf_counter()
-    x = features(gpu, stars, devs, getattr(net, "bin_days", 0.0), device=True)
+    x = features(gpu, stars, devs, getattr(net, "bin_days", 0.0), device=True,
+                 oversample=getattr(net, "map_oversample", 2.0))
     t1 = time.perf_counter()
     logits = scores(net, x)
     ranges = [ranges_for(l, k) for l in logits]
@@ -502,6 +505,11 @@ def main(argv=None):
     ap.add_argument("--workers", type=int, default=0, help="search_batch workers of the labelling search")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--bin-minutes", type=float, default=10.0, help="time bins of the coarse map (0: none)")
+    ap.add_argument("--map-oversample", type=float, default=2.0,
+                    help="phase cells per shortest map duration of the coarse map")
+    ap.add_argument("--labels", default=None,
+                    help="band labels of these seeded stars from an earlier run (its .npz); else the exhaustive "
+                         "search makes them")
     ap.add_argument("--out", required=True)
     args = ap.parse_args(argv)
     t0 = time.time()
@@ -510,12 +518,19 @@ def main(argv=None):
     log(f"prepared {len(stars)} stars")
     with api.Gpu(0) as gpu:
         devs = [gpu.upload(s) for s, _ in stars]
-        res = gpu.search_batch([s for s, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs,
-                               workers=args.workers)
-        y = np.array([top_band(r) for r, _, _ in res])
+        if args.labels:
+            prev = np.load(args.labels)
+            if (int(prev["seed"]), int(prev["max_sectors"]), int(prev["labels"].shape[0])) != (
+                    args.seed, args.max_sectors, len(stars)):
+                raise SystemExit("--labels: made for other stars (seed, sectors or count differ)")
+            y = prev["labels"]
+        else:
+            res = gpu.search_batch([s for s, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs,
+                                   workers=args.workers)
+            y = np.array([top_band(r) for r, _, _ in res])
         log(f"exhaustive labels: {int((y >= 0).sum())} of {len(y)} stars with a detection")
         bin_days = args.bin_minutes / 1440.0
-        x = features(gpu, stars, devs, bin_days)
+        x = features(gpu, stars, devs, bin_days, oversample=args.map_oversample)
         log("coarse maps done")
         net = Net(0, seed=args.seed)
         ntr = args.train
@@ -524,7 +539,8 @@ def main(argv=None):
         rec = recall_at(lt, y[ntr:])
         log("held-out recall@k " + " ".join(f"{k}:{rec[k - 1]:.4f}" for k in (1, 2, 4, 8, 16, 32, 64)))
         np.savez(args.out, weights=net.state_dict(), recall=rec, train=ntr, test=args.test, seed=args.seed,
-                 max_sectors=args.max_sectors, epochs=args.epochs, bin_days=bin_days)
+                 max_sectors=args.max_sectors, epochs=args.epochs, bin_days=bin_days,
+                 map_oversample=args.map_oversample, labels=y.astype(np.int16))
         print(json.dumps({"recall": rec.tolist(), "labelled_test": int((y[ntr:] >= 0).sum())}))
         for d in devs:
             d.free()
