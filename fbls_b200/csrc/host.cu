@@ -512,7 +512,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
             }
             if (!fused) {
                 w.scan_units++;
-                w.scan_ctas += n * (int)tiles;
+                w.scan_ctas += n * scan_ctas_per_period((int)p.nb);
                 w.merge_total += n;
             }
             p.st.templates_scanned += (uint64_t)n * p.bank->nd * p.bank->ns * p.nb;
@@ -672,7 +672,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
                 mp[su] = mtot;
                 mtot += un.n;
                 sc[su++] = scta;
-                scta += un.n * tiles;
+                scta += un.n * scan_ctas_per_period((int)nb);
             }
             ctx->counters.fold_launches += 1;
             ctx->counters.scan_launches += 1;
