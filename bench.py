@@ -463,15 +463,25 @@ def _metric_second_half(gpu, count: int) -> dict:
 
     full, t_ex, ts_ex = timed(lambda: gpu.search_batch(states, cfg, period_max=pmax, devs=devs, workers=0))
     _, t_e2e, _ = timed(lambda: gpu.search_batch(states, cfg, period_max=pmax, workers=0), steps=1)
-    (pruned, _), t_pr, ts_pr = timed(lambda: pr.search_proposed(gpu, net, pstars, devs, cfg, k=pr.TOP_BANDS,
-                                                                workers=0))
-    hits = labelled = 0
-    for (fr, _, _), (pr_rows, _, _) in zip(full, pruned):
-        if fr.shape[0] == 0:
-            continue
-        labelled += 1
-        best = fr[int(np.argmax(fr[:, 3]))]
-        hits += int(pr_rows.shape[0] > 0 and np.array_equal(pr_rows[int(np.argmax(pr_rows[:, 3]))], best))
+    def recall(pruned):
+        hits = labelled = 0
+        for (fr, _, _), (pr_rows, _, _) in zip(full, pruned):
+            if fr.shape[0] == 0:
+                continue
+            labelled += 1
+            best = fr[int(np.argmax(fr[:, 3]))]
+            hits += int(pr_rows.shape[0] > 0 and np.array_equal(pr_rows[int(np.argmax(pr_rows[:, 3]))], best))
+        return hits, labelled
+
+    # At 99 % top-1 recall: the fewest bands whose held-out band recall
+    # reaches 0.99; and at cfg4's 32 bands.
+    k99 = pr.bands_for_recall(0.99)
+    rec_table = np.load(pr.WEIGHTS)["recall"]
+    (pruned, _), t_pr, ts_pr = timed(lambda: pr.search_proposed(gpu, net, pstars, devs, cfg, k=k99, workers=0))
+    hits, labelled = recall(pruned)
+    (pruned32, _), t_32, ts_32 = timed(lambda: pr.search_proposed(gpu, net, pstars, devs, cfg, k=pr.TOP_BANDS,
+                                                                  workers=0))
+    hits32, _ = recall(pruned32)
     trials = sum(t for _, _, t in full)
     for d in devs:
         d.free()
@@ -484,8 +494,14 @@ def _metric_second_half(gpu, count: int) -> dict:
                    "timing": "host clock around the device-synchronised fbls_search_batch (stars fused)"},
         "proposal": {"stars": count, "exhaustive_stars_per_s": count / t_ex, "proposal_stars_per_s": count / t_pr,
                      "speedup": t_ex / t_pr, "top1_recall": hits / max(labelled, 1),
-                     "stars_with_detection": labelled, "bands_searched": pr.TOP_BANDS, "bands": pr.BANDS,
+                     "stars_with_detection": labelled, "bands_searched": k99, "bands": pr.BANDS,
+                     "heldout_band_recall": float(rec_table[k99 - 1]),
+                     "bands_rule": "the fewest bands whose held-out band recall (the training run's labelled held-out "
+                                   "stars) reaches 0.99",
                      "step_ms": [round(1e3 * t, 1) for t in ts_pr],
+                     "top32": {"bands_searched": pr.TOP_BANDS, "proposal_stars_per_s": count / t_32,
+                               "speedup": t_ex / t_32, "top1_recall": hits32 / max(labelled, 1),
+                               "heldout_band_recall": float(rec_table[pr.TOP_BANDS - 1])},
                      "timing": "host clock around coarse maps + network + pruned fbls_search_batch"},
     }
 

@@ -466,6 +466,16 @@ def load_net(device: int = 0, path=None) -> Net:
     return net
 
 
+def bands_for_recall(target: float = 0.99, path=None) -> int:
+    """The fewest bands whose held-out band recall (the committed weights'
+    recall table: the exhaustive search's best band among the network's k
+    best) reaches `target`: the k at which the proposal path runs at that
+    recall."""
+    rec = np.load(path or WEIGHTS)["recall"]
+    hit = np.nonzero(rec >= target)[0]
+    return int(hit[0]) + 1 if hit.size else BANDS
+
+
 def search_proposed(gpu, net: Net, stars, devs, cfg, k: int = TOP_BANDS, workers: int = 0):
     """The proposal-pruned search of many stars: coarse maps and their
     features in one call, band scores, then the exhaustive search of each
