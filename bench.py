@@ -621,6 +621,8 @@ def run_proposal(args):
     from fbls_b200 import api
     from fbls_b200 import proposal as pr
     torch.cuda.set_device(0)
+    if args.bands is None:
+        args.bands = pr.bands_for_recall(0.99)
     stars, cfg = _survey(args.stars, 1000)
     pstars = [(s, p) for _, s, p in stars]
     gpu = api.Gpu(0)
@@ -728,10 +730,11 @@ def run_full(args):
     devs = [gpu.upload(s) for s in states]
     net = pr.load_net(0)
     pstars = list(zip(states, pmax))
+    k = args.bands if args.bands is not None else pr.bands_for_recall(0.99)
 
     def full_form():
         t0 = time.perf_counter()
-        pruned, _ = pr.search_proposed(gpu, net, pstars, devs, cfg, k=pr.TOP_BANDS, workers=0)
+        pruned, _ = pr.search_proposed(gpu, net, pstars, devs, cfg, k=k, workers=0)
         t1 = time.perf_counter()
         idx, cands, cdevs = [], [], []
         for i, (rows, _, _) in enumerate(pruned):
@@ -747,7 +750,7 @@ def run_full(args):
 
     # warm-up on a slice, then the timed full form
     sub = slice(0, min(256, len(states)))
-    pr.search_proposed(gpu, net, pstars[sub], devs[sub], cfg, k=pr.TOP_BANDS, workers=0)
+    pr.search_proposed(gpu, net, pstars[sub], devs[sub], cfg, k=k, workers=0)
     gpu.compare_batch([(states[0], 1.0)], cfg, devs=[devs[0]])
     gpu.set_kernel_timing(True)
     gpu.counters(reset=True)
@@ -791,9 +794,9 @@ def run_full(args):
         "dtype": "f64 search and evidence, bf16 network", "data": "synthetic",
         "config": {"workload": f"full: {len(states)} seeded survey stars (1-13 sectors ~ Geometric(0.4), cadence "
                                "120/200/600 s, white + AR(1) noise; 8 % boxes, 2 % eclipsing-binary-like pairs "
-                               "with unequal depths 1-20 %); proposal (32 of 1024 bands) -> pruned search -> "
+                               f"with unequal depths 1-20 %); proposal ({k} of 1024 bands) -> pruned search -> "
                                "evidence of each star's best candidate",
-                   "stars": len(states), "observations": n_obs,
+                   "stars": len(states), "observations": n_obs, "bands_searched": k,
                    "boxes": sum("box" in x[2] for x in stars), "pairs": sum("pair" in x[2] for x in stars)},
         "seconds": {"proposal_and_pruned_search": t_search, "evidence": t_ev, **{k: v / 1e3 for k, v in parts_ms.items()}},
         "evidence_candidates": len(ev), "evidence_candidates_per_s": len(ev) / t_ev if t_ev > 0 else None,
@@ -1234,8 +1237,9 @@ def main():
     ap.add_argument("--batch-workers", type=int, default=0,
                     help="survey / proposal workloads: search_batch host worker threads (0: stars fused into "
                          "job launches)")
-    ap.add_argument("--bands", type=int, default=32,
-                    help="proposal workload: log-period bands (of 1024) searched per star")
+    ap.add_argument("--bands", type=int, default=None,
+                    help="proposal and full workloads: log-period bands (of 1024) searched per star (default: the "
+                         "fewest whose held-out recall reaches 0.99)")
     ap.add_argument("--period-oversample", type=float, default=None,
                     help="single-star workloads: period grid density (default 3; 19 gives multi_sector's ~1.2M "
                          "periods, 6.9 single_sector's ~30k)")
