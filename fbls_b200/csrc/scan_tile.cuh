@@ -653,13 +653,17 @@ __device__ __forceinline__ void scan_tile_warp(const ScanArgs& a, const Rows& ro
     WarpPassResult res = fast ? warp_pass_reduce<true>(a, rows, sc, tile) : warp_pass_exact(a, rows, sc, tile);
     const bool retry = fast && !f32_only && (res.unsafe_any || res.near_count > 1 || res.near_sensitive);
     bool bad_any = res.bad;
+    // The flags record the last pass's retry decision, as scan_tile's do: a
+    // rescan's (f64) pass never asks for another, so it is cleared there.
+    bool retry_flag = retry;
     if (retry) {
         res = warp_pass_exact(a, rows, sc, tile);  // the whole-tile f64 rescan
         bad_any = bad_any || res.bad;
+        retry_flag = false;
     }
     if ((threadIdx.x & 31) == 0)
-        write_tile_winner(a, rows, sc, f32_only, res.key, res.di, res.value, retry, bad_any, retry, out, key_out,
-                          flag_out);
+        write_tile_winner(a, rows, sc, f32_only, res.key, res.di, res.value, retry_flag, bad_any, retry, out,
+                          key_out, flag_out);
 }
 
 // Period f's record from its best tile's part (PART_STRIDE doubles), its
