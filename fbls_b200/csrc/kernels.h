@@ -265,8 +265,8 @@ cudaError_t launch_fold_jobs(const FoldArgs* jobs, const int* cta0, int njobs, i
 // from `counter` (device memory, zeroed by the launch).
 cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, int units, int threads, bool pair,
                               size_t smem, unsigned int* counter, int sm_count, cudaStream_t stream);
-// CTAs of a period's tile scan (four tiles per CTA); a scan job of n
-// periods takes n times this many CTAs of launch_scan_jobs.
+// CTAs of a period's tile scan (one per tile); a scan job of n periods
+// takes n times this many CTAs of launch_scan_jobs.
 int scan_ctas_per_period(int nb);
 cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, cudaStream_t stream);
 cudaError_t launch_merge_jobs(const MergeArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream);

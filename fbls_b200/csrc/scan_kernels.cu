@@ -13,41 +13,31 @@
 namespace fbls {
 
 // ---------------------------------------------------------------------------
-// Tile scan (kernels.rs:610-845): scan_tile_warp (scan_tile.cuh) over the
-// fold's global rows. A CTA of TILE threads is four warps, each scanning one
-// tile of the same period (tiles 4c .. 4c + 3 of CTA c of the period), after
-// the CTA fills the period's tables once.
+// Tile scan (kernels.rs:610-845): scan_tile (scan_tile.cuh) over the fold's
+// global rows, one CTA of TILE threads per (tile, period). (A warp form with
+// four lanes per thread and no barriers measured slower on B200: 128
+// registers leave 16 warps per SM; the group form keeps 32 at 64 registers.)
 // ---------------------------------------------------------------------------
 
-constexpr int TILES_PER_CTA = TILE / 32;
-
-__device__ __forceinline__ void scan_tiles_cta(const ScanArgs& a, const int group, const int f, const int tiles) {
+__device__ __forceinline__ void scan_tile_cta(const ScanArgs& a, const int tile, const int f, const int tiles) {
     __shared__ TileScratch sc;
-    fill_tile_tables(a, sc, a.scales[f], (int)threadIdx.x, TILE);
-    __syncthreads();
-    const int tile = group * TILES_PER_CTA + (int)(threadIdx.x >> 5);
-    if (tile >= tiles) return;
     GlobalRows rows;
     rows.stride = 2 * (size_t)a.nb + 1;
     rows.r64 = a.cum ? a.cum + (size_t)f * NF * rows.stride : nullptr;
     rows.r32 = a.cum32 + (size_t)f * NF * rows.stride;
     const size_t idx = (size_t)f * tiles + tile;
-    scan_tile_warp(a, rows, sc, tile, a.parts + idx * PART_STRIDE, a.keys + idx, a.flags + idx);
+    scan_tile(a, rows, CtaGroup{}, sc, tile, a.scales[f], a.parts + idx * PART_STRIDE, a.keys + idx, a.flags + idx);
 }
 
-// Tile groups of a period: ceil(tiles / TILES_PER_CTA).
-__host__ __device__ inline int tile_groups(int nb) {
-    const int tiles = (nb + TILE - 1) / TILE;
-    return (tiles + TILES_PER_CTA - 1) / TILES_PER_CTA;
+// Eight CTAs per SM (64 registers): the f32 pass keeps its state in registers;
+// the few spills are on the f64 rescan and winner paths.
+__global__ void __launch_bounds__(TILE, 8) k_scan_tiles(ScanArgs a) {
+    scan_tile_cta(a, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
-__global__ void __launch_bounds__(TILE, 4) k_scan_tiles(ScanArgs a) {
-    scan_tiles_cta(a, blockIdx.x, blockIdx.y, (a.nb + TILE - 1) / TILE);
-}
-
-// Many scans in one launch: CTA c is tile group (c - cta0[j]) % groups of
-// period (c - cta0[j]) / groups of job j, where cta0[j] <= c < cta0[j + 1].
-__global__ void __launch_bounds__(TILE, 4) k_scan_jobs(const ScanArgs* __restrict__ jobs,
+// Many scans in one launch: CTA c is tile (c - cta0[j]) % tiles of period
+// (c - cta0[j]) / tiles of job j, where cta0[j] <= c < cta0[j + 1].
+__global__ void __launch_bounds__(TILE, 8) k_scan_jobs(const ScanArgs* __restrict__ jobs,
                                                        const int* __restrict__ cta0, int njobs) {
     int lo = 0, hi = njobs - 1;
     const int c = blockIdx.x;
@@ -59,9 +49,9 @@ __global__ void __launch_bounds__(TILE, 4) k_scan_jobs(const ScanArgs* __restric
             hi = mid - 1;
     }
     const ScanArgs& a = jobs[lo];
-    const int groups = tile_groups(a.nb);
+    const int tiles = (a.nb + TILE - 1) / TILE;
     const int local = c - cta0[lo];
-    scan_tiles_cta(a, local % groups, local / groups, (a.nb + TILE - 1) / TILE);
+    scan_tile_cta(a, local % tiles, local / tiles, tiles);
 }
 
 // Best tile per period by (score, lowest key) (kernels.rs:1115-1155). Writes
@@ -128,10 +118,10 @@ cudaError_t launch_scan_all(const EventArgs& a, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-int scan_ctas_per_period(int nb) { return tile_groups(nb); }
+int scan_ctas_per_period(int nb) { return (nb + TILE - 1) / TILE; }
 
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream) {
-    dim3 grid(tile_groups(a.nb), periods);
+    dim3 grid((a.nb + TILE - 1) / TILE, periods);
     k_scan_tiles<<<grid, TILE, 0, stream>>>(a);
     return cudaGetLastError();
 }

@@ -470,202 +470,6 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const Rows& rows, c
                           key_out, flag_out);
 }
 
-// The warp form of the tile scan: one warp scans tile `tile`, thread t
-// holding the tile's lanes t, t + 32, t + 64 and t + 96, each with its own
-// state in the reference's order of updates. The tile-level shape gate, the
-// winner (largest value, then smallest key, then lowest lane) and the flag
-// reductions are warp votes and shuffles, so a tile meets no barrier; the
-// per-period tables `sc` are filled beforehand (fill_tile_tables). The same
-// winner, parts and flags as scan_tile. The f32 pre-rank and the f64 pass
-// are separate loops, so each keeps only its own lane state in registers.
-constexpr int WARP_LANES = TILE / 32;  // lanes per thread
-
-// One pass over the durations and shapes for the thread's lanes: FAST ranks
-// in f32 (rank_fast), else in f64 (rank_exact); every lane's state is updated
-// in the reference's order. Returns through the lane states.
-template <bool FAST, typename Rows>
-__device__ __forceinline__ void warp_pass(const ScanArgs& a, const Rows& rows, const TileScratch& sc, const int tile,
-                                          LaneState (&st)[WARP_LANES]) {
-    constexpr unsigned FULL = 0xffffffffu;
-    const int t = (int)(threadIdx.x & 31);
-    const int nb = a.nb;
-    const int nd = a.nd, ns = a.ns, layers = a.layers;
-    const double baseline = a.baseline;
-    const float basef = (float)baseline;
-    const double nobs = a.n;
-    const uint64_t nb1 = (uint64_t)nb + 1;
-    const uint32_t j0 = (uint32_t)(tile * TILE + t);
-    auto jj_of = [&](int r) { return min(j0 + 32u * (uint32_t)r, (uint32_t)(nb - 1)); };
-    float count_max = (float)(nobs - 3.0);
-    if ((double)count_max > nobs - 3.0) count_max = nextafterf(count_max, -__builtin_huge_valf());
-    const double gate_value = FAST ? __ddiv_rn(__dmul_rn(a.gate, a.gate), baseline) : a.gate;
-    float gate_f = (float)gate_value;
-    if ((double)gate_f < gate_value) gate_f = nextafterf(gate_f, __builtin_huge_valf());
-    for (int di = 0; di < nd; di++) {
-        const uint32_t k = sc.k[di];
-        const bool k_ok = sc.kok[di] != 0;
-        uint32_t usable = 0;  // bit r: lane r's box is usable
-        float oa32[WARP_LANES], ow32[WARP_LANES];
-        bool open_any = false;
-#pragma unroll
-        for (int r = 0; r < WARP_LANES; r++) {
-            const uint32_t jj = jj_of(r);
-            const bool in = j0 + 32u * (uint32_t)r < (uint32_t)nb;
-            const uint64_t key = (uint64_t)k * nb1 + jj;
-            bool open, use;
-            if (FAST) {
-                const float count = rows.i32(F_N, jj, k);
-                ow32[r] = rows.i32(F_W, jj, k);
-                oa32[r] = rows.i32(F_V, jj, k);
-                use = in && k_ok && count >= 3.0f && count <= count_max;
-                const bool valid = use && oa32[r] > 0.0f;
-                const float merit =
-                    rank_fast(st[r], oa32[r], ow32[r], ow32[r], sc.r2f[di], basef, valid, key, (uint32_t)di);
-                open = valid && merit >= gate_f;
-            } else {
-                const double count = rows.i64(F_N, jj, k);
-                const double w = rows.i64(F_W, jj, k);
-                const double av = rows.i64(F_V, jj, k);
-                use = in && k_ok && count >= 3.0 && count <= nobs - 3.0;
-                const bool valid = use && av > 0.0;
-                const double merit = rank_exact(st[r], av, w, w, sc.rho[di], baseline, valid, key, (uint32_t)di);
-                open = valid && merit >= gate_value;
-            }
-            usable |= (use ? 1u : 0u) << r;
-            open_any = open_any || open;
-        }
-        // Tile-level shape gate (kernels.rs:715-726).
-        if (!__any_sync(FULL, open_any)) continue;
-        for (int si = 1; si < ns; si++) {
-            const double ing = sc.ing[si];
-#pragma unroll
-            for (int r = 0; r < WARP_LANES; r++) {
-                const uint32_t jj = jj_of(r);
-                const uint64_t skey = ((uint64_t)si * nb1 + k) * nb1 + jj;
-                const bool use = (usable >> r) & 1u;
-                if (FAST) {
-                    float sa, shp, snorm;
-                    shape_sums32(rows, jj, k, oa32[r], ow32[r], ow32[r], ing, sc.fac, si, layers, sa, shp, snorm);
-                    rank_fast(st[r], sa, shp, snorm, sc.r2f[di], basef, use && sa > 0.0f, skey, (uint32_t)di);
-                } else {
-                    const double w = rows.i64(F_W, jj, k);
-                    const double av = rows.i64(F_V, jj, k);
-                    double sa, shp, snorm;
-                    shape_sums64(rows, jj, k, av, w, w, ing, sc.fac, si, layers, sa, shp, snorm);
-                    rank_exact(st[r], sa, shp, snorm, sc.rho[di], baseline, use && sa > 0.0, skey, (uint32_t)di);
-                }
-            }
-        }
-    }
-}
-
-// A pass's tile-level result: the winner (value, key, duration) and the
-// reductions the retry rule and the flags read.
-struct WarpPassResult {
-    double value;
-    uint64_t key;
-    uint32_t di;
-    int near_count;
-    bool near_sensitive, unsafe_any, bad;
-};
-
-// One pass (FAST: the f32 pre-rank, else f64) of the warp's tile and its
-// reductions over the tile's 128 lanes.
-template <bool FAST, typename Rows>
-__device__ __forceinline__ WarpPassResult warp_pass_reduce(const ScanArgs& a, const Rows& rows, const TileScratch& sc,
-                                                           const int tile) {
-    constexpr unsigned FULL = 0xffffffffu;
-    const int t = (int)(threadIdx.x & 31);
-    const uint64_t nb1 = (uint64_t)a.nb + 1;
-    LaneState st[WARP_LANES];
-#pragma unroll
-    for (int r = 0; r < WARP_LANES; r++) st[r].reset();
-    warp_pass<FAST>(a, rows, sc, tile, st);
-#pragma unroll
-    for (int r = 0; r < WARP_LANES; r++) {
-        if (FAST) st[r].best = (double)st[r].bestf;
-        if (FAST && st[r].best <= 0.0)
-            st[r].key = nb1 + min((uint32_t)(tile * TILE + t + 32 * r), (uint32_t)(a.nb - 1));
-    }
-    // Tile winner: largest value, then smallest key, then lowest lane, over
-    // the thread's lanes (in lane order) and then the warp.
-    double v = st[0].best;
-    unsigned long long kk = st[0].key;
-    int l = t;
-#pragma unroll
-    for (int r = 1; r < WARP_LANES; r++) {
-        const double cv = st[r].best;
-        const unsigned long long ck = st[r].key;
-        if (cv > v || (cv == v && ck < kk)) {  // a later lane of the thread wins only outright
-            v = cv;
-            kk = ck;
-            l = t + 32 * r;
-        }
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_xor_sync(FULL, v, off);
-        const unsigned long long ok = __shfl_xor_sync(FULL, kk, off);
-        const int ol = __shfl_xor_sync(FULL, l, off);
-        if (ov > v || (ov == v && (ok < kk || (ok == kk && ol < l)))) {
-            v = ov;
-            kk = ok;
-            l = ol;
-        }
-    }
-    const double guard = FAST ? 1e-5 : 1e-10;
-    int near_here = 0;
-    bool sens_here = false, unsafe_here = false, bad_here = false;
-    uint32_t di_sel = st[0].di;
-#pragma unroll
-    for (int r = 0; r < WARP_LANES; r++) {
-        const bool near_top = st[r].best > 0.0 && st[r].best >= __dmul_rn(v, __dsub_rn(1.0, guard));
-        near_here += near_top ? 1 : 0;
-        sens_here = sens_here || (near_top && st[r].sensitive);
-        unsafe_here = unsafe_here || st[r].unsafe_merit;
-        bad_here = bad_here || st[r].bad;
-        if ((l >> 5) == r) di_sel = st[r].di;  // the winning lane's duration, if it is this thread's
-    }
-    WarpPassResult res;
-    res.value = v;
-    res.key = kk;
-    res.di = __shfl_sync(FULL, di_sel, l & 31);
-    res.near_count = (int)__reduce_add_sync(FULL, (unsigned)near_here);
-    res.near_sensitive = __any_sync(FULL, sens_here);
-    res.unsafe_any = __any_sync(FULL, unsafe_here);
-    res.bad = __any_sync(FULL, bad_here);
-    return res;
-}
-
-// The f64 pass out of line: it runs for f64 ranking and for the rare retried
-// tiles, and its registers stay out of the f32 pass's allocation.
-template <typename Rows>
-__device__ __noinline__ WarpPassResult warp_pass_exact(const ScanArgs& a, const Rows& rows, const TileScratch& sc,
-                                                       const int tile) {
-    return warp_pass_reduce<false>(a, rows, sc, tile);
-}
-
-template <typename Rows>
-__device__ __forceinline__ void scan_tile_warp(const ScanArgs& a, const Rows& rows, const TileScratch& sc,
-                                               const int tile, double* out, uint64_t* key_out, uint32_t* flag_out) {
-    const bool f32_only = a.mixed == 2;
-    const bool fast = a.mixed != 0;
-    WarpPassResult res = fast ? warp_pass_reduce<true>(a, rows, sc, tile) : warp_pass_exact(a, rows, sc, tile);
-    const bool retry = fast && !f32_only && (res.unsafe_any || res.near_count > 1 || res.near_sensitive);
-    bool bad_any = res.bad;
-    // The flags record the last pass's retry decision, as scan_tile's do: a
-    // rescan's (f64) pass never asks for another, so it is cleared there.
-    bool retry_flag = retry;
-    if (retry) {
-        res = warp_pass_exact(a, rows, sc, tile);  // the whole-tile f64 rescan
-        bad_any = bad_any || res.bad;
-        retry_flag = false;
-    }
-    if ((threadIdx.x & 31) == 0)
-        write_tile_winner(a, rows, sc, f32_only, res.key, res.di, res.value, retry_flag, bad_any, retry, out,
-                          key_out, flag_out);
-}
-
 // Period f's record from its best tile's part (PART_STRIDE doubles), its
 // score and its ORed tile flags (kernels.rs:1115-1155).
 __device__ __forceinline__ void merge_record(const MergeArgs& a, const int f, const double* part, double best,
