@@ -474,8 +474,9 @@ def _metric_second_half(gpu, count: int) -> dict:
         return hits, labelled
 
     # At 99 % top-1 recall: the fewest bands whose held-out band recall
-    # reaches 0.99; and at cfg4's 32 bands.
-    k99 = pr.bands_for_recall(0.99)
+    # reaches the operating point's (proposal.OPERATING_RECALL); and at
+    # cfg4's 32 bands.
+    k99 = pr.bands_for_recall(pr.OPERATING_RECALL)
     rec_table = np.load(pr.WEIGHTS)["recall"]
     (pruned, _), t_pr, ts_pr = timed(lambda: pr.search_proposed(gpu, net, pstars, devs, cfg, k=k99, workers=0))
     hits, labelled = recall(pruned)
@@ -496,8 +497,8 @@ def _metric_second_half(gpu, count: int) -> dict:
                      "speedup": t_ex / t_pr, "top1_recall": hits / max(labelled, 1),
                      "stars_with_detection": labelled, "bands_searched": k99, "bands": pr.BANDS,
                      "heldout_band_recall": float(rec_table[k99 - 1]),
-                     "bands_rule": "the fewest bands whose held-out band recall (the training run's labelled held-out "
-                                   "stars) reaches 0.99",
+                     "bands_rule": f"the fewest bands whose held-out band recall (the training run's labelled "
+                                   f"held-out stars) reaches {pr.OPERATING_RECALL}",
                      "step_ms": [round(1e3 * t, 1) for t in ts_pr],
                      "top32": {"bands_searched": pr.TOP_BANDS, "proposal_stars_per_s": count / t_32,
                                "speedup": t_ex / t_32, "top1_recall": hits32 / max(labelled, 1),
@@ -622,7 +623,7 @@ def run_proposal(args):
     from fbls_b200 import proposal as pr
     torch.cuda.set_device(0)
     if args.bands is None:
-        args.bands = pr.bands_for_recall(0.99)
+        args.bands = pr.bands_for_recall(pr.OPERATING_RECALL)
     stars, cfg = _survey(args.stars, 1000)
     pstars = [(s, p) for _, s, p in stars]
     gpu = api.Gpu(0)
@@ -730,7 +731,7 @@ def run_full(args):
     devs = [gpu.upload(s) for s in states]
     net = pr.load_net(0)
     pstars = list(zip(states, pmax))
-    k = args.bands if args.bands is not None else pr.bands_for_recall(0.99)
+    k = args.bands if args.bands is not None else pr.bands_for_recall(pr.OPERATING_RECALL)
 
     def full_form():
         t0 = time.perf_counter()
@@ -1239,7 +1240,7 @@ def main():
                          "job launches)")
     ap.add_argument("--bands", type=int, default=None,
                     help="proposal and full workloads: log-period bands (of 1024) searched per star (default: the "
-                         "fewest whose held-out recall reaches 0.99)")
+                         "fewest whose held-out recall reaches the operating point's)")
     ap.add_argument("--period-oversample", type=float, default=None,
                     help="single-star workloads: period grid density (default 3; 19 gives multi_sector's ~1.2M "
                          "periods, 6.9 single_sector's ~30k)")

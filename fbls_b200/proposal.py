@@ -29,7 +29,13 @@ POOLS = (2, 2, 2, 1, 1, 1)
 HEAD_G = 1
 MAP_CHANNELS = 4
 ACTIVATION = "gelu"
-TOP_BANDS = 32       # bands searched per star
+TOP_BANDS = 32       # bands searched per star (cfg4's top-32)
+# The held-out band recall the operating point asks for: above the metric's
+# 99 % top-1 recall, because the held-out stars share the training stars'
+# distribution (1-4 sectors, every star injected) and survey batches reach
+# beyond it (up to 13 sectors, binary pairs): at 0.995 (3 bands) a 10,000-star
+# survey batch measured 0.983.
+OPERATING_RECALL = 0.999
 WEIGHT_DECAY = 1e-4  # AdamW, on the convolution and head weights (not the biases)
 
 
