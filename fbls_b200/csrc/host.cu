@@ -460,7 +460,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         std::vector<Unit> units;
         std::vector<FoldLaunch> folds;
         size_t cum = 0, parts = 0, hist = 0;
-        int fold_jobs = 0, scan_units = 0, scan_ctas = 0, merge_total = 0, scan_nd = 1;
+        int fold_jobs = 0, scan_units = 0, scan_ctas = 0, merge_total = 0;
         // in the job blob; the fold jobs' fused scans and merges at off_fscan
         // and off_fmerge, in fold-job order; the other units' scans and
         // merges at off_scan and off_merge
@@ -514,7 +514,6 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
                 w.scan_units++;
                 w.scan_ctas += n * scan_ctas_per_period((int)p.nb);
                 w.merge_total += n;
-                w.scan_nd = std::max(w.scan_nd, (int)p.bank->nd);
             }
             p.st.templates_scanned += (uint64_t)n * p.bank->nd * p.bank->ns * p.nb;
             p.st.batches += ((uint64_t)n + p.batch - 1) / p.batch;
@@ -742,7 +741,7 @@ int run_session_fused(fbls_ctx* ctx, std::vector<Pass>& passes, PinBuf& down_buf
         if (w.scan_units) {
             CK(launch_scan_jobs(reinterpret_cast<const ScanArgs*>(din + in_total + w.off_scan),
                                 reinterpret_cast<const int*>(din + in_total + w.off_scta), w.scan_units, w.scan_ctas,
-                                w.scan_nd, s),
+                                s),
                "scan_tiles");
             ctx->counters.launches += 1;
         }

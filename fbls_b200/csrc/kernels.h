@@ -268,9 +268,7 @@ cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, 
 // CTAs of a period's tile scan (one per tile); a scan job of n periods
 // takes n times this many CTAs of launch_scan_jobs.
 int scan_ctas_per_period(int nb);
-// The scan jobs' largest duration count sizes their box cache.
-cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, int max_nd,
-                             cudaStream_t stream);
+cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, cudaStream_t stream);
 cudaError_t launch_merge_jobs(const MergeArgs* jobs, const int* p0, int njobs, int total, cudaStream_t stream);
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream);
 cudaError_t launch_scan_all(const EventArgs& a, cudaStream_t stream);

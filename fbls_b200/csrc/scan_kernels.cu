@@ -19,30 +19,25 @@ namespace fbls {
 // registers leave 16 warps per SM; the group form keeps 32 at 64 registers.)
 // ---------------------------------------------------------------------------
 
-// Dynamic shared memory: the f32 pass's box cache, 2 nd TILE floats.
 __device__ __forceinline__ void scan_tile_cta(const ScanArgs& a, const int tile, const int f, const int tiles) {
     __shared__ TileScratch sc;
-    extern __shared__ float box[];
     GlobalRows rows;
     rows.stride = 2 * (size_t)a.nb + 1;
     rows.r64 = a.cum ? a.cum + (size_t)f * NF * rows.stride : nullptr;
     rows.r32 = a.cum32 + (size_t)f * NF * rows.stride;
     const size_t idx = (size_t)f * tiles + tile;
-    scan_tile(a, rows, CtaGroup{}, sc, tile, a.scales[f], a.parts + idx * PART_STRIDE, a.keys + idx, a.flags + idx,
-              box);
+    scan_tile(a, rows, CtaGroup{}, sc, tile, a.scales[f], a.parts + idx * PART_STRIDE, a.keys + idx, a.flags + idx);
 }
 
-size_t scan_box_bytes(int nd) { return 2 * (size_t)nd * TILE * sizeof(float); }
-
-// Seven CTAs per SM (72 registers): the f32 pass keeps its state and gate
-// masks in registers; the few spills are on the f64 rescan and winner paths.
-__global__ void __launch_bounds__(TILE, 7) k_scan_tiles(ScanArgs a) {
+// Eight CTAs per SM (64 registers): the f32 pass keeps its state in registers;
+// the few spills are on the f64 rescan and winner paths.
+__global__ void __launch_bounds__(TILE, 8) k_scan_tiles(ScanArgs a) {
     scan_tile_cta(a, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 // Many scans in one launch: CTA c is tile (c - cta0[j]) % tiles of period
 // (c - cta0[j]) / tiles of job j, where cta0[j] <= c < cta0[j + 1].
-__global__ void __launch_bounds__(TILE, 7) k_scan_jobs(const ScanArgs* __restrict__ jobs,
+__global__ void __launch_bounds__(TILE, 8) k_scan_jobs(const ScanArgs* __restrict__ jobs,
                                                        const int* __restrict__ cta0, int njobs) {
     int lo = 0, hi = njobs - 1;
     const int c = blockIdx.x;
@@ -126,14 +121,8 @@ cudaError_t launch_scan_all(const EventArgs& a, cudaStream_t stream) {
 int scan_ctas_per_period(int nb) { return (nb + TILE - 1) / TILE; }
 
 cudaError_t launch_scan_tiles(const ScanArgs& a, int periods, cudaStream_t stream) {
-    if (a.nd < 1 || a.nd > MAX_DURATIONS) return cudaErrorInvalidValue;
-    // Set at every launch (the attribute belongs to the module of the current context).
-    const size_t smem = scan_box_bytes(a.nd);
-    const cudaError_t e =
-        cudaFuncSetAttribute(k_scan_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_box_bytes(MAX_DURATIONS));
-    if (e != cudaSuccess) return e;
     dim3 grid((a.nb + TILE - 1) / TILE, periods);
-    k_scan_tiles<<<grid, TILE, smem, stream>>>(a);
+    k_scan_tiles<<<grid, TILE, 0, stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -158,13 +147,9 @@ __global__ void k_merge_jobs(const MergeArgs* __restrict__ jobs, const int* __re
     merge_period(jobs[lo], i - p0[lo]);
 }
 
-cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, int max_nd,
-                             cudaStream_t stream) {
-    if (njobs < 1 || ctas < 1 || max_nd < 1 || max_nd > MAX_DURATIONS) return cudaErrorInvalidValue;
-    const cudaError_t e =
-        cudaFuncSetAttribute(k_scan_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_box_bytes(MAX_DURATIONS));
-    if (e != cudaSuccess) return e;
-    k_scan_jobs<<<ctas, TILE, scan_box_bytes(max_nd), stream>>>(jobs, cta0, njobs);
+cudaError_t launch_scan_jobs(const ScanArgs* jobs, const int* cta0, int njobs, int ctas, cudaStream_t stream) {
+    if (njobs < 1 || ctas < 1) return cudaErrorInvalidValue;
+    k_scan_jobs<<<ctas, TILE, 0, stream>>>(jobs, cta0, njobs);
     return cudaGetLastError();
 }
 

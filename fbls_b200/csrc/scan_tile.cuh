@@ -87,25 +87,7 @@ struct SmemRows {
 };
 
 // A whole CTA of TILE threads.
-// OR of every lane's 64-bit mask over a group of TILE threads (whole warps),
-// through one slot per warp; the group meets once.
-template <typename Group>
-__device__ __forceinline__ uint64_t group_or_mask(const Group& g, uint64_t m, unsigned long long* slots) {
-    const uint32_t lo = __reduce_or_sync(0xffffffffu, (uint32_t)m);
-    const uint32_t hi = __reduce_or_sync(0xffffffffu, (uint32_t)(m >> 32));
-    const int lane = g.lane();
-    if ((lane & 31) == 0) slots[lane >> 5] = ((unsigned long long)hi << 32) | lo;
-    g.sync();
-    unsigned long long all = 0;
-#pragma unroll
-    for (int w = 0; w < TILE / 32; w++) all |= slots[w];
-    return all;
-}
-
 struct CtaGroup {
-    __device__ __forceinline__ uint64_t or_mask(uint64_t m, unsigned long long* slots) const {
-        return group_or_mask(*this, m, slots);
-    }
     __device__ __forceinline__ int lane() const { return threadIdx.x; }
     __device__ __forceinline__ void sync() const { __syncthreads(); }
     __device__ __forceinline__ bool any(bool p) const { return __syncthreads_or(p) != 0; }
@@ -116,9 +98,6 @@ struct CtaGroup {
 struct NamedGroup {
     uint32_t id;
     int base;  // first thread
-    __device__ __forceinline__ uint64_t or_mask(uint64_t m, unsigned long long* slots) const {
-        return group_or_mask(*this, m, slots);
-    }
     __device__ __forceinline__ int lane() const { return (int)threadIdx.x - base; }
     __device__ __forceinline__ void sync() const {
         asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(TILE) : "memory");
@@ -154,26 +133,17 @@ struct TileScratch {
     uint32_t k[MAX_DURATIONS];  // width min(raw, nb / 2)
     int wl[TILE / 32];
     uint32_t di;
-    unsigned long long gmask[TILE / 32];  // per warp: the durations whose shape gate a lane opens
     unsigned char kok[MAX_DURATIONS];  // raw < nb / 2
 };
 
-// f32 merit a^2 / (rho^2 (c norm - hp^2)) and whether it is in the safe
-// range (kernels.rs:389-402); it depends on the template alone.
-__device__ __forceinline__ float f32_merit(float a32, float hp32, float norm32, float rho2f, float basef,
-                                           bool& safe) {
+// f32 merit a^2 / (rho^2 (c norm - hp^2)) and the lane bookkeeping of
+// rank_fast (kernels.rs:389-425).
+__device__ __forceinline__ float rank_fast(LaneState& s, float a32, float hp32, float norm32, float rho2f,
+                                           float basef, bool valid, uint64_t key, uint32_t di) {
     float cn = __fmul_rn(basef, norm32);
     float qq = __fmul_rn(rho2f, __fsub_rn(cn, __fmul_rn(hp32, hp32)));
     float merit = __fdiv_rn(__fmul_rn(a32, a32), qq);
-    safe = cn > 0.0f && qq >= __fmul_rn(0.001f, cn) && merit >= 1e-30f && merit <= 1e30f;
-    return merit;
-}
-
-// The f32 merit and the lane bookkeeping of rank_fast (kernels.rs:389-425).
-__device__ __forceinline__ float rank_fast(LaneState& s, float a32, float hp32, float norm32, float rho2f,
-                                           float basef, bool valid, uint64_t key, uint32_t di) {
-    bool safe;
-    const float merit = f32_merit(a32, hp32, norm32, rho2f, basef, safe);
+    bool safe = cn > 0.0f && qq >= __fmul_rn(0.001f, cn) && merit >= 1e-30f && merit <= 1e30f;
     s.unsafe_merit |= valid && !safe;
     const float best = s.bestf;
     const float guard = 1e-5f;
@@ -360,7 +330,7 @@ __device__ __forceinline__ void write_tile_winner(const ScanArgs& a, const Rows&
 template <typename Rows, typename Group>
 __device__ __forceinline__ void scan_tile(const ScanArgs& a, const Rows& rows, const Group& grp, TileScratch& sc,
                                           const int tile, const double scale, double* out, uint64_t* key_out,
-                                          uint32_t* flag_out, float* box = nullptr) {
+                                          uint32_t* flag_out) {
     const int lane = grp.lane();
     const int nb = a.nb;
     const int nd = a.nd, ns = a.ns, layers = a.layers;
@@ -401,31 +371,6 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const Rows& rows, c
         // For an f32 merit m: (double)m >= gate_value exactly when m >= gate_f.
         float gate_f = (float)gate_value;
         if ((double)gate_f < gate_value) gate_f = nextafterf(gate_f, __builtin_huge_valf());
-        // With a box cache the f32 pass decides every duration's tile-level
-        // shape gate first (the gate reads the box's own merit, not the lane's
-        // ranking state) and meets the group once for all of them; the boxes'
-        // sums wait in the cache for the ranking in the reference's order.
-        const bool cached = fast && box != nullptr;
-        uint64_t usable_bits = 0, gate_bits = 0;
-        if (cached) {
-            uint64_t open_bits = 0;
-            for (int di = 0; di < nd; di++) {
-                const uint32_t k = sc.k[di];
-                const float count = rows.i32(F_N, jj, k);
-                const float w32 = rows.i32(F_W, jj, k);
-                const float a32 = rows.i32(F_V, jj, k);
-                const bool use = j < (uint32_t)nb && sc.kok[di] != 0 && count >= 3.0f && count <= count_max;
-                bool safe;
-                const float merit = f32_merit(a32, w32, w32, sc.r2f[di], basef, safe);
-                const bool valid = use && a32 > 0.0f;
-                const bool open = valid && safe && merit >= gate_f;
-                box[(2 * di) * TILE + lane] = a32;
-                box[(2 * di + 1) * TILE + lane] = w32;
-                usable_bits |= (uint64_t)use << di;
-                open_bits |= (uint64_t)open << di;
-            }
-            gate_bits = grp.or_mask(open_bits, sc.gmask);
-        }
         for (int di = 0; di < nd; di++) {
             const uint32_t k = sc.k[di];
             const bool k_ok = sc.kok[di] != 0;
@@ -433,13 +378,7 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const Rows& rows, c
             const uint64_t key = (uint64_t)k * nb1 + jj;
             bool usable, open;
             float oa32 = 0.f, ow32 = 0.f;
-            if (cached) {
-                oa32 = box[(2 * di) * TILE + lane];
-                ow32 = box[(2 * di + 1) * TILE + lane];
-                usable = (usable_bits >> di) & 1u;
-                rank_fast(st, oa32, ow32, ow32, sc.r2f[di], basef, usable && oa32 > 0.0f, key, (uint32_t)di);
-                open = false;  // decided for the tile above
-            } else if (fast) {
+            if (fast) {
                 float count = rows.i32(F_N, jj, k);
                 ow32 = rows.i32(F_W, jj, k);
                 oa32 = rows.i32(F_V, jj, k);
@@ -457,7 +396,7 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const Rows& rows, c
                 open = valid && merit >= gate_value;
             }
             // Tile-level shape gate (kernels.rs:715-726).
-            if (cached ? !((gate_bits >> di) & 1u) : !grp.any(open)) continue;
+            if (!grp.any(open)) continue;
             for (int si = 1; si < ns; si++) {
                 const double ing = sc.ing[si];
                 const uint64_t skey = ((uint64_t)si * nb1 + k) * nb1 + jj;
