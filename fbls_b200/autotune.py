@@ -3,7 +3,8 @@
 The fold's period group (periods per CTA, sharing each staged observation
 chunk) trades shared memory for histograms against CTAs per launch; the
 built-in rule takes the largest group whose histograms fit while every SM
-still gets a CTA. The CTA size sets how many lanes split a staged chunk per
+still gets a CTA; caps above 32 give a period fewer lanes than a warp (down
+to 8). The CTA size sets how many lanes split a staged chunk per
 period, hence the segment each lane walks, and the lockstep threshold picks
 between lanes stepping together (conflict-free reads, idle steps) and each
 walking its own window. This sweep measures, per nb class floor(log2(nb)),
@@ -14,7 +15,8 @@ of a search) at every allowed group cap, then at every CTA size
 and lockstep threshold, the periods per launch and the fused against the
 separate tile scan on a whole signal_search, and, on a batch of seeded
 survey stars searched together, a CTA per fold unit against the persistent
-work-stealing fold grid and the coarse maps' lockstep threshold; it writes
+work-stealing fold grid and the coarse maps' fold shape (group cap and CTA
+size, then lockstep threshold); it writes
 the fastest as a table:
 
     python -m fbls_b200.autotune --out fbls_b200/data/tuning.json
@@ -35,12 +37,14 @@ import numpy as np
 from . import _native as N
 
 TABLE = Path(__file__).resolve().parent / "data" / "tuning.json"
-GROUPS = (1, 2, 4, 8, 16, 32)
+GROUPS = (1, 2, 4, 8, 16, 32, 64, 128)
 LAUNCHES = (4096, 8192, 16384, 32768)
 THREADS = (1024, 512, 256, 128)
 PAIR_THREADS = (512, 256)
 LOCKSTEP = (0, 3, 7, 15, 4096)  # 0: the built-in 11; 4096: never in lockstep
 MAP_LOCKSTEP = (0, 3, 5, 7, 4096)
+# (group cap, CTA size) of the coarse maps' walking folds; (0, 0) the built-in
+MAP_SHAPES = ((0, 0), (16, 0), (32, 0), (64, 0), (128, 0), (32, 512), (64, 512))
 
 
 def device_name(device: int = 0) -> str:
@@ -63,6 +67,8 @@ def apply(table: dict) -> None:
     t.fold_steal = int(table.get("fold_steal", 0))
     t.fused_scan = int(table.get("fused_scan", 0))
     t.map_lockstep_min = int(table.get("map_lockstep_min", 0))
+    t.map_threads = int(table.get("map_threads", 0))
+    t.map_group_max = int(table.get("map_group_max", 0))
     rc = N.load().fbls_set_tuning(C.byref(t))
     if rc:
         raise ValueError(f"tuning table rejected (status {rc})")
@@ -76,7 +82,8 @@ def current() -> dict:
             "lockstep_min": {str(c): int(v) for c, v in enumerate(t.lockstep_min) if v},
             "fold_pair": {str(c): int(v) for c, v in enumerate(t.fold_pair) if v},
             "launch_periods": int(t.launch_periods), "fold_steal": int(t.fold_steal),
-            "fused_scan": int(t.fused_scan), "map_lockstep_min": int(t.map_lockstep_min)}
+            "fused_scan": int(t.fused_scan), "map_lockstep_min": int(t.map_lockstep_min),
+            "map_threads": int(t.map_threads), "map_group_max": int(t.map_group_max)}
 
 
 def reset() -> None:
@@ -257,17 +264,31 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
         saved = np.load(pr.WEIGHTS)
         bin_days = float(saved["bin_days"])
         oversample = float(saved["map_oversample"]) if "map_oversample" in saved.files else 2.0
-        maps = {}
-        for lm in MAP_LOCKSTEP:
-            apply({**tuned, "launch_periods": out["launch_periods"], "fold_steal": out["fold_steal"],
-                   "map_lockstep_min": lm})
+        def time_maps(knobs):
+            apply({**tuned, "launch_periods": out["launch_periods"], "fold_steal": out["fold_steal"], **knobs})
             pr.features(gpu, pstars, devs, bin_days, oversample=oversample)
             ts = []
             for _ in range(reps):
                 t0 = time.perf_counter()
                 pr.features(gpu, pstars, devs, bin_days, oversample=oversample)
                 ts.append(time.perf_counter() - t0)
-            maps[lm] = _median(ts)
+            return _median(ts)
+
+        # Shapes first (group cap x CTA size: fewer lanes per period, longer
+        # segments), then the lockstep threshold at the best shape.
+        shapes = {}
+        for gm, th in MAP_SHAPES:
+            shapes[(gm, th)] = time_maps({"map_group_max": gm, "map_threads": th})
+            log(f"coarse maps of {survey_stars} stars, group cap {gm or 'rule'}, {th or 1024} threads: "
+                f"{1e3 * shapes[(gm, th)]:.1f} ms")
+        gm, th = min(shapes, key=shapes.get)
+        if shapes[(gm, th)] >= 0.98 * shapes[(0, 0)]:
+            gm, th = 0, 0
+        out["map_shape_ms"] = {f"{g_ or 'rule'}x{t_ or 1024}": round(1e3 * v, 2) for (g_, t_), v in shapes.items()}
+        out["map_group_max"], out["map_threads"] = int(gm), int(th)
+        maps = {}
+        for lm in MAP_LOCKSTEP:
+            maps[lm] = time_maps({"map_group_max": gm, "map_threads": th, "map_lockstep_min": lm})
             log(f"coarse maps of {survey_stars} stars, map lockstep {lm or 'rule'}: {1e3 * maps[lm]:.1f} ms")
         best = min(maps, key=maps.get)
         out["maps_ms"] = {str(k): round(1e3 * v, 2) for k, v in maps.items()}
@@ -288,7 +309,8 @@ def main(argv=None):
     Path(args.out).write_text(json.dumps(table, indent=1) + "\n")
     print(json.dumps({k: table[k] for k in ("fold_group_max", "fold_threads", "lockstep_min", "fold_pair",
                                              "launch_periods",
-                                             "fused_scan", "fold_steal", "map_lockstep_min")}))
+                                             "fused_scan", "fold_steal", "map_lockstep_min", "map_threads",
+                                             "map_group_max")}))
 
 
 if __name__ == "__main__":

@@ -623,7 +623,7 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
                                               const ScanArgs* scan, const MergeArgs* merge) {
     constexpr int F = CAP + 2;  // doubles per staged field
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ double s_scale[MAX_GROUP];
+    __shared__ double s_scale[WALK_MAX_GROUP];
     __shared__ __align__(8) uint64_t s_bar[2];
 
     const int tid = threadIdx.x;
@@ -636,13 +636,15 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
     const int G = a.group;
     // Paired walk: each lane walks two periods, q and q + G / 2, over the
     // same staged observations (one read of t, v, w serves both).
+    // A lane set is WALK_MIN_LANES or more consecutive lanes: part of a warp
+    // (several periods per warp, for short chunks), a warp, or several warps.
     const int GV = PAIR ? G / 2 : G;  // lane sets
-    const int wpp = (T / 32) / GV;    // warps per lane set (>= 1)
-    const int NS = wpp * 32;          // segments per period
+    const int NS = T / GV;            // lanes per lane set = segments per period
+    const int wpp = NS / 32;          // whole warps per lane set (0: a warp holds several sets)
     const int g0 = cta * G;
     const int g = min(G, a.periods - g0);
-    const int q = warp / wpp;
-    const int seg = (warp - q * wpp) * 32 + lane;
+    const int q = tid / NS;
+    const int seg = tid - q * NS;
     const bool live = q < g;
     const bool live_b = PAIR && q + GV < g;
     const int rs = a.row_stride;
@@ -686,9 +688,9 @@ __device__ __forceinline__ bool fold_walk_cta(const FoldArgs& a, const int cta, 
     // Staging blocks: runs of consecutive chunks of at most CAP observations
     // in all, one bulk copy per field. Between the chunks of a block only the
     // warps of a period group synchronise (named barrier 1 + warp / U over U
-    // warps, U >= the period's wpp warps, at most 8 groups): periods share no
-    // bins, so a CTA-wide barrier is needed only when a staging buffer turns
-    // over.
+    // warps, U >= a lane set's wpp warps and a whole number of lane sets, at
+    // most 8 groups): periods share no bins, so a CTA-wide barrier is needed
+    // only when a staging buffer turns over.
     const int* ch = a.chunks;
     auto block_end = [&](int c0) {
         int c1 = c0 + 1;
@@ -995,6 +997,8 @@ std::atomic<uint32_t> g_launch_periods{16384};
 std::atomic<uint32_t> g_fold_steal{0};
 std::atomic<uint32_t> g_fused_scan{0};
 std::atomic<uint32_t> g_map_lockstep{0};
+std::atomic<uint32_t> g_map_threads{0};
+std::atomic<uint32_t> g_map_group{0};
 
 int nb_class(int nb) { return nb > 0 ? 31 - __builtin_clz((unsigned)nb) : 0; }
 
@@ -1002,38 +1006,33 @@ uint32_t group_cap(int nb) { return g_group_cap[nb_class(nb)].load(std::memory_o
 
 bool walk_threads_ok(int t) { return t == 128 || t == 256 || t == 512 || t == 1024; }
 
-bool walk_shape(int nb, int periods, int sm_count, bool tuned, FoldShape* out, bool pair_ok = true) {
+// The walking-fold shape for CTAs of T threads, `pair` (two periods per
+// lane), a group cap (0: the rule's MAX_GROUP; a tuned cap may reach
+// WALK_MAX_GROUP, with lane sets down to WALK_MIN_LANES lanes) and a lockstep
+// threshold. `fill`: groups are cut until the launch gives every SM a CTA
+// (else only to the periods there are: callers whose launch holds many such
+// jobs). False when one lane set's histograms do not fit.
+bool walk_shape_for(int nb, int periods, int sm_count, int T, bool pair, uint32_t gcap, int lockstep, bool fill,
+                    FoldShape* out) {
     FoldShape s{};
     s.kind = FOLD_WALK;
-    s.threads = 1024;
-    const int cls = nb_class(nb);
-    if (tuned) {
-        s.pair = pair_ok && periods >= 2 && g_pair[cls].load(std::memory_order_relaxed) != 0;
-        const uint32_t t = g_threads[cls].load(std::memory_order_relaxed);
-        if (t) s.threads = (int)t;
-        if (s.pair && s.threads > 512) s.threads = 512;
-        s.lockstep_min = (int)g_lockstep[cls].load(std::memory_order_relaxed);
-    }
-    const int T = s.threads;
-    const int PV = s.pair ? 2 : 1;  // periods per lane
+    s.threads = T;
+    s.pair = pair;
+    s.lockstep_min = lockstep;
+    const int PV = pair ? 2 : 1;  // periods per lane
     s.row_stride = nb | 1;
     const size_t stage = 6 * sizeof(double) * (size_t)(WALK_CAP + 2);
     const size_t hist_per = (size_t)s.row_stride * BIN_BYTES;
-    // run starts [g][NS + 1], NS = the segments of a period: 32 x (warps per lane set)
-    auto starts = [&](int g) {
-        const int sets = g / PV > 0 ? g / PV : 1;
-        return ((size_t)g * ((T / 32) / sets * 32 + 1) * sizeof(int) + 15) & ~(size_t)15;
-    };
-    if (stage + starts(PV) + (size_t)PV * hist_per > MAX_FOLD_SMEM) {
-        if (s.pair) return walk_shape(nb, periods, sm_count, tuned, out, false);
-        return false;
-    }
+    // run starts [g][NS + 1], NS = the lanes of a lane set (g / PV sets)
+    auto lanes = [&](int g) { return T / (g / PV > 0 ? g / PV : 1); };
+    auto starts = [&](int g) { return ((size_t)g * (lanes(g) + 1) * sizeof(int) + 15) & ~(size_t)15; };
+    if (stage + starts(PV) + (size_t)PV * hist_per > MAX_FOLD_SMEM) return false;
+    const int gmax = gcap > (uint32_t)MAX_GROUP ? (int)std::min<uint32_t>(gcap, WALK_MAX_GROUP) : MAX_GROUP;
     int g = PV;
-    while (2 * g <= MAX_GROUP && 2 * g <= PV * (T / 32) &&
+    while (2 * g <= gmax && lanes(2 * g) >= WALK_MIN_LANES &&
            stage + starts(2 * g) + (size_t)(2 * g) * hist_per <= MAX_FOLD_SMEM)
         g *= 2;
-    while (g > PV && (g / 2 >= periods || (periods + g - 1) / g < sm_count)) g /= 2;
-    const uint32_t gcap = group_cap(nb);
+    while (g > PV && (g / 2 >= periods || (fill && (periods + g - 1) / g < sm_count))) g /= 2;
     while (gcap && g > PV && (uint32_t)g > gcap) g /= 2;
     s.group = g;
     s.hist_in_smem = true;
@@ -1046,7 +1045,35 @@ bool walk_shape(int nb, int periods, int sm_count, bool tuned, FoldShape* out, b
     return true;
 }
 
+bool walk_shape(int nb, int periods, int sm_count, bool tuned, FoldShape* out) {
+    const int cls = nb_class(nb);
+    int T = 1024, lockstep = 0;
+    bool pair = false;
+    if (tuned) {
+        pair = periods >= 2 && g_pair[cls].load(std::memory_order_relaxed) != 0;
+        const uint32_t t = g_threads[cls].load(std::memory_order_relaxed);
+        if (t) T = (int)t;
+        lockstep = (int)g_lockstep[cls].load(std::memory_order_relaxed);
+    }
+    const uint32_t gcap = group_cap(nb);
+    if (pair && walk_shape_for(nb, periods, sm_count, T > 512 ? 512 : T, true, gcap, lockstep, true, out))
+        return true;
+    return walk_shape_for(nb, periods, sm_count, T, false, gcap, lockstep, true, out);
+}
+
 }  // namespace
+
+FoldShape fold_map_shape(int nb, int periods, int sm_count) {
+    const uint32_t t = g_map_threads.load(std::memory_order_relaxed);
+    const uint32_t gcap = g_map_group.load(std::memory_order_relaxed);
+    FoldShape w;
+    // A tuned cap drops the fill rule: a map batch's launch holds every
+    // star's groups.
+    if (walk_shape_for(nb, periods, sm_count, t ? (int)t : 1024, false, gcap,
+                       (int)g_map_lockstep.load(std::memory_order_relaxed), gcap == 0, &w))
+        return w;
+    return fold_group_shape(nb, periods, sm_count);
+}
 
 // Launch shape: the largest power-of-two period group (<= 32 and at most
 // enough to give every SM one CTA) whose histograms leave room to stage at
@@ -1096,6 +1123,8 @@ void set_fold_tuning(const FoldTuning& t) {
     g_fold_steal.store(t.steal ? 1u : 0u, std::memory_order_relaxed);
     g_fused_scan.store(t.fused_scan ? 1u : 0u, std::memory_order_relaxed);
     g_map_lockstep.store(t.map_lockstep_min, std::memory_order_relaxed);
+    g_map_threads.store(t.map_threads, std::memory_order_relaxed);
+    g_map_group.store(t.map_group_max, std::memory_order_relaxed);
 }
 
 void get_fold_tuning(FoldTuning* t) {
@@ -1109,9 +1138,11 @@ void get_fold_tuning(FoldTuning* t) {
     t->steal = g_fold_steal.load(std::memory_order_relaxed);
     t->fused_scan = g_fused_scan.load(std::memory_order_relaxed);
     t->map_lockstep_min = g_map_lockstep.load(std::memory_order_relaxed);
+    t->map_threads = g_map_threads.load(std::memory_order_relaxed);
+    t->map_group_max = g_map_group.load(std::memory_order_relaxed);
 }
 
-int tuned_map_lockstep() { return (int)g_map_lockstep.load(std::memory_order_relaxed); }
+
 
 bool tuned_fused_scan() { return g_fused_scan.load(std::memory_order_relaxed) != 0; }
 
@@ -1151,12 +1182,13 @@ int fold_chunks(const double* time, int n, double scale_max, int nb, int span_ca
 // threads, at most 512 paired.
 static bool walk_form_ok(int threads, bool pair) { return walk_threads_ok(threads) && (!pair || threads <= 512); }
 
-// A group within a walking-fold shape's CTA: a power of two up to MAX_GROUP,
-// at least one warp per lane set (a period, or a pair of periods).
+// A group within a walking-fold shape's CTA: a power of two up to
+// WALK_MAX_GROUP, at least WALK_MIN_LANES lanes per lane set (a period, or a
+// pair of periods).
 static bool walk_group_ok(int group, const FoldShape& shape) {
     return shape.kind == FOLD_WALK && walk_form_ok(shape.threads, shape.pair) && group == shape.group &&
-           group >= (shape.pair ? 2 : 1) && group <= MAX_GROUP && (group & (group - 1)) == 0 &&
-           (shape.pair ? group / 2 : group) <= shape.threads / 32 && shape.smem <= MAX_FOLD_SMEM;
+           group >= (shape.pair ? 2 : 1) && group <= WALK_MAX_GROUP && (group & (group - 1)) == 0 &&
+           (shape.pair ? group / 2 : group) <= shape.threads / WALK_MIN_LANES && shape.smem <= MAX_FOLD_SMEM;
 }
 
 template <bool PAIR>
@@ -1199,6 +1231,15 @@ cudaError_t launch_fold_steal(const FoldArgs* jobs, const int* cta0, int njobs, 
                 : launch_fold_steal_t<false>(jobs, cta0, njobs, units, threads, smem, counter, sm_count, stream);
 }
 
+// The fused scan's epilogue keeps, in the idle staging buffers (6 F
+// doubles), each row's final carry, the groups' scratch and the CTA's tile
+// winners.
+static bool fused_epilogue_fits(const FoldArgs& a, const FoldShape& shape) {
+    const size_t scratch = (size_t)(shape.threads / TILE) * ((sizeof(TileScratch) + 7) / 8);
+    const size_t winners = (size_t)a.group * ((a.nb + TILE - 1) / TILE) * FUSED_PART_DOUBLES;
+    return (size_t)a.group * NF + scratch + winners <= 6 * (size_t)(WALK_CAP + 2);
+}
+
 // The walking-fold limits on everything but the outputs.
 static bool fold_job_ok_rows(const FoldArgs& a, const FoldShape& shape) {
     return walk_group_ok(a.group, shape) && a.lockstep_min >= 0 && a.nchunks >= 1 && a.nb >= 2 &&
@@ -1215,7 +1256,7 @@ bool fold_job_ok(const FoldArgs& a, const FoldShape& shape) {
            (a.hist_out == nullptr || (a.group == 1 && a.periods == 1 && a.map_out == nullptr)) &&
            a.time && a.v && a.w && a.scales && a.chunks &&
            (a.map_out || a.hist_out || a.scan || (a.cum && a.cum32)) && (!a.scan == !a.merge) &&
-           (!a.scan || (!a.map_out && !a.hist_out)) &&
+           (!a.scan || (!a.map_out && !a.hist_out && fused_epilogue_fits(a, shape))) &&
            (!a.map_out || (a.map_nd >= 1 && a.map_nd <= MAP_MAX_DURATIONS && a.map_durations && a.map_rho)) &&
            !(reinterpret_cast<uintptr_t>(a.time) & 15) && !(reinterpret_cast<uintptr_t>(a.v) & 15) &&
            !(reinterpret_cast<uintptr_t>(a.w) & 15);
@@ -1255,7 +1296,7 @@ cudaError_t launch_fold_scan(const FoldArgs& a, const FoldShape& shape, const Sc
     FoldArgs f = a;
     f.cum = nullptr;
     f.cum32 = nullptr;
-    if (!fold_job_ok_rows(f, shape)) return cudaErrorInvalidValue;
+    if (!fold_job_ok_rows(f, shape) || !fused_epilogue_fits(f, shape)) return cudaErrorInvalidValue;
     const int blocks = (a.periods + a.group - 1) / a.group;
     if (shape.pair) {
         const cudaError_t e = cudaFuncSetAttribute(k_fold_scan<WALK_CAP, true>,

@@ -103,7 +103,7 @@ int plan_map(const fbls_ctx* ctx, MapPlan& m) {
             return bad(FBLS_ERR_ARGUMENT, "phase cell exceeds 32 bits");
         const size_t stride = 2 * (size_t)nb + 1;
         g.per_launch = (uint32_t)std::max<size_t>(1, std::min<size_t>(16384, (512ull << 20) / (NF * stride * 12)));
-        g.shape = fold_group_shape((int)nb, (int)std::min(g.count, g.per_launch), ctx->sm_count);
+        g.shape = fold_map_shape((int)nb, (int)std::min(g.count, g.per_launch), ctx->sm_count);
         g.chunks.resize((size_t)ready->n + 2);
         const int c = fold_chunks(ready->time_host.data(), (int)ready->n, scale_max, (int)nb, g.shape.span_cap,
                                   g.shape.chunk_cap, g.chunks.data(), (int)g.chunks.size());
@@ -151,7 +151,7 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
     struct Wave {
         std::vector<Unit> units;
         size_t cum = 0, hist = 0, smem = 0;
-        int fold_jobs = 0, fold_ctas = 0, map_jobs = 0, map_total = 0;
+        int fold_jobs = 0, fold_ctas = 0, map_jobs = 0, map_total = 0, fold_threads = 0;
         size_t off_fold = 0, off_fcta = 0, off_map = 0, off_mp = 0;
     };
     size_t in_total = 0, out_total = 0, bin_total = 0;
@@ -176,8 +176,10 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
                 const size_t cum = walk ? 0 : (size_t)n * NF * stride;
                 const size_t hist = walk ? 0 : ((n + g.shape.group - 1) / g.shape.group) * (size_t)g.shape.group *
                                                    NF * (size_t)g.shape.row_stride;
+                // one CTA size per wave's job launch
                 if (!waves.back().units.empty() &&
-                    (waves.back().cum + cum) * (sizeof(double) + sizeof(float2)) > MAP_WAVE_BYTES)
+                    ((waves.back().cum + cum) * (sizeof(double) + sizeof(float2)) > MAP_WAVE_BYTES ||
+                     (walk && waves.back().fold_threads && waves.back().fold_threads != g.shape.threads)))
                     waves.emplace_back();
                 Wave& w = waves.back();
                 w.units.push_back({m, &g, c0, n, w.cum, w.hist, walk});
@@ -185,6 +187,7 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
                 w.hist += hist;
                 if (walk) {
                     w.fold_jobs++;
+                    w.fold_threads = g.shape.threads;
                     w.fold_ctas += (n + g.shape.group - 1) / g.shape.group;
                     w.smem = std::max(w.smem, g.shape.smem);
                 } else {
@@ -298,7 +301,7 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
             fa.window = g.shape.window;
             fa.row_stride = g.shape.row_stride;
             fa.fault = as<uint32_t>(ctx->fault);
-            fa.lockstep_min = tuned_map_lockstep();
+            fa.lockstep_min = g.shape.lockstep_min;
             float* out = reinterpret_cast<float*>(dout + m.out_off) + (size_t)(g.i0 + un.c0) * m.job->nd;
             if (un.walk) {
                 fa.map_out = out;
@@ -350,8 +353,8 @@ int run_maps(fbls_ctx* ctx, const std::vector<MapPlan*>& plans, const MapFeature
         const Wave& w = waves[wi];
         if (w.fold_jobs) {
             CK(launch_fold_jobs(reinterpret_cast<const FoldArgs*>(din + w.off_fold),
-                                reinterpret_cast<const int*>(din + w.off_fcta), w.fold_jobs, w.fold_ctas, 1024,
-                                false, w.smem, s),
+                                reinterpret_cast<const int*>(din + w.off_fcta), w.fold_jobs, w.fold_ctas,
+                                w.fold_threads, false, w.smem, s),
                "fold");
             ctx->counters.launches += 1;
         }

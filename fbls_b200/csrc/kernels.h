@@ -7,7 +7,9 @@
 
 namespace fbls {
 
-constexpr int MAX_GROUP = 32;               // periods per fold CTA
+constexpr int MAX_GROUP = 32;               // periods per fold CTA (the built-in rule's largest group)
+constexpr int WALK_MAX_GROUP = 128;         // periods per walking-fold CTA (tuned group caps)
+constexpr int WALK_MIN_LANES = 8;           // lanes per period of a walking-fold CTA at least
 constexpr size_t MAX_FOLD_SMEM = 225 * 1024;  // dynamic shared memory of k_fold
 constexpr int MAX_DURATIONS = 64;
 constexpr int MAX_SHAPES = 8;
@@ -100,6 +102,8 @@ struct FoldTuning {
     uint32_t steal;
     uint32_t fused_scan;  // nonzero: the walking fold scans and merges its own tiles (else separate kernels)
     uint32_t map_lockstep_min;  // the coarse maps' folds: lockstep threshold (0: built-in)
+    uint32_t map_threads;       // the coarse maps' walking folds: CTA size (0: 1024)
+    uint32_t map_group_max;     // the coarse maps' walking folds: largest period group (0: built-in)
 };
 
 struct ScanArgs {
@@ -225,11 +229,15 @@ struct BiweightArgs {
 // walking fold takes its CTA size and lockstep threshold from the tuning
 // table (callers whose job launches mix shapes keep 1024 threads).
 FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned = false);
+// The coarse maps' fold shape: the walking fold with the tuning table's map
+// CTA size, group cap (nonzero: groups up to the cap whatever the SM count,
+// as a batch's launch holds every star's groups) and lockstep threshold,
+// else fold_group_shape's.
+FoldShape fold_map_shape(int nb, int periods, int sm_count);
 void set_fold_tuning(const FoldTuning& t);
 void get_fold_tuning(FoldTuning* t);
 uint32_t tuned_launch_periods();
 bool tuned_fused_scan();
-int tuned_map_lockstep();
 bool tuned_fold_steal();
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
 // spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.

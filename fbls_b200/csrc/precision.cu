@@ -111,13 +111,16 @@ extern "C" int fbls_precision_bins(fbls_ctx* ctx, const fbls_ready* ready, const
     return FBLS_OK;
 }
 
+static bool cta_size_ok(uint32_t th) { return th == 0 || th == 128 || th == 256 || th == 512 || th == 1024; }
+
+static bool group_cap_ok(uint32_t g) { return g <= (uint32_t)WALK_MAX_GROUP && (g & (g - 1)) == 0; }
+
 extern "C" int fbls_set_tuning(const fbls_tuning* tuning) {
     if (!tuning) return FBLS_ERR_ARGUMENT;
     FoldTuning t{};
     for (int c = 0; c < 32; c++) {
         const uint32_t g = tuning->fold_group_max[c], th = tuning->fold_threads[c], l = tuning->lockstep_min[c];
-        if (g > (uint32_t)MAX_GROUP || (g & (g - 1)) != 0) return FBLS_ERR_ARGUMENT;
-        if (th != 0 && th != 128 && th != 256 && th != 512 && th != 1024) return FBLS_ERR_ARGUMENT;
+        if (!group_cap_ok(g) || !cta_size_ok(th)) return FBLS_ERR_ARGUMENT;
         if (l > 4096) return FBLS_ERR_ARGUMENT;
         t.group_cap[c] = g;
         t.threads[c] = th;
@@ -130,6 +133,9 @@ extern "C" int fbls_set_tuning(const fbls_tuning* tuning) {
     t.fused_scan = tuning->fused_scan;
     if (tuning->map_lockstep_min > 4096) return FBLS_ERR_ARGUMENT;
     t.map_lockstep_min = tuning->map_lockstep_min;
+    if (!cta_size_ok(tuning->map_threads) || !group_cap_ok(tuning->map_group_max)) return FBLS_ERR_ARGUMENT;
+    t.map_threads = tuning->map_threads;
+    t.map_group_max = tuning->map_group_max;
     set_fold_tuning(t);
     return FBLS_OK;
 }
@@ -148,5 +154,7 @@ extern "C" int fbls_get_tuning(fbls_tuning* tuning) {
     tuning->fold_steal = t.steal;
     tuning->fused_scan = t.fused_scan;
     tuning->map_lockstep_min = t.map_lockstep_min;
+    tuning->map_threads = t.map_threads;
+    tuning->map_group_max = t.map_group_max;
     return FBLS_OK;
 }

@@ -248,15 +248,17 @@ int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
 
 /* Measured launch-shape tuning (no counterpart in the reference; written by
  * the autotuner, python -m fbls_b200.autotune, and read back from its table):
- * per nb class floor(log2(nb)) the largest fold period group (a power of two;
- * 0 = the built-in rule: the largest group whose histograms fit shared memory
- * while every SM gets a CTA), the periods per launch (0 = 16,384), and
+ * per nb class floor(log2(nb)) the largest fold period group (a power of two
+ * up to 128; 0 = the built-in rule: the largest group up to 32 whose
+ * histograms fit shared memory while every SM gets a CTA; a cap above 32
+ * lets the walking fold give a period fewer than 32 lanes, down to 8), the
+ * periods per launch (0 = 16,384), and
  * fold_steal: nonzero runs a batch's walking-fold jobs (fbls_search_batch
  * with workers 0) as one persistent grid of a CTA per SM that takes the next
  * (star, pass, period-group) unit from a counter, instead of a CTA per unit.
  * Per nb class, for the signal-search folds: fold_threads, the walking
  * fold's CTA size (128, 256, 512 or 1024; 0 = 1024; the period group is cut
- * to at most one period per warp), and lockstep_min, the segment length from
+ * to at least 8 lanes per period), and lockstep_min, the segment length from
  * which a CTA's lanes walk their observations in lockstep rather than each
  * its own window (0 = 11; at most 4096). fused_scan: nonzero has the
  * walking fold's CTAs scan and merge their own periods' tiles from the prefix
@@ -267,7 +269,10 @@ int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
  * families walk short segments), one value for every nb. fold_pair, per nb
  * class of the signal-search folds: nonzero walks two periods per lane, one
  * read of each staged observation serving both (CTAs of at most 512
- * threads; 512 when fold_threads is 0).
+ * threads; 512 when fold_threads is 0). map_threads and map_group_max: the
+ * coarse maps' walking folds' CTA size (as fold_threads) and largest period
+ * group (as fold_group_max, but a nonzero cap is taken whatever the SM count:
+ * a map batch's launch holds every star's groups), one value for every nb.
  * Process-wide; results do not depend on it, only the launch shapes do. */
 typedef struct {
     uint32_t fold_group_max[32];
@@ -278,6 +283,8 @@ typedef struct {
     uint32_t fused_scan;
     uint32_t map_lockstep_min;
     uint32_t fold_pair[32];
+    uint32_t map_threads;
+    uint32_t map_group_max;
 } fbls_tuning;
 int fbls_set_tuning(const fbls_tuning* tuning);
 int fbls_get_tuning(fbls_tuning* tuning);

@@ -131,11 +131,14 @@ def test_work_stealing_fold_gives_the_same_rows(gpu):
         assert np.array_equal(r1, r2) and g1 == g2 and t1 == t2
 
 
-@pytest.mark.parametrize("threads,lockstep,pair", [(128, 0, 0), (256, 3, 0), (512, 4096, 0), (1024, 3, 0),
-                                                   (512, 0, 1), (256, 3, 1), (512, 4096, 1)])
-def test_fold_cta_size_and_lockstep_give_the_same_rows(gpu, threads, lockstep, pair):
-    # The walking fold at every CTA size, lockstep threshold and form (one or
-    # two periods per lane) the tuning table allows, in both the per-star
+@pytest.mark.parametrize("threads,lockstep,pair,group", [
+    (128, 0, 0, 0), (256, 3, 0, 0), (512, 4096, 0, 0), (1024, 3, 0, 0), (512, 0, 1, 0), (256, 3, 1, 0),
+    (512, 4096, 1, 0),
+    # group caps that give a period fewer lanes than a warp (down to 8)
+    (1024, 0, 0, 128), (128, 3, 0, 16), (512, 0, 1, 128), (1024, 4096, 0, 64)])
+def test_fold_cta_size_and_lockstep_give_the_same_rows(gpu, threads, lockstep, pair, group):
+    # The walking fold at every CTA size, lockstep threshold, form (one or
+    # two periods per lane) and group cap the tuning table allows, in both the per-star
     # search and the batch's job launches (where shapes of several CTA sizes
     # and forms share a wave), with and without work stealing: the same rows
     # bit for bit as the built-in shape.
@@ -159,7 +162,8 @@ def test_fold_cta_size_and_lockstep_give_the_same_rows(gpu, threads, lockstep, p
         classes = {str(c): threads for c in range(7, 16)}
         for steal in (0, 1):
             autotune.apply({"fold_threads": classes, "lockstep_min": {str(c): lockstep for c in range(32)} if lockstep
-                            else {}, "fold_pair": {c: pair for c in classes} if pair else {}, "fold_steal": steal})
+                            else {}, "fold_pair": {c: pair for c in classes} if pair else {}, "fold_steal": steal,
+                            "fold_group_max": {str(c): group for c in range(32)} if group else {}})
             got = gpu.search_batch([s for s, _ in stars], base, period_max=[p for _, p in stars], workers=0)
             for (r1, g1, t1), (r2, g2, t2) in zip(got, want):
                 assert np.array_equal(r1, r2) and g1 == g2 and t1 == t2

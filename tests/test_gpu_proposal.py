@@ -160,20 +160,25 @@ def test_coarse_map_batch_matches_single_maps(gpu, bin_days):
         d.free()
 
 
-def test_map_lockstep_threshold_does_not_change_the_maps(gpu):
-    """The coarse maps' folds at every lockstep threshold the tuning table
-    allows give the same network input bit for bit."""
+@pytest.mark.parametrize("bin_days", [0.0, 1200.0 / 86400.0])
+def test_map_fold_shapes_do_not_change_the_maps(gpu, bin_days):
+    """The coarse maps' folds at every lockstep threshold, CTA size and group
+    cap the tuning table allows (caps above 32 give a period fewer lanes than
+    a warp, and a cap drops the rule that every SM gets a CTA) give the same
+    network input bit for bit."""
     from fbls_b200 import autotune
     from fbls_b200 import proposal as pr
     stars, cfg = pr.survey_stars(6, seed=9, max_sectors=3)
     devs = [gpu.upload(s) for s, _ in stars]
     saved = autotune.current()
     try:
-        autotune.apply({**saved, "map_lockstep_min": 0})
-        want = pr.features(gpu, stars, devs, bin_days=600.0 / 86400.0)
-        for lm in (3, 5, 4096):
-            autotune.apply({**saved, "map_lockstep_min": lm})
-            assert np.array_equal(pr.features(gpu, stars, devs, bin_days=600.0 / 86400.0), want)
+        autotune.apply({**saved, "map_lockstep_min": 0, "map_threads": 0, "map_group_max": 0})
+        want = pr.features(gpu, stars, devs, bin_days=bin_days, oversample=1.0)
+        for lm, th, gm in ((3, 0, 0), (5, 0, 0), (4096, 0, 0), (0, 0, 32), (0, 0, 128), (3, 512, 64),
+                           (0, 128, 16), (4096, 256, 32)):
+            autotune.apply({**saved, "map_lockstep_min": lm, "map_threads": th, "map_group_max": gm})
+            got = pr.features(gpu, stars, devs, bin_days=bin_days, oversample=1.0)
+            assert np.array_equal(got, want), (lm, th, gm)
     finally:
         autotune.apply(saved)
     for d in devs:

@@ -182,13 +182,17 @@ def test_tuning_table_round_trip_and_limits():
         table = {"fold_group_max": {"10": 4, "11": 2}, "fold_threads": {"10": 512, "11": 256},
                  "lockstep_min": {"10": 7}, "fold_pair": {"9": 1}, "launch_periods": 8192, "fold_steal": 1,
                  "fused_scan": 1,
-                 "map_lockstep_min": 3}
+                 "map_lockstep_min": 3, "map_threads": 512, "map_group_max": 64}
         autotune.apply(table)
         assert autotune.current() == table
         with pytest.raises(ValueError):
             autotune.apply({"fold_group_max": {"10": 3}})  # not a power of two
         with pytest.raises(ValueError):
-            autotune.apply({"fold_group_max": {"10": 64}})  # above the largest group
+            autotune.apply({"fold_group_max": {"10": 256}})  # above the largest group
+        with pytest.raises(ValueError):
+            autotune.apply({"map_group_max": 256})
+        with pytest.raises(ValueError):
+            autotune.apply({"map_threads": 640})
         with pytest.raises(ValueError):
             autotune.apply({"fold_threads": {"10": 384}})  # not a walking-fold CTA size
         with pytest.raises(ValueError):
@@ -197,4 +201,5 @@ def test_tuning_table_round_trip_and_limits():
         autotune.reset()
     assert autotune.current() == {"fold_group_max": {}, "fold_threads": {}, "lockstep_min": {}, "fold_pair": {},
                                   "launch_periods": 16384,
-                                  "fold_steal": 0, "fused_scan": 0, "map_lockstep_min": 0}
+                                  "fold_steal": 0, "fused_scan": 0, "map_lockstep_min": 0, "map_threads": 0,
+                                  "map_group_max": 0}
