@@ -145,7 +145,7 @@ class Tuning(C.Structure):
     _fields_ = [("fold_group_max", C.c_uint32 * 32), ("launch_periods", C.c_uint32), ("fold_steal", C.c_uint32),
                 ("fold_threads", C.c_uint32 * 32), ("lockstep_min", C.c_uint32 * 32), ("fused_scan", C.c_uint32),
                 ("map_lockstep_min", C.c_uint32), ("fold_pair", C.c_uint32 * 32), ("map_threads", C.c_uint32),
-                ("map_group_max", C.c_uint32)]
+                ("map_group_max", C.c_uint32), ("batch_no_fill", C.c_uint32)]
 
 
 class PrepConfig(C.Structure):

@@ -69,6 +69,7 @@ def apply(table: dict) -> None:
     t.map_lockstep_min = int(table.get("map_lockstep_min", 0))
     t.map_threads = int(table.get("map_threads", 0))
     t.map_group_max = int(table.get("map_group_max", 0))
+    t.batch_no_fill = int(table.get("batch_no_fill", 0))
     rc = N.load().fbls_set_tuning(C.byref(t))
     if rc:
         raise ValueError(f"tuning table rejected (status {rc})")
@@ -83,7 +84,8 @@ def current() -> dict:
             "fold_pair": {str(c): int(v) for c, v in enumerate(t.fold_pair) if v},
             "launch_periods": int(t.launch_periods), "fold_steal": int(t.fold_steal),
             "fused_scan": int(t.fused_scan), "map_lockstep_min": int(t.map_lockstep_min),
-            "map_threads": int(t.map_threads), "map_group_max": int(t.map_group_max)}
+            "map_threads": int(t.map_threads), "map_group_max": int(t.map_group_max),
+            "batch_no_fill": int(t.batch_no_fill)}
 
 
 def reset() -> None:
@@ -257,6 +259,21 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
             log(f"survey of {survey_stars} stars, fold_steal {flag}: {1e3 * steal[flag]:.1f} ms")
         out["survey_ms"] = {"stars": survey_stars, **{str(k): round(1e3 * v, 2) for k, v in steal.items()}}
         out["fold_steal"] = 1 if steal[1] < 0.99 * steal[0] else 0
+        # Whole period groups in the batch's job launches (no per-pass cut
+        # to fill the SMs) on the same stars.
+        whole = {0: steal[out["fold_steal"]]}
+        apply({**tuned, "launch_periods": out["launch_periods"], "fold_steal": out["fold_steal"],
+               "batch_no_fill": 1})
+        gpu.search_batch([s_ for s_, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs, workers=0)
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            gpu.search_batch([s_ for s_, _ in stars], cfg, period_max=[p for _, p in stars], devs=devs, workers=0)
+            ts.append(time.perf_counter() - t0)
+        whole[1] = _median(ts)
+        log(f"survey of {survey_stars} stars, batch_no_fill 1: {1e3 * whole[1]:.1f} ms")
+        out["survey_whole_groups_ms"] = {str(k): round(1e3 * v, 2) for k, v in whole.items()}
+        out["batch_no_fill"] = 1 if whole[1] < 0.99 * whole[0] else 0
         # The coarse maps' folds (the proposal network's input, binned
         # families) by lockstep threshold, on the same stars.
         from . import proposal as pr
@@ -265,7 +282,8 @@ def sweep(reps: int = 3, log=print, survey_stars: int = 256) -> dict:
         bin_days = float(saved["bin_days"])
         oversample = float(saved["map_oversample"]) if "map_oversample" in saved.files else 2.0
         def time_maps(knobs):
-            apply({**tuned, "launch_periods": out["launch_periods"], "fold_steal": out["fold_steal"], **knobs})
+            apply({**tuned, "launch_periods": out["launch_periods"], "fold_steal": out["fold_steal"],
+                   "batch_no_fill": out["batch_no_fill"], **knobs})
             pr.features(gpu, pstars, devs, bin_days, oversample=oversample)
             ts = []
             for _ in range(reps):
@@ -310,7 +328,7 @@ def main(argv=None):
     print(json.dumps({k: table[k] for k in ("fold_group_max", "fold_threads", "lockstep_min", "fold_pair",
                                              "launch_periods",
                                              "fused_scan", "fold_steal", "map_lockstep_min", "map_threads",
-                                             "map_group_max")}))
+                                             "map_group_max", "batch_no_fill")}))
 
 
 if __name__ == "__main__":

@@ -999,6 +999,7 @@ std::atomic<uint32_t> g_fused_scan{0};
 std::atomic<uint32_t> g_map_lockstep{0};
 std::atomic<uint32_t> g_map_threads{0};
 std::atomic<uint32_t> g_map_group{0};
+std::atomic<uint32_t> g_batch_no_fill{0};
 
 int nb_class(int nb) { return nb > 0 ? 31 - __builtin_clz((unsigned)nb) : 0; }
 
@@ -1045,7 +1046,7 @@ bool walk_shape_for(int nb, int periods, int sm_count, int T, bool pair, uint32_
     return true;
 }
 
-bool walk_shape(int nb, int periods, int sm_count, bool tuned, FoldShape* out) {
+bool walk_shape(int nb, int periods, int sm_count, bool tuned, bool fill_sms, FoldShape* out) {
     const int cls = nb_class(nb);
     int T = 1024, lockstep = 0;
     bool pair = false;
@@ -1056,9 +1057,9 @@ bool walk_shape(int nb, int periods, int sm_count, bool tuned, FoldShape* out) {
         lockstep = (int)g_lockstep[cls].load(std::memory_order_relaxed);
     }
     const uint32_t gcap = group_cap(nb);
-    if (pair && walk_shape_for(nb, periods, sm_count, T > 512 ? 512 : T, true, gcap, lockstep, true, out))
+    if (pair && walk_shape_for(nb, periods, sm_count, T > 512 ? 512 : T, true, gcap, lockstep, fill_sms, out))
         return true;
-    return walk_shape_for(nb, periods, sm_count, T, false, gcap, lockstep, true, out);
+    return walk_shape_for(nb, periods, sm_count, T, false, gcap, lockstep, fill_sms, out);
 }
 
 }  // namespace
@@ -1081,9 +1082,9 @@ FoldShape fold_map_shape(int nb, int periods, int sm_count) {
 // STAGE_MAX); the CTA has 1024 threads, or 512 when segments would
 // otherwise be shorter than 16 observations. A single period whose
 // histogram does not fit folds into global scratch.
-FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned) {
+FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned, bool fill_sms) {
     FoldShape w;
-    if (walk_shape(nb, periods, sm_count, tuned, &w)) return w;
+    if (walk_shape(nb, periods, sm_count, tuned, fill_sms, &w)) return w;
     FoldShape s{};
     s.kind = FOLD_SMEM;
     s.row_stride = nb | 1;
@@ -1091,7 +1092,7 @@ FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned) {
     const size_t stage_min = SLOT_BYTES * (2048 + 1024) + 4 * (1024 + 32);
     int g = 1;
     while (g < MAX_GROUP && (size_t)(2 * g) * hist_per + stage_min <= MAX_FOLD_SMEM) g *= 2;
-    const int fill = (periods + sm_count - 1) / sm_count;
+    const int fill = fill_sms ? (periods + sm_count - 1) / sm_count : periods;
     while (g > 1 && g / 2 >= fill) g /= 2;
     const uint32_t gcap = group_cap(nb);
     while (gcap && g > 1 && (uint32_t)g > gcap) g /= 2;
@@ -1125,6 +1126,7 @@ void set_fold_tuning(const FoldTuning& t) {
     g_map_lockstep.store(t.map_lockstep_min, std::memory_order_relaxed);
     g_map_threads.store(t.map_threads, std::memory_order_relaxed);
     g_map_group.store(t.map_group_max, std::memory_order_relaxed);
+    g_batch_no_fill.store(t.batch_no_fill ? 1u : 0u, std::memory_order_relaxed);
 }
 
 void get_fold_tuning(FoldTuning* t) {
@@ -1140,7 +1142,10 @@ void get_fold_tuning(FoldTuning* t) {
     t->map_lockstep_min = g_map_lockstep.load(std::memory_order_relaxed);
     t->map_threads = g_map_threads.load(std::memory_order_relaxed);
     t->map_group_max = g_map_group.load(std::memory_order_relaxed);
+    t->batch_no_fill = g_batch_no_fill.load(std::memory_order_relaxed);
 }
+
+bool tuned_batch_no_fill() { return g_batch_no_fill.load(std::memory_order_relaxed) != 0; }
 
 
 

@@ -117,6 +117,7 @@ struct Pass {
     BandOut out;
     fbls_scan_stats st{};
     bool bad = false;  // a template's precision came out nonpositive
+    bool fill_sms = true;  // the fold's groups are cut so this pass alone gives every SM a CTA
     std::string err;   // plan_pass's message when it rejects the pass
     int fail(int status, const char* message) {
         err = message;
@@ -186,7 +187,7 @@ int plan_pass(const fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
     if (launch > p.P) launch = p.P;
     p.batch = batch;
     p.launch = launch;
-    p.shape = fold_group_shape((int)nb, (int)launch, ctx->sm_count, true);
+    p.shape = fold_group_shape((int)nb, (int)launch, ctx->sm_count, true, p.fill_sms);
     p.chunks.resize((size_t)r->n + 2);
     const int count = fold_chunks(r->time_host.data(), (int)r->n, scale_max, (int)nb, p.shape.span_cap,
                                   p.shape.chunk_cap, p.chunks.data(), (int)p.chunks.size());
@@ -858,6 +859,7 @@ int scan_bands(fbls_ctx* ctx, std::vector<BandJob>& jobs, int mode, bool fused) 
         p.bank = j.bank;
         p.nb = (uint32_t)(j.coarse ? j.nb / j.bank->prescan_factor : j.nb);
         p.mode = mode;
+        p.fill_sms = !(fused && tuned_batch_no_fill());
         j.first = (int)first.size();
         first.push_back(std::move(p));
     }
@@ -890,6 +892,7 @@ int scan_bands(fbls_ctx* ctx, std::vector<BandJob>& jobs, int mode, bool fused) 
         p.bank = j.bank;
         p.nb = (uint32_t)j.nb;
         p.mode = mode;
+        p.fill_sms = !(fused && tuned_batch_no_fill());
         j.second = (int)second.size();
         second.push_back(std::move(p));
     }

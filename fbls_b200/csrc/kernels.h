@@ -104,6 +104,7 @@ struct FoldTuning {
     uint32_t map_lockstep_min;  // the coarse maps' folds: lockstep threshold (0: built-in)
     uint32_t map_threads;       // the coarse maps' walking folds: CTA size (0: 1024)
     uint32_t map_group_max;     // the coarse maps' walking folds: largest period group (0: built-in)
+    uint32_t batch_no_fill;     // nonzero: a batch's job launches do not cut a pass's groups to fill the SMs
 };
 
 struct ScanArgs {
@@ -228,7 +229,9 @@ struct BiweightArgs {
 // Launch shape of a fold of `periods` periods at nb bins. `tuned`: the
 // walking fold takes its CTA size and lockstep threshold from the tuning
 // table (callers whose job launches mix shapes keep 1024 threads).
-FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned = false);
+// `fill_sms`: period groups are cut until the launch gives every SM a CTA
+// (false: a job launch holding many such folds).
+FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned = false, bool fill_sms = true);
 // The coarse maps' fold shape: the walking fold with the tuning table's map
 // CTA size, group cap (nonzero: groups up to the cap whatever the SM count,
 // as a batch's launch holds every star's groups) and lockstep threshold,
@@ -238,6 +241,7 @@ void set_fold_tuning(const FoldTuning& t);
 void get_fold_tuning(FoldTuning* t);
 uint32_t tuned_launch_periods();
 bool tuned_fused_scan();
+bool tuned_batch_no_fill();
 bool tuned_fold_steal();
 // Cuts n ascending times into fold chunks of at most chunk_cap observations
 // spanning at most min(nb, span_cap) - 2 cells at any scale <= scale_max.

@@ -136,6 +136,8 @@ extern "C" int fbls_set_tuning(const fbls_tuning* tuning) {
     if (!cta_size_ok(tuning->map_threads) || !group_cap_ok(tuning->map_group_max)) return FBLS_ERR_ARGUMENT;
     t.map_threads = tuning->map_threads;
     t.map_group_max = tuning->map_group_max;
+    if (tuning->batch_no_fill > 1) return FBLS_ERR_ARGUMENT;
+    t.batch_no_fill = tuning->batch_no_fill;
     set_fold_tuning(t);
     return FBLS_OK;
 }
@@ -156,5 +158,6 @@ extern "C" int fbls_get_tuning(fbls_tuning* tuning) {
     tuning->map_lockstep_min = t.map_lockstep_min;
     tuning->map_threads = t.map_threads;
     tuning->map_group_max = t.map_group_max;
+    tuning->batch_no_fill = t.batch_no_fill;
     return FBLS_OK;
 }

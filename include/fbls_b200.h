@@ -273,6 +273,9 @@ int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
  * coarse maps' walking folds' CTA size (as fold_threads) and largest period
  * group (as fold_group_max, but a nonzero cap is taken whatever the SM count:
  * a map batch's launch holds every star's groups), one value for every nb.
+ * batch_no_fill (0 or 1): 1 keeps a pass's period groups whole in
+ * fbls_search_batch's job launches (workers 0), where the default cuts them
+ * until the pass alone would give every SM a CTA.
  * Process-wide; results do not depend on it, only the launch shapes do. */
 typedef struct {
     uint32_t fold_group_max[32];
@@ -285,6 +288,7 @@ typedef struct {
     uint32_t fold_pair[32];
     uint32_t map_threads;
     uint32_t map_group_max;
+    uint32_t batch_no_fill;
 } fbls_tuning;
 int fbls_set_tuning(const fbls_tuning* tuning);
 int fbls_get_tuning(fbls_tuning* tuning);

@@ -108,9 +108,12 @@ def test_fused_batch_uploads_every_star(gpu):
         d.free()
 
 
-def test_work_stealing_fold_gives_the_same_rows(gpu):
+@pytest.mark.parametrize("knobs", [{"fold_steal": 1}, {"batch_no_fill": 1}, {"fold_steal": 1, "batch_no_fill": 1}])
+def test_work_stealing_and_whole_groups_give_the_same_rows(gpu, knobs):
     # The batch's walking-fold jobs by a persistent grid that takes units from
-    # a counter (fold_steal) against a CTA per unit: the same rows bit for bit.
+    # a counter (fold_steal) against a CTA per unit, and with each pass's
+    # period groups kept whole (batch_no_fill) against groups cut to fill the
+    # SMs pass by pass: the same rows bit for bit.
     from fbls_b200 import autotune
     rng = np.random.default_rng(31)
     stars = []
@@ -121,9 +124,9 @@ def test_work_stealing_fold_gives_the_same_rows(gpu):
     base = synth.survey_config(synth.survey_star(np.random.default_rng(0)))
     saved = autotune.current()
     try:
-        autotune.apply({**saved, "fold_steal": 0})
+        autotune.apply({**saved, "fold_steal": 0, "batch_no_fill": 0})
         want = gpu.search_batch([s for s, _ in stars], base, period_max=[p for _, p in stars], workers=0)
-        autotune.apply({**saved, "fold_steal": 1})
+        autotune.apply({**saved, **knobs})
         got = gpu.search_batch([s for s, _ in stars], base, period_max=[p for _, p in stars], workers=0)
     finally:
         autotune.apply(saved)

@@ -182,7 +182,7 @@ def test_tuning_table_round_trip_and_limits():
         table = {"fold_group_max": {"10": 4, "11": 2}, "fold_threads": {"10": 512, "11": 256},
                  "lockstep_min": {"10": 7}, "fold_pair": {"9": 1}, "launch_periods": 8192, "fold_steal": 1,
                  "fused_scan": 1,
-                 "map_lockstep_min": 3, "map_threads": 512, "map_group_max": 64}
+                 "map_lockstep_min": 3, "map_threads": 512, "map_group_max": 64, "batch_no_fill": 1}
         autotune.apply(table)
         assert autotune.current() == table
         with pytest.raises(ValueError):
@@ -194,6 +194,8 @@ def test_tuning_table_round_trip_and_limits():
         with pytest.raises(ValueError):
             autotune.apply({"map_threads": 640})
         with pytest.raises(ValueError):
+            autotune.apply({"batch_no_fill": 2})
+        with pytest.raises(ValueError):
             autotune.apply({"fold_threads": {"10": 384}})  # not a walking-fold CTA size
         with pytest.raises(ValueError):
             autotune.apply({"lockstep_min": {"10": 5000}})
@@ -202,4 +204,4 @@ def test_tuning_table_round_trip_and_limits():
     assert autotune.current() == {"fold_group_max": {}, "fold_threads": {}, "lockstep_min": {}, "fold_pair": {},
                                   "launch_periods": 16384,
                                   "fold_steal": 0, "fused_scan": 0, "map_lockstep_min": 0, "map_threads": 0,
-                                  "map_group_max": 0}
+                                  "map_group_max": 0, "batch_no_fill": 0}
