@@ -1010,10 +1010,10 @@ bool walk_threads_ok(int t) { return t == 128 || t == 256 || t == 512 || t == 10
 // The walking-fold shape for CTAs of T threads, `pair` (two periods per
 // lane), a group cap (0: the rule's MAX_GROUP; a tuned cap may reach
 // WALK_MAX_GROUP, with lane sets down to WALK_MIN_LANES lanes) and a lockstep
-// threshold. `fill`: groups are cut until the launch gives every SM a CTA
-// (else only to the periods there are: callers whose launch holds many such
-// jobs). False when one lane set's histograms do not fit.
-bool walk_shape_for(int nb, int periods, int sm_count, int T, bool pair, uint32_t gcap, int lockstep, bool fill,
+// threshold. Groups are cut until the fold has at least `fill_ctas` CTAs
+// (0: only to the periods there are, for callers whose launch holds many
+// such jobs). False when one lane set's histograms do not fit.
+bool walk_shape_for(int nb, int periods, int T, bool pair, uint32_t gcap, int lockstep, int fill_ctas,
                     FoldShape* out) {
     FoldShape s{};
     s.kind = FOLD_WALK;
@@ -1033,7 +1033,7 @@ bool walk_shape_for(int nb, int periods, int sm_count, int T, bool pair, uint32_
     while (2 * g <= gmax && lanes(2 * g) >= WALK_MIN_LANES &&
            stage + starts(2 * g) + (size_t)(2 * g) * hist_per <= MAX_FOLD_SMEM)
         g *= 2;
-    while (g > PV && (g / 2 >= periods || (fill && (periods + g - 1) / g < sm_count))) g /= 2;
+    while (g > PV && (g / 2 >= periods || (periods + g - 1) / g < fill_ctas)) g /= 2;
     while (gcap && g > PV && (uint32_t)g > gcap) g /= 2;
     s.group = g;
     s.hist_in_smem = true;
@@ -1046,7 +1046,7 @@ bool walk_shape_for(int nb, int periods, int sm_count, int T, bool pair, uint32_
     return true;
 }
 
-bool walk_shape(int nb, int periods, int sm_count, bool tuned, bool fill_sms, FoldShape* out) {
+bool walk_shape(int nb, int periods, bool tuned, int fill_ctas, FoldShape* out) {
     const int cls = nb_class(nb);
     int T = 1024, lockstep = 0;
     bool pair = false;
@@ -1057,9 +1057,8 @@ bool walk_shape(int nb, int periods, int sm_count, bool tuned, bool fill_sms, Fo
         lockstep = (int)g_lockstep[cls].load(std::memory_order_relaxed);
     }
     const uint32_t gcap = group_cap(nb);
-    if (pair && walk_shape_for(nb, periods, sm_count, T > 512 ? 512 : T, true, gcap, lockstep, fill_sms, out))
-        return true;
-    return walk_shape_for(nb, periods, sm_count, T, false, gcap, lockstep, fill_sms, out);
+    if (pair && walk_shape_for(nb, periods, T > 512 ? 512 : T, true, gcap, lockstep, fill_ctas, out)) return true;
+    return walk_shape_for(nb, periods, T, false, gcap, lockstep, fill_ctas, out);
 }
 
 }  // namespace
@@ -1070,8 +1069,8 @@ FoldShape fold_map_shape(int nb, int periods, int sm_count) {
     FoldShape w;
     // A tuned cap drops the fill rule: a map batch's launch holds every
     // star's groups.
-    if (walk_shape_for(nb, periods, sm_count, t ? (int)t : 1024, false, gcap,
-                       (int)g_map_lockstep.load(std::memory_order_relaxed), gcap == 0, &w))
+    if (walk_shape_for(nb, periods, t ? (int)t : 1024, false, gcap, (int)g_map_lockstep.load(std::memory_order_relaxed),
+                       gcap == 0 ? sm_count : 0, &w))
         return w;
     return fold_group_shape(nb, periods, sm_count);
 }
@@ -1082,9 +1081,10 @@ FoldShape fold_map_shape(int nb, int periods, int sm_count) {
 // STAGE_MAX); the CTA has 1024 threads, or 512 when segments would
 // otherwise be shorter than 16 observations. A single period whose
 // histogram does not fit folds into global scratch.
-FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned, bool fill_sms) {
+FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned, int fill_ctas) {
+    if (fill_ctas < 0) fill_ctas = sm_count;
     FoldShape w;
-    if (walk_shape(nb, periods, sm_count, tuned, fill_sms, &w)) return w;
+    if (walk_shape(nb, periods, tuned, fill_ctas, &w)) return w;
     FoldShape s{};
     s.kind = FOLD_SMEM;
     s.row_stride = nb | 1;
@@ -1092,7 +1092,7 @@ FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned, bool f
     const size_t stage_min = SLOT_BYTES * (2048 + 1024) + 4 * (1024 + 32);
     int g = 1;
     while (g < MAX_GROUP && (size_t)(2 * g) * hist_per + stage_min <= MAX_FOLD_SMEM) g *= 2;
-    const int fill = fill_sms ? (periods + sm_count - 1) / sm_count : periods;
+    const int fill = fill_ctas > 0 ? (periods + fill_ctas - 1) / fill_ctas : periods;
     while (g > 1 && g / 2 >= fill) g /= 2;
     const uint32_t gcap = group_cap(nb);
     while (gcap && g > 1 && (uint32_t)g > gcap) g /= 2;

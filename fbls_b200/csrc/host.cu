@@ -117,7 +117,7 @@ struct Pass {
     BandOut out;
     fbls_scan_stats st{};
     bool bad = false;  // a template's precision came out nonpositive
-    bool fill_sms = true;  // the fold's groups are cut so this pass alone gives every SM a CTA
+    int fill_ctas = -1;  // the fold's groups are cut to give it this many CTAs (-1: one per SM; 0: no cut)
     std::string err;   // plan_pass's message when it rejects the pass
     int fail(int status, const char* message) {
         err = message;
@@ -187,7 +187,7 @@ int plan_pass(const fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
     if (launch > p.P) launch = p.P;
     p.batch = batch;
     p.launch = launch;
-    p.shape = fold_group_shape((int)nb, (int)launch, ctx->sm_count, true, p.fill_sms);
+    p.shape = fold_group_shape((int)nb, (int)launch, ctx->sm_count, true, p.fill_ctas);
     p.chunks.resize((size_t)r->n + 2);
     const int count = fold_chunks(r->time_host.data(), (int)r->n, scale_max, (int)nb, p.shape.span_cap,
                                   p.shape.chunk_cap, p.chunks.data(), (int)p.chunks.size());
@@ -859,10 +859,18 @@ int scan_bands(fbls_ctx* ctx, std::vector<BandJob>& jobs, int mode, bool fused) 
         p.bank = j.bank;
         p.nb = (uint32_t)(j.coarse ? j.nb / j.bank->prescan_factor : j.nb);
         p.mode = mode;
-        p.fill_sms = !(fused && tuned_batch_no_fill());
         j.first = (int)first.size();
         first.push_back(std::move(p));
     }
+    // Job launches hold a session's passes together, so a pass's fold needs
+    // only its share of the SMs (or, tuned, no cut at all).
+    auto share = [&](std::vector<Pass>& passes) {
+        if (!fused) return;
+        const int n = (int)passes.size();
+        const int ctas = tuned_batch_no_fill() ? 0 : std::max(1, (ctx->sm_count + n - 1) / std::max(n, 1));
+        for (Pass& p : passes) p.fill_ctas = ctas;
+    };
+    share(first);
     int rc = plan_passes(ctx, first);
     if (rc) return rc;
     const double t0 = now_seconds();
@@ -892,10 +900,10 @@ int scan_bands(fbls_ctx* ctx, std::vector<BandJob>& jobs, int mode, bool fused) 
         p.bank = j.bank;
         p.nb = (uint32_t)j.nb;
         p.mode = mode;
-        p.fill_sms = !(fused && tuned_batch_no_fill());
         j.second = (int)second.size();
         second.push_back(std::move(p));
     }
+    share(second);
     rc = plan_passes(ctx, second);
     if (rc) return rc;
     rc = session(second, ctx->pin_down2);

@@ -104,7 +104,7 @@ struct FoldTuning {
     uint32_t map_lockstep_min;  // the coarse maps' folds: lockstep threshold (0: built-in)
     uint32_t map_threads;       // the coarse maps' walking folds: CTA size (0: 1024)
     uint32_t map_group_max;     // the coarse maps' walking folds: largest period group (0: built-in)
-    uint32_t batch_no_fill;     // nonzero: a batch's job launches do not cut a pass's groups to fill the SMs
+    uint32_t batch_no_fill;     // nonzero: a batch's job launches never cut a pass's groups (else to its share of the SMs)
 };
 
 struct ScanArgs {
@@ -229,9 +229,9 @@ struct BiweightArgs {
 // Launch shape of a fold of `periods` periods at nb bins. `tuned`: the
 // walking fold takes its CTA size and lockstep threshold from the tuning
 // table (callers whose job launches mix shapes keep 1024 threads).
-// `fill_sms`: period groups are cut until the launch gives every SM a CTA
-// (false: a job launch holding many such folds).
-FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned = false, bool fill_sms = true);
+// `fill_ctas`: period groups are cut until the fold has at least this many
+// CTAs (-1: sm_count; 0: no cut, for a job launch holding many such folds).
+FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned = false, int fill_ctas = -1);
 // The coarse maps' fold shape: the walking fold with the tuning table's map
 // CTA size, group cap (nonzero: groups up to the cap whatever the SM count,
 // as a batch's launch holds every star's groups) and lockstep threshold,

@@ -273,9 +273,10 @@ int fbls_timer_stop(fbls_ctx* ctx, float* milliseconds);
  * coarse maps' walking folds' CTA size (as fold_threads) and largest period
  * group (as fold_group_max, but a nonzero cap is taken whatever the SM count:
  * a map batch's launch holds every star's groups), one value for every nb.
- * batch_no_fill (0 or 1): 1 keeps a pass's period groups whole in
- * fbls_search_batch's job launches (workers 0), where the default cuts them
- * until the pass alone would give every SM a CTA.
+ * batch_no_fill (0 or 1): in fbls_search_batch's job launches (workers 0),
+ * which hold many passes (star, band, prescan or full scan) together, the
+ * default cuts a pass's period groups until it has its share of CTAs
+ * (ceil(SMs / passes of the launch session)); 1 never cuts them.
  * Process-wide; results do not depend on it, only the launch shapes do. */
 typedef struct {
     uint32_t fold_group_max[32];
