@@ -613,6 +613,22 @@ def run_survey(args):
         torch.distributed.destroy_process_group()
 
 
+def _kernel_table(path, steps):
+    """One run of each step under torch.profiler (CUDA activity only):
+    the device time of every kernel and copy, written as text tables."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    out = []
+    for name, fn in steps.items():
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize()
+        out.append(f"## {name}\n\n" + prof.key_averages().table(sort_by="cuda_time_total", row_limit=16,
+                                                                   max_name_column_width=48))
+    Path(path).write_text("\n\n".join(out) + "\n")
+
+
 def run_proposal(args):
     """Proposal-pruned search against the exhaustive search on the survey
     workload: both timed on the same resident stars (host clock around the
@@ -654,6 +670,8 @@ def run_proposal(args):
         t_pr.append(time.perf_counter() - t0)
         parts = dict(pr.search_proposed.last_ms)
     gc.enable()
+    if args.kernel_table:
+        _kernel_table(args.kernel_table, {"exhaustive batch": exhaustive, "proposal step": proposed})
     hits = labelled = 0
     for (fr, _, _), (pr_rows, _, _) in zip(full, pruned):
         if fr.shape[0] == 0:
@@ -1248,6 +1266,9 @@ def main():
                     help="default workload, 1 GPU: survey stars for the metric's survey and proposal keys (0: none)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--kernel-table", default=None,
+                    help="proposal workload: after the timed steps, write the device time per kernel of one "
+                         "exhaustive and one proposal step (torch.profiler, CUPTI) to this file")
     args = ap.parse_args()
     if args.stars is None:
         args.stars = 10000 if args.workload == "full" else 512
