@@ -615,17 +615,20 @@ def run_survey(args):
 
 def _kernel_table(path, steps):
     """One run of each step under torch.profiler (CUDA activity only):
-    the device time of every kernel and copy, written as text tables."""
+    the step's host-clock time and the device time of every kernel and copy,
+    written as text tables."""
     import torch
     from torch.profiler import ProfilerActivity, profile
     out = []
     for name, fn in steps.items():
         torch.cuda.synchronize()
         with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            t0 = time.perf_counter()
             fn()
             torch.cuda.synchronize()
-        out.append(f"## {name}\n\n" + prof.key_averages().table(sort_by="cuda_time_total", row_limit=16,
-                                                                   max_name_column_width=48))
+            wall = time.perf_counter() - t0
+        out.append(f"## {name} ({1e3 * wall:.1f} ms host clock, under the profiler)\n\n" +
+                   prof.key_averages().table(sort_by="cuda_time_total", row_limit=16, max_name_column_width=48))
     Path(path).write_text("\n\n".join(out) + "\n")
 
 
@@ -671,7 +674,15 @@ def run_proposal(args):
         parts = dict(pr.search_proposed.last_ms)
     gc.enable()
     if args.kernel_table:
-        _kernel_table(args.kernel_table, {"exhaustive batch": exhaustive, "proposal step": proposed})
+        # the proposal step whole, then its coarse maps and its pruned search
+        # (the last step's bands) apart
+        ranges = [pr.ranges_for(l, args.bands) for l in logits]
+        _kernel_table(args.kernel_table, {
+            "exhaustive batch": exhaustive, "proposal step": proposed,
+            "coarse maps": lambda: pr.features(gpu, pstars, devs, net.bin_days, device=True,
+                                               oversample=net.map_oversample),
+            "pruned search": lambda: gpu.search_batch(states, cfg, period_max=pmax, devs=devs,
+                                                      workers=args.batch_workers, ranges=ranges)})
     hits = labelled = 0
     for (fr, _, _), (pr_rows, _, _) in zip(full, pruned):
         if fr.shape[0] == 0:
@@ -1214,9 +1225,30 @@ def run_precision_report(args):
 
 
 def run_profile_case(args):
-    """One bounded scan_bank pass for profiler captures: the 13-sector star's
-    octave band [8, 16) d at its coarse grid (1536 bins), first 4096 periods:
-    one k_fold, one k_scan_tiles and one k_merge launch, ~0.6 GB on device."""
+    """One bounded launch set for profiler captures. fold: one scan_bank pass
+    of the 13-sector star's octave band [8, 16) d at its coarse grid (1536
+    bins), first 4096 periods: one k_fold, one k_scan_tiles and one k_merge
+    launch, ~0.6 GB on device. maps: the coarse maps of args.stars seeded
+    survey stars in one fbls_coarse_features call: one k_bin_fields_jobs, one
+    k_fold_walk_jobs and one k_map_features launch."""
+    if args.profile_case == "maps":
+        from fbls_b200 import api
+        from fbls_b200 import proposal as pr
+        stars, _ = _survey(args.stars, 1000)
+        pstars = [(s, p) for _, s, p in stars]
+        saved = np.load(pr.WEIGHTS)
+        with api.Gpu(0) as gpu:
+            devs = [gpu.upload(s) for s, _ in pstars]
+            gpu.counters(reset=True)
+            t0 = time.perf_counter()
+            pr.features(gpu, pstars, devs, float(saved["bin_days"]), oversample=float(saved["map_oversample"]))
+            ms = 1e3 * (time.perf_counter() - t0)
+            ctr = gpu.counters()
+            for d in devs:
+                d.free()
+        print(json.dumps({"case": "maps", "stars": len(pstars), "observations": sum(s.n for s, _ in pstars),
+                          "ms": ms, "fold_updates": ctr["fold_updates"], "launches": ctr["launches"]}))
+        return
     from fbls_b200 import api, synth
     curve, cfg = synth.multi_sector(), synth.multi_sector_config()
     state = api.prepared_family(curve.time, curve.flux, curve.flux_err, cfg)
@@ -1238,7 +1270,7 @@ def run_profile_case(args):
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--profile-case", choices=["fold"], default=None,
+    ap.add_argument("--profile-case", choices=["fold", "maps"], default=None,
                     help="run one bounded launch set for profiler captures instead of the benchmark")
     ap.add_argument("--precision-report", action="store_true",
                     help="compare the mixed f32/f64 ranking with f64 ranking on every period (one JSON line)")
