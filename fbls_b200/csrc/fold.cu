@@ -1183,6 +1183,27 @@ int fold_chunks(const double* time, int n, double scale_max, int nb, int span_ca
     return count;
 }
 
+int fold_chunk_list(const double* time, int n, double scale_max, int nb, int span_cap, int chunk_cap,
+                    std::vector<int>& out) {
+    const size_t full = (size_t)(n > 0 ? n : 0) + 2;
+    size_t cap = full;
+    if (n > 0 && chunk_cap > 0 && scale_max > 0.0) {
+        const int cells = (nb < span_cap ? nb : span_cap) - 4;
+        const double span = (double)(cells > 1 ? cells : 1) / scale_max;
+        const double by_time = (time[n - 1] - time[0]) / span * (1.0 + 1e-9);
+        if (by_time >= 0.0 && by_time < (double)n) cap = (size_t)by_time + (size_t)(n / chunk_cap) + 4;
+        if (cap > full) cap = full;
+    }
+    out.resize(cap);
+    int count = fold_chunks(time, n, scale_max, nb, span_cap, chunk_cap, out.data(), (int)out.size());
+    if (count < 0 && cap < full) {  // the bound was short (it is not expected to be): the full size
+        out.resize(full);
+        count = fold_chunks(time, n, scale_max, nb, span_cap, chunk_cap, out.data(), (int)out.size());
+    }
+    if (count >= 0) out.resize((size_t)count + 1);
+    return count;
+}
+
 // A CTA size and form of the walking fold: a power of two from 128 to 1024
 // threads, at most 512 paired.
 static bool walk_form_ok(int threads, bool pair) { return walk_threads_ok(threads) && (!pair || threads <= 512); }

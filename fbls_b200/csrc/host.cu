@@ -188,11 +188,9 @@ int plan_pass(const fbls_ctx* ctx, const fbls_ready* r, Pass& p) {
     p.batch = batch;
     p.launch = launch;
     p.shape = fold_group_shape((int)nb, (int)launch, ctx->sm_count, true, p.fill_ctas);
-    p.chunks.resize((size_t)r->n + 2);
-    const int count = fold_chunks(r->time_host.data(), (int)r->n, scale_max, (int)nb, p.shape.span_cap,
-                                  p.shape.chunk_cap, p.chunks.data(), (int)p.chunks.size());
+    const int count = fold_chunk_list(r->time_host.data(), (int)r->n, scale_max, (int)nb, p.shape.span_cap,
+                                      p.shape.chunk_cap, p.chunks);
     if (count < 1) return p.fail(FBLS_ERR_ARGUMENT, "fold chunking failed");
-    p.chunks.resize((size_t)count + 1);
     // Device input region: scales | periods | bank | chunks; output region:
     // records | score | depth | flags.
     p.in_scales = 0;

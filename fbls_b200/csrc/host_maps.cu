@@ -104,11 +104,9 @@ int plan_map(const fbls_ctx* ctx, MapPlan& m) {
         const size_t stride = 2 * (size_t)nb + 1;
         g.per_launch = (uint32_t)std::max<size_t>(1, std::min<size_t>(16384, (512ull << 20) / (NF * stride * 12)));
         g.shape = fold_map_shape((int)nb, (int)std::min(g.count, g.per_launch), ctx->sm_count);
-        g.chunks.resize((size_t)ready->n + 2);
-        const int c = fold_chunks(ready->time_host.data(), (int)ready->n, scale_max, (int)nb, g.shape.span_cap,
-                                  g.shape.chunk_cap, g.chunks.data(), (int)g.chunks.size());
+        const int c = fold_chunk_list(ready->time_host.data(), (int)ready->n, scale_max, (int)nb, g.shape.span_cap,
+                                      g.shape.chunk_cap, g.chunks);
         if (c < 1) return bad(FBLS_ERR_ARGUMENT, "fold chunking failed");
-        g.chunks.resize((size_t)c + 1);
         g.off_scales = in_bytes;
         in_bytes += align256(g.count * sizeof(double));
         g.off_chunks = in_bytes;

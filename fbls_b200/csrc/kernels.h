@@ -4,6 +4,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <vector>
 
 namespace fbls {
 
@@ -248,6 +249,12 @@ bool tuned_fold_steal();
 // Writes count + 1 offsets; returns count, or -1 when capacity is too small.
 int fold_chunks(const double* time, int n, double scale_max, int nb, int span_cap, int chunk_cap, int* out,
                 int capacity);
+// fold_chunks into `out` (count + 1 offsets), sized by a bound on the count
+// rather than by n: every chunk but the last ends after chunk_cap
+// observations or at least a span after its first, so there are at most
+// (t_last - t_first) / span + n / chunk_cap + 1 of them.
+int fold_chunk_list(const double* time, int n, double scale_max, int nb, int span_cap, int chunk_cap,
+                    std::vector<int>& out);
 cudaError_t launch_fold(const FoldArgs& a, const FoldShape& shape, cudaStream_t stream);
 // The walking fold with the tile scan and merge fused (FOLD_WALK shapes, no
 // map or histogram output): the prefix rows stay in shared memory, every CTA
