@@ -1075,12 +1075,14 @@ FoldShape fold_map_shape(int nb, int periods, int sm_count) {
     return fold_group_shape(nb, periods, sm_count);
 }
 
-// Launch shape: the largest power-of-two period group (<= 32 and at most
-// enough to give every SM one CTA) whose histograms leave room to stage at
-// least 2048 observations; the staging capacity is what is left (up to
-// STAGE_MAX); the CTA has 1024 threads, or 512 when segments would
-// otherwise be shorter than 16 observations. A single period whose
-// histogram does not fit folds into global scratch.
+// Launch shape: the walking fold's (walk_shape) where one lane set's
+// histograms fit beside its staging buffers; else k_fold's: the largest
+// power-of-two period group (<= 32 and at most enough to give the fold
+// fill_ctas CTAs) whose histograms leave room to stage at least 2048
+// observations; the staging capacity is what is left (up to STAGE_MAX); the
+// CTA has 1024 threads, or 512 when segments would otherwise be shorter than
+// 16 observations. A single period whose histogram does not fit folds into
+// global scratch.
 FoldShape fold_group_shape(int nb, int periods, int sm_count, bool tuned, int fill_ctas) {
     if (fill_ctas < 0) fill_ctas = sm_count;
     FoldShape w;

@@ -76,7 +76,7 @@ struct FoldArgs {
 // Launch shape of the fold (fold_group_shape).
 struct FoldShape {
     int kind;           // FOLD_WALK (k_fold_walk) or FOLD_SMEM (k_fold)
-    int group;          // periods per CTA, a power of two <= MAX_GROUP
+    int group;          // periods per CTA, a power of two <= MAX_GROUP (FOLD_WALK: <= WALK_MAX_GROUP)
     bool hist_in_smem;  // else window mode: 3 G nb doubles of global histogram per CTA
     int window;         // 0 (full mode) or the window's rows (cells)
     int row_stride;     // shared-memory row stride of a period's bins
